@@ -1,0 +1,124 @@
+"""ctypes binding of the C ABI in include/abhsf/abhsf_gpu.h.
+
+Loads the in-tree abhsf_b200/libabhsf_b200.so.  There is no fallback: if the
+library is missing, importing this module raises, naming the build command.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libabhsf_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "abhsf", "abhsf_gpu.h")
+
+SUCCESS, INVALID_VALUE, INDEX_OUT_OF_RANGE, DUPLICATE_ENTRY, OUT_OF_MEMORY, UNSUPPORTED, CUDA_ERROR = range(7)
+SCHEME_COO, SCHEME_CSR, SCHEME_BITMAP, SCHEME_DENSE = range(4)
+SCHEME_NAMES = ("coo", "csr", "bitmap", "dense")
+VALUE_TYPES = {"f64": 0, "f32": 1, "bf16": 2}
+MATRIX_TYPES = {"binary": 0, "integer": 1, "real": 2, "complex": 3}
+
+
+class AbhsfError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"abhsf status {status}: {msg}")
+        self.status = status
+
+
+class InvalidValue(AbhsfError, ValueError):
+    pass
+
+
+class IndexOutOfRange(AbhsfError, IndexError):
+    pass
+
+
+class DuplicateEntry(AbhsfError, ValueError):
+    pass
+
+
+class OutOfMemory(AbhsfError, MemoryError):
+    pass
+
+
+class Unsupported(AbhsfError, NotImplementedError):
+    pass
+
+
+class CudaError(AbhsfError):
+    pass
+
+
+_ERR = {INVALID_VALUE: InvalidValue, INDEX_OUT_OF_RANGE: IndexOutOfRange, DUPLICATE_ENTRY: DuplicateEntry,
+        OUT_OF_MEMORY: OutOfMemory, UNSUPPORTED: Unsupported, CUDA_ERROR: CudaError}
+
+
+class BuildOpts(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("value_type", C.c_int32), ("allow_csr", C.c_int32),
+                ("matrix_type", C.c_int32), ("forced_scheme", C.c_int32), ("inputs_on_device", C.c_int32),
+                ("bits_per_value", C.c_int64)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("nnz", C.c_int64),
+                ("block_size", C.c_int32), ("value_type", C.c_int32),
+                ("block_rows", C.c_int64), ("block_cols", C.c_int64), ("tiles", C.c_int64),
+                ("tiles_per_scheme", C.c_int64 * 4), ("nnz_per_scheme", C.c_int64 * 4),
+                ("stored_values", C.c_int64), ("payload_bytes", C.c_int64), ("format_bytes", C.c_int64),
+                ("msmf_bits", C.c_uint64 * 8)]
+
+
+_vp = C.c_void_p
+_i64 = C.c_int64
+_i32 = C.c_int32
+_u64p = C.POINTER(C.c_uint64)
+
+# name -> (restype, argtypes)
+PROTOTYPES = {
+    "abhsf_abi_version": (_i32, []),
+    "abhsf_last_error_string": (C.c_char_p, []),
+    "abhsf_build_opts_default": (None, [C.POINTER(BuildOpts)]),
+    "abhsf_build": (C.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, C.POINTER(BuildOpts), _vp, C.POINTER(_vp)]),
+    "abhsf_spmv": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "abhsf_spmv_host": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "abhsf_release": (C.c_int, [_vp]),
+    "abhsf_stats_get": (C.c_int, [_vp, C.POINTER(Stats)]),
+    "abhsf_export_host": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "abhsf_block_histogram": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _i32, _i32, _vp, _u64p, _i64,
+                                        C.POINTER(_i64)]),
+    "abhsf_mmf_line": (C.c_int, [_i64, _i64, _i64, _i32, _i32, _i32, _u64p, _i64, _u64p, _u64p]),
+    "abhsf_block_scheme_bits": (C.c_uint64, [_i32, _i64, _i64, _i64, _i64]),
+    "abhsf_block_select_scheme": (_i32, [_i64, _i64, _i64, _i64, _i32, _i32]),
+}
+
+
+def header_functions(path: str = HEADER) -> list[str]:
+    """Names of the functions include/abhsf/*.h declares with ABHSF_API."""
+    names = []
+    hdir = os.path.dirname(path)
+    for fn in sorted(os.listdir(hdir)):
+        if fn.endswith(".h"):
+            names += re.findall(r"ABHSF_API[^;(]*?\b(abhsf_\w+)\s*\(", open(os.path.join(hdir, fn)).read())
+    return names
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m abhsf_b200.build` "
+                          "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in PROTOTYPES.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+lib = _load()
+
+
+def check(status: int) -> None:
+    if status != SUCCESS:
+        msg = lib.abhsf_last_error_string().decode(errors="replace")
+        raise _ERR.get(status, AbhsfError)(status, msg)

@@ -1,0 +1,181 @@
+// capi.cu -- the extern "C" boundary declared in include/abhsf/abhsf_gpu.h.
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <string>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace abhsf {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+void clear_last_error() { g_last_error.clear(); }
+
+}  // namespace abhsf
+
+using abhsf::fail;
+using abhsf::guarded;
+
+extern "C" {
+
+int32_t abhsf_abi_version(void) { return ABHSF_ABI_VERSION; }
+
+const char* abhsf_last_error_string(void) { return abhsf::g_last_error.c_str(); }
+
+void abhsf_build_opts_default(abhsf_build_opts* o)
+{
+    if (!o)
+        return;
+    o->block_size = 64;
+    o->value_type = ABHSF_VALUE_F64;
+    o->allow_csr = 1;
+    o->matrix_type = ABHSF_MATRIX_REAL;
+    o->forced_scheme = -1;
+    o->inputs_on_device = 0;
+    o->bits_per_value = 0;
+}
+
+abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, const double* vals, int64_t nnz, int64_t m,
+                         int64_t n, const abhsf_build_opts* opts, abhsf_stream_t stream, abhsf_matrix** out)
+{
+    return guarded([&] {
+        if (!out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "out must be non-NULL");
+        *out = nullptr;
+        abhsf_build_opts o;
+        abhsf_build_opts_default(&o);
+        if (opts)
+            o = *opts;
+        auto a = std::make_unique<abhsf_matrix>();
+        abhsf::build_matrix(rows, cols, vals, nnz, m, n, o, reinterpret_cast<cudaStream_t>(stream), *a);
+        *out = a.release();
+    });
+}
+
+abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double* y, abhsf_stream_t stream)
+{
+    return guarded([&] {
+        if (!a)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle is NULL");
+        if (a->value_type != ABHSF_VALUE_F64)
+            fail(ABHSF_ERROR_INVALID_VALUE, "abhsf_spmv needs a matrix stored as f64");
+        if ((!x && a->n) || (!y && a->m))
+            fail(ABHSF_ERROR_INVALID_VALUE, "x and y must be non-NULL");
+        if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 7)
+            fail(ABHSF_ERROR_INVALID_VALUE, "x and y must be 8-byte aligned");
+        abhsf::spmv_f64(*a, x, y, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+abhsf_status abhsf_spmv_host(abhsf_matrix* a, const double* x, double* y, abhsf_stream_t stream)
+{
+    return guarded([&] {
+        if (!a)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle is NULL");
+        if (a->value_type != ABHSF_VALUE_F64)
+            fail(ABHSF_ERROR_INVALID_VALUE, "abhsf_spmv_host needs a matrix stored as f64");
+        if ((!x && a->n) || (!y && a->m))
+            fail(ABHSF_ERROR_INVALID_VALUE, "x and y must be non-NULL");
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        if (!a->x_stage.get() || a->x_stage.size() < (size_t)a->n)
+            a->x_stage.alloc(a->n);
+        if (!a->y_stage.get() || a->y_stage.size() < (size_t)a->m)
+            a->y_stage.alloc(a->m);
+        ABHSF_CUDA(cudaMemcpyAsync(a->x_stage.get(), x, a->n * sizeof(double), cudaMemcpyHostToDevice, st));
+        ABHSF_CUDA(cudaMemcpyAsync(a->y_stage.get(), y, a->m * sizeof(double), cudaMemcpyHostToDevice, st));
+        abhsf::spmv_f64(*a, a->x_stage.get(), a->y_stage.get(), st);
+        ABHSF_CUDA(cudaMemcpyAsync(y, a->y_stage.get(), a->m * sizeof(double), cudaMemcpyDeviceToHost, st));
+        ABHSF_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+abhsf_status abhsf_release(abhsf_matrix* a)
+{
+    return guarded([&] { delete a; });
+}
+
+abhsf_status abhsf_stats_get(const abhsf_matrix* a, abhsf_stats* out)
+{
+    return guarded([&] {
+        if (!a || !out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle and out must be non-NULL");
+        *out = a->stats;
+    });
+}
+
+abhsf_status abhsf_export_host(const abhsf_matrix* a, int64_t* brow_ptr, uint32_t* tile_col, uint32_t* tile_nnz,
+                               uint8_t* tile_scheme, int64_t* tile_val_off, int64_t* tile_idx_off, uint8_t* payload,
+                               void* values)
+{
+    return guarded([&] {
+        if (!a)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle is NULL");
+        auto cp = [](void* dst, const void* src, size_t bytes) {
+            if (dst && bytes)
+                ABHSF_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+        };
+        cp(brow_ptr, a->brow_ptr.get(), (a->M + 1) * sizeof(int64_t));
+        cp(tile_col, a->tile_col.get(), a->T * sizeof(uint32_t));
+        cp(tile_nnz, a->tile_nnz.get(), a->T * sizeof(uint32_t));
+        cp(tile_scheme, a->tile_scheme.get(), a->T);
+        cp(tile_val_off, a->tile_val_off.get(), (a->T + 1) * sizeof(int64_t));
+        cp(tile_idx_off, a->tile_idx_off.get(), (a->T + 1) * sizeof(int64_t));
+        cp(payload, a->payload.get(), a->payload_bytes);
+        cp(values, a->values.get(), a->n_values * abhsf::value_size(a->value_type));
+    });
+}
+
+abhsf_status abhsf_block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n,
+                                   int32_t r, int32_t s, int32_t inputs_on_device, abhsf_stream_t stream,
+                                   uint64_t* hist, int64_t hist_len, int64_t* blocks)
+{
+    return guarded([&] {
+        abhsf::block_histogram(rows, cols, nnz, m, n, r, s, inputs_on_device != 0,
+                               reinterpret_cast<cudaStream_t>(stream), hist, hist_len, blocks);
+    });
+}
+
+abhsf_status abhsf_mmf_line(int64_t m, int64_t n, int64_t nnz, int32_t matrix_type, int32_t r, int32_t s,
+                            const uint64_t* hist, int64_t hist_len, uint64_t out_single[8], uint64_t out_double[8])
+{
+    return guarded([&] {
+        if (m <= 0 || n <= 0 || nnz < 0 || r <= 0 || s <= 0 || hist_len < 0 || (hist_len && !hist) ||
+            !out_single || !out_double)
+            fail(ABHSF_ERROR_INVALID_VALUE, "invalid mmf_line arguments");
+        if (matrix_type < 0 || matrix_type > 3)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix_type out of range");
+        // block_statistics/mmf.cpp:34-47
+        const uint64_t bits1 = (matrix_type == ABHSF_MATRIX_INTEGER || matrix_type == ABHSF_MATRIX_REAL) ? 32
+                               : matrix_type == ABHSF_MATRIX_COMPLEX                                    ? 64
+                                                                                                        : 0;
+        std::map<uint64_t, uint64_t> h;
+        for (int64_t z = 0; z < hist_len; ++z)
+            if (hist[z])
+                h[(uint64_t)z] = hist[z];
+        abhsf::mmf_line_from_hist(m, n, nnz, matrix_type, r, s, h, bits1, out_single, out_double);
+    });
+}
+
+uint64_t abhsf_block_scheme_bits(int32_t scheme, int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value)
+{
+    switch (scheme) {
+    case ABHSF_SCHEME_COO: return abhsf_coo_bits(r, s, nnz);
+    case ABHSF_SCHEME_CSR: return abhsf_csr_bits(r, s, nnz);
+    case ABHSF_SCHEME_BITMAP: return abhsf_bitmap_bits(r, s);
+    case ABHSF_SCHEME_DENSE: return abhsf_dense_bits(r, s, nnz, bits_per_value);
+    default: return UINT64_MAX;
+    }
+}
+
+int32_t abhsf_block_select_scheme(int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value, int32_t is_binary,
+                                  int32_t allow_csr)
+{
+    return abhsf_select_scheme(r, s, nnz, bits_per_value, is_binary, allow_csr, nullptr);
+}
+
+}  // extern "C"

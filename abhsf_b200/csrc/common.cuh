@@ -1,0 +1,171 @@
+// common.cuh -- internal definitions shared by the ABHSF sm_100a sources.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <utility>
+
+#include "abhsf/abhsf_cost.h"
+#include "abhsf/abhsf_gpu.h"
+
+namespace abhsf {
+
+// Thrown inside the library, caught at every extern "C" boundary.
+struct error {
+    abhsf_status status;
+    std::string msg;
+};
+
+[[noreturn]] inline void fail(abhsf_status s, std::string msg) { throw error{s, std::move(msg)}; }
+
+inline void cuda_check(cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess)
+        return;
+    cudaGetLastError();  // clear a non-sticky error
+    if (e == cudaErrorMemoryAllocation)
+        fail(ABHSF_ERROR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+    fail(ABHSF_ERROR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define ABHSF_CUDA(call) ::abhsf::cuda_check((call), #call)
+
+void set_last_error(const std::string& msg);
+void clear_last_error();
+
+// Runs f and converts exceptions to a status; the message goes to the
+// thread's last-error string.
+template <typename F>
+abhsf_status guarded(F&& f) noexcept
+{
+    try {
+        f();
+        clear_last_error();
+        return ABHSF_SUCCESS;
+    } catch (const error& e) {
+        set_last_error(e.msg);
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return ABHSF_ERROR_OUT_OF_MEMORY;
+    } catch (...) {
+        set_last_error("unknown internal error");
+        return ABHSF_ERROR_CUDA;
+    }
+}
+
+// Owning device allocation (cudaMalloc / cudaFree).
+template <typename T>
+class dbuf {
+  public:
+    dbuf() = default;
+    explicit dbuf(size_t count) { alloc(count); }
+    ~dbuf() { reset(); }
+    dbuf(const dbuf&) = delete;
+    dbuf& operator=(const dbuf&) = delete;
+    dbuf(dbuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+    dbuf& operator=(dbuf&& o) noexcept
+    {
+        if (this != &o) {
+            reset();
+            p_ = o.p_; n_ = o.n_;
+            o.p_ = nullptr; o.n_ = 0;
+        }
+        return *this;
+    }
+    void alloc(size_t count)
+    {
+        reset();
+        if (count == 0)
+            count = 1;
+        ABHSF_CUDA(cudaMalloc(reinterpret_cast<void**>(&p_), count * sizeof(T)));
+        n_ = count;
+    }
+    void reset()
+    {
+        if (p_)
+            cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    T* release() { T* p = p_; p_ = nullptr; n_ = 0; return p; }
+    T* get() const { return p_; }
+    size_t size() const { return n_; }
+
+  private:
+    T* p_ = nullptr;
+    size_t n_ = 0;
+};
+
+// Plain view of a built matrix passed to kernels by value.
+struct tiles_view {
+    int64_t m, n, M;
+    const int64_t* brow_ptr;
+    const uint32_t* tile_col;
+    const uint32_t* tile_nnz;
+    const uint8_t* tile_scheme;
+    const int64_t* tile_val_off;
+    const int64_t* tile_idx_off;
+    const uint8_t* payload;
+    const void* values;
+};
+
+inline int log2_exact(int64_t s)
+{
+    int lg = 0;
+    while ((int64_t(1) << lg) < s)
+        ++lg;
+    return (int64_t(1) << lg) == s ? lg : -1;
+}
+
+inline int bit_length(uint64_t v)
+{
+    int b = 0;
+    while (b < 64 && (v >> b) != 0)
+        ++b;
+    return b;
+}
+
+inline int64_t pad16(int64_t b) { return (b + 15) & ~int64_t(15); }
+
+inline size_t value_size(int vt) { return vt == ABHSF_VALUE_F64 ? 8 : vt == ABHSF_VALUE_F32 ? 4 : 2; }
+
+__host__ __device__ inline int64_t tile_payload_bytes(int scheme, int64_t s, int64_t nnz)
+{
+    switch (scheme) {
+    case ABHSF_SCHEME_COO: return (2 * nnz + 15) & ~int64_t(15);
+    case ABHSF_SCHEME_CSR: return (2 * s + nnz + 15) & ~int64_t(15);
+    case ABHSF_SCHEME_BITMAP: return (s * s / 8 + 15) & ~int64_t(15);
+    default: return 0;
+    }
+}
+
+}  // namespace abhsf
+
+// The handle behind abhsf_matrix*.
+struct abhsf_matrix {
+    int64_t m = 0, n = 0, nnz = 0;
+    int32_t s = 0, lg = 0, value_type = ABHSF_VALUE_F64, matrix_type = ABHSF_MATRIX_REAL;
+    int64_t M = 0, N = 0, T = 0, n_values = 0, payload_bytes = 0;
+    int device = 0;
+    abhsf::dbuf<int64_t> brow_ptr;
+    abhsf::dbuf<uint32_t> tile_col;
+    abhsf::dbuf<uint32_t> tile_nnz;
+    abhsf::dbuf<uint8_t> tile_scheme;
+    abhsf::dbuf<int64_t> tile_val_off;
+    abhsf::dbuf<int64_t> tile_idx_off;
+    abhsf::dbuf<uint8_t> payload;
+    abhsf::dbuf<uint8_t> values;  // n_values * value_size(value_type) bytes
+    abhsf_stats stats{};
+    // staging for abhsf_spmv_host
+    abhsf::dbuf<double> x_stage, y_stage;
+
+    abhsf::tiles_view view() const
+    {
+        return abhsf::tiles_view{m, n, M, brow_ptr.get(), tile_col.get(), tile_nnz.get(), tile_scheme.get(),
+                                 tile_val_off.get(), tile_idx_off.get(), payload.get(), values.get()};
+    }
+};

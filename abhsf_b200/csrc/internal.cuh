@@ -1,0 +1,22 @@
+// internal.cuh -- entry points shared between the library's translation units.
+#pragma once
+
+#include <map>
+
+#include "common.cuh"
+
+namespace abhsf {
+
+void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, int64_t nnz, int64_t m, int64_t n,
+                  const abhsf_build_opts& o, cudaStream_t st, abhsf_matrix& a);
+
+void block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r, int s,
+                     bool on_device, cudaStream_t st, uint64_t* hist, int64_t hist_len, int64_t* blocks);
+
+void mmf_line_from_hist(int64_t m, int64_t n, int64_t nnz, int type, int64_t r, int64_t s,
+                        const std::map<uint64_t, uint64_t>& hist, uint64_t bits1, uint64_t o1[8], uint64_t o2[8]);
+
+// y += A x for an f64 matrix, device pointers, ordered on st.
+void spmv_f64(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+
+}  // namespace abhsf

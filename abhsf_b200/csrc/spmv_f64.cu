@@ -1,0 +1,319 @@
+// spmv_f64.cu -- y += A x over the ABHSF format, FP64 values, sm_100a.
+//
+// One warp owns one block row (s rows of y) at a time and walks its tiles in
+// column order.  Per tile it dispatches on the scheme:
+//
+//  * bitmap / dense, s >= 32: lane l owns columns l, l+32, ... of the tile and
+//    keeps those x values in registers.  Rows are taken 16 at a time; for each
+//    row a lane loads its value when its bit is set, at the row start plus the
+//    popcount of the lower bits (so the set lanes read one contiguous run:
+//    coalesced), and accumulates value * x.  The 16 per-lane row partials are
+//    reduced by a butterfly reduce-scatter (16 shuffles for 16 rows) that
+//    leaves row r's sum on lane r.  Replaces the bit-by-bit decode loops of
+//    spmv/orig/88_bitmap.cpp:183-354 and 44_bitmap.cpp:187-396, and the dense
+//    loop of spmv/orig/88.cpp:579-605.
+//  * COO / CSR (and every scheme at s = 16): the tile's stored elements are
+//    streamed 32 at a time with coalesced loads of values and local indices;
+//    row indices come from the packed COO key or a binary search of the CSR
+//    row_end array; products are summed per row by a segmented warp reduction
+//    on the (sorted) row index.  Replaces spmv/orig/88.cpp:204-236.
+//
+// Row sums collect in a per-warp shared-memory copy of the block row's y
+// segment and are added to y once per block row: no atomics, so the result is
+// bitwise reproducible run to run.
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace abhsf {
+namespace {
+
+constexpr int kWarps = 8;
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int S>
+struct geom {
+    static constexpr int CPL = S >= 32 ? S / 32 : 1;  // x values per lane
+    static constexpr int AUX = S / 2 > 8 ? S / 2 : 8;  // u32 words of scratch per warp
+};
+
+template <int S>
+struct warp_smem {
+    double ys[S];                  // y segment of the block row
+    double xs[S];                  // x segment of the current tile (element streams)
+    uint32_t aux[geom<S>::AUX];    // bitmap chunks of a 16-row group, or CSR row_end
+    int32_t rowstart[16];
+};
+
+__device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
+__device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t* p) { return __ldcs(p); }
+
+// acc[0..15] per lane -> lane l holds sum over all lanes of acc[l & 15].
+__device__ __forceinline__ double butterfly16(double (&acc)[16], int lane)
+{
+#pragma unroll
+    for (int half = 8; half >= 1; half >>= 1) {
+        const bool upper = (lane & half) != 0;
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+            const double send = upper ? acc[i] : acc[i + half];
+            const double keep = upper ? acc[i + half] : acc[i];
+            acc[i] = keep + __shfl_xor_sync(kFull, send, half);
+        }
+    }
+    return acc[0] + __shfl_xor_sync(kFull, acc[0], 16);
+}
+
+// Bitmap tile, s >= 32.  bm32 = tile bitmap as little-endian u32 words: row
+// r's columns 32j..32j+31 are word r * CPL + j.
+template <int S>
+__device__ __forceinline__ void tile_bitmap(const uint32_t* __restrict__ bm32, const double* __restrict__ vals,
+                                            const double (&xr)[geom<S>::CPL], warp_smem<S>& sm, int lane)
+{
+    constexpr int CPL = geom<S>::CPL;
+    const uint32_t lt = (1u << lane) - 1u;
+    int running = 0;
+#pragma unroll 1
+    for (int g = 0; g < S / 16; ++g) {
+        for (int c = lane; c < 16 * CPL; c += 32)
+            sm.aux[c] = ld_stream_u32(bm32 + g * 16 * CPL + c);
+        __syncwarp();
+        int pc = 0;
+        if (lane < 16) {
+#pragma unroll
+            for (int j = 0; j < CPL; ++j)
+                pc += __popc(sm.aux[lane * CPL + j]);
+        }
+        int inc = pc;
+#pragma unroll
+        for (int d = 1; d < 16; d <<= 1) {
+            const int t = __shfl_up_sync(kFull, inc, d);
+            if (lane >= d)
+                inc += t;
+        }
+        if (lane < 16)
+            sm.rowstart[lane] = running + inc - pc;
+        running += __shfl_sync(kFull, inc, 15);
+        __syncwarp();
+        double acc[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const double* rv = vals + sm.rowstart[i];
+            int run = 0;
+            double a = 0.0;
+#pragma unroll
+            for (int j = 0; j < CPL; ++j) {
+                const uint32_t w = sm.aux[i * CPL + j];
+                double v = 0.0;
+                if ((w >> lane) & 1u)
+                    v = ld_stream(rv + run + __popc(w & lt));
+                a = fma(v, xr[j], a);
+                run += __popc(w);
+            }
+            acc[i] = a;
+        }
+        const double r = butterfly16(acc, lane);
+        if (lane < 16)
+            sm.ys[g * 16 + lane] += r;
+        __syncwarp();
+    }
+}
+
+// Dense tile, s >= 32: all s*s values, row-major.
+template <int S>
+__device__ __forceinline__ void tile_dense(const double* __restrict__ vals, const double (&xr)[geom<S>::CPL],
+                                           warp_smem<S>& sm, int lane)
+{
+    constexpr int CPL = geom<S>::CPL;
+#pragma unroll 1
+    for (int g = 0; g < S / 16; ++g) {
+        double acc[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const double* rv = vals + (size_t)(g * 16 + i) * S + lane;
+            double a = 0.0;
+#pragma unroll
+            for (int j = 0; j < CPL; ++j)
+                a = fma(ld_stream(rv + 32 * j), xr[j], a);
+            acc[i] = a;
+        }
+        const double r = butterfly16(acc, lane);
+        if (lane < 16)
+            sm.ys[g * 16 + lane] += r;
+    }
+    __syncwarp();
+}
+
+// s = 16 bitmap or dense: 32 bit positions (two rows) per step; lanes 0-15
+// take row 2i, lanes 16-31 row 2i+1.
+template <bool DENSE>
+__device__ __forceinline__ void tile_16(const uint32_t* __restrict__ bm32, const double* __restrict__ vals, double xl,
+                                        warp_smem<16>& sm, int lane)
+{
+    const uint32_t lt = (1u << lane) - 1u;
+    int running = 0;
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+        double v = 0.0;
+        if (DENSE) {
+            v = ld_stream(vals + it * 32 + lane);
+        } else {
+            const uint32_t w = ld_stream_u32(bm32 + it);
+            if ((w >> lane) & 1u)
+                v = ld_stream(vals + running + __popc(w & lt));
+            running += __popc(w);
+        }
+        double p = v * xl;
+        p += __shfl_xor_sync(kFull, p, 8);
+        p += __shfl_xor_sync(kFull, p, 4);
+        p += __shfl_xor_sync(kFull, p, 2);
+        p += __shfl_xor_sync(kFull, p, 1);
+        if ((lane & 15) == 0)
+            sm.ys[2 * it + (lane >> 4)] += p;
+    }
+    __syncwarp();
+}
+
+// COO / CSR tile: stream the z stored elements.
+template <int S, bool CSR>
+__device__ __forceinline__ void tile_stream(const uint8_t* __restrict__ pay, const double* __restrict__ vals, int z,
+                                            warp_smem<S>& sm, int lane)
+{
+    constexpr int LG = S == 16 ? 4 : S == 32 ? 5 : S == 64 ? 6 : S == 128 ? 7 : 8;
+    const uint16_t* key16 = reinterpret_cast<const uint16_t*>(pay);
+    const uint8_t* col8 = pay + 2 * S;
+    uint16_t* row_end = reinterpret_cast<uint16_t*>(sm.aux);
+    if (CSR) {
+        for (int r = lane; r < S; r += 32)
+            row_end[r] = __ldcs(key16 + r);
+        __syncwarp();
+    }
+#pragma unroll 1
+    for (int base = 0; base < z; base += 32) {
+        const int k = base + lane;
+        int lr = S;  // sentinel for idle lanes: matches no real row
+        double prod = 0.0;
+        if (k < z) {
+            int lc;
+            if (CSR) {
+                lc = __ldcs(col8 + k);
+                int lo = 0, hi = S;  // first r with row_end[r] > k
+#pragma unroll
+                for (int step = 0; step <= LG; ++step) {
+                    if (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (row_end[mid] > k)
+                            hi = mid;
+                        else
+                            lo = mid + 1;
+                    }
+                }
+                lr = lo;
+            } else {
+                const uint32_t key = __ldcs(key16 + k);
+                lr = (int)(key >> LG);
+                lc = (int)(key & (S - 1));
+            }
+            prod = ld_stream(vals + k) * sm.xs[lc];
+        }
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double o = __shfl_down_sync(kFull, prod, d);
+            const int olr = __shfl_down_sync(kFull, lr, d);
+            if (lane + d < 32 && olr == lr)
+                prod += o;
+        }
+        const int plr = __shfl_up_sync(kFull, lr, 1);
+        if (k < z && (lane == 0 || plr != lr))
+            sm.ys[lr] += prod;
+        __syncwarp();
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(kWarps * 32) k_spmv_f64(tiles_view A, const double* __restrict__ x,
+                                                          double* __restrict__ y)
+{
+    constexpr int CPL = geom<S>::CPL;
+    __shared__ warp_smem<S> smem[kWarps];
+    const int lane = threadIdx.x & 31;
+    warp_smem<S>& sm = smem[threadIdx.x >> 5];
+    const double* __restrict__ values = static_cast<const double*>(A.values);
+    const int64_t nw = (int64_t)gridDim.x * kWarps;
+    for (int64_t I = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); I < A.M; I += nw) {
+        const int64_t t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
+        if (t0 == t1)
+            continue;
+        for (int r = lane; r < S; r += 32)
+            sm.ys[r] = 0.0;
+        __syncwarp();
+#pragma unroll 1
+        for (int64_t t = t0; t < t1; ++t) {
+            const int64_t c0 = (int64_t)A.tile_col[t] * S;
+            const int z = (int)A.tile_nnz[t];
+            const int sch = A.tile_scheme[t];
+            const double* vals = values + A.tile_val_off[t];
+            const uint8_t* pay = A.payload + A.tile_idx_off[t];
+            double xr[CPL];
+#pragma unroll
+            for (int j = 0; j < CPL; ++j) {
+                const int64_t c = c0 + (S >= 32 ? 32 * j + lane : (lane & (S - 1)));
+                xr[j] = c < A.n ? __ldg(x + c) : 0.0;
+            }
+            if (S >= 32 && sch == ABHSF_SCHEME_BITMAP) {
+                if constexpr (S >= 32)
+                    tile_bitmap<S>(reinterpret_cast<const uint32_t*>(pay), vals, xr, sm, lane);
+            } else if (S >= 32 && sch == ABHSF_SCHEME_DENSE) {
+                if constexpr (S >= 32)
+                    tile_dense<S>(vals, xr, sm, lane);
+            } else if (S == 16 && sch == ABHSF_SCHEME_BITMAP) {
+                if constexpr (S == 16)
+                    tile_16<false>(reinterpret_cast<const uint32_t*>(pay), vals, xr[0], sm, lane);
+            } else if (S == 16 && sch == ABHSF_SCHEME_DENSE) {
+                if constexpr (S == 16)
+                    tile_16<true>(nullptr, vals, xr[0], sm, lane);
+            } else {
+#pragma unroll
+                for (int j = 0; j < CPL; ++j)
+                    if (S >= 32 || lane < S)
+                        sm.xs[S >= 32 ? 32 * j + lane : lane] = xr[j];
+                __syncwarp();
+                if (sch == ABHSF_SCHEME_CSR)
+                    tile_stream<S, true>(pay, vals, z, sm, lane);
+                else
+                    tile_stream<S, false>(pay, vals, z, sm, lane);
+            }
+        }
+        const int64_t r0 = I * S;
+        for (int r = lane; r < S; r += 32)
+            if (r0 + r < A.m)
+                y[r0 + r] += sm.ys[r];
+        __syncwarp();
+    }
+}
+
+template <int S>
+void launch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+{
+    const int64_t blocks = (a.M + kWarps - 1) / kWarps;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(blocks, int64_t(1) << 30));
+    k_spmv_f64<S><<<grid, kWarps * 32, 0, st>>>(a.view(), x, y);
+    ABHSF_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void spmv_f64(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+{
+    if (a.M == 0 || a.T == 0)
+        return;
+    switch (a.s) {
+    case 16: launch<16>(a, x, y, st); break;
+    case 32: launch<32>(a, x, y, st); break;
+    case 64: launch<64>(a, x, y, st); break;
+    case 128: launch<128>(a, x, y, st); break;
+    case 256: launch<256>(a, x, y, st); break;
+    default: fail(ABHSF_ERROR_UNSUPPORTED, "block size without an SpMV kernel");
+    }
+}
+
+}  // namespace abhsf

@@ -1,0 +1,237 @@
+"""Host-side mirror of the reference's per-format matrix class.
+
+The reference's formats share one shape (spmv/unified/spmv.cpp:74-127,
+140-159, 210-226; spmv/bottlenecks/spmv.cpp:43-64,125-133):
+
+    A.from_elements(elements, props)   # build
+    A.spmv(x, y)                       # y += A x
+    A.release()                        # free
+
+:class:`AbhsfMatrix` keeps that shape over the C ABI of libabhsf_b200.so.
+Inputs are numpy arrays (host memory) or torch CUDA tensors (device memory);
+``spmv`` on CUDA tensors is ordered on torch's current stream, on numpy
+arrays it copies through the device and returns when y holds the result.
+Errors raise :class:`abhsf_b200.capi.AbhsfError` subclasses, the analogue of
+the reference's ``std::runtime_error``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+
+try:  # torch is plumbing only: device memory and streams
+    import torch
+except ImportError:  # pragma: no cover
+    torch = None
+
+
+def _is_cuda(t) -> bool:
+    return torch is not None and isinstance(t, torch.Tensor) and t.is_cuda
+
+
+def _stream_ptr(stream=None) -> int | None:
+    if stream is not None:
+        return int(stream.cuda_stream) if hasattr(stream, "cuda_stream") else int(stream)
+    if torch is not None and torch.cuda.is_available():
+        return int(torch.cuda.current_stream().cuda_stream)
+    return None
+
+
+def _ptr(a) -> int:
+    if _is_cuda(a):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_device) -> capi.BuildOpts:
+    o = capi.BuildOpts()
+    capi.lib.abhsf_build_opts_default(C.byref(o))
+    o.block_size = int(block_size)
+    o.value_type = capi.VALUE_TYPES[value_type]
+    o.allow_csr = 1 if allow_csr else 0
+    o.matrix_type = capi.MATRIX_TYPES[matrix_type]
+    if forced_scheme is None:
+        o.forced_scheme = -1
+    else:
+        o.forced_scheme = capi.SCHEME_NAMES.index(forced_scheme) if isinstance(forced_scheme, str) else int(forced_scheme)
+    o.bits_per_value = int(bits_per_value)
+    o.inputs_on_device = 1 if on_device else 0
+    return o
+
+
+class AbhsfMatrix:
+    """ABHSF matrix resident on the GPU."""
+
+    def __init__(self):
+        self._h = None
+        self.m = self.n = self.nnz = 0
+        self.block_size = 0
+        self.value_type = "f64"
+
+    # ------------------------------------------------------------------ build
+    @classmethod
+    def from_elements(cls, rows, cols, vals, m: int, n: int, *, block_size: int = 64, value_type: str = "f64",
+                      allow_csr: bool = True, matrix_type: str = "real", forced_scheme=None,
+                      bits_per_value: int = 0, stream=None) -> "AbhsfMatrix":
+        """Builds from COO triplets (0-based, any order, no duplicates).
+        Scheme per tile by exact minimum storage (msmf.h:35-63) unless
+        forced_scheme names one.  vals may be None for binary matrices."""
+        on_dev = _is_cuda(rows)
+        if on_dev:
+            if not (_is_cuda(cols) and (vals is None or _is_cuda(vals))):
+                raise capi.InvalidValue(capi.INVALID_VALUE, "rows, cols and vals must all be host or all be CUDA")
+            rows = rows.to(torch.int64).contiguous()
+            cols = cols.to(torch.int64).contiguous()
+            vals = None if vals is None else vals.to(torch.float64).contiguous()
+        else:
+            rows = np.ascontiguousarray(rows, dtype=np.int64)
+            cols = np.ascontiguousarray(cols, dtype=np.int64)
+            vals = None if vals is None else np.ascontiguousarray(vals, dtype=np.float64)
+        nnz = int(rows.numel() if on_dev else rows.size)
+        if (cols.numel() if on_dev else cols.size) != nnz or (
+                vals is not None and (vals.numel() if on_dev else vals.size) != nnz):
+            raise capi.InvalidValue(capi.INVALID_VALUE, "rows, cols and vals differ in length")
+        o = _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_dev)
+        h = C.c_void_p()
+        capi.check(capi.lib.abhsf_build(_ptr(rows) if nnz else None, _ptr(cols) if nnz else None,
+                                        _ptr(vals) if (vals is not None and nnz) else None, nnz, int(m), int(n),
+                                        C.byref(o), _stream_ptr(stream), C.byref(h)))
+        A = cls()
+        A._h = h
+        A.m, A.n, A.nnz = int(m), int(n), nnz
+        A.block_size = int(block_size)
+        A.value_type = value_type
+        return A
+
+    # ------------------------------------------------------------------ spmv
+    def spmv(self, x, y, stream=None) -> None:
+        """y += A x.  CUDA tensors: asynchronous on the (current) stream;
+        numpy arrays: synchronous through device staging buffers."""
+        self._check_open()
+        if _is_cuda(x) or _is_cuda(y):
+            if not (_is_cuda(x) and _is_cuda(y)):
+                raise capi.InvalidValue(capi.INVALID_VALUE, "x and y must both be CUDA tensors or both numpy")
+            self._check_vec(x, y, torch.float64, x.numel(), y.numel(), x.is_contiguous() and y.is_contiguous())
+            capi.check(capi.lib.abhsf_spmv(self._h, x.data_ptr(), y.data_ptr(), _stream_ptr(stream)))
+        else:
+            if not (isinstance(x, np.ndarray) and isinstance(y, np.ndarray)):
+                raise capi.InvalidValue(capi.INVALID_VALUE, "x and y must be numpy arrays or CUDA tensors")
+            self._check_vec(x, y, np.float64, x.size, y.size, x.flags.c_contiguous and y.flags.c_contiguous)
+            capi.check(capi.lib.abhsf_spmv_host(self._h, x.ctypes.data, y.ctypes.data, _stream_ptr(stream)))
+
+    def _check_vec(self, x, y, dtype, nx, ny, contiguous):
+        if x.dtype != dtype or y.dtype != dtype:
+            raise capi.InvalidValue(capi.INVALID_VALUE, f"x and y must be float64, got {x.dtype}, {y.dtype}")
+        if nx != self.n or ny != self.m:
+            raise capi.InvalidValue(capi.INVALID_VALUE, f"x must have n={self.n} and y m={self.m} entries")
+        if not contiguous:
+            raise capi.InvalidValue(capi.INVALID_VALUE, "x and y must be contiguous")
+
+    # ------------------------------------------------------------------ release
+    def release(self) -> None:
+        if self._h is not None and self._h.value:
+            capi.check(capi.lib.abhsf_release(self._h))
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.release()
+
+    def _check_open(self):
+        if self._h is None or not self._h.value:
+            raise capi.InvalidValue(capi.INVALID_VALUE, "matrix was released or never built")
+
+    @property
+    def handle(self) -> int:
+        self._check_open()
+        return int(self._h.value)
+
+    # ------------------------------------------------------------------ introspection
+    def stats(self) -> dict:
+        self._check_open()
+        s = capi.Stats()
+        capi.check(capi.lib.abhsf_stats_get(self._h, C.byref(s)))
+        return {
+            "m": s.m, "n": s.n, "nnz": s.nnz, "block_size": s.block_size,
+            "value_type": [k for k, v in capi.VALUE_TYPES.items() if v == s.value_type][0],
+            "block_rows": s.block_rows, "block_cols": s.block_cols, "tiles": s.tiles,
+            "tiles_per_scheme": dict(zip(capi.SCHEME_NAMES, list(s.tiles_per_scheme))),
+            "nnz_per_scheme": dict(zip(capi.SCHEME_NAMES, list(s.nnz_per_scheme))),
+            "stored_values": s.stored_values, "payload_bytes": s.payload_bytes, "format_bytes": s.format_bytes,
+            "msmf_bits": list(s.msmf_bits),
+        }
+
+    def export(self) -> dict:
+        """Host copies of every format array (layout in include/abhsf/abhsf_gpu.h)."""
+        st = self.stats()
+        T, M = st["tiles"], st["block_rows"]
+        vdt = {"f64": np.float64, "f32": np.float32, "bf16": np.uint16}[st["value_type"]]
+        out = {
+            "brow_ptr": np.zeros(M + 1, np.int64), "tile_col": np.zeros(T, np.uint32),
+            "tile_nnz": np.zeros(T, np.uint32), "tile_scheme": np.zeros(T, np.uint8),
+            "tile_val_off": np.zeros(T + 1, np.int64), "tile_idx_off": np.zeros(T + 1, np.int64),
+            "payload": np.zeros(st["payload_bytes"], np.uint8), "values": np.zeros(st["stored_values"], vdt),
+        }
+        p = [out[k].ctypes.data if out[k].size else None for k in
+             ("brow_ptr", "tile_col", "tile_nnz", "tile_scheme", "tile_val_off", "tile_idx_off", "payload", "values")]
+        capi.check(capi.lib.abhsf_export_host(self._h, *p))
+        return out
+
+
+# ---------------------------------------------------------------------- block statistics
+def block_histogram(rows, cols, m: int, n: int, r: int, s: int, stream=None) -> dict[int, int]:
+    """block nnz -> number of r x s blocks, computed on the GPU
+    (block_statistics/block_stats.cpp:69-100)."""
+    on_dev = _is_cuda(rows)
+    if on_dev:
+        rows = rows.to(torch.int64).contiguous()
+        cols = cols.to(torch.int64).contiguous()
+        nnz = rows.numel()
+    else:
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        cols = np.ascontiguousarray(cols, dtype=np.int64)
+        nnz = rows.size
+    hist = np.zeros(r * s + 1, dtype=np.uint64)
+    blocks = C.c_int64()
+    capi.check(capi.lib.abhsf_block_histogram(_ptr(rows) if nnz else None, _ptr(cols) if nnz else None, nnz, m, n,
+                                              r, s, 1 if on_dev else 0, _stream_ptr(stream),
+                                              hist.ctypes.data_as(capi._u64p), hist.size, C.byref(blocks)))
+    nz = np.nonzero(hist)[0]
+    return {int(z): int(hist[z]) for z in nz}
+
+
+def mmf_line(m: int, n: int, nnz: int, matrix_type: str | int, r: int, s: int, hist: dict[int, int]):
+    """One line of the reference's mmf-single / mmf-double
+    (block_statistics/mmf.cpp:53-138): [coo32, csr32, coo, csr, bitmap, dense,
+    abhsf, abhsf134], values included."""
+    mt = capi.MATRIX_TYPES[matrix_type] if isinstance(matrix_type, str) else int(matrix_type)
+    h = np.zeros((max(hist) + 1) if hist else 1, dtype=np.uint64)
+    for z, c in hist.items():
+        h[z] = c
+    o1 = np.zeros(8, dtype=np.uint64)
+    o2 = np.zeros(8, dtype=np.uint64)
+    capi.check(capi.lib.abhsf_mmf_line(m, n, nnz, mt, r, s, h.ctypes.data_as(capi._u64p), h.size,
+                                       o1.ctypes.data_as(capi._u64p), o2.ctypes.data_as(capi._u64p)))
+    return [int(v) for v in o1], [int(v) for v in o2]
+
+
+def block_scheme_bits(scheme, r: int, s: int, nnz: int, bits_per_value: int = 64) -> int:
+    sc = capi.SCHEME_NAMES.index(scheme) if isinstance(scheme, str) else int(scheme)
+    return int(capi.lib.abhsf_block_scheme_bits(sc, r, s, nnz, bits_per_value))
+
+
+def block_select_scheme(r: int, s: int, nnz: int, bits_per_value: int = 64, is_binary: bool = False,
+                        allow_csr: bool = True) -> str:
+    return capi.SCHEME_NAMES[capi.lib.abhsf_block_select_scheme(r, s, nnz, bits_per_value, int(is_binary),
+                                                                int(allow_csr))]

@@ -1,0 +1,181 @@
+"""Seeded synthetic sparse matrices with the shapes the ABHSF SpMV path is
+measured on.  SuiteSparse matrices (block_statistics/experiments/matrices in
+the reference) are not available offline; these generators stand in for them.
+
+All generators return a :class:`Coo` with int64 row/column indices and float64
+values, rows and columns 0-based (the convention of the reference's
+matrix_market_reader, include/abhsf/utils/matrix_market_reader.h:135-136).
+Randomness comes from numpy's PCG64 ``default_rng(seed)``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class Coo:
+    rows: np.ndarray  # int64 [nnz]
+    cols: np.ndarray  # int64 [nnz]
+    vals: np.ndarray  # float64 [nnz]
+    m: int
+    n: int
+    name: str = ""
+
+    @property
+    def nnz(self) -> int:
+        return int(self.rows.size)
+
+
+def laplacian_2d(g: int = 512, diag: float = 4.0, off: float = -1.0) -> Coo:
+    """5-point Laplacian on a g x g grid, i = gy*g + gx, elements in row-major
+    order.  g = 512 gives n = 262,144 and nnz = 1,308,672."""
+    n = g * g
+    i = np.arange(n, dtype=np.int64)
+    gx, gy = i % g, i // g
+    parts = []
+    # column order within a row: i-g, i-1, i, i+1, i+g
+    for dc, mask, v in ((-g, gy > 0, off), (-1, gx > 0, off), (0, None, diag),
+                        (1, gx < g - 1, off), (g, gy < g - 1, off)):
+        r = i if mask is None else i[mask]
+        parts.append((r, r + dc, np.full(r.size, v)))
+    rows = np.concatenate([p[0] for p in parts])
+    cols = np.concatenate([p[1] for p in parts])
+    vals = np.concatenate([p[2] for p in parts])
+    order = np.lexsort((cols, rows))
+    return Coo(rows[order], cols[order], vals[order].astype(np.float64), n, n, f"laplace2d_{g}")
+
+
+def laplacian_3d(g: int = 256, diag: float = 6.0, off: float = -1.0) -> Coo:
+    """7-point Laplacian on a g^3 grid (SPD), elements in row-major order.
+    g = 256 gives n = 16,777,216 and nnz = 117,047,296."""
+    n = g ** 3
+    i = np.arange(n, dtype=np.int64)
+    gx, gy, gz = i % g, (i // g) % g, i // (g * g)
+    parts = []
+    for dc, mask, v in ((-g * g, gz > 0, off), (-g, gy > 0, off), (-1, gx > 0, off),
+                        (0, None, diag), (1, gx < g - 1, off), (g, gy < g - 1, off),
+                        (g * g, gz < g - 1, off)):
+        r = i if mask is None else i[mask]
+        parts.append((r, r + dc, v))
+    rows = np.concatenate([p[0] for p in parts])
+    cols = np.concatenate([p[1] for p in parts])
+    vals = np.concatenate([np.full(p[0].size, p[2], dtype=np.float64) for p in parts])
+    order = np.lexsort((cols, rows))
+    return Coo(rows[order], cols[order], vals[order], n, n, f"laplace3d_{g}")
+
+
+# Tile-occupancy probability that gives ~60M nnz for the tiled mixture below
+# (52.7k occupied 64x64 tiles of 4.29e9).  The nominal p = 0.002 would give
+# ~8.6M tiles and ~9.8e9 nnz, which contradicts the stated ~60M nnz.
+TILED_MIXTURE_P = 1.2266e-5
+
+
+def tiled_mixture(n: int = 4_194_304, tile: int = 64, p: float = TILED_MIXTURE_P, seed: int = 1,
+                  chunk_tiles: int = 1024) -> Coo:
+    """n x n matrix tiled tile x tile; each tile occupied with probability p.
+    Occupied tiles draw their density from the mixture 20% dense (each entry
+    present with probability 0.9), 30% bitmap-range (density U[0.15, 0.5]) and
+    50% sparse (1-8 nnz placed uniformly).  Values N(0,1)."""
+    rng = np.random.default_rng(seed)
+    nb = (n + tile - 1) // tile
+    total = nb * nb
+    n_occ = int(rng.binomial(total, p))
+    tiles = np.unique(rng.integers(0, total, size=n_occ, dtype=np.int64))
+    kind = rng.random(tiles.size)
+    dens = np.where(kind < 0.2, 0.9, rng.uniform(0.15, 0.5, size=tiles.size))
+    sparse = kind >= 0.5
+    tt = tile * tile
+    rows_l, cols_l = [], []
+    # dense / bitmap-range tiles: Bernoulli(density) per entry, in chunks
+    dtiles = np.nonzero(~sparse)[0]
+    for c0 in range(0, dtiles.size, chunk_tiles):
+        sel = dtiles[c0:c0 + chunk_tiles]
+        u = rng.random((sel.size, tt), dtype=np.float32)
+        hit = u < dens[sel, None].astype(np.float32)
+        ti, loc = np.nonzero(hit)
+        tid = tiles[sel][ti]
+        rows_l.append((tid // nb) * tile + loc // tile)
+        cols_l.append((tid % nb) * tile + loc % tile)
+    # sparse tiles: k in [1, 8] distinct positions
+    stiles = np.nonzero(sparse)[0]
+    ks = rng.integers(1, 9, size=stiles.size)
+    locs = [rng.choice(tt, size=int(k), replace=False) for k in ks]
+    if stiles.size:
+        loc = np.concatenate(locs).astype(np.int64)
+        tid = np.repeat(tiles[stiles], ks)
+        rows_l.append((tid // nb) * tile + loc // tile)
+        cols_l.append((tid % nb) * tile + loc % tile)
+    rows = np.concatenate(rows_l).astype(np.int64)
+    cols = np.concatenate(cols_l).astype(np.int64)
+    keep = (rows < n) & (cols < n)
+    rows, cols = rows[keep], cols[keep]
+    vals = rng.standard_normal(rows.size)
+    return Coo(rows, cols, vals, n, n, f"tiled_mixture_{n}_s{seed}")
+
+
+def random_uniform(m: int, n: int, nnz: int, seed: int = 0, values: str = "normal") -> Coo:
+    """nnz distinct positions uniformly at random (unsorted), values N(0,1)."""
+    rng = np.random.default_rng(seed)
+    nnz = min(nnz, m * n)
+    keys = np.unique(rng.integers(0, m * n, size=int(nnz * 1.2) + 8, dtype=np.int64))
+    keys = rng.permutation(keys)[:nnz]
+    vals = rng.standard_normal(keys.size) if values == "normal" else np.ones(keys.size)
+    return Coo(keys // n, keys % n, vals, m, n, f"random_{m}x{n}_{nnz}_s{seed}")
+
+
+def random_blocky(m: int, n: int, s: int, n_tiles: int, seed: int = 0) -> Coo:
+    """Tiles with densities spread over the whole COO/CSR/bitmap/dense range,
+    so that every scheme is exercised at block size s."""
+    rng = np.random.default_rng(seed)
+    M, N = (m + s - 1) // s, (n + s - 1) // s
+    tiles = np.unique(rng.integers(0, M * N, size=n_tiles, dtype=np.int64))
+    rows_l, cols_l = [], []
+    for t in tiles:
+        d = rng.choice([0.002, 0.02, 0.08, 0.3, 0.7, 0.995, 1.0])
+        hit = np.nonzero(rng.random(s * s) < d)[0]
+        if hit.size == 0:
+            hit = rng.integers(0, s * s, size=1)
+        r = (t // N) * s + hit // s
+        c = (t % N) * s + hit % s
+        ok = (r < m) & (c < n)
+        rows_l.append(r[ok])
+        cols_l.append(c[ok])
+    rows = np.concatenate(rows_l).astype(np.int64)
+    cols = np.concatenate(cols_l).astype(np.int64)
+    perm = rng.permutation(rows.size)
+    return Coo(rows[perm], cols[perm], rng.standard_normal(rows.size), m, n,
+               f"blocky_{m}x{n}_s{s}_seed{seed}")
+
+
+def edge_shapes(n: int = 1000) -> list[Coo]:
+    """The reference's pathological shapes (include/abhsf/utils/synthetic.h:8-91),
+    seeded, at small size, plus ragged edges and a 1x1 matrix."""
+    out = []
+    i = np.arange(n, dtype=np.int64)
+    one = np.ones(n)
+    out.append(Coo(i, i, one.copy(), n, n, "diagonal"))
+    out.append(Coo(i, np.zeros(n, dtype=np.int64), one.copy(), n, n, "single_column"))
+    out.append(Coo(np.full(n, n - 1, dtype=np.int64), i, one.copy(), n, n, "single_row"))
+    rr = np.concatenate([np.zeros(n, dtype=np.int64), i[1:]])
+    cc = np.concatenate([i, np.zeros(n - 1, dtype=np.int64)])
+    out.append(Coo(rr, cc, np.ones(rr.size), n, n, "single_row_column"))
+    rng = np.random.default_rng(7)
+    out.append(Coo(i, rng.integers(0, n, size=n), rng.standard_normal(n), n, n, "random_column"))
+    d = 70
+    dr, dc = np.divmod(np.arange(d * d, dtype=np.int64), d)
+    out.append(Coo(dr, dc, rng.standard_normal(d * d), d, d, "dense_70"))
+    out.append(Coo(np.array([0], dtype=np.int64), np.array([0], dtype=np.int64), np.array([2.5]), 1, 1, "one_by_one"))
+    # ragged rectangular, empty rows and columns
+    m2, n2 = 333, 517
+    k = rng.choice(m2 * n2, size=4000, replace=False)
+    keep = (k // n2) % 7 != 3
+    k = k[keep]
+    out.append(Coo(k // n2, k % n2, rng.standard_normal(k.size), m2, n2, "ragged_empty_rows"))
+    return out
+
+
+def rhs(n: int, seed: int = 0) -> np.ndarray:
+    """x uniform[-1, 1]."""
+    return np.random.default_rng(seed).uniform(-1.0, 1.0, size=n)

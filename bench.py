@@ -1,0 +1,307 @@
+"""Throughput benchmark of the ABHSF FP64 SpMV hot path on B200.
+
+Workload: the tiled-mixture matrix (n = 4,194,304, 64 x 64 tiles; 20% dense
+0.9, 30% density U[0.15, 0.5], 50% 1-8 nnz; ~60M nnz; values N(0,1), x
+U[-1, 1], seed 1), block size 64, scheme per tile by exact minimum storage.
+
+A step is one y += A x over the whole matrix.  value = algorithmic bytes per
+step / kernel time, where algorithmic bytes B = format bytes + 8 n (x read
+once) + 16 m (y read and written).  e2e is the same metric through the
+host-memory call (x, y in pinned host memory; copies inside the timed region).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU (torchrun): every rank runs an independent replica (the SpMV has no
+exchange step); value is the bytes all ranks processed / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SpMV GB/s (% HBM peak) + CG solve time, tuned vs plain on one B200 at same tol"
+UNIT = "GB/s"
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 256 << 20
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "spmv_f64_tiled_mixture_s64.md")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes (read + write) per SpMV launch from the committed ncu summary."""
+    try:
+        txt = open(TRAFFIC_FILE).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        self.idx = gpu_index
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(gpu_index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = [[t.strip() for t in line.split(",")] for line in out.strip().splitlines() if line.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def workload():
+    from abhsf_b200 import workloads as W
+    t0 = time.time()
+    c = W.tiled_mixture()
+    log(f"workload: tiled mixture n={c.n} nnz={c.nnz} ({time.time() - t0:.1f} s to generate)")
+    return c
+
+
+def algorithmic_bytes(st: dict, m: int, n: int) -> int:
+    return int(st["format_bytes"]) + 8 * n + 16 * m
+
+
+def cpu_reference_run(c, bytes_per_step: float, max_seconds: float, max_iters: int):
+    """Reference CSR spmv_naive (oracle/_ref, compiled from the reference
+    sources) on all host threads; falls back to the single-thread oracle port."""
+    from oracle import oracle
+    x = np.random.default_rng(0).uniform(-1, 1, c.n)
+    y = np.zeros(c.m)
+    if oracle.RefCSR.available():
+        t0 = time.time()
+        R = oracle.RefCSR(c.rows, c.cols, c.vals, c.m, c.n)
+        log(f"reference CSR built in {time.time() - t0:.1f} s")
+        R.spmv(x, y)  # warm-up
+        R.spmv(x, y)
+        times = []
+        t_start = time.perf_counter()
+        while len(times) < max_iters and time.perf_counter() - t_start < max_seconds:
+            t0 = time.perf_counter()
+            R.spmv(x, y)
+            times.append(time.perf_counter() - t0)
+        cores = oracle.RefCSR.threads()
+        R.release()
+        kind = "reference"
+        sample = (f"{len(times)} full y += A x of the same matrix, csr_matrix<double,int,int>::spmv_naive "
+                  f"(spmv/bottlenecks/spmv.cpp:58-64) built from the reference sources, OpenMP static rows")
+    else:
+        oracle.spmv_elements(c.rows, c.cols, c.vals, x, y)
+        times = []
+        t_start = time.perf_counter()
+        while len(times) < max_iters and time.perf_counter() - t_start < max_seconds:
+            t0 = time.perf_counter()
+            oracle.spmv_elements(c.rows, c.cols, c.vals, x, y)
+            times.append(time.perf_counter() - t0)
+        cores = 1
+        kind = "port"
+        sample = f"{len(times)} full y += A x with the oracle's element-order FP64 loop (1 thread)"
+    t = statistics.median(times)
+    return {"value": bytes_per_step / t / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+            "ms_per_step": t * 1e3, "gflops": 2.0 * c.nnz / t / 1e9}
+
+
+def build_format_stats(c):
+    """Format statistics without a GPU (for the reference arm): the oracle
+    builder gives the same bytes as the device format."""
+    from oracle import oracle
+    b = oracle.build(c.rows, c.cols, c.vals, c.m, c.n, 64)
+    fmt = (b.M + 1) * 8 + b.T * 9 + (b.T + 1) * 16 + b.idx.size + b.values.size * 8
+    return {"format_bytes": fmt}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    c = workload()
+    st = build_format_stats(c)
+    B = algorithmic_bytes(st, c.m, c.n)
+    cpu = cpu_reference_run(c, B, max_seconds=30.0, max_iters=max(args.steps, 10))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "tiled_mixture n=4194304 tile=64 p=1.2266e-5 seed=1 (values N(0,1))",
+                   "nnz": c.nnz, "bytes_per_step": B, "gflops": cpu["gflops"]},
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from abhsf_b200 import AbhsfMatrix
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+
+    c = workload()
+    t0 = time.time()
+    A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    st = A.stats()
+    B = algorithmic_bytes(st, c.m, c.n)
+    log(f"built in {build_s:.2f} s: tiles {st['tiles']} {st['tiles_per_scheme']}, format {st['format_bytes']/1e6:.1f} MB, "
+        f"B = {B/1e6:.1f} MB per step")
+
+    rng = np.random.default_rng(1)
+    x_h = rng.uniform(-1, 1, c.n)
+    xd = torch.from_numpy(x_h).to(dev)
+    yd = torch.zeros(c.m, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        A.spmv(xd, yd)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record(stream)
+        A.spmv(xd, yd)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    times_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    t_mean = sum(times_ms) / len(times_ms)
+    t_red = torch.tensor([t_mean], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_red, op=dist.ReduceOp.MAX)
+    t_max = float(t_red.item())
+
+    # e2e: host buffers (pinned), copies inside every step
+    x_pin = torch.from_numpy(x_h).pin_memory().numpy()
+    y_pin = torch.zeros(c.m, dtype=torch.float64).pin_memory().numpy()
+    for _ in range(max(2, args.warmup)):
+        A.spmv(x_pin, y_pin)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        A.spmv(x_pin, y_pin)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    e_red = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e_red, op=dist.ReduceOp.MAX)
+    e2e_s = float(e_red.item())
+
+    peak, peak_src = hbm_peak()
+    achieved = B / (t_mean * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_run(c, B, max_seconds=20.0, max_iters=40)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * B / (t_max * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {
+                "workload": "tiled_mixture n=4194304 tile=64 p=1.2266e-5 seed=1 (values N(0,1), x U[-1,1])",
+                "block_size": 64, "nnz": c.nnz, "tiles": st["tiles"], "tiles_per_scheme": st["tiles_per_scheme"],
+                "bytes_per_step": B, "format_bytes": st["format_bytes"],
+                "msmf_min_bytes_per_step": st["msmf_bits"][6] // 8 + 8 * c.n + 16 * c.m,
+                "l2": "256 MiB buffer written between steps (and 600 MB working set > 126 MB L2)",
+                "gflops": 2.0 * c.nnz / (t_mean * 1e-3) / 1e9, "build_s": build_s,
+                "parallelism": f"replicas x{world}",
+            },
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": ncu_traffic_per_launch(),
+                         "peak_source": peak_src, "kernel": "k_spmv_f64<64>"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * B / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
+                    "d2h_bytes_per_step": 8 * c.m, "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    A.release()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

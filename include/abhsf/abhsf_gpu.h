@@ -1,0 +1,177 @@
+/*
+ * abhsf_gpu.h -- C ABI of the B200 (sm_100a) ABHSF builder and SpMV.
+ *
+ * Drop-in for the reference's per-format call surface
+ *   from_elements(elements_t&, const matrix_properties&)   build
+ *   spmv(const real_type* x, real_type* y)                  y += A x
+ *   release()                                               free
+ * (spmv/unified/spmv.cpp:74-127,140-159,210-226; spmv/bottlenecks/spmv.cpp:43-64,
+ * 125-133; spmv/orig/88.cpp:150-236) and for the block-statistics tools
+ * (block_statistics/block_stats.cpp:69-100, block_statistics/mmf.cpp:53-138,
+ * include/abhsf/msmf.h:9-63).
+ *
+ * Conventions: every call returns abhsf_status and never throws; the reason
+ * for the last failure on the calling thread is abhsf_last_error_string().
+ * Indices are 0-based (matrix_market_reader.h:135-136).  A handle owns all of
+ * its device memory.  Calls taking a stream are ordered on it; a NULL stream
+ * is the legacy default stream.  A handle may be used from several threads
+ * for abhsf_spmv / abhsf_stats / abhsf_export_host at once; abhsf_spmv_host
+ * and abhsf_release need exclusive use.
+ *
+ * Format (device arrays, s = block size, M = ceil(m/s), T = nonzero tiles):
+ *   brow_ptr[M+1]  int64  tiles of block row I are [brow_ptr[I], brow_ptr[I+1])
+ *   tile_col[T]    uint32 block column J, ascending within a block row
+ *   tile_nnz[T]    uint32 nonzeros of the tile
+ *   tile_scheme[T] uint8  ABHSF_SCHEME_*
+ *   tile_val_off[T+1] int64  first stored value of the tile
+ *   tile_idx_off[T+1] int64  first payload byte of the tile (16-byte aligned)
+ *   payload: COO    uint16 (lrow << log2 s) | lcol per nonzero
+ *            CSR    uint16 row_end[s] (nonzeros in rows <= r), uint8 lcol[nnz]
+ *            bitmap uint64 words; bit lrow*s + lcol, LSB first
+ *            dense  none
+ *            each tile's payload zero-padded to a multiple of 16 bytes
+ *   values: nonzeros in row-major order inside the tile; dense tiles store
+ *           all s*s entries, zeros included.
+ */
+#ifndef ABHSF_GPU_H
+#define ABHSF_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ABHSF_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define ABHSF_API __attribute__((visibility("default")))
+#else
+#define ABHSF_API
+#endif
+
+/* Same object as cudaStream_t / CUstream. */
+typedef struct CUstream_st* abhsf_stream_t;
+
+typedef enum abhsf_status {
+    ABHSF_SUCCESS = 0,
+    ABHSF_ERROR_INVALID_VALUE = 1,      /* bad argument or option */
+    ABHSF_ERROR_INDEX_OUT_OF_RANGE = 2, /* an element outside m x n */
+    ABHSF_ERROR_DUPLICATE_ENTRY = 3,    /* two elements at one (row, col) */
+    ABHSF_ERROR_OUT_OF_MEMORY = 4,
+    ABHSF_ERROR_UNSUPPORTED = 5,        /* valid request this build does not handle */
+    ABHSF_ERROR_CUDA = 6                /* CUDA runtime error, see the error string */
+} abhsf_status;
+
+typedef enum abhsf_scheme {
+    ABHSF_SCHEME_COO = 0,
+    ABHSF_SCHEME_CSR = 1,
+    ABHSF_SCHEME_BITMAP = 2,
+    ABHSF_SCHEME_DENSE = 3
+} abhsf_scheme;
+
+typedef enum abhsf_value_type {
+    ABHSF_VALUE_F64 = 0,
+    ABHSF_VALUE_F32 = 1, /* RN(f64) */
+    ABHSF_VALUE_BF16 = 2 /* RNE(RN_f32(f64)) */
+} abhsf_value_type;
+
+/* include/abhsf/utils/matrix_properties.h:8-14 */
+typedef enum abhsf_matrix_type {
+    ABHSF_MATRIX_BINARY = 0,
+    ABHSF_MATRIX_INTEGER = 1,
+    ABHSF_MATRIX_REAL = 2,
+    ABHSF_MATRIX_COMPLEX = 3
+} abhsf_matrix_type;
+
+typedef struct abhsf_build_opts {
+    int32_t block_size;       /* s: 16, 32, 64, 128 or 256 */
+    int32_t value_type;       /* abhsf_value_type of the stored values */
+    int32_t allow_csr;        /* 1: block_min_msmf (msmf.h:35-48); 0: block_min_msmf_wocsr (msmf.h:50-63) */
+    int32_t matrix_type;      /* abhsf_matrix_type; BINARY never selects dense and stores 1.0 values */
+    int32_t forced_scheme;    /* -1: minimum storage; 0..3: this scheme for every tile */
+    int32_t inputs_on_device; /* rows / cols / vals are device pointers */
+    int64_t bits_per_value;   /* dense-cost element width; 0 = width of value_type */
+} abhsf_build_opts;
+
+typedef struct abhsf_matrix abhsf_matrix;
+
+typedef struct abhsf_stats {
+    int64_t m, n, nnz;
+    int32_t block_size, value_type;
+    int64_t block_rows, block_cols, tiles;
+    int64_t tiles_per_scheme[4];
+    int64_t nnz_per_scheme[4];
+    int64_t stored_values;
+    int64_t payload_bytes;
+    int64_t format_bytes;   /* all device arrays of the format (B_fmt) */
+    uint64_t msmf_bits[8];  /* this block size's mmf line at the dense-cost width:
+                               coo32 csr32 coo csr bitmap dense abhsf abhsf134,
+                               values included (block_statistics/mmf.cpp:122-138) */
+} abhsf_stats;
+
+/* Fills the defaults: s = 64, f64, CSR allowed, REAL, minimum storage, host inputs. */
+ABHSF_API void abhsf_build_opts_default(abhsf_build_opts* opts);
+
+/* Builds the format on the GPU from COO triplets (any order, no duplicates).
+ * vals may be NULL for BINARY matrices (values 1.0).  Synchronises stream.
+ * Replaces from_elements/assemble (spmv/unified/spmv.cpp:74-127,
+ * spmv/bottlenecks/spmv.cpp:43-49, spmv/orig/88.cpp:150-202); unlike the
+ * reference it leaves the caller's arrays untouched. */
+ABHSF_API abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, const double* vals, int64_t nnz,
+                         int64_t m, int64_t n, const abhsf_build_opts* opts, abhsf_stream_t stream,
+                         abhsf_matrix** out);
+
+/* y += A x, x[n] and y[m] float64 in device memory; matrix stored as f64.
+ * Replaces spmv(x, y) (spmv/bottlenecks/spmv.cpp:58-64, spmv/orig/88.cpp:204-236). */
+ABHSF_API abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double* y, abhsf_stream_t stream);
+
+/* The same with x and y in host memory: copies x and y in, runs, copies y
+ * back and synchronises.  The drop-in for callers of the reference's
+ * host-memory spmv(x, y).  Device staging buffers are allocated on first use
+ * and kept by the handle. */
+ABHSF_API abhsf_status abhsf_spmv_host(abhsf_matrix* a, const double* x, double* y, abhsf_stream_t stream);
+
+/* Frees the handle and its device memory (release(), spmv/bottlenecks/spmv.cpp:125-133). */
+ABHSF_API abhsf_status abhsf_release(abhsf_matrix* a);
+
+/* Format statistics, including the reference's per-scheme storage totals. */
+ABHSF_API abhsf_status abhsf_stats_get(const abhsf_matrix* a, abhsf_stats* out);
+
+/* Copies the format arrays (layout above) to host buffers sized from
+ * abhsf_stats_get (tiles, stored_values, payload_bytes); NULL skips one. */
+ABHSF_API abhsf_status abhsf_export_host(const abhsf_matrix* a, int64_t* brow_ptr, uint32_t* tile_col,
+                               uint32_t* tile_nnz, uint8_t* tile_scheme, int64_t* tile_val_off,
+                               int64_t* tile_idx_off, uint8_t* payload, void* values);
+
+/* Block histogram for block size r x s (powers of two, 2..256) computed on
+ * the GPU: hist[z] = number of r x s blocks holding z nonzeros, for
+ * z < hist_len (hist_len >= r*s + 1).  *blocks = nonzero blocks.
+ * Replaces process_block_size_powers (block_statistics/block_stats.cpp:69-100). */
+ABHSF_API abhsf_status abhsf_block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m,
+                                   int64_t n, int32_t r, int32_t s, int32_t inputs_on_device,
+                                   abhsf_stream_t stream, uint64_t* hist, int64_t hist_len,
+                                   int64_t* blocks);
+
+/* One line of the reference's mmf-single / mmf-double (block_statistics/mmf.cpp:53-138)
+ * from props and a block histogram; out_* = coo32 csr32 coo csr bitmap dense abhsf abhsf134. */
+ABHSF_API abhsf_status abhsf_mmf_line(int64_t m, int64_t n, int64_t nnz, int32_t matrix_type, int32_t r, int32_t s,
+                            const uint64_t* hist, int64_t hist_len, uint64_t out_single[8],
+                            uint64_t out_double[8]);
+
+/* Bits of one r x s block with nnz nonzeros under `scheme` (msmf.h:9-33), and
+ * the scheme minimum storage selects (msmf.h:35-63, ties COO > CSR > bitmap > dense). */
+ABHSF_API uint64_t abhsf_block_scheme_bits(int32_t scheme, int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value);
+ABHSF_API int32_t abhsf_block_select_scheme(int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value, int32_t is_binary,
+                                  int32_t allow_csr);
+
+/* Reason for the last non-success status returned on this thread. */
+ABHSF_API const char* abhsf_last_error_string(void);
+
+ABHSF_API int32_t abhsf_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ABHSF_GPU_H */

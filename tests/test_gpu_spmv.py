@@ -1,0 +1,138 @@
+"""GPU SpMV parity: y += A x on the B200 against the FP64 oracle (the
+reference's verification loop) and the reference CSR spmv_naive (golden),
+with non-unit random values and x so that order and placement errors show."""
+import numpy as np
+import pytest
+
+from conftest import assert_spmv_close, golden_matrices, golden_spmv, golden_stats
+from abhsf_b200 import AbhsfMatrix, capi
+from abhsf_b200 import workloads as W
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+MATS = golden_matrices()
+STATS = golden_stats()
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def run_spmv(A, x, y0):
+    import torch
+    xd, yd = _dev(x), _dev(y0.copy())
+    A.spmv(xd, yd)
+    torch.cuda.synchronize()
+    return yd.cpu().numpy()
+
+
+@pytest.mark.parametrize("s", [16, 32, 64, 128, 256])
+@pytest.mark.parametrize("forced", [None, "coo", "csr", "bitmap", "dense"])
+def test_spmv_matches_oracle_all_schemes(gpu, s, forced):
+    for name, coo in MATS.items():
+        x = W.rhs(coo.n, 11)
+        y0 = W.rhs(coo.m, 12)
+        ref = oracle.spmv_elements(coo.rows, coo.cols, coo.vals, x, y0.copy())
+        scale = oracle.abs_spmv(coo.rows, coo.cols, coo.vals, x, coo.m) + np.abs(y0)
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, forced_scheme=forced)
+        y = run_spmv(A, x, y0)
+        assert_spmv_close(y, ref, scale)
+        A.release()
+
+
+def test_spmv_matches_reference_csr_golden(gpu):
+    ref = golden_spmv()
+    n_checked = 0
+    for name, coo in MATS.items():
+        if name + "__y" not in ref:
+            continue
+        x, y0, yr = ref[name + "__x"], ref[name + "__y0"], ref[name + "__y"]
+        scale = oracle.abs_spmv(coo.rows, coo.cols, coo.vals, x, coo.m) + np.abs(y0)
+        for s in (16, 64, 256):
+            A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s)
+            assert_spmv_close(run_spmv(A, x, y0), yr, scale)
+            A.release()
+        n_checked += 1
+    assert n_checked >= 6
+
+
+def test_spmv_config1_against_golden(gpu):
+    c = W.laplacian_2d(512)
+    x = W.rhs(c.n, 0)
+    yr = golden_spmv()["laplace2d_512__y_seed0"]
+    A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64)
+    y = run_spmv(A, x, np.zeros(c.m))
+    scale = oracle.abs_spmv(c.rows, c.cols, c.vals, x, c.m)
+    worst_scaled, worst_rel = assert_spmv_close(y, yr, scale)
+    assert worst_rel <= 1e-13, worst_rel
+
+
+def test_host_pointer_path_equals_device_path(gpu):
+    coo = MATS["blocky64"]
+    x = W.rhs(coo.n, 3)
+    y0 = W.rhs(coo.m, 4)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    yh = y0.copy()
+    A.spmv(x, yh)  # numpy: host buffers, copies inside the call
+    yd = run_spmv(A, x, y0)
+    np.testing.assert_array_equal(yh, yd)
+
+
+def test_spmv_is_deterministic(gpu):
+    coo = W.random_blocky(3000, 3000, 64, 400, seed=21)
+    x = W.rhs(coo.n, 5)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    ys = [run_spmv(A, x, np.zeros(coo.m)) for _ in range(3)]
+    np.testing.assert_array_equal(ys[0], ys[1])
+    np.testing.assert_array_equal(ys[0], ys[2])
+
+
+def test_spmv_argument_errors(gpu):
+    import torch
+    coo = MATS["rand_real"]
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=32)
+    with pytest.raises(capi.InvalidValue):
+        A.spmv(torch.zeros(coo.n, device="cuda"), torch.zeros(coo.m, device="cuda"))  # float32
+    with pytest.raises(capi.InvalidValue):
+        A.spmv(torch.zeros(coo.n + 1, dtype=torch.float64, device="cuda"),
+               torch.zeros(coo.m, dtype=torch.float64, device="cuda"))
+    B = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=32, value_type="f32")
+    with pytest.raises(capi.InvalidValue):
+        B.spmv(torch.zeros(coo.n, dtype=torch.float64, device="cuda"),
+               torch.zeros(coo.m, dtype=torch.float64, device="cuda"))
+    A.release()
+    with pytest.raises(capi.InvalidValue):
+        A.spmv(np.zeros(coo.n), np.zeros(coo.m))
+
+
+def test_device_inputs_build(gpu):
+    coo = MATS["blocky16"]
+    A = AbhsfMatrix.from_elements(_dev(coo.rows), _dev(coo.cols), _dev(coo.vals), coo.m, coo.n, block_size=16)
+    B = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=16)
+    ea, eb = A.export(), B.export()
+    for k in ea:
+        np.testing.assert_array_equal(ea[k], eb[k])
+
+
+@pytest.mark.parametrize("s", [64])
+def test_tiled_mixture_full_size(gpu, s):
+    """The throughput workload at full size (n = 4,194,304, ~60M nnz): format
+    statistics against the oracle histogram and the cost model, y against the
+    FP64 oracle loop."""
+    c = W.tiled_mixture()
+    assert 50_000_000 < c.nnz < 70_000_000
+    A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=s)
+    st = A.stats()
+    hist = oracle.block_histogram(c.rows, c.cols, 6, 6)
+    assert st["tiles"] == sum(hist.values())
+    want = {k: 0 for k in capi.SCHEME_NAMES}
+    for z, cnt in hist.items():
+        want[capi.SCHEME_NAMES[oracle.select_scheme(64, 64, z, 64)]] += cnt
+    assert st["tiles_per_scheme"] == want
+    x = W.rhs(c.n, 1)
+    y0 = W.rhs(c.m, 2)
+    ref = oracle.spmv_elements(c.rows, c.cols, c.vals, x, y0.copy())
+    scale = oracle.abs_spmv(c.rows, c.cols, c.vals, x, c.m) + np.abs(y0)
+    assert_spmv_close(run_spmv(A, x, y0), ref, scale)
