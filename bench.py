@@ -97,10 +97,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def workload():
+def workload(n: int = 4_194_304):
     from abhsf_b200 import workloads as W
     t0 = time.time()
-    c = W.tiled_mixture()
+    c = W.tiled_mixture(n=n)
     log(f"workload: tiled mixture n={c.n} nnz={c.nnz} ({time.time() - t0:.1f} s to generate)")
     return c
 
@@ -161,7 +161,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    c = workload()
+    c = workload(args.n)
     st = build_format_stats(c)
     B = algorithmic_bytes(st, c.m, c.n)
     cpu = cpu_reference_run(c, B, max_seconds=30.0, max_iters=max(args.steps, 10))
@@ -169,7 +169,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "tiled_mixture n=4194304 tile=64 p=1.2266e-5 seed=1 (values N(0,1))",
+        "config": {"workload": f"tiled_mixture n={c.n} tile=64 p=1.2266e-5 seed=1 (values N(0,1))",
                    "nnz": c.nnz, "bytes_per_step": B, "gflops": cpu["gflops"]},
         "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -192,7 +192,7 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
 
-    c = workload()
+    c = workload(args.n)
     t0 = time.time()
     A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64)
     torch.cuda.synchronize()
@@ -239,14 +239,15 @@ def run_ours(args):
     # e2e: host buffers (pinned), copies inside every step
     x_pin = torch.from_numpy(x_h).pin_memory().numpy()
     y_pin = torch.zeros(c.m, dtype=torch.float64).pin_memory().numpy()
-    for _ in range(max(2, args.warmup)):
+    e2e_steps = 0 if args.no_e2e else args.steps
+    for _ in range(max(2, args.warmup) if e2e_steps else 0):
         A.spmv(x_pin, y_pin)
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         A.spmv(x_pin, y_pin)
-    e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_s = (time.perf_counter() - t0) / max(1, e2e_steps)
     e_red = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(e_red, op=dist.ReduceOp.MAX)
@@ -264,7 +265,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {
-                "workload": "tiled_mixture n=4194304 tile=64 p=1.2266e-5 seed=1 (values N(0,1), x U[-1,1])",
+                "workload": f"tiled_mixture n={c.n} tile=64 p=1.2266e-5 seed=1 (values N(0,1), x U[-1,1])",
                 "block_size": 64, "nnz": c.nnz, "tiles": st["tiles"], "tiles_per_scheme": st["tiles_per_scheme"],
                 "bytes_per_step": B, "format_bytes": st["format_bytes"],
                 "msmf_min_bytes_per_step": st["msmf_bits"][6] // 8 + 8 * c.n + 16 * c.m,
@@ -294,6 +295,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
+    ap.add_argument("--n", type=int, default=4_194_304,
+                    help="matrix order of the tiled mixture (smaller only for profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -66,7 +66,9 @@ def test_spmv_config1_against_golden(gpu):
     y = run_spmv(A, x, np.zeros(c.m))
     scale = oracle.abs_spmv(c.rows, c.cols, c.vals, x, c.m)
     worst_scaled, worst_rel = assert_spmv_close(y, yr, scale)
-    assert worst_rel <= 1e-13, worst_rel
+    # tree-ordered sums: the scaled bound holds; |dy|/|y| alone is order
+    # dependent on rows that cancel (4 x_i minus four neighbours)
+    assert worst_scaled <= 1e-13, worst_scaled
 
 
 def test_host_pointer_path_equals_device_path(gpu):
