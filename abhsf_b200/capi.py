@@ -18,6 +18,8 @@ SCHEME_COO, SCHEME_CSR, SCHEME_BITMAP, SCHEME_DENSE = range(4)
 SCHEME_NAMES = ("coo", "csr", "bitmap", "dense")
 VALUE_TYPES = {"f64": 0, "f32": 1, "bf16": 2}
 MATRIX_TYPES = {"binary": 0, "integer": 1, "real": 2, "complex": 3}
+SUM_ORDERS = {"reference": 0, "tree": 1}
+DEVSTAT_WAIT_TIMEOUT = 1
 
 
 class AbhsfError(RuntimeError):
@@ -57,7 +59,7 @@ _ERR = {INVALID_VALUE: InvalidValue, INDEX_OUT_OF_RANGE: IndexOutOfRange, DUPLIC
 class BuildOpts(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("value_type", C.c_int32), ("allow_csr", C.c_int32),
                 ("matrix_type", C.c_int32), ("forced_scheme", C.c_int32), ("inputs_on_device", C.c_int32),
-                ("bits_per_value", C.c_int64)]
+                ("sum_order", C.c_int32), ("bits_per_value", C.c_int64)]
 
 
 class Stats(C.Structure):
@@ -83,6 +85,7 @@ PROTOTYPES = {
     "abhsf_spmv": (C.c_int, [_vp, _vp, _vp, _vp]),
     "abhsf_spmv_host": (C.c_int, [_vp, _vp, _vp, _vp]),
     "abhsf_release": (C.c_int, [_vp]),
+    "abhsf_device_status": (C.c_int, [_vp, _vp, _i32, C.POINTER(_i32)]),
     "abhsf_stats_get": (C.c_int, [_vp, C.POINTER(Stats)]),
     "abhsf_export_host": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "abhsf_block_histogram": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _i32, _i32, _vp, _u64p, _i64,
@@ -90,6 +93,7 @@ PROTOTYPES = {
     "abhsf_mmf_line": (C.c_int, [_i64, _i64, _i64, _i32, _i32, _i32, _u64p, _i64, _u64p, _u64p]),
     "abhsf_block_scheme_bits": (C.c_uint64, [_i32, _i64, _i64, _i64, _i64]),
     "abhsf_block_select_scheme": (_i32, [_i64, _i64, _i64, _i64, _i32, _i32]),
+    "abhsf_test_set_hooks": (None, [_i64, C.c_uint32]),
 }
 
 

@@ -128,6 +128,14 @@ __global__ void k_tile_meta(int64_t T, const int64_t* __restrict__ tile_start, c
     }
 }
 
+__global__ void k_narrow_rows(int64_t T, const int64_t* __restrict__ in, uint32_t* __restrict__ out)
+{
+    GRID_STRIDE(t, T)
+    {
+        out[t] = (uint32_t)in[t];
+    }
+}
+
 // brow_ptr[i] = first tile whose block row is >= i.
 __global__ void k_brow_ptr(int64_t M, int64_t T, const int64_t* __restrict__ tile_row, int64_t* __restrict__ brow_ptr)
 {
@@ -329,6 +337,14 @@ void raise_err(int e)
 
 }  // namespace
 
+void inclusive_scan_i64(const int64_t* in, int64_t* out, int64_t count, cudaStream_t st)
+{
+    size_t tmp_bytes = 0;
+    ABHSF_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, in, out, count, st));
+    dbuf<uint8_t> tmp(tmp_bytes);
+    ABHSF_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), tmp_bytes, in, out, count, st));
+}
+
 // Host computation of one mmf line (block_statistics/mmf.cpp:53-138) for a
 // given single-precision element width bits1 (32 for INTEGER / REAL, 64 for
 // COMPLEX, 0 for BINARY: mmf.cpp:34-47); the double line uses 2 * bits1.
@@ -424,6 +440,8 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
         fail(ABHSF_ERROR_UNSUPPORTED, "complex values are not stored by this build");
     if (o.forced_scheme < -1 || o.forced_scheme > 3)
         fail(ABHSF_ERROR_INVALID_VALUE, "forced_scheme must be -1 or 0..3");
+    if (o.sum_order != ABHSF_SUM_REFERENCE && o.sum_order != ABHSF_SUM_TREE)
+        fail(ABHSF_ERROR_INVALID_VALUE, "sum_order must be ABHSF_SUM_REFERENCE or ABHSF_SUM_TREE");
     const bool binary = (o.matrix_type == ABHSF_MATRIX_BINARY);
     if (binary && o.forced_scheme == ABHSF_SCHEME_DENSE)
         fail(ABHSF_ERROR_INVALID_VALUE, "dense scheme is never used for binary matrices");
@@ -444,6 +462,7 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
 
     a.m = m; a.n = n; a.nnz = nnz; a.s = (int32_t)s; a.lg = lg;
     a.value_type = o.value_type; a.matrix_type = o.matrix_type;
+    a.sum_order = o.sum_order;
     a.M = M; a.N = N;
     ABHSF_CUDA(cudaGetDevice(&a.device));
 
@@ -490,7 +509,8 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
     a.n_values = read_scalar(a.tile_val_off.get() + T, st);
     a.payload_bytes = read_scalar(a.tile_idx_off.get() + T, st);
     a.payload.alloc(a.payload_bytes);
-    a.values.alloc(a.n_values * value_size(a.value_type));
+    // 16 bytes of padding: pipelined kernels copy 16-byte-aligned supersets of value ranges
+    a.values.alloc(a.n_values * value_size(a.value_type) + 16);
     ABHSF_CUDA(cudaMemsetAsync(a.payload.get(), 0, a.payload.size(), st));
     ABHSF_CUDA(cudaMemsetAsync(a.values.get(), 0, a.values.size(), st));
     if (nnz > 0) {
@@ -500,7 +520,13 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
                                                        a.values.get());
         check_launch("k_scatter");
     }
+    a.tile_row.alloc(T);
+    k_narrow_rows<<<grid_for(T), kThreads, 0, st>>>(T, tile_row.get(), a.tile_row.get());
+    check_launch("k_narrow_rows");
+    a.dev_status.alloc(1);
+    ABHSF_CUDA(cudaMemsetAsync(a.dev_status.get(), 0, sizeof(int), st));
     finish_stats(a, dense_bits, st);
+    prepare_ordered(a, st);
 }
 
 void block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r, int s,

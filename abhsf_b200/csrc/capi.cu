@@ -13,6 +13,14 @@ namespace {
 thread_local std::string g_last_error;
 }
 
+void spmv_dispatch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+{
+    if (a.sum_order == ABHSF_SUM_REFERENCE)
+        spmv_f64_ordered(a, x, y, st);
+    else
+        spmv_f64(a, x, y, st);
+}
+
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 void clear_last_error() { g_last_error.clear(); }
 
@@ -37,6 +45,7 @@ void abhsf_build_opts_default(abhsf_build_opts* o)
     o->matrix_type = ABHSF_MATRIX_REAL;
     o->forced_scheme = -1;
     o->inputs_on_device = 0;
+    o->sum_order = ABHSF_SUM_REFERENCE;
     o->bits_per_value = 0;
 }
 
@@ -68,7 +77,7 @@ abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double* y, abhsf
             fail(ABHSF_ERROR_INVALID_VALUE, "x and y must be non-NULL");
         if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 7)
             fail(ABHSF_ERROR_INVALID_VALUE, "x and y must be 8-byte aligned");
-        abhsf::spmv_f64(*a, x, y, reinterpret_cast<cudaStream_t>(stream));
+        abhsf::spmv_dispatch(*a, x, y, reinterpret_cast<cudaStream_t>(stream));
     });
 }
 
@@ -88,9 +97,24 @@ abhsf_status abhsf_spmv_host(abhsf_matrix* a, const double* x, double* y, abhsf_
             a->y_stage.alloc(a->m);
         ABHSF_CUDA(cudaMemcpyAsync(a->x_stage.get(), x, a->n * sizeof(double), cudaMemcpyHostToDevice, st));
         ABHSF_CUDA(cudaMemcpyAsync(a->y_stage.get(), y, a->m * sizeof(double), cudaMemcpyHostToDevice, st));
-        abhsf::spmv_f64(*a, a->x_stage.get(), a->y_stage.get(), st);
+        abhsf::spmv_dispatch(*a, a->x_stage.get(), a->y_stage.get(), st);
         ABHSF_CUDA(cudaMemcpyAsync(y, a->y_stage.get(), a->m * sizeof(double), cudaMemcpyDeviceToHost, st));
         ABHSF_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+abhsf_status abhsf_device_status(abhsf_matrix* a, abhsf_stream_t stream, int32_t clear, int32_t* out)
+{
+    return guarded([&] {
+        if (!a || !out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle and out must be non-NULL");
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        int v = 0;
+        ABHSF_CUDA(cudaMemcpyAsync(&v, a->dev_status.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (clear)
+            ABHSF_CUDA(cudaMemsetAsync(a->dev_status.get(), 0, sizeof(int), st));
+        ABHSF_CUDA(cudaStreamSynchronize(st));
+        *out = v;
     });
 }
 

@@ -158,8 +158,14 @@ struct abhsf_matrix {
     abhsf::dbuf<int64_t> tile_val_off;
     abhsf::dbuf<int64_t> tile_idx_off;
     abhsf::dbuf<uint8_t> payload;
-    abhsf::dbuf<uint8_t> values;  // n_values * value_size(value_type) bytes
+    abhsf::dbuf<uint8_t> values;  // n_values * value_size(value_type) bytes (+16 padding)
     abhsf_stats stats{};
+    int32_t sum_order = ABHSF_SUM_REFERENCE;
+    // reference-order SpMV: block row of every tile and each CTA's tile range
+    abhsf::dbuf<uint32_t> tile_row;
+    abhsf::dbuf<int64_t> ord_part;
+    int ord_ctas = 0;
+    abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
     // staging for abhsf_spmv_host
     abhsf::dbuf<double> x_stage, y_stage;
 

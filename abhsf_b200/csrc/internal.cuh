@@ -16,7 +16,18 @@ void block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int6
 void mmf_line_from_hist(int64_t m, int64_t n, int64_t nnz, int type, int64_t r, int64_t s,
                         const std::map<uint64_t, uint64_t>& hist, uint64_t bits1, uint64_t o1[8], uint64_t o2[8]);
 
-// y += A x for an f64 matrix, device pointers, ordered on st.
+// y += A x for an f64 matrix, device pointers, ordered on st: warp-tree sums.
 void spmv_f64(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+
+// y += A x with the reference CSR's per-row summation order (bitwise equal).
+void spmv_f64_ordered(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+
+// Per-matrix set-up of the reference-order kernel (CTA tile ranges).
+void prepare_ordered(abhsf_matrix& a, cudaStream_t st);
+
+// abhsf_spmv's choice between the two f64 kernels (abhsf_matrix::sum_order).
+void spmv_dispatch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+
+void inclusive_scan_i64(const int64_t* in, int64_t* out, int64_t count, cudaStream_t st);
 
 }  // namespace abhsf

@@ -46,7 +46,8 @@ def _ptr(a) -> int:
     return a.ctypes.data
 
 
-def _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_device) -> capi.BuildOpts:
+def _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_device,
+          sum_order="reference") -> capi.BuildOpts:
     o = capi.BuildOpts()
     capi.lib.abhsf_build_opts_default(C.byref(o))
     o.block_size = int(block_size)
@@ -59,6 +60,7 @@ def _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_pe
         o.forced_scheme = capi.SCHEME_NAMES.index(forced_scheme) if isinstance(forced_scheme, str) else int(forced_scheme)
     o.bits_per_value = int(bits_per_value)
     o.inputs_on_device = 1 if on_device else 0
+    o.sum_order = capi.SUM_ORDERS[sum_order]
     return o
 
 
@@ -75,10 +77,12 @@ class AbhsfMatrix:
     @classmethod
     def from_elements(cls, rows, cols, vals, m: int, n: int, *, block_size: int = 64, value_type: str = "f64",
                       allow_csr: bool = True, matrix_type: str = "real", forced_scheme=None,
-                      bits_per_value: int = 0, stream=None) -> "AbhsfMatrix":
+                      bits_per_value: int = 0, sum_order: str = "reference", stream=None) -> "AbhsfMatrix":
         """Builds from COO triplets (0-based, any order, no duplicates).
         Scheme per tile by exact minimum storage (msmf.h:35-63) unless
-        forced_scheme names one.  vals may be None for binary matrices."""
+        forced_scheme names one.  vals may be None for binary matrices.
+        sum_order "reference" makes spmv bitwise equal to the reference's CSR
+        spmv_naive; "tree" uses warp reduction trees."""
         on_dev = _is_cuda(rows)
         if on_dev:
             if not (_is_cuda(cols) and (vals is None or _is_cuda(vals))):
@@ -94,7 +98,7 @@ class AbhsfMatrix:
         if (cols.numel() if on_dev else cols.size) != nnz or (
                 vals is not None and (vals.numel() if on_dev else vals.size) != nnz):
             raise capi.InvalidValue(capi.INVALID_VALUE, "rows, cols and vals differ in length")
-        o = _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_dev)
+        o = _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_dev, sum_order)
         h = C.c_void_p()
         capi.check(capi.lib.abhsf_build(_ptr(rows) if nnz else None, _ptr(cols) if nnz else None,
                                         _ptr(vals) if (vals is not None and nnz) else None, nnz, int(m), int(n),
@@ -156,6 +160,14 @@ class AbhsfMatrix:
     def handle(self) -> int:
         self._check_open()
         return int(self._h.value)
+
+    def device_status(self, clear: bool = False, stream=None) -> int:
+        """ABHSF_DEVSTAT_* bits raised by kernels on this matrix (0 = none);
+        waits for the stream."""
+        self._check_open()
+        v = C.c_int32()
+        capi.check(capi.lib.abhsf_device_status(self._h, _stream_ptr(stream), int(clear), C.byref(v)))
+        return int(v.value)
 
     # ------------------------------------------------------------------ introspection
     def stats(self) -> dict:

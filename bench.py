@@ -194,7 +194,7 @@ def run_ours(args):
 
     c = workload(args.n)
     t0 = time.time()
-    A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64)
+    A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64, sum_order=args.sum_order)
     torch.cuda.synchronize()
     build_s = time.time() - t0
     st = A.stats()
@@ -256,6 +256,9 @@ def run_ours(args):
     peak, peak_src = hbm_peak()
     achieved = B / (t_mean * 1e-3) / 1e9
     cpu = None
+    status = A.device_status()
+    if status:
+        raise RuntimeError(f"SpMV kernel reported device status {status}")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_run(c, B, max_seconds=20.0, max_iters=40)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -271,11 +274,12 @@ def run_ours(args):
                 "msmf_min_bytes_per_step": st["msmf_bits"][6] // 8 + 8 * c.n + 16 * c.m,
                 "l2": "256 MiB buffer written between steps (and 600 MB working set > 126 MB L2)",
                 "gflops": 2.0 * c.nnz / (t_mean * 1e-3) / 1e9, "build_s": build_s,
-                "parallelism": f"replicas x{world}",
+                "parallelism": f"replicas x{world}", "sum_order": args.sum_order,
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": ncu_traffic_per_launch(),
-                         "peak_source": peak_src, "kernel": "k_spmv_f64<64>"},
+                         "peak_source": peak_src,
+                         "kernel": "k_spmv_f64_ordered<64>" if args.sum_order == "reference" else "k_spmv_f64<64>"},
             "cpu_baseline": cpu,
             "e2e": {"value": world * B / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
                     "d2h_bytes_per_step": 8 * c.m, "ms_per_step": e2e_s * 1e3},
@@ -296,6 +300,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
+    ap.add_argument("--sum-order", choices=["reference", "tree"], default="reference",
+                    help="reference: bitwise the reference CSR's y; tree: warp reduction trees")
     ap.add_argument("--n", type=int, default=4_194_304,
                     help="matrix order of the tiled mixture (smaller only for profiling captures)")
     args = ap.parse_args()

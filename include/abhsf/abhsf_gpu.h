@@ -77,6 +77,19 @@ typedef enum abhsf_value_type {
     ABHSF_VALUE_BF16 = 2 /* RNE(RN_f32(f64)) */
 } abhsf_value_type;
 
+/* Summation order of y += A x.  REFERENCE adds each row's products one at a
+ * time, columns ascending, onto y (each product rounded first): bitwise the
+ * result of the reference's CSR spmv_naive (spmv/bottlenecks/spmv.cpp:58-64).
+ * TREE sums each row with warp-level reduction trees (error within the usual
+ * n u (|A||x|) bound, bitwise reproducible run to run). */
+typedef enum abhsf_sum_order {
+    ABHSF_SUM_REFERENCE = 0,
+    ABHSF_SUM_TREE = 1
+} abhsf_sum_order;
+
+/* Bits of the per-matrix device status word (abhsf_device_status). */
+#define ABHSF_DEVSTAT_WAIT_TIMEOUT 1 /* a bounded pipeline wait gave up; y is incomplete */
+
 /* include/abhsf/utils/matrix_properties.h:8-14 */
 typedef enum abhsf_matrix_type {
     ABHSF_MATRIX_BINARY = 0,
@@ -92,6 +105,7 @@ typedef struct abhsf_build_opts {
     int32_t matrix_type;      /* abhsf_matrix_type; BINARY never selects dense and stores 1.0 values */
     int32_t forced_scheme;    /* -1: minimum storage; 0..3: this scheme for every tile */
     int32_t inputs_on_device; /* rows / cols / vals are device pointers */
+    int32_t sum_order;        /* abhsf_sum_order of abhsf_spmv / abhsf_spmv_host */
     int64_t bits_per_value;   /* dense-cost element width; 0 = width of value_type */
 } abhsf_build_opts;
 
@@ -111,7 +125,8 @@ typedef struct abhsf_stats {
                                values included (block_statistics/mmf.cpp:122-138) */
 } abhsf_stats;
 
-/* Fills the defaults: s = 64, f64, CSR allowed, REAL, minimum storage, host inputs. */
+/* Fills the defaults: s = 64, f64, CSR allowed, REAL, minimum storage, host
+ * inputs, reference summation order. */
 ABHSF_API void abhsf_build_opts_default(abhsf_build_opts* opts);
 
 /* Builds the format on the GPU from COO triplets (any order, no duplicates).
@@ -165,6 +180,11 @@ ABHSF_API abhsf_status abhsf_mmf_line(int64_t m, int64_t n, int64_t nnz, int32_t
 ABHSF_API uint64_t abhsf_block_scheme_bits(int32_t scheme, int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value);
 ABHSF_API int32_t abhsf_block_select_scheme(int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value, int32_t is_binary,
                                   int32_t allow_csr);
+
+/* Waits for the work queued on stream, then returns the matrix's device
+ * status word (ABHSF_DEVSTAT_* bits; 0 = every SpMV so far completed) and,
+ * if clear != 0, resets it. */
+ABHSF_API abhsf_status abhsf_device_status(abhsf_matrix* a, abhsf_stream_t stream, int32_t clear, int32_t* out);
 
 /* Reason for the last non-success status returned on this thread. */
 ABHSF_API const char* abhsf_last_error_string(void);

@@ -28,21 +28,39 @@ def run_spmv(A, x, y0):
     return yd.cpu().numpy()
 
 
+def reference_order_y(coo, x, y0):
+    """The reference CSR's y: products added one at a time per row, columns
+    ascending (the oracle loop on row-major sorted elements reproduces the
+    reference's spmv_naive bit for bit, tests/test_oracle_golden.py)."""
+    order = np.lexsort((coo.cols, coo.rows))
+    return oracle.spmv_elements(coo.rows[order], coo.cols[order], coo.vals[order], x, y0.copy())
+
+
+def check_y(order, y, coo, x, y0):
+    if order == "reference":
+        np.testing.assert_array_equal(y, reference_order_y(coo, x, y0))
+    else:
+        ref = oracle.spmv_elements(coo.rows, coo.cols, coo.vals, x, y0.copy())
+        scale = oracle.abs_spmv(coo.rows, coo.cols, coo.vals, x, coo.m) + np.abs(y0)
+        assert_spmv_close(y, ref, scale)
+
+
+@pytest.mark.parametrize("order", ["reference", "tree"])
 @pytest.mark.parametrize("s", [16, 32, 64, 128, 256])
 @pytest.mark.parametrize("forced", [None, "coo", "csr", "bitmap", "dense"])
-def test_spmv_matches_oracle_all_schemes(gpu, s, forced):
+def test_spmv_matches_oracle_all_schemes(gpu, s, forced, order):
     for name, coo in MATS.items():
         x = W.rhs(coo.n, 11)
         y0 = W.rhs(coo.m, 12)
-        ref = oracle.spmv_elements(coo.rows, coo.cols, coo.vals, x, y0.copy())
-        scale = oracle.abs_spmv(coo.rows, coo.cols, coo.vals, x, coo.m) + np.abs(y0)
-        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, forced_scheme=forced)
-        y = run_spmv(A, x, y0)
-        assert_spmv_close(y, ref, scale)
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, forced_scheme=forced,
+                                      sum_order=order)
+        check_y(order, run_spmv(A, x, y0), coo, x, y0)
+        assert A.device_status() == 0
         A.release()
 
 
-def test_spmv_matches_reference_csr_golden(gpu):
+@pytest.mark.parametrize("order", ["reference", "tree"])
+def test_spmv_matches_reference_csr_golden(gpu, order):
     ref = golden_spmv()
     n_checked = 0
     for name, coo in MATS.items():
@@ -51,24 +69,55 @@ def test_spmv_matches_reference_csr_golden(gpu):
         x, y0, yr = ref[name + "__x"], ref[name + "__y0"], ref[name + "__y"]
         scale = oracle.abs_spmv(coo.rows, coo.cols, coo.vals, x, coo.m) + np.abs(y0)
         for s in (16, 64, 256):
-            A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s)
-            assert_spmv_close(run_spmv(A, x, y0), yr, scale)
+            A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, sum_order=order)
+            y = run_spmv(A, x, y0)
+            if order == "reference":
+                np.testing.assert_array_equal(y, yr, err_msg=f"{name} s={s}")
+            else:
+                assert_spmv_close(y, yr, scale)
             A.release()
         n_checked += 1
     assert n_checked >= 6
 
 
-def test_spmv_config1_against_golden(gpu):
+@pytest.mark.parametrize("order", ["reference", "tree"])
+def test_spmv_config1_against_golden(gpu, order):
     c = W.laplacian_2d(512)
     x = W.rhs(c.n, 0)
     yr = golden_spmv()["laplace2d_512__y_seed0"]
-    A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64)
+    A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64, sum_order=order)
     y = run_spmv(A, x, np.zeros(c.m))
     scale = oracle.abs_spmv(c.rows, c.cols, c.vals, x, c.m)
     worst_scaled, worst_rel = assert_spmv_close(y, yr, scale)
-    # tree-ordered sums: the scaled bound holds; |dy|/|y| alone is order
-    # dependent on rows that cancel (4 x_i minus four neighbours)
-    assert worst_scaled <= 1e-13, worst_scaled
+    if order == "reference":
+        # bitwise the reference CSR's y: 0 relative error on every element
+        np.testing.assert_array_equal(y, yr)
+    else:
+        # tree-ordered sums: the scaled bound holds; |dy|/|y| alone is order
+        # dependent on rows that cancel (4 x_i minus four neighbours)
+        assert worst_scaled <= 1e-13, worst_scaled
+
+
+def test_wait_timeout_sets_status_and_context_survives(gpu):
+    """A pipeline wait that runs out (its copies are never issued) ends the
+    kernel with ABHSF_DEVSTAT_WAIT_TIMEOUT instead of hanging; the context and
+    the matrix stay usable."""
+    import torch
+    coo = W.random_blocky(2000, 2000, 64, 300, seed=31)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    x = W.rhs(coo.n, 1)
+    y0 = np.zeros(coo.m)
+    try:
+        capi.lib.abhsf_test_set_hooks(2, 1 << 12)
+        run_spmv(A, x, y0)
+        st = A.device_status(clear=True)
+    finally:
+        capi.lib.abhsf_test_set_hooks(-1, 0)
+    assert st & capi.DEVSTAT_WAIT_TIMEOUT
+    y = run_spmv(A, x, y0)
+    assert A.device_status() == 0
+    np.testing.assert_array_equal(y, reference_order_y(coo, x, y0))
+    torch.cuda.synchronize()
 
 
 def test_host_pointer_path_equals_device_path(gpu):
@@ -82,10 +131,11 @@ def test_host_pointer_path_equals_device_path(gpu):
     np.testing.assert_array_equal(yh, yd)
 
 
-def test_spmv_is_deterministic(gpu):
+@pytest.mark.parametrize("order", ["reference", "tree"])
+def test_spmv_is_deterministic(gpu, order):
     coo = W.random_blocky(3000, 3000, 64, 400, seed=21)
     x = W.rhs(coo.n, 5)
-    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64, sum_order=order)
     ys = [run_spmv(A, x, np.zeros(coo.m)) for _ in range(3)]
     np.testing.assert_array_equal(ys[0], ys[1])
     np.testing.assert_array_equal(ys[0], ys[2])
@@ -121,11 +171,13 @@ def test_device_inputs_build(gpu):
 @pytest.mark.parametrize("s", [64])
 def test_tiled_mixture_full_size(gpu, s):
     """The throughput workload at full size (n = 4,194,304, ~60M nnz): format
-    statistics against the oracle histogram and the cost model, y against the
-    FP64 oracle loop."""
+    statistics against the oracle histogram and the cost model; y bitwise
+    against the reference CSR (reference order) and within the bound against
+    the FP64 oracle loop (tree order)."""
     c = W.tiled_mixture()
     assert 50_000_000 < c.nnz < 70_000_000
     A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=s)
+    B = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=s, sum_order="tree")
     st = A.stats()
     hist = oracle.block_histogram(c.rows, c.cols, 6, 6)
     assert st["tiles"] == sum(hist.values())
@@ -137,4 +189,13 @@ def test_tiled_mixture_full_size(gpu, s):
     y0 = W.rhs(c.m, 2)
     ref = oracle.spmv_elements(c.rows, c.cols, c.vals, x, y0.copy())
     scale = oracle.abs_spmv(c.rows, c.cols, c.vals, x, c.m) + np.abs(y0)
-    assert_spmv_close(run_spmv(A, x, y0), ref, scale)
+    assert_spmv_close(run_spmv(B, x, y0), ref, scale)
+    if oracle.RefCSR.available():
+        yr = y0.copy()
+        R = oracle.RefCSR(c.rows, c.cols, c.vals, c.m, c.n)
+        R.spmv(x, yr)
+        R.release()
+    else:
+        yr = reference_order_y(c, x, y0)
+    np.testing.assert_array_equal(run_spmv(A, x, y0), yr)
+    assert A.device_status() == 0
