@@ -337,6 +337,14 @@ void raise_err(int e)
 
 }  // namespace
 
+void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t count, cudaStream_t st)
+{
+    size_t tmp_bytes = 0;
+    ABHSF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, in, out, count, st));
+    dbuf<uint8_t> tmp(tmp_bytes);
+    ABHSF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tmp_bytes, in, out, count, st));
+}
+
 void inclusive_scan_i64(const int64_t* in, int64_t* out, int64_t count, cudaStream_t st)
 {
     size_t tmp_bytes = 0;

@@ -161,9 +161,11 @@ struct abhsf_matrix {
     abhsf::dbuf<uint8_t> values;  // n_values * value_size(value_type) bytes (+16 padding)
     abhsf_stats stats{};
     int32_t sum_order = ABHSF_SUM_REFERENCE;
-    // reference-order SpMV: block row of every tile and each CTA's tile range
+    // reference-order SpMV: block row of every tile, chunk schedule, stream ranges
     abhsf::dbuf<uint32_t> tile_row;
-    abhsf::dbuf<int64_t> ord_part;
+    abhsf::dbuf<uint8_t> ord_items;     // 64-byte chunk descriptors
+    abhsf::dbuf<int64_t> ord_streams;   // [ord_ctas * groups + 1] chunk range of each stream
+    int64_t ord_nitems = 0;
     int ord_ctas = 0;
     abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
     // staging for abhsf_spmv_host

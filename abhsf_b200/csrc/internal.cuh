@@ -29,5 +29,6 @@ void prepare_ordered(abhsf_matrix& a, cudaStream_t st);
 void spmv_dispatch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
 
 void inclusive_scan_i64(const int64_t* in, int64_t* out, int64_t count, cudaStream_t st);
+void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t count, cudaStream_t st);
 
 }  // namespace abhsf

@@ -1,7 +1,7 @@
 // spmv_f64.cu -- y += A x over the ABHSF format, FP64 values, sm_100a.
 //
-// One warp owns one block row (s rows of y) at a time and walks its tiles in
-// column order.  Per tile it dispatches on the scheme:
+// One warp (a CTA of its own) owns one block row (s rows of y) and walks its
+// tiles in column order.  Per tile it dispatches on the scheme:
 //
 //  * bitmap / dense, s >= 32: lane l owns columns l, l+32, ... of the tile and
 //    keeps those x values in registers.  Rows are taken 16 at a time; for each
@@ -27,7 +27,10 @@
 namespace abhsf {
 namespace {
 
-constexpr int kWarps = 8;
+// One warp (one block row) per CTA: block rows differ widely in work, and a
+// CTA of several warps holds its SM slot until its slowest warp is done.
+constexpr int kWarps = 1;
+constexpr int kMinCtasPerSm = 24;  // caps registers so ~24-32 warps stay resident per SM
 constexpr unsigned kFull = 0xffffffffu;
 
 template <int S>
@@ -230,7 +233,7 @@ __device__ __forceinline__ void tile_stream(const uint8_t* __restrict__ pay, con
 }
 
 template <int S>
-__global__ void __launch_bounds__(kWarps * 32) k_spmv_f64(tiles_view A, const double* __restrict__ x,
+__global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_f64(tiles_view A, const double* __restrict__ x,
                                                           double* __restrict__ y)
 {
     constexpr int CPL = geom<S>::CPL;

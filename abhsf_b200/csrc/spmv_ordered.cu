@@ -4,24 +4,36 @@
 // The reference's CSR SpMV (csr_matrix::spmv_naive,
 // spmv/bottlenecks/spmv.cpp:58-64) adds the products of a row one at a time,
 // columns ascending, onto y[row], each product rounded before its add.  This
-// kernel reproduces that order exactly: thread r of a CTA owns row r of the
-// current block row, walks the block row's tiles in column order and, inside
-// a tile, its row's nonzeros in column order, accumulating
-// acc = dadd_rn(acc, dmul_rn(v, x)) from acc = y0.  The result is therefore
-// bitwise identical to the reference CSR's y.
+// kernel reproduces that order exactly: thread r of a row group owns row r of
+// the current block row, walks the block row's tiles in column order and,
+// inside a tile, its row's nonzeros in column order, accumulating
+// acc = dadd_rn(acc, product) from acc = y0.  The result is bitwise the
+// reference CSR's y.
 //
-// The bytes reach shared memory through a TMA bulk-copy pipeline: each tile
-// is cut into chunks of at most kVcap stored values; one lane issues
-// cp.async.bulk copies of a chunk's values, payload (COO keys / CSR row ends
-// and columns / bitmap) and the x and y segments into one of kSlots shared
-// memory slots, kSlots - 1 chunks ahead of the chunk being summed, with an
-// mbarrier tracking the bytes.  Global reads are therefore whole contiguous
-// ranges (no per-lane gathers); the per-row sequential sums read shared
-// memory.  Each CTA owns a contiguous, byte-balanced range of block rows
-// (computed once per matrix), so no two CTAs touch one y entry.
+// Data movement (persistent, one CTA per SM):
+//  * Once per matrix a schedule is built: tiles are cut into chunks of at most
+//    VC stored values (fewer for COO / CSR when their index payload would not
+//    fit), and the chunk list is split into G * gridDim byte-balanced streams,
+//    each a whole number of block rows.  A chunk descriptor holds the
+//    16-byte-aligned value and payload ranges to copy.
+//  * Warp 0 is the producer: lane g feeds row group g.  For each chunk of its
+//    stream it waits until a slot of the group's R-slot ring is free (empty
+//    mbarrier), copies the descriptor in, and issues cp.async.bulk copies of
+//    the values, payload, x segment and (at a block row's start) y segment,
+//    counted on the slot's full mbarrier.  Up to R chunks per group are in
+//    flight, so shared memory is mostly bytes in transit.
+//  * Row group g (NTG >= S threads, named barrier 1 + g) consumes its chunks
+//    in order, up to s = 64 a chunk being a whole tile: (A) a tile's first
+//    chunk puts its row starts (bitmap popcount scan / CSR row ends) and
+//    bitmap in shared memory; (B) all NTG threads turn values into products
+//    in place, the lanes of a warp on consecutive columns of one row (a dense
+//    tile's stored zeros become -0.0, which leaves any sum bitwise unchanged);
+//    (C) thread r < S adds its row's products -- a contiguous range -- one at
+//    a time onto its accumulator.  Thread 0 then releases the slot.
 //
-// Every mbarrier wait is bounded: after kSpinLimit failed polls the CTA
-// records ABHSF_DEVSTAT_WAIT_TIMEOUT in the matrix's status word and stops.
+// Every wait is bounded.  A wait that gives up records
+// ABHSF_DEVSTAT_WAIT_TIMEOUT in the matrix's status word; the producer then
+// waits (bounded) for every copy it issued before the CTA exits.
 #include <algorithm>
 
 #include "abhsf/abhsf_test.h"
@@ -35,45 +47,89 @@ namespace {
 int64_t g_drop_item = -1;
 uint32_t g_spin_limit = 0;
 
-constexpr int kSlots = 4;         // pipeline depth (chunks resident per CTA)
-constexpr int kVcap = 1024;       // stored values per chunk
-constexpr int kHdr = 64;          // tile headers cached per refill
-constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr uint32_t kConsumerPolls = 1u << 21;  // try_wait polls of <= ~1 us each
+constexpr uint32_t kProducerPolls = 1u << 27;  // non-blocking test_wait polls
 
-enum : int32_t { F_FIRST_CHUNK = 1, F_ROW_BEGIN = 2, F_ROW_END = 4, F_X_STAGED = 8, F_Y_STAGED = 16, F_NONE = 32 };
+enum : uint32_t { F_FIRST_CHUNK = 1, F_ROW_BEGIN = 2, F_ROW_END = 4, F_X_OK = 8, F_Y_OK = 16, F_X_STAGED = 32, F_Y_STAGED = 64 };
 
+// Geometry per block size.  G row groups of NTG threads, R slots per group.
 template <int S>
 struct og {
-    static constexpr int NT = S < 32 ? 32 : S;  // threads per CTA; thread r owns row r
+    // NTG threads per row group: all of them form products, the first S sum rows
+    static constexpr int NTG = S <= 32 ? 64 : S == 64 ? 128 : 256;
+    static constexpr int NWG = NTG / 32;
+    // row groups per CTA and slots per group: smem ~ G * R * SLOT <= 225 KB
+    static constexpr int G = S == 16 ? 12 : S == 32 ? 7 : S == 64 ? 2 : 1;
+    static constexpr int R = S == 16 ? 4 : S == 32 ? 3 : S == 64 ? 3 : S == 128 ? 3 : 4;
+    // stored values per chunk: a whole tile up to s = 64
+    static constexpr int VC = S <= 64 ? S * S : S == 128 ? 8192 : 4096;
     static constexpr int LG = S == 16 ? 4 : S == 32 ? 5 : S == 64 ? 6 : S == 128 ? 7 : 8;
-    static constexpr int W64 = S >= 64 ? S / 64 : 1;  // u64 words per bitmap row
+    static constexpr int CPL = S >= 32 ? S / 32 : 1;         // 32-column groups per row
+    static constexpr int LPR = S >= 32 ? 32 : S;             // lanes per row in the product phase
     static constexpr int BM_BYTES = S * S / 8;
-    static constexpr int c1 = BM_BYTES > 2 * kVcap ? BM_BYTES : 2 * kVcap;
-    static constexpr int c2 = 2 * S + kVcap;
-    static constexpr int PCAP = ((c1 > c2 ? c1 : c2) + 16 + 15) & ~15;  // payload area
-    static constexpr int VBYTES = kVcap * 8 + 16;                       // value area
-    static constexpr int SEG = S * 8 < 16 ? 16 : S * 8;                 // x / y segment
-    static constexpr int SLOT = 2 * SEG + PCAP + VBYTES;
+    static constexpr int BMW = S * S / 32 < 4 ? 4 : S * S / 32;  // u32 words of a tile bitmap
+    static constexpr int PCAP = (BM_BYTES > 1024 ? BM_BYTES : 1024) + 16;  // payload area
+    // chunk caps: the values (VC) and the index payload (PCAP) must both fit
+    static constexpr int COO_MAX = (PCAP - 16) / 2 < VC ? (PCAP - 16) / 2 : VC;  // COO elements per chunk
+    static constexpr int CSR0_MAX = PCAP - 16 - 2 * S < VC ? PCAP - 16 - 2 * S : VC;  // CSR, tile's first chunk
+    static constexpr int CSR_MAX = PCAP - 16 < VC ? PCAP - 16 : VC;                 // CSR, later chunks
+    static constexpr int SEG = S * 8 < 16 ? 16 : S * 8;      // x / y segment bytes
+    static constexpr int VBYTES = VC * 8 + 16;
+    static constexpr int DESC = 64;
+    static constexpr int SLOT = DESC + 2 * SEG + PCAP + VBYTES;
+    static constexpr int NT = 32 + G * NTG;
 };
 
-struct item_desc {
+struct __align__(16) item_t {
+    uint64_t voff;    // byte offset of the copied (16-byte aligned) value range
+    uint64_t poff;    // byte offset of the copied payload range
+    uint32_t vbytes;  // bytes copied (multiple of 16)
+    uint32_t pbytes;
     uint32_t row, col;
-    int32_t z, k0, k1, scheme, vpre, ppre, flags, pad;
+    int32_t k0, k1;   // stored-value range [k0, k1) of the tile in this chunk
+    int32_t z;
+    int16_t vpre;     // bytes from the copy start to value k0
+    int16_t ppre;     // bytes from the copy start to this chunk's payload
+    uint8_t scheme, flags;
+    uint8_t pad[14];
 };
+static_assert(sizeof(item_t) == 64, "descriptor is 64 bytes");
 
-struct hdr_cache {
-    uint32_t col[kHdr], nnz[kHdr], row[kHdr];
-    int64_t val_off[kHdr], idx_off[kHdr];
-    uint8_t scheme[kHdr];
+// Every bulk copy stays inside its slot area (values <= VC, payload <= PCAP).
+template <int S>
+struct og_checks {
+    using Gm = og<S>;
+    static_assert(Gm::COO_MAX <= Gm::VC && Gm::CSR0_MAX <= Gm::VC && Gm::CSR_MAX <= Gm::VC, "chunk values fit");
+    static_assert(((2 * Gm::COO_MAX + 15 + 15) & ~15) <= Gm::PCAP, "COO keys fit");
+    static_assert(((2 * S + Gm::CSR0_MAX + 15) & ~15) <= Gm::PCAP, "CSR first chunk fits");
+    static_assert(((Gm::CSR_MAX + 15 + 15) & ~15) <= Gm::PCAP, "CSR later chunk fits");
+    static_assert(Gm::BM_BYTES <= Gm::PCAP, "bitmap fits");
+    static_assert(((Gm::VC * 8 + 8 + 15) & ~15) <= Gm::VBYTES, "values fit");
+    static constexpr bool ok = true;
+};
+static_assert(og_checks<16>::ok && og_checks<32>::ok && og_checks<64>::ok && og_checks<128>::ok &&
+                  og_checks<256>::ok,
+              "slot geometry");
+// one CTA per SM: G rings of R slots within the 227 KB a CTA may use
+static_assert(og<16>::G * og<16>::R * og<16>::SLOT <= 225 * 1024 && og<32>::G * og<32>::R * og<32>::SLOT <= 225 * 1024 &&
+                  og<64>::G * og<64>::R * og<64>::SLOT <= 225 * 1024 &&
+                  og<128>::G * og<128>::R * og<128>::SLOT <= 225 * 1024 &&
+                  og<256>::G * og<256>::R * og<256>::SLOT <= 225 * 1024,
+              "shared memory per CTA");
+
+template <int S>
+struct group_smem {
+    unsigned long long full[og<S>::R], empty[og<S>::R];
+    int32_t scan[og<S>::NWG + 1];
+    int32_t failed;
+    int32_t rs[S + 1];                         // current tile: first stored value of each row
+    alignas(16) uint32_t tbm[og<S>::BMW];      // current tile's bitmap (bitmap tiles)
+    alignas(16) unsigned char slot[og<S>::R][og<S>::SLOT];
 };
 
 template <int S>
-struct __align__(16) ordered_smem {
-    unsigned long long bar[kSlots];
-    item_desc desc[kSlots];
-    hdr_cache hc;
-    int32_t scan[og<S>::NT / 32 + 1];
-    alignas(16) unsigned char slot[kSlots][og<S>::SLOT];
+struct ordered_smem {
+    group_smem<S> g[og<S>::G];
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -89,15 +145,41 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, uint32_t
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Blocking poll, suspended at most ~1 us per call.
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t parity)
 {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(1000u)
+        : "memory");
+    return ok != 0;
+}
+
+// Non-blocking probe.
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
         : "r"(smem_addr(bar)), "r"(parity)
         : "memory");
     return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity, uint32_t limit)
+{
+    for (uint32_t it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, parity))
+            return true;
+    return false;
 }
 
 // Global -> shared bulk copy (no multicast); completion counted on bar.
@@ -109,385 +191,481 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  : "memory");
 }
 
-// Bounded wait; false (and the status word set) on timeout.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity, int* status, uint32_t limit)
+__device__ __forceinline__ void group_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+
+// Group-wide OR of pred (named barrier reduction).
+__device__ __forceinline__ bool group_any(int id, int n, bool pred)
 {
-    for (uint32_t it = 0; it < limit; ++it)
-        if (mbar_try_wait(bar, parity))
-            return true;
-    atomicOr(status, ABHSF_DEVSTAT_WAIT_TIMEOUT);
-    return false;
+    uint32_t out;
+    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+                 : "=r"(out)
+                 : "r"((uint32_t)pred), "r"(id), "r"(n)
+                 : "memory");
+    return out != 0;
 }
 
 __device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
 
 struct ord_args {
-    tiles_view A;
-    const uint32_t* tile_row;
-    const int64_t* part;  // [gridDim.x + 1] tile ranges
+    const item_t* items;
+    const int64_t* sb;  // [gridDim.x * G + 1] item range of each stream
+    const unsigned char* values;
+    const unsigned char* payload;
     const double* x;
     double* y;
+    int64_t m, n;
     int* status;
     int aligned_xy;       // x and y 16-byte aligned: segments may be bulk-copied
-    uint32_t spin_limit;  // polls per wait before giving up
-    int64_t drop_item;    // test hook: pipeline item whose copies are not issued (-1: none)
+    uint32_t spin_limit;  // consumer polls per wait (0: default)
+    int64_t drop_item;    // test hook: per-stream item whose copies are not issued (-1: none)
 };
 
 template <int S>
-__global__ void __launch_bounds__(og<S>::NT) k_spmv_f64_ordered(ord_args P)
+__device__ void producer(const ord_args& P, ordered_smem<S>& sm, int lane)
 {
-    using G = og<S>;
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    ordered_smem<S>& sm = *reinterpret_cast<ordered_smem<S>*>(dyn_smem);
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int64_t t_begin = P.part[blockIdx.x], t_end = P.part[blockIdx.x + 1];
-    if (t_begin >= t_end)
+    using Gm = og<S>;
+    if (lane >= Gm::G)
         return;
-    const tiles_view& A = P.A;
-    const double* __restrict__ values = static_cast<const double*>(A.values);
-
-    if (tid == 0) {
-        for (int s = 0; s < kSlots; ++s)
-            mbar_init(&sm.bar[s], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    group_smem<S>& gs = sm.g[lane];
+    const int64_t q = (int64_t)blockIdx.x * Gm::G + lane;
+    const int64_t ib = P.sb[q], ie = P.sb[q + 1];
+    int64_t it = ib;
+    uint32_t polls = 0;
+    bool gave_up = false;
+    while (it < ie) {
+        const int64_t u = it - ib;  // chunk number within the stream
+        const int slot = (int)(u % Gm::R);
+        const uint32_t use = (uint32_t)(u / Gm::R);
+        if (!mbar_test_wait(&gs.empty[slot], (use & 1) ^ 1)) {
+            if (++polls > kProducerPolls || *(volatile int32_t*)&gs.failed) {
+                gave_up = true;
+                break;
+            }
+            continue;
+        }
+        item_t d = P.items[it];
+        unsigned char* base = gs.slot[slot];
+        const bool xst = P.aligned_xy && (d.flags & F_X_OK);
+        const bool yst = P.aligned_xy && (d.flags & F_Y_OK) && (d.flags & F_ROW_BEGIN);
+        d.flags |= (xst ? F_X_STAGED : 0) | (yst ? F_Y_STAGED : 0);
+        *reinterpret_cast<item_t*>(base) = d;
+        unsigned char* ys = base + Gm::DESC;
+        unsigned char* xs = ys + Gm::SEG;
+        unsigned char* pay = xs + Gm::SEG;
+        unsigned char* vb = pay + Gm::PCAP;
+        const uint32_t bytes = d.vbytes + d.pbytes + (xst ? S * 8 : 0) + (yst ? S * 8 : 0);
+        if (u != P.drop_item) {
+            mbar_expect_tx(&gs.full[slot], bytes);
+            bulk_g2s(vb, P.values + d.voff, d.vbytes, &gs.full[slot]);
+            if (d.pbytes)
+                bulk_g2s(pay, P.payload + d.poff, d.pbytes, &gs.full[slot]);
+            if (xst)
+                bulk_g2s(xs, P.x + (int64_t)d.col * S, S * 8, &gs.full[slot]);
+            if (yst)
+                bulk_g2s(ys, P.y + (int64_t)d.row * S, S * 8, &gs.full[slot]);
+        }
+        ++it;
     }
-    __syncthreads();
+    if (gave_up)
+        atomicOr(P.status, ABHSF_DEVSTAT_WAIT_TIMEOUT);
+    // drain: every chunk this lane issued has landed before the CTA exits
+    const int64_t issued = it - ib;
+    for (int64_t u = (issued > Gm::R ? issued - Gm::R : 0); u < issued; ++u) {
+        if (u == P.drop_item)
+            continue;
+        if (!mbar_wait(&gs.full[u % Gm::R], (uint32_t)((u / Gm::R) & 1), kConsumerPolls))
+            atomicOr(P.status, ABHSF_DEVSTAT_WAIT_TIMEOUT);
+    }
+}
 
-    // ---------------- producer state (warp 0; lane 0 issues) ----------------
-    int64_t p_t = t_begin;  // tile of the next chunk to issue
-    int32_t p_k0 = 0;       // its first stored value
-    int64_t p_item = 0;     // index of the next chunk to issue
-    int64_t hc_base = -1;   // tiles cached in sm.hc: [hc_base, hc_base + kHdr)
-
-    // Issues the next chunk into slot s (warp 0 only, uniform control flow).
-    auto produce = [&](int s) {
-        if (p_t >= t_end) {
-            if (lane == 0)
-                sm.desc[s].flags = F_NONE;
+template <int S>
+__device__ void consumer(const ord_args& P, ordered_smem<S>& sm, int gidx, int r)
+{
+    using Gm = og<S>;
+    group_smem<S>& gs = sm.g[gidx];
+    const int bar_id = 1 + gidx;
+    const int lane = r & 31, warp = r >> 5;
+    const int64_t q = (int64_t)blockIdx.x * Gm::G + gidx;
+    const int64_t nitems = P.sb[q + 1] - P.sb[q];
+    const uint32_t limit = P.spin_limit ? P.spin_limit : kConsumerPolls;
+    double acc = 0.0;
+    for (int64_t u = 0; u < nitems; ++u) {
+        const int slot = (int)(u % Gm::R);
+        const bool ok = mbar_wait(&gs.full[slot], (uint32_t)((u / Gm::R) & 1), limit);
+        if (group_any(bar_id, Gm::NTG, !ok)) {
+            if (r == 0) {
+                *(volatile int32_t*)&gs.failed = 1;
+                atomicOr(P.status, ABHSF_DEVSTAT_WAIT_TIMEOUT);
+            }
             return;
         }
-        if (hc_base < 0 || p_t + 1 >= hc_base + kHdr) {  // refill: tile p_t and its successors
-            hc_base = p_t;
-            __syncwarp();
-            for (int j = lane; j < kHdr; j += 32) {
-                const int64_t t = hc_base + j;
-                if (t < t_end) {
-                    sm.hc.col[j] = A.tile_col[t];
-                    sm.hc.nnz[j] = A.tile_nnz[t];
-                    sm.hc.row[j] = P.tile_row[t];
-                    sm.hc.val_off[j] = A.tile_val_off[t];
-                    sm.hc.idx_off[j] = A.tile_idx_off[t];
-                    sm.hc.scheme[j] = A.tile_scheme[t];
-                }
-            }
-            __syncwarp();
-        }
-        const int h = (int)(p_t - hc_base);
-        const int sch = sm.hc.scheme[h];
-        const int32_t z = (int32_t)sm.hc.nnz[h];
-        const int32_t stored = sch == ABHSF_SCHEME_DENSE ? S * S : z;
-        const int32_t k0 = p_k0;
-        const int32_t k1 = min(stored, k0 + kVcap);
-        const uint32_t row = sm.hc.row[h], col = sm.hc.col[h];
-        int32_t flags = 0;
-        if (k0 == 0)
-            flags |= F_FIRST_CHUNK;
-        // the cache holds p_t and p_t + 1; p_t - 1 is read from global memory
-        // when it lies before the cache
-        if (k0 == 0) {
-            bool begin = (p_t == t_begin);
-            if (!begin)
-                begin = (h > 0 ? sm.hc.row[h - 1] : __ldg(P.tile_row + p_t - 1)) != row;
-            if (begin)
-                flags |= F_ROW_BEGIN;
-        }
-        if (k1 == stored) {
-            const bool end = (p_t + 1 == t_end) || sm.hc.row[h + 1] != row;
-            if (end)
-                flags |= F_ROW_END;
-        }
-        if (lane == 0) {
-            unsigned char* base = sm.slot[s];
-            unsigned char* ys = base;
-            unsigned char* xs = base + G::SEG;
-            unsigned char* pay = base + 2 * G::SEG;
-            unsigned char* vb = pay + G::PCAP;
-            uint32_t bytes = 0;
-            // values [k0, k1)
-            const uintptr_t vsrc = reinterpret_cast<uintptr_t>(values + sm.hc.val_off[h] + k0);
-            const uintptr_t val = vsrc & ~uintptr_t(15);
-            const int32_t vpre = (int32_t)(vsrc - val);
-            const uint32_t vbytes = (uint32_t)((vpre + (k1 - k0) * 8 + 15) & ~15);
-            // payload
-            const unsigned char* pbase = A.payload + sm.hc.idx_off[h];
-            uintptr_t psrc = 0;
-            uint32_t pbytes = 0;
-            int32_t ppre = 0;
-            if (sch == ABHSF_SCHEME_COO) {
-                const uintptr_t a = reinterpret_cast<uintptr_t>(pbase + 2 * k0);
-                psrc = a & ~uintptr_t(15);
-                ppre = (int32_t)(a - psrc);
-                pbytes = (uint32_t)((ppre + 2 * (k1 - k0) + 15) & ~15);
-            } else if (sch == ABHSF_SCHEME_CSR) {
-                if (k0 == 0) {
-                    psrc = reinterpret_cast<uintptr_t>(pbase);
-                    pbytes = (uint32_t)((2 * S + k1 + 15) & ~15);
-                } else {
-                    const uintptr_t a = reinterpret_cast<uintptr_t>(pbase + 2 * S + k0);
-                    psrc = a & ~uintptr_t(15);
-                    ppre = (int32_t)(a - psrc);
-                    pbytes = (uint32_t)((ppre + (k1 - k0) + 15) & ~15);
-                }
-            } else if (sch == ABHSF_SCHEME_BITMAP && k0 == 0) {
-                psrc = reinterpret_cast<uintptr_t>(pbase);
-                pbytes = (uint32_t)G::BM_BYTES;
-            }
-            const bool xst = P.aligned_xy && (int64_t)(col + 1) * S <= A.n && S * 8 >= 16;
-            const bool yst = P.aligned_xy && (flags & F_ROW_BEGIN) && (int64_t)(row + 1) * S <= A.m && S * 8 >= 16;
-            bytes = vbytes + pbytes + (xst ? S * 8 : 0) + (yst ? S * 8 : 0);
-            if (p_item != P.drop_item) {
-                mbar_expect_tx(&sm.bar[s], bytes);
-                bulk_g2s(vb, reinterpret_cast<const void*>(val), vbytes, &sm.bar[s]);
-                if (pbytes)
-                    bulk_g2s(pay, reinterpret_cast<const void*>(psrc), pbytes, &sm.bar[s]);
-                if (xst)
-                    bulk_g2s(xs, P.x + (int64_t)col * S, S * 8, &sm.bar[s]);
-                if (yst)
-                    bulk_g2s(ys, P.y + (int64_t)row * S, S * 8, &sm.bar[s]);
-            }
-            item_desc& d = sm.desc[s];
-            d.row = row;
-            d.col = col;
-            d.z = z;
-            d.k0 = k0;
-            d.k1 = k1;
-            d.scheme = sch;
-            d.vpre = vpre;
-            d.ppre = ppre;
-            d.flags = flags | (xst ? F_X_STAGED : 0) | (yst ? F_Y_STAGED : 0);
-        }
-        ++p_item;
-        if (k1 == stored) {
-            ++p_t;
-            p_k0 = 0;
-        } else {
-            p_k0 = k1;
-        }
-    };
-
-    if (tid < 32) {
-        for (int s = 0; s < kSlots - 1; ++s)
-            produce(s);
-    }
-    __syncthreads();
-
-    // ---------------- consumer state (thread r = row r) ----------------
-    const int r = tid;
-    double acc = 0.0;
-    // bitmap row still to visit: current word `cur` (index jb) and the rest
-    uint64_t bw[G::W64];
-    uint64_t cur = 0;
-    int jb = G::W64;
-    int32_t kr = 0;          // next stored-value index of this row (bitmap)
-    int32_t ra = 0, rb = 0;  // this row's element range (CSR)
-#pragma unroll
-    for (int j = 0; j < G::W64; ++j)
-        bw[j] = 0;
-
-    int64_t step = 0;
-    bool failed = false;
-    for (;; ++step) {
-        const int s = (int)(step % kSlots);
-        const item_desc d = sm.desc[s];
-        if (d.flags & F_NONE)
-            break;
-        if (tid < 32)
-            produce((int)((step + kSlots - 1) % kSlots));
-        const bool ok = mbar_wait(&sm.bar[s], (uint32_t)((step / kSlots) & 1), P.status, P.spin_limit);
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-            break;
-        }
-        const unsigned char* base = sm.slot[s];
-        const double* ys = reinterpret_cast<const double*>(base);
-        const double* xs = reinterpret_cast<const double*>(base + G::SEG);
-        const unsigned char* pay = base + 2 * G::SEG + d.ppre;
-        const double* vb = reinterpret_cast<const double*>(base + 2 * G::SEG + G::PCAP + d.vpre);
+        unsigned char* base = gs.slot[slot];
+        const item_t d = *reinterpret_cast<const item_t*>(base);
+        const double* ys = reinterpret_cast<const double*>(base + Gm::DESC);
+        const double* xs = reinterpret_cast<const double*>(base + Gm::DESC + Gm::SEG);
+        const unsigned char* pay = base + Gm::DESC + 2 * Gm::SEG + d.ppre;
+        double* vb = reinterpret_cast<double*>(base + Gm::DESC + 2 * Gm::SEG + Gm::PCAP + d.vpre);
         const int64_t grow = (int64_t)d.row * S + r;
-        const bool row_ok = r < S && grow < A.m;
+        const bool row_ok = r < S && grow < P.m;
         const int64_t c0 = (int64_t)d.col * S;
         const bool xst = (d.flags & F_X_STAGED) != 0;
         auto X = [&](int c) -> double { return xst ? xs[c] : __ldg(P.x + c0 + c); };
+        const int k0 = d.k0, k1 = d.k1, n = k1 - k0;
 
         if (d.flags & F_ROW_BEGIN)
             acc = row_ok ? ((d.flags & F_Y_STAGED) ? ys[r] : P.y[grow]) : 0.0;
 
-        const int k0 = d.k0, k1 = d.k1;
-        if (d.scheme == ABHSF_SCHEME_BITMAP) {
-            if (d.flags & F_FIRST_CHUNK) {
+        // ---- phase A: tile metadata (first chunk of a tile) ----
+        if (d.flags & F_FIRST_CHUNK) {
+            if (d.scheme == ABHSF_SCHEME_BITMAP) {
+                const uint4* src = reinterpret_cast<const uint4*>(pay);
+                uint4* dst = reinterpret_cast<uint4*>(gs.tbm);
+                for (int i = r; i < Gm::BM_BYTES / 16; i += Gm::NTG)
+                    dst[i] = src[i];
                 int pc = 0;
                 if (r < S) {
+                    if (S >= 32) {
 #pragma unroll
-                    for (int j = 0; j < G::W64; ++j) {
-                        uint64_t w;
-                        if (S >= 64) {
-                            w = reinterpret_cast<const uint64_t*>(pay + r * (S / 8))[j];
-                        } else {
-                            const uint64_t word = reinterpret_cast<const uint64_t*>(pay)[(r * S) >> 6];
-                            w = (word >> ((r * S) & 63)) & ((1ull << (S & 63)) - 1);
-                        }
-                        bw[j] = w;
-                        pc += __popcll(w);
+                        for (int j = 0; j < Gm::CPL; ++j)
+                            pc += __popc(reinterpret_cast<const uint32_t*>(pay)[r * Gm::CPL + j]);
+                    } else {
+                        const uint32_t w = reinterpret_cast<const uint32_t*>(pay)[(r * S) >> 5];
+                        pc = __popc((w >> ((r * S) & 31)) & ((1u << (S & 31)) - 1));
                     }
                 }
-                cur = bw[0];
-                jb = 0;
-                // block-wide exclusive scan of the row popcounts -> row starts
-                int inc = pc;
+                int inc = pc;  // exclusive scan of the row popcounts over the group
 #pragma unroll
                 for (int dd = 1; dd < 32; dd <<= 1) {
                     const int t = __shfl_up_sync(0xffffffffu, inc, dd);
                     if (lane >= dd)
                         inc += t;
                 }
-                if (G::NT > 32) {
+                if (Gm::NWG > 1) {
                     if (lane == 31)
-                        sm.scan[tid >> 5] = inc;
-                    __syncthreads();
+                        gs.scan[warp] = inc;
+                    group_sync(bar_id, Gm::NTG);
                     int off = 0;
-                    for (int w = 0; w < (tid >> 5); ++w)
-                        off += sm.scan[w];
+                    for (int w = 0; w < warp; ++w)
+                        off += gs.scan[w];
                     inc += off;
-                    __syncthreads();
                 }
-                kr = inc - pc;
-            }
-            if (r < S) {
-                // the row's values with index in [k0, k1), columns ascending
-                while (kr < k1) {
-                    double p[4];
-                    int cnt = 0;
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        while (cur == 0 && jb < G::W64 - 1) {
-                            ++jb;
-#pragma unroll
-                            for (int q = 0; q < G::W64; ++q)
-                                if (q == jb)
-                                    cur = bw[q];
-                        }
-                        if (cur != 0 && kr + cnt < k1) {
-                            const int b = __ffsll((long long)cur) - 1;
-                            cur &= cur - 1;
-                            p[u] = fmul(vb[kr + cnt - k0], X(jb * 64 + b));
-                            ++cnt;
-                        }
-                    }
-                    for (int u = 0; u < cnt; ++u)
-                        acc = fadd(acc, p[u]);
-                    kr += cnt;
-                    if (cnt < 4)
-                        break;
-                }
-            }
-        } else if (d.scheme == ABHSF_SCHEME_CSR) {
-            const unsigned char* cols;
-            if (d.flags & F_FIRST_CHUNK) {
-                const uint16_t* re = reinterpret_cast<const uint16_t*>(pay);
                 if (r < S) {
-                    ra = r == 0 ? 0 : re[r - 1];
-                    rb = re[r];
+                    gs.rs[r] = inc - pc;
+                    if (r == S - 1)
+                        gs.rs[S] = inc;
                 }
-                cols = pay + 2 * S;
-            } else {
-                cols = pay;
+            } else if (d.scheme == ABHSF_SCHEME_CSR) {
+                const uint16_t* re = reinterpret_cast<const uint16_t*>(pay);
+                if (r < S)
+                    gs.rs[r + 1] = re[r];
+                if (r == 0)
+                    gs.rs[0] = 0;
             }
-            if (r < S) {
-                const int lo = max(ra, k0), hi = min(rb, k1);
-                for (int i = lo; i < hi; i += 4) {
-                    double p[4];
-                    const int cnt = min(4, hi - i);
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        if (u < cnt)
-                            p[u] = fmul(vb[i + u - k0], X(cols[i + u - k0]));
-                    for (int u = 0; u < cnt; ++u)
-                        acc = fadd(acc, p[u]);
-                }
-            }
-        } else if (d.scheme == ABHSF_SCHEME_COO) {
-            if (r < S) {
-                const uint16_t* keys = reinterpret_cast<const uint16_t*>(pay);
-                const int n = k1 - k0;
-                // [lo, e): this row's elements inside the chunk (keys sorted)
-                const uint32_t kr0 = (uint32_t)r << G::LG, kr1 = (uint32_t)(r + 1) << G::LG;
-                int lo = 0, hi = n;
-                while (lo < hi) {
+            group_sync(bar_id, Gm::NTG);
+        }
+
+        // ---- phase B: products in place ----
+        if (d.scheme == ABHSF_SCHEME_BITMAP) {
+            int r_lo = 0, r_hi = S;
+            if (Gm::VC < S * S) {  // a tile may span chunks: rows overlapping [k0, k1)
+                int lo = 0, hi = S;
+                while (hi - lo > 1) {
                     const int mid = (lo + hi) >> 1;
-                    if (keys[mid] < kr0)
-                        lo = mid + 1;
+                    if (gs.rs[mid] <= k0)
+                        lo = mid;
                     else
                         hi = mid;
                 }
-                int e = lo;
-                hi = n;
-                while (e < hi) {
-                    const int mid = (e + hi) >> 1;
+                int a = lo, b = S;
+                while (a < b) {
+                    const int mid = (a + b) >> 1;
+                    if (gs.rs[mid] < k1)
+                        a = mid + 1;
+                    else
+                        b = mid;
+                }
+                r_lo = lo;
+                r_hi = a;
+            }
+            constexpr int RPW = 32 / Gm::LPR;  // rows per warp pass
+            constexpr int BATCH = 4;           // rows per batch: loads of a batch precede its stores
+            const int sub = lane / Gm::LPR, cl = lane % Gm::LPR;
+            const uint32_t lt = (1u << cl) - 1u;
+            // x for this lane's columns, once per chunk
+            double xr[Gm::CPL];
+#pragma unroll
+            for (int j = 0; j < Gm::CPL; ++j) {
+                const int c = j * 32 + cl;
+                xr[j] = (c0 + c < P.n) ? X(c) : 0.0;
+            }
+            const uint32_t* __restrict__ tbm = gs.tbm;
+            const int32_t* __restrict__ rsv = gs.rs;
+            double* __restrict__ vv = vb;
+            for (int row0 = r_lo + (warp * RPW + sub) * BATCH; row0 < r_hi; row0 += Gm::NWG * RPW * BATCH) {
+                int idx[BATCH][Gm::CPL];
+                bool on[BATCH][Gm::CPL];
+                double v[BATCH][Gm::CPL];
+#pragma unroll
+                for (int b = 0; b < BATCH; ++b) {
+                    const int row = row0 + b;
+                    const bool live = row < r_hi;
+                    int run = live ? rsv[row] : 0;
+#pragma unroll
+                    for (int j = 0; j < Gm::CPL; ++j) {
+                        uint32_t w = 0;
+                        if (live) {
+                            if (S >= 32)
+                                w = tbm[row * Gm::CPL + j];
+                            else
+                                w = (tbm[(row * S) >> 5] >> ((row * S) & 31)) & ((1u << (S & 31)) - 1);
+                        }
+                        idx[b][j] = run + __popc(w & lt);
+                        on[b][j] = ((w >> cl) & 1u) && idx[b][j] >= k0 && idx[b][j] < k1;
+                        run += __popc(w);
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < BATCH; ++b)
+#pragma unroll
+                    for (int j = 0; j < Gm::CPL; ++j)
+                        v[b][j] = on[b][j] ? vv[idx[b][j] - k0] : 0.0;
+#pragma unroll
+                for (int b = 0; b < BATCH; ++b)
+#pragma unroll
+                    for (int j = 0; j < Gm::CPL; ++j)
+                        if (on[b][j])
+                            vv[idx[b][j] - k0] = fmul(v[b][j], xr[j]);
+            }
+        } else if (d.scheme == ABHSF_SCHEME_COO) {
+            const uint16_t* keys = reinterpret_cast<const uint16_t*>(pay);
+            for (int i = r; i < n; i += Gm::NTG)
+                vb[i] = fmul(vb[i], X(keys[i] & (S - 1)));
+        } else if (d.scheme == ABHSF_SCHEME_CSR) {
+            const unsigned char* cols = (d.flags & F_FIRST_CHUNK) ? pay + 2 * S : pay;
+            for (int i = r; i < n; i += Gm::NTG)
+                vb[i] = fmul(vb[i], X(cols[i]));
+        } else {
+            for (int i = r; i < n; i += Gm::NTG) {
+                const int c = (k0 + i) & (S - 1);
+                const double v = vb[i];
+                // stored zeros (absent from the reference's CSR) become -0.0: a + -0.0 == a
+                vb[i] = (v != 0.0 && c0 + c < P.n) ? fmul(v, X(c)) : -0.0;
+            }
+        }
+        group_sync(bar_id, Gm::NTG);
+
+        // ---- phase C: this row's products, one at a time, in column order ----
+        if (r < S) {
+            int lo, hi;
+            if (d.scheme == ABHSF_SCHEME_COO) {
+                const uint16_t* keys = reinterpret_cast<const uint16_t*>(pay);
+                const uint32_t kr0 = (uint32_t)r << Gm::LG, kr1 = (uint32_t)(r + 1) << Gm::LG;
+                int a = 0, b = n;
+                while (a < b) {
+                    const int mid = (a + b) >> 1;
+                    if (keys[mid] < kr0)
+                        a = mid + 1;
+                    else
+                        b = mid;
+                }
+                int e = a;
+                b = n;
+                while (e < b) {
+                    const int mid = (e + b) >> 1;
                     if (keys[mid] < kr1)
                         e = mid + 1;
                     else
-                        hi = mid;
+                        b = mid;
                 }
-                for (int i = lo; i < e; i += 4) {
-                    double p[4];
-                    const int cnt = min(4, e - i);
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        if (u < cnt)
-                            p[u] = fmul(vb[i + u], X(keys[i + u] & (S - 1)));
-                    for (int u = 0; u < cnt; ++u)
-                        acc = fadd(acc, p[u]);
-                }
+                lo = a;
+                hi = e;
+            } else {
+                const int rs0 = d.scheme == ABHSF_SCHEME_DENSE ? r * S : gs.rs[r];
+                const int rs1 = d.scheme == ABHSF_SCHEME_DENSE ? r * S + S : gs.rs[r + 1];
+                lo = max(rs0, k0) - k0;
+                hi = min(rs1, k1) - k0;
             }
-        } else {  // dense: the stored zeros are skipped (the reference's CSR has no such elements)
-            if (r < S) {
-                const int lo = max(r * S, k0), hi = min(r * S + S, k1);
-                for (int i = lo; i < hi; i += 4) {
-                    double v[4], p[4];
-                    const int cnt = min(4, hi - i);
+            int i = lo;
+            for (; i + 8 <= hi; i += 8) {
+                double t[8];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        v[u] = 0.0;
-                        p[u] = 0.0;
-                        const int c = i + u - r * S;
-                        // columns past n (ragged right edge) hold stored zeros: never read x there
-                        if (u < cnt && c0 + c < A.n) {
-                            v[u] = vb[i + u - k0];
-                            if (v[u] != 0.0)
-                                p[u] = fmul(v[u], X(c));
-                        }
-                    }
-                    for (int u = 0; u < cnt; ++u)
-                        if (v[u] != 0.0)
-                            acc = fadd(acc, p[u]);
-                }
+                for (int v = 0; v < 8; ++v)
+                    t[v] = vb[i + v];
+#pragma unroll
+                for (int v = 0; v < 8; ++v)
+                    acc = fadd(acc, t[v]);
             }
+            for (; i < hi; ++i)
+                acc = fadd(acc, vb[i]);
         }
         if ((d.flags & F_ROW_END) && row_ok)
             P.y[grow] = acc;
-        __syncthreads();
-    }
-    if (failed && tid == 0) {
-        // drain: wait (bounded) for the copies still in flight before exiting;
-        // items step .. step + kSlots - 1 were issued
-        for (int64_t q = step; q < step + kSlots; ++q) {
-            const int s = (int)(q % kSlots);
-            if (sm.desc[s].flags & F_NONE)
-                break;
-            mbar_wait(&sm.bar[s], (uint32_t)((q / kSlots) & 1), P.status, P.spin_limit);
+        group_sync(bar_id, Gm::NTG);
+        if (r == 0) {
+            // the slot was written in place by the generic proxy; order that
+            // before the bulk copies that will refill it
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(&gs.empty[slot]);
         }
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(og<S>::NT, 1) k_spmv_f64_ordered(ord_args P)
+{
+    using Gm = og<S>;
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    ordered_smem<S>& sm = *reinterpret_cast<ordered_smem<S>*>(dyn_smem);
+    const int tid = threadIdx.x;
+    if (tid < Gm::G) {
+        group_smem<S>& gs = sm.g[tid];
+        for (int s = 0; s < Gm::R; ++s) {
+            mbar_init(&gs.full[s], 1);
+            mbar_init(&gs.empty[s], 1);
+        }
+        gs.failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid < 32) {
+        producer<S>(P, sm, tid);
+        __syncwarp();  // lanes >= G returned at once; reconverge before the CTA barrier
+    } else
+        consumer<S>(P, sm, (tid - 32) / Gm::NTG, (tid - 32) % Gm::NTG);
+    __syncthreads();
+}
+
+// ------------------------------------------------------------ schedule build
+
+template <int S>
+__device__ __forceinline__ int chunk_cap(int sch, int k0)
+{
+    using Gm = og<S>;
+    if (sch == ABHSF_SCHEME_COO)
+        return Gm::COO_MAX;
+    if (sch == ABHSF_SCHEME_CSR)
+        return k0 == 0 ? Gm::CSR0_MAX : Gm::CSR_MAX;
+    return Gm::VC;
+}
+
+template <int S>
+__device__ __forceinline__ int tile_chunks(int sch, int z)
+{
+    const int stored = sch == ABHSF_SCHEME_DENSE ? S * S : z;
+    int c = 0;
+    for (int k0 = 0; k0 < stored; k0 += chunk_cap<S>(sch, k0))
+        ++c;
+    return c;
+}
+
+template <int S>
+__global__ void k_count_chunks(int64_t T, const uint32_t* __restrict__ nnz, const uint8_t* __restrict__ sch,
+                               const int64_t* __restrict__ val_off, const int64_t* __restrict__ idx_off,
+                               const uint32_t* __restrict__ tile_row, int64_t* __restrict__ cnt,
+                               int64_t* __restrict__ w)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x) {
+        const int c = tile_chunks<S>(sch[t], (int)nnz[t]);
+        cnt[t] = c;
+        // work estimate for stream balancing: bytes moved plus a per-chunk cost
+        int64_t b = (val_off[t + 1] - val_off[t]) * 8 + (idx_off[t + 1] - idx_off[t]) + 640 * c;
+        if (t == 0 || tile_row[t - 1] != tile_row[t])
+            b += 1024;
+        w[t] = b;
+    }
+}
+
+template <int S>
+__global__ void k_fill_items(int64_t T, int64_t m, int64_t n, const uint32_t* __restrict__ nnz,
+                             const uint8_t* __restrict__ sch, const uint32_t* __restrict__ tcol,
+                             const uint32_t* __restrict__ tile_row, const int64_t* __restrict__ val_off,
+                             const int64_t* __restrict__ idx_off, const int64_t* __restrict__ item_off,
+                             item_t* __restrict__ items)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x) {
+        const int s = sch[t];
+        const int z = (int)nnz[t];
+        const int stored = s == ABHSF_SCHEME_DENSE ? S * S : z;
+        const uint32_t row = tile_row[t], col = tcol[t];
+        const bool rb = (t == 0 || tile_row[t - 1] != row);
+        const bool re = (t == T - 1 || tile_row[t + 1] != row);
+        int64_t it = item_off[t];
+        for (int k0 = 0; k0 < stored; ++it) {
+            const int k1 = min(stored, k0 + chunk_cap<S>(s, k0));
+            item_t d;
+            for (int i = 0; i < 14; ++i)
+                d.pad[i] = 0;
+            const uint64_t va = (uint64_t)(val_off[t] + k0) * 8;
+            const uint64_t va0 = va & ~uint64_t(15);
+            d.voff = va0;
+            d.vpre = (int16_t)(va - va0);
+            d.vbytes = (uint32_t)((d.vpre + (k1 - k0) * 8 + 15) & ~15);
+            const uint64_t pb = (uint64_t)idx_off[t];
+            uint64_t pa = pb, pe = pb;
+            if (s == ABHSF_SCHEME_COO) {
+                pa = pb + 2 * (uint64_t)k0;
+                pe = pb + 2 * (uint64_t)k1;
+            } else if (s == ABHSF_SCHEME_CSR) {
+                pa = k0 == 0 ? pb : pb + 2 * S + k0;
+                pe = pb + 2 * S + k1;
+            } else if (s == ABHSF_SCHEME_BITMAP && k0 == 0) {
+                pe = pb + S * S / 8;
+            }
+            const uint64_t pa0 = pa & ~uint64_t(15);
+            d.poff = pa0;
+            d.ppre = (int16_t)(pa - pa0);
+            d.pbytes = pe > pa ? (uint32_t)((pe - pa0 + 15) & ~uint64_t(15)) : 0;
+            d.row = row;
+            d.col = col;
+            d.k0 = k0;
+            d.k1 = k1;
+            d.z = z;
+            d.scheme = (uint8_t)s;
+            uint8_t f = 0;
+            if (k0 == 0)
+                f |= F_FIRST_CHUNK;
+            if (k0 == 0 && rb)
+                f |= F_ROW_BEGIN;
+            if (k1 == stored && re)
+                f |= F_ROW_END;
+            if ((int64_t)(col + 1) * S <= n)
+                f |= F_X_OK;
+            if ((int64_t)(row + 1) * S <= m)
+                f |= F_Y_OK;
+            d.flags = f;
+            items[it] = d;
+            k0 = k1;
+        }
+    }
+}
+
+// sb[q] = first chunk of stream q: chunk 0 of the first tile of the block row
+// holding the tile where the inclusive work prefix first reaches q / Q of it.
+__global__ void k_partition(int64_t T, int64_t Q, const int64_t* __restrict__ incl,
+                            const uint32_t* __restrict__ tile_row, const int64_t* __restrict__ brow_ptr,
+                            const int64_t* __restrict__ item_off, int64_t* __restrict__ sb)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q <= Q; q += (int64_t)gridDim.x * blockDim.x) {
+        int64_t t0;
+        if (q == 0) {
+            t0 = 0;
+        } else if (q == Q) {
+            t0 = T;
+        } else {
+            const int64_t total = incl[T - 1];
+            const int64_t target = (int64_t)((__int128)total * q / Q);
+            int64_t lo = 0, hi = T;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (incl[mid] < target)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            t0 = lo < T ? brow_ptr[tile_row[lo]] : T;
+        }
+        sb[q] = item_off[t0];
     }
 }
 
@@ -498,91 +676,64 @@ size_t ordered_smem_bytes()
 }
 
 template <int S>
-int ordered_ctas_per_sm()
-{
-    const size_t smem = ordered_smem_bytes<S>();
-    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ordered<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int nb = 0;
-    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ordered<S>, og<S>::NT, smem));
-    return std::max(nb, 1);
-}
-
-// Per-tile work estimate used to balance the CTAs' tile ranges.
-__global__ void k_tile_weight(int64_t T, const int64_t* __restrict__ val_off, const int64_t* __restrict__ idx_off,
-                              const uint32_t* __restrict__ tile_row, int64_t* __restrict__ w)
-{
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x) {
-        int64_t b = (val_off[t + 1] - val_off[t]) * 8 + (idx_off[t + 1] - idx_off[t]) + 512;
-        if (t == 0 || tile_row[t - 1] != tile_row[t])
-            b += 1024;
-        w[t] = b;
-    }
-}
-
-// part[p] = first tile of CTA p: the start of the block row holding the tile
-// where the inclusive weight prefix first reaches p / P of the total.
-__global__ void k_partition(int64_t T, int P, const int64_t* __restrict__ incl, const uint32_t* __restrict__ tile_row,
-                            const int64_t* __restrict__ brow_ptr, int64_t* __restrict__ part)
-{
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= P; p += gridDim.x * blockDim.x) {
-        if (p == 0) {
-            part[0] = 0;
-            continue;
-        }
-        if (p == P) {
-            part[P] = T;
-            continue;
-        }
-        const int64_t total = incl[T - 1];
-        const int64_t target = (int64_t)((__int128)total * p / P);
-        int64_t lo = 0, hi = T;
-        while (lo < hi) {
-            const int64_t mid = (lo + hi) >> 1;
-            if (incl[mid] < target)
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
-        part[p] = lo < T ? brow_ptr[tile_row[lo]] : T;
-    }
-}
-
-template <int S>
 void prepare_ordered_s(abhsf_matrix& a, cudaStream_t st)
 {
+    using Gm = og<S>;
     int dev = 0, nsm = 0;
     ABHSF_CUDA(cudaGetDevice(&dev));
     ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const int P = nsm * ordered_ctas_per_sm<S>();
-    a.ord_ctas = P;
-    a.ord_part.alloc(P + 1);
+    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ordered<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)ordered_smem_bytes<S>()));
+    const int64_t P = nsm;
+    const int64_t Q = P * Gm::G;
+    a.ord_ctas = (int)P;
+    a.ord_streams.alloc(Q + 1);
     if (a.T == 0) {
-        ABHSF_CUDA(cudaMemsetAsync(a.ord_part.get(), 0, (P + 1) * sizeof(int64_t), st));
+        ABHSF_CUDA(cudaMemsetAsync(a.ord_streams.get(), 0, (Q + 1) * sizeof(int64_t), st));
+        a.ord_items.alloc(1);
+        ABHSF_CUDA(cudaStreamSynchronize(st));
         return;
     }
-    dbuf<int64_t> w(a.T), incl(a.T);
-    k_tile_weight<<<(unsigned)std::min<int64_t>((a.T + 255) / 256, 4096), 256, 0, st>>>(
-        a.T, a.tile_val_off.get(), a.tile_idx_off.get(), a.tile_row.get(), w.get());
+    const int64_t T = a.T;
+    const unsigned g = (unsigned)std::min<int64_t>((T + 255) / 256, 4096);
+    dbuf<int64_t> cnt(T + 1), item_off(T + 1), w(T), incl(T);
+    ABHSF_CUDA(cudaMemsetAsync(cnt.get() + T, 0, sizeof(int64_t), st));
+    k_count_chunks<S><<<g, 256, 0, st>>>(T, a.tile_nnz.get(), a.tile_scheme.get(), a.tile_val_off.get(),
+                                         a.tile_idx_off.get(), a.tile_row.get(), cnt.get(), w.get());
     ABHSF_CUDA(cudaGetLastError());
-    inclusive_scan_i64(w.get(), incl.get(), a.T, st);
-    k_partition<<<(P + 1 + 255) / 256, 256, 0, st>>>(a.T, P, incl.get(), a.tile_row.get(), a.brow_ptr.get(),
-                                                     a.ord_part.get());
+    exclusive_scan_i64(cnt.get(), item_off.get(), T + 1, st);
+    int64_t nitems = 0;
+    ABHSF_CUDA(cudaMemcpyAsync(&nitems, item_off.get() + T, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    ABHSF_CUDA(cudaStreamSynchronize(st));
+    a.ord_items.alloc((size_t)nitems * sizeof(item_t));
+    k_fill_items<S><<<g, 256, 0, st>>>(T, a.m, a.n, a.tile_nnz.get(), a.tile_scheme.get(), a.tile_col.get(),
+                                       a.tile_row.get(), a.tile_val_off.get(), a.tile_idx_off.get(), item_off.get(),
+                                       reinterpret_cast<item_t*>(a.ord_items.get()));
+    ABHSF_CUDA(cudaGetLastError());
+    inclusive_scan_i64(w.get(), incl.get(), T, st);
+    k_partition<<<(unsigned)((Q + 1 + 255) / 256), 256, 0, st>>>(T, Q, incl.get(), a.tile_row.get(),
+                                                                  a.brow_ptr.get(), item_off.get(),
+                                                                  a.ord_streams.get());
     ABHSF_CUDA(cudaGetLastError());
     ABHSF_CUDA(cudaStreamSynchronize(st));
+    a.ord_nitems = nitems;
 }
 
 template <int S>
 void launch_ordered(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
     ord_args P;
-    P.A = a.view();
-    P.tile_row = a.tile_row.get();
-    P.part = a.ord_part.get();
+    P.items = reinterpret_cast<const item_t*>(a.ord_items.get());
+    P.sb = a.ord_streams.get();
+    P.values = a.values.get();
+    P.payload = a.payload.get();
     P.x = x;
     P.y = y;
+    P.m = a.m;
+    P.n = a.n;
     P.status = a.dev_status.get();
     P.aligned_xy = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
-    P.spin_limit = g_spin_limit ? g_spin_limit : kSpinLimit;
+    P.spin_limit = g_spin_limit;
     P.drop_item = g_drop_item;
     k_spmv_f64_ordered<S><<<a.ord_ctas, og<S>::NT, ordered_smem_bytes<S>(), st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
