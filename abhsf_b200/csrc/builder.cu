@@ -535,6 +535,7 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
     ABHSF_CUDA(cudaMemsetAsync(a.dev_status.get(), 0, sizeof(int), st));
     finish_stats(a, dense_bits, st);
     prepare_ordered(a, st);
+    prepare_tree(a, st);
 }
 
 void block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r, int s,

@@ -168,6 +168,11 @@ struct abhsf_matrix {
     int64_t ord_nitems = 0;
     int ord_ctas = 0;
     abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
+    // tree-order SpMV: non-empty block rows and the work counter of its persistent warps
+    abhsf::dbuf<uint32_t> tree_rows;
+    int64_t tree_nrows = 0;
+    abhsf::dbuf<unsigned int> tree_counter;
+    int tree_ctas = 0;
     // staging for abhsf_spmv_host
     abhsf::dbuf<double> x_stage, y_stage;
 

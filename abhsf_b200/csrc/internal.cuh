@@ -22,6 +22,9 @@ void spmv_f64(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st
 // y += A x with the reference CSR's per-row summation order (bitwise equal).
 void spmv_f64_ordered(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
 
+// Per-matrix set-up of the tree-order kernel (non-empty block rows, counter).
+void prepare_tree(abhsf_matrix& a, cudaStream_t st);
+
 // Per-matrix set-up of the reference-order kernel (CTA tile ranges).
 void prepare_ordered(abhsf_matrix& a, cudaStream_t st);
 

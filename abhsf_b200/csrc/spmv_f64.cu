@@ -1,7 +1,8 @@
 // spmv_f64.cu -- y += A x over the ABHSF format, FP64 values, sm_100a.
 //
-// One warp (a CTA of its own) owns one block row (s rows of y) and walks its
-// tiles in column order.  Per tile it dispatches on the scheme:
+// Persistent warps take non-empty block rows from a work counter, a few at a
+// time; one warp owns a block row (s rows of y) and walks its tiles in column
+// order.  Per tile it dispatches on the scheme:
 //
 //  * bitmap / dense, s >= 32: lane l owns columns l, l+32, ... of the tile and
 //    keeps those x values in registers.  Rows are taken 16 at a time; for each
@@ -21,30 +22,36 @@
 // Row sums collect in a per-warp shared-memory copy of the block row's y
 // segment and are added to y once per block row: no atomics, so the result is
 // bitwise reproducible run to run.
+#include <algorithm>
+
 #include "common.cuh"
 #include "internal.cuh"
 
 namespace abhsf {
 namespace {
 
-// One warp (one block row) per CTA: block rows differ widely in work, and a
-// CTA of several warps holds its SM slot until its slowest warp is done.
-constexpr int kWarps = 1;
-constexpr int kMinCtasPerSm = 24;  // caps registers so ~24-32 warps stay resident per SM
+// Persistent warps: each warp repeatedly takes kGrain consecutive non-empty
+// block rows from a work counter, so empty rows cost nothing and a long row
+// delays only its own warp.
+constexpr int kWarps = 4;
+constexpr int kMinCtasPerSm = 6;  // 24 resident warps per SM; caps registers at 80
+constexpr int kGrain = 4;
 constexpr unsigned kFull = 0xffffffffu;
 
 template <int S>
 struct geom {
     static constexpr int CPL = S >= 32 ? S / 32 : 1;  // x values per lane
-    static constexpr int AUX = S / 2 > 8 ? S / 2 : 8;  // u32 words of scratch per warp
+    static constexpr int RB = S >= 64 ? 64 : S;       // bitmap rows staged at once
+    static constexpr int WPB = RB * CPL;              // u32 words of a staged bitmap block
+    static constexpr int AUX = WPB > S / 2 ? (WPB > 8 ? WPB : 8) : (S / 2 > 8 ? S / 2 : 8);
 };
 
 template <int S>
 struct warp_smem {
-    double ys[S];                  // y segment of the block row
-    double xs[S];                  // x segment of the current tile (element streams)
-    uint32_t aux[geom<S>::AUX];    // bitmap chunks of a 16-row group, or CSR row_end
-    int32_t rowstart[16];
+    alignas(16) uint32_t aux[geom<S>::AUX];  // a staged bitmap block, or CSR row_end
+    double ys[S];                            // y segment of the block row
+    double xs[S];                            // x segment of the current tile (element streams)
+    int32_t rowstart[64];
 };
 
 __device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
@@ -67,56 +74,76 @@ __device__ __forceinline__ double butterfly16(double (&acc)[16], int lane)
 }
 
 // Bitmap tile, s >= 32.  bm32 = tile bitmap as little-endian u32 words: row
-// r's columns 32j..32j+31 are word r * CPL + j.
+// r's columns 32j..32j+31 are word r * CPL + j.  Up to 64 rows of bitmap are
+// staged in shared memory with one vector load per lane, their row starts
+// found by one popcount scan; rows are then summed 16 at a time.
 template <int S>
 __device__ __forceinline__ void tile_bitmap(const uint32_t* __restrict__ bm32, const double* __restrict__ vals,
                                             const double (&xr)[geom<S>::CPL], warp_smem<S>& sm, int lane)
 {
     constexpr int CPL = geom<S>::CPL;
+    constexpr int RB = geom<S>::RB;
+    constexpr int WPB = geom<S>::WPB;
     const uint32_t lt = (1u << lane) - 1u;
     int running = 0;
 #pragma unroll 1
-    for (int g = 0; g < S / 16; ++g) {
-        for (int c = lane; c < 16 * CPL; c += 32)
-            sm.aux[c] = ld_stream_u32(bm32 + g * 16 * CPL + c);
+    for (int blk = 0; blk < S / RB; ++blk) {
+        const uint4* src = reinterpret_cast<const uint4*>(bm32 + blk * WPB);
+        uint4* dst = reinterpret_cast<uint4*>(sm.aux);
+        for (int i = lane; i < WPB / 4; i += 32)
+            dst[i] = __ldcs(src + i);
         __syncwarp();
-        int pc = 0;
-        if (lane < 16) {
+        // rows lane and lane + 32 of the block
+        int pc0 = 0, pc1 = 0;
 #pragma unroll
-            for (int j = 0; j < CPL; ++j)
-                pc += __popc(sm.aux[lane * CPL + j]);
+        for (int j = 0; j < CPL; ++j) {
+            if (lane < RB)
+                pc0 += __popc(sm.aux[lane * CPL + j]);
+            if (RB == 64)
+                pc1 += __popc(sm.aux[(lane + 32) * CPL + j]);
         }
-        int inc = pc;
+        int inc0 = pc0, inc1 = pc1;
 #pragma unroll
-        for (int d = 1; d < 16; d <<= 1) {
-            const int t = __shfl_up_sync(kFull, inc, d);
-            if (lane >= d)
-                inc += t;
-        }
-        if (lane < 16)
-            sm.rowstart[lane] = running + inc - pc;
-        running += __shfl_sync(kFull, inc, 15);
-        __syncwarp();
-        double acc[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const double* rv = vals + sm.rowstart[i];
-            int run = 0;
-            double a = 0.0;
-#pragma unroll
-            for (int j = 0; j < CPL; ++j) {
-                const uint32_t w = sm.aux[i * CPL + j];
-                double v = 0.0;
-                if ((w >> lane) & 1u)
-                    v = ld_stream(rv + run + __popc(w & lt));
-                a = fma(v, xr[j], a);
-                run += __popc(w);
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t0 = __shfl_up_sync(kFull, inc0, d);
+            const int t1 = __shfl_up_sync(kFull, inc1, d);
+            if (lane >= d) {
+                inc0 += t0;
+                inc1 += t1;
             }
-            acc[i] = a;
         }
-        const double r = butterfly16(acc, lane);
-        if (lane < 16)
-            sm.ys[g * 16 + lane] += r;
+        const int tot0 = __shfl_sync(kFull, inc0, 31);
+        const int tot1 = __shfl_sync(kFull, inc1, 31);
+        if (lane < RB)
+            sm.rowstart[lane] = running + inc0 - pc0;
+        if (RB == 64)
+            sm.rowstart[lane + 32] = running + tot0 + inc1 - pc1;
+        running += tot0 + tot1;
+        __syncwarp();
+#pragma unroll 1
+        for (int g = 0; g < RB / 16; ++g) {
+            double acc[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int row = g * 16 + i;
+                const double* rv = vals + sm.rowstart[row];
+                int run = 0;
+                double a = 0.0;
+#pragma unroll
+                for (int j = 0; j < CPL; ++j) {
+                    const uint32_t w = sm.aux[row * CPL + j];
+                    double v = 0.0;
+                    if ((w >> lane) & 1u)
+                        v = ld_stream(rv + run + __popc(w & lt));
+                    a = fma(v, xr[j], a);
+                    run += __popc(w);
+                }
+                acc[i] = a;
+            }
+            const double r = butterfly16(acc, lane);
+            if (lane < 16)
+                sm.ys[blk * RB + g * 16 + lane] += r;
+        }
         __syncwarp();
     }
 }
@@ -232,78 +259,171 @@ __device__ __forceinline__ void tile_stream(const uint8_t* __restrict__ pay, con
     }
 }
 
+struct tree_args {
+    tiles_view A;
+    const uint32_t* rows;  // non-empty block rows, ascending
+    int64_t nrows;
+    unsigned int* counter;  // next entry of rows to hand out (zeroed before each launch)
+    const double* x;
+    double* y;
+};
+
 template <int S>
-__global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_f64(tiles_view A, const double* __restrict__ x,
-                                                          double* __restrict__ y)
+__device__ __forceinline__ void block_row(const tree_args& P, int64_t I, warp_smem<S>& sm, int lane)
 {
     constexpr int CPL = geom<S>::CPL;
+    const tiles_view& A = P.A;
+    const double* __restrict__ values = static_cast<const double*>(A.values);
+    const double* __restrict__ x = P.x;
+    const int64_t t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
+    for (int r = lane; r < S; r += 32)
+        sm.ys[r] = 0.0;
+    __syncwarp();
+    // the next tile's header is loaded while the current tile is summed
+    uint32_t n_col = A.tile_col[t0], n_z = A.tile_nnz[t0];
+    uint8_t n_sch = A.tile_scheme[t0];
+    int64_t n_vo = A.tile_val_off[t0], n_io = A.tile_idx_off[t0];
+#pragma unroll 1
+    for (int64_t t = t0; t < t1; ++t) {
+        const int64_t c0 = (int64_t)n_col * S;
+        const int z = (int)n_z;
+        const int sch = n_sch;
+        const double* vals = values + n_vo;
+        const uint8_t* pay = A.payload + n_io;
+        if (t + 1 < t1) {
+            n_col = A.tile_col[t + 1];
+            n_z = A.tile_nnz[t + 1];
+            n_sch = A.tile_scheme[t + 1];
+            n_vo = A.tile_val_off[t + 1];
+            n_io = A.tile_idx_off[t + 1];
+        }
+        double xr[CPL];
+#pragma unroll
+        for (int j = 0; j < CPL; ++j) {
+            const int64_t c = c0 + (S >= 32 ? 32 * j + lane : (lane & (S - 1)));
+            xr[j] = c < A.n ? __ldg(x + c) : 0.0;
+        }
+        if (S >= 32 && sch == ABHSF_SCHEME_BITMAP) {
+            if constexpr (S >= 32)
+                tile_bitmap<S>(reinterpret_cast<const uint32_t*>(pay), vals, xr, sm, lane);
+        } else if (S >= 32 && sch == ABHSF_SCHEME_DENSE) {
+            if constexpr (S >= 32)
+                tile_dense<S>(vals, xr, sm, lane);
+        } else if (S == 16 && sch == ABHSF_SCHEME_BITMAP) {
+            if constexpr (S == 16)
+                tile_16<false>(reinterpret_cast<const uint32_t*>(pay), vals, xr[0], sm, lane);
+        } else if (S == 16 && sch == ABHSF_SCHEME_DENSE) {
+            if constexpr (S == 16)
+                tile_16<true>(nullptr, vals, xr[0], sm, lane);
+        } else {
+#pragma unroll
+            for (int j = 0; j < CPL; ++j)
+                if (S >= 32 || lane < S)
+                    sm.xs[S >= 32 ? 32 * j + lane : lane] = xr[j];
+            __syncwarp();
+            if (sch == ABHSF_SCHEME_CSR)
+                tile_stream<S, true>(pay, vals, z, sm, lane);
+            else
+                tile_stream<S, false>(pay, vals, z, sm, lane);
+        }
+    }
+    const int64_t r0 = I * S;
+    for (int r = lane; r < S; r += 32)
+        if (r0 + r < A.m)
+            P.y[r0 + r] += sm.ys[r];
+    __syncwarp();
+}
+
+template <int S>
+__global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_f64(tree_args P)
+{
     __shared__ warp_smem<S> smem[kWarps];
     const int lane = threadIdx.x & 31;
     warp_smem<S>& sm = smem[threadIdx.x >> 5];
-    const double* __restrict__ values = static_cast<const double*>(A.values);
-    const int64_t nw = (int64_t)gridDim.x * kWarps;
-    for (int64_t I = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); I < A.M; I += nw) {
-        const int64_t t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
-        if (t0 == t1)
-            continue;
-        for (int r = lane; r < S; r += 32)
-            sm.ys[r] = 0.0;
-        __syncwarp();
-#pragma unroll 1
-        for (int64_t t = t0; t < t1; ++t) {
-            const int64_t c0 = (int64_t)A.tile_col[t] * S;
-            const int z = (int)A.tile_nnz[t];
-            const int sch = A.tile_scheme[t];
-            const double* vals = values + A.tile_val_off[t];
-            const uint8_t* pay = A.payload + A.tile_idx_off[t];
-            double xr[CPL];
-#pragma unroll
-            for (int j = 0; j < CPL; ++j) {
-                const int64_t c = c0 + (S >= 32 ? 32 * j + lane : (lane & (S - 1)));
-                xr[j] = c < A.n ? __ldg(x + c) : 0.0;
-            }
-            if (S >= 32 && sch == ABHSF_SCHEME_BITMAP) {
-                if constexpr (S >= 32)
-                    tile_bitmap<S>(reinterpret_cast<const uint32_t*>(pay), vals, xr, sm, lane);
-            } else if (S >= 32 && sch == ABHSF_SCHEME_DENSE) {
-                if constexpr (S >= 32)
-                    tile_dense<S>(vals, xr, sm, lane);
-            } else if (S == 16 && sch == ABHSF_SCHEME_BITMAP) {
-                if constexpr (S == 16)
-                    tile_16<false>(reinterpret_cast<const uint32_t*>(pay), vals, xr[0], sm, lane);
-            } else if (S == 16 && sch == ABHSF_SCHEME_DENSE) {
-                if constexpr (S == 16)
-                    tile_16<true>(nullptr, vals, xr[0], sm, lane);
-            } else {
-#pragma unroll
-                for (int j = 0; j < CPL; ++j)
-                    if (S >= 32 || lane < S)
-                        sm.xs[S >= 32 ? 32 * j + lane : lane] = xr[j];
-                __syncwarp();
-                if (sch == ABHSF_SCHEME_CSR)
-                    tile_stream<S, true>(pay, vals, z, sm, lane);
-                else
-                    tile_stream<S, false>(pay, vals, z, sm, lane);
-            }
-        }
-        const int64_t r0 = I * S;
-        for (int r = lane; r < S; r += 32)
-            if (r0 + r < A.m)
-                y[r0 + r] += sm.ys[r];
-        __syncwarp();
+    for (;;) {
+        unsigned int base = 0;
+        if (lane == 0)
+            base = atomicAdd(P.counter, (unsigned int)kGrain);
+        base = __shfl_sync(kFull, base, 0);
+        if ((int64_t)base >= P.nrows)
+            break;
+        const int64_t end = min((int64_t)base + kGrain, P.nrows);
+        for (int64_t k = base; k < end; ++k)
+            block_row<S>(P, (int64_t)P.rows[k], sm, lane);
     }
+}
+
+// Lists the non-empty block rows (the work items of k_spmv_f64).
+__global__ void k_nonempty_flags(int64_t M, const int64_t* __restrict__ brow_ptr, int64_t* __restrict__ flag)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x)
+        flag[i] = brow_ptr[i + 1] > brow_ptr[i] ? 1 : 0;
+}
+
+__global__ void k_nonempty_scatter(int64_t M, const int64_t* __restrict__ brow_ptr, const int64_t* __restrict__ pos,
+                                   uint32_t* __restrict__ rows)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x)
+        if (brow_ptr[i + 1] > brow_ptr[i])
+            rows[pos[i]] = (uint32_t)i;
+}
+
+template <int S>
+int tree_ctas_per_sm()
+{
+    int nb = 0;
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64<S>, kWarps * 32, 0));
+    return std::max(nb, 1);
 }
 
 template <int S>
 void launch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
-    const int64_t blocks = (a.M + kWarps - 1) / kWarps;
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(blocks, int64_t(1) << 30));
-    k_spmv_f64<S><<<grid, kWarps * 32, 0, st>>>(a.view(), x, y);
+    if (a.tree_nrows == 0)
+        return;
+    tree_args P{a.view(), a.tree_rows.get(), a.tree_nrows, a.tree_counter.get(), x, y};
+    ABHSF_CUDA(cudaMemsetAsync(a.tree_counter.get(), 0, sizeof(unsigned int), st));
+    const int64_t want = (a.tree_nrows + (int64_t)kGrain * kWarps - 1) / ((int64_t)kGrain * kWarps);
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)a.tree_ctas));
+    k_spmv_f64<S><<<grid, kWarps * 32, 0, st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }
 
 }  // namespace
+
+void prepare_tree(abhsf_matrix& a, cudaStream_t st)
+{
+    int dev = 0, nsm = 0;
+    ABHSF_CUDA(cudaGetDevice(&dev));
+    ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    int per_sm = 1;
+    switch (a.s) {
+    case 16: per_sm = tree_ctas_per_sm<16>(); break;
+    case 32: per_sm = tree_ctas_per_sm<32>(); break;
+    case 64: per_sm = tree_ctas_per_sm<64>(); break;
+    case 128: per_sm = tree_ctas_per_sm<128>(); break;
+    case 256: per_sm = tree_ctas_per_sm<256>(); break;
+    default: fail(ABHSF_ERROR_UNSUPPORTED, "block size without an SpMV kernel");
+    }
+    a.tree_ctas = nsm * per_sm;
+    a.tree_counter.alloc(1);
+    dbuf<int64_t> flag(a.M + 1), pos(a.M + 1);
+    ABHSF_CUDA(cudaMemsetAsync(flag.get() + a.M, 0, sizeof(int64_t), st));
+    const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((a.M + 255) / 256, 4096));
+    k_nonempty_flags<<<g, 256, 0, st>>>(a.M, a.brow_ptr.get(), flag.get());
+    ABHSF_CUDA(cudaGetLastError());
+    exclusive_scan_i64(flag.get(), pos.get(), a.M + 1, st);
+    int64_t nr = 0;
+    ABHSF_CUDA(cudaMemcpyAsync(&nr, pos.get() + a.M, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    ABHSF_CUDA(cudaStreamSynchronize(st));
+    if (nr > int64_t(UINT32_MAX))
+        fail(ABHSF_ERROR_UNSUPPORTED, "more than 2^32 non-empty block rows");
+    a.tree_rows.alloc(nr);
+    k_nonempty_scatter<<<g, 256, 0, st>>>(a.M, a.brow_ptr.get(), pos.get(), a.tree_rows.get());
+    ABHSF_CUDA(cudaGetLastError());
+    ABHSF_CUDA(cudaStreamSynchronize(st));
+    a.tree_nrows = nr;
+}
 
 void spmv_f64(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {

@@ -123,7 +123,8 @@ struct group_smem {
     int32_t scan[og<S>::NWG + 1];
     int32_t failed;
     int32_t rs[S + 1];                         // current tile: first stored value of each row
-    alignas(16) uint32_t tbm[og<S>::BMW];      // current tile's bitmap (bitmap tiles)
+    int32_t clo[S], chi[S], ctag[S];           // COO chunk: row r's elements [clo, chi) if ctag == item
+    alignas(16) uint32_t tbm[og<S>::BMW];      // current tile's bitmap (tiles spanning chunks)
     alignas(16) unsigned char slot[og<S>::R][og<S>::SLOT];
 };
 
@@ -290,9 +291,11 @@ __device__ void consumer(const ord_args& P, ordered_smem<S>& sm, int gidx, int r
     const int64_t nitems = P.sb[q + 1] - P.sb[q];
     const uint32_t limit = P.spin_limit ? P.spin_limit : kConsumerPolls;
     double acc = 0.0;
+    int prev_slot = -1;
     for (int64_t u = 0; u < nitems; ++u) {
         const int slot = (int)(u % Gm::R);
         const bool ok = mbar_wait(&gs.full[slot], (uint32_t)((u / Gm::R) & 1), limit);
+        // this barrier also ends the previous chunk: its slot can be refilled
         if (group_any(bar_id, Gm::NTG, !ok)) {
             if (r == 0) {
                 *(volatile int32_t*)&gs.failed = 1;
@@ -300,6 +303,13 @@ __device__ void consumer(const ord_args& P, ordered_smem<S>& sm, int gidx, int r
             }
             return;
         }
+        if (r == 0 && prev_slot >= 0) {
+            // the slot was written in place by the generic proxy; order that
+            // before the bulk copies that will refill it
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(&gs.empty[prev_slot]);
+        }
+        prev_slot = slot;
         unsigned char* base = gs.slot[slot];
         const item_t d = *reinterpret_cast<const item_t*>(base);
         const double* ys = reinterpret_cast<const double*>(base + Gm::DESC);
@@ -319,10 +329,12 @@ __device__ void consumer(const ord_args& P, ordered_smem<S>& sm, int gidx, int r
         // ---- phase A: tile metadata (first chunk of a tile) ----
         if (d.flags & F_FIRST_CHUNK) {
             if (d.scheme == ABHSF_SCHEME_BITMAP) {
-                const uint4* src = reinterpret_cast<const uint4*>(pay);
-                uint4* dst = reinterpret_cast<uint4*>(gs.tbm);
-                for (int i = r; i < Gm::BM_BYTES / 16; i += Gm::NTG)
-                    dst[i] = src[i];
+                if (Gm::VC < S * S) {  // later chunks of the tile need the bitmap
+                    const uint4* src = reinterpret_cast<const uint4*>(pay);
+                    uint4* dst = reinterpret_cast<uint4*>(gs.tbm);
+                    for (int i = r; i < Gm::BM_BYTES / 16; i += Gm::NTG)
+                        dst[i] = src[i];
+                }
                 int pc = 0;
                 if (r < S) {
                     if (S >= 32) {
@@ -399,7 +411,9 @@ __device__ void consumer(const ord_args& P, ordered_smem<S>& sm, int gidx, int r
                 const int c = j * 32 + cl;
                 xr[j] = (c0 + c < P.n) ? X(c) : 0.0;
             }
-            const uint32_t* __restrict__ tbm = gs.tbm;
+            // a whole tile's bitmap is read where it landed; a spanning tile's from its copy
+            const uint32_t* __restrict__ tbm =
+                Gm::VC < S * S ? gs.tbm : reinterpret_cast<const uint32_t*>(pay);
             const int32_t* __restrict__ rsv = gs.rs;
             double* __restrict__ vv = vb;
             for (int row0 = r_lo + (warp * RPW + sub) * BATCH; row0 < r_hi; row0 += Gm::NWG * RPW * BATCH) {
@@ -439,8 +453,19 @@ __device__ void consumer(const ord_args& P, ordered_smem<S>& sm, int gidx, int r
             }
         } else if (d.scheme == ABHSF_SCHEME_COO) {
             const uint16_t* keys = reinterpret_cast<const uint16_t*>(pay);
-            for (int i = r; i < n; i += Gm::NTG)
-                vb[i] = fmul(vb[i], X(keys[i] & (S - 1)));
+            const int tag = (int)(u & 0x7fffffff);
+            for (int i = r; i < n; i += Gm::NTG) {
+                const uint32_t key = keys[i];
+                const int row = (int)(key >> Gm::LG);
+                vb[i] = fmul(vb[i], X(key & (S - 1)));
+                // keys are sorted: the first and last element of each row mark its range
+                if (i == 0 || (keys[i - 1] >> Gm::LG) != (uint32_t)row) {
+                    gs.clo[row] = i;
+                    gs.ctag[row] = tag;
+                }
+                if (i == n - 1 || (keys[i + 1] >> Gm::LG) != (uint32_t)row)
+                    gs.chi[row] = i + 1;
+            }
         } else if (d.scheme == ABHSF_SCHEME_CSR) {
             const unsigned char* cols = (d.flags & F_FIRST_CHUNK) ? pay + 2 * S : pay;
             for (int i = r; i < n; i += Gm::NTG)
@@ -459,27 +484,9 @@ __device__ void consumer(const ord_args& P, ordered_smem<S>& sm, int gidx, int r
         if (r < S) {
             int lo, hi;
             if (d.scheme == ABHSF_SCHEME_COO) {
-                const uint16_t* keys = reinterpret_cast<const uint16_t*>(pay);
-                const uint32_t kr0 = (uint32_t)r << Gm::LG, kr1 = (uint32_t)(r + 1) << Gm::LG;
-                int a = 0, b = n;
-                while (a < b) {
-                    const int mid = (a + b) >> 1;
-                    if (keys[mid] < kr0)
-                        a = mid + 1;
-                    else
-                        b = mid;
-                }
-                int e = a;
-                b = n;
-                while (e < b) {
-                    const int mid = (e + b) >> 1;
-                    if (keys[mid] < kr1)
-                        e = mid + 1;
-                    else
-                        b = mid;
-                }
-                lo = a;
-                hi = e;
+                const bool has = gs.ctag[r] == (int)(u & 0x7fffffff);
+                lo = has ? gs.clo[r] : 0;
+                hi = has ? gs.chi[r] : 0;
             } else {
                 const int rs0 = d.scheme == ABHSF_SCHEME_DENSE ? r * S : gs.rs[r];
                 const int rs1 = d.scheme == ABHSF_SCHEME_DENSE ? r * S + S : gs.rs[r + 1];
@@ -501,13 +508,6 @@ __device__ void consumer(const ord_args& P, ordered_smem<S>& sm, int gidx, int r
         }
         if ((d.flags & F_ROW_END) && row_ok)
             P.y[grow] = acc;
-        group_sync(bar_id, Gm::NTG);
-        if (r == 0) {
-            // the slot was written in place by the generic proxy; order that
-            // before the bulk copies that will refill it
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_arrive(&gs.empty[slot]);
-        }
     }
 }
 
@@ -525,6 +525,8 @@ __global__ void __launch_bounds__(og<S>::NT, 1) k_spmv_f64_ordered(ord_args P)
             mbar_init(&gs.empty[s], 1);
         }
         gs.failed = 0;
+        for (int i = 0; i < S; ++i)
+            gs.ctag[i] = -1;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
