@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -581,6 +582,120 @@ void block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int6
     ABHSF_CUDA(cudaMemcpyAsync(hist, dh.get(), hist_len * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
     ABHSF_CUDA(cudaStreamSynchronize(st));
     raise_err(read_scalar(err.get(), st));
+    if (blocks)
+        *blocks = B;
+}
+
+// ---------------------------------------------------------------------------
+// Block histogram that allocates nothing (abhsf_block_histogram_noalloc).
+//
+// For callers that may not call cudaMalloc: processes whose device memory is
+// handed out by their own allocator or pool, paths where a cudaMalloc (which
+// can synchronise the device) is not acceptable, and processes already at
+// their device-memory limit.  All scratch lives in the array below, which is
+// part of the library's device image: every GPU that loads the library holds
+// it until the process exits.  Every call reuses it; a call clears what must
+// start at zero, and calls that overlap on the GPU race on it.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  Looked up once
+// per device with that device current; host code may not use the symbol
+// itself as an address.
+unsigned char* noalloc_scratch()
+{
+    int dev = 0;
+    ABHSF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        fail(ABHSF_ERROR_UNSUPPORTED, "device index beyond the no-allocation table");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        ABHSF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
+// Hands out 256-byte-aligned pieces of the scratch array.
+struct scratch_arena {
+    unsigned char* base;
+    size_t cap, used = 0;
+    template <typename T>
+    T* take(size_t count)
+    {
+        const size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+        if (used + bytes > cap)
+            fail(ABHSF_ERROR_INVALID_VALUE, "input too large for the no-allocation scratch");
+        T* p = reinterpret_cast<T*>(base + used);
+        used += bytes;
+        return p;
+    }
+};
+
+}  // namespace
+
+void block_histogram_noalloc(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r,
+                             int s, cudaStream_t st, uint64_t* hist, int64_t hist_len, int64_t* blocks)
+{
+    const int k = log2_exact(r), l = log2_exact(s);
+    if (k < 1 || k > 8 || l < 1 || l > 8)
+        fail(ABHSF_ERROR_INVALID_VALUE, "r and s must be powers of two in 2..256");
+    if (m <= 0 || n <= 0 || nnz < 0)
+        fail(ABHSF_ERROR_INVALID_VALUE, "m and n must be positive and nnz non-negative");
+    if (nnz > ABHSF_NOALLOC_MAX_NNZ)
+        fail(ABHSF_ERROR_INVALID_VALUE, "nnz exceeds ABHSF_NOALLOC_MAX_NNZ, the no-allocation limit");
+    if (!hist || hist_len < (int64_t)r * s + 1)
+        fail(ABHSF_ERROR_INVALID_VALUE, "hist must hold r*s + 1 counters");
+    if (((uint64_t)(m - 1) >> k) >= (uint64_t(1) << 32) || ((uint64_t)(n - 1) >> l) >= (uint64_t(1) << 32))
+        fail(ABHSF_ERROR_UNSUPPORTED, "block row or column index beyond 32 bits");
+    if (nnz > 0 && (!rows || !cols))
+        fail(ABHSF_ERROR_INVALID_VALUE, "rows and cols must be non-NULL device pointers");
+    unsigned char* base = noalloc_scratch();  // before any early return: the set-up is per device
+    std::fill(hist, hist + hist_len, 0);
+    if (blocks)
+        *blocks = 0;
+    if (nnz == 0)
+        return;
+    const int64_t hl = (int64_t)r * s + 1;  // counters the device fills
+    scratch_arena ar{base, kNoAllocScratchBytes};
+    int* err = ar.take<int>(1);
+    uint64_t* keys = ar.take<uint64_t>(nnz);
+    uint64_t* keys_out = ar.take<uint64_t>(nnz);
+    int64_t* head = ar.take<int64_t>(nnz);
+    int64_t* run_of = ar.take<int64_t>(nnz);
+    int64_t* start = ar.take<int64_t>(nnz + 1);
+    unsigned long long* dh = ar.take<unsigned long long>(hl);
+    const int end_bit = 32 + bit_length((uint64_t)(m - 1) >> k);
+    size_t sort_bytes = 0, scan_bytes = 0;
+    ABHSF_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, keys, keys_out, nnz, 0, end_bit, st));
+    ABHSF_CUDA(cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, head, run_of, nnz, st));
+    unsigned char* sort_tmp = ar.take<unsigned char>(sort_bytes);
+    unsigned char* scan_tmp = ar.take<unsigned char>(scan_bytes);
+    // the scratch keeps the previous call's contents: clear what must start at zero
+    ABHSF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    ABHSF_CUDA(cudaMemsetAsync(dh, 0, hl * sizeof(unsigned long long), st));
+    k_block_keys<<<grid_for(nnz), kThreads, 0, st>>>(rows, cols, nnz, m, n, k, l, keys, err);
+    check_launch("k_block_keys");
+    raise_err(read_scalar(err, st));
+    ABHSF_CUDA(cub::DeviceRadixSort::SortKeys(sort_tmp, sort_bytes, keys, keys_out, nnz, 0, end_bit, st));
+    k_heads<<<grid_for(nnz), kThreads, 0, st>>>(keys_out, nnz, 0, 0, head, err);
+    check_launch("k_heads");
+    ABHSF_CUDA(cub::DeviceScan::InclusiveSum(scan_tmp, scan_bytes, head, run_of, nnz, st));
+    const int64_t B = read_scalar(run_of + nnz - 1, st);
+    k_tile_starts<<<grid_for(nnz), kThreads, 0, st>>>(keys_out, run_of, nnz, 0, start, nullptr);
+    check_launch("k_tile_starts");
+    k_len_hist<<<grid_for(B), kThreads, 0, st>>>(B, start, dh, hl, err);
+    check_launch("k_len_hist");
+    ABHSF_CUDA(cudaMemcpyAsync(hist, dh, hl * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    ABHSF_CUDA(cudaStreamSynchronize(st));
+    raise_err(read_scalar(err, st));
     if (blocks)
         *blocks = B;
 }

@@ -164,6 +164,16 @@ abhsf_status abhsf_block_histogram(const int64_t* rows, const int64_t* cols, int
     });
 }
 
+abhsf_status abhsf_block_histogram_noalloc(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m,
+                                           int64_t n, int32_t r, int32_t s, abhsf_stream_t stream, uint64_t* hist,
+                                           int64_t hist_len, int64_t* blocks)
+{
+    return guarded([&] {
+        abhsf::block_histogram_noalloc(rows, cols, nnz, m, n, r, s, reinterpret_cast<cudaStream_t>(stream), hist,
+                                       hist_len, blocks);
+    });
+}
+
 abhsf_status abhsf_mmf_line(int64_t m, int64_t n, int64_t nnz, int32_t matrix_type, int32_t r, int32_t s,
                             const uint64_t* hist, int64_t hist_len, uint64_t out_single[8], uint64_t out_double[8])
 {

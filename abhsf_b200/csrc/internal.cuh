@@ -13,6 +13,10 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
 void block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r, int s,
                      bool on_device, cudaStream_t st, uint64_t* hist, int64_t hist_len, int64_t* blocks);
 
+// abhsf_block_histogram with device inputs and all scratch in a static array.
+void block_histogram_noalloc(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r,
+                             int s, cudaStream_t st, uint64_t* hist, int64_t hist_len, int64_t* blocks);
+
 void mmf_line_from_hist(int64_t m, int64_t n, int64_t nnz, int type, int64_t r, int64_t s,
                         const std::map<uint64_t, uint64_t>& hist, uint64_t bits1, uint64_t o1[8], uint64_t o2[8]);
 

@@ -169,6 +169,26 @@ ABHSF_API abhsf_status abhsf_block_histogram(const int64_t* rows, const int64_t*
                                    abhsf_stream_t stream, uint64_t* hist, int64_t hist_len,
                                    int64_t* blocks);
 
+/* Largest nnz abhsf_block_histogram_noalloc accepts. */
+#define ABHSF_NOALLOC_MAX_NNZ 1048576
+
+/* abhsf_block_histogram for callers that may not allocate device memory: no
+ * cudaMalloc, cudaFree or allocating library call is made.  Such callers are,
+ * for example, programs whose device memory is handed out by their own
+ * allocator or pool, code paths where a cudaMalloc (which can synchronise the
+ * device) is not acceptable, and processes already at their memory limit.
+ * No counterpart in the reference (its block_stats runs on the host).
+ * rows and cols are device pointers; nnz <= ABHSF_NOALLOC_MAX_NNZ.  The
+ * scratch is one 64 MiB array inside the library's device image, held by
+ * every GPU that loads the library until the process exits.  The first call
+ * on a device looks up that array's device address, so make it before any
+ * stream capture.  All calls share the array: calls whose GPU work overlaps
+ * (other streams, other host threads) race on it.  Synchronises stream. */
+ABHSF_API abhsf_status abhsf_block_histogram_noalloc(const int64_t* rows, const int64_t* cols, int64_t nnz,
+                                                     int64_t m, int64_t n, int32_t r, int32_t s,
+                                                     abhsf_stream_t stream, uint64_t* hist, int64_t hist_len,
+                                                     int64_t* blocks);
+
 /* One line of the reference's mmf-single / mmf-double (block_statistics/mmf.cpp:53-138)
  * from props and a block histogram; out_* = coo32 csr32 coo csr bitmap dense abhsf abhsf134. */
 ABHSF_API abhsf_status abhsf_mmf_line(int64_t m, int64_t n, int64_t nnz, int32_t matrix_type, int32_t r, int32_t s,
