@@ -5,12 +5,11 @@
 // order.  Per tile it dispatches on the scheme:
 //
 //  * bitmap / dense, s >= 32: lane l owns columns l, l+32, ... of the tile and
-//    keeps those x values in registers.  Rows are taken 16 at a time; for each
-//    row a lane loads its value when its bit is set, at the row start plus the
-//    popcount of the lower bits (so the set lanes read one contiguous run:
-//    coalesced), and accumulates value * x.  The 16 per-lane row partials are
-//    reduced by a butterfly reduce-scatter (16 shuffles for 16 rows) that
-//    leaves row r's sum on lane r.  Replaces the bit-by-bit decode loops of
+//    keeps those x values in registers.  Rows are taken kRG (8) at a time; for
+//    each row a lane loads its value when its bit is set, at the row start plus
+//    the popcount of the lower bits (so the set lanes read one contiguous run:
+//    coalesced), and accumulates value * x.  The per-lane row partials are
+//    reduced by a butterfly reduce-scatter that leaves row r's sum on lane r.  Replaces the bit-by-bit decode loops of
 //    spmv/orig/88_bitmap.cpp:183-354 and 44_bitmap.cpp:187-396, and the dense
 //    loop of spmv/orig/88.cpp:579-605.
 //  * COO / CSR (and every scheme at s = 16): the tile's stored elements are
@@ -34,8 +33,15 @@ namespace {
 // block rows from a work counter, so empty rows cost nothing and a long row
 // delays only its own warp.
 constexpr int kWarps = 4;
-constexpr int kMinCtasPerSm = 6;  // 24 resident warps per SM; caps registers at 80
+#ifndef ABHSF_TREE_MINB
+#define ABHSF_TREE_MINB 6
+#endif
+constexpr int kMinCtasPerSm = ABHSF_TREE_MINB;  // resident CTAs per SM the register budget must allow
 constexpr int kGrain = 4;
+#ifndef ABHSF_TREE_RG
+#define ABHSF_TREE_RG 8
+#endif
+constexpr int kRG = ABHSF_TREE_RG;  // rows reduced together in bitmap / dense tiles
 constexpr unsigned kFull = 0xffffffffu;
 
 template <int S>
@@ -57,11 +63,13 @@ struct warp_smem {
 __device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
 __device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t* p) { return __ldcs(p); }
 
-// acc[0..15] per lane -> lane l holds sum over all lanes of acc[l & 15].
-__device__ __forceinline__ double butterfly16(double (&acc)[16], int lane)
+// acc[0..RG-1] per lane -> lane l holds the sum over all lanes of acc[l % RG]
+// (a reduce-scatter: RG-1 shuffles, then log2(32/RG) to finish).
+template <int RG>
+__device__ __forceinline__ double butterfly(double (&acc)[RG], int lane)
 {
 #pragma unroll
-    for (int half = 8; half >= 1; half >>= 1) {
+    for (int half = RG / 2; half >= 1; half >>= 1) {
         const bool upper = (lane & half) != 0;
 #pragma unroll
         for (int i = 0; i < half; ++i) {
@@ -70,13 +78,17 @@ __device__ __forceinline__ double butterfly16(double (&acc)[16], int lane)
             acc[i] = keep + __shfl_xor_sync(kFull, send, half);
         }
     }
-    return acc[0] + __shfl_xor_sync(kFull, acc[0], 16);
+    double r = acc[0];
+#pragma unroll
+    for (int d = RG; d < 32; d <<= 1)
+        r += __shfl_xor_sync(kFull, r, d);
+    return r;
 }
 
 // Bitmap tile, s >= 32.  bm32 = tile bitmap as little-endian u32 words: row
 // r's columns 32j..32j+31 are word r * CPL + j.  Up to 64 rows of bitmap are
 // staged in shared memory with one vector load per lane, their row starts
-// found by one popcount scan; rows are then summed 16 at a time.
+// found by one popcount scan; rows are then summed kRG at a time.
 template <int S>
 __device__ __forceinline__ void tile_bitmap(const uint32_t* __restrict__ bm32, const double* __restrict__ vals,
                                             const double (&xr)[geom<S>::CPL], warp_smem<S>& sm, int lane)
@@ -121,28 +133,56 @@ __device__ __forceinline__ void tile_bitmap(const uint32_t* __restrict__ bm32, c
         running += tot0 + tot1;
         __syncwarp();
 #pragma unroll 1
-        for (int g = 0; g < RB / 16; ++g) {
-            double acc[16];
+        for (int g = 0; g < RB / kRG; ++g) {
+            double acc[kRG];
+            if constexpr (CPL <= 2) {
+                // all of the group's value loads are issued before any is used,
+                // so kRG * CPL loads per lane are in flight at once
+                double v[kRG][CPL];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const int row = g * 16 + i;
-                const double* rv = vals + sm.rowstart[row];
-                int run = 0;
-                double a = 0.0;
+                for (int i = 0; i < kRG; ++i) {
+                    const int row = g * kRG + i;
+                    const double* rv = vals + sm.rowstart[row];
+                    int run = 0;
 #pragma unroll
-                for (int j = 0; j < CPL; ++j) {
-                    const uint32_t w = sm.aux[row * CPL + j];
-                    double v = 0.0;
-                    if ((w >> lane) & 1u)
-                        v = ld_stream(rv + run + __popc(w & lt));
-                    a = fma(v, xr[j], a);
-                    run += __popc(w);
+                    for (int j = 0; j < CPL; ++j) {
+                        const uint32_t w = sm.aux[row * CPL + j];
+                        v[i][j] = 0.0;
+                        if ((w >> lane) & 1u)
+                            v[i][j] = ld_stream(rv + run + __popc(w & lt));
+                        run += __popc(w);
+                    }
                 }
-                acc[i] = a;
+#pragma unroll
+                for (int i = 0; i < kRG; ++i) {
+                    double a = 0.0;
+#pragma unroll
+                    for (int j = 0; j < CPL; ++j)
+                        a = fma(v[i][j], xr[j], a);
+                    acc[i] = a;
+                }
+            } else {  // wide tiles: loads and FMAs interleaved (registers)
+#pragma unroll
+                for (int i = 0; i < kRG; ++i) {
+                    const int row = g * kRG + i;
+                    const double* rv = vals + sm.rowstart[row];
+                    int run = 0;
+                    double a = 0.0;
+#pragma unroll
+                    for (int j = 0; j < CPL; ++j) {
+                        const uint32_t w = sm.aux[row * CPL + j];
+                        double v = 0.0;
+                        if ((w >> lane) & 1u)
+                            v = ld_stream(rv + run + __popc(w & lt));
+                        a = fma(v, xr[j], a);
+                        run += __popc(w);
+                    }
+                    acc[i] = a;
+                }
             }
-            const double r = butterfly16(acc, lane);
-            if (lane < 16)
-                sm.ys[blk * RB + g * 16 + lane] += r;
+            const double r = butterfly<kRG>(acc, lane);
+            if (lane < kRG)
+                sm.ys[blk * RB + g * kRG + lane] += r;
         }
         __syncwarp();
     }
@@ -155,20 +195,37 @@ __device__ __forceinline__ void tile_dense(const double* __restrict__ vals, cons
 {
     constexpr int CPL = geom<S>::CPL;
 #pragma unroll 1
-    for (int g = 0; g < S / 16; ++g) {
-        double acc[16];
+    for (int g = 0; g < S / kRG; ++g) {
+        double acc[kRG];
+        if constexpr (CPL <= 2) {
+            double v[kRG][CPL];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const double* rv = vals + (size_t)(g * 16 + i) * S + lane;
-            double a = 0.0;
+            for (int i = 0; i < kRG; ++i)
 #pragma unroll
-            for (int j = 0; j < CPL; ++j)
-                a = fma(ld_stream(rv + 32 * j), xr[j], a);
-            acc[i] = a;
+                for (int j = 0; j < CPL; ++j)
+                    v[i][j] = ld_stream(vals + (size_t)(g * kRG + i) * S + lane + 32 * j);
+#pragma unroll
+            for (int i = 0; i < kRG; ++i) {
+                double a = 0.0;
+#pragma unroll
+                for (int j = 0; j < CPL; ++j)
+                    a = fma(v[i][j], xr[j], a);
+                acc[i] = a;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < kRG; ++i) {
+                const double* rv = vals + (size_t)(g * kRG + i) * S + lane;
+                double a = 0.0;
+#pragma unroll
+                for (int j = 0; j < CPL; ++j)
+                    a = fma(ld_stream(rv + 32 * j), xr[j], a);
+                acc[i] = a;
+            }
         }
-        const double r = butterfly16(acc, lane);
-        if (lane < 16)
-            sm.ys[g * 16 + lane] += r;
+        const double r = butterfly<kRG>(acc, lane);
+        if (lane < kRG)
+            sm.ys[g * kRG + lane] += r;
     }
     __syncwarp();
 }
@@ -383,8 +440,10 @@ void launch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
         return;
     tree_args P{a.view(), a.tree_rows.get(), a.tree_nrows, a.tree_counter.get(), x, y};
     ABHSF_CUDA(cudaMemsetAsync(a.tree_counter.get(), 0, sizeof(unsigned int), st));
-    const int64_t want = (a.tree_nrows + (int64_t)kGrain * kWarps - 1) / ((int64_t)kGrain * kWarps);
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)a.tree_ctas));
+    // every resident warp takes part unless there are fewer grains than warps
+    const int64_t want = (a.tree_nrows + (int64_t)kGrain - 1) / kGrain;
+    const int64_t ctas = (want + kWarps - 1) / kWarps;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)a.tree_ctas));
     k_spmv_f64<S><<<grid, kWarps * 32, 0, st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }
