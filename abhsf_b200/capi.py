@@ -19,7 +19,6 @@ SCHEME_NAMES = ("coo", "csr", "bitmap", "dense")
 VALUE_TYPES = {"f64": 0, "f32": 1, "bf16": 2}
 MATRIX_TYPES = {"binary": 0, "integer": 1, "real": 2, "complex": 3}
 SUM_ORDERS = {"reference": 0, "tree": 1}
-DEVSTAT_WAIT_TIMEOUT = 1
 NOALLOC_MAX_NNZ = 1048576
 
 
@@ -86,7 +85,6 @@ PROTOTYPES = {
     "abhsf_spmv": (C.c_int, [_vp, _vp, _vp, _vp]),
     "abhsf_spmv_host": (C.c_int, [_vp, _vp, _vp, _vp]),
     "abhsf_release": (C.c_int, [_vp]),
-    "abhsf_device_status": (C.c_int, [_vp, _vp, _i32, C.POINTER(_i32)]),
     "abhsf_stats_get": (C.c_int, [_vp, C.POINTER(Stats)]),
     "abhsf_export_host": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "abhsf_block_histogram": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _i32, _i32, _vp, _u64p, _i64,
@@ -96,7 +94,6 @@ PROTOTYPES = {
     "abhsf_mmf_line": (C.c_int, [_i64, _i64, _i64, _i32, _i32, _i32, _u64p, _i64, _u64p, _u64p]),
     "abhsf_block_scheme_bits": (C.c_uint64, [_i32, _i64, _i64, _i64, _i64]),
     "abhsf_block_select_scheme": (_i32, [_i64, _i64, _i64, _i64, _i32, _i32]),
-    "abhsf_test_set_hooks": (None, [_i64, C.c_uint32]),
 }
 
 

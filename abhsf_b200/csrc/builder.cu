@@ -129,14 +129,6 @@ __global__ void k_tile_meta(int64_t T, const int64_t* __restrict__ tile_start, c
     }
 }
 
-__global__ void k_narrow_rows(int64_t T, const int64_t* __restrict__ in, uint32_t* __restrict__ out)
-{
-    GRID_STRIDE(t, T)
-    {
-        out[t] = (uint32_t)in[t];
-    }
-}
-
 // brow_ptr[i] = first tile whose block row is >= i.
 __global__ void k_brow_ptr(int64_t M, int64_t T, const int64_t* __restrict__ tile_row, int64_t* __restrict__ brow_ptr)
 {
@@ -529,13 +521,7 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
                                                        a.values.get());
         check_launch("k_scatter");
     }
-    a.tile_row.alloc(T);
-    k_narrow_rows<<<grid_for(T), kThreads, 0, st>>>(T, tile_row.get(), a.tile_row.get());
-    check_launch("k_narrow_rows");
-    a.dev_status.alloc(1);
-    ABHSF_CUDA(cudaMemsetAsync(a.dev_status.get(), 0, sizeof(int), st));
     finish_stats(a, dense_bits, st);
-    prepare_ordered(a, st);
     prepare_tree(a, st);
 }
 

@@ -16,7 +16,7 @@ thread_local std::string g_last_error;
 void spmv_dispatch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
     if (a.sum_order == ABHSF_SUM_REFERENCE)
-        spmv_f64_ordered(a, x, y, st);
+        spmv_f64_seq(a, x, y, st);
     else
         spmv_f64(a, x, y, st);
 }
@@ -100,21 +100,6 @@ abhsf_status abhsf_spmv_host(abhsf_matrix* a, const double* x, double* y, abhsf_
         abhsf::spmv_dispatch(*a, a->x_stage.get(), a->y_stage.get(), st);
         ABHSF_CUDA(cudaMemcpyAsync(y, a->y_stage.get(), a->m * sizeof(double), cudaMemcpyDeviceToHost, st));
         ABHSF_CUDA(cudaStreamSynchronize(st));
-    });
-}
-
-abhsf_status abhsf_device_status(abhsf_matrix* a, abhsf_stream_t stream, int32_t clear, int32_t* out)
-{
-    return guarded([&] {
-        if (!a || !out)
-            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle and out must be non-NULL");
-        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-        int v = 0;
-        ABHSF_CUDA(cudaMemcpyAsync(&v, a->dev_status.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
-        if (clear)
-            ABHSF_CUDA(cudaMemsetAsync(a->dev_status.get(), 0, sizeof(int), st));
-        ABHSF_CUDA(cudaStreamSynchronize(st));
-        *out = v;
     });
 }
 

@@ -162,12 +162,6 @@ struct abhsf_matrix {
     abhsf_stats stats{};
     int32_t sum_order = ABHSF_SUM_REFERENCE;
     // reference-order SpMV: block row of every tile, chunk schedule, stream ranges
-    abhsf::dbuf<uint32_t> tile_row;
-    abhsf::dbuf<uint8_t> ord_items;     // 64-byte chunk descriptors
-    abhsf::dbuf<int64_t> ord_streams;   // [ord_ctas * groups + 1] chunk range of each stream
-    int64_t ord_nitems = 0;
-    int ord_ctas = 0;
-    abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
     // tree-order SpMV: non-empty block rows and the work counter of its persistent warps
     abhsf::dbuf<uint32_t> tree_rows;
     int64_t tree_nrows = 0;

@@ -24,13 +24,15 @@ void mmf_line_from_hist(int64_t m, int64_t n, int64_t nnz, int type, int64_t r, 
 void spmv_f64(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
 
 // y += A x with the reference CSR's per-row summation order (bitwise equal).
-void spmv_f64_ordered(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
 
 // Per-matrix set-up of the tree-order kernel (non-empty block rows, counter).
 void prepare_tree(abhsf_matrix& a, cudaStream_t st);
 
+// y += A x with the reference CSR's per-row summation order, streaming through
+// registers (shares the tree kernel's work list).
+void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+
 // Per-matrix set-up of the reference-order kernel (CTA tile ranges).
-void prepare_ordered(abhsf_matrix& a, cudaStream_t st);
 
 // abhsf_spmv's choice between the two f64 kernels (abhsf_matrix::sum_order).
 void spmv_dispatch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);

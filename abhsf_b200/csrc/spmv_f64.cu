@@ -23,21 +23,22 @@
 // bitwise reproducible run to run.
 #include <algorithm>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "common.cuh"
 #include "internal.cuh"
 
 namespace abhsf {
 namespace {
 
-// Persistent warps: each warp repeatedly takes kGrain consecutive non-empty
-// block rows from a work counter, so empty rows cost nothing and a long row
-// delays only its own warp.
+// Persistent warps: warp w first takes the w-th non-empty block row, then
+// takes the next untaken one from a work counter, heaviest block rows first,
+// so empty rows cost nothing and the warps finish close together.
 constexpr int kWarps = 4;
 #ifndef ABHSF_TREE_MINB
 #define ABHSF_TREE_MINB 6
 #endif
 constexpr int kMinCtasPerSm = ABHSF_TREE_MINB;  // resident CTAs per SM the register budget must allow
-constexpr int kGrain = 4;
 #ifndef ABHSF_TREE_RG
 #define ABHSF_TREE_RG 8
 #endif
@@ -397,16 +398,14 @@ __global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_f64(tree_ar
     __shared__ warp_smem<S> smem[kWarps];
     const int lane = threadIdx.x & 31;
     warp_smem<S>& sm = smem[threadIdx.x >> 5];
-    for (;;) {
-        unsigned int base = 0;
+    const unsigned int nw = gridDim.x * kWarps;
+    unsigned int k = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    while ((int64_t)k < P.nrows) {
+        unsigned int next = 0;
         if (lane == 0)
-            base = atomicAdd(P.counter, (unsigned int)kGrain);
-        base = __shfl_sync(kFull, base, 0);
-        if ((int64_t)base >= P.nrows)
-            break;
-        const int64_t end = min((int64_t)base + kGrain, P.nrows);
-        for (int64_t k = base; k < end; ++k)
-            block_row<S>(P, (int64_t)P.rows[k], sm, lane);
+            next = atomicAdd(P.counter, 1u) + nw;  // in flight during this block row
+        block_row<S>(P, (int64_t)P.rows[k], sm, lane);
+        k = __shfl_sync(kFull, next, 0);
     }
 }
 
@@ -425,6 +424,18 @@ __global__ void k_nonempty_scatter(int64_t M, const int64_t* __restrict__ brow_p
             rows[pos[i]] = (uint32_t)i;
 }
 
+// A block row's weight: the bytes an SpMV reads for it (values, index payload,
+// and per tile its x segment and header).
+__global__ void k_row_weight(int64_t nr, const uint32_t* __restrict__ rows, tiles_view A, int vsize, int s,
+                             uint64_t* __restrict__ weight)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nr; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t I = rows[k], t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
+        weight[k] = (uint64_t)((A.tile_val_off[t1] - A.tile_val_off[t0]) * vsize +
+                               (A.tile_idx_off[t1] - A.tile_idx_off[t0]) + (t1 - t0) * (8 * (int64_t)s + 32));
+    }
+}
+
 template <int S>
 int tree_ctas_per_sm()
 {
@@ -440,9 +451,8 @@ void launch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
         return;
     tree_args P{a.view(), a.tree_rows.get(), a.tree_nrows, a.tree_counter.get(), x, y};
     ABHSF_CUDA(cudaMemsetAsync(a.tree_counter.get(), 0, sizeof(unsigned int), st));
-    // every resident warp takes part unless there are fewer grains than warps
-    const int64_t want = (a.tree_nrows + (int64_t)kGrain - 1) / kGrain;
-    const int64_t ctas = (want + kWarps - 1) / kWarps;
+    // every resident warp takes part unless there are fewer block rows than warps
+    const int64_t ctas = (a.tree_nrows + kWarps - 1) / kWarps;
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)a.tree_ctas));
     k_spmv_f64<S><<<grid, kWarps * 32, 0, st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
@@ -478,10 +488,28 @@ void prepare_tree(abhsf_matrix& a, cudaStream_t st)
     if (nr > int64_t(UINT32_MAX))
         fail(ABHSF_ERROR_UNSUPPORTED, "more than 2^32 non-empty block rows");
     a.tree_rows.alloc(nr);
-    k_nonempty_scatter<<<g, 256, 0, st>>>(a.M, a.brow_ptr.get(), pos.get(), a.tree_rows.get());
-    ABHSF_CUDA(cudaGetLastError());
-    ABHSF_CUDA(cudaStreamSynchronize(st));
     a.tree_nrows = nr;
+    if (nr == 0)
+        return;
+    // Heaviest block rows first: the SpMV kernels hand out one block row at a
+    // time in this order, so the last ones to start are the shortest and all
+    // warps finish close together.  The sort is stable (ties keep ascending
+    // row order), so the order is deterministic; it does not affect results,
+    // since each block row is summed by one warp on its own.
+    dbuf<uint32_t> asc(nr);
+    dbuf<uint64_t> w(nr), w_sorted(nr);
+    k_nonempty_scatter<<<g, 256, 0, st>>>(a.M, a.brow_ptr.get(), pos.get(), asc.get());
+    ABHSF_CUDA(cudaGetLastError());
+    const unsigned gw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nr + 255) / 256, 4096));
+    k_row_weight<<<gw, 256, 0, st>>>(nr, asc.get(), a.view(), (int)value_size(a.value_type), (int)a.s, w.get());
+    ABHSF_CUDA(cudaGetLastError());
+    size_t tmp_bytes = 0;
+    ABHSF_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, w.get(), w_sorted.get(), asc.get(),
+                                                         a.tree_rows.get(), nr, 0, 64, st));
+    dbuf<uint8_t> tmp(std::max<size_t>(tmp_bytes, 1));
+    ABHSF_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.get(), tmp_bytes, w.get(), w_sorted.get(), asc.get(),
+                                                         a.tree_rows.get(), nr, 0, 64, st));
+    ABHSF_CUDA(cudaStreamSynchronize(st));
 }
 
 void spmv_f64(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)

@@ -1,0 +1,435 @@
+// spmv_seq.cu -- y += A x over the ABHSF format in the reference's summation
+// order, FP64, sm_100a, streaming through registers.
+//
+// The reference's CSR SpMV (csr_matrix::spmv_naive,
+// spmv/bottlenecks/spmv.cpp:58-64) adds a row's products one at a time,
+// columns ascending, onto y[row], each product rounded before its add.  Here
+// persistent warps take non-empty block rows one at a time, heaviest first
+// (the order prepare_tree lists them in), from a work counter; a warp keeps
+// its block row's y segment in shared memory (starting from y0) and walks the
+// tiles in column order.  For a group of rows of a bitmap or dense
+// tile the lanes load the values with coalesced, predicated loads (lane l
+// owns columns l, l+32, ...; a set bit's value sits at the row start plus the
+// popcount of the lower bits), form value * x, and store the products
+// compactly -- row-major, columns ascending -- in a small per-warp buffer.
+// Then one lane per row adds its row's products, a contiguous run, one at a
+// time onto the row's y entry (dadd_rn(acc, p), p = dmul_rn(v, x)): exactly
+// the reference's order, so y is bitwise the reference CSR's.  The next
+// group's loads are issued before these add chains so that they overlap.
+// COO / CSR tiles stream 32 elements at a time: each lane forms one product,
+// and the first lane of each row segment adds the segment in order.  A dense
+// tile's stored zeros become -0.0, which leaves a sum bitwise unchanged (the
+// reference's CSR has no such elements).
+#include <algorithm>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace abhsf {
+namespace {
+
+constexpr int kWarps = 4;
+#ifndef ABHSF_SEQ_MINB
+#define ABHSF_SEQ_MINB 6
+#endif
+constexpr int kMinCtasPerSm = ABHSF_SEQ_MINB;
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int S>
+struct sg {
+    static constexpr int CPL = S >= 32 ? S / 32 : 1;       // columns per lane
+    static constexpr int RB = S >= 64 ? 64 : S;            // bitmap rows staged at once
+    static constexpr int WPB = RB * CPL;                   // u32 words of a staged bitmap block
+#ifndef ABHSF_SEQ_VALS
+#define ABHSF_SEQ_VALS 16
+#endif
+    // rows per load group: ABHSF_SEQ_VALS values per lane in flight
+    // (s >= 128 keeps 16 so that four warps' buffers fit the static shared-memory limit)
+    static constexpr int RG = S <= 16 ? 16 : S >= 128 ? 16 / CPL : (ABHSF_SEQ_VALS / CPL > 32 ? 32 : ABHSF_SEQ_VALS / CPL);
+    static constexpr int BUF = RG * S;                     // product buffer (doubles)
+    static constexpr int AUX = WPB > 8 ? WPB : 8;
+};
+
+template <int S>
+struct seq_smem {
+    alignas(16) uint32_t aux[sg<S>::AUX];  // a staged bitmap block, or CSR row_end
+    double ys[S];                          // the block row's y segment
+    double xs[S];                          // x segment (element streams)
+    int32_t rowstart[sg<S>::RB + 1];       // staged rows' first values (tile-relative), + end
+    double buf[sg<S>::BUF];                // a group's products, row-major
+};
+
+struct seq_args {
+    tiles_view A;
+    const uint32_t* rows;  // non-empty block rows, ascending
+    int64_t nrows;
+    unsigned int* counter;
+    const double* x;
+    double* y;
+};
+
+__device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
+__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+
+// acc + p[0] + p[1] + ... + p[n-1], one at a time, left to right.
+__device__ __forceinline__ double chain(double acc, const double* p, int n)
+{
+    int i = 0;
+    for (; i + 8 <= n; i += 8) {
+        double t[8];
+#pragma unroll
+        for (int v = 0; v < 8; ++v)
+            t[v] = p[i + v];
+#pragma unroll
+        for (int v = 0; v < 8; ++v)
+            acc = fadd(acc, t[v]);
+    }
+    for (; i < n; ++i)
+        acc = fadd(acc, p[i]);
+    return acc;
+}
+
+// Bitmap tile, s >= 32: row r's columns 32j..32j+31 are bitmap word r*CPL + j.
+template <int S>
+__device__ __forceinline__ void seq_bitmap(const uint32_t* __restrict__ bm32, const double* __restrict__ vals,
+                                           const double (&xr)[sg<S>::CPL], seq_smem<S>& sm, int lane)
+{
+    constexpr int CPL = sg<S>::CPL, RB = sg<S>::RB, WPB = sg<S>::WPB, RG = sg<S>::RG;
+    constexpr int NG = RB / RG;
+    const uint32_t lt = (1u << lane) - 1u;
+    int running = 0;
+#pragma unroll 1
+    for (int blk = 0; blk < S / RB; ++blk) {
+        const uint4* src = reinterpret_cast<const uint4*>(bm32 + blk * WPB);
+        uint4* dst = reinterpret_cast<uint4*>(sm.aux);
+        for (int i = lane; i < WPB / 4; i += 32)
+            dst[i] = __ldcs(src + i);
+        __syncwarp();
+        int pc0 = 0, pc1 = 0;  // rows lane and lane + 32 of the block
+#pragma unroll
+        for (int j = 0; j < CPL; ++j) {
+            if (lane < RB)
+                pc0 += __popc(sm.aux[lane * CPL + j]);
+            if (RB == 64)
+                pc1 += __popc(sm.aux[(lane + 32) * CPL + j]);
+        }
+        int inc0 = pc0, inc1 = pc1;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t0 = __shfl_up_sync(kFull, inc0, d);
+            const int t1 = __shfl_up_sync(kFull, inc1, d);
+            if (lane >= d) {
+                inc0 += t0;
+                inc1 += t1;
+            }
+        }
+        const int tot0 = __shfl_sync(kFull, inc0, 31);
+        const int tot1 = __shfl_sync(kFull, inc1, 31);
+        if (lane < RB)
+            sm.rowstart[lane] = running + inc0 - pc0;
+        if (RB == 64)
+            sm.rowstart[lane + 32] = running + tot0 + inc1 - pc1;
+        running += tot0 + tot1;
+        if (lane == 0)
+            sm.rowstart[RB] = running;
+        __syncwarp();
+
+        // a group's value indices (tile-relative; -1: bit clear) and values
+        int idx[RG][CPL];
+        double v[RG][CPL];
+        auto load_group = [&](int g) {
+#pragma unroll
+            for (int i = 0; i < RG; ++i) {
+                const int row = g * RG + i;
+                int run = sm.rowstart[row];
+#pragma unroll
+                for (int j = 0; j < CPL; ++j) {
+                    const uint32_t w = sm.aux[row * CPL + j];
+                    idx[i][j] = ((w >> lane) & 1u) ? run + __popc(w & lt) : -1;
+                    v[i][j] = idx[i][j] >= 0 ? ld_stream(vals + idx[i][j]) : 0.0;
+                    run += __popc(w);
+                }
+            }
+        };
+        load_group(0);
+#pragma unroll 1
+        for (int g = 0; g < NG; ++g) {
+            const int base = sm.rowstart[g * RG];
+#pragma unroll
+            for (int i = 0; i < RG; ++i)
+#pragma unroll
+                for (int j = 0; j < CPL; ++j)
+                    if (idx[i][j] >= 0)
+                        sm.buf[idx[i][j] - base] = fmul(v[i][j], xr[j]);
+            __syncwarp();
+            if (g + 1 < NG)
+                load_group(g + 1);  // in flight during the add chains below
+            if (lane < RG) {
+                const int row = g * RG + lane;
+                const int lo = sm.rowstart[row] - base, hi = sm.rowstart[row + 1] - base;
+                double& yr = sm.ys[blk * RB + row];
+                yr = chain(yr, sm.buf + lo, hi - lo);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Dense tile, s >= 32: all s*s values, row-major.
+template <int S>
+__device__ __forceinline__ void seq_dense(const double* __restrict__ vals, const double (&xr)[sg<S>::CPL],
+                                          int64_t c0, int64_t n, seq_smem<S>& sm, int lane)
+{
+    constexpr int CPL = sg<S>::CPL, RG = sg<S>::RG, NG = S / RG;
+    double v[RG][CPL];
+    auto load_group = [&](int g) {
+#pragma unroll
+        for (int i = 0; i < RG; ++i)
+#pragma unroll
+            for (int j = 0; j < CPL; ++j)
+                v[i][j] = ld_stream(vals + (size_t)(g * RG + i) * S + lane + 32 * j);
+    };
+    load_group(0);
+#pragma unroll 1
+    for (int g = 0; g < NG; ++g) {
+#pragma unroll
+        for (int i = 0; i < RG; ++i)
+#pragma unroll
+            for (int j = 0; j < CPL; ++j) {
+                const int c = lane + 32 * j;
+                // stored zeros become -0.0, a no-op in the sums
+                sm.buf[i * S + c] = (v[i][j] != 0.0 && c0 + c < n) ? fmul(v[i][j], xr[j]) : -0.0;
+            }
+        __syncwarp();
+        if (g + 1 < NG)
+            load_group(g + 1);
+        if (lane < RG) {
+            double& yr = sm.ys[g * RG + lane];
+            yr = chain(yr, sm.buf + lane * S, S);
+        }
+        __syncwarp();
+    }
+}
+
+// s = 16 bitmap or dense: the whole tile (256 positions) at once.
+template <bool DENSE>
+__device__ __forceinline__ void seq_16(const uint32_t* __restrict__ bm32, const double* __restrict__ vals, double xl,
+                                       int64_t c0, int64_t n, seq_smem<16>& sm, int lane)
+{
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t w[8];
+    double v[8];
+    int running = 0;
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+        w[it] = DENSE ? 0xffffffffu : __ldcs(bm32 + it);
+        v[it] = 0.0;
+        if ((w[it] >> lane) & 1u)
+            v[it] = ld_stream(vals + (DENSE ? it * 32 + lane : running + __popc(w[it] & lt)));
+        running += __popc(w[it]);
+    }
+    running = 0;
+    const bool col_ok = c0 + (lane & 15) < n;
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+        if ((w[it] >> lane) & 1u)
+            sm.buf[running + __popc(w[it] & lt)] =
+                DENSE && !(v[it] != 0.0 && col_ok) ? -0.0 : fmul(v[it], xl);
+        running += __popc(w[it]);
+    }
+    // row r's bits: half (r & 1) of word r >> 1
+    int pc = 0;
+    if (lane < 16) {
+        uint32_t wr = 0;
+#pragma unroll
+        for (int it = 0; it < 8; ++it)
+            if (it == (lane >> 1))
+                wr = w[it];
+        pc = __popc((wr >> ((lane & 1) * 16)) & 0xffffu);
+    }
+    int inc = pc;
+#pragma unroll
+    for (int d = 1; d < 16; d <<= 1) {
+        const int t = __shfl_up_sync(kFull, inc, d);
+        if (lane >= d)
+            inc += t;
+    }
+    __syncwarp();
+    if (lane < 16)
+        sm.ys[lane] = chain(sm.ys[lane], sm.buf + inc - pc, pc);
+    __syncwarp();
+}
+
+// COO / CSR tile: 32 stored elements at a time; the first lane of each row
+// segment adds the segment's products onto the row, in element order.
+template <int S, bool CSR>
+__device__ __forceinline__ void seq_stream(const uint8_t* __restrict__ pay, const double* __restrict__ vals, int z,
+                                           seq_smem<S>& sm, int lane)
+{
+    constexpr int LG = S == 16 ? 4 : S == 32 ? 5 : S == 64 ? 6 : S == 128 ? 7 : 8;
+    const uint16_t* key16 = reinterpret_cast<const uint16_t*>(pay);
+    const uint8_t* col8 = pay + 2 * S;
+    uint16_t* row_end = reinterpret_cast<uint16_t*>(sm.aux);
+    if (CSR) {
+        for (int r = lane; r < S; r += 32)
+            row_end[r] = __ldcs(key16 + r);
+        __syncwarp();
+    }
+#pragma unroll 1
+    for (int base = 0; base < z; base += 32) {
+        const int k = base + lane;
+        int lr = S;  // idle lanes: no row
+        if (k < z) {
+            int lc;
+            if (CSR) {
+                lc = __ldcs(col8 + k);
+                int lo = 0, hi = S;  // first r with row_end[r] > k
+#pragma unroll
+                for (int step = 0; step <= LG; ++step) {
+                    if (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (row_end[mid] > k)
+                            hi = mid;
+                        else
+                            lo = mid + 1;
+                    }
+                }
+                lr = lo;
+            } else {
+                const uint32_t key = __ldcs(key16 + k);
+                lr = (int)(key >> LG);
+                lc = (int)(key & (S - 1));
+            }
+            sm.buf[lane] = fmul(ld_stream(vals + k), sm.xs[lc]);
+        }
+        const int plr = __shfl_up_sync(kFull, lr, 1);
+        const bool head = k < z && (lane == 0 || plr != lr);
+        const unsigned heads = __ballot_sync(kFull, head);
+        __syncwarp();
+        if (head) {
+            const unsigned later = heads & ~((2u << lane) - 1u);  // heads after this lane (lane 31: none)
+            const int cnt = min(z - base, 32);
+            const int end = later ? __ffs(later) - 1 : cnt;
+            sm.ys[lr] = chain(sm.ys[lr], sm.buf + lane, end - lane);
+        }
+        __syncwarp();
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void seq_block_row(const seq_args& P, int64_t I, seq_smem<S>& sm, int lane)
+{
+    constexpr int CPL = sg<S>::CPL;
+    const tiles_view& A = P.A;
+    const double* __restrict__ values = static_cast<const double*>(A.values);
+    const int64_t t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
+    const int64_t r0 = I * S;
+    for (int r = lane; r < S; r += 32)
+        sm.ys[r] = (r0 + r < A.m) ? P.y[r0 + r] : 0.0;
+    __syncwarp();
+    uint32_t n_col = A.tile_col[t0], n_z = A.tile_nnz[t0];
+    uint8_t n_sch = A.tile_scheme[t0];
+    int64_t n_vo = A.tile_val_off[t0], n_io = A.tile_idx_off[t0];
+#pragma unroll 1
+    for (int64_t t = t0; t < t1; ++t) {
+        const int64_t c0 = (int64_t)n_col * S;
+        const int z = (int)n_z;
+        const int sch = n_sch;
+        const double* vals = values + n_vo;
+        const uint8_t* pay = A.payload + n_io;
+        if (t + 1 < t1) {
+            n_col = A.tile_col[t + 1];
+            n_z = A.tile_nnz[t + 1];
+            n_sch = A.tile_scheme[t + 1];
+            n_vo = A.tile_val_off[t + 1];
+            n_io = A.tile_idx_off[t + 1];
+        }
+        double xr[CPL];
+#pragma unroll
+        for (int j = 0; j < CPL; ++j) {
+            const int64_t c = c0 + (S >= 32 ? 32 * j + lane : (lane & (S - 1)));
+            xr[j] = c < A.n ? __ldg(P.x + c) : 0.0;
+        }
+        if (S >= 32 && sch == ABHSF_SCHEME_BITMAP) {
+            if constexpr (S >= 32)
+                seq_bitmap<S>(reinterpret_cast<const uint32_t*>(pay), vals, xr, sm, lane);
+        } else if (S >= 32 && sch == ABHSF_SCHEME_DENSE) {
+            if constexpr (S >= 32)
+                seq_dense<S>(vals, xr, c0, A.n, sm, lane);
+        } else if (S == 16 && sch == ABHSF_SCHEME_BITMAP) {
+            if constexpr (S == 16)
+                seq_16<false>(reinterpret_cast<const uint32_t*>(pay), vals, xr[0], c0, A.n, sm, lane);
+        } else if (S == 16 && sch == ABHSF_SCHEME_DENSE) {
+            if constexpr (S == 16)
+                seq_16<true>(nullptr, vals, xr[0], c0, A.n, sm, lane);
+        } else {
+#pragma unroll
+            for (int j = 0; j < CPL; ++j)
+                if (S >= 32 || lane < S)
+                    sm.xs[S >= 32 ? 32 * j + lane : lane] = xr[j];
+            __syncwarp();
+            if (sch == ABHSF_SCHEME_CSR)
+                seq_stream<S, true>(pay, vals, z, sm, lane);
+            else
+                seq_stream<S, false>(pay, vals, z, sm, lane);
+        }
+    }
+    __syncwarp();
+    for (int r = lane; r < S; r += 32)
+        if (r0 + r < A.m)
+            P.y[r0 + r] = sm.ys[r];
+    __syncwarp();
+}
+
+template <int S>
+__global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_f64_seq(seq_args P)
+{
+    __shared__ seq_smem<S> smem[kWarps];
+    const int lane = threadIdx.x & 31;
+    seq_smem<S>& sm = smem[threadIdx.x >> 5];
+    const unsigned int nw = gridDim.x * kWarps;
+    unsigned int k = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    while ((int64_t)k < P.nrows) {
+        unsigned int next = 0;
+        if (lane == 0)
+            next = atomicAdd(P.counter, 1u) + nw;  // in flight during this block row
+        seq_block_row<S>(P, (int64_t)P.rows[k], sm, lane);
+        k = __shfl_sync(kFull, next, 0);
+    }
+}
+
+template <int S>
+void launch_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+{
+    if (a.tree_nrows == 0)
+        return;
+    int dev = 0, nsm = 0, per_sm = 0;
+    ABHSF_CUDA(cudaGetDevice(&dev));
+    ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_f64_seq<S>, kWarps * 32, 0));
+    seq_args P{a.view(), a.tree_rows.get(), a.tree_nrows, a.tree_counter.get(), x, y};
+    ABHSF_CUDA(cudaMemsetAsync(a.tree_counter.get(), 0, sizeof(unsigned int), st));
+    const int64_t ctas = (a.tree_nrows + kWarps - 1) / kWarps;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)nsm * std::max(per_sm, 1)));
+    k_spmv_f64_seq<S><<<grid, kWarps * 32, 0, st>>>(P);
+    ABHSF_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+{
+    if (a.M == 0 || a.T == 0)
+        return;
+    switch (a.s) {
+    case 16: launch_seq<16>(a, x, y, st); break;
+    case 32: launch_seq<32>(a, x, y, st); break;
+    case 64: launch_seq<64>(a, x, y, st); break;
+    case 128: launch_seq<128>(a, x, y, st); break;
+    case 256: launch_seq<256>(a, x, y, st); break;
+    default: fail(ABHSF_ERROR_UNSUPPORTED, "block size without an SpMV kernel");
+    }
+}
+
+}  // namespace abhsf

@@ -14,9 +14,11 @@
  * for the last failure on the calling thread is abhsf_last_error_string().
  * Indices are 0-based (matrix_market_reader.h:135-136).  A handle owns all of
  * its device memory.  Calls taking a stream are ordered on it; a NULL stream
- * is the legacy default stream.  A handle may be used from several threads
- * for abhsf_spmv / abhsf_stats / abhsf_export_host at once; abhsf_spmv_host
- * and abhsf_release need exclusive use.
+ * is the legacy default stream.  abhsf_stats_get may be called from several
+ * threads at once.  abhsf_spmv keeps a work counter in the handle: SpMVs on
+ * one handle must not overlap on the GPU (queue them on one stream, or order
+ * the streams).  abhsf_spmv_host, abhsf_export_host and abhsf_release need
+ * exclusive use of the handle.
  *
  * Format (device arrays, s = block size, M = ceil(m/s), T = nonzero tiles):
  *   brow_ptr[M+1]  int64  tiles of block row I are [brow_ptr[I], brow_ptr[I+1])
@@ -86,9 +88,6 @@ typedef enum abhsf_sum_order {
     ABHSF_SUM_REFERENCE = 0,
     ABHSF_SUM_TREE = 1
 } abhsf_sum_order;
-
-/* Bits of the per-matrix device status word (abhsf_device_status). */
-#define ABHSF_DEVSTAT_WAIT_TIMEOUT 1 /* a bounded pipeline wait gave up; y is incomplete */
 
 /* include/abhsf/utils/matrix_properties.h:8-14 */
 typedef enum abhsf_matrix_type {
@@ -200,11 +199,6 @@ ABHSF_API abhsf_status abhsf_mmf_line(int64_t m, int64_t n, int64_t nnz, int32_t
 ABHSF_API uint64_t abhsf_block_scheme_bits(int32_t scheme, int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value);
 ABHSF_API int32_t abhsf_block_select_scheme(int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value, int32_t is_binary,
                                   int32_t allow_csr);
-
-/* Waits for the work queued on stream, then returns the matrix's device
- * status word (ABHSF_DEVSTAT_* bits; 0 = every SpMV so far completed) and,
- * if clear != 0, resets it. */
-ABHSF_API abhsf_status abhsf_device_status(abhsf_matrix* a, abhsf_stream_t stream, int32_t clear, int32_t* out);
 
 /* Reason for the last non-success status returned on this thread. */
 ABHSF_API const char* abhsf_last_error_string(void);
