@@ -523,6 +523,7 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
     }
     finish_stats(a, dense_bits, st);
     prepare_tree(a, st);
+    prepare_ring(a, st);
 }
 
 void block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r, int s,

@@ -15,8 +15,10 @@ thread_local std::string g_last_error;
 
 void spmv_dispatch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
-    if (a.sum_order == ABHSF_SUM_REFERENCE)
-        spmv_f64_seq(a, x, y, st);
+    if (a.sum_order == ABHSF_SUM_REFERENCE) {
+        if (!spmv_f64_ring(a, x, y, st))
+            spmv_f64_seq(a, x, y, st);
+    }
     else
         spmv_f64(a, x, y, st);
 }

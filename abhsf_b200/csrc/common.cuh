@@ -161,12 +161,15 @@ struct abhsf_matrix {
     abhsf::dbuf<uint8_t> values;  // n_values * value_size(value_type) bytes (+16 padding)
     abhsf_stats stats{};
     int32_t sum_order = ABHSF_SUM_REFERENCE;
-    // reference-order SpMV: block row of every tile, chunk schedule, stream ranges
     // tree-order SpMV: non-empty block rows and the work counter of its persistent warps
     abhsf::dbuf<uint32_t> tree_rows;
     int64_t tree_nrows = 0;
     abhsf::dbuf<unsigned int> tree_counter;
     int tree_ctas = 0;
+    // reference-order SpMV, s = 32 / 64: every warp's tile descriptors and their ranges
+    abhsf::dbuf<uint8_t> ring_desc;
+    abhsf::dbuf<int64_t> ring_wbeg;
+    int ring_warps = 0;  // 0: the streaming kernel serves this matrix
     // staging for abhsf_spmv_host
     abhsf::dbuf<double> x_stage, y_stage;
 

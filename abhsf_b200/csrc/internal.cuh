@@ -27,12 +27,17 @@ void spmv_f64(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st
 
 // Per-matrix set-up of the tree-order kernel (non-empty block rows, counter).
 void prepare_tree(abhsf_matrix& a, cudaStream_t st);
+// Per-matrix set-up of the ring kernel (block rows dealt to warps, tile
+// descriptors); leaves ring_warps = 0 where that kernel does not apply.
+void prepare_ring(abhsf_matrix& a, cudaStream_t st);
 
 // y += A x with the reference CSR's per-row summation order, streaming through
 // registers (shares the tree kernel's work list).
 void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+// The same order through per-warp shared-memory rings (s = 32, 64); false
+// when the matrix has no ring schedule.
+bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
 
-// Per-matrix set-up of the reference-order kernel (CTA tile ranges).
 
 // abhsf_spmv's choice between the two f64 kernels (abhsf_matrix::sum_order).
 void spmv_dispatch(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
