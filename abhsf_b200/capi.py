@@ -20,6 +20,7 @@ VALUE_TYPES = {"f64": 0, "f32": 1, "bf16": 2}
 MATRIX_TYPES = {"binary": 0, "integer": 1, "real": 2, "complex": 3}
 SUM_ORDERS = {"reference": 0, "tree": 1}
 NOALLOC_MAX_NNZ = 1048576
+DEVSTAT_WAIT_TIMEOUT = 1
 
 
 class AbhsfError(RuntimeError):
@@ -79,6 +80,8 @@ _u64p = C.POINTER(C.c_uint64)
 # name -> (restype, argtypes)
 PROTOTYPES = {
     "abhsf_abi_version": (_i32, []),
+    "abhsf_device_status": (C.c_int, [_vp, _vp, _i32, C.POINTER(_i32)]),
+    "abhsf_test_set_hooks": (None, [_i64, C.c_uint32]),
     "abhsf_last_error_string": (C.c_char_p, []),
     "abhsf_build_opts_default": (None, [C.POINTER(BuildOpts)]),
     "abhsf_build": (C.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, C.POINTER(BuildOpts), _vp, C.POINTER(_vp)]),

@@ -521,6 +521,8 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
                                                        a.values.get());
         check_launch("k_scatter");
     }
+    a.dev_status.alloc(1);
+    ABHSF_CUDA(cudaMemsetAsync(a.dev_status.get(), 0, sizeof(int), st));
     finish_stats(a, dense_bits, st);
     prepare_tree(a, st);
     prepare_ring(a, st);

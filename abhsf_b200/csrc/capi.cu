@@ -105,6 +105,21 @@ abhsf_status abhsf_spmv_host(abhsf_matrix* a, const double* x, double* y, abhsf_
     });
 }
 
+abhsf_status abhsf_device_status(abhsf_matrix* a, abhsf_stream_t stream, int32_t clear, int32_t* out)
+{
+    return guarded([&] {
+        if (!a || !out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle and out must be non-NULL");
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        int v = 0;
+        ABHSF_CUDA(cudaMemcpyAsync(&v, a->dev_status.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (clear)
+            ABHSF_CUDA(cudaMemsetAsync(a->dev_status.get(), 0, sizeof(int), st));
+        ABHSF_CUDA(cudaStreamSynchronize(st));
+        *out = v;
+    });
+}
+
 abhsf_status abhsf_release(abhsf_matrix* a)
 {
     return guarded([&] { delete a; });

@@ -166,10 +166,11 @@ struct abhsf_matrix {
     int64_t tree_nrows = 0;
     abhsf::dbuf<unsigned int> tree_counter;
     int tree_ctas = 0;
-    // reference-order SpMV, s = 32 / 64: every warp's tile descriptors and their ranges
+    // reference-order SpMV, s = 32 / 64: every CTA's tile descriptors and their ranges
     abhsf::dbuf<uint8_t> ring_desc;
     abhsf::dbuf<int64_t> ring_wbeg;
-    int ring_warps = 0;  // 0: the streaming kernel serves this matrix
+    int ring_warps = 0;  // CTAs of the ring kernel; 0: the streaming kernel serves this matrix
+    abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
     // staging for abhsf_spmv_host
     abhsf::dbuf<double> x_stage, y_stage;
 

@@ -6,40 +6,49 @@
 // columns ascending, onto y[row], each product rounded before its add.  This
 // kernel keeps that order and so returns y bitwise equal to the reference's.
 //
-// One warp per CTA.  At build time the non-empty block rows are dealt to the
-// warps (longest processing time first, by the bytes each block row moves)
-// and every warp gets its tiles as a list of 32-byte descriptors, in block-row
-// order.  The warp streams its tiles through a private ring in shared memory:
-// for each tile, asynchronous copies (cp.async) bring the x segment, the index
-// payload, the values and -- for the first tile of a block row -- the y
-// segment into one ring slot, several tiles ahead of the one being summed, so
-// that HBM latency is covered without holding data in registers.  Waits are
-// cp.async.wait_group: the hardware's own completion, never a spin.
+// A CTA is s / 32 warps; warp w owns rows 32 w .. 32 w + 31 of every tile.  At
+// build time the non-empty block rows are dealt to the CTAs (longest
+// processing time first, by the bytes each block row moves) and every CTA gets
+// its tiles as a list of 32-byte descriptors, in block-row order.  The CTA
+// streams its tiles through a ring in shared memory, several tiles ahead of
+// the one being summed: one thread issues a bulk copy (cp.async.bulk) each for
+// the tile's index payload and its values, the threads copy the x segment and
+// -- for the first tile of a block row -- the y segment with 8-byte cp.async,
+// and all of it completes on the queue slot's mbarrier.  Every wait on an
+// mbarrier is bounded: a wait that runs out sets ABHSF_DEVSTAT_WAIT_TIMEOUT in
+// the matrix's status word, the CTA waits (again bounded) for the copies it
+// still has in flight, and returns.
 //
-// Summing a bitmap tile, lane l owns rows l and l + 32: it walks its rows'
-// bits in column order and adds v * x onto the row's accumulator, where the
-// value sits at the row's first value (a warp scan of the rows' popcounts)
-// plus the set bits before it, and x[c] is a broadcast read of the staged x
-// segment.  A dense tile is summed the same way with the lanes skewed by one
-// column each, so that the row-major values do not meet in one bank; its
-// stored zeros are skipped (an exact identity for the sum).  COO and CSR
-// tiles go 32 elements at a time: each lane forms one product, and the first
-// lane of each row segment adds the segment onto the row in element order.
+// Summing a bitmap tile, a lane owns one row: it walks the row's bits in
+// column order and adds v * x onto the row's accumulator, where the value sits
+// at the row's first value (a warp scan of the rows' popcounts) plus the set
+// bits before it, and x[c] is a broadcast read of the staged x segment.  A
+// dense tile is summed the same way with the lanes skewed by one column each,
+// so that the row-major values do not meet in one bank; its stored zeros are
+// skipped (an exact identity for the sum).  COO and CSR tiles go 32 elements
+// at a time: each lane forms one product, and the first lane of each row
+// segment adds the segment onto the row in element order.
 #include <algorithm>
 #include <queue>
 #include <vector>
 
+#include "abhsf/abhsf_test.h"
 #include "common.cuh"
 #include "internal.cuh"
 
 namespace abhsf {
 namespace {
 
-constexpr int kRingBytes = 41 * 1024 + 32;  // per warp; holds any single s = 64 tile slot
-constexpr int kMaxQ = 8;               // tiles in flight per warp (cp.async groups)
-constexpr int kCtasPerSm = 5;          // resident one-warp CTAs per SM the shared memory allows
+constexpr int kRingBytes = 41 * 1024 + 32;     // per CTA; holds any single s = 64 tile slot
+constexpr int kMaxQ = 8;                       // tiles in flight per CTA (queue slots, one mbarrier each)
+constexpr int kCtasPerSm = 5;                  // resident CTAs per SM the shared memory allows
+constexpr uint32_t kWaitPolls = 1u << 21;      // try_wait polls of at most ~1 us each
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kFirst = 1u << 30, kLast = 1u << 31, kRowMask = kFirst - 1;
+
+// test hooks (abhsf_test_set_hooks)
+int64_t g_drop_desc = -1;
+uint32_t g_spin_limit = 0;
 
 // One tile as the kernel needs it; derived from the format arrays at build time.
 struct __align__(16) ring_desc {
@@ -65,18 +74,22 @@ static_assert(kRingBytes % 16 == 0, "ring slots are 16-byte aligned");
 template <int S>
 struct ring_smem {
     alignas(16) uint8_t ring[kRingBytes];
-    ring_desc tab[64];  // descriptors of two windows of 32 tiles
-    uint32_t slot[64];  // ring offset of each window entry's slot
-    double ys[S];       // the block row's y segment
-    double buf[32];     // products of a COO / CSR chunk
+    ring_desc tab[64];               // descriptors of two windows of 32 tiles
+    unsigned long long mbar[kMaxQ];  // completion of queue slot i % kMaxQ
+    uint32_t slot[64];               // ring offset of each window entry's slot
+    double ys[S];                    // the block row's y segment
+    double buf[S / 32][32];          // each warp's products of a COO / CSR chunk
 };
 
 struct ring_args {
     tiles_view A;
-    const ring_desc* desc;  // every warp's tiles, warp after warp
-    const int64_t* wbeg;    // [warps + 1] each warp's range in desc
+    const ring_desc* desc;  // every CTA's tiles, CTA after CTA
+    const int64_t* wbeg;    // [ctas + 1] each CTA's range in desc
     const double* x;
     double* y;
+    int* status;     // ABHSF_DEVSTAT_* bits
+    int64_t drop;    // test hook: descriptor whose bulk copies are not issued (-1: none)
+    uint32_t polls;  // bound of every mbarrier wait
 };
 
 // Byte offsets of a slot's parts.  Every part is a multiple of 16 bytes.
@@ -105,64 +118,83 @@ __device__ __forceinline__ void cp8(uint32_t dst, const void* src, int src_bytes
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 
-__device__ __forceinline__ void cp16(uint32_t dst, const void* src)
+// The mbarrier sees one arrival when this thread's earlier cp.async copies land.
+__device__ __forceinline__ void cp_arrive(unsigned long long* bar)
 {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
 }
 
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <int N>
-__device__ __forceinline__ void cp_wait()
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count)
 {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
 
-// Waits until at most `newer` of this thread's copy groups are still pending.
-__device__ __forceinline__ void cp_wait_newer(int newer)
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, uint32_t bytes)
 {
-    switch (newer) {
-    case 7: cp_wait<7>(); break;
-    case 6: cp_wait<6>(); break;
-    case 5: cp_wait<5>(); break;
-    case 4: cp_wait<4>(); break;
-    case 3: cp_wait<3>(); break;
-    case 2: cp_wait<2>(); break;
-    case 1: cp_wait<1>(); break;
-    default: cp_wait<0>(); break;
-    }
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Blocking poll, suspended at most ~1 us per call.
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(1000u)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity, uint32_t limit)
+{
+    for (uint32_t it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, parity))
+            return true;
+    return false;
+}
+
+// Global -> shared bulk copy (no multicast); completion counted on bar.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
 }
 
 __device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
 
-// Queues the copies of one tile's slot at ring offset off, as one group.
+// Queues one tile's slot at ring offset `slot`; it completes on bar.  All
+// threads take part.
 template <int S>
 __device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, const slot_geo& g, uint8_t* slot,
-                                      int lane)
+                                      unsigned long long* bar, int64_t e, int tid)
 {
     const uint32_t base = smem_addr(slot);
     if (d.info & kFirst) {
         const int64_t r0 = (int64_t)(d.info & kRowMask) * S;
-#pragma unroll
-        for (int r = lane; r < S; r += 32) {
-            const bool ok = r0 + r < P.A.m;
-            cp8(base + 8 * r, ok ? P.y + r0 + r : P.y, ok ? 8 : 0);
-        }
+        const bool ok = r0 + tid < P.A.m;
+        cp8(base + 8 * tid, ok ? P.y + r0 + tid : P.y, ok ? 8 : 0);
     }
     const int64_t c0 = (int64_t)d.col * S;
-#pragma unroll
-    for (int c = lane; c < S; c += 32) {
-        const bool ok = c0 + c < P.A.n;
-        cp8(base + g.x + 8 * c, ok ? P.x + c0 + c : P.x, ok ? 8 : 0);
+    const bool ok = c0 + tid < P.A.n;
+    cp8(base + g.x + 8 * tid, ok ? P.x + c0 + tid : P.x, ok ? 8 : 0);
+    cp_arrive(bar);
+    if (tid == 0) {
+        const uint32_t pb = (uint32_t)(g.val - g.pay), vb = (uint32_t)(g.size - g.val);
+        mbar_expect_tx(bar, pb + vb);
+        if (e != P.drop) {
+            // the slot's bytes were last read through the generic proxy
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (pb)
+                bulk_g2s(base + g.pay, P.A.payload + d.io, pb, bar);
+            bulk_g2s(base + g.val, static_cast<const double*>(P.A.values) + (d.vo & ~(int64_t)1), vb, bar);
+        }
     }
-    const uint8_t* pay = P.A.payload + d.io;
-    for (int k = lane; k < (g.val - g.pay) / 16; k += 32)
-        cp16(base + g.pay + 16 * k, pay + 16 * k);
-    const double* vsrc = static_cast<const double*>(P.A.values) + (d.vo & ~(int64_t)1);
-    for (int k = lane; k < (g.size - g.val) / 16; k += 32)
-        cp16(base + g.val + 16 * k, vsrc + 2 * k);
-    cp_commit();
 }
 
 __device__ __forceinline__ int warp_inclusive_sum(int v, int lane)
@@ -176,132 +208,150 @@ __device__ __forceinline__ int warp_inclusive_sum(int v, int lane)
     return v;
 }
 
-// Bitmap tile: lane l sums rows l (+ 32).  Row r's bits are u32 words
+__device__ __forceinline__ int warp_sum(int v)
+{
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1)
+        v += __shfl_xor_sync(kFull, v, d);
+    return v;
+}
+
+// Bitmap tile, row `row` = 32 warp + lane.  Row r's bits are u32 words
 // r * W .. r * W + W - 1 (W = S / 32), bit b of word j = column 32 j + b.
 template <int S>
-__device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& g, int parity, double* ys, int lane)
+__device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& g, int parity, double* ys, int warp,
+                                           int lane)
 {
-    constexpr int R = S / 32, W = S / 32;
+    constexpr int W = S / 32;
     const double* xs = reinterpret_cast<const double*>(slot + g.x);
     const double* vs = reinterpret_cast<const double*>(slot + g.val) + parity;
-    uint32_t w[R][W];
-    int q[R];
-    double acc[R];
-    int before = 0;
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-        const int row = 32 * i + lane;
-        if (W == 2) {
-            const uint2 ww = reinterpret_cast<const uint2*>(slot + g.pay)[row];
-            w[i][0] = ww.x;
-            w[i][W - 1] = ww.y;
-        } else {
-            w[i][0] = reinterpret_cast<const uint32_t*>(slot + g.pay)[row];
+    const int row = 32 * warp + lane;
+    uint32_t w[W];
+    int cnt = 0, before = 0;
+    if (W == 2) {
+        const uint2* bm = reinterpret_cast<const uint2*>(slot + g.pay);
+        const uint2 ww = bm[row];
+        w[0] = ww.x;
+        w[W - 1] = ww.y;
+        if (warp == 1) {  // values of rows 0..31 come first
+            const uint2 u = bm[lane];
+            before = warp_sum(__popc(u.x) + __popc(u.y));
         }
-        int cnt = 0;
-#pragma unroll
-        for (int j = 0; j < W; ++j)
-            cnt += __popc(w[i][j]);
-        const int inc = warp_inclusive_sum(cnt, lane);
-        q[i] = before + inc - cnt;
-        before += __shfl_sync(kFull, inc, 31);
-        acc[i] = ys[row];
+    } else {
+        w[0] = reinterpret_cast<const uint32_t*>(slot + g.pay)[row];
     }
+#pragma unroll
+    for (int j = 0; j < W; ++j)
+        cnt += __popc(w[j]);
+    int q = before + warp_inclusive_sum(cnt, lane) - cnt;
+    double acc = ys[row];
 #pragma unroll
     for (int j = 0; j < W; ++j) {
 #pragma unroll
         for (int b = 0; b < 32; ++b) {
             const double xv = xs[32 * j + b];
-#pragma unroll
-            for (int i = 0; i < R; ++i) {
-                if ((w[i][j] >> b) & 1u) {
-                    acc[i] = fadd(acc[i], fmul(vs[q[i]], xv));
-                    ++q[i];
-                }
+            if ((w[j] >> b) & 1u) {
+                acc = fadd(acc, fmul(vs[q], xv));
+                ++q;
             }
         }
     }
-#pragma unroll
-    for (int i = 0; i < R; ++i)
-        ys[32 * i + lane] = acc[i];
+    ys[row] = acc;
 }
 
 // Dense tile: all S * S values, row-major.  Lane l runs l columns behind
 // lane 0 so that the lanes' values fall in different banks.
 template <int S>
-__device__ __forceinline__ void sum_dense(const uint8_t* slot, const slot_geo& g, int parity, double* ys, int lane)
+__device__ __forceinline__ void sum_dense(const uint8_t* slot, const slot_geo& g, int parity, double* ys, int warp,
+                                          int lane)
 {
-    constexpr int R = S / 32;
     const double* xs = reinterpret_cast<const double*>(slot + g.x);
     const double* vs = reinterpret_cast<const double*>(slot + g.val) + parity;
-    double acc[R];
-#pragma unroll
-    for (int i = 0; i < R; ++i)
-        acc[i] = ys[32 * i + lane];
+    const int row = 32 * warp + lane;
+    double acc = ys[row];
 #pragma unroll 4
     for (int k = 0; k < S + 31; ++k) {
         const int c = k - lane;
         if (c >= 0 && c < S) {
-            const double xv = xs[c];
-#pragma unroll
-            for (int i = 0; i < R; ++i) {
-                const double v = vs[(32 * i + lane) * S + c];
-                if (v != 0.0)  // stored zeros and the zero padding past n
-                    acc[i] = fadd(acc[i], fmul(v, xv));
-            }
+            const double v = vs[row * S + c];
+            if (v != 0.0)  // stored zeros and the zero padding past n
+                acc = fadd(acc, fmul(v, xs[c]));
         }
     }
-#pragma unroll
-    for (int i = 0; i < R; ++i)
-        ys[32 * i + lane] = acc[i];
+    ys[row] = acc;
 }
 
-// COO / CSR tile, 32 stored elements at a time.
+// COO / CSR tile: this warp's rows' elements, 32 at a time.
 template <int S, bool CSR>
 __device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& g, int parity, int z, double* ys,
-                                           double* buf, int lane)
+                                           double* buf, int warp, int lane)
 {
     constexpr int LG = S == 32 ? 5 : 6;
     const double* xs = reinterpret_cast<const double*>(slot + g.x);
     const double* vs = reinterpret_cast<const double*>(slot + g.val) + parity;
     const uint16_t* key16 = reinterpret_cast<const uint16_t*>(slot + g.pay);  // COO keys / CSR row ends
     const uint8_t* col8 = slot + g.pay + 2 * S;                                // CSR local columns
+    int lo = 0, hi = z;  // elements of rows 32 warp .. 32 warp + 31 (sorted by row)
+    if (S == 64) {
+        int split;  // first element of row 32 or later
+        if (CSR) {
+            split = key16[31];
+        } else if (z <= 32) {
+            split = __popc(__ballot_sync(kFull, lane < z && key16[lane] < (32u << LG)));
+        } else {
+            int a = 0, b = z;
+            while (a < b) {
+                const int mid = (a + b) >> 1;
+                if (key16[mid] < (32u << LG))
+                    a = mid + 1;
+                else
+                    b = mid;
+            }
+            split = a;
+        }
+        if (warp == 0)
+            hi = split;
+        else
+            lo = split;
+    }
 #pragma unroll 1
-    for (int base = 0; base < z; base += 32) {
+    for (int base = lo; base < hi; base += 32) {
         const int k = base + lane;
         int lr = S;  // idle lanes: no row
-        if (k < z) {
+        double p = 0.0;
+        if (k < hi) {
             int lc;
             if (CSR) {
                 lc = col8[k];
-                int lo = 0, hi = S;  // first r with row_end[r] > k
+                int a = 0, b = S;  // first r with row_end[r] > k
 #pragma unroll
                 for (int step = 0; step <= LG; ++step) {
-                    if (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
+                    if (a < b) {
+                        const int mid = (a + b) >> 1;
                         if ((int)key16[mid] > k)
-                            hi = mid;
+                            b = mid;
                         else
-                            lo = mid + 1;
+                            a = mid + 1;
                     }
                 }
-                lr = lo;
+                lr = a;
             } else {
                 const uint32_t key = key16[k];
                 lr = (int)(key >> LG);
                 lc = (int)(key & (S - 1));
             }
-            buf[lane] = fmul(vs[k], xs[lc]);
+            p = fmul(vs[k], xs[lc]);
+            buf[lane] = p;
         }
         const int plr = __shfl_up_sync(kFull, lr, 1);
-        const bool head = k < z && (lane == 0 || plr != lr);
+        const bool head = k < hi && (lane == 0 || plr != lr);
         const unsigned heads = __ballot_sync(kFull, head);
         __syncwarp();
         if (head) {
             const unsigned later = heads & ~((2u << lane) - 1u);  // heads after this lane (lane 31: none)
-            const int end = later ? __ffs(later) - 1 : min(z - base, 32);
-            double acc = ys[lr];
-            for (int e = lane; e < end; ++e)
+            const int end = later ? __ffs(later) - 1 : min(hi - base, 32);
+            double acc = fadd(ys[lr], p);
+            for (int e = lane + 1; e < end; ++e)
                 acc = fadd(acc, buf[e]);
             ys[lr] = acc;
         }
@@ -311,62 +361,68 @@ __device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& 
 
 template <int S>
 __device__ __forceinline__ void sum_tile(const ring_args& P, const ring_desc& d, const uint8_t* slot,
-                                         ring_smem<S>& sm, int lane)
+                                         ring_smem<S>& sm, int warp, int lane)
 {
     const slot_geo g = geometry<S>(d);
     const int parity = (int)(d.vo & 1);
-    const int64_t r0 = (int64_t)(d.info & kRowMask) * S;
+    const int row = 32 * warp + lane;
     if (d.info & kFirst) {
-        const double* ysrc = reinterpret_cast<const double*>(slot);
-#pragma unroll
-        for (int r = lane; r < S; r += 32)
-            sm.ys[r] = ysrc[r];
+        sm.ys[row] = reinterpret_cast<const double*>(slot)[row];
         __syncwarp();
     }
     switch (d.pb_sch >> 24) {
-    case ABHSF_SCHEME_BITMAP: sum_bitmap<S>(slot, g, parity, sm.ys, lane); break;
-    case ABHSF_SCHEME_DENSE: sum_dense<S>(slot, g, parity, sm.ys, lane); break;
-    case ABHSF_SCHEME_CSR: sum_stream<S, true>(slot, g, parity, (int)d.nv, sm.ys, sm.buf, lane); break;
-    default: sum_stream<S, false>(slot, g, parity, (int)d.nv, sm.ys, sm.buf, lane); break;
+    case ABHSF_SCHEME_BITMAP: sum_bitmap<S>(slot, g, parity, sm.ys, warp, lane); break;
+    case ABHSF_SCHEME_DENSE: sum_dense<S>(slot, g, parity, sm.ys, warp, lane); break;
+    case ABHSF_SCHEME_CSR: sum_stream<S, true>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
+    default: sum_stream<S, false>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
     }
     if (d.info & kLast) {
         __syncwarp();
-#pragma unroll
-        for (int r = lane; r < S; r += 32)
-            if (r0 + r < P.A.m)
-                P.y[r0 + r] = sm.ys[r];
+        const int64_t r = (int64_t)(d.info & kRowMask) * S + row;
+        if (r < P.A.m)
+            P.y[r] = sm.ys[row];
     }
 }
 
 template <int S>
-__global__ void __launch_bounds__(32, kCtasPerSm) k_spmv_f64_ring(ring_args P)
+__global__ void __launch_bounds__(S, kCtasPerSm) k_spmv_f64_ring(ring_args P)
 {
     __shared__ ring_smem<S> sm;
-    const int lane = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t eb = P.wbeg[blockIdx.x];
     const int n = (int)(P.wbeg[blockIdx.x + 1] - eb);
     const ring_desc* D = P.desc + eb;
-    // descriptors: window 0 into the table, window 1 into registers
+    if (tid == 0) {
+        for (int b = 0; b < kMaxQ; ++b)
+            mbar_init(&sm.mbar[b], S + 1);  // S threads' cp.async arrivals + the expect_tx arrival
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // descriptors: window 0 into the table, window 1 into warp 0's registers
     ring_desc nd{};
-    if (lane < n)
-        sm.tab[lane] = D[lane];
-    if (32 + lane < n)
-        nd = D[32 + lane];
-    __syncwarp();
-    int win = 1;                              // next window to move into the table
+    if (warp == 0) {
+        if (lane < n)
+            sm.tab[lane] = D[lane];
+        if (32 + lane < n)
+            nd = D[32 + lane];
+    }
+    __syncthreads();
+    int win = 1;                               // next window to move into the table
     int iss = 0, con = 0, head = 0, tail = 0;  // tiles issued / summed; ring in use: [tail, head), maybe wrapped
+    bool failed = false;
 #pragma unroll 1
     while (con < n) {
 #pragma unroll 1
         while (iss < n && iss - con < kMaxQ) {
             if (iss == 32 * win) {
                 // window win-2, the table half being replaced, is fully summed (con > iss - kMaxQ)
-                if (iss + lane < n)
-                    sm.tab[(iss + lane) & 63] = nd;
-                if (iss + 32 + lane < n)
-                    nd = D[iss + 32 + lane];
+                if (warp == 0) {
+                    if (iss + lane < n)
+                        sm.tab[(iss + lane) & 63] = nd;
+                    if (iss + 32 + lane < n)
+                        nd = D[iss + 32 + lane];
+                }
                 ++win;
-                __syncwarp();
+                __syncthreads();
             }
             const ring_desc d = sm.tab[iss & 63];
             const slot_geo g = geometry<S>(d);
@@ -379,23 +435,35 @@ __global__ void __launch_bounds__(32, kCtasPerSm) k_spmv_f64_ring(ring_args P)
                 off = head + g.size <= tail ? head : -1;
             if (off < 0)
                 break;  // no room until the oldest tile is summed
-            issue<S>(P, d, g, sm.ring + off, lane);
-            if (lane == 0)
+            issue<S>(P, d, g, sm.ring + off, &sm.mbar[iss % kMaxQ], eb + iss, tid);
+            if (tid == 0)
                 sm.slot[iss & 63] = (uint32_t)off;
             if (iss == con)
                 tail = 0;
             head = off + g.size;
             ++iss;
         }
-        cp_wait_newer(iss - con - 1);
-        __syncwarp();
-        sum_tile<S>(P, sm.tab[con & 63], sm.ring + sm.slot[con & 63], sm, lane);
-        __syncwarp();
+        const bool ok = mbar_wait(&sm.mbar[con % kMaxQ], (uint32_t)(con / kMaxQ) & 1u, P.polls);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        sum_tile<S>(P, sm.tab[con & 63], sm.ring + sm.slot[con & 63], sm, warp, lane);
+        __syncthreads();
         ++con;
         if (con == iss)
             head = tail = 0;
         else
             tail = (int)sm.slot[con & 63];
+    }
+    if (failed) {
+        // leave no copy in flight into this CTA's shared memory
+        if (tid == 0)
+            atomicOr(P.status, ABHSF_DEVSTAT_WAIT_TIMEOUT);
+        for (int i = con; i < iss; ++i)
+            mbar_wait(&sm.mbar[i % kMaxQ], (uint32_t)(i / kMaxQ) & 1u, P.polls);
+        cp_wait_all();
+        __syncthreads();
     }
 }
 
@@ -435,8 +503,9 @@ __global__ void k_ring_fill(int64_t nitems, const uint32_t* __restrict__ rows, c
 template <int S>
 void launch_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
-    ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()), a.ring_wbeg.get(), x, y};
-    k_spmv_f64_ring<S><<<(unsigned)a.ring_warps, 32, 0, st>>>(P);
+    ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()), a.ring_wbeg.get(), x, y,
+                a.dev_status.get(), g_drop_desc, g_spin_limit ? g_spin_limit : kWaitPolls};
+    k_spmv_f64_ring<S><<<(unsigned)a.ring_warps, S, 0, st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }
 
@@ -444,7 +513,7 @@ template <int S>
 int ring_ctas_per_sm()
 {
     int nb = 0;
-    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S>, 32, 0));
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S>, S, 0));
     return std::max(nb, 1);
 }
 
@@ -460,7 +529,7 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const int per_sm = a.s == 32 ? ring_ctas_per_sm<32>() : ring_ctas_per_sm<64>();
     const int64_t nr = a.tree_nrows;
-    const int64_t warps = std::min<int64_t>((int64_t)nsm * per_sm, nr);
+    const int64_t ctas = std::min<int64_t>((int64_t)nsm * per_sm, nr);
 
     dbuf<uint64_t> w_d(nr);
     dbuf<uint32_t> n_d(nr);
@@ -474,16 +543,16 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     ABHSF_CUDA(cudaMemcpyAsync(ntiles.data(), n_d.get(), nr * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     ABHSF_CUDA(cudaStreamSynchronize(st));
 
-    // longest processing time first: heaviest block row to the least loaded warp
+    // longest processing time first: heaviest block row to the least loaded CTA
     std::vector<int64_t> order(nr);
     for (int64_t k = 0; k < nr; ++k)
         order[k] = k;
     std::stable_sort(order.begin(), order.end(), [&](int64_t p, int64_t q) { return wt[p] > wt[q]; });
     using load_t = std::pair<uint64_t, int64_t>;
     std::priority_queue<load_t, std::vector<load_t>, std::greater<load_t>> heap;
-    for (int64_t w = 0; w < warps; ++w)
-        heap.push({0, w});
-    std::vector<std::vector<int64_t>> items(warps);
+    for (int64_t c = 0; c < ctas; ++c)
+        heap.push({0, c});
+    std::vector<std::vector<int64_t>> items(ctas);
     for (int64_t k : order) {
         load_t top = heap.top();
         heap.pop();
@@ -491,38 +560,38 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
         heap.push({top.first + wt[k], top.second});
     }
     std::vector<uint32_t> item_rows;
-    std::vector<int64_t> item_base, wbeg(warps + 1, 0);
+    std::vector<int64_t> item_base, wbeg(ctas + 1, 0);
     item_rows.reserve(nr);
     item_base.reserve(nr);
     int64_t tiles = 0;
-    for (int64_t w = 0; w < warps; ++w) {
-        std::sort(items[w].begin(), items[w].end(), [&](int64_t p, int64_t q) { return rows[p] < rows[q]; });
-        wbeg[w] = tiles;
-        for (int64_t k : items[w]) {
+    for (int64_t c = 0; c < ctas; ++c) {
+        std::sort(items[c].begin(), items[c].end(), [&](int64_t p, int64_t q) { return rows[p] < rows[q]; });
+        wbeg[c] = tiles;
+        for (int64_t k : items[c]) {
             item_rows.push_back(rows[k]);
             item_base.push_back(tiles);
             tiles += ntiles[k];
         }
-        if (tiles - wbeg[w] > INT32_MAX)
-            return;  // too many tiles for one warp's counters: the streaming kernel serves this matrix
+        if (tiles - wbeg[c] > INT32_MAX)
+            return;  // too many tiles for one CTA's counters: the streaming kernel serves this matrix
     }
-    wbeg[warps] = tiles;
+    wbeg[ctas] = tiles;
     if (tiles != a.T)
         fail(ABHSF_ERROR_CUDA, "reference-order SpMV schedule does not cover every tile");
 
     dbuf<uint32_t> rows_d(nr);
     dbuf<int64_t> base_d(nr);
     a.ring_desc.alloc(a.T * (int64_t)sizeof(ring_desc));
-    a.ring_wbeg.alloc(warps + 1);
+    a.ring_wbeg.alloc(ctas + 1);
     ABHSF_CUDA(cudaMemcpyAsync(rows_d.get(), item_rows.data(), nr * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     ABHSF_CUDA(cudaMemcpyAsync(base_d.get(), item_base.data(), nr * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-    ABHSF_CUDA(cudaMemcpyAsync(a.ring_wbeg.get(), wbeg.data(), (warps + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+    ABHSF_CUDA(cudaMemcpyAsync(a.ring_wbeg.get(), wbeg.data(), (ctas + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
                                st));
     k_ring_fill<<<g, 256, 0, st>>>(nr, rows_d.get(), base_d.get(), a.view(),
                                    reinterpret_cast<ring_desc*>(a.ring_desc.get()));
     ABHSF_CUDA(cudaGetLastError());
     ABHSF_CUDA(cudaStreamSynchronize(st));
-    a.ring_warps = (int)warps;
+    a.ring_warps = (int)ctas;
 }
 
 bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
@@ -537,3 +606,9 @@ bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream
 }
 
 }  // namespace abhsf
+
+extern "C" void abhsf_test_set_hooks(int64_t drop_desc, uint32_t spin_limit)
+{
+    abhsf::g_drop_desc = drop_desc < 0 ? -1 : drop_desc;
+    abhsf::g_spin_limit = spin_limit;
+}

@@ -161,6 +161,14 @@ class AbhsfMatrix:
         self._check_open()
         return int(self._h.value)
 
+    def device_status(self, clear: bool = False, stream=None) -> int:
+        """ABHSF_DEVSTAT_* bits raised by kernels on this matrix (0 = none);
+        waits for the stream."""
+        self._check_open()
+        v = C.c_int32()
+        capi.check(capi.lib.abhsf_device_status(self._h, _stream_ptr(stream), int(clear), C.byref(v)))
+        return int(v.value)
+
     # ------------------------------------------------------------------ introspection
     def stats(self) -> dict:
         self._check_open()

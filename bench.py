@@ -272,6 +272,9 @@ def run_ours(args):
     peak, peak_src = hbm_peak()
     achieved = B / (t_mean * 1e-3) / 1e9
     cpu = None
+    status = A.device_status()
+    if status:
+        raise RuntimeError(f"SpMV kernel reported device status {status}")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_run(c, B, max_seconds=20.0, max_iters=40)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -89,6 +89,9 @@ typedef enum abhsf_sum_order {
     ABHSF_SUM_TREE = 1
 } abhsf_sum_order;
 
+/* Bits of the per-matrix device status word (abhsf_device_status). */
+#define ABHSF_DEVSTAT_WAIT_TIMEOUT 1 /* a bounded copy wait gave up; that SpMV's y is incomplete */
+
 /* include/abhsf/utils/matrix_properties.h:8-14 */
 typedef enum abhsf_matrix_type {
     ABHSF_MATRIX_BINARY = 0,
@@ -199,6 +202,12 @@ ABHSF_API abhsf_status abhsf_mmf_line(int64_t m, int64_t n, int64_t nnz, int32_t
 ABHSF_API uint64_t abhsf_block_scheme_bits(int32_t scheme, int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value);
 ABHSF_API int32_t abhsf_block_select_scheme(int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value, int32_t is_binary,
                                   int32_t allow_csr);
+
+/* Waits for the work queued on stream, then returns the matrix's device
+ * status word (ABHSF_DEVSTAT_* bits; 0 = every SpMV so far completed) and,
+ * if clear != 0, resets it.  No reference counterpart (the reference has no
+ * device code). */
+ABHSF_API abhsf_status abhsf_device_status(abhsf_matrix* a, abhsf_stream_t stream, int32_t clear, int32_t* out);
 
 /* Reason for the last non-success status returned on this thread. */
 ABHSF_API const char* abhsf_last_error_string(void);

@@ -55,6 +55,7 @@ def test_spmv_matches_oracle_all_schemes(gpu, s, forced, order):
         A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, forced_scheme=forced,
                                       sum_order=order)
         check_y(order, run_spmv(A, x, y0), coo, x, y0)
+        assert A.device_status() == 0
         A.release()
 
 
@@ -95,6 +96,28 @@ def test_spmv_config1_against_golden(gpu, order):
         # tree-ordered sums: the scaled bound holds; |dy|/|y| alone is order
         # dependent on rows that cancel (4 x_i minus four neighbours)
         assert worst_scaled <= 1e-13, worst_scaled
+
+
+def test_wait_timeout_sets_status_and_context_survives(gpu):
+    """A copy wait that runs out (the bulk copies of one tile are never
+    issued) ends the kernel with ABHSF_DEVSTAT_WAIT_TIMEOUT instead of hanging;
+    the context and the matrix stay usable."""
+    import torch
+    coo = W.random_blocky(2000, 2000, 64, 300, seed=31)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    x = W.rhs(coo.n, 1)
+    y0 = np.zeros(coo.m)
+    try:
+        capi.lib.abhsf_test_set_hooks(2, 1 << 12)
+        run_spmv(A, x, y0)
+        st = A.device_status(clear=True)
+    finally:
+        capi.lib.abhsf_test_set_hooks(-1, 0)
+    assert st & capi.DEVSTAT_WAIT_TIMEOUT
+    y = run_spmv(A, x, y0)
+    assert A.device_status() == 0
+    np.testing.assert_array_equal(y, reference_order_y(coo, x, y0))
+    torch.cuda.synchronize()
 
 
 def test_host_pointer_path_equals_device_path(gpu):
