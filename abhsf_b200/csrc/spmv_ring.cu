@@ -43,6 +43,9 @@ constexpr int kRingBytes = 41 * 1024 + 32;     // per CTA; holds any single s = 
 constexpr int kMaxQ = 8;                       // tiles in flight per CTA (queue slots, one mbarrier each)
 constexpr int kCtasPerSm = 5;                  // resident CTAs per SM the shared memory allows
 constexpr uint32_t kWaitPolls = 1u << 21;      // try_wait polls of at most ~1 us each
+#ifndef ABHSF_RING_TILE_COST
+#define ABHSF_RING_TILE_COST 32768
+#endif
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kFirst = 1u << 30, kLast = 1u << 31, kRowMask = kFirst - 1;
 
@@ -71,14 +74,22 @@ constexpr int max_slot_bytes()
 static_assert(max_slot_bytes<64>() <= kRingBytes && max_slot_bytes<32>() <= kRingBytes, "ring holds any slot");
 static_assert(kRingBytes % 16 == 0, "ring slots are 16-byte aligned");
 
+// What the producer tells the consumers about a queued tile.
+struct __align__(16) slot_rec {
+    ring_desc d;
+    uint32_t off;  // ring offset of the tile's slot
+    uint32_t pad[3];
+};
+
 template <int S>
 struct ring_smem {
     alignas(16) uint8_t ring[kRingBytes];
-    ring_desc tab[64];               // descriptors of two windows of 32 tiles
-    unsigned long long mbar[kMaxQ];  // completion of queue slot i % kMaxQ
-    uint32_t slot[64];               // ring offset of each window entry's slot
-    double ys[S];                    // the block row's y segment
-    double buf[S / 32][32];          // each warp's products of a COO / CSR chunk
+    slot_rec rec[kMaxQ];              // queue slot i % kMaxQ
+    unsigned long long full[kMaxQ];   // the slot's copies have landed
+    unsigned long long empty[kMaxQ];  // the consumers are done with the slot
+    double ys[S];                     // the block row's y segment
+    double buf[S / 32][32];           // each consumer warp's products of a COO / CSR chunk
+    int abort;                        // a wait ran out: everyone stops
 };
 
 struct ring_args {
@@ -137,6 +148,11 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, uint32_t
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // Blocking poll, suspended at most ~1 us per call.
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t parity)
 {
@@ -168,25 +184,34 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
 __device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
 
-// Queues one tile's slot at ring offset `slot`; it completes on bar.  All
-// threads take part.
+// Producer warp: queues tile d's slot at ring offset off as queue slot q; it
+// completes on full[q].
 template <int S>
-__device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, const slot_geo& g, uint8_t* slot,
-                                      unsigned long long* bar, int64_t e, int tid)
+__device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, const slot_geo& g, uint32_t off, int q,
+                                      ring_smem<S>& sm, int64_t e, int lane)
 {
-    const uint32_t base = smem_addr(slot);
+    const uint32_t base = smem_addr(sm.ring + off);
+    unsigned long long* bar = &sm.full[q];
     if (d.info & kFirst) {
         const int64_t r0 = (int64_t)(d.info & kRowMask) * S;
-        const bool ok = r0 + tid < P.A.m;
-        cp8(base + 8 * tid, ok ? P.y + r0 + tid : P.y, ok ? 8 : 0);
+#pragma unroll
+        for (int r = lane; r < S; r += 32) {
+            const bool ok = r0 + r < P.A.m;
+            cp8(base + 8 * r, ok ? P.y + r0 + r : P.y, ok ? 8 : 0);
+        }
     }
     const int64_t c0 = (int64_t)d.col * S;
-    const bool ok = c0 + tid < P.A.n;
-    cp8(base + g.x + 8 * tid, ok ? P.x + c0 + tid : P.x, ok ? 8 : 0);
+#pragma unroll
+    for (int c = lane; c < S; c += 32) {
+        const bool ok = c0 + c < P.A.n;
+        cp8(base + g.x + 8 * c, ok ? P.x + c0 + c : P.x, ok ? 8 : 0);
+    }
     cp_arrive(bar);
-    if (tid == 0) {
+    if (lane == 0) {
+        sm.rec[q].d = d;
+        sm.rec[q].off = off;
         const uint32_t pb = (uint32_t)(g.val - g.pay), vb = (uint32_t)(g.size - g.val);
-        mbar_expect_tx(bar, pb + vb);
+        mbar_expect_tx(bar, pb + vb);  // also publishes rec[q]
         if (e != P.drop) {
             // the slot's bytes were last read through the generic proxy
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -195,6 +220,17 @@ __device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, co
             bulk_g2s(base + g.val, static_cast<const double*>(P.A.values) + (d.vo & ~(int64_t)1), vb, bar);
         }
     }
+}
+
+__device__ __forceinline__ ring_desc shfl_desc(const ring_desc& v, int src)
+{
+    ring_desc r;
+    const uint32_t* a = reinterpret_cast<const uint32_t*>(&v);
+    uint32_t* b = reinterpret_cast<uint32_t*>(&r);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        b[k] = __shfl_sync(kFull, a[k], src);
+    return r;
 }
 
 __device__ __forceinline__ int warp_inclusive_sum(int v, int lane)
@@ -384,85 +420,112 @@ __device__ __forceinline__ void sum_tile(const ring_args& P, const ring_desc& d,
     }
 }
 
+// Warps 0 .. S/32 - 1 sum; warp S/32 produces.
 template <int S>
-__global__ void __launch_bounds__(S, kCtasPerSm) k_spmv_f64_ring(ring_args P)
+__global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args P)
 {
+    constexpr int NC = S / 32;  // consumer warps
     __shared__ ring_smem<S> sm;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t eb = P.wbeg[blockIdx.x];
     const int n = (int)(P.wbeg[blockIdx.x + 1] - eb);
     const ring_desc* D = P.desc + eb;
+    volatile int* abort = &sm.abort;
     if (tid == 0) {
-        for (int b = 0; b < kMaxQ; ++b)
-            mbar_init(&sm.mbar[b], S + 1);  // S threads' cp.async arrivals + the expect_tx arrival
+        for (int b = 0; b < kMaxQ; ++b) {
+            mbar_init(&sm.full[b], 32 + 1);  // the producer lanes' cp.async arrivals + the expect_tx arrival
+            mbar_init(&sm.empty[b], NC);     // one arrival per consumer warp
+        }
+        sm.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // descriptors: window 0 into the table, window 1 into warp 0's registers
-    ring_desc nd{};
-    if (warp == 0) {
-        if (lane < n)
-            sm.tab[lane] = D[lane];
-        if (32 + lane < n)
-            nd = D[32 + lane];
-    }
     __syncthreads();
-    int win = 1;                               // next window to move into the table
-    int iss = 0, con = 0, head = 0, tail = 0;  // tiles issued / summed; ring in use: [tail, head), maybe wrapped
-    bool failed = false;
+    int issued = 0;  // producer: tiles queued
+    if (warp == NC) {
+        // descriptors of tiles 32 k .. 32 k + 31, lane j holding tile 32 k + j
+        ring_desc cur{}, nxt{};
+        if (lane < n)
+            cur = D[lane];
+        if (32 + lane < n)
+            nxt = D[32 + lane];
+        int done = 0, head = 0, tail = 0;  // done: tiles the consumers released; ring in use [tail, head)
+        int my_off = 0;                    // lane q: ring offset of the tile in queue slot q
 #pragma unroll 1
-    while (con < n) {
-#pragma unroll 1
-        while (iss < n && iss - con < kMaxQ) {
-            if (iss == 32 * win) {
-                // window win-2, the table half being replaced, is fully summed (con > iss - kMaxQ)
-                if (warp == 0) {
-                    if (iss + lane < n)
-                        sm.tab[(iss + lane) & 63] = nd;
-                    if (iss + 32 + lane < n)
-                        nd = D[iss + 32 + lane];
-                }
-                ++win;
-                __syncthreads();
+        for (int i = 0; i < n; ++i) {
+            if (i > 0 && (i & 31) == 0) {
+                cur = nxt;
+                if (i + 32 + lane < n)
+                    nxt = D[i + 32 + lane];
             }
-            const ring_desc d = sm.tab[iss & 63];
+            const ring_desc d = shfl_desc(cur, i & 31);
             const slot_geo g = geometry<S>(d);
-            int off;
-            if (iss == con)
-                off = 0;
-            else if (head > tail)
-                off = head + g.size <= kRingBytes ? head : (g.size <= tail ? 0 : -1);
-            else
-                off = head + g.size <= tail ? head : -1;
-            if (off < 0)
-                break;  // no room until the oldest tile is summed
-            issue<S>(P, d, g, sm.ring + off, &sm.mbar[iss % kMaxQ], eb + iss, tid);
-            if (tid == 0)
-                sm.slot[iss & 63] = (uint32_t)off;
-            if (iss == con)
+            int off = -1;
+#pragma unroll 1
+            for (;;) {
+                if (__any_sync(kFull, *abort != 0))
+                    break;
+                if (i - done < kMaxQ) {
+                    if (i == done)
+                        off = 0;
+                    else if (head > tail)
+                        off = head + g.size <= kRingBytes ? head : (g.size <= tail ? 0 : -1);
+                    else
+                        off = head + g.size <= tail ? head : -1;
+                    if (off >= 0)
+                        break;
+                }
+                // wait until the oldest queued tile is released
+                const bool ok =
+                    __all_sync(kFull, mbar_wait(&sm.empty[done % kMaxQ], (uint32_t)(done / kMaxQ) & 1u, P.polls));
+                if (!ok)
+                    break;
+                ++done;
+                const int oldest = __shfl_sync(kFull, my_off, done % kMaxQ);
+                if (done == i)
+                    head = tail = 0;
+                else
+                    tail = oldest;
+            }
+            if (off < 0) {
+                if (lane == 0)
+                    *abort = 1;
+                break;
+            }
+            issue<S>(P, d, g, (uint32_t)off, i % kMaxQ, sm, eb + i, lane);
+            if (lane == i % kMaxQ)
+                my_off = off;
+            if (i == done)
                 tail = 0;
             head = off + g.size;
-            ++iss;
+            issued = i + 1;
         }
-        const bool ok = mbar_wait(&sm.mbar[con % kMaxQ], (uint32_t)(con / kMaxQ) & 1u, P.polls);
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-            break;
+    } else {
+#pragma unroll 1
+        for (int i = 0; i < n; ++i) {
+            const int q = i % kMaxQ;
+            const bool ok = __all_sync(kFull, mbar_wait(&sm.full[q], (uint32_t)(i / kMaxQ) & 1u, P.polls));
+            if (!ok || __any_sync(kFull, *abort != 0)) {
+                if (lane == 0)
+                    *abort = 1;
+                break;
+            }
+            const slot_rec& r = sm.rec[q];
+            sum_tile<S>(P, r.d, sm.ring + r.off, sm, warp, lane);
+            __syncwarp();
+            if (lane == 0)
+                mbar_arrive(&sm.empty[q]);
         }
-        sum_tile<S>(P, sm.tab[con & 63], sm.ring + sm.slot[con & 63], sm, warp, lane);
-        __syncthreads();
-        ++con;
-        if (con == iss)
-            head = tail = 0;
-        else
-            tail = (int)sm.slot[con & 63];
     }
-    if (failed) {
+    __syncthreads();
+    if (sm.abort) {
         // leave no copy in flight into this CTA's shared memory
         if (tid == 0)
             atomicOr(P.status, ABHSF_DEVSTAT_WAIT_TIMEOUT);
-        for (int i = con; i < iss; ++i)
-            mbar_wait(&sm.mbar[i % kMaxQ], (uint32_t)(i / kMaxQ) & 1u, P.polls);
-        cp_wait_all();
+        if (warp == NC) {
+            for (int i = max(0, issued - kMaxQ); i < issued; ++i)
+                mbar_wait(&sm.full[i % kMaxQ], (uint32_t)(i / kMaxQ) & 1u, P.polls);
+            cp_wait_all();
+        }
         __syncthreads();
     }
 }
@@ -475,7 +538,7 @@ __global__ void k_ring_weight(int64_t nr, const uint32_t* __restrict__ rows, til
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nr; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t I = rows[k], t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
         weight[k] = (uint64_t)(8 * (A.tile_val_off[t1] - A.tile_val_off[t0]) + (A.tile_idx_off[t1] - A.tile_idx_off[t0]) +
-                               (t1 - t0) * (8 * (int64_t)s + 1024) + 8 * (int64_t)s + 512);
+                               (t1 - t0) * (8 * (int64_t)s + ABHSF_RING_TILE_COST) + 8 * (int64_t)s + 512);
         ntiles[k] = (uint32_t)(t1 - t0);
     }
 }
@@ -505,7 +568,7 @@ void launch_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t
 {
     ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()), a.ring_wbeg.get(), x, y,
                 a.dev_status.get(), g_drop_desc, g_spin_limit ? g_spin_limit : kWaitPolls};
-    k_spmv_f64_ring<S><<<(unsigned)a.ring_warps, S, 0, st>>>(P);
+    k_spmv_f64_ring<S><<<(unsigned)a.ring_warps, S + 32, 0, st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }
 
@@ -513,7 +576,7 @@ template <int S>
 int ring_ctas_per_sm()
 {
     int nb = 0;
-    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S>, S, 0));
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S>, S + 32, 0));
     return std::max(nb, 1);
 }
 
