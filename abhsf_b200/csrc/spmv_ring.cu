@@ -51,14 +51,6 @@ constexpr int kMaxQ = ABHSF_RING_Q;          // tiles in flight per CTA (queue s
 // split over kCtasPerSm CTAs, less the queue and y bookkeeping
 constexpr int kRingBytes = ((233472 / kCtasPerSm - 1024 - 2560) / 16) * 16;
 constexpr uint32_t kWaitPolls = 1u << 21;      // try_wait polls of at most ~1 us each
-#ifndef ABHSF_RING_PREFETCH
-#define ABHSF_RING_PREFETCH 0
-#endif
-constexpr int kPrefetch = ABHSF_RING_PREFETCH;  // tiles between the L2 prefetch and the copy into the ring
-static_assert(kPrefetch >= 0 && kPrefetch <= 32, "the prefetched tile's descriptor is in the producer's windows");
-#ifndef ABHSF_RING_LDGSTS
-#define ABHSF_RING_LDGSTS 0
-#endif
 #ifndef ABHSF_RING_TILE_COST
 #define ABHSF_RING_TILE_COST 32768
 #endif
@@ -146,11 +138,6 @@ __device__ __forceinline__ void cp8(uint32_t dst, const void* src, int src_bytes
 }
 
 // The mbarrier sees one arrival when this thread's earlier cp.async copies land.
-__device__ __forceinline__ void cp16(uint32_t dst, const void* src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
-}
-
 __device__ __forceinline__ void cp_arrive(unsigned long long* bar)
 {
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
@@ -202,37 +189,8 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                  : "memory");
 }
 
-// L2 prefetch of a 16-byte aligned range whose size is a multiple of 16.
-__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes)
-{
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
 __device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
-
-// Producer warp: asks L2 for tile d's bytes ahead of its copy into the ring.
-template <int S>
-__device__ __forceinline__ void prefetch_tile(const ring_args& P, const ring_desc& d, int lane)
-{
-    const slot_geo g = geometry<S>(d);
-    const int64_t c0 = (int64_t)d.col * S;
-    if (lane < S / 16 && c0 + 16 * lane < P.A.n)  // x segment, one 128-byte line per lane
-        prefetch_l2(P.x + c0 + 16 * lane);
-    if (d.info & kFirst) {
-        const int64_t r0 = (int64_t)(d.info & kRowMask) * S;
-        if (lane >= 16 && lane < 16 + S / 16 && r0 + 16 * (lane - 16) < P.A.m)
-            prefetch_l2(P.y + r0 + 16 * (lane - 16));
-    }
-    if (lane == 0) {
-        const uint32_t pb = (uint32_t)(g.val - g.pay), vb = (uint32_t)(g.size - g.val);
-        if (pb)
-            bulk_prefetch_l2(P.A.payload + d.io, pb);
-        bulk_prefetch_l2(static_cast<const double*>(P.A.values) + (d.vo & ~(int64_t)1), vb);
-    }
-}
 
 // Producer warp: queues tile d's slot at ring offset off as queue slot q; it
 // completes on full[q].
@@ -255,21 +213,6 @@ __device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, co
     for (int c = lane; c < S; c += 32) {
         const bool ok = c0 + c < P.A.n;
         cp8(base + g.x + 8 * c, ok ? P.x + c0 + c : P.x, ok ? 8 : 0);
-    }
-    if (ABHSF_RING_LDGSTS) {
-        const uint8_t* pay = P.A.payload + d.io;
-        for (int k = lane; k < (g.val - g.pay) / 16; k += 32)
-            cp16(base + g.pay + 16 * k, pay + 16 * k);
-        const double* vsrc = static_cast<const double*>(P.A.values) + (d.vo & ~(int64_t)1);
-        for (int k = lane; k < (g.size - g.val) / 16; k += 32)
-            cp16(base + g.val + 16 * k, vsrc + 2 * k);
-        cp_arrive(bar);
-        if (lane == 0) {
-            sm.rec[q].d = d;
-            sm.rec[q].off = off;
-            mbar_expect_tx(bar, 0);  // the arrival that publishes rec[q]
-        }
-        return;
     }
     cp_arrive(bar);
     if (lane == 0) {
@@ -516,8 +459,6 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
             nxt = D[32 + lane];
         int done = 0, head = 0, tail = 0;  // done: tiles the consumers released; ring in use [tail, head)
         int my_off = 0;                    // lane q: ring offset of the tile in queue slot q
-        for (int j = 0; j < kPrefetch && j < n; ++j)
-            prefetch_tile<S>(P, shfl_desc(j < 32 ? cur : nxt, j & 31), lane);
 #pragma unroll 1
         for (int i = 0; i < n; ++i) {
             if (i > 0 && (i & 31) == 0) {
@@ -558,10 +499,6 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                 if (lane == 0)
                     *abort = 1;
                 break;
-            }
-            if (kPrefetch > 0 && i + kPrefetch < n) {
-                const int j = i + kPrefetch;  // in this window or the next
-                prefetch_tile<S>(P, shfl_desc((j & ~31) == (i & ~31) ? cur : nxt, j & 31), lane);
             }
             issue<S>(P, d, g, (uint32_t)off, i % kMaxQ, sm, eb + i, lane);
             if (lane == i % kMaxQ)
