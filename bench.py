@@ -35,7 +35,7 @@ UNIT = "GB/s"
 FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 256 << 20
 DEFAULT_N = 4_194_304
-KERNELS = {"reference": "k_spmv_f64_seq", "tree": "k_spmv_f64"}
+KERNELS = {"reference": "k_spmv_f64_ring", "tree": "k_spmv_f64"}
 
 
 def traffic_file(sum_order):
@@ -215,7 +215,7 @@ def run_ours(args):
     xd = torch.from_numpy(x_h).to(dev)
     yd = torch.zeros(c.m, dtype=torch.float64, device=dev)
     flush_w = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
-    flush_r = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    flush_r = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)  # summed in place, no copy
     stream = torch.cuda.current_stream()
 
     def l2_flush():
