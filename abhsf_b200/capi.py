@@ -87,6 +87,7 @@ PROTOTYPES = {
     "abhsf_build": (C.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, C.POINTER(BuildOpts), _vp, C.POINTER(_vp)]),
     "abhsf_spmv": (C.c_int, [_vp, _vp, _vp, _vp]),
     "abhsf_spmv_host": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "abhsf_spmm": (C.c_int, [_vp, _i32, _vp, _i64, _vp, _i64, _vp]),
     "abhsf_release": (C.c_int, [_vp]),
     "abhsf_stats_get": (C.c_int, [_vp, C.POINTER(Stats)]),
     "abhsf_export_host": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

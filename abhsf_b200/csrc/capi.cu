@@ -23,6 +23,34 @@ void spmv_dispatch(const abhsf_matrix& a, const double* x, double* y, cudaStream
         spmv_f64(a, x, y, st);
 }
 
+// Y += A X, k columns.  The reference order for block sizes 32 / 64 runs the
+// ring kernel with several right-hand sides per pass; otherwise each column is
+// gathered into a contiguous vector, multiplied by the SpMV kernels and
+// scattered back, so column j is bitwise the SpMV of column j in every case.
+void spmm_dispatch(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,
+                   cudaStream_t st)
+{
+    if (k == 0 || a.m == 0 || a.T == 0)
+        return;
+    if (a.sum_order == ABHSF_SUM_REFERENCE && spmm_f64_ring(a, k, X, ldx, Y, ldy, st))
+        return;
+    if (k == 1 && ldx == 1 && ldy == 1) {
+        spmv_dispatch(a, X, Y, st);
+        return;
+    }
+    dbuf<double> xc(a.n), yc(a.m);
+    for (int j = 0; j < k; ++j) {
+        ABHSF_CUDA(cudaMemcpy2DAsync(xc.get(), sizeof(double), X + j, ldx * sizeof(double), sizeof(double), a.n,
+                                     cudaMemcpyDeviceToDevice, st));
+        ABHSF_CUDA(cudaMemcpy2DAsync(yc.get(), sizeof(double), Y + j, ldy * sizeof(double), sizeof(double), a.m,
+                                     cudaMemcpyDeviceToDevice, st));
+        spmv_dispatch(a, xc.get(), yc.get(), st);
+        ABHSF_CUDA(cudaMemcpy2DAsync(Y + j, ldy * sizeof(double), yc.get(), sizeof(double), sizeof(double), a.m,
+                                     cudaMemcpyDeviceToDevice, st));
+    }
+    ABHSF_CUDA(cudaStreamSynchronize(st));  // before the column buffers are freed
+}
+
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 void clear_last_error() { g_last_error.clear(); }
 
@@ -80,6 +108,28 @@ abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double* y, abhsf
         if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 7)
             fail(ABHSF_ERROR_INVALID_VALUE, "x and y must be 8-byte aligned");
         abhsf::spmv_dispatch(*a, x, y, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+abhsf_status abhsf_spmm(const abhsf_matrix* a, int32_t k, const double* X, int64_t ldx, double* Y, int64_t ldy,
+                        abhsf_stream_t stream)
+{
+    return guarded([&] {
+        if (!a)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle is NULL");
+        if (a->value_type != ABHSF_VALUE_F64)
+            fail(ABHSF_ERROR_INVALID_VALUE, "abhsf_spmm needs a matrix stored as f64");
+        if (k < 0)
+            fail(ABHSF_ERROR_INVALID_VALUE, "k must be >= 0");
+        if (k == 0)
+            return;
+        if (ldx < k || ldy < k)
+            fail(ABHSF_ERROR_INVALID_VALUE, "ldx and ldy must be >= k");
+        if ((!X && a->n) || (!Y && a->m))
+            fail(ABHSF_ERROR_INVALID_VALUE, "X and Y must be non-NULL");
+        if ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) & 7)
+            fail(ABHSF_ERROR_INVALID_VALUE, "X and Y must be 8-byte aligned");
+        abhsf::spmm_dispatch(*a, k, X, ldx, Y, ldy, reinterpret_cast<cudaStream_t>(stream));
     });
 }
 

@@ -169,6 +169,7 @@ struct abhsf_matrix {
     // reference-order SpMV, s = 32 / 64: every CTA's tile descriptors and their ranges
     abhsf::dbuf<uint8_t> ring_desc;
     abhsf::dbuf<int64_t> ring_wbeg;
+    int ring_max_pv = 0;  // largest payload + values bytes of one tile (picks the SpMM pass width)
     int ring_warps = 0;  // CTAs of the ring kernel; 0: the streaming kernel serves this matrix
     abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
     // staging for abhsf_spmv_host

@@ -37,6 +37,10 @@ void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_
 // The same order through per-warp shared-memory rings (s = 32, 64); false
 // when the matrix has no ring schedule.
 bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+// Y += A X (k columns, row-major X and Y) through the same kernel, several
+// right-hand sides per pass; false when the matrix has no ring schedule.
+bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,
+                   cudaStream_t st);
 
 
 // abhsf_spmv's choice between the two f64 kernels (abhsf_matrix::sum_order).

@@ -1,5 +1,6 @@
-// spmv_ring.cu -- y += A x over the ABHSF format in the reference's summation
-// order, FP64, block sizes 32 and 64, sm_100a.
+// spmv_ring.cu -- y += A x and Y += A X (K right-hand sides per pass) over the
+// ABHSF format in the reference's summation order, FP64, block sizes 32 and
+// 64, sm_100a.
 //
 // The reference's CSR SpMV (csr_matrix::spmv_naive,
 // spmv/bottlenecks/spmv.cpp:58-64) adds a row's products one at a time,
@@ -28,6 +29,11 @@
 // skipped (an exact identity for the sum).  COO and CSR tiles go 32 elements
 // at a time: each lane forms one product, and the first lane of each row
 // segment adds the segment onto the row in element order.
+//
+// With K right-hand sides (X and Y row-major, leading dimensions ldx / ldy)
+// a slot holds the tile's S x K block of X (and of Y at a block row's start),
+// a lane keeps K accumulators for its row, and each of the K sums follows the
+// same order: column j of Y is bitwise what the SpMV of column j gives.
 #include <algorithm>
 #include <queue>
 #include <vector>
@@ -47,9 +53,6 @@ namespace {
 #endif
 constexpr int kCtasPerSm = ABHSF_RING_CTAS;  // resident CTAs per SM
 constexpr int kMaxQ = ABHSF_RING_Q;          // tiles in flight per CTA (queue slots, one mbarrier each)
-// per CTA: the shared memory of an SM (228 KiB, 1 KiB of it reserved per CTA)
-// split over kCtasPerSm CTAs, less the queue and y bookkeeping
-constexpr int kRingBytes = ((233472 / kCtasPerSm - 1024 - 2560) / 16) * 16;
 constexpr uint32_t kWaitPolls = 1u << 21;      // try_wait polls of at most ~1 us each
 #ifndef ABHSF_RING_TILE_COST
 #define ABHSF_RING_TILE_COST 32768
@@ -72,15 +75,32 @@ struct __align__(16) ring_desc {
 };
 static_assert(sizeof(ring_desc) == 32, "ring_desc is 32 bytes");
 
-// The largest slot: y and x segments, a COO payload of s * s keys (2 bytes
-// each), s * s values and one granule of alignment slack.
+// Bytes of a CTA's shared memory other than the ring (queue records and
+// barriers, the y block, the product buffers, the abort flag), rounded up.
+template <int S, int K>
+constexpr int ring_overhead()
+{
+    return kMaxQ * (48 + 16) + S * K * 8 + (S / 32) * 32 * 8 + 64;
+}
+
+// The ring: the shared memory of an SM (228 KiB, 1 KiB of it reserved per
+// CTA) split over kCtasPerSm CTAs, less the rest of the CTA's shared memory.
+template <int S, int K>
+constexpr int ring_bytes()
+{
+    return ((233472 / kCtasPerSm - 1024 - ring_overhead<S, K>()) / 16) * 16;
+}
+
+// The largest slot of a single-right-hand-side pass: y and x segments, a COO
+// payload of s * s keys (2 bytes each), s * s values and one granule of
+// alignment slack.  Every matrix can take that pass.
 template <int S>
 constexpr int max_slot_bytes()
 {
     return 2 * S * 8 + 2 * S * S + 8 * S * S + 16;
 }
-static_assert(max_slot_bytes<64>() <= kRingBytes && max_slot_bytes<32>() <= kRingBytes, "ring holds any slot");
-static_assert(kRingBytes % 16 == 0, "ring slots are 16-byte aligned");
+static_assert(max_slot_bytes<64>() <= ring_bytes<64, 1>() && max_slot_bytes<32>() <= ring_bytes<32, 1>(),
+              "the ring holds any single-right-hand-side slot");
 
 // What the producer tells the consumers about a queued tile.
 struct __align__(16) slot_rec {
@@ -89,13 +109,13 @@ struct __align__(16) slot_rec {
     uint32_t pad[3];
 };
 
-template <int S>
+template <int S, int K>
 struct ring_smem {
-    alignas(16) uint8_t ring[kRingBytes];
+    alignas(16) uint8_t ring[ring_bytes<S, K>()];
     slot_rec rec[kMaxQ];              // queue slot i % kMaxQ
     unsigned long long full[kMaxQ];   // the slot's copies have landed
     unsigned long long empty[kMaxQ];  // the consumers are done with the slot
-    double ys[S];                     // the block row's y segment
+    double ys[S * K];                 // the block row's y block, row-major
     double buf[S / 32][32];           // each consumer warp's products of a COO / CSR chunk
     int abort;                        // a wait ran out: everyone stops
 };
@@ -104,8 +124,9 @@ struct ring_args {
     tiles_view A;
     const ring_desc* desc;  // every CTA's tiles, CTA after CTA
     const int64_t* wbeg;    // [ctas + 1] each CTA's range in desc
-    const double* x;
-    double* y;
+    const double* x;  // X, row-major: element (i, j) at x[i * ldx + j]
+    double* y;        // Y, row-major: element (i, j) at y[i * ldy + j]
+    int64_t ldx, ldy;
     int* status;     // ABHSF_DEVSTAT_* bits
     int64_t drop;    // test hook: descriptor whose bulk copies are not issued (-1: none)
     uint32_t polls;  // bound of every mbarrier wait
@@ -116,12 +137,12 @@ struct slot_geo {
     int x, pay, val, size;
 };
 
-template <int S>
-__device__ __forceinline__ slot_geo geometry(const ring_desc& d)
+template <int S, int K>
+__host__ __device__ __forceinline__ slot_geo geometry(const ring_desc& d)
 {
     slot_geo g;
-    g.x = (d.info & kFirst) ? S * 8 : 0;  // the y segment comes first
-    g.pay = g.x + S * 8;
+    g.x = (d.info & kFirst) ? S * K * 8 : 0;  // the y block comes first
+    g.pay = g.x + S * K * 8;
     g.val = g.pay + (int)(d.pb_sch & 0xffffffu);
     // values are copied in 16-byte granules from the even element at or below vo
     const int nv2 = ((int)d.nv + (int)(d.vo & 1) + 1) & ~1;
@@ -194,25 +215,27 @@ __device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a,
 
 // Producer warp: queues tile d's slot at ring offset off as queue slot q; it
 // completes on full[q].
-template <int S>
+template <int S, int K>
 __device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, const slot_geo& g, uint32_t off, int q,
-                                      ring_smem<S>& sm, int64_t e, int lane)
+                                      ring_smem<S, K>& sm, int64_t e, int lane)
 {
     const uint32_t base = smem_addr(sm.ring + off);
     unsigned long long* bar = &sm.full[q];
     if (d.info & kFirst) {
         const int64_t r0 = (int64_t)(d.info & kRowMask) * S;
 #pragma unroll
-        for (int r = lane; r < S; r += 32) {
+        for (int k = lane; k < S * K; k += 32) {
+            const int r = k / K, j = k % K;
             const bool ok = r0 + r < P.A.m;
-            cp8(base + 8 * r, ok ? P.y + r0 + r : P.y, ok ? 8 : 0);
+            cp8(base + 8 * k, ok ? P.y + (r0 + r) * P.ldy + j : P.y, ok ? 8 : 0);
         }
     }
     const int64_t c0 = (int64_t)d.col * S;
 #pragma unroll
-    for (int c = lane; c < S; c += 32) {
+    for (int k = lane; k < S * K; k += 32) {
+        const int c = k / K, j = k % K;
         const bool ok = c0 + c < P.A.n;
-        cp8(base + g.x + 8 * c, ok ? P.x + c0 + c : P.x, ok ? 8 : 0);
+        cp8(base + g.x + 8 * k, ok ? P.x + (c0 + c) * P.ldx + j : P.x, ok ? 8 : 0);
     }
     cp_arrive(bar);
     if (lane == 0) {
@@ -262,7 +285,7 @@ __device__ __forceinline__ int warp_sum(int v)
 
 // Bitmap tile, row `row` = 32 warp + lane.  Row r's bits are u32 words
 // r * W .. r * W + W - 1 (W = S / 32), bit b of word j = column 32 j + b.
-template <int S>
+template <int S, int K>
 __device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& g, int parity, double* ys, int warp,
                                            int lane)
 {
@@ -288,45 +311,64 @@ __device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& 
     for (int j = 0; j < W; ++j)
         cnt += __popc(w[j]);
     int q = before + warp_inclusive_sum(cnt, lane) - cnt;
-    double acc = ys[row];
+    double acc[K];
+#pragma unroll
+    for (int h = 0; h < K; ++h)
+        acc[h] = ys[row * K + h];
 #pragma unroll
     for (int j = 0; j < W; ++j) {
 #pragma unroll
         for (int b = 0; b < 32; ++b) {
-            const double xv = xs[32 * j + b];
+            double xv[K];
+#pragma unroll
+            for (int h = 0; h < K; ++h)
+                xv[h] = xs[(32 * j + b) * K + h];
             if ((w[j] >> b) & 1u) {
-                acc = fadd(acc, fmul(vs[q], xv));
+                const double v = vs[q];
+#pragma unroll
+                for (int h = 0; h < K; ++h)
+                    acc[h] = fadd(acc[h], fmul(v, xv[h]));
                 ++q;
             }
         }
     }
-    ys[row] = acc;
+#pragma unroll
+    for (int h = 0; h < K; ++h)
+        ys[row * K + h] = acc[h];
 }
 
 // Dense tile: all S * S values, row-major.  Lane l runs l columns behind
 // lane 0 so that the lanes' values fall in different banks.
-template <int S>
+template <int S, int K>
 __device__ __forceinline__ void sum_dense(const uint8_t* slot, const slot_geo& g, int parity, double* ys, int warp,
                                           int lane)
 {
     const double* xs = reinterpret_cast<const double*>(slot + g.x);
     const double* vs = reinterpret_cast<const double*>(slot + g.val) + parity;
     const int row = 32 * warp + lane;
-    double acc = ys[row];
+    double acc[K];
+#pragma unroll
+    for (int h = 0; h < K; ++h)
+        acc[h] = ys[row * K + h];
 #pragma unroll 4
     for (int k = 0; k < S + 31; ++k) {
         const int c = k - lane;
         if (c >= 0 && c < S) {
             const double v = vs[row * S + c];
-            if (v != 0.0)  // stored zeros and the zero padding past n
-                acc = fadd(acc, fmul(v, xs[c]));
+            if (v != 0.0) {  // stored zeros and the zero padding past n
+#pragma unroll
+                for (int h = 0; h < K; ++h)
+                    acc[h] = fadd(acc[h], fmul(v, xs[c * K + h]));
+            }
         }
     }
-    ys[row] = acc;
+#pragma unroll
+    for (int h = 0; h < K; ++h)
+        ys[row * K + h] = acc[h];
 }
 
 // COO / CSR tile: this warp's rows' elements, 32 at a time.
-template <int S, bool CSR>
+template <int S, int K, bool CSR>
 __device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& g, int parity, int z, double* ys,
                                            double* buf, int warp, int lane)
 {
@@ -362,9 +404,9 @@ __device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& 
     for (int base = lo; base < hi; base += 32) {
         const int k = base + lane;
         int lr = S;  // idle lanes: no row
-        double p = 0.0;
+        int lc = 0;
+        double v = 0.0;
         if (k < hi) {
-            int lc;
             if (CSR) {
                 lc = col8[k];
                 int a = 0, b = S;  // first r with row_end[r] > k
@@ -384,57 +426,67 @@ __device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& 
                 lr = (int)(key >> LG);
                 lc = (int)(key & (S - 1));
             }
-            p = fmul(vs[k], xs[lc]);
-            buf[lane] = p;
+            v = vs[k];
         }
         const int plr = __shfl_up_sync(kFull, lr, 1);
         const bool head = k < hi && (lane == 0 || plr != lr);
         const unsigned heads = __ballot_sync(kFull, head);
-        __syncwarp();
-        if (head) {
-            const unsigned later = heads & ~((2u << lane) - 1u);  // heads after this lane (lane 31: none)
-            const int end = later ? __ffs(later) - 1 : min(hi - base, 32);
-            double acc = fadd(ys[lr], p);
-            for (int e = lane + 1; e < end; ++e)
-                acc = fadd(acc, buf[e]);
-            ys[lr] = acc;
+        const unsigned later = heads & ~((2u << lane) - 1u);  // heads after this lane (lane 31: none)
+        const int end = later ? __ffs(later) - 1 : min(hi - base, 32);
+#pragma unroll 1
+        for (int h = 0; h < K; ++h) {
+            const double p = k < hi ? fmul(v, xs[lc * K + h]) : 0.0;
+            buf[lane] = p;
+            __syncwarp();
+            if (head) {
+                double acc = fadd(ys[lr * K + h], p);
+                for (int e = lane + 1; e < end; ++e)
+                    acc = fadd(acc, buf[e]);
+                ys[lr * K + h] = acc;
+            }
+            __syncwarp();
         }
-        __syncwarp();
     }
 }
 
-template <int S>
+template <int S, int K>
 __device__ __forceinline__ void sum_tile(const ring_args& P, const ring_desc& d, const uint8_t* slot,
-                                         ring_smem<S>& sm, int warp, int lane)
+                                         ring_smem<S, K>& sm, int warp, int lane)
 {
-    const slot_geo g = geometry<S>(d);
+    const slot_geo g = geometry<S, K>(d);
     const int parity = (int)(d.vo & 1);
     const int row = 32 * warp + lane;
     if (d.info & kFirst) {
-        sm.ys[row] = reinterpret_cast<const double*>(slot)[row];
+#pragma unroll
+        for (int h = 0; h < K; ++h)
+            sm.ys[row * K + h] = reinterpret_cast<const double*>(slot)[row * K + h];
         __syncwarp();
     }
     switch (d.pb_sch >> 24) {
-    case ABHSF_SCHEME_BITMAP: sum_bitmap<S>(slot, g, parity, sm.ys, warp, lane); break;
-    case ABHSF_SCHEME_DENSE: sum_dense<S>(slot, g, parity, sm.ys, warp, lane); break;
-    case ABHSF_SCHEME_CSR: sum_stream<S, true>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
-    default: sum_stream<S, false>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
+    case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K>(slot, g, parity, sm.ys, warp, lane); break;
+    case ABHSF_SCHEME_DENSE: sum_dense<S, K>(slot, g, parity, sm.ys, warp, lane); break;
+    case ABHSF_SCHEME_CSR: sum_stream<S, K, true>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
+    default: sum_stream<S, K, false>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
     }
     if (d.info & kLast) {
         __syncwarp();
         const int64_t r = (int64_t)(d.info & kRowMask) * S + row;
-        if (r < P.A.m)
-            P.y[r] = sm.ys[row];
+        if (r < P.A.m) {
+#pragma unroll
+            for (int h = 0; h < K; ++h)
+                P.y[r * P.ldy + h] = sm.ys[row * K + h];
+        }
     }
 }
 
 // Warps 0 .. S/32 - 1 sum; warp S/32 produces.
-template <int S>
+template <int S, int K>
 __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args P)
 {
     constexpr int NC = S / 32;  // consumer warps
+    constexpr int kRingBytes = ring_bytes<S, K>();
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    ring_smem<S>& sm = *reinterpret_cast<ring_smem<S>*>(smem_raw);
+    ring_smem<S, K>& sm = *reinterpret_cast<ring_smem<S, K>*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t eb = P.wbeg[blockIdx.x];
     const int n = (int)(P.wbeg[blockIdx.x + 1] - eb);
@@ -467,7 +519,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                     nxt = D[i + 32 + lane];
             }
             const ring_desc d = shfl_desc(cur, i & 31);
-            const slot_geo g = geometry<S>(d);
+            const slot_geo g = geometry<S, K>(d);
             int off = -1;
 #pragma unroll 1
             for (;;) {
@@ -500,7 +552,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                     *abort = 1;
                 break;
             }
-            issue<S>(P, d, g, (uint32_t)off, i % kMaxQ, sm, eb + i, lane);
+            issue<S, K>(P, d, g, (uint32_t)off, i % kMaxQ, sm, eb + i, lane);
             if (lane == i % kMaxQ)
                 my_off = off;
             if (i == done)
@@ -519,7 +571,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                 break;
             }
             const slot_rec& r = sm.rec[q];
-            sum_tile<S>(P, r.d, sm.ring + r.off, sm, warp, lane);
+            sum_tile<S, K>(P, r.d, sm.ring + r.off, sm, warp, lane);
             __syncwarp();
             if (lane == 0)
                 mbar_arrive(&sm.empty[q]);
@@ -572,23 +624,75 @@ __global__ void k_ring_fill(int64_t nitems, const uint32_t* __restrict__ rows, c
     }
 }
 
-template <int S>
-void launch_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+// Largest payload + values part of any tile's slot (bytes).
+__global__ void k_ring_max_pv(int64_t T, tiles_view A, unsigned int* __restrict__ out)
 {
-    ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()), a.ring_wbeg.get(), x, y,
+    unsigned int best = 0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t vo = A.tile_val_off[t], nv = A.tile_val_off[t + 1] - vo;
+        const int64_t pv = (A.tile_idx_off[t + 1] - A.tile_idx_off[t]) + ((nv + (vo & 1) + 1) & ~(int64_t)1) * 8;
+        best = max(best, (unsigned int)pv);
+    }
+    atomicMax(out, best);
+}
+
+// One pass: K right-hand sides, X and Y starting at their first column.
+template <int S, int K>
+void launch_ring(const abhsf_matrix& a, const double* x, int64_t ldx, double* y, int64_t ldy, cudaStream_t st)
+{
+    static_assert(sizeof(ring_smem<S, K>) + 1024 <= 233472 / kCtasPerSm, "kCtasPerSm CTAs fit an SM");
+    ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()), a.ring_wbeg.get(), x, y, ldx, ldy,
                 a.dev_status.get(), g_drop_desc, g_spin_limit ? g_spin_limit : kWaitPolls};
-    k_spmv_f64_ring<S><<<(unsigned)a.ring_warps, S + 32, sizeof(ring_smem<S>), st>>>(P);
+    k_spmv_f64_ring<S, K><<<(unsigned)a.ring_warps, S + 32, sizeof(ring_smem<S, K>), st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }
 
-template <int S>
+template <int S, int K>
 int ring_ctas_per_sm()
 {
     int nb = 0;
-    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(ring_smem<S>)));
-    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S>, S + 32, sizeof(ring_smem<S>)));
+    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(ring_smem<S, K>)));
+    ABHSF_CUDA(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S, K>, S + 32, sizeof(ring_smem<S, K>)));
     return std::max(nb, 1);
+}
+
+// Does a pass of K right-hand sides fit every tile of this matrix in the ring?
+template <int S, int K>
+bool ring_fits(const abhsf_matrix& a)
+{
+    return 2 * S * K * 8 + (int64_t)a.ring_max_pv <= ring_bytes<S, K>();
+}
+
+// Y += A X over columns [0, k) in passes of the largest K that fits.
+template <int S>
+void spmm_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy, cudaStream_t st)
+{
+    for (int j = 0; j < k;) {
+        const int left = k - j;
+        if (left >= 8 && ring_fits<S, 8>(a)) {
+            launch_ring<S, 8>(a, X + j, ldx, Y + j, ldy, st);
+            j += 8;
+        } else if (left >= 4 && ring_fits<S, 4>(a)) {
+            launch_ring<S, 4>(a, X + j, ldx, Y + j, ldy, st);
+            j += 4;
+        } else if (left >= 2 && ring_fits<S, 2>(a)) {
+            launch_ring<S, 2>(a, X + j, ldx, Y + j, ldy, st);
+            j += 2;
+        } else {
+            launch_ring<S, 1>(a, X + j, ldx, Y + j, ldy, st);
+            j += 1;
+        }
+    }
+}
+
+template <int S>
+void ring_set_up_all()
+{
+    ring_ctas_per_sm<S, 2>();
+    ring_ctas_per_sm<S, 4>();
+    ring_ctas_per_sm<S, 8>();
 }
 
 }  // namespace
@@ -601,7 +705,11 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     int dev = 0, nsm = 0;
     ABHSF_CUDA(cudaGetDevice(&dev));
     ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const int per_sm = a.s == 32 ? ring_ctas_per_sm<32>() : ring_ctas_per_sm<64>();
+    const int per_sm = a.s == 32 ? ring_ctas_per_sm<32, 1>() : ring_ctas_per_sm<64, 1>();
+    if (a.s == 32)
+        ring_set_up_all<32>();
+    else
+        ring_set_up_all<64>();
     const int64_t nr = a.tree_nrows;
     const int64_t ctas = std::min<int64_t>((int64_t)nsm * per_sm, nr);
 
@@ -664,7 +772,15 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     k_ring_fill<<<g, 256, 0, st>>>(nr, rows_d.get(), base_d.get(), a.view(),
                                    reinterpret_cast<ring_desc*>(a.ring_desc.get()));
     ABHSF_CUDA(cudaGetLastError());
+    dbuf<unsigned int> max_pv(1);
+    ABHSF_CUDA(cudaMemsetAsync(max_pv.get(), 0, sizeof(unsigned int), st));
+    const unsigned gt = (unsigned)std::max<int64_t>(1, std::min<int64_t>((a.T + 255) / 256, 4096));
+    k_ring_max_pv<<<gt, 256, 0, st>>>(a.T, a.view(), max_pv.get());
+    ABHSF_CUDA(cudaGetLastError());
+    unsigned int mpv = 0;
+    ABHSF_CUDA(cudaMemcpyAsync(&mpv, max_pv.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
     ABHSF_CUDA(cudaStreamSynchronize(st));
+    a.ring_max_pv = (int)mpv;
     a.ring_warps = (int)ctas;
 }
 
@@ -673,9 +789,21 @@ bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream
     if (a.ring_warps == 0)
         return false;
     if (a.s == 32)
-        launch_ring<32>(a, x, y, st);
+        launch_ring<32, 1>(a, x, 1, y, 1, st);
     else
-        launch_ring<64>(a, x, y, st);
+        launch_ring<64, 1>(a, x, 1, y, 1, st);
+    return true;
+}
+
+bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,
+                   cudaStream_t st)
+{
+    if (a.ring_warps == 0)
+        return false;
+    if (a.s == 32)
+        spmm_ring<32>(a, k, X, ldx, Y, ldy, st);
+    else
+        spmm_ring<64>(a, k, X, ldx, Y, ldy, st);
     return true;
 }
 

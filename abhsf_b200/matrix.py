@@ -126,6 +126,22 @@ class AbhsfMatrix:
             self._check_vec(x, y, np.float64, x.size, y.size, x.flags.c_contiguous and y.flags.c_contiguous)
             capi.check(capi.lib.abhsf_spmv_host(self._h, x.ctypes.data, y.ctypes.data, _stream_ptr(stream)))
 
+    def spmm(self, X, Y, stream=None) -> None:
+        """Y += A X for 2-D CUDA float64 tensors X (n x k) and Y (m x k) whose
+        rows are contiguous (stride 1 along k), asynchronous on the stream."""
+        self._check_open()
+        if not (_is_cuda(X) and _is_cuda(Y)):
+            raise capi.InvalidValue(capi.INVALID_VALUE, "X and Y must be CUDA tensors")
+        if X.dim() != 2 or Y.dim() != 2 or X.shape[0] != self.n or Y.shape[0] != self.m or X.shape[1] != Y.shape[1]:
+            raise capi.InvalidValue(capi.INVALID_VALUE, f"X must be {self.n} x k and Y {self.m} x k")
+        if X.dtype != torch.float64 or Y.dtype != torch.float64:
+            raise capi.InvalidValue(capi.INVALID_VALUE, "X and Y must be float64")
+        k = X.shape[1]
+        if k and ((X.stride(1) != 1 and X.shape[0] > 0) or (Y.stride(1) != 1 and Y.shape[0] > 0)):
+            raise capi.InvalidValue(capi.INVALID_VALUE, "X and Y rows must be contiguous")
+        ldx, ldy = max(X.stride(0), k), max(Y.stride(0), k)
+        capi.check(capi.lib.abhsf_spmm(self._h, k, X.data_ptr(), ldx, Y.data_ptr(), ldy, _stream_ptr(stream)))
+
     def _check_vec(self, x, y, dtype, nx, ny, contiguous):
         if x.dtype != dtype or y.dtype != dtype:
             raise capi.InvalidValue(capi.INVALID_VALUE, f"x and y must be float64, got {x.dtype}, {y.dtype}")

@@ -144,6 +144,16 @@ ABHSF_API abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, con
  * Replaces spmv(x, y) (spmv/bottlenecks/spmv.cpp:58-64, spmv/orig/88.cpp:204-236). */
 ABHSF_API abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double* y, abhsf_stream_t stream);
 
+/* Y += A X for k right-hand sides, X (n x k) and Y (m x k) float64 row-major
+ * in device memory: element (i, j) of X at X[i * ldx + j], ldx >= k, and the
+ * same for Y with ldy.  Column j of Y gets exactly what abhsf_spmv gives for
+ * column j.  The matrix is read once per pass of up to 8 columns (block sizes
+ * 32 and 64, reference order); otherwise the columns go through abhsf_spmv one
+ * at a time.  No reference counterpart: the reference has single-vector
+ * SpMV only (spmv/bottlenecks/spmv.cpp:58-64); this is its multi-vector form. */
+ABHSF_API abhsf_status abhsf_spmm(const abhsf_matrix* a, int32_t k, const double* X, int64_t ldx, double* Y,
+                                  int64_t ldy, abhsf_stream_t stream);
+
 /* The same with x and y in host memory: copies x and y in, runs, copies y
  * back and synchronises.  The drop-in for callers of the reference's
  * host-memory spmv(x, y).  Device staging buffers are allocated on first use
