@@ -84,11 +84,12 @@ constexpr int ring_overhead()
 }
 
 // The ring: the shared memory of an SM (228 KiB, 1 KiB of it reserved per
-// CTA) split over kCtasPerSm CTAs, less the rest of the CTA's shared memory.
+// CTA) split over kCtasPerSm CTAs, less the rest of the CTA's shared memory
+// and 1 KiB for the granularity of shared-memory allocations.
 template <int S, int K>
 constexpr int ring_bytes()
 {
-    return ((233472 / kCtasPerSm - 1024 - ring_overhead<S, K>()) / 16) * 16;
+    return ((233472 / kCtasPerSm - 2048 - ring_overhead<S, K>()) / 16) * 16;
 }
 
 // The largest slot of a single-right-hand-side pass: y and x segments, a COO
@@ -640,7 +641,8 @@ __global__ void k_ring_max_pv(int64_t T, tiles_view A, unsigned int* __restrict_
 template <int S, int K>
 void launch_ring(const abhsf_matrix& a, const double* x, int64_t ldx, double* y, int64_t ldy, cudaStream_t st)
 {
-    static_assert(sizeof(ring_smem<S, K>) + 1024 <= 233472 / kCtasPerSm, "kCtasPerSm CTAs fit an SM");
+    static_assert(((sizeof(ring_smem<S, K>) + 1023) / 1024 + 1) * 1024 * kCtasPerSm <= 233472,
+                  "kCtasPerSm CTAs fit an SM even with shared memory allocated in 1 KiB granules");
     ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()), a.ring_wbeg.get(), x, y, ldx, ldy,
                 a.dev_status.get(), g_drop_desc, g_spin_limit ? g_spin_limit : kWaitPolls};
     k_spmv_f64_ring<S, K><<<(unsigned)a.ring_warps, S + 32, sizeof(ring_smem<S, K>), st>>>(P);

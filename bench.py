@@ -117,6 +117,35 @@ def algorithmic_bytes(st: dict, m: int, n: int) -> int:
     return int(st["format_bytes"]) + 8 * n + 16 * m
 
 
+def time_spmm(A, c, st, dev, stream, l2_flush, warmup, ks=(4, 8, 16, 32), steps=5):
+    """Y += A X on the same matrix for a few k (X, Y row-major, resident in
+    HBM); bytes per call B_fmt + k (8 n + 16 m), FLOPs 2 nnz k."""
+    import torch
+    out = {}
+    for k in ks:
+        X = torch.rand((c.n, k), dtype=torch.float64, device=dev)
+        Y = torch.zeros((c.m, k), dtype=torch.float64, device=dev)
+        for _ in range(max(warmup, 1)):
+            l2_flush()
+            A.spmm(X, Y)
+        ts = []
+        for _ in range(steps):
+            l2_flush()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            A.spmm(X, Y)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        t = sum(ts) / len(ts)
+        b = int(st["format_bytes"]) + k * (8 * c.n + 16 * c.m)
+        out[str(k)] = {"ms": t, "GB/s": b / (t * 1e-3) / 1e9, "gflops": 2.0 * c.nnz * k / (t * 1e-3) / 1e9,
+                       "bytes": b}
+        del X, Y
+    return out
+
+
 def cpu_reference_run(c, bytes_per_step: float, max_seconds: float, max_iters: int):
     """Reference CSR spmv_naive (oracle/_ref, compiled from the reference
     sources) on all host threads; falls back to the single-thread oracle port."""
@@ -269,6 +298,8 @@ def run_ours(args):
         dist.all_reduce(e_red, op=dist.ReduceOp.MAX)
     e2e_s = float(e_red.item())
 
+    spmm = None if args.no_spmm else time_spmm(A, c, st, dev, stream, l2_flush, args.warmup)
+
     peak, peak_src = hbm_peak()
     achieved = B / (t_mean * 1e-3) / 1e9
     cpu = None
@@ -297,6 +328,7 @@ def run_ours(args):
                          "peak_source": peak_src,
                          "kernel": KERNELS[args.sum_order] + "<64>"},
             "cpu_baseline": cpu,
+            "spmm": spmm,
             "e2e": {"value": world * B / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
                     "d2h_bytes_per_step": 8 * c.m, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": args.steps,
@@ -316,6 +348,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
+    ap.add_argument("--no-spmm", action="store_true", help="skip the multi-right-hand-side timings")
     ap.add_argument("--sum-order", choices=["reference", "tree"], default="reference",
                     help="reference: bitwise the reference CSR's y; tree: warp reduction trees")
     ap.add_argument("--n", type=int, default=DEFAULT_N,
