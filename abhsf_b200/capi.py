@@ -63,6 +63,11 @@ class BuildOpts(C.Structure):
                 ("sum_order", C.c_int32), ("bits_per_value", C.c_int64)]
 
 
+class CgInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("outer_iterations", C.c_int32), ("converged", C.c_int32),
+                ("reserved", C.c_int32), ("rel_residual", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("nnz", C.c_int64),
                 ("block_size", C.c_int32), ("value_type", C.c_int32),
@@ -88,6 +93,10 @@ PROTOTYPES = {
     "abhsf_spmv": (C.c_int, [_vp, _vp, _vp, _vp]),
     "abhsf_spmv_host": (C.c_int, [_vp, _vp, _vp, _vp]),
     "abhsf_spmm": (C.c_int, [_vp, _i32, _vp, _i64, _vp, _i64, _vp]),
+    "abhsf_spmv_f32": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "abhsf_cg": (C.c_int, [_vp, _vp, _vp, C.c_double, _i32, C.POINTER(CgInfo), _vp]),
+    "abhsf_cg_mixed": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, _i32, C.c_double, _i32, C.POINTER(CgInfo),
+                                 _vp]),
     "abhsf_release": (C.c_int, [_vp]),
     "abhsf_stats_get": (C.c_int, [_vp, C.POINTER(Stats)]),
     "abhsf_export_host": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

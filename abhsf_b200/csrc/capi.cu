@@ -111,6 +111,58 @@ abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double* y, abhsf
     });
 }
 
+abhsf_status abhsf_spmv_f32(const abhsf_matrix* a, const float* x, float* y, abhsf_stream_t stream)
+{
+    return guarded([&] {
+        if (!a)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle is NULL");
+        if (a->value_type == ABHSF_VALUE_F64)
+            fail(ABHSF_ERROR_INVALID_VALUE, "abhsf_spmv_f32 needs a matrix stored as f32 or bf16");
+        if ((!x && a->n) || (!y && a->m))
+            fail(ABHSF_ERROR_INVALID_VALUE, "x and y must be non-NULL");
+        if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 3)
+            fail(ABHSF_ERROR_INVALID_VALUE, "x and y must be 4-byte aligned");
+        if (a->m == 0 || a->T == 0)
+            return;
+        if (!abhsf::spmv_f32_ring(*a, x, y, reinterpret_cast<cudaStream_t>(stream)))
+            fail(ABHSF_ERROR_UNSUPPORTED, "abhsf_spmv_f32 supports block sizes 32 and 64");
+    });
+}
+
+abhsf_status abhsf_cg(const abhsf_matrix* a, const double* b, double* x, double rtol, int32_t max_iters,
+                      abhsf_cg_info* info, abhsf_stream_t stream)
+{
+    return guarded([&] {
+        if (!a || !info)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle and info must be non-NULL");
+        if (a->value_type != ABHSF_VALUE_F64)
+            fail(ABHSF_ERROR_INVALID_VALUE, "abhsf_cg needs a matrix stored as f64");
+        if ((!b || !x) && a->n)
+            fail(ABHSF_ERROR_INVALID_VALUE, "b and x must be non-NULL");
+        if (!(rtol >= 0.0))
+            fail(ABHSF_ERROR_INVALID_VALUE, "rtol must be >= 0");
+        abhsf::cg_solve(*a, b, x, rtol, max_iters, info, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+abhsf_status abhsf_cg_mixed(const abhsf_matrix* a64, const abhsf_matrix* a_lo, const double* b, double* x,
+                            double rtol, int32_t max_iters, double inner_rtol, int32_t max_outer,
+                            abhsf_cg_info* info, abhsf_stream_t stream)
+{
+    return guarded([&] {
+        if (!a64 || !a_lo || !info)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handles and info must be non-NULL");
+        if (a64->value_type != ABHSF_VALUE_F64 || a_lo->value_type == ABHSF_VALUE_F64)
+            fail(ABHSF_ERROR_INVALID_VALUE, "abhsf_cg_mixed needs a64 stored as f64 and a_lo as f32 or bf16");
+        if ((!b || !x) && a64->n)
+            fail(ABHSF_ERROR_INVALID_VALUE, "b and x must be non-NULL");
+        if (!(rtol >= 0.0) || !(inner_rtol > 0.0 && inner_rtol < 1.0))
+            fail(ABHSF_ERROR_INVALID_VALUE, "rtol must be >= 0 and inner_rtol in (0, 1)");
+        abhsf::cg_solve_mixed(*a64, *a_lo, b, x, rtol, max_iters, inner_rtol, max_outer, info,
+                              reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
 abhsf_status abhsf_spmm(const abhsf_matrix* a, int32_t k, const double* X, int64_t ldx, double* Y, int64_t ldy,
                         abhsf_stream_t stream)
 {

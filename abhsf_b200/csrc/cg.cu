@@ -1,0 +1,337 @@
+// cg.cu -- conjugate gradients on ABHSF matrices: plain FP64, and mixed
+// precision (FP64 iterative refinement around an f32 CG on an f32 or bf16
+// copy of the matrix).
+//
+// The reference has no solver; its SpMV is the kernel such a solver calls
+// (spmv/bottlenecks/spmv.cpp:58-64).  Both solvers here keep every scalar
+// (alpha, beta, r.r) on the device: a CG iteration is one SpMV and five small
+// kernels, and chunks of iterations are captured once into a CUDA graph and
+// replayed, with one host read of the state per chunk.  Dot products are
+// summed in FP64 over a fixed grid (deterministic).  Once the recurrence
+// residual meets the tolerance, the state's `done` flag turns the rest of the
+// chunk's updates into no-ops.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace abhsf {
+namespace {
+
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs
+constexpr int kRedThreads = 256;
+constexpr int kChunk = 8;  // CG iterations per captured graph
+
+struct cg_state {
+    double rr;     // r . r of the current residual
+    double alpha;  // step of this iteration
+    double beta;   // p update of this iteration
+    double tol2;   // stop when r . r <= tol2
+    int done;      // tolerance met, or iteration limit reached
+    int iters;     // iterations performed
+    int max_iters;
+    int pad;
+};
+
+__device__ __forceinline__ double block_sum(double v)
+{
+    __shared__ double part[kRedThreads / 32];
+    for (int d = 16; d > 0; d >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, d);
+    if ((threadIdx.x & 31) == 0)
+        part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    v = threadIdx.x < kRedThreads / 32 ? part[threadIdx.x] : 0.0;
+    if (threadIdx.x < 32)
+        for (int d = 16; d > 0; d >>= 1)
+            v += __shfl_xor_sync(0xffffffffu, v, d);
+    return v;  // valid in thread 0
+}
+
+// partial[blockIdx.x] = sum over this block's grid-stride share of a[i] b[i]
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_dot(int64_t n, const T* __restrict__ a, const T* __restrict__ b,
+                                                     double* __restrict__ partial)
+{
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)kRedBlocks * kRedThreads)
+        s += (double)a[i] * (double)b[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0)
+        partial[blockIdx.x] = s;
+}
+
+__device__ __forceinline__ double sum_partials(const double* __restrict__ partial)
+{
+    double s = 0.0;
+    for (int i = threadIdx.x; i < kRedBlocks; i += kRedThreads)
+        s += partial[i];
+    return block_sum(s);
+}
+
+// state from r . r (first partials), with tolerance tol2 = rtol^2 * bb
+__global__ void __launch_bounds__(kRedThreads) k_cg_init(const double* __restrict__ partial, cg_state* st,
+                                                         double tol2, int max_iters)
+{
+    const double rr = sum_partials(partial);
+    if (threadIdx.x == 0) {
+        st->rr = rr;
+        st->alpha = st->beta = 0.0;
+        st->tol2 = tol2;
+        st->iters = 0;
+        st->max_iters = max_iters;
+        st->done = (rr <= tol2 || max_iters <= 0) ? 1 : 0;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_cg_alpha(const double* __restrict__ partial, cg_state* st)
+{
+    const double pap = sum_partials(partial);
+    if (threadIdx.x == 0) {
+        if (st->done || !(pap > 0.0)) {  // converged, or breakdown (p = 0 or A not positive definite on p)
+            st->alpha = 0.0;
+            st->done = 1;
+        } else {
+            st->alpha = st->rr / pap;
+        }
+    }
+}
+
+// x += alpha p; r -= alpha Ap; Ap = 0 (ready for the next y += A p); partial r . r
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_cg_update_xr(int64_t n, T* __restrict__ x, T* __restrict__ r,
+                                                              T* __restrict__ ap, const T* __restrict__ p,
+                                                              const cg_state* st, double* __restrict__ partial)
+{
+    const T alpha = (T)st->alpha;
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)kRedBlocks * kRedThreads) {
+        const T ri = r[i] - alpha * ap[i];
+        x[i] += alpha * p[i];
+        r[i] = ri;
+        ap[i] = T(0);
+        s += (double)ri * (double)ri;
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0)
+        partial[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_cg_beta(const double* __restrict__ partial, cg_state* st)
+{
+    const double rr_new = sum_partials(partial);
+    if (threadIdx.x == 0 && !st->done) {
+        st->beta = rr_new / st->rr;
+        st->rr = rr_new;
+        st->iters += 1;
+        if (rr_new <= st->tol2 || st->iters >= st->max_iters)
+            st->done = 1;
+    }
+}
+
+template <typename T>
+__global__ void k_cg_update_p(int64_t n, T* __restrict__ p, const T* __restrict__ r, const cg_state* st)
+{
+    if (st->done)
+        return;
+    const T beta = (T)st->beta;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = r[i] + beta * p[i];
+}
+
+template <typename T>
+__global__ void k_neg(int64_t n, const T* __restrict__ a, T* __restrict__ out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = -a[i];
+}
+
+// r32 = r64 / ||r64|| (rr = r64 . r64 from the state)
+__global__ void k_to_unit_f32(int64_t n, const double* __restrict__ r, float* __restrict__ out, const cg_state* st)
+{
+    const double inv = st->rr > 0.0 ? 1.0 / sqrt(st->rr) : 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (float)(r[i] * inv);
+}
+
+// x += ||r64|| d
+__global__ void k_add_scaled(int64_t n, double* __restrict__ x, const float* __restrict__ d, const cg_state* st)
+{
+    const double scale = sqrt(st->rr);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += scale * (double)d[i];
+}
+
+unsigned elem_grid(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+// y += A x in T (f64 or f32 kernels)
+void spmv_t(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st) { spmv_dispatch(a, x, y, st); }
+void spmv_t(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st)
+{
+    if (!spmv_f32_ring(a, x, y, st))
+        fail(ABHSF_ERROR_UNSUPPORTED, "the f32 SpMV supports block sizes 32 and 64");
+}
+
+template <typename T>
+struct cg_work {
+    dbuf<T> r, p, ap;
+    explicit cg_work(int64_t n) : r(n), p(n), ap(n) {}
+};
+
+// r = b - A x (xn: scratch)
+template <typename T>
+void residual(const abhsf_matrix& a, const T* b, const T* x, T* r, T* xn, int64_t n, cudaStream_t st)
+{
+    k_neg<T><<<elem_grid(n), 256, 0, st>>>(n, x, xn);
+    ABHSF_CUDA(cudaMemcpyAsync(r, b, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    spmv_t(a, xn, r, st);
+}
+
+template <typename T>
+void dot(const T* a, const T* b, int64_t n, double* partial, cudaStream_t st)
+{
+    k_dot<T><<<kRedBlocks, kRedThreads, 0, st>>>(n, a, b, partial);
+}
+
+// CG on A x = (current r), starting from x with residual w.r, until r . r <=
+// tol2 or max_iters iterations.  Returns the iterations done.
+template <typename T>
+int cg_iterate(const abhsf_matrix& a, T* x, cg_work<T>& w, int64_t n, cg_state* st_d, cg_state* st_h,
+               double* partial, double tol2, int max_iters, cudaStream_t cs)
+{
+    ABHSF_CUDA(cudaMemcpyAsync(w.p.get(), w.r.get(), n * sizeof(T), cudaMemcpyDeviceToDevice, cs));
+    ABHSF_CUDA(cudaMemsetAsync(w.ap.get(), 0, n * sizeof(T), cs));
+    dot<T>(w.r.get(), w.r.get(), n, partial, cs);
+    k_cg_init<<<1, kRedThreads, 0, cs>>>(partial, st_d, tol2, max_iters);
+    ABHSF_CUDA(cudaGetLastError());
+
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ABHSF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    for (int it = 0; it < kChunk; ++it) {
+        spmv_t(a, w.p.get(), w.ap.get(), cs);
+        dot<T>(w.p.get(), w.ap.get(), n, partial, cs);
+        k_cg_alpha<<<1, kRedThreads, 0, cs>>>(partial, st_d);
+        k_cg_update_xr<T><<<kRedBlocks, kRedThreads, 0, cs>>>(n, x, w.r.get(), w.ap.get(), w.p.get(), st_d, partial);
+        k_cg_beta<<<1, kRedThreads, 0, cs>>>(partial, st_d);
+        k_cg_update_p<T><<<elem_grid(n), 256, 0, cs>>>(n, w.p.get(), w.r.get(), st_d);
+    }
+    const cudaError_t cap = cudaStreamEndCapture(cs, &graph);
+    if (cap != cudaSuccess || !graph)
+        fail(ABHSF_ERROR_CUDA, std::string("CG graph capture: ") + cudaGetErrorString(cap));
+    const cudaError_t ins = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ins != cudaSuccess)
+        fail(ABHSF_ERROR_CUDA, std::string("CG graph instantiation: ") + cudaGetErrorString(ins));
+    struct exec_guard {
+        cudaGraphExec_t e;
+        ~exec_guard() { cudaGraphExecDestroy(e); }
+    } guard{exec};
+
+    for (;;) {
+        ABHSF_CUDA(cudaMemcpyAsync(st_h, st_d, sizeof(cg_state), cudaMemcpyDeviceToHost, cs));
+        ABHSF_CUDA(cudaStreamSynchronize(cs));
+        if (st_h->done)
+            break;
+        ABHSF_CUDA(cudaGraphLaunch(exec, cs));
+    }
+    return st_h->iters;
+}
+
+struct solve_stream {
+    cudaStream_t user, cs = nullptr;
+    cudaEvent_t ev = nullptr;
+    explicit solve_stream(cudaStream_t u) : user(u)
+    {
+        ABHSF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        ABHSF_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        ABHSF_CUDA(cudaEventRecord(ev, user));  // the solve starts after the caller's queued work
+        ABHSF_CUDA(cudaStreamWaitEvent(cs, ev, 0));
+    }
+    ~solve_stream()
+    {
+        cudaStreamSynchronize(cs);
+        cudaEventDestroy(ev);
+        cudaStreamDestroy(cs);
+    }
+};
+
+double norm2(const double* a, int64_t n, double* partial, cg_state* st_d, cg_state* st_h, cudaStream_t cs)
+{
+    dot<double>(a, a, n, partial, cs);
+    k_cg_init<<<1, kRedThreads, 0, cs>>>(partial, st_d, 0.0, 0);
+    ABHSF_CUDA(cudaMemcpyAsync(st_h, st_d, sizeof(cg_state), cudaMemcpyDeviceToHost, cs));
+    ABHSF_CUDA(cudaStreamSynchronize(cs));
+    return st_h->rr;
+}
+
+void check_square(const abhsf_matrix& a)
+{
+    if (a.m != a.n)
+        fail(ABHSF_ERROR_INVALID_VALUE, "CG needs a square matrix");
+}
+
+}  // namespace
+
+void cg_solve(const abhsf_matrix& a, const double* b, double* x, double rtol, int max_iters, abhsf_cg_info* info,
+              cudaStream_t user)
+{
+    check_square(a);
+    const int64_t n = a.n;
+    solve_stream ss(user);
+    cudaStream_t cs = ss.cs;
+    cg_work<double> w(n);
+    dbuf<double> xn(n), partial(kRedBlocks);
+    dbuf<cg_state> st_d(1);
+    cg_state st_h{};
+    const double bb = norm2(b, n, partial.get(), st_d.get(), &st_h, cs);
+    residual<double>(a, b, x, w.r.get(), xn.get(), n, cs);
+    const int iters =
+        cg_iterate<double>(a, x, w, n, st_d.get(), &st_h, partial.get(), rtol * rtol * bb, max_iters, cs);
+    residual<double>(a, b, x, w.r.get(), xn.get(), n, cs);
+    const double rr = norm2(w.r.get(), n, partial.get(), st_d.get(), &st_h, cs);
+    info->iterations = iters;
+    info->outer_iterations = 1;
+    info->rel_residual = bb > 0.0 ? std::sqrt(rr / bb) : std::sqrt(rr);
+    info->converged = info->rel_residual <= rtol ? 1 : 0;
+}
+
+void cg_solve_mixed(const abhsf_matrix& a64, const abhsf_matrix& a32, const double* b, double* x, double rtol,
+                    int max_iters, double inner_rtol, int max_outer, abhsf_cg_info* info, cudaStream_t user)
+{
+    check_square(a64);
+    if (a32.m != a64.m || a32.n != a64.n)
+        fail(ABHSF_ERROR_INVALID_VALUE, "the two matrices of the mixed solver differ in shape");
+    if (a32.ring_warps == 0 && a32.T > 0)
+        fail(ABHSF_ERROR_UNSUPPORTED, "the f32 SpMV of the mixed solver supports block sizes 32 and 64");
+    const int64_t n = a64.n;
+    solve_stream ss(user);
+    cudaStream_t cs = ss.cs;
+    dbuf<double> r64(n), xn(n), partial(kRedBlocks);
+    cg_work<float> w(n);
+    dbuf<float> d(n);
+    dbuf<cg_state> st_d(1), st64_d(1);
+    cg_state st_h{};
+    const double bb = norm2(b, n, partial.get(), st_d.get(), &st_h, cs);
+    residual<double>(a64, b, x, r64.get(), xn.get(), n, cs);
+    double rr = norm2(r64.get(), n, partial.get(), st64_d.get(), &st_h, cs);
+    int iters = 0, outer = 0;
+    while (rr > rtol * rtol * bb && outer < max_outer && iters < max_iters) {
+        // correction: A d = r / ||r|| in f32 to inner_rtol, then x += ||r|| d
+        k_to_unit_f32<<<elem_grid(n), 256, 0, cs>>>(n, r64.get(), w.r.get(), st64_d.get());
+        ABHSF_CUDA(cudaMemsetAsync(d.get(), 0, n * sizeof(float), cs));
+        iters += cg_iterate<float>(a32, d.get(), w, n, st_d.get(), &st_h, partial.get(), inner_rtol * inner_rtol,
+                                   max_iters - iters, cs);
+        k_add_scaled<<<elem_grid(n), 256, 0, cs>>>(n, x, d.get(), st64_d.get());
+        residual<double>(a64, b, x, r64.get(), xn.get(), n, cs);
+        rr = norm2(r64.get(), n, partial.get(), st64_d.get(), &st_h, cs);
+        ++outer;
+    }
+    info->iterations = iters;
+    info->outer_iterations = outer;
+    info->rel_residual = bb > 0.0 ? std::sqrt(rr / bb) : std::sqrt(rr);
+    info->converged = info->rel_residual <= rtol ? 1 : 0;
+}
+
+}  // namespace abhsf

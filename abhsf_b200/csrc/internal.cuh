@@ -37,6 +37,15 @@ void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_
 // The same order through per-warp shared-memory rings (s = 32, 64); false
 // when the matrix has no ring schedule.
 bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+// Conjugate gradients (cg.cu).
+void cg_solve(const abhsf_matrix& a, const double* b, double* x, double rtol, int max_iters, abhsf_cg_info* info,
+              cudaStream_t st);
+void cg_solve_mixed(const abhsf_matrix& a64, const abhsf_matrix& a32, const double* b, double* x, double rtol,
+                    int max_iters, double inner_rtol, int max_outer, abhsf_cg_info* info, cudaStream_t st);
+
+// y += A x in f32 for matrices stored as f32 or bf16 (values widened to f32,
+// same per-row order); false when the matrix has no ring schedule.
+bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st);
 // Y += A X (k columns, row-major X and Y) through the same kernel, several
 // right-hand sides per pass; false when the matrix has no ring schedule.
 bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,

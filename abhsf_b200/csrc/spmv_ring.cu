@@ -75,32 +75,55 @@ struct __align__(16) ring_desc {
 };
 static_assert(sizeof(ring_desc) == 32, "ring_desc is 32 bytes");
 
+// Stored value type V and compute type T (x, y, accumulators) of each
+// abhsf_value_type: f64 values in f64; f32 and bf16 values in f32.
+template <int VT>
+struct val_traits {
+    using V = double;
+    using T = double;
+};
+template <>
+struct val_traits<ABHSF_VALUE_F32> {
+    using V = float;
+    using T = float;
+};
+template <>
+struct val_traits<ABHSF_VALUE_BF16> {
+    using V = uint16_t;
+    using T = float;
+};
+
 // Bytes of a CTA's shared memory other than the ring (queue records and
 // barriers, the y block, the product buffers, the abort flag), rounded up.
-template <int S, int K>
+template <int S, int K, int VT>
 constexpr int ring_overhead()
 {
-    return kMaxQ * (48 + 16) + S * K * 8 + (S / 32) * 32 * 8 + 64;
+    using T = typename val_traits<VT>::T;
+    return kMaxQ * (48 + 16) + (S * K + (S / 32) * 32) * (int)sizeof(T) + 64;
 }
 
 // The ring: the shared memory of an SM (228 KiB, 1 KiB of it reserved per
 // CTA) split over kCtasPerSm CTAs, less the rest of the CTA's shared memory
 // and 1 KiB for the granularity of shared-memory allocations.
-template <int S, int K>
+template <int S, int K, int VT>
 constexpr int ring_bytes()
 {
-    return ((233472 / kCtasPerSm - 2048 - ring_overhead<S, K>()) / 16) * 16;
+    return ((233472 / kCtasPerSm - 2048 - ring_overhead<S, K, VT>()) / 16) * 16;
 }
 
 // The largest slot of a single-right-hand-side pass: y and x segments, a COO
 // payload of s * s keys (2 bytes each), s * s values and one granule of
 // alignment slack.  Every matrix can take that pass.
-template <int S>
+template <int S, int VT>
 constexpr int max_slot_bytes()
 {
-    return 2 * S * 8 + 2 * S * S + 8 * S * S + 16;
+    return 2 * S * (int)sizeof(typename val_traits<VT>::T) + 2 * S * S +
+           (int)sizeof(typename val_traits<VT>::V) * S * S + 16;
 }
-static_assert(max_slot_bytes<64>() <= ring_bytes<64, 1>() && max_slot_bytes<32>() <= ring_bytes<32, 1>(),
+static_assert(max_slot_bytes<64, ABHSF_VALUE_F64>() <= ring_bytes<64, 1, ABHSF_VALUE_F64>() &&
+                  max_slot_bytes<32, ABHSF_VALUE_F64>() <= ring_bytes<32, 1, ABHSF_VALUE_F64>() &&
+                  max_slot_bytes<64, ABHSF_VALUE_F32>() <= ring_bytes<64, 1, ABHSF_VALUE_F32>() &&
+                  max_slot_bytes<64, ABHSF_VALUE_BF16>() <= ring_bytes<64, 1, ABHSF_VALUE_BF16>(),
               "the ring holds any single-right-hand-side slot");
 
 // What the producer tells the consumers about a queued tile.
@@ -110,14 +133,14 @@ struct __align__(16) slot_rec {
     uint32_t pad[3];
 };
 
-template <int S, int K>
+template <int S, int K, int VT>
 struct ring_smem {
-    alignas(16) uint8_t ring[ring_bytes<S, K>()];
+    alignas(16) uint8_t ring[ring_bytes<S, K, VT>()];
     slot_rec rec[kMaxQ];              // queue slot i % kMaxQ
     unsigned long long full[kMaxQ];   // the slot's copies have landed
     unsigned long long empty[kMaxQ];  // the consumers are done with the slot
-    double ys[S * K];                 // the block row's y block, row-major
-    double buf[S / 32][32];           // each consumer warp's products of a COO / CSR chunk
+    typename val_traits<VT>::T ys[S * K];        // the block row's y block, row-major
+    typename val_traits<VT>::T buf[S / 32][32];  // each consumer warp's products of a COO / CSR chunk
     int abort;                        // a wait ran out: everyone stops
 };
 
@@ -125,8 +148,8 @@ struct ring_args {
     tiles_view A;
     const ring_desc* desc;  // every CTA's tiles, CTA after CTA
     const int64_t* wbeg;    // [ctas + 1] each CTA's range in desc
-    const double* x;  // X, row-major: element (i, j) at x[i * ldx + j]
-    double* y;        // Y, row-major: element (i, j) at y[i * ldy + j]
+    const void* x;  // X (T), row-major: element (i, j) at x[i * ldx + j]
+    void* y;        // Y (T), row-major: element (i, j) at y[i * ldy + j]
     int64_t ldx, ldy;
     int* status;     // ABHSF_DEVSTAT_* bits
     int64_t drop;    // test hook: descriptor whose bulk copies are not issued (-1: none)
@@ -138,16 +161,24 @@ struct slot_geo {
     int x, pay, val, size;
 };
 
-template <int S, int K>
+// Values before the tile's first value in its first 16-byte granule.
+template <int VT>
+__host__ __device__ __forceinline__ int lead(const ring_desc& d)
+{
+    return (int)(d.vo & (16 / (int)sizeof(typename val_traits<VT>::V) - 1));
+}
+
+template <int S, int K, int VT>
 __host__ __device__ __forceinline__ slot_geo geometry(const ring_desc& d)
 {
+    constexpr int TB = sizeof(typename val_traits<VT>::T), VB = sizeof(typename val_traits<VT>::V), G = 16 / VB;
     slot_geo g;
-    g.x = (d.info & kFirst) ? S * K * 8 : 0;  // the y block comes first
-    g.pay = g.x + S * K * 8;
+    g.x = (d.info & kFirst) ? S * K * TB : 0;  // the y block comes first
+    g.pay = g.x + S * K * TB;
     g.val = g.pay + (int)(d.pb_sch & 0xffffffu);
-    // values are copied in 16-byte granules from the even element at or below vo
-    const int nv2 = ((int)d.nv + (int)(d.vo & 1) + 1) & ~1;
-    g.size = g.val + nv2 * 8;
+    // values are copied in 16-byte granules from the granule holding value vo
+    const int span = ((int)(d.vo & (G - 1)) + (int)d.nv + G - 1) & ~(G - 1);
+    g.size = g.val + span * VB;
     return g;
 }
 
@@ -213,22 +244,44 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
 
 __device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+
+// x, y and accumulators in T, stored values V widened to T.
+__device__ __forceinline__ double widen(double v) { return v; }
+__device__ __forceinline__ float widen(float v) { return v; }
+__device__ __forceinline__ float widen(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }  // bf16 bits
+
+// 4- or 8-byte copy of one x / y element (src_bytes = 0 writes zeros)
+template <typename T>
+__device__ __forceinline__ void cp_elem(uint32_t dst, const T* src, int src_bytes)
+{
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
 
 // Producer warp: queues tile d's slot at ring offset off as queue slot q; it
 // completes on full[q].
-template <int S, int K>
+template <int S, int K, int VT>
 __device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, const slot_geo& g, uint32_t off, int q,
-                                      ring_smem<S, K>& sm, int64_t e, int lane)
+                                      ring_smem<S, K, VT>& sm, int64_t e, int lane)
 {
+    using T = typename val_traits<VT>::T;
+    using V = typename val_traits<VT>::V;
+    constexpr int TB = sizeof(T);
     const uint32_t base = smem_addr(sm.ring + off);
     unsigned long long* bar = &sm.full[q];
+    const T* X = static_cast<const T*>(P.x);
+    const T* Y = static_cast<const T*>(P.y);
     if (d.info & kFirst) {
         const int64_t r0 = (int64_t)(d.info & kRowMask) * S;
 #pragma unroll
         for (int k = lane; k < S * K; k += 32) {
             const int r = k / K, j = k % K;
             const bool ok = r0 + r < P.A.m;
-            cp8(base + 8 * k, ok ? P.y + (r0 + r) * P.ldy + j : P.y, ok ? 8 : 0);
+            cp_elem(base + TB * k, ok ? Y + (r0 + r) * P.ldy + j : Y, ok ? TB : 0);
         }
     }
     const int64_t c0 = (int64_t)d.col * S;
@@ -236,7 +289,7 @@ __device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, co
     for (int k = lane; k < S * K; k += 32) {
         const int c = k / K, j = k % K;
         const bool ok = c0 + c < P.A.n;
-        cp8(base + g.x + 8 * k, ok ? P.x + (c0 + c) * P.ldx + j : P.x, ok ? 8 : 0);
+        cp_elem(base + g.x + TB * k, ok ? X + (c0 + c) * P.ldx + j : X, ok ? TB : 0);
     }
     cp_arrive(bar);
     if (lane == 0) {
@@ -249,7 +302,7 @@ __device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, co
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             if (pb)
                 bulk_g2s(base + g.pay, P.A.payload + d.io, pb, bar);
-            bulk_g2s(base + g.val, static_cast<const double*>(P.A.values) + (d.vo & ~(int64_t)1), vb, bar);
+            bulk_g2s(base + g.val, static_cast<const V*>(P.A.values) + (d.vo - lead<VT>(d)), vb, bar);
         }
     }
 }
@@ -286,13 +339,15 @@ __device__ __forceinline__ int warp_sum(int v)
 
 // Bitmap tile, row `row` = 32 warp + lane.  Row r's bits are u32 words
 // r * W .. r * W + W - 1 (W = S / 32), bit b of word j = column 32 j + b.
-template <int S, int K>
-__device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& g, int parity, double* ys, int warp,
-                                           int lane)
+template <int S, int K, int VT>
+__device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& g, int parity,
+                                           typename val_traits<VT>::T* ys, int warp, int lane)
 {
+    using T = typename val_traits<VT>::T;
+    using V = typename val_traits<VT>::V;
     constexpr int W = S / 32;
-    const double* xs = reinterpret_cast<const double*>(slot + g.x);
-    const double* vs = reinterpret_cast<const double*>(slot + g.val) + parity;
+    const T* xs = reinterpret_cast<const T*>(slot + g.x);
+    const V* vs = reinterpret_cast<const V*>(slot + g.val) + parity;
     const int row = 32 * warp + lane;
     uint32_t w[W];
     int cnt = 0, before = 0;
@@ -312,7 +367,7 @@ __device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& 
     for (int j = 0; j < W; ++j)
         cnt += __popc(w[j]);
     int q = before + warp_inclusive_sum(cnt, lane) - cnt;
-    double acc[K];
+    T acc[K];
 #pragma unroll
     for (int h = 0; h < K; ++h)
         acc[h] = ys[row * K + h];
@@ -320,12 +375,12 @@ __device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& 
     for (int j = 0; j < W; ++j) {
 #pragma unroll
         for (int b = 0; b < 32; ++b) {
-            double xv[K];
+            T xv[K];
 #pragma unroll
             for (int h = 0; h < K; ++h)
                 xv[h] = xs[(32 * j + b) * K + h];
             if ((w[j] >> b) & 1u) {
-                const double v = vs[q];
+                const T v = widen(vs[q]);
 #pragma unroll
                 for (int h = 0; h < K; ++h)
                     acc[h] = fadd(acc[h], fmul(v, xv[h]));
@@ -340,14 +395,16 @@ __device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& 
 
 // Dense tile: all S * S values, row-major.  Lane l runs l columns behind
 // lane 0 so that the lanes' values fall in different banks.
-template <int S, int K>
-__device__ __forceinline__ void sum_dense(const uint8_t* slot, const slot_geo& g, int parity, double* ys, int warp,
-                                          int lane)
+template <int S, int K, int VT>
+__device__ __forceinline__ void sum_dense(const uint8_t* slot, const slot_geo& g, int parity,
+                                          typename val_traits<VT>::T* ys, int warp, int lane)
 {
-    const double* xs = reinterpret_cast<const double*>(slot + g.x);
-    const double* vs = reinterpret_cast<const double*>(slot + g.val) + parity;
+    using T = typename val_traits<VT>::T;
+    using V = typename val_traits<VT>::V;
+    const T* xs = reinterpret_cast<const T*>(slot + g.x);
+    const V* vs = reinterpret_cast<const V*>(slot + g.val) + parity;
     const int row = 32 * warp + lane;
-    double acc[K];
+    T acc[K];
 #pragma unroll
     for (int h = 0; h < K; ++h)
         acc[h] = ys[row * K + h];
@@ -355,8 +412,8 @@ __device__ __forceinline__ void sum_dense(const uint8_t* slot, const slot_geo& g
     for (int k = 0; k < S + 31; ++k) {
         const int c = k - lane;
         if (c >= 0 && c < S) {
-            const double v = vs[row * S + c];
-            if (v != 0.0) {  // stored zeros and the zero padding past n
+            const T v = widen(vs[row * S + c]);
+            if (v != T(0)) {  // stored zeros and the zero padding past n
 #pragma unroll
                 for (int h = 0; h < K; ++h)
                     acc[h] = fadd(acc[h], fmul(v, xs[c * K + h]));
@@ -369,13 +426,16 @@ __device__ __forceinline__ void sum_dense(const uint8_t* slot, const slot_geo& g
 }
 
 // COO / CSR tile: this warp's rows' elements, 32 at a time.
-template <int S, int K, bool CSR>
-__device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& g, int parity, int z, double* ys,
-                                           double* buf, int warp, int lane)
+template <int S, int K, int VT, bool CSR>
+__device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& g, int parity, int z,
+                                           typename val_traits<VT>::T* ys, typename val_traits<VT>::T* buf, int warp,
+                                           int lane)
 {
+    using T = typename val_traits<VT>::T;
+    using V = typename val_traits<VT>::V;
     constexpr int LG = S == 32 ? 5 : 6;
-    const double* xs = reinterpret_cast<const double*>(slot + g.x);
-    const double* vs = reinterpret_cast<const double*>(slot + g.val) + parity;
+    const T* xs = reinterpret_cast<const T*>(slot + g.x);
+    const V* vs = reinterpret_cast<const V*>(slot + g.val) + parity;
     const uint16_t* key16 = reinterpret_cast<const uint16_t*>(slot + g.pay);  // COO keys / CSR row ends
     const uint8_t* col8 = slot + g.pay + 2 * S;                                // CSR local columns
     int lo = 0, hi = z;  // elements of rows 32 warp .. 32 warp + 31 (sorted by row)
@@ -406,7 +466,7 @@ __device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& 
         const int k = base + lane;
         int lr = S;  // idle lanes: no row
         int lc = 0;
-        double v = 0.0;
+        T v = T(0);
         if (k < hi) {
             if (CSR) {
                 lc = col8[k];
@@ -427,7 +487,7 @@ __device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& 
                 lr = (int)(key >> LG);
                 lc = (int)(key & (S - 1));
             }
-            v = vs[k];
+            v = widen(vs[k]);
         }
         const int plr = __shfl_up_sync(kFull, lr, 1);
         const bool head = k < hi && (lane == 0 || plr != lr);
@@ -436,11 +496,11 @@ __device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& 
         const int end = later ? __ffs(later) - 1 : min(hi - base, 32);
 #pragma unroll 1
         for (int h = 0; h < K; ++h) {
-            const double p = k < hi ? fmul(v, xs[lc * K + h]) : 0.0;
+            const T p = k < hi ? fmul(v, xs[lc * K + h]) : T(0);
             buf[lane] = p;
             __syncwarp();
             if (head) {
-                double acc = fadd(ys[lr * K + h], p);
+                T acc = fadd(ys[lr * K + h], p);
                 for (int e = lane + 1; e < end; ++e)
                     acc = fadd(acc, buf[e]);
                 ys[lr * K + h] = acc;
@@ -450,24 +510,25 @@ __device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& 
     }
 }
 
-template <int S, int K>
+template <int S, int K, int VT>
 __device__ __forceinline__ void sum_tile(const ring_args& P, const ring_desc& d, const uint8_t* slot,
-                                         ring_smem<S, K>& sm, int warp, int lane)
+                                         ring_smem<S, K, VT>& sm, int warp, int lane)
 {
-    const slot_geo g = geometry<S, K>(d);
-    const int parity = (int)(d.vo & 1);
+    using T = typename val_traits<VT>::T;
+    const slot_geo g = geometry<S, K, VT>(d);
+    const int parity = lead<VT>(d);
     const int row = 32 * warp + lane;
     if (d.info & kFirst) {
 #pragma unroll
         for (int h = 0; h < K; ++h)
-            sm.ys[row * K + h] = reinterpret_cast<const double*>(slot)[row * K + h];
+            sm.ys[row * K + h] = reinterpret_cast<const T*>(slot)[row * K + h];
         __syncwarp();
     }
     switch (d.pb_sch >> 24) {
-    case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K>(slot, g, parity, sm.ys, warp, lane); break;
-    case ABHSF_SCHEME_DENSE: sum_dense<S, K>(slot, g, parity, sm.ys, warp, lane); break;
-    case ABHSF_SCHEME_CSR: sum_stream<S, K, true>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
-    default: sum_stream<S, K, false>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
+    case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K, VT>(slot, g, parity, sm.ys, warp, lane); break;
+    case ABHSF_SCHEME_DENSE: sum_dense<S, K, VT>(slot, g, parity, sm.ys, warp, lane); break;
+    case ABHSF_SCHEME_CSR: sum_stream<S, K, VT, true>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
+    default: sum_stream<S, K, VT, false>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
     }
     if (d.info & kLast) {
         __syncwarp();
@@ -475,19 +536,19 @@ __device__ __forceinline__ void sum_tile(const ring_args& P, const ring_desc& d,
         if (r < P.A.m) {
 #pragma unroll
             for (int h = 0; h < K; ++h)
-                P.y[r * P.ldy + h] = sm.ys[row * K + h];
+                static_cast<T*>(P.y)[r * P.ldy + h] = sm.ys[row * K + h];
         }
     }
 }
 
 // Warps 0 .. S/32 - 1 sum; warp S/32 produces.
-template <int S, int K>
+template <int S, int K, int VT>
 __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args P)
 {
     constexpr int NC = S / 32;  // consumer warps
-    constexpr int kRingBytes = ring_bytes<S, K>();
+    constexpr int kRingBytes = ring_bytes<S, K, VT>();
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    ring_smem<S, K>& sm = *reinterpret_cast<ring_smem<S, K>*>(smem_raw);
+    ring_smem<S, K, VT>& sm = *reinterpret_cast<ring_smem<S, K, VT>*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t eb = P.wbeg[blockIdx.x];
     const int n = (int)(P.wbeg[blockIdx.x + 1] - eb);
@@ -520,7 +581,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                     nxt = D[i + 32 + lane];
             }
             const ring_desc d = shfl_desc(cur, i & 31);
-            const slot_geo g = geometry<S, K>(d);
+            const slot_geo g = geometry<S, K, VT>(d);
             int off = -1;
 #pragma unroll 1
             for (;;) {
@@ -553,7 +614,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                     *abort = 1;
                 break;
             }
-            issue<S, K>(P, d, g, (uint32_t)off, i % kMaxQ, sm, eb + i, lane);
+            issue<S, K, VT>(P, d, g, (uint32_t)off, i % kMaxQ, sm, eb + i, lane);
             if (lane == i % kMaxQ)
                 my_off = off;
             if (i == done)
@@ -572,7 +633,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                 break;
             }
             const slot_rec& r = sm.rec[q];
-            sum_tile<S, K>(P, r.d, sm.ring + r.off, sm, warp, lane);
+            sum_tile<S, K, VT>(P, r.d, sm.ring + r.off, sm, warp, lane);
             __syncwarp();
             if (lane == 0)
                 mbar_arrive(&sm.empty[q]);
@@ -594,12 +655,13 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
 
 // Bytes a block row moves through the ring, plus a fixed cost per tile and
 // per block row: the weight the build-time deal balances.
-__global__ void k_ring_weight(int64_t nr, const uint32_t* __restrict__ rows, tiles_view A, int s,
+__global__ void k_ring_weight(int64_t nr, const uint32_t* __restrict__ rows, tiles_view A, int s, int vsize,
                               uint64_t* __restrict__ weight, uint32_t* __restrict__ ntiles)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nr; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t I = rows[k], t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
-        weight[k] = (uint64_t)(8 * (A.tile_val_off[t1] - A.tile_val_off[t0]) + (A.tile_idx_off[t1] - A.tile_idx_off[t0]) +
+        weight[k] = (uint64_t)(vsize * (A.tile_val_off[t1] - A.tile_val_off[t0]) +
+                               (A.tile_idx_off[t1] - A.tile_idx_off[t0]) +
                                (t1 - t0) * (8 * (int64_t)s + ABHSF_RING_TILE_COST) + 8 * (int64_t)s + 512);
         ntiles[k] = (uint32_t)(t1 - t0);
     }
@@ -625,46 +687,49 @@ __global__ void k_ring_fill(int64_t nitems, const uint32_t* __restrict__ rows, c
     }
 }
 
-// Largest payload + values part of any tile's slot (bytes).
-__global__ void k_ring_max_pv(int64_t T, tiles_view A, unsigned int* __restrict__ out)
+// Largest payload + values part of any tile's slot (bytes; vsize-byte values
+// copied in 16-byte granules).
+__global__ void k_ring_max_pv(int64_t T, tiles_view A, int vsize, unsigned int* __restrict__ out)
 {
+    const int64_t G = 16 / vsize;
     unsigned int best = 0;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t vo = A.tile_val_off[t], nv = A.tile_val_off[t + 1] - vo;
-        const int64_t pv = (A.tile_idx_off[t + 1] - A.tile_idx_off[t]) + ((nv + (vo & 1) + 1) & ~(int64_t)1) * 8;
+        const int64_t pv =
+            (A.tile_idx_off[t + 1] - A.tile_idx_off[t]) + (((vo & (G - 1)) + nv + G - 1) & ~(G - 1)) * vsize;
         best = max(best, (unsigned int)pv);
     }
     atomicMax(out, best);
 }
 
 // One pass: K right-hand sides, X and Y starting at their first column.
-template <int S, int K>
-void launch_ring(const abhsf_matrix& a, const double* x, int64_t ldx, double* y, int64_t ldy, cudaStream_t st)
+template <int S, int K, int VT>
+void launch_ring(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int64_t ldy, cudaStream_t st)
 {
-    static_assert(((sizeof(ring_smem<S, K>) + 1023) / 1024 + 1) * 1024 * kCtasPerSm <= 233472,
+    static_assert(((sizeof(ring_smem<S, K, VT>) + 1023) / 1024 + 1) * 1024 * kCtasPerSm <= 233472,
                   "kCtasPerSm CTAs fit an SM even with shared memory allocated in 1 KiB granules");
     ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()), a.ring_wbeg.get(), x, y, ldx, ldy,
                 a.dev_status.get(), g_drop_desc, g_spin_limit ? g_spin_limit : kWaitPolls};
-    k_spmv_f64_ring<S, K><<<(unsigned)a.ring_warps, S + 32, sizeof(ring_smem<S, K>), st>>>(P);
+    k_spmv_f64_ring<S, K, VT><<<(unsigned)a.ring_warps, S + 32, sizeof(ring_smem<S, K, VT>), st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }
 
-template <int S, int K>
+template <int S, int K, int VT>
 int ring_ctas_per_sm()
 {
     int nb = 0;
-    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(ring_smem<S, K>)));
+    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S, K, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(ring_smem<S, K, VT>)));
     ABHSF_CUDA(
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S, K>, S + 32, sizeof(ring_smem<S, K>)));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S, K, VT>, S + 32, sizeof(ring_smem<S, K, VT>)));
     return std::max(nb, 1);
 }
 
 // Does a pass of K right-hand sides fit every tile of this matrix in the ring?
-template <int S, int K>
+template <int S, int K, int VT>
 bool ring_fits(const abhsf_matrix& a)
 {
-    return 2 * S * K * 8 + (int64_t)a.ring_max_pv <= ring_bytes<S, K>();
+    return 2 * S * K * (int64_t)sizeof(typename val_traits<VT>::T) + (int64_t)a.ring_max_pv <= ring_bytes<S, K, VT>();
 }
 
 // Y += A X over columns [0, k) in passes of the largest K that fits.
@@ -673,17 +738,17 @@ void spmm_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, doubl
 {
     for (int j = 0; j < k;) {
         const int left = k - j;
-        if (left >= 8 && ring_fits<S, 8>(a)) {
-            launch_ring<S, 8>(a, X + j, ldx, Y + j, ldy, st);
+        if (left >= 8 && ring_fits<S, 8, ABHSF_VALUE_F64>(a)) {
+            launch_ring<S, 8, ABHSF_VALUE_F64>(a, X + j, ldx, Y + j, ldy, st);
             j += 8;
-        } else if (left >= 4 && ring_fits<S, 4>(a)) {
-            launch_ring<S, 4>(a, X + j, ldx, Y + j, ldy, st);
+        } else if (left >= 4 && ring_fits<S, 4, ABHSF_VALUE_F64>(a)) {
+            launch_ring<S, 4, ABHSF_VALUE_F64>(a, X + j, ldx, Y + j, ldy, st);
             j += 4;
-        } else if (left >= 2 && ring_fits<S, 2>(a)) {
-            launch_ring<S, 2>(a, X + j, ldx, Y + j, ldy, st);
+        } else if (left >= 2 && ring_fits<S, 2, ABHSF_VALUE_F64>(a)) {
+            launch_ring<S, 2, ABHSF_VALUE_F64>(a, X + j, ldx, Y + j, ldy, st);
             j += 2;
         } else {
-            launch_ring<S, 1>(a, X + j, ldx, Y + j, ldy, st);
+            launch_ring<S, 1, ABHSF_VALUE_F64>(a, X + j, ldx, Y + j, ldy, st);
             j += 1;
         }
     }
@@ -692,9 +757,9 @@ void spmm_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, doubl
 template <int S>
 void ring_set_up_all()
 {
-    ring_ctas_per_sm<S, 2>();
-    ring_ctas_per_sm<S, 4>();
-    ring_ctas_per_sm<S, 8>();
+    ring_ctas_per_sm<S, 2, ABHSF_VALUE_F64>();
+    ring_ctas_per_sm<S, 4, ABHSF_VALUE_F64>();
+    ring_ctas_per_sm<S, 8, ABHSF_VALUE_F64>();
 }
 
 }  // namespace
@@ -702,23 +767,31 @@ void ring_set_up_all()
 void prepare_ring(abhsf_matrix& a, cudaStream_t st)
 {
     a.ring_warps = 0;
-    if ((a.s != 32 && a.s != 64) || a.value_type != ABHSF_VALUE_F64 || a.tree_nrows == 0 || a.M > (int64_t)kRowMask)
+    if ((a.s != 32 && a.s != 64) || a.tree_nrows == 0 || a.M > (int64_t)kRowMask)
         return;
     int dev = 0, nsm = 0;
     ABHSF_CUDA(cudaGetDevice(&dev));
     ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const int per_sm = a.s == 32 ? ring_ctas_per_sm<32, 1>() : ring_ctas_per_sm<64, 1>();
-    if (a.s == 32)
-        ring_set_up_all<32>();
-    else
-        ring_set_up_all<64>();
+    int per_sm = 1;
+    if (a.value_type == ABHSF_VALUE_F64) {
+        per_sm = a.s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_F64>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_F64>();
+        if (a.s == 32)
+            ring_set_up_all<32>();
+        else
+            ring_set_up_all<64>();
+    } else if (a.value_type == ABHSF_VALUE_F32) {
+        per_sm = a.s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_F32>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_F32>();
+    } else {
+        per_sm = a.s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_BF16>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_BF16>();
+    }
+    const int vsize = (int)value_size(a.value_type);
     const int64_t nr = a.tree_nrows;
     const int64_t ctas = std::min<int64_t>((int64_t)nsm * per_sm, nr);
 
     dbuf<uint64_t> w_d(nr);
     dbuf<uint32_t> n_d(nr);
     const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nr + 255) / 256, 4096));
-    k_ring_weight<<<g, 256, 0, st>>>(nr, a.tree_rows.get(), a.view(), (int)a.s, w_d.get(), n_d.get());
+    k_ring_weight<<<g, 256, 0, st>>>(nr, a.tree_rows.get(), a.view(), (int)a.s, vsize, w_d.get(), n_d.get());
     ABHSF_CUDA(cudaGetLastError());
     std::vector<uint32_t> rows(nr), ntiles(nr);
     std::vector<uint64_t> wt(nr);
@@ -777,7 +850,7 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     dbuf<unsigned int> max_pv(1);
     ABHSF_CUDA(cudaMemsetAsync(max_pv.get(), 0, sizeof(unsigned int), st));
     const unsigned gt = (unsigned)std::max<int64_t>(1, std::min<int64_t>((a.T + 255) / 256, 4096));
-    k_ring_max_pv<<<gt, 256, 0, st>>>(a.T, a.view(), max_pv.get());
+    k_ring_max_pv<<<gt, 256, 0, st>>>(a.T, a.view(), vsize, max_pv.get());
     ABHSF_CUDA(cudaGetLastError());
     unsigned int mpv = 0;
     ABHSF_CUDA(cudaMemcpyAsync(&mpv, max_pv.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
@@ -788,19 +861,39 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
 
 bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
-    if (a.ring_warps == 0)
+    if (a.ring_warps == 0 || a.value_type != ABHSF_VALUE_F64)
         return false;
     if (a.s == 32)
-        launch_ring<32, 1>(a, x, 1, y, 1, st);
+        launch_ring<32, 1, ABHSF_VALUE_F64>(a, x, 1, y, 1, st);
     else
-        launch_ring<64, 1>(a, x, 1, y, 1, st);
+        launch_ring<64, 1, ABHSF_VALUE_F64>(a, x, 1, y, 1, st);
+    return true;
+}
+
+bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st)
+{
+    if (a.ring_warps == 0)
+        return false;
+    if (a.value_type == ABHSF_VALUE_F32) {
+        if (a.s == 32)
+            launch_ring<32, 1, ABHSF_VALUE_F32>(a, x, 1, y, 1, st);
+        else
+            launch_ring<64, 1, ABHSF_VALUE_F32>(a, x, 1, y, 1, st);
+    } else if (a.value_type == ABHSF_VALUE_BF16) {
+        if (a.s == 32)
+            launch_ring<32, 1, ABHSF_VALUE_BF16>(a, x, 1, y, 1, st);
+        else
+            launch_ring<64, 1, ABHSF_VALUE_BF16>(a, x, 1, y, 1, st);
+    } else {
+        return false;
+    }
     return true;
 }
 
 bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,
                    cudaStream_t st)
 {
-    if (a.ring_warps == 0)
+    if (a.ring_warps == 0 || a.value_type != ABHSF_VALUE_F64)
         return false;
     if (a.s == 32)
         spmm_ring<32>(a, k, X, ldx, Y, ldy, st);

@@ -126,6 +126,15 @@ class AbhsfMatrix:
             self._check_vec(x, y, np.float64, x.size, y.size, x.flags.c_contiguous and y.flags.c_contiguous)
             capi.check(capi.lib.abhsf_spmv_host(self._h, x.ctypes.data, y.ctypes.data, _stream_ptr(stream)))
 
+    def spmv_f32(self, x, y, stream=None) -> None:
+        """y += A x in f32 (matrix stored as f32 or bf16); CUDA float32
+        tensors, asynchronous on the stream."""
+        self._check_open()
+        if not (_is_cuda(x) and _is_cuda(y)):
+            raise capi.InvalidValue(capi.INVALID_VALUE, "x and y must be CUDA tensors")
+        self._check_vec(x, y, torch.float32, x.numel(), y.numel(), x.is_contiguous() and y.is_contiguous())
+        capi.check(capi.lib.abhsf_spmv_f32(self._h, x.data_ptr(), y.data_ptr(), _stream_ptr(stream)))
+
     def spmm(self, X, Y, stream=None) -> None:
         """Y += A X for 2-D CUDA float64 tensors X (n x k) and Y (m x k) whose
         rows are contiguous (stride 1 along k), asynchronous on the stream."""
@@ -144,7 +153,7 @@ class AbhsfMatrix:
 
     def _check_vec(self, x, y, dtype, nx, ny, contiguous):
         if x.dtype != dtype or y.dtype != dtype:
-            raise capi.InvalidValue(capi.INVALID_VALUE, f"x and y must be float64, got {x.dtype}, {y.dtype}")
+            raise capi.InvalidValue(capi.INVALID_VALUE, f"x and y must be {dtype}, got {x.dtype}, {y.dtype}")
         if nx != self.n or ny != self.m:
             raise capi.InvalidValue(capi.INVALID_VALUE, f"x must have n={self.n} and y m={self.m} entries")
         if not contiguous:
@@ -263,3 +272,41 @@ def block_select_scheme(r: int, s: int, nnz: int, bits_per_value: int = 64, is_b
                         allow_csr: bool = True) -> str:
     return capi.SCHEME_NAMES[capi.lib.abhsf_block_select_scheme(r, s, nnz, bits_per_value, int(is_binary),
                                                                 int(allow_csr))]
+
+
+def _info(i: "capi.CgInfo") -> dict:
+    return {"iterations": int(i.iterations), "outer_iterations": int(i.outer_iterations),
+            "converged": bool(i.converged), "rel_residual": float(i.rel_residual)}
+
+
+def _solver_vectors(A, b, x):
+    if not (_is_cuda(b) and _is_cuda(x)):
+        raise capi.InvalidValue(capi.INVALID_VALUE, "b and x must be CUDA tensors")
+    if b.dtype != torch.float64 or x.dtype != torch.float64 or b.numel() != A.n or x.numel() != A.n:
+        raise capi.InvalidValue(capi.INVALID_VALUE, f"b and x must be float64 with n={A.n} entries")
+    if not (b.is_contiguous() and x.is_contiguous()):
+        raise capi.InvalidValue(capi.INVALID_VALUE, "b and x must be contiguous")
+
+
+def cg(A: AbhsfMatrix, b, x, rtol: float = 1e-10, max_iters: int = 100000, stream=None) -> dict:
+    """Solves A x = b (A SPD, f64) by FP64 conjugate gradients; x (CUDA
+    float64) is the initial guess and receives the solution."""
+    A._check_open()
+    _solver_vectors(A, b, x)
+    info = capi.CgInfo()
+    capi.check(capi.lib.abhsf_cg(A._h, b.data_ptr(), x.data_ptr(), float(rtol), int(max_iters), C.byref(info),
+                                 _stream_ptr(stream)))
+    return _info(info)
+
+
+def cg_mixed(A64: AbhsfMatrix, A_lo: AbhsfMatrix, b, x, rtol: float = 1e-10, max_iters: int = 100000,
+             inner_rtol: float = 1e-5, max_outer: int = 50, stream=None) -> dict:
+    """Solves A x = b by FP64 iterative refinement around an f32 CG on A_lo
+    (the same matrix stored as f32 or bf16); residuals with A64 in FP64."""
+    A64._check_open()
+    A_lo._check_open()
+    _solver_vectors(A64, b, x)
+    info = capi.CgInfo()
+    capi.check(capi.lib.abhsf_cg_mixed(A64._h, A_lo._h, b.data_ptr(), x.data_ptr(), float(rtol), int(max_iters),
+                                       float(inner_rtol), int(max_outer), C.byref(info), _stream_ptr(stream)))
+    return _info(info)

@@ -113,6 +113,15 @@ typedef struct abhsf_build_opts {
 
 typedef struct abhsf_matrix abhsf_matrix;
 
+/* Outcome of abhsf_cg / abhsf_cg_mixed. */
+typedef struct abhsf_cg_info {
+    int32_t iterations;       /* CG iterations (for the mixed solver: inner f32 iterations, all outer steps) */
+    int32_t outer_iterations; /* refinement steps (1 for plain CG) */
+    int32_t converged;        /* rel_residual <= rtol */
+    int32_t reserved;
+    double rel_residual;      /* ||b - A x|| / ||b|| in FP64 with the FP64 matrix, at return */
+} abhsf_cg_info;
+
 typedef struct abhsf_stats {
     int64_t m, n, nnz;
     int32_t block_size, value_type;
@@ -143,6 +152,33 @@ ABHSF_API abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, con
 /* y += A x, x[n] and y[m] float64 in device memory; matrix stored as f64.
  * Replaces spmv(x, y) (spmv/bottlenecks/spmv.cpp:58-64, spmv/orig/88.cpp:204-236). */
 ABHSF_API abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double* y, abhsf_stream_t stream);
+
+/* y += A x in f32 for a matrix stored as f32 or bf16: x[n], y[m] float in
+ * device memory, values widened to f32, each product and each sum rounded to
+ * f32, per row in the reference's column order.  Block sizes 32 and 64.  The
+ * reference's f32 kernels (spmv/orig/88.cpp:204-236, value type float) are
+ * the counterpart. */
+ABHSF_API abhsf_status abhsf_spmv_f32(const abhsf_matrix* a, const float* x, float* y, abhsf_stream_t stream);
+
+/* Solves A x = b by conjugate gradients in FP64 (A symmetric positive
+ * definite, stored as f64): b[n] and x[n] in device memory, x holding the
+ * initial guess on entry.  Stops when the recurrence residual reaches
+ * rtol * ||b|| or after max_iters iterations; info gets the true residual.
+ * Ordered after the work queued on stream; returns when the solve is done.
+ * No reference counterpart (the reference has SpMV only); this is the
+ * solver its SpMV serves. */
+ABHSF_API abhsf_status abhsf_cg(const abhsf_matrix* a, const double* b, double* x, double rtol, int32_t max_iters,
+                                abhsf_cg_info* info, abhsf_stream_t stream);
+
+/* The same system solved by FP64 iterative refinement around an f32 CG:
+ * each outer step normalises the FP64 residual r = b - A x (computed with
+ * the f64 matrix a64), solves a_lo d = r / ||r|| in f32 (a_lo: the same
+ * matrix stored as f32 or bf16, block size 32 or 64) to inner_rtol, and adds
+ * ||r|| d to x in FP64.  Stops when ||b - A x|| <= rtol ||b||, after
+ * max_outer steps, or after max_iters inner iterations in total. */
+ABHSF_API abhsf_status abhsf_cg_mixed(const abhsf_matrix* a64, const abhsf_matrix* a_lo, const double* b, double* x,
+                                      double rtol, int32_t max_iters, double inner_rtol, int32_t max_outer,
+                                      abhsf_cg_info* info, abhsf_stream_t stream);
 
 /* Y += A X for k right-hand sides, X (n x k) and Y (m x k) float64 row-major
  * in device memory: element (i, j) of X at X[i * ldx + j], ldx >= k, and the

@@ -545,6 +545,26 @@ void orc_spmv_elements(const int64_t* rows, const int64_t* cols, const double* v
         y[rows[k]] += vals[k] * x[cols[k]];
 }
 
+/* Values as a matrix stored as f32 (vt 1) or bf16 (vt 2) holds them, widened
+ * to f32: what an f32 SpMV multiplies. */
+void orc_values_as_f32(const double* v, int64_t n, int vt, float* out)
+{
+    for (int64_t k = 0; k < n; ++k)
+        out[k] = vt == ORC_VAL_F32 ? orc_f64_to_f32(v[k]) : (float)orc_bf16_to_f64(orc_f64_to_bf16(v[k]));
+}
+
+/* The same loop in f32 for matrices stored as f32 or bf16 (vals already
+ * converted to f32): each product and each sum rounded to f32, the order of
+ * the reference's loop (spmv/unified/spmv.cpp:1195-1201) kept. */
+void orc_spmv_elements_f32(const int64_t* rows, const int64_t* cols, const float* vals,
+                           int64_t nnz, const float* x, float* y)
+{
+    for (int64_t k = 0; k < nnz; ++k) {
+        const float p = vals[k] * x[cols[k]];
+        y[rows[k]] = y[rows[k]] + p;
+    }
+}
+
 void orc_abs_spmv_elements(const int64_t* rows, const int64_t* cols, const double* vals,
                            int64_t nnz, const double* x, double* out)
 {

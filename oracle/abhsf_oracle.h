@@ -111,6 +111,11 @@ void orc_abs_spmv_elements(const int64_t* rows, const int64_t* cols, const doubl
 
 /* Value conversions the format declares: f32 = RN(f64); bf16 = RNE(f32). */
 float orc_f64_to_f32(double v);
+/* Values as stored in an f32 (vt 1) or bf16 (vt 2) matrix, widened to f32. */
+void orc_values_as_f32(const double* v, int64_t n, int vt, float* out);
+/* y += A x in f32, element order, product and sum each rounded to f32. */
+void orc_spmv_elements_f32(const int64_t* rows, const int64_t* cols, const float* vals,
+                           int64_t nnz, const float* x, float* y);
 uint16_t orc_f64_to_bf16(double v);
 double orc_bf16_to_f64(uint16_t b);
 

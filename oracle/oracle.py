@@ -87,6 +87,11 @@ def lib() -> C.CDLL:
         for name in ("orc_spmv_elements", "orc_abs_spmv_elements"):
             getattr(L, name).restype = None
             getattr(L, name).argtypes = [_i64p, _i64p, _f64p, C.c_int64, _f64p, _f64p]
+        f32p = C.POINTER(C.c_float)
+        L.orc_spmv_elements_f32.restype = None
+        L.orc_spmv_elements_f32.argtypes = [_i64p, _i64p, f32p, C.c_int64, f32p, f32p]
+        L.orc_values_as_f32.restype = None
+        L.orc_values_as_f32.argtypes = [_f64p, C.c_int64, C.c_int, f32p]
         _lib = L
     return _lib
 
@@ -220,6 +225,26 @@ def spmv_elements(rows, cols, vals, x, y=None) -> np.ndarray:
         y = np.zeros(int(rows.max()) + 1 if rows.size else 0, dtype=np.float64)
     lib().orc_spmv_elements(_p(rows, _i64p), _p(cols, _i64p), _p(vals, _f64p), rows.size,
                             _p(x, _f64p), _p(y, _f64p))
+    return y
+
+
+def values_as_f32(vals, value_type: str) -> np.ndarray:
+    """Values as a matrix stored as `value_type` ("f32" / "bf16") holds them,
+    widened to f32 (orc_values_as_f32)."""
+    v = np.ascontiguousarray(vals, dtype=np.float64)
+    out = np.empty(v.size, dtype=np.float32)
+    lib().orc_values_as_f32(_p(v, _f64p), v.size, VALUE_TYPES[value_type], _p(out, C.POINTER(C.c_float)))
+    return out
+
+
+def spmv_elements_f32(rows, cols, vals_f32, x_f32, y_f32) -> np.ndarray:
+    """The element-order loop in f32 (orc_spmv_elements_f32)."""
+    rows, cols = _i64(rows), _i64(cols)
+    vals = np.ascontiguousarray(vals_f32, dtype=np.float32)
+    x = np.ascontiguousarray(x_f32, dtype=np.float32)
+    y = np.array(y_f32, dtype=np.float32, copy=True)
+    f32p = C.POINTER(C.c_float)
+    lib().orc_spmv_elements_f32(_p(rows, _i64p), _p(cols, _i64p), _p(vals, f32p), rows.size, _p(x, f32p), _p(y, f32p))
     return y
 
 
