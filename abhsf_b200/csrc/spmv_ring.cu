@@ -7,28 +7,32 @@
 // columns ascending, onto y[row], each product rounded before its add.  This
 // kernel keeps that order and so returns y bitwise equal to the reference's.
 //
-// A CTA is s / 32 warps; warp w owns rows 32 w .. 32 w + 31 of every tile.  At
-// build time the non-empty block rows are dealt to the CTAs (longest
-// processing time first, by the bytes each block row moves) and every CTA gets
-// its tiles as a list of 32-byte descriptors, in block-row order.  The CTA
-// streams its tiles through a ring in shared memory, several tiles ahead of
-// the one being summed: one thread issues a bulk copy (cp.async.bulk) each for
-// the tile's index payload and its values, the threads copy the x segment and
-// -- for the first tile of a block row -- the y segment with 8-byte cp.async,
-// and all of it completes on the queue slot's mbarrier.  Every wait on an
-// mbarrier is bounded: a wait that runs out sets ABHSF_DEVSTAT_WAIT_TIMEOUT in
-// the matrix's status word, the CTA waits (again bounded) for the copies it
-// still has in flight, and returns.
+// A CTA is s / 32 consumer warps and one producer warp; consumer warp w owns
+// rows 32 w .. 32 w + 31 of every tile, one row per lane, and keeps the row's
+// accumulator in a register for the whole block row.  At build time the
+// non-empty block rows are dealt to the CTAs (longest processing time first,
+// by the bytes each block row moves) and every CTA gets its tiles as a list
+// of 32-byte descriptors, in block-row order.  The producer streams them
+// through a ring in shared memory several slots ahead of the consumers.  A
+// slot carries one tile, or a group of up to kGroupMax small tiles that are
+// contiguous in the format arrays: their descriptors, the y blocks of the
+// tiles that start a block row, one x block per tile (8- or 4-byte cp.async by
+// the producer lanes), and one bulk copy (cp.async.bulk) each for the group's
+// index payloads and values, all completing on the slot's mbarrier.  Every
+// wait on an mbarrier is bounded: a wait that runs out sets
+// ABHSF_DEVSTAT_WAIT_TIMEOUT in the matrix's status word, the CTA waits (again
+// bounded) for the copies it still has in flight, and returns.
 //
-// Summing a bitmap tile, a lane owns one row: it walks the row's bits in
-// column order and adds v * x onto the row's accumulator, where the value sits
-// at the row's first value (a warp scan of the rows' popcounts) plus the set
-// bits before it, and x[c] is a broadcast read of the staged x segment.  A
-// dense tile is summed the same way with the lanes skewed by one column each,
-// so that the row-major values do not meet in one bank; its stored zeros are
-// skipped (an exact identity for the sum).  COO and CSR tiles go 32 elements
-// at a time: each lane forms one product, and the first lane of each row
-// segment adds the segment onto the row in element order.
+// Summing a bitmap tile, a lane walks its row's bits in column order and adds
+// v * x, where the value sits at the row's first value (a warp scan of the
+// rows' popcounts) plus the set bits before it, and x[c] is a broadcast read
+// of the staged x block.  A dense tile is summed the same way with the lanes
+// skewed by one column each, so that the row-major values do not meet in one
+// bank; its stored zeros are skipped (an exact identity for the sum).  A CSR
+// tile gives each lane its row's range in row_end.  A COO tile of up to 32
+// elements hands each element's product to its row's lane by warp shuffles,
+// in key order; a larger one first marks where each row's run of keys starts
+// and ends.  In every case a row's products are added in column order.
 //
 // With K right-hand sides (X and Y row-major, leading dimensions ldx / ldy)
 // a slot holds the tile's S x K block of X (and of Y at a block row's start),
@@ -49,10 +53,11 @@ namespace {
 #define ABHSF_RING_CTAS 5
 #endif
 #ifndef ABHSF_RING_Q
-#define ABHSF_RING_Q 8
+#define ABHSF_RING_Q 24
 #endif
 constexpr int kCtasPerSm = ABHSF_RING_CTAS;  // resident CTAs per SM
 constexpr int kMaxQ = ABHSF_RING_Q;          // tiles in flight per CTA (queue slots, one mbarrier each)
+static_assert(kMaxQ <= 32, "the producer keeps one queue slot's ring offset per lane");
 constexpr uint32_t kWaitPolls = 1u << 21;      // try_wait polls of at most ~1 us each
 #ifndef ABHSF_RING_TILE_COST
 #define ABHSF_RING_TILE_COST 32768
@@ -98,8 +103,7 @@ struct val_traits<ABHSF_VALUE_BF16> {
 template <int S, int K, int VT>
 constexpr int ring_overhead()
 {
-    using T = typename val_traits<VT>::T;
-    return kMaxQ * (48 + 16) + (S * K + (S / 32) * 32) * (int)sizeof(T) + 64;
+    return kMaxQ * (48 + 16) + (S / 32) * 64 * 4 + 64;
 }
 
 // The ring: the shared memory of an SM (228 KiB, 1 KiB of it reserved per
@@ -111,13 +115,31 @@ constexpr int ring_bytes()
     return ((233472 / kCtasPerSm - 2048 - ring_overhead<S, K, VT>()) / 16) * 16;
 }
 
-// The largest slot of a single-right-hand-side pass: y and x segments, a COO
-// payload of s * s keys (2 bytes each), s * s values and one granule of
-// alignment slack.  Every matrix can take that pass.
+// Small consecutive tiles travel together: a queue slot carries up to
+// kGroupMax tiles whose payloads and values are contiguous in the format
+// arrays, while their slot bytes stay within kGroupBytes (a larger tile
+// travels alone).
+#ifndef ABHSF_RING_GROUP_MAX
+#define ABHSF_RING_GROUP_MAX 16
+#endif
+#ifndef ABHSF_RING_GROUP_BYTES
+#define ABHSF_RING_GROUP_BYTES 12288
+#endif
+constexpr int kGroupMax = ABHSF_RING_GROUP_MAX;
+constexpr int kGroupBytes = ABHSF_RING_GROUP_BYTES;
+#ifndef ABHSF_RING_SINGLE_BYTES
+#define ABHSF_RING_SINGLE_BYTES (ABHSF_RING_GROUP_BYTES / 2)
+#endif
+constexpr int kSingleBytes = ABHSF_RING_SINGLE_BYTES;  // a first tile above this travels alone
+
+// The largest slot of a single tile in a single-right-hand-side pass: its
+// descriptor, y and x segments, a COO payload of s * s keys (2 bytes each),
+// s * s values and one granule of alignment slack.  Every matrix can take
+// that pass.
 template <int S, int VT>
 constexpr int max_slot_bytes()
 {
-    return 2 * S * (int)sizeof(typename val_traits<VT>::T) + 2 * S * S +
+    return 32 + 2 * S * (int)sizeof(typename val_traits<VT>::T) + 2 * S * S +
            (int)sizeof(typename val_traits<VT>::V) * S * S + 16;
 }
 static_assert(max_slot_bytes<64, ABHSF_VALUE_F64>() <= ring_bytes<64, 1, ABHSF_VALUE_F64>() &&
@@ -126,21 +148,25 @@ static_assert(max_slot_bytes<64, ABHSF_VALUE_F64>() <= ring_bytes<64, 1, ABHSF_V
                   max_slot_bytes<64, ABHSF_VALUE_BF16>() <= ring_bytes<64, 1, ABHSF_VALUE_BF16>(),
               "the ring holds any single-right-hand-side slot");
 
-// What the producer tells the consumers about a queued tile.
+// What the producer tells the consumers about a queued group.  The slot holds
+// the group's descriptors, the y blocks of its tiles that start a block row,
+// one x block per tile, the payload block and the value block.
 struct __align__(16) slot_rec {
-    ring_desc d;
-    uint32_t off;  // ring offset of the tile's slot
-    uint32_t pad[3];
+    int64_t io0;    // payload offset of the group's first tile
+    int64_t vbase;  // value index at the start of the value block
+    uint32_t off;   // ring offset of the slot
+    int32_t ntiles;
+    int32_t y_off, x_off, pay_off, val_off;  // parts, relative to the slot
 };
+static_assert(sizeof(slot_rec) == 48, "slot_rec is 48 bytes");
 
 template <int S, int K, int VT>
 struct ring_smem {
     alignas(16) uint8_t ring[ring_bytes<S, K, VT>()];
-    slot_rec rec[kMaxQ];              // queue slot i % kMaxQ
+    slot_rec rec[kMaxQ];              // queue slot g % kMaxQ
     unsigned long long full[kMaxQ];   // the slot's copies have landed
     unsigned long long empty[kMaxQ];  // the consumers are done with the slot
-    typename val_traits<VT>::T ys[S * K];        // the block row's y block, row-major
-    typename val_traits<VT>::T buf[S / 32][32];  // each consumer warp's products of a COO / CSR chunk
+    int rng[S / 32][64];              // each consumer warp's COO row ranges: first, end
     int abort;                        // a wait ran out: everyone stops
 };
 
@@ -152,13 +178,8 @@ struct ring_args {
     void* y;        // Y (T), row-major: element (i, j) at y[i * ldy + j]
     int64_t ldx, ldy;
     int* status;     // ABHSF_DEVSTAT_* bits
-    int64_t drop;    // test hook: descriptor whose bulk copies are not issued (-1: none)
+    int64_t drop;    // test hook: a descriptor whose group's bulk copies are not issued (-1: none)
     uint32_t polls;  // bound of every mbarrier wait
-};
-
-// Byte offsets of a slot's parts.  Every part is a multiple of 16 bytes.
-struct slot_geo {
-    int x, pay, val, size;
 };
 
 // Values before the tile's first value in its first 16-byte granule.
@@ -168,27 +189,7 @@ __host__ __device__ __forceinline__ int lead(const ring_desc& d)
     return (int)(d.vo & (16 / (int)sizeof(typename val_traits<VT>::V) - 1));
 }
 
-template <int S, int K, int VT>
-__host__ __device__ __forceinline__ slot_geo geometry(const ring_desc& d)
-{
-    constexpr int TB = sizeof(typename val_traits<VT>::T), VB = sizeof(typename val_traits<VT>::V), G = 16 / VB;
-    slot_geo g;
-    g.x = (d.info & kFirst) ? S * K * TB : 0;  // the y block comes first
-    g.pay = g.x + S * K * TB;
-    g.val = g.pay + (int)(d.pb_sch & 0xffffffu);
-    // values are copied in 16-byte granules from the granule holding value vo
-    const int span = ((int)(d.vo & (G - 1)) + (int)d.nv + G - 1) & ~(G - 1);
-    g.size = g.val + span * VB;
-    return g;
-}
-
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// 8-byte copy; src_bytes = 0 writes zeros (src must still be a valid address)
-__device__ __forceinline__ void cp8(uint32_t dst, const void* src, int src_bytes)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
-}
 
 // The mbarrier sees one arrival when this thread's earlier cp.async copies land.
 __device__ __forceinline__ void cp_arrive(unsigned long long* bar)
@@ -262,47 +263,81 @@ __device__ __forceinline__ void cp_elem(uint32_t dst, const T* src, int src_byte
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 
-// Producer warp: queues tile d's slot at ring offset off as queue slot q; it
-// completes on full[q].
+// A group the producer warp has formed: lane j < ntiles holds tile j's
+// descriptor (d) and the index of its y block (yk).
+struct group_geo {
+    int ntiles, y_off, x_off, pay_off, val_off, size;
+    int64_t io0, vbase;
+    uint32_t pay_bytes, val_bytes;
+};
+
+// Producer warp: queues the group's slot at ring offset off as queue slot q;
+// it completes on full[q].
 template <int S, int K, int VT>
-__device__ __forceinline__ void issue(const ring_args& P, const ring_desc& d, const slot_geo& g, uint32_t off, int q,
-                                      ring_smem<S, K, VT>& sm, int64_t e, int lane)
+__device__ __forceinline__ void issue_group(const ring_args& P, const ring_desc& d, int yk, const group_geo& gg,
+                                            uint32_t off, int q, ring_smem<S, K, VT>& sm, bool drop, int lane)
 {
     using T = typename val_traits<VT>::T;
     using V = typename val_traits<VT>::V;
-    constexpr int TB = sizeof(T);
-    const uint32_t base = smem_addr(sm.ring + off);
+    constexpr int TB = sizeof(T), XB = S * K * TB;
+    uint8_t* slot = sm.ring + off;
+    const uint32_t base = smem_addr(slot);
     unsigned long long* bar = &sm.full[q];
+    if (lane < gg.ntiles)
+        reinterpret_cast<ring_desc*>(slot)[lane] = d;
+    __syncwarp();  // lane 0's arrival below publishes every lane's descriptor
     const T* X = static_cast<const T*>(P.x);
     const T* Y = static_cast<const T*>(P.y);
-    if (d.info & kFirst) {
-        const int64_t r0 = (int64_t)(d.info & kRowMask) * S;
+    const int total = gg.ntiles * S * K;
+    if (gg.ntiles == 1) {  // lane 0 holds the tile's descriptor
+        const uint32_t col = __shfl_sync(kFull, d.col, 0), info = __shfl_sync(kFull, d.info, 0);
+        const int64_t c0 = (int64_t)col * S, r0 = (int64_t)(info & kRowMask) * S;
 #pragma unroll
         for (int k = lane; k < S * K; k += 32) {
-            const int r = k / K, j = k % K;
-            const bool ok = r0 + r < P.A.m;
-            cp_elem(base + TB * k, ok ? Y + (r0 + r) * P.ldy + j : Y, ok ? TB : 0);
+            const int c = k / K, h = k % K;
+            const bool okx = c0 + c < P.A.n;
+            cp_elem(base + gg.x_off + TB * k, okx ? X + (c0 + c) * P.ldx + h : X, okx ? TB : 0);
+            if (info & kFirst) {
+                const bool oky = r0 + c < P.A.m;
+                cp_elem(base + gg.y_off + TB * k, oky ? Y + (r0 + c) * P.ldy + h : Y, oky ? TB : 0);
+            }
         }
     }
-    const int64_t c0 = (int64_t)d.col * S;
-#pragma unroll
-    for (int k = lane; k < S * K; k += 32) {
-        const int c = k / K, j = k % K;
-        const bool ok = c0 + c < P.A.n;
-        cp_elem(base + g.x + TB * k, ok ? X + (c0 + c) * P.ldx + j : X, ok ? TB : 0);
+    for (int e0 = 0; gg.ntiles > 1 && e0 < total; e0 += 32) {
+        const int e = e0 + lane, jj = (e / (S * K)) & 31, k = e % (S * K);
+        const uint32_t col = __shfl_sync(kFull, d.col, jj);
+        const uint32_t info = __shfl_sync(kFull, d.info, jj);
+        const int ykk = __shfl_sync(kFull, yk, jj);
+        if (e < total) {
+            const int c = k / K, h = k % K;
+            const int64_t c0 = (int64_t)col * S;
+            const bool okx = c0 + c < P.A.n;
+            cp_elem(base + gg.x_off + jj * XB + TB * k, okx ? X + (c0 + c) * P.ldx + h : X, okx ? TB : 0);
+            if (info & kFirst) {
+                const int64_t r0 = (int64_t)(info & kRowMask) * S;
+                const bool oky = r0 + c < P.A.m;
+                cp_elem(base + gg.y_off + ykk * XB + TB * k, oky ? Y + (r0 + c) * P.ldy + h : Y, oky ? TB : 0);
+            }
+        }
     }
     cp_arrive(bar);
     if (lane == 0) {
-        sm.rec[q].d = d;
-        sm.rec[q].off = off;
-        const uint32_t pb = (uint32_t)(g.val - g.pay), vb = (uint32_t)(g.size - g.val);
-        mbar_expect_tx(bar, pb + vb);  // also publishes rec[q]
-        if (e != P.drop) {
+        slot_rec& r = sm.rec[q];
+        r.io0 = gg.io0;
+        r.vbase = gg.vbase;
+        r.off = off;
+        r.ntiles = gg.ntiles;
+        r.y_off = gg.y_off;
+        r.x_off = gg.x_off;
+        r.pay_off = gg.pay_off;
+        r.val_off = gg.val_off;
+        mbar_expect_tx(bar, gg.pay_bytes + gg.val_bytes);  // also publishes rec[q] and the descriptors
+        if (!drop) {
             // the slot's bytes were last read through the generic proxy
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (pb)
-                bulk_g2s(base + g.pay, P.A.payload + d.io, pb, bar);
-            bulk_g2s(base + g.val, static_cast<const V*>(P.A.values) + (d.vo - lead<VT>(d)), vb, bar);
+            if (gg.pay_bytes)
+                bulk_g2s(base + gg.pay_off, P.A.payload + gg.io0, gg.pay_bytes, bar);
+            bulk_g2s(base + gg.val_off, static_cast<const V*>(P.A.values) + gg.vbase, gg.val_bytes, bar);
         }
     }
 }
@@ -340,19 +375,17 @@ __device__ __forceinline__ int warp_sum(int v)
 // Bitmap tile, row `row` = 32 warp + lane.  Row r's bits are u32 words
 // r * W .. r * W + W - 1 (W = S / 32), bit b of word j = column 32 j + b.
 template <int S, int K, int VT>
-__device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& g, int parity,
-                                           typename val_traits<VT>::T* ys, int warp, int lane)
+__device__ __forceinline__ void sum_bitmap(const typename val_traits<VT>::T* xs, const uint8_t* pay,
+                                           const typename val_traits<VT>::V* vs,
+                                           typename val_traits<VT>::T (&acc)[K], int warp, int lane)
 {
     using T = typename val_traits<VT>::T;
-    using V = typename val_traits<VT>::V;
     constexpr int W = S / 32;
-    const T* xs = reinterpret_cast<const T*>(slot + g.x);
-    const V* vs = reinterpret_cast<const V*>(slot + g.val) + parity;
     const int row = 32 * warp + lane;
     uint32_t w[W];
     int cnt = 0, before = 0;
     if (W == 2) {
-        const uint2* bm = reinterpret_cast<const uint2*>(slot + g.pay);
+        const uint2* bm = reinterpret_cast<const uint2*>(pay);
         const uint2 ww = bm[row];
         w[0] = ww.x;
         w[W - 1] = ww.y;
@@ -361,16 +394,12 @@ __device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& 
             before = warp_sum(__popc(u.x) + __popc(u.y));
         }
     } else {
-        w[0] = reinterpret_cast<const uint32_t*>(slot + g.pay)[row];
+        w[0] = reinterpret_cast<const uint32_t*>(pay)[row];
     }
 #pragma unroll
     for (int j = 0; j < W; ++j)
         cnt += __popc(w[j]);
     int q = before + warp_inclusive_sum(cnt, lane) - cnt;
-    T acc[K];
-#pragma unroll
-    for (int h = 0; h < K; ++h)
-        acc[h] = ys[row * K + h];
 #pragma unroll
     for (int j = 0; j < W; ++j) {
 #pragma unroll
@@ -388,26 +417,17 @@ __device__ __forceinline__ void sum_bitmap(const uint8_t* slot, const slot_geo& 
             }
         }
     }
-#pragma unroll
-    for (int h = 0; h < K; ++h)
-        ys[row * K + h] = acc[h];
 }
 
 // Dense tile: all S * S values, row-major.  Lane l runs l columns behind
 // lane 0 so that the lanes' values fall in different banks.
 template <int S, int K, int VT>
-__device__ __forceinline__ void sum_dense(const uint8_t* slot, const slot_geo& g, int parity,
-                                          typename val_traits<VT>::T* ys, int warp, int lane)
+__device__ __forceinline__ void sum_dense(const typename val_traits<VT>::T* xs,
+                                          const typename val_traits<VT>::V* vs,
+                                          typename val_traits<VT>::T (&acc)[K], int warp, int lane)
 {
     using T = typename val_traits<VT>::T;
-    using V = typename val_traits<VT>::V;
-    const T* xs = reinterpret_cast<const T*>(slot + g.x);
-    const V* vs = reinterpret_cast<const V*>(slot + g.val) + parity;
     const int row = 32 * warp + lane;
-    T acc[K];
-#pragma unroll
-    for (int h = 0; h < K; ++h)
-        acc[h] = ys[row * K + h];
 #pragma unroll 4
     for (int k = 0; k < S + 31; ++k) {
         const int c = k - lane;
@@ -420,123 +440,116 @@ __device__ __forceinline__ void sum_dense(const uint8_t* slot, const slot_geo& g
             }
         }
     }
-#pragma unroll
-    for (int h = 0; h < K; ++h)
-        ys[row * K + h] = acc[h];
 }
 
-// COO / CSR tile: this warp's rows' elements, 32 at a time.
+// COO / CSR tile, row `row` = 32 warp + lane: the lane adds its row's
+// elements in stored order (columns ascending).  A CSR tile gives each row's
+// range in its row_end array; for a COO tile the warp first marks where each
+// of its rows starts and ends in the sorted keys.
 template <int S, int K, int VT, bool CSR>
-__device__ __forceinline__ void sum_stream(const uint8_t* slot, const slot_geo& g, int parity, int z,
-                                           typename val_traits<VT>::T* ys, typename val_traits<VT>::T* buf, int warp,
-                                           int lane)
+__device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs, const uint8_t* pay,
+                                           const typename val_traits<VT>::V* vs, int z,
+                                           typename val_traits<VT>::T (&acc)[K], int* rng, int warp, int lane)
+{
+    using T = typename val_traits<VT>::T;
+    constexpr int LG = S == 32 ? 5 : 6;
+    const uint16_t* key16 = reinterpret_cast<const uint16_t*>(pay);  // COO keys / CSR row ends
+    const uint8_t* col8 = pay + 2 * S;                                // CSR local columns
+    const int row = 32 * warp + lane;
+    if (!CSR && z <= 32) {
+        // few elements: element lane k forms its product, and each row lane
+        // takes the products of its row from the element lanes in key order
+        int rk = -1, ck = 0;
+        T vk = T(0);
+        if (lane < z) {
+            const uint32_t key = key16[lane];
+            rk = (int)(key >> LG);
+            ck = (int)(key & (S - 1));
+            vk = widen(vs[lane]);
+        }
+        T pk[K];
+#pragma unroll
+        for (int h = 0; h < K; ++h)
+            pk[h] = lane < z ? fmul(vk, xs[ck * K + h]) : T(0);
+        for (int k = 0; k < z; ++k) {
+            const int r = __shfl_sync(kFull, rk, k);
+#pragma unroll
+            for (int h = 0; h < K; ++h) {
+                const T p = __shfl_sync(kFull, pk[h], k);
+                if (r == row)
+                    acc[h] = fadd(acc[h], p);
+            }
+        }
+        return;
+    }
+    int lo, hi;
+    if (CSR) {
+        lo = row > 0 ? key16[row - 1] : 0;
+        hi = key16[row];
+    } else {
+        // every element whose row is one of this warp's marks where the row
+        // starts and ends (keys sorted by row, so a row's elements are a run)
+        rng[lane] = 0;
+        rng[32 + lane] = 0;
+        __syncwarp();
+        for (int k = lane; k < z; k += 32) {
+            const int rk = key16[k] >> LG;
+            const int r = rk - 32 * warp;
+            if (r >= 0 && r < 32) {
+                if (k == 0 || (key16[k - 1] >> LG) != rk)
+                    rng[r] = k;
+                if (k + 1 == z || (key16[k + 1] >> LG) != rk)
+                    rng[32 + r] = k + 1;
+            }
+        }
+        __syncwarp();
+        lo = rng[lane];
+        hi = rng[32 + lane];
+        __syncwarp();  // read before the next tile rewrites rng
+    }
+    for (int k = lo; k < hi; ++k) {
+        const int c = CSR ? (int)col8[k] : (int)(key16[k] & (S - 1));
+        const T v = widen(vs[k]);
+#pragma unroll
+        for (int h = 0; h < K; ++h)
+            acc[h] = fadd(acc[h], fmul(v, xs[c * K + h]));
+    }
+}
+
+// Adds tile j of a queued group onto the lane's row accumulators; the first
+// tile of a block row loads them from its y block, the last writes them to y.
+template <int S, int K, int VT>
+__device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot, const slot_rec& r, int j, int& yk,
+                                         ring_smem<S, K, VT>& sm, typename val_traits<VT>::T (&acc)[K], int warp,
+                                         int lane)
 {
     using T = typename val_traits<VT>::T;
     using V = typename val_traits<VT>::V;
-    constexpr int LG = S == 32 ? 5 : 6;
-    const T* xs = reinterpret_cast<const T*>(slot + g.x);
-    const V* vs = reinterpret_cast<const V*>(slot + g.val) + parity;
-    const uint16_t* key16 = reinterpret_cast<const uint16_t*>(slot + g.pay);  // COO keys / CSR row ends
-    const uint8_t* col8 = slot + g.pay + 2 * S;                                // CSR local columns
-    int lo = 0, hi = z;  // elements of rows 32 warp .. 32 warp + 31 (sorted by row)
-    if (S == 64) {
-        int split;  // first element of row 32 or later
-        if (CSR) {
-            split = key16[31];
-        } else if (z <= 32) {
-            split = __popc(__ballot_sync(kFull, lane < z && key16[lane] < (32u << LG)));
-        } else {
-            int a = 0, b = z;
-            while (a < b) {
-                const int mid = (a + b) >> 1;
-                if (key16[mid] < (32u << LG))
-                    a = mid + 1;
-                else
-                    b = mid;
-            }
-            split = a;
-        }
-        if (warp == 0)
-            hi = split;
-        else
-            lo = split;
-    }
-#pragma unroll 1
-    for (int base = lo; base < hi; base += 32) {
-        const int k = base + lane;
-        int lr = S;  // idle lanes: no row
-        int lc = 0;
-        T v = T(0);
-        if (k < hi) {
-            if (CSR) {
-                lc = col8[k];
-                int a = 0, b = S;  // first r with row_end[r] > k
-#pragma unroll
-                for (int step = 0; step <= LG; ++step) {
-                    if (a < b) {
-                        const int mid = (a + b) >> 1;
-                        if ((int)key16[mid] > k)
-                            b = mid;
-                        else
-                            a = mid + 1;
-                    }
-                }
-                lr = a;
-            } else {
-                const uint32_t key = key16[k];
-                lr = (int)(key >> LG);
-                lc = (int)(key & (S - 1));
-            }
-            v = widen(vs[k]);
-        }
-        const int plr = __shfl_up_sync(kFull, lr, 1);
-        const bool head = k < hi && (lane == 0 || plr != lr);
-        const unsigned heads = __ballot_sync(kFull, head);
-        const unsigned later = heads & ~((2u << lane) - 1u);  // heads after this lane (lane 31: none)
-        const int end = later ? __ffs(later) - 1 : min(hi - base, 32);
-#pragma unroll 1
-        for (int h = 0; h < K; ++h) {
-            const T p = k < hi ? fmul(v, xs[lc * K + h]) : T(0);
-            buf[lane] = p;
-            __syncwarp();
-            if (head) {
-                T acc = fadd(ys[lr * K + h], p);
-                for (int e = lane + 1; e < end; ++e)
-                    acc = fadd(acc, buf[e]);
-                ys[lr * K + h] = acc;
-            }
-            __syncwarp();
-        }
-    }
-}
-
-template <int S, int K, int VT>
-__device__ __forceinline__ void sum_tile(const ring_args& P, const ring_desc& d, const uint8_t* slot,
-                                         ring_smem<S, K, VT>& sm, int warp, int lane)
-{
-    using T = typename val_traits<VT>::T;
-    const slot_geo g = geometry<S, K, VT>(d);
-    const int parity = lead<VT>(d);
+    constexpr int XB = S * K * (int)sizeof(T);
+    const ring_desc d = reinterpret_cast<const ring_desc*>(slot)[j];
     const int row = 32 * warp + lane;
     if (d.info & kFirst) {
+        const T* ys = reinterpret_cast<const T*>(slot + r.y_off + yk * XB);
 #pragma unroll
         for (int h = 0; h < K; ++h)
-            sm.ys[row * K + h] = reinterpret_cast<const T*>(slot)[row * K + h];
-        __syncwarp();
+            acc[h] = ys[row * K + h];
+        ++yk;
     }
+    const T* xs = reinterpret_cast<const T*>(slot + r.x_off + j * XB);
+    const uint8_t* pay = slot + r.pay_off + (d.io - r.io0);
+    const V* vs = reinterpret_cast<const V*>(slot + r.val_off) + (d.vo - r.vbase);
     switch (d.pb_sch >> 24) {
-    case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K, VT>(slot, g, parity, sm.ys, warp, lane); break;
-    case ABHSF_SCHEME_DENSE: sum_dense<S, K, VT>(slot, g, parity, sm.ys, warp, lane); break;
-    case ABHSF_SCHEME_CSR: sum_stream<S, K, VT, true>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
-    default: sum_stream<S, K, VT, false>(slot, g, parity, (int)d.nv, sm.ys, sm.buf[warp], warp, lane); break;
+    case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K, VT>(xs, pay, vs, acc, warp, lane); break;
+    case ABHSF_SCHEME_DENSE: sum_dense<S, K, VT>(xs, vs, acc, warp, lane); break;
+    case ABHSF_SCHEME_CSR: sum_sparse<S, K, VT, true>(xs, pay, vs, (int)d.nv, acc, sm.rng[warp], warp, lane); break;
+    default: sum_sparse<S, K, VT, false>(xs, pay, vs, (int)d.nv, acc, sm.rng[warp], warp, lane); break;
     }
     if (d.info & kLast) {
-        __syncwarp();
-        const int64_t r = (int64_t)(d.info & kRowMask) * S + row;
-        if (r < P.A.m) {
+        const int64_t rr = (int64_t)(d.info & kRowMask) * S + row;
+        if (rr < P.A.m) {
 #pragma unroll
             for (int h = 0; h < K; ++h)
-                static_cast<T*>(P.y)[r * P.ldy + h] = sm.ys[row * K + h];
+                static_cast<T*>(P.y)[rr * P.ldy + h] = acc[h];
         }
     }
 }
@@ -563,48 +576,98 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    int issued = 0;  // producer: tiles queued
+    int issued = 0;  // producer: groups queued
     if (warp == NC) {
-        // descriptors of tiles 32 k .. 32 k + 31, lane j holding tile 32 k + j
+        using V = typename val_traits<VT>::V;
+        constexpr int XB = S * K * (int)sizeof(typename val_traits<VT>::T), VB = sizeof(V), G = 16 / VB;
+        // descriptors of tiles wbase .. wbase + 63, lane j holding tiles wbase + j and wbase + 32 + j
         ring_desc cur{}, nxt{};
+        int wbase = 0;
         if (lane < n)
             cur = D[lane];
         if (32 + lane < n)
             nxt = D[32 + lane];
-        int done = 0, head = 0, tail = 0;  // done: tiles the consumers released; ring in use [tail, head)
-        int my_off = 0;                    // lane q: ring offset of the tile in queue slot q
+        int done = 0, head = 0, tail = 0;  // done: groups the consumers released; ring in use [tail, head)
+        int my_off = 0;                    // lane q: ring offset of the group in queue slot q
 #pragma unroll 1
-        for (int i = 0; i < n; ++i) {
-            if (i > 0 && (i & 31) == 0) {
+        for (int i = 0; i < n;) {
+            while (i >= wbase + 32) {
                 cur = nxt;
-                if (i + 32 + lane < n)
-                    nxt = D[i + 32 + lane];
+                wbase += 32;
+                if (wbase + 32 + lane < n)
+                    nxt = D[wbase + 32 + lane];
             }
-            const ring_desc d = shfl_desc(cur, i & 31);
-            const slot_geo g = geometry<S, K, VT>(d);
+            // a tile that would fill most of a group travels alone (every lane holds it)
+            ring_desc d = shfl_desc(cur, i - wbase);
+            const int est0 = 32 + ((d.info & kFirst) ? XB : 0) + XB + (int)(d.pb_sch & 0xffffffu) + (int)d.nv * VB;
+            group_geo gg;
+            int yk = 0;
+            if (est0 > kSingleBytes || kGroupMax == 1) {
+                gg.ntiles = 1;
+                gg.io0 = d.io;
+                gg.vbase = d.vo - lead<VT>(d);
+                gg.pay_bytes = d.pb_sch & 0xffffffu;
+                gg.val_bytes = (uint32_t)(((d.vo + d.nv - gg.vbase + G - 1) & ~(int64_t)(G - 1)) * VB);
+                gg.y_off = 32;
+                gg.x_off = gg.y_off + ((d.info & kFirst) ? XB : 0);
+            } else {
+                // lane j considers tile i + j (within the two windows: i - wbase < 32)
+                const int rel = i - wbase + lane;
+                d = shfl_desc(cur, rel & 31);
+                if (i - wbase + kGroupMax > 32) {  // only then can the group reach the next window
+                    const ring_desc b = shfl_desc(nxt, rel & 31);
+                    if (rel >= 32)
+                        d = b;
+                }
+                const bool have = lane < kGroupMax && i + lane < n;
+                // contiguous with the previous tile in the format arrays?
+                const int64_t pvo = __shfl_up_sync(kFull, d.vo, 1), pio = __shfl_up_sync(kFull, d.io, 1);
+                const uint32_t pnv = __shfl_up_sync(kFull, d.nv, 1), ppb = __shfl_up_sync(kFull, d.pb_sch, 1) & 0xffffffu;
+                const bool contig = lane == 0 || (d.vo == pvo + pnv && d.io == pio + ppb);
+                const bool first = (d.info & kFirst) != 0;
+                const int est = have ? 32 + (first ? XB : 0) + XB + (int)(d.pb_sch & 0xffffffu) + (int)d.nv * VB : 0;
+                const int cum = warp_inclusive_sum(est, lane);
+                const unsigned okm = __ballot_sync(kFull, have && contig && (lane == 0 || cum <= kGroupBytes));
+                const int L = __ffs(~okm) - 1;  // leading tiles that form the group (lane 0 always qualifies)
+                const unsigned firsts = __ballot_sync(kFull, lane < L && first);
+                yk = __popc(firsts & ((1u << lane) - 1u));
+                gg.ntiles = L;
+                gg.io0 = __shfl_sync(kFull, d.io, 0);
+                gg.vbase = __shfl_sync(kFull, d.vo, 0) - __shfl_sync(kFull, lead<VT>(d), 0);
+                const int64_t io_end = __shfl_sync(kFull, d.io + (d.pb_sch & 0xffffffu), L - 1);
+                const int64_t vo_end = __shfl_sync(kFull, d.vo + d.nv, L - 1);
+                gg.pay_bytes = (uint32_t)(io_end - gg.io0);
+                gg.val_bytes = (uint32_t)(((vo_end - gg.vbase + G - 1) & ~(int64_t)(G - 1)) * VB);
+                gg.y_off = 32 * L;
+                gg.x_off = gg.y_off + __popc(firsts) * XB;
+            }
+            const int L = gg.ntiles;
+            gg.pay_off = gg.x_off + L * XB;
+            gg.val_off = gg.pay_off + (int)gg.pay_bytes;
+            gg.size = gg.val_off + (int)gg.val_bytes;
             int off = -1;
 #pragma unroll 1
             for (;;) {
                 if (__any_sync(kFull, *abort != 0))
                     break;
-                if (i - done < kMaxQ) {
-                    if (i == done)
+                if (issued - done < kMaxQ) {
+                    if (issued == done)
                         off = 0;
                     else if (head > tail)
-                        off = head + g.size <= kRingBytes ? head : (g.size <= tail ? 0 : -1);
+                        off = head + gg.size <= kRingBytes ? head : (gg.size <= tail ? 0 : -1);
                     else
-                        off = head + g.size <= tail ? head : -1;
+                        off = head + gg.size <= tail ? head : -1;
                     if (off >= 0)
                         break;
                 }
-                // wait until the oldest queued tile is released
+                // wait until the oldest queued group is released
                 const bool ok =
                     __all_sync(kFull, mbar_wait(&sm.empty[done % kMaxQ], (uint32_t)(done / kMaxQ) & 1u, P.polls));
                 if (!ok)
                     break;
                 ++done;
                 const int oldest = __shfl_sync(kFull, my_off, done % kMaxQ);
-                if (done == i)
+                if (done == issued)
                     head = tail = 0;
                 else
                     tail = oldest;
@@ -614,29 +677,41 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                     *abort = 1;
                 break;
             }
-            issue<S, K, VT>(P, d, g, (uint32_t)off, i % kMaxQ, sm, eb + i, lane);
-            if (lane == i % kMaxQ)
+            const bool drop = P.drop >= eb + i && P.drop < eb + i + L;
+            issue_group<S, K, VT>(P, d, yk, gg, (uint32_t)off, issued % kMaxQ, sm, drop, lane);
+            if (lane == issued % kMaxQ)
                 my_off = off;
-            if (i == done)
+            if (issued == done)
                 tail = 0;
-            head = off + g.size;
-            issued = i + 1;
+            head = off + gg.size;
+            ++issued;
+            i += L;
         }
     } else {
+        typename val_traits<VT>::T acc[K];  // the lane's row of the current block row
+#pragma unroll
+        for (int h = 0; h < K; ++h)
+            acc[h] = 0;
 #pragma unroll 1
-        for (int i = 0; i < n; ++i) {
-            const int q = i % kMaxQ;
-            const bool ok = __all_sync(kFull, mbar_wait(&sm.full[q], (uint32_t)(i / kMaxQ) & 1u, P.polls));
+        for (int g = 0, t = 0; t < n; ++g) {
+            const int q = g % kMaxQ;
+            const bool ok = __all_sync(kFull, mbar_wait(&sm.full[q], (uint32_t)(g / kMaxQ) & 1u, P.polls));
             if (!ok || __any_sync(kFull, *abort != 0)) {
                 if (lane == 0)
                     *abort = 1;
                 break;
             }
             const slot_rec& r = sm.rec[q];
-            sum_tile<S, K, VT>(P, r.d, sm.ring + r.off, sm, warp, lane);
+            const uint8_t* slot = sm.ring + r.off;
+            const int L = r.ntiles;
+            int yk = 0;
+#pragma unroll 1
+            for (int j = 0; j < L; ++j)
+                sum_tile<S, K, VT>(P, slot, r, j, yk, sm, acc, warp, lane);
             __syncwarp();
             if (lane == 0)
                 mbar_arrive(&sm.empty[q]);
+            t += L;
         }
     }
     __syncthreads();
@@ -729,7 +804,8 @@ int ring_ctas_per_sm()
 template <int S, int K, int VT>
 bool ring_fits(const abhsf_matrix& a)
 {
-    return 2 * S * K * (int64_t)sizeof(typename val_traits<VT>::T) + (int64_t)a.ring_max_pv <= ring_bytes<S, K, VT>();
+    return 32 + 2 * S * K * (int64_t)sizeof(typename val_traits<VT>::T) + (int64_t)a.ring_max_pv <=
+           ring_bytes<S, K, VT>();
 }
 
 // Y += A X over columns [0, k) in passes of the largest K that fits.

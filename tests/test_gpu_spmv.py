@@ -198,3 +198,14 @@ def test_tiled_mixture_full_size(gpu, s):
     else:
         yr = reference_order_y(c, x, y0)
     np.testing.assert_array_equal(run_spmv(A, x, y0), yr)
+
+
+def test_tiled_mixture_medium_every_row(gpu):
+    """n = 1,048,576: many block rows made of one small COO tile (most of
+    whose rows have no element) next to bitmap-heavy ones; every row,
+    including the untouched ones, bitwise in the reference order."""
+    c = W.tiled_mixture(n=1048576)
+    A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64)
+    x = np.random.default_rng(3).uniform(-1, 1, c.n)
+    y0 = np.random.default_rng(4).standard_normal(c.m)
+    np.testing.assert_array_equal(run_spmv(A, x, y0), reference_order_y(c, x, y0))
