@@ -146,7 +146,7 @@ abhsf_status abhsf_cg(const abhsf_matrix* a, const double* b, double* x, double 
 }
 
 abhsf_status abhsf_cg_mixed(const abhsf_matrix* a64, const abhsf_matrix* a_lo, const double* b, double* x,
-                            double rtol, int32_t max_iters, double inner_rtol, int32_t max_outer,
+                            double rtol, int32_t max_iters, double update_factor, int32_t max_updates,
                             abhsf_cg_info* info, abhsf_stream_t stream)
 {
     return guarded([&] {
@@ -156,9 +156,9 @@ abhsf_status abhsf_cg_mixed(const abhsf_matrix* a64, const abhsf_matrix* a_lo, c
             fail(ABHSF_ERROR_INVALID_VALUE, "abhsf_cg_mixed needs a64 stored as f64 and a_lo as f32 or bf16");
         if ((!b || !x) && a64->n)
             fail(ABHSF_ERROR_INVALID_VALUE, "b and x must be non-NULL");
-        if (!(rtol >= 0.0) || !(inner_rtol > 0.0 && inner_rtol < 1.0))
-            fail(ABHSF_ERROR_INVALID_VALUE, "rtol must be >= 0 and inner_rtol in (0, 1)");
-        abhsf::cg_solve_mixed(*a64, *a_lo, b, x, rtol, max_iters, inner_rtol, max_outer, info,
+        if (!(rtol >= 0.0) || !(update_factor > 0.0 && update_factor < 1.0))
+            fail(ABHSF_ERROR_INVALID_VALUE, "rtol must be >= 0 and update_factor in (0, 1)");
+        abhsf::cg_solve_mixed(*a64, *a_lo, b, x, rtol, max_iters, update_factor, max_updates, info,
                               reinterpret_cast<cudaStream_t>(stream));
     });
 }

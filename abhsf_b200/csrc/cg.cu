@@ -1,6 +1,7 @@
 // cg.cu -- conjugate gradients on ABHSF matrices: plain FP64, and mixed
-// precision (FP64 iterative refinement around an f32 CG on an f32 or bf16
-// copy of the matrix).
+// precision (an f32 CG on an f32 or bf16 copy of the matrix whose solution
+// accumulates in FP64 and whose residual is replaced by the FP64 residual of
+// the f64 matrix each time it has fallen by a set factor: reliable updates).
 //
 // The reference has no solver; its SpMV is the kernel such a solver calls
 // (spmv/bottlenecks/spmv.cpp:58-64).  Both solvers here keep every scalar
@@ -31,7 +32,7 @@ struct cg_state {
     int done;      // tolerance met, or iteration limit reached
     int iters;     // iterations performed
     int max_iters;
-    int pad;
+    int active;  // this iteration updates x, r and p (done was not set before it)
 };
 
 __device__ __forceinline__ double block_sum(double v)
@@ -81,7 +82,22 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_init(const double* __restric
         st->tol2 = tol2;
         st->iters = 0;
         st->max_iters = max_iters;
+        st->active = 0;
         st->done = (rr <= tol2 || max_iters <= 0) ? 1 : 0;
+    }
+}
+
+// restart the recurrence from a replaced residual: r . r from the partials,
+// the tolerance factor2 * r . r, the search direction and iteration count kept
+__global__ void __launch_bounds__(kRedThreads) k_cg_resume(const double* __restrict__ partial, cg_state* st,
+                                                           double factor2)
+{
+    const double rr = sum_partials(partial);
+    if (threadIdx.x == 0) {
+        const double tol2 = factor2 * rr;
+        st->rr = rr;
+        st->tol2 = tol2;
+        st->done = (rr <= tol2 || st->iters >= st->max_iters) ? 1 : 0;
     }
 }
 
@@ -92,8 +108,10 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_alpha(const double* __restri
         if (st->done || !(pap > 0.0)) {  // converged, or breakdown (p = 0 or A not positive definite on p)
             st->alpha = 0.0;
             st->done = 1;
+            st->active = 0;
         } else {
             st->alpha = st->rr / pap;
+            st->active = 1;
         }
     }
 }
@@ -130,10 +148,12 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_beta(const double* __restric
     }
 }
 
+// p = r + beta p, also in the iteration that met the tolerance, so that a
+// recurrence resumed from a replaced residual continues from the right p
 template <typename T>
 __global__ void k_cg_update_p(int64_t n, T* __restrict__ p, const T* __restrict__ r, const cg_state* st)
 {
-    if (st->done)
+    if (!st->active)
         return;
     const T beta = (T)st->beta;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -147,20 +167,20 @@ __global__ void k_neg(int64_t n, const T* __restrict__ a, T* __restrict__ out)
         out[i] = -a[i];
 }
 
-// r32 = r64 / ||r64|| (rr = r64 . r64 from the state)
-__global__ void k_to_unit_f32(int64_t n, const double* __restrict__ r, float* __restrict__ out, const cg_state* st)
+// out = (float) r
+__global__ void k_to_f32(int64_t n, const double* __restrict__ r, float* __restrict__ out)
 {
-    const double inv = st->rr > 0.0 ? 1.0 / sqrt(st->rr) : 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = (float)(r[i] * inv);
+        out[i] = (float)r[i];
 }
 
-// x += ||r64|| d
-__global__ void k_add_scaled(int64_t n, double* __restrict__ x, const float* __restrict__ d, const cg_state* st)
+// x += d; d = 0 (the f32 correction folded into the FP64 solution)
+__global__ void k_fold(int64_t n, double* __restrict__ x, float* __restrict__ d)
 {
-    const double scale = sqrt(st->rr);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        x[i] += scale * (double)d[i];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += (double)d[i];
+        d[i] = 0.0f;
+    }
 }
 
 unsigned elem_grid(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
@@ -194,50 +214,63 @@ void dot(const T* a, const T* b, int64_t n, double* partial, cudaStream_t st)
     k_dot<T><<<kRedBlocks, kRedThreads, 0, st>>>(n, a, b, partial);
 }
 
-// CG on A x = (current r), starting from x with residual w.r, until r . r <=
-// tol2 or max_iters iterations.  Returns the iterations done.
+// p = r, Ap = 0 and the state from r . r: the start of a CG recurrence.
 template <typename T>
-int cg_iterate(const abhsf_matrix& a, T* x, cg_work<T>& w, int64_t n, cg_state* st_d, cg_state* st_h,
-               double* partial, double tol2, int max_iters, cudaStream_t cs)
+void cg_start(cg_work<T>& w, int64_t n, cg_state* st_d, double* partial, double tol2, int max_iters,
+              cudaStream_t cs)
 {
     ABHSF_CUDA(cudaMemcpyAsync(w.p.get(), w.r.get(), n * sizeof(T), cudaMemcpyDeviceToDevice, cs));
     ABHSF_CUDA(cudaMemsetAsync(w.ap.get(), 0, n * sizeof(T), cs));
     dot<T>(w.r.get(), w.r.get(), n, partial, cs);
     k_cg_init<<<1, kRedThreads, 0, cs>>>(partial, st_d, tol2, max_iters);
     ABHSF_CUDA(cudaGetLastError());
-
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    ABHSF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    for (int it = 0; it < kChunk; ++it) {
-        spmv_t(a, w.p.get(), w.ap.get(), cs);
-        dot<T>(w.p.get(), w.ap.get(), n, partial, cs);
-        k_cg_alpha<<<1, kRedThreads, 0, cs>>>(partial, st_d);
-        k_cg_update_xr<T><<<kRedBlocks, kRedThreads, 0, cs>>>(n, x, w.r.get(), w.ap.get(), w.p.get(), st_d, partial);
-        k_cg_beta<<<1, kRedThreads, 0, cs>>>(partial, st_d);
-        k_cg_update_p<T><<<elem_grid(n), 256, 0, cs>>>(n, w.p.get(), w.r.get(), st_d);
-    }
-    const cudaError_t cap = cudaStreamEndCapture(cs, &graph);
-    if (cap != cudaSuccess || !graph)
-        fail(ABHSF_ERROR_CUDA, std::string("CG graph capture: ") + cudaGetErrorString(cap));
-    const cudaError_t ins = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ins != cudaSuccess)
-        fail(ABHSF_ERROR_CUDA, std::string("CG graph instantiation: ") + cudaGetErrorString(ins));
-    struct exec_guard {
-        cudaGraphExec_t e;
-        ~exec_guard() { cudaGraphExecDestroy(e); }
-    } guard{exec};
-
-    for (;;) {
-        ABHSF_CUDA(cudaMemcpyAsync(st_h, st_d, sizeof(cg_state), cudaMemcpyDeviceToHost, cs));
-        ABHSF_CUDA(cudaStreamSynchronize(cs));
-        if (st_h->done)
-            break;
-        ABHSF_CUDA(cudaGraphLaunch(exec, cs));
-    }
-    return st_h->iters;
 }
+
+// kChunk CG iterations on A x = b (x, w.r, w.p, w.ap and the state on the
+// device), captured once into a graph and replayed until the state is done.
+template <typename T>
+class cg_graph {
+  public:
+    cg_graph(const abhsf_matrix& a, T* x, cg_work<T>& w, int64_t n, cg_state* st_d, double* partial, cudaStream_t cs)
+    {
+        cudaGraph_t graph = nullptr;
+        ABHSF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        for (int it = 0; it < kChunk; ++it) {
+            spmv_t(a, w.p.get(), w.ap.get(), cs);
+            dot<T>(w.p.get(), w.ap.get(), n, partial, cs);
+            k_cg_alpha<<<1, kRedThreads, 0, cs>>>(partial, st_d);
+            k_cg_update_xr<T>
+                <<<kRedBlocks, kRedThreads, 0, cs>>>(n, x, w.r.get(), w.ap.get(), w.p.get(), st_d, partial);
+            k_cg_beta<<<1, kRedThreads, 0, cs>>>(partial, st_d);
+            k_cg_update_p<T><<<elem_grid(n), 256, 0, cs>>>(n, w.p.get(), w.r.get(), st_d);
+        }
+        const cudaError_t cap = cudaStreamEndCapture(cs, &graph);
+        if (cap != cudaSuccess || !graph)
+            fail(ABHSF_ERROR_CUDA, std::string("CG graph capture: ") + cudaGetErrorString(cap));
+        const cudaError_t ins = cudaGraphInstantiate(&exec_, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ins != cudaSuccess)
+            fail(ABHSF_ERROR_CUDA, std::string("CG graph instantiation: ") + cudaGetErrorString(ins));
+    }
+    ~cg_graph() { cudaGraphExecDestroy(exec_); }
+    cg_graph(const cg_graph&) = delete;
+    cg_graph& operator=(const cg_graph&) = delete;
+
+    // replays chunks until the state says done; returns the iteration count
+    int run(cg_state* st_d, cg_state* st_h, cudaStream_t cs)
+    {
+        for (;;) {
+            ABHSF_CUDA(cudaMemcpyAsync(st_h, st_d, sizeof(cg_state), cudaMemcpyDeviceToHost, cs));
+            ABHSF_CUDA(cudaStreamSynchronize(cs));
+            if (st_h->done)
+                return st_h->iters;
+            ABHSF_CUDA(cudaGraphLaunch(exec_, cs));
+        }
+    }
+
+  private:
+    cudaGraphExec_t exec_ = nullptr;
+};
 
 struct solve_stream {
     cudaStream_t user, cs = nullptr;
@@ -287,8 +320,9 @@ void cg_solve(const abhsf_matrix& a, const double* b, double* x, double rtol, in
     cg_state st_h{};
     const double bb = norm2(b, n, partial.get(), st_d.get(), &st_h, cs);
     residual<double>(a, b, x, w.r.get(), xn.get(), n, cs);
-    const int iters =
-        cg_iterate<double>(a, x, w, n, st_d.get(), &st_h, partial.get(), rtol * rtol * bb, max_iters, cs);
+    cg_start<double>(w, n, st_d.get(), partial.get(), rtol * rtol * bb, max_iters, cs);
+    cg_graph<double> g(a, x, w, n, st_d.get(), partial.get(), cs);
+    const int iters = g.run(st_d.get(), &st_h, cs);
     residual<double>(a, b, x, w.r.get(), xn.get(), n, cs);
     const double rr = norm2(w.r.get(), n, partial.get(), st_d.get(), &st_h, cs);
     info->iterations = iters;
@@ -298,7 +332,7 @@ void cg_solve(const abhsf_matrix& a, const double* b, double* x, double rtol, in
 }
 
 void cg_solve_mixed(const abhsf_matrix& a64, const abhsf_matrix& a32, const double* b, double* x, double rtol,
-                    int max_iters, double inner_rtol, int max_outer, abhsf_cg_info* info, cudaStream_t user)
+                    int max_iters, double update_factor, int max_updates, abhsf_cg_info* info, cudaStream_t user)
 {
     check_square(a64);
     if (a32.m != a64.m || a32.n != a64.n)
@@ -306,30 +340,42 @@ void cg_solve_mixed(const abhsf_matrix& a64, const abhsf_matrix& a32, const doub
     if (a32.ring_warps == 0 && a32.T > 0)
         fail(ABHSF_ERROR_UNSUPPORTED, "the f32 SpMV of the mixed solver supports block sizes 32 and 64");
     const int64_t n = a64.n;
+    const double f2 = update_factor * update_factor;
     solve_stream ss(user);
     cudaStream_t cs = ss.cs;
     dbuf<double> r64(n), xn(n), partial(kRedBlocks);
     cg_work<float> w(n);
-    dbuf<float> d(n);
+    dbuf<float> d(n);  // the f32 solution since the last update
     dbuf<cg_state> st_d(1), st64_d(1);
     cg_state st_h{};
-    const double bb = norm2(b, n, partial.get(), st_d.get(), &st_h, cs);
+    const double bb = norm2(b, n, partial.get(), st64_d.get(), &st_h, cs);
+    const double tol2 = rtol * rtol * bb;
     residual<double>(a64, b, x, r64.get(), xn.get(), n, cs);
     double rr = norm2(r64.get(), n, partial.get(), st64_d.get(), &st_h, cs);
-    int iters = 0, outer = 0;
-    while (rr > rtol * rtol * bb && outer < max_outer && iters < max_iters) {
-        // correction: A d = r / ||r|| in f32 to inner_rtol, then x += ||r|| d
-        k_to_unit_f32<<<elem_grid(n), 256, 0, cs>>>(n, r64.get(), w.r.get(), st64_d.get());
+    int iters = 0, updates = 0;
+    if (rr > tol2 && max_iters > 0) {
+        k_to_f32<<<elem_grid(n), 256, 0, cs>>>(n, r64.get(), w.r.get());
         ABHSF_CUDA(cudaMemsetAsync(d.get(), 0, n * sizeof(float), cs));
-        iters += cg_iterate<float>(a32, d.get(), w, n, st_d.get(), &st_h, partial.get(), inner_rtol * inner_rtol,
-                                   max_iters - iters, cs);
-        k_add_scaled<<<elem_grid(n), 256, 0, cs>>>(n, x, d.get(), st64_d.get());
-        residual<double>(a64, b, x, r64.get(), xn.get(), n, cs);
-        rr = norm2(r64.get(), n, partial.get(), st64_d.get(), &st_h, cs);
-        ++outer;
+        cg_start<float>(w, n, st_d.get(), partial.get(), 0.0, max_iters, cs);
+        k_cg_resume<<<1, kRedThreads, 0, cs>>>(partial.get(), st_d.get(), f2);  // partials of r32 . r32
+        cg_graph<float> g(a32, d.get(), w, n, st_d.get(), partial.get(), cs);
+        for (;;) {
+            iters = g.run(st_d.get(), &st_h, cs);
+            // reliable update: fold the f32 solution into x, replace r by b - A x in FP64
+            k_fold<<<elem_grid(n), 256, 0, cs>>>(n, x, d.get());
+            residual<double>(a64, b, x, r64.get(), xn.get(), n, cs);
+            rr = norm2(r64.get(), n, partial.get(), st64_d.get(), &st_h, cs);
+            ++updates;
+            if (rr <= tol2 || iters >= max_iters || updates >= max_updates)
+                break;
+            k_to_f32<<<elem_grid(n), 256, 0, cs>>>(n, r64.get(), w.r.get());
+            dot<float>(w.r.get(), w.r.get(), n, partial.get(), cs);
+            k_cg_resume<<<1, kRedThreads, 0, cs>>>(partial.get(), st_d.get(), f2);
+            ABHSF_CUDA(cudaGetLastError());
+        }
     }
     info->iterations = iters;
-    info->outer_iterations = outer;
+    info->outer_iterations = updates;
     info->rel_residual = bb > 0.0 ? std::sqrt(rr / bb) : std::sqrt(rr);
     info->converged = info->rel_residual <= rtol ? 1 : 0;
 }

@@ -41,7 +41,7 @@ bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream
 void cg_solve(const abhsf_matrix& a, const double* b, double* x, double rtol, int max_iters, abhsf_cg_info* info,
               cudaStream_t st);
 void cg_solve_mixed(const abhsf_matrix& a64, const abhsf_matrix& a32, const double* b, double* x, double rtol,
-                    int max_iters, double inner_rtol, int max_outer, abhsf_cg_info* info, cudaStream_t st);
+                    int max_iters, double update_factor, int max_updates, abhsf_cg_info* info, cudaStream_t st);
 
 // y += A x in f32 for matrices stored as f32 or bf16 (values widened to f32,
 // same per-row order); false when the matrix has no ring schedule.

@@ -300,13 +300,14 @@ def cg(A: AbhsfMatrix, b, x, rtol: float = 1e-10, max_iters: int = 100000, strea
 
 
 def cg_mixed(A64: AbhsfMatrix, A_lo: AbhsfMatrix, b, x, rtol: float = 1e-10, max_iters: int = 100000,
-             inner_rtol: float = 1e-5, max_outer: int = 50, stream=None) -> dict:
-    """Solves A x = b by FP64 iterative refinement around an f32 CG on A_lo
-    (the same matrix stored as f32 or bf16); residuals with A64 in FP64."""
+             update_factor: float = 1e-1, max_updates: int = 1000, stream=None) -> dict:
+    """Solves A x = b by an f32 CG on A_lo (the same matrix stored as f32 or
+    bf16) whose solution accumulates in FP64 and whose residual is replaced
+    by the FP64 residual of A64 each time it falls by update_factor."""
     A64._check_open()
     A_lo._check_open()
     _solver_vectors(A64, b, x)
     info = capi.CgInfo()
     capi.check(capi.lib.abhsf_cg_mixed(A64._h, A_lo._h, b.data_ptr(), x.data_ptr(), float(rtol), int(max_iters),
-                                       float(inner_rtol), int(max_outer), C.byref(info), _stream_ptr(stream)))
+                                       float(update_factor), int(max_updates), C.byref(info), _stream_ptr(stream)))
     return _info(info)

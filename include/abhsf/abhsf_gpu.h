@@ -115,8 +115,8 @@ typedef struct abhsf_matrix abhsf_matrix;
 
 /* Outcome of abhsf_cg / abhsf_cg_mixed. */
 typedef struct abhsf_cg_info {
-    int32_t iterations;       /* CG iterations (for the mixed solver: inner f32 iterations, all outer steps) */
-    int32_t outer_iterations; /* refinement steps (1 for plain CG) */
+    int32_t iterations;       /* CG iterations (for the mixed solver: its f32 iterations) */
+    int32_t outer_iterations; /* residual replacements of the mixed solver (1 for plain CG) */
     int32_t converged;        /* rel_residual <= rtol */
     int32_t reserved;
     double rel_residual;      /* ||b - A x|| / ||b|| in FP64 with the FP64 matrix, at return */
@@ -170,14 +170,16 @@ ABHSF_API abhsf_status abhsf_spmv_f32(const abhsf_matrix* a, const float* x, flo
 ABHSF_API abhsf_status abhsf_cg(const abhsf_matrix* a, const double* b, double* x, double rtol, int32_t max_iters,
                                 abhsf_cg_info* info, abhsf_stream_t stream);
 
-/* The same system solved by FP64 iterative refinement around an f32 CG:
- * each outer step normalises the FP64 residual r = b - A x (computed with
- * the f64 matrix a64), solves a_lo d = r / ||r|| in f32 (a_lo: the same
- * matrix stored as f32 or bf16, block size 32 or 64) to inner_rtol, and adds
- * ||r|| d to x in FP64.  Stops when ||b - A x|| <= rtol ||b||, after
- * max_outer steps, or after max_iters inner iterations in total. */
+/* The same system solved in mixed precision: CG runs in f32 on a_lo (the
+ * same matrix stored as f32 or bf16, block size 32 or 64) with f32 vectors;
+ * its solution is folded into x in FP64, and each time its residual has
+ * fallen by update_factor (in (0, 1), e.g. 0.1) it is replaced by the FP64
+ * residual b - A x of the f64 matrix a64 (a reliable update), the search
+ * direction kept.  Stops when ||b - A x|| <= rtol ||b|| at an update, after
+ * max_iters iterations, or after max_updates updates.  info.iterations counts
+ * f32 iterations, info.outer_iterations the updates. */
 ABHSF_API abhsf_status abhsf_cg_mixed(const abhsf_matrix* a64, const abhsf_matrix* a_lo, const double* b, double* x,
-                                      double rtol, int32_t max_iters, double inner_rtol, int32_t max_outer,
+                                      double rtol, int32_t max_iters, double update_factor, int32_t max_updates,
                                       abhsf_cg_info* info, abhsf_stream_t stream);
 
 /* Y += A X for k right-hand sides, X (n x k) and Y (m x k) float64 row-major
