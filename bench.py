@@ -146,6 +146,72 @@ def time_spmm(A, c, st, dev, stream, l2_flush, warmup, ks=(4, 8, 16, 32), steps=
     return out
 
 
+def time_lowprec(c, dev, l2_flush, warmup, steps=10):
+    """f32 and bf16 copies of the same matrix: f32 SpMV time, algorithmic GB/s
+    (B_fmt + 4 n + 8 m) and normwise error against the FP64 product of the
+    same (f32) x."""
+    import torch
+    from abhsf_b200 import AbhsfMatrix
+    x32 = torch.rand(c.n, dtype=torch.float32, device=dev) * 2 - 1
+    A64 = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64)
+    y64 = torch.zeros(c.m, dtype=torch.float64, device=dev)
+    A64.spmv(x32.double(), y64)
+    A64.release()
+    out = {}
+    for vt in ("f32", "bf16"):
+        A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64, value_type=vt)
+        y = torch.zeros(c.m, dtype=torch.float32, device=dev)
+        A.spmv_f32(x32, y)
+        err = float(torch.linalg.norm(y.double() - y64) / torch.linalg.norm(y64))
+        for _ in range(max(warmup, 1)):
+            l2_flush()
+            A.spmv_f32(x32, y)
+        ts = []
+        for _ in range(steps):
+            l2_flush()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            A.spmv_f32(x32, y)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        t = sum(ts) / len(ts)
+        b = int(A.stats()["format_bytes"]) + 4 * c.n + 8 * c.m
+        out[vt] = {"ms": t, "GB/s": b / (t * 1e-3) / 1e9, "bytes": b, "rel_err_vs_fp64": err}
+        A.release()
+    return out
+
+
+def time_cg(dev, g=256, rtol=1e-10):
+    """CG solve time on the 3D 7-point Laplacian g^3 (n = g^3, SPD, b U[-1,1]
+    seed 1, x0 = 0) to ||b - A x|| <= rtol ||b||: plain FP64 CG against the
+    tuned solver (f32 CG on an f32 copy, FP64 solution and reliable updates)."""
+    import torch
+    from abhsf_b200 import AbhsfMatrix, cg, cg_mixed
+    from abhsf_b200 import workloads as W
+    lap = W.laplacian_3d(g)
+    A64 = AbhsfMatrix.from_elements(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=64)
+    A32 = AbhsfMatrix.from_elements(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=64, value_type="f32")
+    b = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, lap.n)).to(dev)
+    out = {"workload": f"3D 7-point Laplacian {g}^3 (n={lap.n}, nnz={lap.nnz}, diag 6, off -1), b U[-1,1] seed 1, "
+                       f"x0 = 0, block size 64", "rtol": rtol}
+    for name, fn in (("plain", lambda x: cg(A64, b, x, rtol=rtol)),
+                     ("tuned", lambda x: cg_mixed(A64, A32, b, x, rtol=rtol, update_factor=0.1))):
+        x = torch.zeros(lap.n, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info = fn(x)
+        torch.cuda.synchronize()
+        out[name] = dict(info, seconds=time.perf_counter() - t0)
+    out["plain"]["solver"] = "FP64 CG, reference-order f64 SpMV"
+    out["tuned"]["solver"] = "f32 CG on an f32 copy, FP64 solution, FP64 residual replacement each 10x drop"
+    out["tuned_speedup"] = out["plain"]["seconds"] / out["tuned"]["seconds"]
+    A64.release()
+    A32.release()
+    return out
+
+
 def cpu_reference_run(c, bytes_per_step: float, max_seconds: float, max_iters: int):
     """Reference CSR spmv_naive (oracle/_ref, compiled from the reference
     sources) on all host threads; falls back to the single-thread oracle port."""
@@ -299,6 +365,8 @@ def run_ours(args):
     e2e_s = float(e_red.item())
 
     spmm = None if args.no_spmm else time_spmm(A, c, st, dev, stream, l2_flush, args.warmup)
+    lowprec = None if args.no_lowprec else time_lowprec(c, dev, l2_flush, args.warmup)
+    cg_times = None if args.no_cg or rank != 0 else time_cg(dev)
 
     peak, peak_src = hbm_peak()
     achieved = B / (t_mean * 1e-3) / 1e9
@@ -329,6 +397,8 @@ def run_ours(args):
                          "kernel": KERNELS[args.sum_order] + "<64>"},
             "cpu_baseline": cpu,
             "spmm": spmm,
+            "lowprec": lowprec,
+            "cg": cg_times,
             "e2e": {"value": world * B / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
                     "d2h_bytes_per_step": 8 * c.m, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": args.steps,
@@ -349,6 +419,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
     ap.add_argument("--no-spmm", action="store_true", help="skip the multi-right-hand-side timings")
+    ap.add_argument("--no-lowprec", action="store_true", help="skip the f32 / bf16 SpMV timings")
+    ap.add_argument("--no-cg", action="store_true", help="skip the CG solves on the 3D Laplacian")
     ap.add_argument("--sum-order", choices=["reference", "tree"], default="reference",
                     help="reference: bitwise the reference CSR's y; tree: warp reduction trees")
     ap.add_argument("--n", type=int, default=DEFAULT_N,
