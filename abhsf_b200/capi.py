@@ -94,6 +94,10 @@ PROTOTYPES = {
     "abhsf_spmv_host": (C.c_int, [_vp, _vp, _vp, _vp]),
     "abhsf_spmm": (C.c_int, [_vp, _i32, _vp, _i64, _vp, _i64, _vp]),
     "abhsf_spmv_f32": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "abhsf_batch_create": (C.c_int, [_vp, _i32, _vp, C.POINTER(_vp)]),
+    "abhsf_batch_spmv": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "abhsf_batch_status": (C.c_int, [_vp, _vp, _i32, C.POINTER(_i32)]),
+    "abhsf_batch_release": (C.c_int, [_vp]),
     "abhsf_cg": (C.c_int, [_vp, _vp, _vp, C.c_double, _i32, C.POINTER(CgInfo), _vp]),
     "abhsf_cg_mixed": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, _i32, C.c_double, _i32, C.POINTER(CgInfo),
                                  _vp]),

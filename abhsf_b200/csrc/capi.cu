@@ -163,6 +163,70 @@ abhsf_status abhsf_cg_mixed(const abhsf_matrix* a64, const abhsf_matrix* a_lo, c
     });
 }
 
+abhsf_status abhsf_batch_create(const abhsf_matrix* const* mats, int32_t count, abhsf_stream_t stream,
+                                abhsf_batch** out)
+{
+    return guarded([&] {
+        if (!mats || !out || count <= 0)
+            fail(ABHSF_ERROR_INVALID_VALUE, "mats and out must be non-NULL and count > 0");
+        *out = nullptr;
+        if (count > abhsf::kBatchMax)
+            fail(ABHSF_ERROR_UNSUPPORTED, "a batch holds at most 4096 matrices");
+        auto b = std::make_unique<abhsf_batch>();
+        for (int32_t i = 0; i < count; ++i) {
+            const abhsf_matrix* a = mats[i];
+            if (!a)
+                fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle is NULL");
+            if (a->value_type != ABHSF_VALUE_F64)
+                fail(ABHSF_ERROR_INVALID_VALUE, "batched matrices must be stored as f64");
+            if (a->s != 32 && a->s != 64)
+                fail(ABHSF_ERROR_UNSUPPORTED, "batched matrices must have block size 32 or 64");
+            if (i > 0 && a->s != mats[0]->s)
+                fail(ABHSF_ERROR_INVALID_VALUE, "batched matrices must share one block size");
+            if (a->N >= (int64_t(1) << abhsf::kBatchColBits) || a->M >= (int64_t(1) << 30))
+                fail(ABHSF_ERROR_UNSUPPORTED, "a batched matrix has too many block rows or columns");
+            b->mats.push_back(a);
+            b->total_tiles += a->T;
+        }
+        b->s = mats[0]->s;
+        ABHSF_CUDA(cudaGetDevice(&b->device));
+        abhsf::prepare_batch(*b, reinterpret_cast<cudaStream_t>(stream));
+        *out = b.release();
+    });
+}
+
+abhsf_status abhsf_batch_spmv(const abhsf_batch* b, const double* const* xs, double* const* ys,
+                              abhsf_stream_t stream)
+{
+    return guarded([&] {
+        if (!b)
+            fail(ABHSF_ERROR_INVALID_VALUE, "batch handle is NULL");
+        if (!xs || !ys)
+            fail(ABHSF_ERROR_INVALID_VALUE, "xs and ys must be non-NULL device arrays");
+        abhsf::batch_spmv(*b, xs, ys, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+abhsf_status abhsf_batch_status(abhsf_batch* b, abhsf_stream_t stream, int32_t clear, int32_t* out)
+{
+    return guarded([&] {
+        if (!b || !out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "batch handle and out must be non-NULL");
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        int v = 0;
+        ABHSF_CUDA(cudaMemcpyAsync(&v, b->dev_status.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (clear)
+            ABHSF_CUDA(cudaMemsetAsync(b->dev_status.get(), 0, sizeof(int), st));
+        ABHSF_CUDA(cudaStreamSynchronize(st));
+        *out = v;
+    });
+}
+
+abhsf_status abhsf_batch_release(abhsf_batch* b)
+{
+    return guarded([&] { delete b; });
+}
+
 abhsf_status abhsf_spmm(const abhsf_matrix* a, int32_t k, const double* X, int64_t ldx, double* Y, int64_t ldy,
                         abhsf_stream_t stream)
 {

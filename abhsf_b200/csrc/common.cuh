@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "abhsf/abhsf_cost.h"
 #include "abhsf/abhsf_gpu.h"
@@ -180,4 +181,24 @@ struct abhsf_matrix {
         return abhsf::tiles_view{m, n, M, brow_ptr.get(), tile_col.get(), tile_nnz.get(), tile_scheme.get(),
                                  tile_val_off.get(), tile_idx_off.get(), payload.get(), values.get()};
     }
+};
+
+// Several f64 matrices of one block size (32 or 64) multiplied by one launch
+// of the ring kernel (abhsf_batch_*).  The matrices belong to the caller and
+// must outlive the batch.
+namespace abhsf {
+constexpr int kBatchColBits = 20;  // descriptor column = block column | matrix index << 20
+constexpr int kBatchMax = 1 << (32 - kBatchColBits);
+}  // namespace abhsf
+
+struct abhsf_batch {
+    std::vector<const abhsf_matrix*> mats;
+    int32_t s = 0;
+    int device = 0;
+    int64_t total_tiles = 0;
+    abhsf::dbuf<uint8_t> desc;   // every CTA's tile descriptors
+    abhsf::dbuf<int64_t> wbeg;   // each CTA's range in desc
+    abhsf::dbuf<uint8_t> table;  // per matrix: arrays and shape
+    abhsf::dbuf<int> dev_status;
+    int ctas = 0;
 };

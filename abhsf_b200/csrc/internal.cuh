@@ -37,6 +37,12 @@ void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_
 // The same order through per-warp shared-memory rings (s = 32, 64); false
 // when the matrix has no ring schedule.
 bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+// Batches (spmv_ring.cu): the ring kernel's schedule over every matrix of the
+// batch, and y_i += A_i x_i for all of them in one launch (xs, ys: device
+// arrays of device pointers).
+void prepare_batch(abhsf_batch& b, cudaStream_t st);
+void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);
+
 // Conjugate gradients (cg.cu).
 void cg_solve(const abhsf_matrix& a, const double* b, double* x, double rtol, int max_iters, abhsf_cg_info* info,
               cudaStream_t st);

@@ -103,7 +103,7 @@ struct val_traits<ABHSF_VALUE_BF16> {
 template <int S, int K, int VT>
 constexpr int ring_overhead()
 {
-    return kMaxQ * (48 + 16) + (S / 32) * 64 * 4 + 64;
+    return kMaxQ * (64 + 16) + (S / 32) * 64 * 4 + 64;
 }
 
 // The ring: the shared memory of an SM (228 KiB, 1 KiB of it reserved per
@@ -157,8 +157,10 @@ struct __align__(16) slot_rec {
     uint32_t off;   // ring offset of the slot
     int32_t ntiles;
     int32_t y_off, x_off, pay_off, val_off;  // parts, relative to the slot
+    void* y;        // the group's matrix: y and its rows
+    int64_t m;
 };
-static_assert(sizeof(slot_rec) == 48, "slot_rec is 48 bytes");
+static_assert(sizeof(slot_rec) == 64, "slot_rec is 64 bytes");
 
 template <int S, int K, int VT>
 struct ring_smem {
@@ -170,6 +172,13 @@ struct ring_smem {
     int abort;                        // a wait ran out: everyone stops
 };
 
+// One matrix of a batch: its arrays and shape (x and y come per call).
+struct ring_mat {
+    const uint8_t* payload;
+    const void* values;
+    int64_t m, n;
+};
+
 struct ring_args {
     tiles_view A;
     const ring_desc* desc;  // every CTA's tiles, CTA after CTA
@@ -177,10 +186,43 @@ struct ring_args {
     const void* x;  // X (T), row-major: element (i, j) at x[i * ldx + j]
     void* y;        // Y (T), row-major: element (i, j) at y[i * ldy + j]
     int64_t ldx, ldy;
+    // a batch: descriptor column = block column | matrix index << col_bits,
+    // and matrix i's arrays, x and y come from mats[i], xs[i], ys[i]
+    const ring_mat* mats;  // nullptr: the single matrix A, x, y above
+    const void* const* xs;
+    void* const* ys;
+    int col_bits;
     int* status;     // ABHSF_DEVSTAT_* bits
     int64_t drop;    // test hook: a descriptor whose group's bulk copies are not issued (-1: none)
     uint32_t polls;  // bound of every mbarrier wait
 };
+
+// The matrix a group's tiles belong to, as the producer and consumers use it.
+struct mat_view {
+    const uint8_t* payload;
+    const void* values;
+    const void* x;
+    void* y;
+    int64_t m, n;
+};
+
+__device__ __forceinline__ mat_view view_of(const ring_args& P, int mid)
+{
+    if (!P.mats)
+        return mat_view{P.A.payload, P.A.values, P.x, P.y, P.A.m, P.A.n};
+    const ring_mat& a = P.mats[mid];
+    return mat_view{a.payload, a.values, P.xs[mid], P.ys[mid], a.m, a.n};
+}
+
+__device__ __forceinline__ uint32_t col_of(const ring_args& P, uint32_t col)
+{
+    return P.col_bits >= 32 ? col : col & ((1u << P.col_bits) - 1u);
+}
+
+__device__ __forceinline__ int mid_of(const ring_args& P, uint32_t col)
+{
+    return P.col_bits >= 32 ? 0 : (int)(col >> P.col_bits);
+}
 
 // Values before the tile's first value in its first 16-byte granule.
 template <int VT>
@@ -274,8 +316,9 @@ struct group_geo {
 // Producer warp: queues the group's slot at ring offset off as queue slot q;
 // it completes on full[q].
 template <int S, int K, int VT>
-__device__ __forceinline__ void issue_group(const ring_args& P, const ring_desc& d, int yk, const group_geo& gg,
-                                            uint32_t off, int q, ring_smem<S, K, VT>& sm, bool drop, int lane)
+__device__ __forceinline__ void issue_group(const ring_args& P, const mat_view& mv, const ring_desc& d, int yk,
+                                            const group_geo& gg, uint32_t off, int q, ring_smem<S, K, VT>& sm,
+                                            bool drop, int lane)
 {
     using T = typename val_traits<VT>::T;
     using V = typename val_traits<VT>::V;
@@ -286,36 +329,36 @@ __device__ __forceinline__ void issue_group(const ring_args& P, const ring_desc&
     if (lane < gg.ntiles)
         reinterpret_cast<ring_desc*>(slot)[lane] = d;
     __syncwarp();  // lane 0's arrival below publishes every lane's descriptor
-    const T* X = static_cast<const T*>(P.x);
-    const T* Y = static_cast<const T*>(P.y);
+    const T* X = static_cast<const T*>(mv.x);
+    const T* Y = static_cast<const T*>(mv.y);
     const int total = gg.ntiles * S * K;
     if (gg.ntiles == 1) {  // lane 0 holds the tile's descriptor
-        const uint32_t col = __shfl_sync(kFull, d.col, 0), info = __shfl_sync(kFull, d.info, 0);
+        const uint32_t col = col_of(P, __shfl_sync(kFull, d.col, 0)), info = __shfl_sync(kFull, d.info, 0);
         const int64_t c0 = (int64_t)col * S, r0 = (int64_t)(info & kRowMask) * S;
 #pragma unroll
         for (int k = lane; k < S * K; k += 32) {
             const int c = k / K, h = k % K;
-            const bool okx = c0 + c < P.A.n;
+            const bool okx = c0 + c < mv.n;
             cp_elem(base + gg.x_off + TB * k, okx ? X + (c0 + c) * P.ldx + h : X, okx ? TB : 0);
             if (info & kFirst) {
-                const bool oky = r0 + c < P.A.m;
+                const bool oky = r0 + c < mv.m;
                 cp_elem(base + gg.y_off + TB * k, oky ? Y + (r0 + c) * P.ldy + h : Y, oky ? TB : 0);
             }
         }
     }
     for (int e0 = 0; gg.ntiles > 1 && e0 < total; e0 += 32) {
         const int e = e0 + lane, jj = (e / (S * K)) & 31, k = e % (S * K);
-        const uint32_t col = __shfl_sync(kFull, d.col, jj);
+        const uint32_t col = col_of(P, __shfl_sync(kFull, d.col, jj));
         const uint32_t info = __shfl_sync(kFull, d.info, jj);
         const int ykk = __shfl_sync(kFull, yk, jj);
         if (e < total) {
             const int c = k / K, h = k % K;
             const int64_t c0 = (int64_t)col * S;
-            const bool okx = c0 + c < P.A.n;
+            const bool okx = c0 + c < mv.n;
             cp_elem(base + gg.x_off + jj * XB + TB * k, okx ? X + (c0 + c) * P.ldx + h : X, okx ? TB : 0);
             if (info & kFirst) {
                 const int64_t r0 = (int64_t)(info & kRowMask) * S;
-                const bool oky = r0 + c < P.A.m;
+                const bool oky = r0 + c < mv.m;
                 cp_elem(base + gg.y_off + ykk * XB + TB * k, oky ? Y + (r0 + c) * P.ldy + h : Y, oky ? TB : 0);
             }
         }
@@ -331,13 +374,15 @@ __device__ __forceinline__ void issue_group(const ring_args& P, const ring_desc&
         r.x_off = gg.x_off;
         r.pay_off = gg.pay_off;
         r.val_off = gg.val_off;
+        r.y = mv.y;
+        r.m = mv.m;
         mbar_expect_tx(bar, gg.pay_bytes + gg.val_bytes);  // also publishes rec[q] and the descriptors
         if (!drop) {
             // the slot's bytes were last read through the generic proxy
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             if (gg.pay_bytes)
-                bulk_g2s(base + gg.pay_off, P.A.payload + gg.io0, gg.pay_bytes, bar);
-            bulk_g2s(base + gg.val_off, static_cast<const V*>(P.A.values) + gg.vbase, gg.val_bytes, bar);
+                bulk_g2s(base + gg.pay_off, mv.payload + gg.io0, gg.pay_bytes, bar);
+            bulk_g2s(base + gg.val_off, static_cast<const V*>(mv.values) + gg.vbase, gg.val_bytes, bar);
         }
     }
 }
@@ -546,10 +591,10 @@ __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot
     }
     if (d.info & kLast) {
         const int64_t rr = (int64_t)(d.info & kRowMask) * S + row;
-        if (rr < P.A.m) {
+        if (rr < r.m) {
 #pragma unroll
             for (int h = 0; h < K; ++h)
-                static_cast<T*>(P.y)[rr * P.ldy + h] = acc[h];
+                static_cast<T*>(r.y)[rr * P.ldy + h] = acc[h];
         }
     }
 }
@@ -623,7 +668,8 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                 // contiguous with the previous tile in the format arrays?
                 const int64_t pvo = __shfl_up_sync(kFull, d.vo, 1), pio = __shfl_up_sync(kFull, d.io, 1);
                 const uint32_t pnv = __shfl_up_sync(kFull, d.nv, 1), ppb = __shfl_up_sync(kFull, d.pb_sch, 1) & 0xffffffu;
-                const bool contig = lane == 0 || (d.vo == pvo + pnv && d.io == pio + ppb);
+                const uint32_t pcol = __shfl_up_sync(kFull, d.col, 1);
+            const bool contig = lane == 0 || (d.vo == pvo + pnv && d.io == pio + ppb && mid_of(P, d.col) == mid_of(P, pcol));
                 const bool first = (d.info & kFirst) != 0;
                 const int est = have ? 32 + (first ? XB : 0) + XB + (int)(d.pb_sch & 0xffffffu) + (int)d.nv * VB : 0;
                 const int cum = warp_inclusive_sum(est, lane);
@@ -678,7 +724,8 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                 break;
             }
             const bool drop = P.drop >= eb + i && P.drop < eb + i + L;
-            issue_group<S, K, VT>(P, d, yk, gg, (uint32_t)off, issued % kMaxQ, sm, drop, lane);
+            const mat_view mv = view_of(P, mid_of(P, __shfl_sync(kFull, d.col, 0)));
+            issue_group<S, K, VT>(P, mv, d, yk, gg, (uint32_t)off, issued % kMaxQ, sm, drop, lane);
             if (lane == issued % kMaxQ)
                 my_off = off;
             if (issued == done)
@@ -743,7 +790,7 @@ __global__ void k_ring_weight(int64_t nr, const uint32_t* __restrict__ rows, til
 }
 
 __global__ void k_ring_fill(int64_t nitems, const uint32_t* __restrict__ rows, const int64_t* __restrict__ base,
-                            tiles_view A, ring_desc* __restrict__ out)
+                            tiles_view A, uint32_t col_or, ring_desc* __restrict__ out)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nitems;
          k += (int64_t)gridDim.x * blockDim.x) {
@@ -753,7 +800,7 @@ __global__ void k_ring_fill(int64_t nitems, const uint32_t* __restrict__ rows, c
             ring_desc d;
             d.vo = A.tile_val_off[t];
             d.io = A.tile_idx_off[t];
-            d.col = A.tile_col[t];
+            d.col = A.tile_col[t] | col_or;
             d.nv = (uint32_t)(A.tile_val_off[t + 1] - d.vo);
             d.pb_sch = (uint32_t)(A.tile_idx_off[t + 1] - d.io) | ((uint32_t)A.tile_scheme[t] << 24);
             d.info = I | (t == t0 ? kFirst : 0u) | (t == t1 - 1 ? kLast : 0u);
@@ -783,7 +830,8 @@ void launch_ring(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int
 {
     static_assert(((sizeof(ring_smem<S, K, VT>) + 1023) / 1024 + 1) * 1024 * kCtasPerSm <= 233472,
                   "kCtasPerSm CTAs fit an SM even with shared memory allocated in 1 KiB granules");
-    ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()), a.ring_wbeg.get(), x, y, ldx, ldy,
+    ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()),
+                a.ring_wbeg.get(), x, y, ldx, ldy, nullptr, nullptr, nullptr, 32,
                 a.dev_status.get(), g_drop_desc, g_spin_limit ? g_spin_limit : kWaitPolls};
     k_spmv_f64_ring<S, K, VT><<<(unsigned)a.ring_warps, S + 32, sizeof(ring_smem<S, K, VT>), st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
@@ -830,6 +878,129 @@ void spmm_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, doubl
     }
 }
 
+int ring_per_sm(int s, int vt)
+{
+    if (vt == ABHSF_VALUE_F64)
+        return s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_F64>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_F64>();
+    if (vt == ABHSF_VALUE_F32)
+        return s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_F32>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_F32>();
+    return s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_BF16>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_BF16>();
+}
+
+// Deals the non-empty block rows of one or several matrices (same block size
+// and value type) over the ring kernel's grid, longest processing time first,
+// and writes every CTA's tile descriptors, matrix i's columns tagged with
+// i << col_bits.  Returns false when a CTA would get more tiles than its
+// counters hold.
+bool build_ring_schedule(const std::vector<const abhsf_matrix*>& mats, int col_bits, dbuf<uint8_t>& desc,
+                         dbuf<int64_t>& wbeg_d, int& ctas_out, int& max_pv_out, cudaStream_t st)
+{
+    const int s = mats[0]->s, vt = mats[0]->value_type;
+    const int vsize = (int)value_size(vt);
+    int dev = 0, nsm = 0;
+    ABHSF_CUDA(cudaGetDevice(&dev));
+    ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int per_sm = ring_per_sm(s, vt);
+    std::vector<uint32_t> mid, rows, ntiles;
+    std::vector<uint64_t> wt;
+    int64_t total_tiles = 0;
+    unsigned int mpv = 0;
+    dbuf<unsigned int> max_pv(1);
+    for (size_t i = 0; i < mats.size(); ++i) {
+        const abhsf_matrix& a = *mats[i];
+        const int64_t nr = a.tree_nrows;
+        if (nr == 0)
+            continue;
+        total_tiles += a.T;
+        dbuf<uint64_t> w_d(nr);
+        dbuf<uint32_t> n_d(nr);
+        const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nr + 255) / 256, 4096));
+        k_ring_weight<<<g, 256, 0, st>>>(nr, a.tree_rows.get(), a.view(), s, vsize, w_d.get(), n_d.get());
+        ABHSF_CUDA(cudaGetLastError());
+        ABHSF_CUDA(cudaMemsetAsync(max_pv.get(), 0, sizeof(unsigned int), st));
+        const unsigned gt = (unsigned)std::max<int64_t>(1, std::min<int64_t>((a.T + 255) / 256, 4096));
+        k_ring_max_pv<<<gt, 256, 0, st>>>(a.T, a.view(), vsize, max_pv.get());
+        ABHSF_CUDA(cudaGetLastError());
+        const size_t o = rows.size();
+        rows.resize(o + nr);
+        ntiles.resize(o + nr);
+        wt.resize(o + nr);
+        mid.resize(o + nr, (uint32_t)i);
+        unsigned int m_pv = 0;
+        ABHSF_CUDA(cudaMemcpyAsync(rows.data() + o, a.tree_rows.get(), nr * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                   st));
+        ABHSF_CUDA(cudaMemcpyAsync(wt.data() + o, w_d.get(), nr * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+        ABHSF_CUDA(cudaMemcpyAsync(ntiles.data() + o, n_d.get(), nr * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        ABHSF_CUDA(cudaMemcpyAsync(&m_pv, max_pv.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+        ABHSF_CUDA(cudaStreamSynchronize(st));
+        mpv = std::max(mpv, m_pv);
+    }
+    const int64_t nitems = (int64_t)rows.size();
+    if (nitems == 0)
+        return false;
+    const int64_t ctas = std::min<int64_t>((int64_t)nsm * per_sm, nitems);
+
+    // longest processing time first: heaviest block row to the least loaded CTA
+    std::vector<int64_t> order(nitems);
+    for (int64_t k = 0; k < nitems; ++k)
+        order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t p, int64_t q) { return wt[p] > wt[q]; });
+    using load_t = std::pair<uint64_t, int64_t>;
+    std::priority_queue<load_t, std::vector<load_t>, std::greater<load_t>> heap;
+    for (int64_t c = 0; c < ctas; ++c)
+        heap.push({0, c});
+    std::vector<std::vector<int64_t>> items(ctas);
+    for (int64_t k : order) {
+        load_t top = heap.top();
+        heap.pop();
+        items[top.second].push_back(k);
+        heap.push({top.first + wt[k], top.second});
+    }
+    // every CTA's items in (matrix, block row) order; each item's first descriptor
+    std::vector<std::vector<uint32_t>> m_rows(mats.size());
+    std::vector<std::vector<int64_t>> m_base(mats.size());
+    std::vector<int64_t> wbeg(ctas + 1, 0);
+    int64_t tiles = 0;
+    for (int64_t c = 0; c < ctas; ++c) {
+        std::sort(items[c].begin(), items[c].end(), [&](int64_t p, int64_t q) {
+            return mid[p] != mid[q] ? mid[p] < mid[q] : rows[p] < rows[q];
+        });
+        wbeg[c] = tiles;
+        for (int64_t k : items[c]) {
+            m_rows[mid[k]].push_back(rows[k]);
+            m_base[mid[k]].push_back(tiles);
+            tiles += ntiles[k];
+        }
+        if (tiles - wbeg[c] > INT32_MAX)
+            return false;
+    }
+    wbeg[ctas] = tiles;
+    if (tiles != total_tiles)
+        fail(ABHSF_ERROR_CUDA, "ring SpMV schedule does not cover every tile");
+
+    desc.alloc(std::max<int64_t>(tiles, 1) * (int64_t)sizeof(ring_desc));
+    wbeg_d.alloc(ctas + 1);
+    ABHSF_CUDA(cudaMemcpyAsync(wbeg_d.get(), wbeg.data(), (ctas + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    for (size_t i = 0; i < mats.size(); ++i) {
+        const int64_t n = (int64_t)m_rows[i].size();
+        if (n == 0)
+            continue;
+        dbuf<uint32_t> rows_d(n);
+        dbuf<int64_t> base_d(n);
+        ABHSF_CUDA(cudaMemcpyAsync(rows_d.get(), m_rows[i].data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        ABHSF_CUDA(cudaMemcpyAsync(base_d.get(), m_base[i].data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+        const uint32_t col_or = col_bits >= 32 ? 0u : (uint32_t)i << col_bits;
+        const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 4096));
+        k_ring_fill<<<g, 256, 0, st>>>(n, rows_d.get(), base_d.get(), mats[i]->view(), col_or,
+                                       reinterpret_cast<ring_desc*>(desc.get()));
+        ABHSF_CUDA(cudaGetLastError());
+        ABHSF_CUDA(cudaStreamSynchronize(st));  // before the host vectors and staging buffers go
+    }
+    ctas_out = (int)ctas;
+    max_pv_out = (int)mpv;
+    return true;
+}
+
 template <int S>
 void ring_set_up_all()
 {
@@ -845,94 +1016,58 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     a.ring_warps = 0;
     if ((a.s != 32 && a.s != 64) || a.tree_nrows == 0 || a.M > (int64_t)kRowMask)
         return;
-    int dev = 0, nsm = 0;
-    ABHSF_CUDA(cudaGetDevice(&dev));
-    ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    int per_sm = 1;
     if (a.value_type == ABHSF_VALUE_F64) {
-        per_sm = a.s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_F64>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_F64>();
         if (a.s == 32)
             ring_set_up_all<32>();
         else
             ring_set_up_all<64>();
-    } else if (a.value_type == ABHSF_VALUE_F32) {
-        per_sm = a.s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_F32>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_F32>();
-    } else {
-        per_sm = a.s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_BF16>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_BF16>();
     }
-    const int vsize = (int)value_size(a.value_type);
-    const int64_t nr = a.tree_nrows;
-    const int64_t ctas = std::min<int64_t>((int64_t)nsm * per_sm, nr);
+    int ctas = 0, mpv = 0;
+    if (!build_ring_schedule({&a}, 32, a.ring_desc, a.ring_wbeg, ctas, mpv, st))
+        return;  // the streaming kernel serves this matrix
+    a.ring_max_pv = mpv;
+    a.ring_warps = ctas;
+}
 
-    dbuf<uint64_t> w_d(nr);
-    dbuf<uint32_t> n_d(nr);
-    const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nr + 255) / 256, 4096));
-    k_ring_weight<<<g, 256, 0, st>>>(nr, a.tree_rows.get(), a.view(), (int)a.s, vsize, w_d.get(), n_d.get());
-    ABHSF_CUDA(cudaGetLastError());
-    std::vector<uint32_t> rows(nr), ntiles(nr);
-    std::vector<uint64_t> wt(nr);
-    ABHSF_CUDA(cudaMemcpyAsync(rows.data(), a.tree_rows.get(), nr * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    ABHSF_CUDA(cudaMemcpyAsync(wt.data(), w_d.get(), nr * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-    ABHSF_CUDA(cudaMemcpyAsync(ntiles.data(), n_d.get(), nr * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    ABHSF_CUDA(cudaStreamSynchronize(st));
-
-    // longest processing time first: heaviest block row to the least loaded CTA
-    std::vector<int64_t> order(nr);
-    for (int64_t k = 0; k < nr; ++k)
-        order[k] = k;
-    std::stable_sort(order.begin(), order.end(), [&](int64_t p, int64_t q) { return wt[p] > wt[q]; });
-    using load_t = std::pair<uint64_t, int64_t>;
-    std::priority_queue<load_t, std::vector<load_t>, std::greater<load_t>> heap;
-    for (int64_t c = 0; c < ctas; ++c)
-        heap.push({0, c});
-    std::vector<std::vector<int64_t>> items(ctas);
-    for (int64_t k : order) {
-        load_t top = heap.top();
-        heap.pop();
-        items[top.second].push_back(k);
-        heap.push({top.first + wt[k], top.second});
-    }
-    std::vector<uint32_t> item_rows;
-    std::vector<int64_t> item_base, wbeg(ctas + 1, 0);
-    item_rows.reserve(nr);
-    item_base.reserve(nr);
-    int64_t tiles = 0;
-    for (int64_t c = 0; c < ctas; ++c) {
-        std::sort(items[c].begin(), items[c].end(), [&](int64_t p, int64_t q) { return rows[p] < rows[q]; });
-        wbeg[c] = tiles;
-        for (int64_t k : items[c]) {
-            item_rows.push_back(rows[k]);
-            item_base.push_back(tiles);
-            tiles += ntiles[k];
-        }
-        if (tiles - wbeg[c] > INT32_MAX)
-            return;  // too many tiles for one CTA's counters: the streaming kernel serves this matrix
-    }
-    wbeg[ctas] = tiles;
-    if (tiles != a.T)
-        fail(ABHSF_ERROR_CUDA, "reference-order SpMV schedule does not cover every tile");
-
-    dbuf<uint32_t> rows_d(nr);
-    dbuf<int64_t> base_d(nr);
-    a.ring_desc.alloc(a.T * (int64_t)sizeof(ring_desc));
-    a.ring_wbeg.alloc(ctas + 1);
-    ABHSF_CUDA(cudaMemcpyAsync(rows_d.get(), item_rows.data(), nr * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-    ABHSF_CUDA(cudaMemcpyAsync(base_d.get(), item_base.data(), nr * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-    ABHSF_CUDA(cudaMemcpyAsync(a.ring_wbeg.get(), wbeg.data(), (ctas + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+void prepare_batch(abhsf_batch& b, cudaStream_t st)
+{
+    std::vector<ring_mat> table;
+    for (const abhsf_matrix* a : b.mats)
+        table.push_back(ring_mat{a->payload.get(), a->values.get(), a->m, a->n});
+    b.table.alloc((int64_t)(table.size() * sizeof(ring_mat)));
+    ABHSF_CUDA(cudaMemcpyAsync(b.table.get(), table.data(), table.size() * sizeof(ring_mat), cudaMemcpyHostToDevice,
                                st));
-    k_ring_fill<<<g, 256, 0, st>>>(nr, rows_d.get(), base_d.get(), a.view(),
-                                   reinterpret_cast<ring_desc*>(a.ring_desc.get()));
-    ABHSF_CUDA(cudaGetLastError());
-    dbuf<unsigned int> max_pv(1);
-    ABHSF_CUDA(cudaMemsetAsync(max_pv.get(), 0, sizeof(unsigned int), st));
-    const unsigned gt = (unsigned)std::max<int64_t>(1, std::min<int64_t>((a.T + 255) / 256, 4096));
-    k_ring_max_pv<<<gt, 256, 0, st>>>(a.T, a.view(), vsize, max_pv.get());
-    ABHSF_CUDA(cudaGetLastError());
-    unsigned int mpv = 0;
-    ABHSF_CUDA(cudaMemcpyAsync(&mpv, max_pv.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    b.dev_status.alloc(1);
+    ABHSF_CUDA(cudaMemsetAsync(b.dev_status.get(), 0, sizeof(int), st));
+    int mpv = 0;
+    b.ctas = 0;
+    if (!build_ring_schedule(b.mats, kBatchColBits, b.desc, b.wbeg, b.ctas, mpv, st) && b.total_tiles > 0)
+        fail(ABHSF_ERROR_UNSUPPORTED, "batch too large for the ring kernel's per-CTA counters");
     ABHSF_CUDA(cudaStreamSynchronize(st));
-    a.ring_max_pv = (int)mpv;
-    a.ring_warps = (int)ctas;
+}
+
+void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st)
+{
+    if (b.ctas == 0)
+        return;
+    ring_args P{};
+    P.desc = reinterpret_cast<const ring_desc*>(b.desc.get());
+    P.wbeg = b.wbeg.get();
+    P.ldx = P.ldy = 1;
+    P.mats = reinterpret_cast<const ring_mat*>(b.table.get());
+    P.xs = reinterpret_cast<const void* const*>(xs);
+    P.ys = reinterpret_cast<void* const*>(ys);
+    P.col_bits = kBatchColBits;
+    P.status = b.dev_status.get();
+    P.drop = -1;
+    P.polls = g_spin_limit ? g_spin_limit : kWaitPolls;
+    if (b.s == 32)
+        k_spmv_f64_ring<32, 1, ABHSF_VALUE_F64>
+            <<<(unsigned)b.ctas, 32 + 32, sizeof(ring_smem<32, 1, ABHSF_VALUE_F64>), st>>>(P);
+    else
+        k_spmv_f64_ring<64, 1, ABHSF_VALUE_F64>
+            <<<(unsigned)b.ctas, 64 + 32, sizeof(ring_smem<64, 1, ABHSF_VALUE_F64>), st>>>(P);
+    ABHSF_CUDA(cudaGetLastError());
 }
 
 bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)

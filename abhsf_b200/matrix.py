@@ -311,3 +311,56 @@ def cg_mixed(A64: AbhsfMatrix, A_lo: AbhsfMatrix, b, x, rtol: float = 1e-10, max
     capi.check(capi.lib.abhsf_cg_mixed(A64._h, A_lo._h, b.data_ptr(), x.data_ptr(), float(rtol), int(max_iters),
                                        float(update_factor), int(max_updates), C.byref(info), _stream_ptr(stream)))
     return _info(info)
+
+
+class AbhsfBatch:
+    """Several f64 matrices of one block size (32 or 64) whose SpMVs run as
+    one kernel launch (abhsf_batch_*).  Keeps the matrices alive."""
+
+    def __init__(self, mats, stream=None):
+        self._mats = list(mats)
+        for a in self._mats:
+            a._check_open()
+        arr = (C.c_void_p * len(self._mats))(*[a._h.value for a in self._mats])
+        self._h = C.c_void_p()
+        capi.check(capi.lib.abhsf_batch_create(arr, len(self._mats), _stream_ptr(stream), C.byref(self._h)))
+
+    def pointer_tables(self, xs, ys):
+        """Device int64 tensors with the data pointers of xs and ys (CUDA
+        float64 vectors of n_i and m_i entries), for spmv_tables."""
+        if len(xs) != len(self._mats) or len(ys) != len(self._mats):
+            raise capi.InvalidValue(capi.INVALID_VALUE, "one x and one y per matrix")
+        for a, x, y in zip(self._mats, xs, ys):
+            if not (_is_cuda(x) and _is_cuda(y)) or x.dtype != torch.float64 or y.dtype != torch.float64:
+                raise capi.InvalidValue(capi.INVALID_VALUE, "x and y must be CUDA float64 tensors")
+            if x.numel() != a.n or y.numel() != a.m or not (x.is_contiguous() and y.is_contiguous()):
+                raise capi.InvalidValue(capi.INVALID_VALUE, "x_i / y_i must be contiguous with n_i / m_i entries")
+        px = torch.tensor([x.data_ptr() for x in xs], dtype=torch.int64, device=xs[0].device)
+        py = torch.tensor([y.data_ptr() for y in ys], dtype=torch.int64, device=ys[0].device)
+        return px, py
+
+    def spmv_tables(self, px, py, stream=None) -> None:
+        """y_i += A_i x_i with device pointer tables (graph-capturable)."""
+        capi.check(capi.lib.abhsf_batch_spmv(self._h, px.data_ptr(), py.data_ptr(), _stream_ptr(stream)))
+
+    def spmv(self, xs, ys, stream=None) -> None:
+        """y_i += A_i x_i for every matrix, one launch."""
+        px, py = self.pointer_tables(xs, ys)
+        self.spmv_tables(px, py, stream)
+        self._keep = (px, py)  # until the next call: the launch reads them asynchronously
+
+    def status(self, clear: bool = False, stream=None) -> int:
+        v = C.c_int32()
+        capi.check(capi.lib.abhsf_batch_status(self._h, _stream_ptr(stream), int(clear), C.byref(v)))
+        return int(v.value)
+
+    def release(self) -> None:
+        if self._h is not None and self._h.value:
+            capi.check(capi.lib.abhsf_batch_release(self._h))
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass

@@ -176,6 +176,52 @@ def edge_shapes(n: int = 1000) -> list[Coo]:
     return out
 
 
+def banded(n: int, bandwidth: int, seed: int = 0) -> Coo:
+    """Every entry within `bandwidth` of the diagonal (|i - j| <= bandwidth),
+    values N(0,1): the banded half of the batched workload."""
+    rng = np.random.default_rng(seed)
+    offs = np.arange(-bandwidth, bandwidth + 1, dtype=np.int64)
+    rows = np.repeat(np.arange(n, dtype=np.int64), offs.size)
+    cols = rows + np.tile(offs, n)
+    ok = (cols >= 0) & (cols < n)
+    rows, cols = rows[ok], cols[ok]
+    return Coo(rows, cols, rng.standard_normal(rows.size), n, n, f"banded_{n}_bw{bandwidth}_s{seed}")
+
+
+def rmat(n: int, edge_factor: int = 8, a: float = 0.57, b: float = 0.19, c: float = 0.19, seed: int = 0) -> Coo:
+    """R-MAT graph on n vertices: edge_factor * n edges, each placed by
+    recursive quadrant choice with probabilities (a, b, c, 1 - a - b - c) on
+    the 2^k x 2^k grid that covers n, those outside n x n dropped, duplicates
+    merged; values N(0,1)."""
+    rng = np.random.default_rng(seed)
+    k = max(1, int(np.ceil(np.log2(max(n, 2)))))
+    e = edge_factor * n
+    r = np.zeros(e, dtype=np.int64)
+    col = np.zeros(e, dtype=np.int64)
+    for level in range(k):
+        u = rng.random(e)
+        bit = np.int64(1) << (k - 1 - level)
+        r += np.where(u >= a + b, bit, 0)                      # quadrants c, d: lower half
+        col += np.where(((u >= a) & (u < a + b)) | (u >= a + b + c), bit, 0)  # quadrants b, d: right half
+    ok = (r < n) & (col < n)
+    key = np.unique(r[ok] * n + col[ok])
+    return Coo(key // n, key % n, rng.standard_normal(key.size), n, n, f"rmat_{n}_ef{edge_factor}_s{seed}")
+
+
+def batched_set(count: int = 256, n_min: int = 1000, n_max: int = 200000, seed: int = 0):
+    """The batched workload: count matrices, n log-uniform in [n_min, n_max];
+    even ones banded (bandwidth U[3, 64]), odd ones R-MAT(0.57, 0.19, 0.19)
+    with edge factor 8.  Yields the matrices one at a time."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max), count)).astype(np.int64)
+    bws = rng.integers(3, 65, count)
+    for i in range(count):
+        if i % 2 == 0:
+            yield banded(int(ns[i]), int(bws[i]), seed=seed * 100003 + i)
+        else:
+            yield rmat(int(ns[i]), 8, seed=seed * 100003 + i)
+
+
 def rhs(n: int, seed: int = 0) -> np.ndarray:
     """x uniform[-1, 1]."""
     return np.random.default_rng(seed).uniform(-1.0, 1.0, size=n)

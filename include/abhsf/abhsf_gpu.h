@@ -112,6 +112,7 @@ typedef struct abhsf_build_opts {
 } abhsf_build_opts;
 
 typedef struct abhsf_matrix abhsf_matrix;
+typedef struct abhsf_batch abhsf_batch;
 
 /* Outcome of abhsf_cg / abhsf_cg_mixed. */
 typedef struct abhsf_cg_info {
@@ -181,6 +182,27 @@ ABHSF_API abhsf_status abhsf_cg(const abhsf_matrix* a, const double* b, double* 
 ABHSF_API abhsf_status abhsf_cg_mixed(const abhsf_matrix* a64, const abhsf_matrix* a_lo, const double* b, double* x,
                                       double rtol, int32_t max_iters, double update_factor, int32_t max_updates,
                                       abhsf_cg_info* info, abhsf_stream_t stream);
+
+/* A batch: count f64 matrices of one block size (32 or 64), at most 4096,
+ * each with fewer than 2^20 block columns, whose SpMVs run as one launch.
+ * The matrices stay owned by the caller and must outlive the batch.  The
+ * non-empty block rows of all of them are dealt over one grid at creation.
+ * No reference counterpart (the reference multiplies one matrix per call). */
+ABHSF_API abhsf_status abhsf_batch_create(const abhsf_matrix* const* mats, int32_t count, abhsf_stream_t stream,
+                                          abhsf_batch** out);
+
+/* y_i += A_i x_i for every matrix of the batch in one kernel launch, in the
+ * reference's summation order (each y_i bitwise what abhsf_spmv gives).  xs
+ * and ys are DEVICE arrays of count device pointers (x_i of n_i doubles,
+ * y_i of m_i), so the call can be captured in a CUDA graph.  Calls on one
+ * batch must not overlap on the GPU. */
+ABHSF_API abhsf_status abhsf_batch_spmv(const abhsf_batch* b, const double* const* xs, double* const* ys,
+                                        abhsf_stream_t stream);
+
+/* The batch's device status word (ABHSF_DEVSTAT_* bits), as abhsf_device_status. */
+ABHSF_API abhsf_status abhsf_batch_status(abhsf_batch* b, abhsf_stream_t stream, int32_t clear, int32_t* out);
+
+ABHSF_API abhsf_status abhsf_batch_release(abhsf_batch* b);
 
 /* Y += A X for k right-hand sides, X (n x k) and Y (m x k) float64 row-major
  * in device memory: element (i, j) of X at X[i * ldx + j], ldx >= k, and the
