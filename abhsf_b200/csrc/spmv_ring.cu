@@ -186,12 +186,11 @@ struct ring_args {
     const void* x;  // X (T), row-major: element (i, j) at x[i * ldx + j]
     void* y;        // Y (T), row-major: element (i, j) at y[i * ldy + j]
     int64_t ldx, ldy;
-    // a batch: descriptor column = block column | matrix index << col_bits,
+    // a batch: descriptor column = block column | matrix index << kBatchColBits,
     // and matrix i's arrays, x and y come from mats[i], xs[i], ys[i]
-    const ring_mat* mats;  // nullptr: the single matrix A, x, y above
+    const ring_mat* mats;
     const void* const* xs;
     void* const* ys;
-    int col_bits;
     int* status;     // ABHSF_DEVSTAT_* bits
     int64_t drop;    // test hook: a descriptor whose group's bulk copies are not issued (-1: none)
     uint32_t polls;  // bound of every mbarrier wait
@@ -206,22 +205,28 @@ struct mat_view {
     int64_t m, n;
 };
 
+// B: a batch kernel (the matrix index rides in the descriptor's column)
+template <bool B>
 __device__ __forceinline__ mat_view view_of(const ring_args& P, int mid)
 {
-    if (!P.mats)
+    if constexpr (!B) {
         return mat_view{P.A.payload, P.A.values, P.x, P.y, P.A.m, P.A.n};
-    const ring_mat& a = P.mats[mid];
-    return mat_view{a.payload, a.values, P.xs[mid], P.ys[mid], a.m, a.n};
+    } else {
+        const ring_mat& a = P.mats[mid];
+        return mat_view{a.payload, a.values, P.xs[mid], P.ys[mid], a.m, a.n};
+    }
 }
 
-__device__ __forceinline__ uint32_t col_of(const ring_args& P, uint32_t col)
+template <bool B>
+__device__ __forceinline__ uint32_t col_of(uint32_t col)
 {
-    return P.col_bits >= 32 ? col : col & ((1u << P.col_bits) - 1u);
+    return B ? col & ((1u << kBatchColBits) - 1u) : col;
 }
 
-__device__ __forceinline__ int mid_of(const ring_args& P, uint32_t col)
+template <bool B>
+__device__ __forceinline__ int mid_of(uint32_t col)
 {
-    return P.col_bits >= 32 ? 0 : (int)(col >> P.col_bits);
+    return B ? (int)(col >> kBatchColBits) : 0;
 }
 
 // Values before the tile's first value in its first 16-byte granule.
@@ -315,7 +320,7 @@ struct group_geo {
 
 // Producer warp: queues the group's slot at ring offset off as queue slot q;
 // it completes on full[q].
-template <int S, int K, int VT>
+template <int S, int K, int VT, bool B>
 __device__ __forceinline__ void issue_group(const ring_args& P, const mat_view& mv, const ring_desc& d, int yk,
                                             const group_geo& gg, uint32_t off, int q, ring_smem<S, K, VT>& sm,
                                             bool drop, int lane)
@@ -333,7 +338,7 @@ __device__ __forceinline__ void issue_group(const ring_args& P, const mat_view& 
     const T* Y = static_cast<const T*>(mv.y);
     const int total = gg.ntiles * S * K;
     if (gg.ntiles == 1) {  // lane 0 holds the tile's descriptor
-        const uint32_t col = col_of(P, __shfl_sync(kFull, d.col, 0)), info = __shfl_sync(kFull, d.info, 0);
+        const uint32_t col = col_of<B>(__shfl_sync(kFull, d.col, 0)), info = __shfl_sync(kFull, d.info, 0);
         const int64_t c0 = (int64_t)col * S, r0 = (int64_t)(info & kRowMask) * S;
 #pragma unroll
         for (int k = lane; k < S * K; k += 32) {
@@ -348,7 +353,7 @@ __device__ __forceinline__ void issue_group(const ring_args& P, const mat_view& 
     }
     for (int e0 = 0; gg.ntiles > 1 && e0 < total; e0 += 32) {
         const int e = e0 + lane, jj = (e / (S * K)) & 31, k = e % (S * K);
-        const uint32_t col = col_of(P, __shfl_sync(kFull, d.col, jj));
+        const uint32_t col = col_of<B>(__shfl_sync(kFull, d.col, jj));
         const uint32_t info = __shfl_sync(kFull, d.info, jj);
         const int ykk = __shfl_sync(kFull, yk, jj);
         if (e < total) {
@@ -563,7 +568,7 @@ __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs,
 
 // Adds tile j of a queued group onto the lane's row accumulators; the first
 // tile of a block row loads them from its y block, the last writes them to y.
-template <int S, int K, int VT>
+template <int S, int K, int VT, bool B>
 __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot, const slot_rec& r, int j, int& yk,
                                          ring_smem<S, K, VT>& sm, typename val_traits<VT>::T (&acc)[K], int warp,
                                          int lane)
@@ -591,16 +596,18 @@ __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot
     }
     if (d.info & kLast) {
         const int64_t rr = (int64_t)(d.info & kRowMask) * S + row;
-        if (rr < r.m) {
+        const int64_t m = B ? r.m : P.A.m;
+        T* y = static_cast<T*>(B ? r.y : P.y);
+        if (rr < m) {
 #pragma unroll
             for (int h = 0; h < K; ++h)
-                static_cast<T*>(r.y)[rr * P.ldy + h] = acc[h];
+                y[rr * P.ldy + h] = acc[h];
         }
     }
 }
 
 // Warps 0 .. S/32 - 1 sum; warp S/32 produces.
-template <int S, int K, int VT>
+template <int S, int K, int VT, bool B>
 __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args P)
 {
     constexpr int NC = S / 32;  // consumer warps
@@ -669,7 +676,8 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                 const int64_t pvo = __shfl_up_sync(kFull, d.vo, 1), pio = __shfl_up_sync(kFull, d.io, 1);
                 const uint32_t pnv = __shfl_up_sync(kFull, d.nv, 1), ppb = __shfl_up_sync(kFull, d.pb_sch, 1) & 0xffffffu;
                 const uint32_t pcol = __shfl_up_sync(kFull, d.col, 1);
-            const bool contig = lane == 0 || (d.vo == pvo + pnv && d.io == pio + ppb && mid_of(P, d.col) == mid_of(P, pcol));
+            const bool contig =
+                lane == 0 || (d.vo == pvo + pnv && d.io == pio + ppb && (!B || mid_of<B>(d.col) == mid_of<B>(pcol)));
                 const bool first = (d.info & kFirst) != 0;
                 const int est = have ? 32 + (first ? XB : 0) + XB + (int)(d.pb_sch & 0xffffffu) + (int)d.nv * VB : 0;
                 const int cum = warp_inclusive_sum(est, lane);
@@ -724,8 +732,8 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                 break;
             }
             const bool drop = P.drop >= eb + i && P.drop < eb + i + L;
-            const mat_view mv = view_of(P, mid_of(P, __shfl_sync(kFull, d.col, 0)));
-            issue_group<S, K, VT>(P, mv, d, yk, gg, (uint32_t)off, issued % kMaxQ, sm, drop, lane);
+            const mat_view mv = view_of<B>(P, mid_of<B>(__shfl_sync(kFull, d.col, 0)));
+            issue_group<S, K, VT, B>(P, mv, d, yk, gg, (uint32_t)off, issued % kMaxQ, sm, drop, lane);
             if (lane == issued % kMaxQ)
                 my_off = off;
             if (issued == done)
@@ -754,7 +762,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
             int yk = 0;
 #pragma unroll 1
             for (int j = 0; j < L; ++j)
-                sum_tile<S, K, VT>(P, slot, r, j, yk, sm, acc, warp, lane);
+                sum_tile<S, K, VT, B>(P, slot, r, j, yk, sm, acc, warp, lane);
             __syncwarp();
             if (lane == 0)
                 mbar_arrive(&sm.empty[q]);
@@ -831,20 +839,20 @@ void launch_ring(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int
     static_assert(((sizeof(ring_smem<S, K, VT>) + 1023) / 1024 + 1) * 1024 * kCtasPerSm <= 233472,
                   "kCtasPerSm CTAs fit an SM even with shared memory allocated in 1 KiB granules");
     ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()),
-                a.ring_wbeg.get(), x, y, ldx, ldy, nullptr, nullptr, nullptr, 32,
+                a.ring_wbeg.get(), x, y, ldx, ldy, nullptr, nullptr, nullptr,
                 a.dev_status.get(), g_drop_desc, g_spin_limit ? g_spin_limit : kWaitPolls};
-    k_spmv_f64_ring<S, K, VT><<<(unsigned)a.ring_warps, S + 32, sizeof(ring_smem<S, K, VT>), st>>>(P);
+    k_spmv_f64_ring<S, K, VT, false><<<(unsigned)a.ring_warps, S + 32, sizeof(ring_smem<S, K, VT>), st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }
 
-template <int S, int K, int VT>
+template <int S, int K, int VT, bool B = false>
 int ring_ctas_per_sm()
 {
     int nb = 0;
-    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S, K, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S, K, VT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sizeof(ring_smem<S, K, VT>)));
-    ABHSF_CUDA(
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S, K, VT>, S + 32, sizeof(ring_smem<S, K, VT>)));
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S, K, VT, B>, S + 32,
+                                                             sizeof(ring_smem<S, K, VT>)));
     return std::max(nb, 1);
 }
 
@@ -1031,6 +1039,10 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
 
 void prepare_batch(abhsf_batch& b, cudaStream_t st)
 {
+    if (b.s == 32)
+        ring_ctas_per_sm<32, 1, ABHSF_VALUE_F64, true>();
+    else
+        ring_ctas_per_sm<64, 1, ABHSF_VALUE_F64, true>();
     std::vector<ring_mat> table;
     for (const abhsf_matrix* a : b.mats)
         table.push_back(ring_mat{a->payload.get(), a->values.get(), a->m, a->n});
@@ -1057,15 +1069,14 @@ void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys
     P.mats = reinterpret_cast<const ring_mat*>(b.table.get());
     P.xs = reinterpret_cast<const void* const*>(xs);
     P.ys = reinterpret_cast<void* const*>(ys);
-    P.col_bits = kBatchColBits;
     P.status = b.dev_status.get();
     P.drop = -1;
     P.polls = g_spin_limit ? g_spin_limit : kWaitPolls;
     if (b.s == 32)
-        k_spmv_f64_ring<32, 1, ABHSF_VALUE_F64>
+        k_spmv_f64_ring<32, 1, ABHSF_VALUE_F64, true>
             <<<(unsigned)b.ctas, 32 + 32, sizeof(ring_smem<32, 1, ABHSF_VALUE_F64>), st>>>(P);
     else
-        k_spmv_f64_ring<64, 1, ABHSF_VALUE_F64>
+        k_spmv_f64_ring<64, 1, ABHSF_VALUE_F64, true>
             <<<(unsigned)b.ctas, 64 + 32, sizeof(ring_smem<64, 1, ABHSF_VALUE_F64>), st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }

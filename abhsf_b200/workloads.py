@@ -222,6 +222,44 @@ def batched_set(count: int = 256, n_min: int = 1000, n_max: int = 200000, seed: 
             yield rmat(int(ns[i]), 8, seed=seed * 100003 + i)
 
 
+def batched_set_device(count: int = 256, n_min: int = 1000, n_max: int = 200000, seed: int = 0, device="cuda"):
+    """The batched workload generated on the GPU (torch's seeded Philox
+    generator; the same distributions as batched_set, other random streams):
+    yields (rows, cols, vals, m, n, name) with int64 / float64 CUDA tensors."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max), count)).astype(np.int64)
+    bws = rng.integers(3, 65, count)
+    for i in range(count):
+        n = int(ns[i])
+        if i % 2 == 0:
+            bw = int(bws[i])
+            offs = torch.arange(-bw, bw + 1, device=device, dtype=torch.int64)
+            rows = torch.arange(n, device=device, dtype=torch.int64).repeat_interleave(offs.numel())
+            cols = rows + offs.repeat(n)
+            ok = (cols >= 0) & (cols < n)
+            rows, cols = rows[ok], cols[ok]
+            name = f"banded_{n}_bw{bw}"
+        else:
+            k = max(1, int(np.ceil(np.log2(max(n, 2)))))
+            e = 8 * n
+            r = torch.zeros(e, device=device, dtype=torch.int64)
+            c = torch.zeros(e, device=device, dtype=torch.int64)
+            for level in range(k):
+                u = torch.rand(e, device=device, generator=g, dtype=torch.float64)
+                bit = 1 << (k - 1 - level)
+                r += (u >= 0.76).to(torch.int64) * bit
+                c += (((u >= 0.57) & (u < 0.76)) | (u >= 0.95)).to(torch.int64) * bit
+            ok = (r < n) & (c < n)
+            key = torch.unique(r[ok] * n + c[ok])
+            rows, cols = key // n, key % n
+            name = f"rmat_{n}_ef8"
+        vals = torch.randn(rows.numel(), device=device, generator=g, dtype=torch.float64)
+        yield rows, cols, vals, n, n, name
+
+
 def rhs(n: int, seed: int = 0) -> np.ndarray:
     """x uniform[-1, 1]."""
     return np.random.default_rng(seed).uniform(-1.0, 1.0, size=n)

@@ -183,6 +183,71 @@ def time_lowprec(c, dev, l2_flush, warmup, steps=10):
     return out
 
 
+def time_batched(dev, l2_flush, warmup, count=256, steps=10):
+    """The batched workload (count matrices, n log-uniform [1k, 200k], half
+    banded with bandwidth U[3, 64], half R-MAT(0.57, 0.19, 0.19) edge factor 8,
+    values N(0,1), generated on the GPU), block size 64: all SpMVs as one
+    launch (abhsf_batch_spmv) against one abhsf_spmv launch per matrix."""
+    import torch
+    from abhsf_b200 import AbhsfBatch, AbhsfMatrix
+    from abhsf_b200 import workloads as W
+    t0 = time.time()
+    mats, byts, nnz = [], 0, 0
+    for rows, cols, vals, m, n, _ in W.batched_set_device(count, seed=0, device=dev):
+        A = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=64)
+        mats.append(A)
+        byts += int(A.stats()["format_bytes"]) + 8 * n + 16 * m
+        nnz += int(rows.numel())
+        del rows, cols, vals
+    build_s = time.time() - t0
+    xs = [torch.rand(A.n, dtype=torch.float64, device=dev) for A in mats]
+    ys = [torch.zeros(A.m, dtype=torch.float64, device=dev) for A in mats]
+    batch = AbhsfBatch(mats)
+    px, py = batch.pointer_tables(xs, ys)
+
+    def timed(fn):
+        for _ in range(max(warmup, 1)):
+            l2_flush()
+            fn()
+        ts = []
+        for _ in range(steps):
+            l2_flush()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return sum(ts) / len(ts)
+
+    def one_by_one():
+        for A, x, y in zip(mats, xs, ys):
+            A.spmv(x, y)
+
+    t_batch = timed(lambda: batch.spmv_tables(px, py))
+    t_loop = timed(one_by_one)
+    # spot check: matrix 0 through the batch equals its own SpMV
+    y_a, y_b = ys[0].clone(), ys[0].clone()
+    mats[0].spmv(xs[0], y_a)
+    ys[0].copy_(y_b)
+    batch.spmv_tables(px, py)
+    torch.cuda.synchronize()
+    same = bool(torch.equal(ys[0], y_a))
+    if batch.status() != 0:
+        raise RuntimeError("batched SpMV reported a device status")
+    out = {"workload": f"{count} matrices, n log-uniform [1k, 200k], even banded (bandwidth U[3,64]), odd R-MAT"
+                       f"(0.57, 0.19, 0.19) edge factor 8, values N(0,1), generated on the GPU, block size 64",
+           "nnz": nnz, "bytes_per_step": byts, "build_s": build_s,
+           "batched": {"ms": t_batch, "GB/s": byts / (t_batch * 1e-3) / 1e9, "launches": 1},
+           "one_by_one": {"ms": t_loop, "GB/s": byts / (t_loop * 1e-3) / 1e9, "launches": count},
+           "speedup": t_loop / t_batch, "matrix0_bitwise": same}
+    batch.release()
+    for A in mats:
+        A.release()
+    return out
+
+
 def time_cg(dev, g=256, rtol=1e-10):
     """CG solve time on the 3D 7-point Laplacian g^3 (n = g^3, SPD, b U[-1,1]
     seed 1, x0 = 0) to ||b - A x|| <= rtol ||b||: plain FP64 CG against the
@@ -367,6 +432,7 @@ def run_ours(args):
     spmm = None if args.no_spmm else time_spmm(A, c, st, dev, stream, l2_flush, args.warmup)
     lowprec = None if args.no_lowprec else time_lowprec(c, dev, l2_flush, args.warmup)
     cg_times = None if args.no_cg or rank != 0 else time_cg(dev)
+    batched = None if args.no_batched or rank != 0 else time_batched(dev, l2_flush, args.warmup)
 
     peak, peak_src = hbm_peak()
     achieved = B / (t_mean * 1e-3) / 1e9
@@ -399,6 +465,7 @@ def run_ours(args):
             "spmm": spmm,
             "lowprec": lowprec,
             "cg": cg_times,
+            "batched": batched,
             "e2e": {"value": world * B / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
                     "d2h_bytes_per_step": 8 * c.m, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": args.steps,
@@ -421,6 +488,7 @@ def main():
     ap.add_argument("--no-spmm", action="store_true", help="skip the multi-right-hand-side timings")
     ap.add_argument("--no-lowprec", action="store_true", help="skip the f32 / bf16 SpMV timings")
     ap.add_argument("--no-cg", action="store_true", help="skip the CG solves on the 3D Laplacian")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 256-matrix batched launch")
     ap.add_argument("--sum-order", choices=["reference", "tree"], default="reference",
                     help="reference: bitwise the reference CSR's y; tree: warp reduction trees")
     ap.add_argument("--n", type=int, default=DEFAULT_N,
