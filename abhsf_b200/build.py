@@ -28,7 +28,7 @@ def _sources() -> list[str]:
 
 
 def _deps() -> list[str]:
-    return (_sources() + glob.glob(os.path.join(CSRC, "*.cuh")) +
+    return (_sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.inc")) +
             glob.glob(os.path.join(ROOT, "include", "abhsf", "*.h")))
 
 

@@ -21,6 +21,11 @@ MATRIX_TYPES = {"binary": 0, "integer": 1, "real": 2, "complex": 3}
 SUM_ORDERS = {"reference": 0, "tree": 1}
 NOALLOC_MAX_NNZ = 1048576
 DEVSTAT_WAIT_TIMEOUT = 1
+SELECTORS = {"minbss": 0, "learned": 1}
+FEATURES, MLP_HIDDEN, MLP_CLASSES = 12, 64, 5
+MLP_PARAMS = (FEATURES * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN +
+              MLP_HIDDEN * MLP_CLASSES + MLP_CLASSES + 2 * FEATURES)
+BLOCK_SIZES = (16, 32, 64, 128, 256)
 
 
 class AbhsfError(RuntimeError):
@@ -60,7 +65,8 @@ _ERR = {INVALID_VALUE: InvalidValue, INDEX_OUT_OF_RANGE: IndexOutOfRange, DUPLIC
 class BuildOpts(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("value_type", C.c_int32), ("allow_csr", C.c_int32),
                 ("matrix_type", C.c_int32), ("forced_scheme", C.c_int32), ("inputs_on_device", C.c_int32),
-                ("sum_order", C.c_int32), ("bits_per_value", C.c_int64)]
+                ("sum_order", C.c_int32), ("bits_per_value", C.c_int64), ("selector", C.c_int32),
+                ("reserved", C.c_int32), ("selector_model", C.c_void_p)]
 
 
 class CgInfo(C.Structure):
@@ -81,6 +87,7 @@ _vp = C.c_void_p
 _i64 = C.c_int64
 _i32 = C.c_int32
 _u64p = C.POINTER(C.c_uint64)
+_fp = C.POINTER(C.c_float)
 
 # name -> (restype, argtypes)
 PROTOTYPES = {
@@ -109,6 +116,14 @@ PROTOTYPES = {
     "abhsf_block_histogram_noalloc": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _i32, _vp, _u64p, _i64,
                                                 C.POINTER(_i64)]),
     "abhsf_mmf_line": (C.c_int, [_i64, _i64, _i64, _i32, _i32, _i32, _u64p, _i64, _u64p, _u64p]),
+    "abhsf_block_size_storage": (C.c_int, [_vp, _vp, _i64, _i64, _i64, C.POINTER(BuildOpts), _vp, _u64p,
+                                           C.POINTER(_i32)]),
+    "abhsf_selector_features": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _vp, _fp]),
+    "abhsf_selector_predict": (C.c_int, [_vp, _fp, _vp, C.POINTER(_i32)]),
+    "abhsf_selector_builtin_model": (C.c_int, [_fp]),
+    "abhsf_mlp_forward": (C.c_int, [_vp, _vp, _i32, _vp, _vp, _vp]),
+    "abhsf_mlp_backward": (C.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "abhsf_mlp_adam": (C.c_int, [_vp, _vp, _vp, _vp, _i32, C.c_float, _vp]),
     "abhsf_block_scheme_bits": (C.c_uint64, [_i32, _i64, _i64, _i64, _i64]),
     "abhsf_block_select_scheme": (_i32, [_i64, _i64, _i64, _i64, _i32, _i32]),
 }

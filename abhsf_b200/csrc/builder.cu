@@ -391,6 +391,45 @@ void mmf_line_from_hist(int64_t m, int64_t n, int64_t nnz, int type, int64_t r, 
     std::copy(s2, s2 + 8, o2);
 }
 
+// ABHSF storage (bits, the mmf line's abhsf column at the stored value width,
+// CSR as the options allow) of square block sizes 16, 32, 64, 128, 256: the
+// quantity the reference's min-bss tool minimises (block_statistics/min-bss.cpp:14-58).
+void block_size_storage(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n,
+                        const abhsf_build_opts& o, cudaStream_t st, uint64_t bits[kNumBlockSizes])
+{
+    if (o.value_type < 0 || o.value_type > 2)
+        fail(ABHSF_ERROR_INVALID_VALUE, "value_type out of range");
+    if (o.matrix_type < 0 || o.matrix_type > 3)
+        fail(ABHSF_ERROR_INVALID_VALUE, "matrix_type out of range");
+    const uint64_t dense_bits = o.bits_per_value > 0 ? (uint64_t)o.bits_per_value : 8 * value_size(o.value_type);
+    const uint64_t bits1 = (o.matrix_type == ABHSF_MATRIX_BINARY) ? 0 : dense_bits / 2;
+    if (nnz > 0 && (!rows || !cols))
+        fail(ABHSF_ERROR_INVALID_VALUE, "rows and cols must be non-NULL");
+    coo_inputs in(rows, cols, nullptr, nnz, o.inputs_on_device != 0, st);  // host inputs cross once
+    for (int k = 0; k < kNumBlockSizes; ++k) {
+        const int s = 16 << k;
+        std::vector<uint64_t> h((size_t)s * s + 1);
+        int64_t blocks = 0;
+        block_histogram(in.rows, in.cols, nnz, m, n, s, s, true, st, h.data(), (int64_t)h.size(), &blocks);
+        std::map<uint64_t, uint64_t> hist;
+        for (size_t z = 1; z < h.size(); ++z)
+            if (h[z])
+                hist[z] = h[z];
+        uint64_t o1[8], o2[8];
+        mmf_line_from_hist(m, n, nnz, o.matrix_type, s, s, hist, bits1, o1, o2);
+        bits[k] = o.allow_csr ? o2[6] : o2[7];
+    }
+}
+
+int select_block_size(const uint64_t bits[kNumBlockSizes])
+{
+    int best = 0;
+    for (int k = 1; k < kNumBlockSizes; ++k)
+        if (bits[k] < bits[best])
+            best = k;
+    return 16 << best;
+}
+
 namespace {
 
 void finish_stats(abhsf_matrix& a, uint64_t dense_bits, cudaStream_t st)

@@ -77,6 +77,9 @@ void abhsf_build_opts_default(abhsf_build_opts* o)
     o->inputs_on_device = 0;
     o->sum_order = ABHSF_SUM_REFERENCE;
     o->bits_per_value = 0;
+    o->selector = ABHSF_SELECT_MINBSS;
+    o->reserved = 0;
+    o->selector_model = nullptr;
 }
 
 abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, const double* vals, int64_t nnz, int64_t m,
@@ -90,6 +93,20 @@ abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, const double*
         abhsf_build_opts_default(&o);
         if (opts)
             o = *opts;
+        if (o.block_size == 0) {
+            const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+            if (o.selector == ABHSF_SELECT_MINBSS) {
+                uint64_t bits[abhsf::kNumBlockSizes];
+                abhsf::block_size_storage(rows, cols, nnz, m, n, o, st, bits);
+                o.block_size = abhsf::select_block_size(bits);
+            } else if (o.selector == ABHSF_SELECT_LEARNED) {
+                float f[ABHSF_FEATURES];
+                abhsf::selector_features(rows, cols, nnz, m, n, o.inputs_on_device != 0, st, f);
+                o.block_size = abhsf::mlp_predict(o.selector_model, f, st);
+            } else {
+                fail(ABHSF_ERROR_INVALID_VALUE, "selector out of range");
+            }
+        }
         auto a = std::make_unique<abhsf_matrix>();
         abhsf::build_matrix(rows, cols, vals, nnz, m, n, o, reinterpret_cast<cudaStream_t>(stream), *a);
         *out = a.release();
@@ -339,6 +356,81 @@ abhsf_status abhsf_block_histogram_noalloc(const int64_t* rows, const int64_t* c
     return guarded([&] {
         abhsf::block_histogram_noalloc(rows, cols, nnz, m, n, r, s, reinterpret_cast<cudaStream_t>(stream), hist,
                                        hist_len, blocks);
+    });
+}
+
+abhsf_status abhsf_block_size_storage(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n,
+                                      const abhsf_build_opts* opts, abhsf_stream_t stream, uint64_t bits[5],
+                                      int32_t* best)
+{
+    static_assert(abhsf::kNumBlockSizes == 5, "bits[5] in the header");
+    return guarded([&] {
+        if (!bits)
+            fail(ABHSF_ERROR_INVALID_VALUE, "bits must be non-NULL");
+        if (m <= 0 || n <= 0 || nnz < 0)
+            fail(ABHSF_ERROR_INVALID_VALUE, "m and n must be positive and nnz non-negative");
+        abhsf_build_opts o;
+        abhsf_build_opts_default(&o);
+        if (opts)
+            o = *opts;
+        abhsf::block_size_storage(rows, cols, nnz, m, n, o, reinterpret_cast<cudaStream_t>(stream), bits);
+        if (best)
+            *best = abhsf::select_block_size(bits);
+    });
+}
+
+abhsf_status abhsf_selector_features(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n,
+                                     int32_t inputs_on_device, abhsf_stream_t stream, float out[12])
+{
+    static_assert(ABHSF_FEATURES == 12, "out[12] in the header");
+    return guarded([&] {
+        abhsf::selector_features(rows, cols, nnz, m, n, inputs_on_device != 0,
+                                 reinterpret_cast<cudaStream_t>(stream), out);
+    });
+}
+
+abhsf_status abhsf_selector_predict(const float* model, const float features[12], abhsf_stream_t stream,
+                                    int32_t* block_size)
+{
+    return guarded([&] {
+        if (!block_size)
+            fail(ABHSF_ERROR_INVALID_VALUE, "block_size must be non-NULL");
+        *block_size = abhsf::mlp_predict(model, features, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+abhsf_status abhsf_selector_builtin_model(float* out)
+{
+    return guarded([&] {
+        if (!out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "out must be non-NULL");
+        std::copy(abhsf::builtin_model(), abhsf::builtin_model() + ABHSF_MLP_PARAMS, out);
+    });
+}
+
+abhsf_status abhsf_mlp_forward(const float* params, const float* x, int32_t batch, float* probs, float* act,
+                               abhsf_stream_t stream)
+{
+    return guarded([&] {
+        abhsf::mlp_forward(params, x, batch, probs, act, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+abhsf_status abhsf_mlp_backward(const float* params, const float* x, const float* targets, int32_t batch,
+                                const float* probs, const float* act, float* delta, float* grad, float* loss,
+                                abhsf_stream_t stream)
+{
+    return guarded([&] {
+        abhsf::mlp_backward(params, x, targets, batch, probs, act, delta, grad, loss,
+                            reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+abhsf_status abhsf_mlp_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr,
+                            abhsf_stream_t stream)
+{
+    return guarded([&] {
+        abhsf::mlp_adam(params, grad, m, v, step, lr, reinterpret_cast<cudaStream_t>(stream));
     });
 }
 

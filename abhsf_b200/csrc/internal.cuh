@@ -17,6 +17,23 @@ void block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int6
 void block_histogram_noalloc(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r,
                              int s, cudaStream_t st, uint64_t* hist, int64_t hist_len, int64_t* blocks);
 
+// ABHSF storage of square block sizes 16 .. 256 (index k: size 16 << k) and
+// the size of least storage, ties to the smaller (min-bss).
+constexpr int kNumBlockSizes = 5;
+void block_size_storage(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n,
+                        const abhsf_build_opts& o, cudaStream_t st, uint64_t bits[kNumBlockSizes]);
+int select_block_size(const uint64_t bits[kNumBlockSizes]);
+
+// Learned block-size selector (selector.cu): per-matrix features and the MLP.
+void selector_features(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, bool on_device,
+                       cudaStream_t st, float out[ABHSF_FEATURES]);
+void mlp_forward(const float* p, const float* x, int batch, float* probs, float* act, cudaStream_t st);
+void mlp_backward(const float* p, const float* x, const float* target, int batch, const float* probs, const float* act,
+                  float* delta, float* grad, float* loss, cudaStream_t st);
+void mlp_adam(float* p, const float* g, float* m, float* v, int step, float lr, cudaStream_t st);
+int mlp_predict(const float* model_host, const float features[ABHSF_FEATURES], cudaStream_t st);
+const float* builtin_model();  // ABHSF_MLP_PARAMS floats, host memory
+
 void mmf_line_from_hist(int64_t m, int64_t n, int64_t nnz, int type, int64_t r, int64_t s,
                         const std::map<uint64_t, uint64_t>& hist, uint64_t bits1, uint64_t o1[8], uint64_t o2[8]);
 

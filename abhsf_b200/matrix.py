@@ -47,10 +47,16 @@ def _ptr(a) -> int:
 
 
 def _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_device,
-          sum_order="reference") -> capi.BuildOpts:
+          sum_order="reference", selector="minbss", selector_model=None) -> capi.BuildOpts:
     o = capi.BuildOpts()
     capi.lib.abhsf_build_opts_default(C.byref(o))
-    o.block_size = int(block_size)
+    o.block_size = 0 if block_size == "auto" else int(block_size)
+    o.selector = capi.SELECTORS[selector]
+    if selector_model is not None:
+        if selector_model.dtype != np.float32 or selector_model.size != capi.MLP_PARAMS \
+                or not selector_model.flags.c_contiguous:
+            raise capi.InvalidValue(capi.INVALID_VALUE, f"selector_model must be {capi.MLP_PARAMS} contiguous float32")
+        o.selector_model = selector_model.ctypes.data
     o.value_type = capi.VALUE_TYPES[value_type]
     o.allow_csr = 1 if allow_csr else 0
     o.matrix_type = capi.MATRIX_TYPES[matrix_type]
@@ -75,14 +81,18 @@ class AbhsfMatrix:
 
     # ------------------------------------------------------------------ build
     @classmethod
-    def from_elements(cls, rows, cols, vals, m: int, n: int, *, block_size: int = 64, value_type: str = "f64",
-                      allow_csr: bool = True, matrix_type: str = "real", forced_scheme=None,
-                      bits_per_value: int = 0, sum_order: str = "reference", stream=None) -> "AbhsfMatrix":
+    def from_elements(cls, rows, cols, vals, m: int, n: int, *, block_size: int | str = 64,
+                      value_type: str = "f64", allow_csr: bool = True, matrix_type: str = "real",
+                      forced_scheme=None, bits_per_value: int = 0, sum_order: str = "reference",
+                      selector: str = "minbss", selector_model=None, stream=None) -> "AbhsfMatrix":
         """Builds from COO triplets (0-based, any order, no duplicates).
         Scheme per tile by exact minimum storage (msmf.h:35-63) unless
         forced_scheme names one.  vals may be None for binary matrices.
         sum_order "reference" makes spmv bitwise equal to the reference's CSR
-        spmv_naive; "tree" uses warp reduction trees."""
+        spmv_naive; "tree" uses warp reduction trees.  block_size "auto"
+        lets `selector` choose it: "minbss" (least storage over 16..256, the
+        exhaustive sweep) or "learned" (the MLP; selector_model: float32
+        parameters, None = the built-in model)."""
         on_dev = _is_cuda(rows)
         if on_dev:
             if not (_is_cuda(cols) and (vals is None or _is_cuda(vals))):
@@ -98,7 +108,8 @@ class AbhsfMatrix:
         if (cols.numel() if on_dev else cols.size) != nnz or (
                 vals is not None and (vals.numel() if on_dev else vals.size) != nnz):
             raise capi.InvalidValue(capi.INVALID_VALUE, "rows, cols and vals differ in length")
-        o = _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_dev, sum_order)
+        o = _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_dev, sum_order,
+                  selector, selector_model)
         h = C.c_void_p()
         capi.check(capi.lib.abhsf_build(_ptr(rows) if nnz else None, _ptr(cols) if nnz else None,
                                         _ptr(vals) if (vals is not None and nnz) else None, nnz, int(m), int(n),
@@ -106,8 +117,8 @@ class AbhsfMatrix:
         A = cls()
         A._h = h
         A.m, A.n, A.nnz = int(m), int(n), nnz
-        A.block_size = int(block_size)
         A.value_type = value_type
+        A.block_size = A.stats()["block_size"] if block_size == "auto" else int(block_size)
         return A
 
     # ------------------------------------------------------------------ spmv

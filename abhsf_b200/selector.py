@@ -1,0 +1,327 @@
+"""Block-size selection: the exhaustive min-bss sweep and the learned MLP.
+
+The reference picks the block size of a matrix by computing its block
+statistics at every candidate size and taking the one of least storage
+(block_statistics/min-bss.cpp:14-58), and judges restricted choices by their
+regret, the storage above the minimum in percent, averaged and maximised over
+matrices (block_statistics/consistency.cpp:140-174).
+
+Here the sweep runs on the GPU (abhsf_block_size_storage: five block
+histograms, sizes 16..256) and a small MLP (12 features -> 64 -> 64 -> 5,
+ReLU, FP32; abhsf_selector_features / abhsf_mlp_*) predicts its answer from
+one pass of features.  The network is trained on the GPU by the library's own
+forward, backward and Adam kernels; this module holds the data set, the
+training loop and the regret report:
+
+    python -m abhsf_b200.selector train --out DIR [--train 2000 --heldout 200]
+
+writes DIR/selector_model.inc (the model built into the library, copied to
+abhsf_b200/csrc/), DIR/selector_model.f32, DIR/selector_data.npz (features
+and storage of every matrix), DIR/selector_heldout.npz (the held-out part,
+copied to tests/golden/) and DIR/selector_report.json.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import time
+
+import numpy as np
+
+from . import capi
+
+F, H, NC, P = capi.FEATURES, capi.MLP_HIDDEN, capi.MLP_CLASSES, capi.MLP_PARAMS
+SIZES = capi.BLOCK_SIZES
+# parameter offsets, the layout of include/abhsf/abhsf_gpu.h
+OW1 = 0
+OB1 = OW1 + F * H
+OW2 = OB1 + H
+OB2 = OW2 + H * H
+OW3 = OB2 + H
+OB3 = OW3 + H * NC
+OMEAN = OB3 + NC
+OISTD = OMEAN + F
+TRAINABLE = OMEAN
+
+
+# ---------------------------------------------------------------- library calls
+
+def _stream_ptr(stream=None):
+    import torch
+    if not torch.cuda.is_available():
+        return None
+    return (stream or torch.cuda.current_stream()).cuda_stream
+
+
+def _coo_args(rows, cols):
+    import torch
+    on_dev = isinstance(rows, torch.Tensor) and rows.is_cuda
+    if on_dev:
+        rows = rows.to(torch.int64).contiguous()
+        cols = cols.to(torch.int64).contiguous()
+        return rows, cols, rows.numel(), rows.data_ptr(), cols.data_ptr(), True
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    cols = np.ascontiguousarray(cols, dtype=np.int64)
+    return rows, cols, rows.size, rows.ctypes.data, cols.ctypes.data, False
+
+
+def block_size_storage(rows, cols, m: int, n: int, allow_csr: bool = True, value_type: str = "f64",
+                       stream=None) -> tuple[np.ndarray, int]:
+    """ABHSF storage in bits at block sizes 16..256 (uint64[5]) and the size
+    of least storage (ties to the smaller)."""
+    rows, cols, nnz, rp, cp, on_dev = _coo_args(rows, cols)
+    o = capi.BuildOpts()
+    capi.lib.abhsf_build_opts_default(C.byref(o))
+    o.inputs_on_device = int(on_dev)
+    o.allow_csr = int(allow_csr)
+    o.value_type = capi.VALUE_TYPES[value_type]
+    bits = np.zeros(5, np.uint64)
+    best = C.c_int32()
+    capi.check(capi.lib.abhsf_block_size_storage(rp if nnz else None, cp if nnz else None, nnz, int(m), int(n),
+                                                 C.byref(o), _stream_ptr(stream),
+                                                 bits.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(best)))
+    return bits, int(best.value)
+
+
+def features(rows, cols, m: int, n: int, stream=None) -> np.ndarray:
+    """The selector's 12 features of a matrix (float32), computed on the GPU."""
+    rows, cols, nnz, rp, cp, on_dev = _coo_args(rows, cols)
+    out = np.zeros(F, np.float32)
+    capi.check(capi.lib.abhsf_selector_features(rp if nnz else None, cp if nnz else None, nnz, int(m), int(n),
+                                                int(on_dev), _stream_ptr(stream),
+                                                out.ctypes.data_as(C.POINTER(C.c_float))))
+    return out
+
+
+def builtin_model() -> np.ndarray:
+    """The model built into the library (float32[MLP_PARAMS])."""
+    out = np.zeros(P, np.float32)
+    capi.check(capi.lib.abhsf_selector_builtin_model(out.ctypes.data_as(C.POINTER(C.c_float))))
+    return out
+
+
+def predict(feats: np.ndarray, model: np.ndarray | None = None, stream=None) -> int:
+    """Block size the model (None = built-in) predicts for one feature vector."""
+    feats = np.ascontiguousarray(feats, dtype=np.float32)
+    mp = None if model is None else np.ascontiguousarray(model, dtype=np.float32)
+    bs = C.c_int32()
+    capi.check(capi.lib.abhsf_selector_predict(None if mp is None else mp.ctypes.data,
+                                               feats.ctypes.data_as(C.POINTER(C.c_float)), _stream_ptr(stream),
+                                               C.byref(bs)))
+    return int(bs.value)
+
+
+class Mlp:
+    """The selector network on the GPU: parameters, Adam moments and the
+    library's forward / backward / Adam kernels over torch buffers."""
+
+    def __init__(self, params: np.ndarray):
+        import torch
+        self.p = torch.from_numpy(np.ascontiguousarray(params, dtype=np.float32)).cuda()
+        self.m = torch.zeros(P, dtype=torch.float32, device="cuda")
+        self.v = torch.zeros(P, dtype=torch.float32, device="cuda")
+        self.g = torch.zeros(P, dtype=torch.float32, device="cuda")
+        self.loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        self.step_count = 0
+
+    def forward(self, x, keep: bool = False):
+        """probs[batch][5] (and the activations when keep) for x[batch][12] (CUDA float32)."""
+        import torch
+        b = x.shape[0]
+        probs = torch.empty(b, NC, dtype=torch.float32, device="cuda")
+        act = torch.empty(b, 2 * H, dtype=torch.float32, device="cuda") if keep else None
+        capi.check(capi.lib.abhsf_mlp_forward(self.p.data_ptr(), x.data_ptr(), b, probs.data_ptr(),
+                                              act.data_ptr() if keep else None, _stream_ptr()))
+        return (probs, act) if keep else probs
+
+    def backward(self, x, targets, probs, act):
+        """Fills self.g (trainable part) and self.loss."""
+        import torch
+        b = x.shape[0]
+        delta = torch.empty(b, NC + 2 * H, dtype=torch.float32, device="cuda")
+        capi.check(capi.lib.abhsf_mlp_backward(self.p.data_ptr(), x.data_ptr(), targets.data_ptr(), b,
+                                               probs.data_ptr(), act.data_ptr(), delta.data_ptr(),
+                                               self.g.data_ptr(), self.loss.data_ptr(), _stream_ptr()))
+
+    def adam(self, lr: float):
+        self.step_count += 1
+        capi.check(capi.lib.abhsf_mlp_adam(self.p.data_ptr(), self.g.data_ptr(), self.m.data_ptr(),
+                                           self.v.data_ptr(), self.step_count, float(lr), _stream_ptr()))
+
+    def params(self) -> np.ndarray:
+        return self.p.cpu().numpy().copy()
+
+
+# ---------------------------------------------------------------- host logic
+
+def init_params(x_train: np.ndarray, seed: int = 0) -> np.ndarray:
+    """He-initialised weights, zero biases, and the input normalisation
+    (mean, 1 / stdev) of the training features."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(P, np.float32)
+    p[OW1:OB1] = rng.standard_normal(F * H) * np.sqrt(2.0 / F)
+    p[OW2:OB2] = rng.standard_normal(H * H) * np.sqrt(2.0 / H)
+    p[OW3:OB3] = rng.standard_normal(H * NC) * np.sqrt(2.0 / H)
+    mean = x_train.mean(axis=0)
+    std = x_train.std(axis=0)
+    p[OMEAN:OISTD] = mean
+    p[OISTD:OISTD + F] = np.where(std > 1e-6, 1.0 / np.maximum(std, 1e-6), 1.0)
+    return p
+
+
+def targets_from_bits(bits: np.ndarray, tau: float = 0.0) -> np.ndarray:
+    """Training targets from the storage of each size: the one-hot argmin
+    (tau = 0) or a softmax of -excess / tau over the sizes, excess being the
+    storage above the minimum as a fraction of it."""
+    b = bits.astype(np.float64)
+    mn = b.min(axis=1, keepdims=True)
+    if tau <= 0:
+        t = np.zeros_like(b)
+        t[np.arange(b.shape[0]), b.argmin(axis=1)] = 1.0
+        return t.astype(np.float32)
+    z = -(b - mn) / mn / tau
+    z -= z.max(axis=1, keepdims=True)
+    e = np.exp(z)
+    return (e / e.sum(axis=1, keepdims=True)).astype(np.float32)
+
+
+def regret(bits: np.ndarray, choice: np.ndarray) -> np.ndarray:
+    """Per matrix: (storage of the chosen size - least storage) / least
+    storage * 100 (block_statistics/consistency.cpp:147-160); choice holds
+    indices 0..4 into bits' columns."""
+    b = bits.astype(np.float64)
+    mn = b.min(axis=1)
+    return (b[np.arange(b.shape[0]), choice] - mn) / mn * 100.0
+
+
+def regret_summary(bits: np.ndarray, choice: np.ndarray) -> dict:
+    """Average and maximum regret over matrices (consistency.cpp:161-173),
+    and the share of matrices whose choice is a minimum."""
+    r = regret(bits, choice)
+    return {"avg_pct": float(r.mean()), "max_pct": float(r.max()), "exact": float((r == 0).mean())}
+
+
+def write_model_inc(params: np.ndarray, path: str) -> None:
+    """The model as the C++ initialiser selector.cu includes."""
+    params = np.asarray(params, dtype=np.float32)
+    assert params.size == P
+    lines = ["// Trained block-size selector: ABHSF_MLP_PARAMS floats in the layout of",
+             "// include/abhsf/abhsf_gpu.h.  Written by abhsf_b200/selector.py; do not edit.",
+             "static const float kBuiltinModel[ABHSF_MLP_PARAMS] = {"]
+    vals = [np.format_float_scientific(v, precision=8, unique=False) + "f" for v in params]
+    for i in range(0, P, 8):
+        lines.append("    " + ", ".join(vals[i:i + 8]) + ",")
+    lines.append("};")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def untrained_model() -> np.ndarray:
+    """A model that always predicts block size 64 (zero weights, b3 one-hot)."""
+    p = np.zeros(P, np.float32)
+    p[OB3 + SIZES.index(64)] = 1.0
+    p[OISTD:OISTD + F] = 1.0
+    return p
+
+
+# ---------------------------------------------------------------- data and training
+
+def dataset(seeds, n_min=10_000, n_max=4_000_000, nnz_max=16_000_000, log=None):
+    """Features (float32[len][12]) and storage at sizes 16..256
+    (uint64[len][5]) of the selector workload's matrices, both on the GPU."""
+    import torch
+    from . import workloads as W
+    X = np.zeros((len(seeds), F), np.float32)
+    B = np.zeros((len(seeds), 5), np.uint64)
+    names = []
+    t_feat = t_sweep = 0.0
+    for i, seed in enumerate(seeds):
+        rows, cols, m, n, name = W.selector_matrix(int(seed), n_min, n_max, nnz_max)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        X[i] = features(rows, cols, m, n)
+        t1 = time.perf_counter()
+        B[i], _ = block_size_storage(rows, cols, m, n)
+        t2 = time.perf_counter()
+        t_feat += t1 - t0
+        t_sweep += t2 - t1
+        names.append(name)
+        if log and (i + 1) % 200 == 0:
+            log(f"{i + 1}/{len(seeds)} matrices  features {t_feat:.1f}s  sweep {t_sweep:.1f}s")
+        del rows, cols
+    return X, B, names, {"features_s": t_feat, "sweep_s": t_sweep}
+
+
+def train(X: np.ndarray, bits: np.ndarray, steps: int = 6000, batch: int = 256, lr: float = 3e-3,
+          tau: float = 0.02, seed: int = 0, log=None) -> np.ndarray:
+    """Adam on the GPU kernels, mini-batches drawn by numpy's default_rng(seed),
+    learning rate decayed by cosine to lr / 20."""
+    import torch
+    net = Mlp(init_params(X, seed))
+    xt = torch.from_numpy(X).cuda()
+    tt = torch.from_numpy(targets_from_bits(bits, tau)).cuda()
+    rng = np.random.default_rng(seed)
+    for step in range(steps):
+        idx = torch.from_numpy(rng.integers(0, X.shape[0], min(batch, X.shape[0]))).cuda()
+        xb, tb = xt[idx].contiguous(), tt[idx].contiguous()
+        probs, act = net.forward(xb, keep=True)
+        net.backward(xb, tb, probs, act)
+        net.adam(lr * (0.05 + 0.95 * 0.5 * (1 + np.cos(np.pi * step / steps))))
+        if log and (step + 1) % 1000 == 0:
+            log(f"step {step + 1}  loss {float(net.loss):.4f}")
+    return net.params()
+
+
+def choose(model: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """Indices 0..4 of the sizes the model picks for each row of X, through
+    the library's forward kernel."""
+    import torch
+    net = Mlp(model)
+    probs = net.forward(torch.from_numpy(np.ascontiguousarray(X, np.float32)).cuda())
+    return probs.argmax(dim=1).cpu().numpy()
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--train", type=int, default=2000)
+    ap.add_argument("--heldout", type=int, default=200)
+    ap.add_argument("--n-max", type=int, default=4_000_000)
+    ap.add_argument("--steps", type=int, default=6000)
+    args = ap.parse_args(argv)
+    os.makedirs(args.out, exist_ok=True)
+
+    def log(msg):
+        print(msg, flush=True)
+
+    seeds_train = np.arange(args.train)
+    seeds_held = np.arange(args.train, args.train + args.heldout)
+    Xtr, Btr, ntr, ttr = dataset(seeds_train, n_max=args.n_max, log=log)
+    Xho, Bho, nho, tho = dataset(seeds_held, n_max=args.n_max, log=log)
+    np.savez_compressed(os.path.join(args.out, "selector_data.npz"), X_train=Xtr, bits_train=Btr,
+                        X_heldout=Xho, bits_heldout=Bho, names_train=np.array(ntr), names_heldout=np.array(nho))
+    # the held-out part alone: the fixture tests/golden/selector_heldout.npz
+    np.savez_compressed(os.path.join(args.out, "selector_heldout.npz"), X=Xho, bits=Bho, names=np.array(nho))
+    t0 = time.perf_counter()
+    model = train(Xtr, Btr, steps=args.steps, log=log)
+    t_train = time.perf_counter() - t0
+    model.tofile(os.path.join(args.out, "selector_model.f32"))
+    write_model_inc(model, os.path.join(args.out, "selector_model.inc"))
+    report = {"train": len(seeds_train), "heldout": len(seeds_held), "train_s": t_train,
+              "features_s_heldout": tho["features_s"], "sweep_s_heldout": tho["sweep_s"]}
+    for split, X, B in (("train", Xtr, Btr), ("heldout", Xho, Bho)):
+        report[split + "_learned"] = regret_summary(B, choose(model, X))
+        for s in SIZES:
+            report[f"{split}_fixed{s}"] = regret_summary(B, np.full(B.shape[0], SIZES.index(s)))
+        report[split + "_label_counts"] = np.bincount(B.astype(np.float64).argmin(axis=1), minlength=5).tolist()
+    with open(os.path.join(args.out, "selector_report.json"), "w") as f:
+        json.dump(report, f, indent=1)
+    log(json.dumps(report))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

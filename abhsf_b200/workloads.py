@@ -260,6 +260,118 @@ def batched_set_device(count: int = 256, n_min: int = 1000, n_max: int = 200000,
         yield rows, cols, vals, n, n, name
 
 
+SELECTOR_FAMILIES = ("banded", "block_diagonal", "rmat", "stencil_2d", "stencil_3d")
+
+
+def selector_matrix(seed: int, n_min: int = 10_000, n_max: int = 4_000_000, nnz_max: int = 16_000_000,
+                    device="cuda"):
+    """One matrix of the block-size selector's workload, generated with torch
+    on `device` (Philox on CUDA; the CPU generator gives other matrices):
+    family seed % 5 of SELECTOR_FAMILIES, n log-uniform in [n_min, n_max]
+    (lowered so that the candidate entries stay within nnz_max), structure
+    parameters drawn from numpy's default_rng(seed):
+
+    banded          |i - j| <= w, w log-uniform [1, 300], each entry kept with
+                    probability U[0.2, 1] (the diagonal always)
+    block_diagonal  b x b diagonal blocks, b log-uniform [2, 512], fill U[0.05, 1]
+    rmat            R-MAT with a U[0.45, 0.65], b = c = d = (1 - a) / 3, edge
+                    factor log-uniform [2, 32], duplicates merged
+    stencil_2d      5- or 9-point stencil on a g1 x g2 grid, g1 / g2 in [1/4, 4]
+    stencil_3d      7- or 27-point stencil on a g1 x g2 x g3 grid
+
+    Returns (rows, cols, m, n, name): int64 tensors on `device`, sorted by
+    row then column."""
+    import torch
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    fam = SELECTOR_FAMILIES[seed % len(SELECTOR_FAMILIES)]
+    n = int(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+    i64 = dict(device=device, dtype=torch.int64)
+
+    def keep(rows, cols, p):
+        u = torch.rand(rows.numel(), device=device, generator=g)
+        ok = (u < p) | (rows == cols)
+        return rows[ok], cols[ok]
+
+    if fam == "banded":
+        w = int(round(np.exp(rng.uniform(0.0, np.log(300.0)))))
+        p = float(rng.uniform(0.2, 1.0))
+        n = max(n_min // 4, min(n, nnz_max // (2 * w + 1)))
+        offs = torch.arange(-w, w + 1, **i64)
+        rows = torch.arange(n, **i64).repeat_interleave(offs.numel())
+        cols = rows + offs.repeat(n)
+        ok = (cols >= 0) & (cols < n)
+        rows, cols = keep(rows[ok], cols[ok], p)
+        name = f"banded_n{n}_w{w}_p{p:.2f}"
+    elif fam == "block_diagonal":
+        b = int(round(np.exp(rng.uniform(np.log(2.0), np.log(512.0)))))
+        p = float(rng.uniform(0.05, 1.0))
+        n = max(n_min // 4, min(n, nnz_max // b))
+        loc = torch.arange(b * b, **i64)
+        base = torch.arange(0, n, b, **i64)
+        rows = (base[:, None] + loc[None, :] // b).reshape(-1)
+        cols = (base[:, None] + loc[None, :] % b).reshape(-1)
+        ok = (rows < n) & (cols < n)
+        rows, cols = keep(rows[ok], cols[ok], p)
+        name = f"block_diagonal_n{n}_b{b}_p{p:.2f}"
+    elif fam == "rmat":
+        a = float(rng.uniform(0.45, 0.65))
+        q = (1.0 - a) / 3.0
+        ef = int(round(np.exp(rng.uniform(np.log(2.0), np.log(32.0)))))
+        n = max(n_min // 4, min(n, nnz_max // ef))
+        k = max(1, int(np.ceil(np.log2(max(n, 2)))))
+        e = ef * n
+        r = torch.zeros(e, **i64)
+        c = torch.zeros(e, **i64)
+        for level in range(k):
+            u = torch.rand(e, device=device, generator=g, dtype=torch.float64)
+            bit = 1 << (k - 1 - level)
+            r += (u >= a + q).to(torch.int64) * bit
+            c += (((u >= a) & (u < a + q)) | (u >= a + 2 * q)).to(torch.int64) * bit
+        ok = (r < n) & (c < n)
+        key = torch.unique(r[ok] * n + c[ok])
+        rows, cols = key // n, key % n
+        name = f"rmat_n{n}_a{a:.2f}_ef{ef}"
+    else:
+        d = 2 if fam == "stencil_2d" else 3
+        wide = bool(rng.integers(0, 2))
+        pts = (9 if wide else 5) if d == 2 else (27 if wide else 7)
+        n = max(n_min // 4, min(n, nnz_max // pts))
+        ratio = np.exp(rng.uniform(np.log(0.25), np.log(4.0), d - 1))
+        side = n ** (1.0 / d)
+        dims = [max(2, int(round(side * r))) for r in ratio]
+        dims.append(max(2, n // int(np.prod(dims))))
+        n = int(np.prod(dims))
+        if wide:
+            offs = np.array(np.meshgrid(*[[-1, 0, 1]] * d, indexing="ij")).reshape(d, -1).T
+        else:
+            offs = np.vstack([np.zeros(d, np.int64)] + [s * np.eye(d, dtype=np.int64)[k]
+                                                        for k in range(d) for s in (-1, 1)])
+        coord = torch.arange(n, **i64)
+        idx = []
+        rem = coord
+        for size in dims[::-1]:
+            idx.append(rem % size)
+            rem = rem // size
+        idx = idx[::-1]  # idx[k]: coordinate along dims[k], the last varying fastest
+        stride = np.cumprod([1] + dims[::-1])[:-1][::-1]
+        rl, cl = [], []
+        for off in offs:
+            ok = torch.ones(n, device=device, dtype=torch.bool)
+            shift = 0
+            for k in range(d):
+                t = idx[k] + int(off[k])
+                ok &= (t >= 0) & (t < dims[k])
+                shift += int(off[k]) * int(stride[k])
+            rl.append(coord[ok])
+            cl.append(coord[ok] + shift)
+        rows, cols = torch.cat(rl), torch.cat(cl)
+        name = f"{fam}_{'x'.join(map(str, dims))}_{pts}pt"
+    key = torch.sort(rows * n + cols).values
+    return key // n, key % n, n, n, name
+
+
 def rhs(n: int, seed: int = 0) -> np.ndarray:
     """x uniform[-1, 1]."""
     return np.random.default_rng(seed).uniform(-1.0, 1.0, size=n)

@@ -100,8 +100,32 @@ typedef enum abhsf_matrix_type {
     ABHSF_MATRIX_COMPLEX = 3
 } abhsf_matrix_type;
 
+/* How abhsf_build picks the block size when opts.block_size is 0.  MINBSS
+ * builds the block histograms of all five sizes and takes the one of least
+ * ABHSF storage, ties to the smaller (block_statistics/min-bss.cpp:14-58).
+ * LEARNED computes ABHSF_FEATURES features in one pass and lets a small MLP
+ * predict that size.  Either way only the block size is chosen: every tile's
+ * scheme, indices and values follow from it exactly. */
+typedef enum abhsf_selector {
+    ABHSF_SELECT_MINBSS = 0,
+    ABHSF_SELECT_LEARNED = 1
+} abhsf_selector;
+
+/* The learned selector's MLP: ABHSF_FEATURES inputs, two hidden layers of
+ * ABHSF_MLP_HIDDEN ReLU units, ABHSF_MLP_CLASSES outputs (block size 16 << k),
+ * FP32.  A model is ABHSF_MLP_PARAMS floats laid out as
+ *   W1[F][H] b1[H] W2[H][H] b2[H] W3[H][C] b3[C] mean[F] inv_std[F]
+ * (row-major, h = relu(x W + b)); the network's input is
+ * (features - mean) * inv_std. */
+#define ABHSF_FEATURES 12
+#define ABHSF_MLP_HIDDEN 64
+#define ABHSF_MLP_CLASSES 5
+#define ABHSF_MLP_PARAMS (ABHSF_FEATURES * ABHSF_MLP_HIDDEN + ABHSF_MLP_HIDDEN + \
+                          ABHSF_MLP_HIDDEN * ABHSF_MLP_HIDDEN + ABHSF_MLP_HIDDEN + \
+                          ABHSF_MLP_HIDDEN * ABHSF_MLP_CLASSES + ABHSF_MLP_CLASSES + 2 * ABHSF_FEATURES)
+
 typedef struct abhsf_build_opts {
-    int32_t block_size;       /* s: 16, 32, 64, 128 or 256 */
+    int32_t block_size;       /* s: 16, 32, 64, 128 or 256; 0 = chosen by `selector` */
     int32_t value_type;       /* abhsf_value_type of the stored values */
     int32_t allow_csr;        /* 1: block_min_msmf (msmf.h:35-48); 0: block_min_msmf_wocsr (msmf.h:50-63) */
     int32_t matrix_type;      /* abhsf_matrix_type; BINARY never selects dense and stores 1.0 values */
@@ -109,6 +133,9 @@ typedef struct abhsf_build_opts {
     int32_t inputs_on_device; /* rows / cols / vals are device pointers */
     int32_t sum_order;        /* abhsf_sum_order of abhsf_spmv / abhsf_spmv_host */
     int64_t bits_per_value;   /* dense-cost element width; 0 = width of value_type */
+    int32_t selector;         /* abhsf_selector, used when block_size is 0 */
+    int32_t reserved;         /* must be 0 */
+    const float* selector_model; /* host, ABHSF_MLP_PARAMS floats; NULL = the model built into the library */
 } abhsf_build_opts;
 
 typedef struct abhsf_matrix abhsf_matrix;
@@ -272,6 +299,62 @@ ABHSF_API abhsf_status abhsf_mmf_line(int64_t m, int64_t n, int64_t nnz, int32_t
 ABHSF_API uint64_t abhsf_block_scheme_bits(int32_t scheme, int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value);
 ABHSF_API int32_t abhsf_block_select_scheme(int64_t r, int64_t s, int64_t nnz, int64_t bits_per_value, int32_t is_binary,
                                   int32_t allow_csr);
+
+/* ABHSF storage in bits (the mmf line's abhsf column, or abhsf134 when
+ * opts->allow_csr is 0, at opts' value width) of the square block sizes 16,
+ * 32, 64, 128, 256 (bits[k]: size 16 << k), from five block histograms on the
+ * GPU, and in *best the size of least storage, ties to the smaller: the
+ * exhaustive block-size sweep of block_statistics/min-bss.cpp:14-58 over
+ * square sizes.  Uses opts' value_type, allow_csr, matrix_type,
+ * inputs_on_device and bits_per_value; NULL opts = defaults.  best may be
+ * NULL.  Synchronises stream. */
+ABHSF_API abhsf_status abhsf_block_size_storage(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m,
+                                                int64_t n, const abhsf_build_opts* opts, abhsf_stream_t stream,
+                                                uint64_t bits[5], int32_t* best);
+
+/* The learned selector's features of a matrix, computed on the GPU
+ * (inputs_on_device: rows / cols are device pointers).  out[12] =
+ *   log2 m, log2 n, log2(nnz/m + 1),
+ *   log2(population stdev of row nnz + 1) (block_statistics/rows-nnz-stdev.cpp:11-30),
+ *   max |i - j| / max(m, n), mean |i - j| / max(m, n),
+ *   shares of the nonzeros lying in 64 x 64 tiles with 1-4, 5-32, 33-256,
+ *   257-1024 and 1025-4096 nonzeros (the tile density histogram),
+ *   log2(nonzero 64 x 64 tiles per block row + 1).
+ * No counterpart in the reference.  Synchronises stream. */
+ABHSF_API abhsf_status abhsf_selector_features(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m,
+                                               int64_t n, int32_t inputs_on_device, abhsf_stream_t stream,
+                                               float out[12]);
+
+/* Block size the MLP `model` (host, ABHSF_MLP_PARAMS floats; NULL = the
+ * built-in model) predicts for features[12]: 16 << argmax of its outputs.
+ * Runs the forward kernel on the current device.  No counterpart in the
+ * reference. */
+ABHSF_API abhsf_status abhsf_selector_predict(const float* model, const float features[12], abhsf_stream_t stream,
+                                              int32_t* block_size);
+
+/* The built-in model (ABHSF_MLP_PARAMS floats) into out. */
+ABHSF_API abhsf_status abhsf_selector_builtin_model(float* out);
+
+/* Training kernels of the MLP, all pointers device memory, ordered on stream.
+ * forward: probs[batch][C] = softmax of the network at x[batch][F]; act
+ * (NULL, or batch * 2 * H floats) keeps the hidden activations for backward.
+ * backward: grad[P] = gradient of the mean cross-entropy against targets
+ * (batch x C probabilities, rows summing to 1; a one-hot row is a label) with
+ * respect to the trainable parameters (all but mean / inv_std, whose entries
+ * of grad are left alone), from forward's probs and act; delta
+ * is scratch of batch * (C + 2 H) floats; loss (NULL allowed) gets the mean
+ * cross-entropy.  The sums over the batch run in sample order, so gradients
+ * are bitwise reproducible.  adam: one Adam step (beta 0.9 / 0.999, eps 1e-8,
+ * bias-corrected by step >= 1) of the trainable parameters with moment
+ * buffers m, v (P floats each, zero at step 1).  No counterpart in the
+ * reference. */
+ABHSF_API abhsf_status abhsf_mlp_forward(const float* params, const float* x, int32_t batch, float* probs,
+                                         float* act, abhsf_stream_t stream);
+ABHSF_API abhsf_status abhsf_mlp_backward(const float* params, const float* x, const float* targets, int32_t batch,
+                                          const float* probs, const float* act, float* delta, float* grad,
+                                          float* loss, abhsf_stream_t stream);
+ABHSF_API abhsf_status abhsf_mlp_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr,
+                                      abhsf_stream_t stream);
 
 /* Waits for the work queued on stream, then returns the matrix's device
  * status word (ABHSF_DEVSTAT_* bits; 0 = every SpMV so far completed) and,
