@@ -21,7 +21,7 @@ MATRIX_TYPES = {"binary": 0, "integer": 1, "real": 2, "complex": 3}
 SUM_ORDERS = {"reference": 0, "tree": 1}
 NOALLOC_MAX_NNZ = 1048576
 DEVSTAT_WAIT_TIMEOUT = 1
-SELECTORS = {"minbss": 0, "learned": 1}
+SELECTORS = {"minbss": 0, "learned": 1, "autotune": 2}
 FEATURES, MLP_HIDDEN, MLP_CLASSES = 12, 64, 5
 MLP_PARAMS = (FEATURES * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN +
               MLP_HIDDEN * MLP_CLASSES + MLP_CLASSES + 2 * FEATURES)
@@ -118,6 +118,8 @@ PROTOTYPES = {
     "abhsf_mmf_line": (C.c_int, [_i64, _i64, _i64, _i32, _i32, _i32, _u64p, _i64, _u64p, _u64p]),
     "abhsf_block_size_storage": (C.c_int, [_vp, _vp, _i64, _i64, _i64, C.POINTER(BuildOpts), _vp, _u64p,
                                            C.POINTER(_i32)]),
+    "abhsf_autotune": (C.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, C.POINTER(BuildOpts), _i32, _i32, _vp, _fp,
+                                 C.POINTER(_i32), C.POINTER(_vp)]),
     "abhsf_selector_features": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _vp, _fp]),
     "abhsf_selector_predict": (C.c_int, [_vp, _fp, _vp, C.POINTER(_i32)]),
     "abhsf_selector_builtin_model": (C.c_int, [_fp]),

@@ -103,6 +103,13 @@ abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, const double*
                 float f[ABHSF_FEATURES];
                 abhsf::selector_features(rows, cols, nnz, m, n, o.inputs_on_device != 0, st, f);
                 o.block_size = abhsf::mlp_predict(o.selector_model, f, st);
+            } else if (o.selector == ABHSF_SELECT_AUTOTUNE) {
+                float ms[abhsf::kNumBlockSizes];
+                int best = 0;
+                std::unique_ptr<abhsf_matrix> a;
+                abhsf::autotune(rows, cols, vals, nnz, m, n, o, 0, 10, st, ms, &best, &a);
+                *out = a.release();
+                return;
             } else {
                 fail(ABHSF_ERROR_INVALID_VALUE, "selector out of range");
             }
@@ -376,6 +383,29 @@ abhsf_status abhsf_block_size_storage(const int64_t* rows, const int64_t* cols, 
         abhsf::block_size_storage(rows, cols, nnz, m, n, o, reinterpret_cast<cudaStream_t>(stream), bits);
         if (best)
             *best = abhsf::select_block_size(bits);
+    });
+}
+
+abhsf_status abhsf_autotune(const int64_t* rows, const int64_t* cols, const double* vals, int64_t nnz, int64_t m,
+                            int64_t n, const abhsf_build_opts* opts, int32_t candidates, int32_t reps,
+                            abhsf_stream_t stream, float ms[5], int32_t* best, abhsf_matrix** out)
+{
+    return guarded([&] {
+        if (out)
+            *out = nullptr;
+        if (!ms || !best)
+            fail(ABHSF_ERROR_INVALID_VALUE, "ms and best must be non-NULL");
+        abhsf_build_opts o;
+        abhsf_build_opts_default(&o);
+        if (opts)
+            o = *opts;
+        std::unique_ptr<abhsf_matrix> a;
+        int b = 0;
+        abhsf::autotune(rows, cols, vals, nnz, m, n, o, candidates, reps, reinterpret_cast<cudaStream_t>(stream), ms,
+                        &b, out ? &a : nullptr);
+        *best = b;
+        if (out)
+            *out = a.release();
     });
 }
 

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <map>
+#include <memory>
 
 #include "common.cuh"
 
@@ -23,6 +24,13 @@ constexpr int kNumBlockSizes = 5;
 void block_size_storage(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n,
                         const abhsf_build_opts& o, cudaStream_t st, uint64_t bits[kNumBlockSizes]);
 int select_block_size(const uint64_t bits[kNumBlockSizes]);
+
+// Block size by measured SpMV time (autotune.cu): builds each candidate size
+// (bit k of candidates: 16 << k), times reps SpMVs of it, ms[k] = -1 where not
+// timed; keep (may be NULL) receives the fastest size's matrix.
+void autotune(const int64_t* rows, const int64_t* cols, const double* vals, int64_t nnz, int64_t m, int64_t n,
+              const abhsf_build_opts& o, int candidates, int reps, cudaStream_t st, float ms[kNumBlockSizes],
+              int* best, std::unique_ptr<abhsf_matrix>* keep);
 
 // Learned block-size selector (selector.cu): per-matrix features and the MLP.
 void selector_features(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, bool on_device,

@@ -113,6 +113,45 @@ def predict(feats: np.ndarray, model: np.ndarray | None = None, stream=None) -> 
     return int(bs.value)
 
 
+def autotune(rows, cols, vals, m: int, n: int, candidates=SIZES, reps: int = 10, value_type: str = "f64",
+             keep: bool = False, stream=None):
+    """Block size by measured SpMV time (abhsf_autotune): the matrix is built
+    at each candidate size and reps SpMVs of it are timed on the stream.
+    Returns (ms per SpMV at sizes 16..256, -1 where not timed; the fastest
+    size; that size's AbhsfMatrix when keep, else None)."""
+    from .matrix import AbhsfMatrix
+    rows, cols, nnz, rp, cp, on_dev = _coo_args(rows, cols)
+    if vals is not None:
+        if on_dev:
+            import torch
+            vals = vals.to(torch.float64).contiguous()
+            vp = vals.data_ptr()
+        else:
+            vals = np.ascontiguousarray(vals, dtype=np.float64)
+            vp = vals.ctypes.data
+    o = capi.BuildOpts()
+    capi.lib.abhsf_build_opts_default(C.byref(o))
+    o.inputs_on_device = int(on_dev)
+    o.value_type = capi.VALUE_TYPES[value_type]
+    mask = sum(1 << SIZES.index(s) for s in candidates)
+    ms = np.zeros(5, np.float32)
+    best = C.c_int32()
+    h = C.c_void_p()
+    capi.check(capi.lib.abhsf_autotune(rp if nnz else None, cp if nnz else None,
+                                       vp if (vals is not None and nnz) else None, nnz, int(m), int(n), C.byref(o),
+                                       mask, int(reps), _stream_ptr(stream),
+                                       ms.ctypes.data_as(C.POINTER(C.c_float)), C.byref(best),
+                                       C.byref(h) if keep else None))
+    A = None
+    if keep:
+        A = AbhsfMatrix()
+        A._h = h
+        A.m, A.n, A.nnz = int(m), int(n), int(nnz)
+        A.block_size = int(best.value)
+        A.value_type = value_type
+    return ms, int(best.value), A
+
+
 class Mlp:
     """The selector network on the GPU: parameters, Adam moments and the
     library's forward / backward / Adam kernels over torch buffers."""

@@ -260,6 +260,30 @@ def batched_set_device(count: int = 256, n_min: int = 1000, n_max: int = 200000,
         yield rows, cols, vals, n, n, name
 
 
+def rmat_device(scale: int = 22, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+                seed: int = 0, device="cuda"):
+    """R-MAT graph on n = 2^scale vertices generated with torch on `device`
+    (the distribution of rmat(); torch's seeded generator, so other random
+    streams): edge_factor * n edges before duplicates are merged, values
+    N(0,1).  Returns (rows, cols, vals, n) tensors sorted by row then column."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    n = 1 << scale
+    e = edge_factor * n
+    r = torch.zeros(e, device=device, dtype=torch.int64)
+    col = torch.zeros(e, device=device, dtype=torch.int64)
+    for level in range(scale):
+        u = torch.rand(e, device=device, generator=g, dtype=torch.float64)
+        bit = 1 << (scale - 1 - level)
+        r += (u >= a + b).to(torch.int64) * bit
+        col += (((u >= a) & (u < a + b)) | (u >= a + b + c)).to(torch.int64) * bit
+    key = torch.unique(r * n + col)
+    del r, col
+    vals = torch.randn(key.numel(), device=device, generator=g, dtype=torch.float64)
+    return key // n, key % n, vals, n
+
+
 SELECTOR_FAMILIES = ("banded", "block_diagonal", "rmat", "stencil_2d", "stencil_3d")
 
 

@@ -148,21 +148,35 @@ def time_spmm(A, c, st, dev, stream, l2_flush, warmup, ks=(4, 8, 16, 32), steps=
 
 def time_lowprec(c, dev, l2_flush, warmup, steps=10):
     """f32 and bf16 copies of the same matrix: f32 SpMV time, algorithmic GB/s
-    (B_fmt + 4 n + 8 m) and normwise error against the FP64 product of the
-    same (f32) x."""
+    (B_fmt + 4 n + 8 m) and error against the FP64 product of the same (f32)
+    x: normwise, and the largest |y - y64| / (|A| |x|) per element.  The same
+    errors on R-MAT scale 22 (n = 4,194,304, edge factor 16, values N(0,1))."""
     import torch
     from abhsf_b200 import AbhsfMatrix
+    from abhsf_b200 import workloads as W
+
+    def errors(rows, cols, vals, m, n, vt, x32):
+        A64 = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=64)
+        y64 = torch.zeros(m, dtype=torch.float64, device=dev)
+        A64.spmv(x32.double(), y64)
+        A64.release()
+        absA = AbhsfMatrix.from_elements(rows, cols, vals.abs() if torch.is_tensor(vals) else np.abs(vals), m, n,
+                                         block_size=64)
+        scale = torch.zeros(m, dtype=torch.float64, device=dev)
+        absA.spmv(x32.double().abs(), scale)
+        absA.release()
+        A = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=64, value_type=vt)
+        y = torch.zeros(m, dtype=torch.float32, device=dev)
+        A.spmv_f32(x32, y)
+        d = (y.double() - y64).abs()
+        nz = scale > 0
+        return A, y, {"rel_err_vs_fp64": float(torch.linalg.norm(y.double() - y64) / torch.linalg.norm(y64)),
+                      "max_err_over_absAx": float((d[nz] / scale[nz]).max())}
+
     x32 = torch.rand(c.n, dtype=torch.float32, device=dev) * 2 - 1
-    A64 = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64)
-    y64 = torch.zeros(c.m, dtype=torch.float64, device=dev)
-    A64.spmv(x32.double(), y64)
-    A64.release()
     out = {}
     for vt in ("f32", "bf16"):
-        A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64, value_type=vt)
-        y = torch.zeros(c.m, dtype=torch.float32, device=dev)
-        A.spmv_f32(x32, y)
-        err = float(torch.linalg.norm(y.double() - y64) / torch.linalg.norm(y64))
+        A, y, err = errors(c.rows, c.cols, c.vals, c.m, c.n, vt, x32)
         for _ in range(max(warmup, 1)):
             l2_flush()
             A.spmv_f32(x32, y)
@@ -178,8 +192,17 @@ def time_lowprec(c, dev, l2_flush, warmup, steps=10):
             ts.append(e0.elapsed_time(e1))
         t = sum(ts) / len(ts)
         b = int(A.stats()["format_bytes"]) + 4 * c.n + 8 * c.m
-        out[vt] = {"ms": t, "GB/s": b / (t * 1e-3) / 1e9, "bytes": b, "rel_err_vs_fp64": err}
+        out[vt] = dict(err, ms=t, bytes=b, **{"GB/s": b / (t * 1e-3) / 1e9})
         A.release()
+    rows, cols, vals, n = W.rmat_device(22, 16, seed=1, device=dev)
+    x32 = torch.rand(n, dtype=torch.float32, device=dev) * 2 - 1
+    out["rmat22"] = {"workload": f"R-MAT scale 22 edge factor 16 (0.57, 0.19, 0.19), nnz={rows.numel()}, "
+                                 "values N(0,1), x U[-1,1] f32, block size 64"}
+    for vt in ("f32", "bf16"):
+        A, _, err = errors(rows, cols, vals, n, n, vt, x32)
+        A.release()
+        out["rmat22"][vt] = err
+    del rows, cols, vals
     return out
 
 
@@ -192,18 +215,19 @@ def time_batched(dev, l2_flush, warmup, count=256, steps=10):
     from abhsf_b200 import AbhsfBatch, AbhsfMatrix
     from abhsf_b200 import workloads as W
     t0 = time.time()
-    mats, byts, nnz = [], 0, 0
+    sets = {32: [], 64: []}
+    byts = {32: 0, 64: 0}
+    nnz = 0
     for rows, cols, vals, m, n, _ in W.batched_set_device(count, seed=0, device=dev):
-        A = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=64)
-        mats.append(A)
-        byts += int(A.stats()["format_bytes"]) + 8 * n + 16 * m
+        for s in sets:
+            A = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=s)
+            sets[s].append(A)
+            byts[s] += int(A.stats()["format_bytes"]) + 8 * n + 16 * m
         nnz += int(rows.numel())
         del rows, cols, vals
     build_s = time.time() - t0
-    xs = [torch.rand(A.n, dtype=torch.float64, device=dev) for A in mats]
-    ys = [torch.zeros(A.m, dtype=torch.float64, device=dev) for A in mats]
-    batch = AbhsfBatch(mats)
-    px, py = batch.pointer_tables(xs, ys)
+    xs = [torch.rand(A.n, dtype=torch.float64, device=dev) for A in sets[64]]
+    ys = [torch.zeros(A.m, dtype=torch.float64, device=dev) for A in sets[64]]
 
     def timed(fn):
         for _ in range(max(warmup, 1)):
@@ -221,6 +245,19 @@ def time_batched(dev, l2_flush, warmup, count=256, steps=10):
             ts.append(e0.elapsed_time(e1))
         return sum(ts) / len(ts)
 
+    # autotune the batch's block size: the one batched launch timed at each size the batched kernel serves
+    tune = {}
+    for s, ms_ in sets.items():
+        b_ = AbhsfBatch(ms_)
+        px_, py_ = b_.pointer_tables(xs, ys)
+        tune[s] = timed(lambda: b_.spmv_tables(px_, py_))
+        b_.release()
+    s_best = min(tune, key=tune.get)
+    mats = sets[s_best]
+    byts = byts[s_best]
+    batch = AbhsfBatch(mats)
+    px, py = batch.pointer_tables(xs, ys)
+
     def one_by_one():
         for A, x, y in zip(mats, xs, ys):
             A.spmv(x, y)
@@ -237,14 +274,16 @@ def time_batched(dev, l2_flush, warmup, count=256, steps=10):
     if batch.status() != 0:
         raise RuntimeError("batched SpMV reported a device status")
     out = {"workload": f"{count} matrices, n log-uniform [1k, 200k], even banded (bandwidth U[3,64]), odd R-MAT"
-                       f"(0.57, 0.19, 0.19) edge factor 8, values N(0,1), generated on the GPU, block size 64",
+                       f"(0.57, 0.19, 0.19) edge factor 8, values N(0,1), generated on the GPU",
+           "block_size": s_best, "autotune_ms": {str(k): v for k, v in tune.items()},
            "nnz": nnz, "bytes_per_step": byts, "build_s": build_s,
            "batched": {"ms": t_batch, "GB/s": byts / (t_batch * 1e-3) / 1e9, "launches": 1},
            "one_by_one": {"ms": t_loop, "GB/s": byts / (t_loop * 1e-3) / 1e9, "launches": count},
            "speedup": t_loop / t_batch, "matrix0_bitwise": same}
     batch.release()
-    for A in mats:
-        A.release()
+    for ms_ in sets.values():
+        for A in ms_:
+            A.release()
     return out
 
 
@@ -261,8 +300,16 @@ def time_cg(dev, g=256, rtol=1e-10):
     b = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, lap.n)).to(dev)
     out = {"workload": f"3D 7-point Laplacian {g}^3 (n={lap.n}, nnz={lap.nnz}, diag 6, off -1), b U[-1,1] seed 1, "
                        f"x0 = 0, block size 64", "rtol": rtol}
+    from abhsf_b200 import selector as sel
+    t0 = time.perf_counter()
+    _, s64, T64 = sel.autotune(lap.rows, lap.cols, lap.vals, lap.m, lap.n, candidates=(32, 64), keep=True)
+    ms32, s32, T32 = sel.autotune(lap.rows, lap.cols, lap.vals, lap.m, lap.n, candidates=(32, 64), value_type="f32",
+                                  keep=True)
+    out["autotune"] = {"f64_block_size": s64, "f32_block_size": s32, "f32_ms": ms32[1:3].tolist(),
+                       "seconds": time.perf_counter() - t0}
     for name, fn in (("plain", lambda x: cg(A64, b, x, rtol=rtol)),
-                     ("tuned", lambda x: cg_mixed(A64, A32, b, x, rtol=rtol, update_factor=0.1))):
+                     ("tuned", lambda x: cg_mixed(A64, A32, b, x, rtol=rtol, update_factor=0.1)),
+                     ("tuned_autotuned", lambda x: cg_mixed(T64, T32, b, x, rtol=rtol, update_factor=0.1))):
         x = torch.zeros(lap.n, dtype=torch.float64, device=dev)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -271,9 +318,84 @@ def time_cg(dev, g=256, rtol=1e-10):
         out[name] = dict(info, seconds=time.perf_counter() - t0)
     out["plain"]["solver"] = "FP64 CG, reference-order f64 SpMV"
     out["tuned"]["solver"] = "f32 CG on an f32 copy, FP64 solution, FP64 residual replacement each 10x drop"
+    out["tuned_autotuned"]["solver"] = out["tuned"]["solver"] + ", block sizes autotuned over {32, 64}"
     out["tuned_speedup"] = out["plain"]["seconds"] / out["tuned"]["seconds"]
-    A64.release()
-    A32.release()
+    out["tuned_autotuned_speedup"] = out["plain"]["seconds"] / out["tuned_autotuned"]["seconds"]
+    for M in (A64, A32, T64, T32):
+        M.release()
+    return out
+
+
+def time_cusparse(c, dev, l2_flush, warmup, ours_ms, steps=10):
+    """A further reference point on the same GPU: cuSPARSE's CSR SpMV (through
+    torch.mv on a CSR tensor, int32 indices, FP64 values) on the same matrix
+    and x.  Its own CSR bytes are 12 nnz + 4 (m + 1) + 8 n + 8 m (y written,
+    not read: it computes y = A x)."""
+    import torch
+    try:
+        order = np.lexsort((c.cols, c.rows))
+        crow = np.zeros(c.m + 1, np.int64)
+        np.cumsum(np.bincount(c.rows, minlength=c.m), out=crow[1:])
+        A = torch.sparse_csr_tensor(torch.from_numpy(crow.astype(np.int32)).to(dev),
+                                    torch.from_numpy(c.cols[order].astype(np.int32)).to(dev),
+                                    torch.from_numpy(c.vals[order]).to(dev), size=(c.m, c.n))
+        x = torch.rand(c.n, dtype=torch.float64, device=dev) * 2 - 1
+        for _ in range(max(warmup, 1)):
+            l2_flush()
+            y = torch.mv(A, x)
+        ts = []
+        for _ in range(steps):
+            l2_flush()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            y = torch.mv(A, x)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        t = sum(ts) / len(ts)
+        b = 12 * c.nnz + 4 * (c.m + 1) + 8 * c.n + 8 * c.m
+        del A, y
+        return {"ms": t, "GB/s_own_csr_bytes": b / (t * 1e-3) / 1e9, "csr_bytes": b,
+                "gflops": 2.0 * c.nnz / (t * 1e-3) / 1e9, "ours_speedup": t / ours_ms,
+                "call": "torch.mv(sparse_csr_tensor int32 indices, f64 values) -> cuSPARSE SpMV"}
+    except Exception as e:  # a reference point only: report why it is missing
+        return {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+
+
+def time_selector(dev, seeds=range(2000, 2050)):
+    """Block-size selection on held-out matrices of the selector workload
+    (seeds past the 2,000 training seeds; banded, block-diagonal, R-MAT, 2D /
+    3D stencils, n log-uniform [10k, 4M]): the learned MLP's regret against
+    the exhaustive min-bss sweep (block_statistics/consistency.cpp:147-173),
+    next to every fixed block size, and the time of each way to choose."""
+    import torch
+    from abhsf_b200 import selector as sel
+    from abhsf_b200 import workloads as W
+    X, bits, pick = [], [], []
+    t_learned = t_sweep = 0.0
+    for seed in seeds:
+        r, c, m, n, _ = W.selector_matrix(int(seed))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f = sel.features(r, c, m, n)
+        s = sel.predict(f)
+        t1 = time.perf_counter()
+        b, _ = sel.block_size_storage(r, c, m, n)
+        t2 = time.perf_counter()
+        t_learned += t1 - t0
+        t_sweep += t2 - t1
+        X.append(f)
+        bits.append(b)
+        pick.append(sel.SIZES.index(s))
+        del r, c
+    bits = np.array(bits)
+    out = {"workload": f"{len(bits)} held-out selector matrices (seeds {seeds[0]}-{seeds[-1]})",
+           "learned": sel.regret_summary(bits, np.array(pick)),
+           "fixed": {str(s): sel.regret_summary(bits, np.full(len(bits), k)) for k, s in enumerate(sel.SIZES)},
+           "learned_ms_per_matrix": 1e3 * t_learned / len(bits),
+           "sweep_ms_per_matrix": 1e3 * t_sweep / len(bits)}
+    out["choose_speedup"] = t_sweep / t_learned
     return out
 
 
@@ -433,6 +555,8 @@ def run_ours(args):
     lowprec = None if args.no_lowprec else time_lowprec(c, dev, l2_flush, args.warmup)
     cg_times = None if args.no_cg or rank != 0 else time_cg(dev)
     batched = None if args.no_batched or rank != 0 else time_batched(dev, l2_flush, args.warmup)
+    cusparse = None if args.no_cusparse or rank != 0 else time_cusparse(c, dev, l2_flush, args.warmup, t_mean)
+    selector = None if args.no_selector or rank != 0 else time_selector(dev)
 
     peak, peak_src = hbm_peak()
     achieved = B / (t_mean * 1e-3) / 1e9
@@ -466,6 +590,8 @@ def run_ours(args):
             "lowprec": lowprec,
             "cg": cg_times,
             "batched": batched,
+            "cusparse_csr": cusparse,
+            "selector": selector,
             "e2e": {"value": world * B / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
                     "d2h_bytes_per_step": 8 * c.m, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": args.steps,
@@ -489,6 +615,8 @@ def main():
     ap.add_argument("--no-lowprec", action="store_true", help="skip the f32 / bf16 SpMV timings")
     ap.add_argument("--no-cg", action="store_true", help="skip the CG solves on the 3D Laplacian")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-matrix batched launch")
+    ap.add_argument("--no-cusparse", action="store_true", help="skip the cuSPARSE CSR reference point")
+    ap.add_argument("--no-selector", action="store_true", help="skip the block-size selector evaluation")
     ap.add_argument("--sum-order", choices=["reference", "tree"], default="reference",
                     help="reference: bitwise the reference CSR's y; tree: warp reduction trees")
     ap.add_argument("--n", type=int, default=DEFAULT_N,

@@ -104,11 +104,15 @@ typedef enum abhsf_matrix_type {
  * builds the block histograms of all five sizes and takes the one of least
  * ABHSF storage, ties to the smaller (block_statistics/min-bss.cpp:14-58).
  * LEARNED computes ABHSF_FEATURES features in one pass and lets a small MLP
- * predict that size.  Either way only the block size is chosen: every tile's
- * scheme, indices and values follow from it exactly. */
+ * predict that size.  AUTOTUNE builds the matrix at every size and keeps the
+ * one whose SpMV (abhsf_spmv, or abhsf_spmv_f32 for f32 / bf16 values) ran
+ * fastest on the stream (abhsf_autotune, 10 timed calls each).  Whichever
+ * selector, only the block size is chosen: every tile's scheme, indices and
+ * values follow from it exactly. */
 typedef enum abhsf_selector {
     ABHSF_SELECT_MINBSS = 0,
-    ABHSF_SELECT_LEARNED = 1
+    ABHSF_SELECT_LEARNED = 1,
+    ABHSF_SELECT_AUTOTUNE = 2
 } abhsf_selector;
 
 /* The learned selector's MLP: ABHSF_FEATURES inputs, two hidden layers of
@@ -311,6 +315,21 @@ ABHSF_API int32_t abhsf_block_select_scheme(int64_t r, int64_t s, int64_t nnz, i
 ABHSF_API abhsf_status abhsf_block_size_storage(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m,
                                                 int64_t n, const abhsf_build_opts* opts, abhsf_stream_t stream,
                                                 uint64_t bits[5], int32_t* best);
+
+/* Block size by measured time: builds the matrix at each candidate size
+ * (bit k of candidates: size 16 << k; 0 = all five), runs one untimed and
+ * then reps timed SpMVs of it on stream (x = 0, y = 0 device scratch; the
+ * kernels' speed does not depend on the values) and writes the mean time per
+ * SpMV in milliseconds to ms[k] (-1 for sizes not timed, and for f32 / bf16
+ * values at sizes abhsf_spmv_f32 does not serve).  *best = the fastest size;
+ * out (NULL allowed) receives that size's matrix, which the caller releases.
+ * Uses opts as abhsf_build does (block_size ignored).  No counterpart in the
+ * reference, which chooses by storage only (block_statistics/min-bss.cpp:14-58).
+ * Synchronises stream. */
+ABHSF_API abhsf_status abhsf_autotune(const int64_t* rows, const int64_t* cols, const double* vals, int64_t nnz,
+                                      int64_t m, int64_t n, const abhsf_build_opts* opts, int32_t candidates,
+                                      int32_t reps, abhsf_stream_t stream, float ms[5], int32_t* best,
+                                      abhsf_matrix** out);
 
 /* The learned selector's features of a matrix, computed on the GPU
  * (inputs_on_device: rows / cols are device pointers).  out[12] =

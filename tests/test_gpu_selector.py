@@ -177,3 +177,46 @@ def test_learned_selector_beats_a_fixed_block_size(gpu):
     fixed = [sel.regret_summary(bits, np.full(len(X), k)) for k in range(5)]
     assert learned["avg_pct"] < min(f["avg_pct"] for f in fixed), (learned, fixed)
     assert learned["avg_pct"] < 0.5 * fixed[2]["avg_pct"], (learned, fixed[2])
+
+
+def test_autotune_times_every_size_and_keeps_the_fastest(gpu):
+    import torch
+    rows, cols, m, n, name = _small(12)
+    vals = np.random.default_rng(1).standard_normal(rows.size)
+    ms, best, A = sel.autotune(rows, cols, vals, m, n, reps=5, keep=True)
+    assert np.all(ms > 0) and best == sel.SIZES[int(np.argmin(ms))] and A.block_size == best
+    B = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=best)
+    ea, eb = A.export(), B.export()
+    for k in ea:
+        assert np.array_equal(ea[k], eb[k]), k
+    x = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, n)).cuda()
+    ya = torch.zeros(m, dtype=torch.float64, device="cuda")
+    yb = ya.clone()
+    A.spmv(x, ya)
+    B.spmv(x, yb)
+    assert torch.equal(ya, yb)
+    # device inputs, one candidate
+    ms1, best1, _ = sel.autotune(torch.from_numpy(rows).cuda(), torch.from_numpy(cols).cuda(),
+                                 torch.from_numpy(vals).cuda(), m, n, candidates=(128,), reps=2)
+    assert best1 == 128 and ms1[3] > 0 and np.all(np.delete(ms1, 3) == -1)
+    # f32 values: only the sizes abhsf_spmv_f32 serves are timed
+    ms2, best2, _ = sel.autotune(rows, cols, vals, m, n, reps=2, value_type="f32")
+    assert best2 in (32, 64) and ms2[1] > 0 and ms2[2] > 0 and ms2[0] == ms2[3] == ms2[4] == -1
+    C_ = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size="auto", selector="autotune")
+    assert C_.block_size in capi.BLOCK_SIZES
+    for M in (A, B, C_):
+        M.release()
+
+
+def test_autotune_arguments(gpu):
+    rows = np.array([0, 1], np.int64)
+    cols = np.array([0, 1], np.int64)
+    vals = np.array([1.0, 2.0])
+    ms = np.zeros(5, np.float32)
+    b = C.c_int32()
+    for cand, reps in ((32, 1), (-1, 1), (1, 0)):
+        st = capi.lib.abhsf_autotune(rows.ctypes.data, cols.ctypes.data, vals.ctypes.data, 2, 2, 2, None, cand,
+                                     reps, None, ms.ctypes.data_as(C.POINTER(C.c_float)), C.byref(b), None)
+        assert st == capi.INVALID_VALUE
+    with pytest.raises(capi.Unsupported):
+        sel.autotune(rows, cols, vals, 2, 2, candidates=(16, 128), value_type="bf16")
