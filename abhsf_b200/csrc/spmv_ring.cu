@@ -53,9 +53,15 @@ namespace {
 #define ABHSF_RING_CTAS 5
 #endif
 #ifndef ABHSF_RING_Q
-#define ABHSF_RING_Q 24
+#define ABHSF_RING_Q 16
 #endif
 constexpr int kCtasPerSm = ABHSF_RING_CTAS;  // resident CTAs per SM
+// Consumer teams per CTA (a template parameter, 1 or 2): S / 32 warps each,
+// one row per lane.  Teams take block rows in turn, so while one team's
+// dependent loads wait the other sums; matrices of few large tiles run
+// faster with one team, matrices of many small tiles with two (the choice is
+// timed per matrix when it is prepared).
+constexpr int kMaxTeams = 2;
 constexpr int kMaxQ = ABHSF_RING_Q;          // tiles in flight per CTA (queue slots, one mbarrier each)
 static_assert(kMaxQ <= 32, "the producer keeps one queue slot's ring offset per lane");
 constexpr uint32_t kWaitPolls = 1u << 21;      // try_wait polls of at most ~1 us each
@@ -103,16 +109,22 @@ struct val_traits<ABHSF_VALUE_BF16> {
 template <int S, int K, int VT>
 constexpr int ring_overhead()
 {
-    return kMaxQ * (64 + 16) + (S / 32) * 64 * 4 + 64;
+    return kMaxQ * (64 + 16) + kMaxTeams * (S / 32) * 64 * 2 + 64;
 }
 
-// The ring: the shared memory of an SM (228 KiB, 1 KiB of it reserved per
-// CTA) split over kCtasPerSm CTAs, less the rest of the CTA's shared memory
-// and 1 KiB for the granularity of shared-memory allocations.
+template <int S, int TM>
+constexpr int ring_threads()
+{
+    return TM * S + 32;
+}
+
+// The ring: the shared memory of an SM (228 KiB, allocated in 1 KiB granules
+// with 1 KiB reserved per CTA) split over kCtasPerSm CTAs, less the rest of
+// the CTA's shared memory.
 template <int S, int K, int VT>
 constexpr int ring_bytes()
 {
-    return ((233472 / kCtasPerSm - 2048 - ring_overhead<S, K, VT>()) / 16) * 16;
+    return (((233472 / kCtasPerSm / 1024 - 1) * 1024 - ring_overhead<S, K, VT>()) / 16) * 16;
 }
 
 // Small consecutive tiles travel together: a queue slot carries up to
@@ -159,6 +171,8 @@ struct __align__(16) slot_rec {
     int32_t y_off, x_off, pay_off, val_off;  // parts, relative to the slot
     void* y;        // the group's matrix: y and its rows
     int64_t m;
+    int32_t team;   // the consumer team that sums the group
+    int32_t unused;
 };
 static_assert(sizeof(slot_rec) == 64, "slot_rec is 64 bytes");
 
@@ -168,7 +182,7 @@ struct ring_smem {
     slot_rec rec[kMaxQ];              // queue slot g % kMaxQ
     unsigned long long full[kMaxQ];   // the slot's copies have landed
     unsigned long long empty[kMaxQ];  // the consumers are done with the slot
-    int rng[S / 32][64];              // each consumer warp's COO row ranges: first, end
+    uint16_t rng[kMaxTeams * (S / 32)][64];  // each consumer warp's COO row ranges: first, end
     int abort;                        // a wait ran out: everyone stops
 };
 
@@ -192,6 +206,7 @@ struct ring_args {
     const void* const* xs;
     void* const* ys;
     int* status;     // ABHSF_DEVSTAT_* bits
+    int bulk;        // x and y blocks may travel as bulk copies
     int64_t drop;    // test hook: a descriptor whose group's bulk copies are not issued (-1: none)
     uint32_t polls;  // bound of every mbarrier wait
 };
@@ -319,11 +334,19 @@ struct group_geo {
 };
 
 // Producer warp: queues the group's slot at ring offset off as queue slot q;
-// it completes on full[q].
+// it completes on full[q].  The payload and value blocks go first: when the
+// ring holds one large tile at a time, the time from a freed slot to their
+// issue is on the critical path.  (Their bytes may land before the expected
+// count is posted; the count only goes negative meanwhile, and the phase
+// cannot complete before lane 0's arrival, which posts it.)  Where every x
+// block (and y block) of the group lies whole inside x (y), is contiguous
+// (one right-hand side per row of X, or ldx = K) and 16-byte aligned, each
+// travels as one bulk copy issued by its tile's lane; otherwise the warp
+// copies them element by element, filling zeros past n (m).
 template <int S, int K, int VT, bool B>
 __device__ __forceinline__ void issue_group(const ring_args& P, const mat_view& mv, const ring_desc& d, int yk,
-                                            const group_geo& gg, uint32_t off, int q, ring_smem<S, K, VT>& sm,
-                                            bool drop, int lane)
+                                            const group_geo& gg, uint32_t off, int q, int team,
+                                            ring_smem<S, K, VT>& sm, bool drop, int lane)
 {
     using T = typename val_traits<VT>::T;
     using V = typename val_traits<VT>::V;
@@ -331,64 +354,85 @@ __device__ __forceinline__ void issue_group(const ring_args& P, const mat_view& 
     uint8_t* slot = sm.ring + off;
     const uint32_t base = smem_addr(slot);
     unsigned long long* bar = &sm.full[q];
-    if (lane < gg.ntiles)
+    const int nt = gg.ntiles;
+    if (lane == 0 && !drop) {
+        // the slot's bytes were last read through the generic proxy
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (gg.pay_bytes)
+            bulk_g2s(base + gg.pay_off, mv.payload + gg.io0, gg.pay_bytes, bar);
+        bulk_g2s(base + gg.val_off, static_cast<const V*>(mv.values) + gg.vbase, gg.val_bytes, bar);
+    }
+    if (lane < nt)
         reinterpret_cast<ring_desc*>(slot)[lane] = d;
-    __syncwarp();  // lane 0's arrival below publishes every lane's descriptor
     const T* X = static_cast<const T*>(mv.x);
     const T* Y = static_cast<const T*>(mv.y);
-    const int total = gg.ntiles * S * K;
-    if (gg.ntiles == 1) {  // lane 0 holds the tile's descriptor
+    // lane j < nt holds tile j (a single tile: every lane holds it)
+    const int64_t c0 = (int64_t)col_of<B>(d.col) * S, r0 = (int64_t)(d.info & kRowMask) * S;
+    const bool first = (d.info & kFirst) != 0;
+    const bool whole = lane >= nt || (c0 + S <= mv.n && (!first || r0 + S <= mv.m));
+    // (a dropped group -- a test hook -- copies x and y element by element, so
+    // that cp.async.wait_all covers them when the kernel gives up)
+    const bool bulk = P.bulk && !drop && P.ldx == K && P.ldy == K &&
+                      ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) & 15) == 0 &&
+                      __all_sync(kFull, whole);
+    uint32_t xy_bytes = 0;
+    if (bulk) {
+        xy_bytes = (uint32_t)(nt + __popc(__ballot_sync(kFull, lane < nt && first))) * XB;
+        if (lane < nt) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bulk_g2s(base + gg.x_off + lane * XB, X + c0 * K, XB, bar);
+            if (first)
+                bulk_g2s(base + gg.y_off + yk * XB, Y + r0 * K, XB, bar);
+        }
+    } else if (nt == 1) {
         const uint32_t col = col_of<B>(__shfl_sync(kFull, d.col, 0)), info = __shfl_sync(kFull, d.info, 0);
-        const int64_t c0 = (int64_t)col * S, r0 = (int64_t)(info & kRowMask) * S;
+        const int64_t c1 = (int64_t)col * S, r1 = (int64_t)(info & kRowMask) * S;
 #pragma unroll
         for (int k = lane; k < S * K; k += 32) {
             const int c = k / K, h = k % K;
-            const bool okx = c0 + c < mv.n;
-            cp_elem(base + gg.x_off + TB * k, okx ? X + (c0 + c) * P.ldx + h : X, okx ? TB : 0);
+            const bool okx = c1 + c < mv.n;
+            cp_elem(base + gg.x_off + TB * k, okx ? X + (c1 + c) * P.ldx + h : X, okx ? TB : 0);
             if (info & kFirst) {
-                const bool oky = r0 + c < mv.m;
-                cp_elem(base + gg.y_off + TB * k, oky ? Y + (r0 + c) * P.ldy + h : Y, oky ? TB : 0);
+                const bool oky = r1 + c < mv.m;
+                cp_elem(base + gg.y_off + TB * k, oky ? Y + (r1 + c) * P.ldy + h : Y, oky ? TB : 0);
+            }
+        }
+    } else {
+        const int total = nt * S * K;
+        for (int e0 = 0; e0 < total; e0 += 32) {
+            const int e = e0 + lane, jj = (e / (S * K)) & 31, k = e % (S * K);
+            const uint32_t col = col_of<B>(__shfl_sync(kFull, d.col, jj));
+            const uint32_t info = __shfl_sync(kFull, d.info, jj);
+            const int ykk = __shfl_sync(kFull, yk, jj);
+            if (e < total) {
+                const int c = k / K, h = k % K;
+                const int64_t c1 = (int64_t)col * S;
+                const bool okx = c1 + c < mv.n;
+                cp_elem(base + gg.x_off + jj * XB + TB * k, okx ? X + (c1 + c) * P.ldx + h : X, okx ? TB : 0);
+                if (info & kFirst) {
+                    const int64_t r1 = (int64_t)(info & kRowMask) * S;
+                    const bool oky = r1 + c < mv.m;
+                    cp_elem(base + gg.y_off + ykk * XB + TB * k, oky ? Y + (r1 + c) * P.ldy + h : Y, oky ? TB : 0);
+                }
             }
         }
     }
-    for (int e0 = 0; gg.ntiles > 1 && e0 < total; e0 += 32) {
-        const int e = e0 + lane, jj = (e / (S * K)) & 31, k = e % (S * K);
-        const uint32_t col = col_of<B>(__shfl_sync(kFull, d.col, jj));
-        const uint32_t info = __shfl_sync(kFull, d.info, jj);
-        const int ykk = __shfl_sync(kFull, yk, jj);
-        if (e < total) {
-            const int c = k / K, h = k % K;
-            const int64_t c0 = (int64_t)col * S;
-            const bool okx = c0 + c < mv.n;
-            cp_elem(base + gg.x_off + jj * XB + TB * k, okx ? X + (c0 + c) * P.ldx + h : X, okx ? TB : 0);
-            if (info & kFirst) {
-                const int64_t r0 = (int64_t)(info & kRowMask) * S;
-                const bool oky = r0 + c < mv.m;
-                cp_elem(base + gg.y_off + ykk * XB + TB * k, oky ? Y + (r0 + c) * P.ldy + h : Y, oky ? TB : 0);
-            }
-        }
-    }
+    __syncwarp();  // lane 0's arrival below publishes every lane's descriptor
     cp_arrive(bar);
     if (lane == 0) {
         slot_rec& r = sm.rec[q];
         r.io0 = gg.io0;
         r.vbase = gg.vbase;
         r.off = off;
-        r.ntiles = gg.ntiles;
+        r.ntiles = nt;
         r.y_off = gg.y_off;
         r.x_off = gg.x_off;
         r.pay_off = gg.pay_off;
         r.val_off = gg.val_off;
         r.y = mv.y;
         r.m = mv.m;
-        mbar_expect_tx(bar, gg.pay_bytes + gg.val_bytes);  // also publishes rec[q] and the descriptors
-        if (!drop) {
-            // the slot's bytes were last read through the generic proxy
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (gg.pay_bytes)
-                bulk_g2s(base + gg.pay_off, mv.payload + gg.io0, gg.pay_bytes, bar);
-            bulk_g2s(base + gg.val_off, static_cast<const V*>(mv.values) + gg.vbase, gg.val_bytes, bar);
-        }
+        r.team = team;
+        mbar_expect_tx(bar, gg.pay_bytes + gg.val_bytes + xy_bytes);  // also publishes rec[q] and the descriptors
     }
 }
 
@@ -499,7 +543,7 @@ __device__ __forceinline__ void sum_dense(const typename val_traits<VT>::T* xs,
 template <int S, int K, int VT, bool CSR>
 __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs, const uint8_t* pay,
                                            const typename val_traits<VT>::V* vs, int z,
-                                           typename val_traits<VT>::T (&acc)[K], int* rng, int warp, int lane)
+                                           typename val_traits<VT>::T (&acc)[K], uint16_t* rng, int warp, int lane)
 {
     using T = typename val_traits<VT>::T;
     constexpr int LG = S == 32 ? 5 : 6;
@@ -570,8 +614,7 @@ __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs,
 // tile of a block row loads them from its y block, the last writes them to y.
 template <int S, int K, int VT, bool B>
 __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot, const slot_rec& r, int j, int& yk,
-                                         ring_smem<S, K, VT>& sm, typename val_traits<VT>::T (&acc)[K], int warp,
-                                         int lane)
+                                         uint16_t* rng, typename val_traits<VT>::T (&acc)[K], int warp, int lane)
 {
     using T = typename val_traits<VT>::T;
     using V = typename val_traits<VT>::V;
@@ -591,8 +634,8 @@ __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot
     switch (d.pb_sch >> 24) {
     case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K, VT>(xs, pay, vs, acc, warp, lane); break;
     case ABHSF_SCHEME_DENSE: sum_dense<S, K, VT>(xs, vs, acc, warp, lane); break;
-    case ABHSF_SCHEME_CSR: sum_sparse<S, K, VT, true>(xs, pay, vs, (int)d.nv, acc, sm.rng[warp], warp, lane); break;
-    default: sum_sparse<S, K, VT, false>(xs, pay, vs, (int)d.nv, acc, sm.rng[warp], warp, lane); break;
+    case ABHSF_SCHEME_CSR: sum_sparse<S, K, VT, true>(xs, pay, vs, (int)d.nv, acc, rng, warp, lane); break;
+    default: sum_sparse<S, K, VT, false>(xs, pay, vs, (int)d.nv, acc, rng, warp, lane); break;
     }
     if (d.info & kLast) {
         const int64_t rr = (int64_t)(d.info & kRowMask) * S + row;
@@ -606,11 +649,13 @@ __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot
     }
 }
 
-// Warps 0 .. S/32 - 1 sum; warp S/32 produces.
-template <int S, int K, int VT, bool B>
-__global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args P)
+// Warps 0 .. TM * S/32 - 1 sum, S/32 per team; the last warp produces.
+template <int S, int K, int VT, bool B, int TM>
+__global__ void __launch_bounds__(ring_threads<S, TM>(), kCtasPerSm) k_spmv_f64_ring(ring_args P)
 {
-    constexpr int NC = S / 32;  // consumer warps
+    static_assert(TM >= 1 && TM <= kMaxTeams, "teams");
+    constexpr int NC = S / 32;    // consumer warps of a team
+    constexpr int NW = TM * NC;  // consumer warps
     constexpr int kRingBytes = ring_bytes<S, K, VT>();
     extern __shared__ __align__(16) uint8_t smem_raw[];
     ring_smem<S, K, VT>& sm = *reinterpret_cast<ring_smem<S, K, VT>*>(smem_raw);
@@ -622,14 +667,14 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
     if (tid == 0) {
         for (int b = 0; b < kMaxQ; ++b) {
             mbar_init(&sm.full[b], 32 + 1);  // the producer lanes' cp.async arrivals + the expect_tx arrival
-            mbar_init(&sm.empty[b], NC);     // one arrival per consumer warp
+            mbar_init(&sm.empty[b], NW);     // one arrival per consumer warp (owner team or not)
         }
         sm.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     int issued = 0;  // producer: groups queued
-    if (warp == NC) {
+    if (warp == NW) {
         using V = typename val_traits<VT>::V;
         constexpr int XB = S * K * (int)sizeof(typename val_traits<VT>::T), VB = sizeof(V), G = 16 / VB;
         // descriptors of tiles wbase .. wbase + 63, lane j holding tiles wbase + j and wbase + 32 + j
@@ -641,6 +686,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
             nxt = D[32 + lane];
         int done = 0, head = 0, tail = 0;  // done: groups the consumers released; ring in use [tail, head)
         int my_off = 0;                    // lane q: ring offset of the group in queue slot q
+        int team = TM - 1;                 // team of the last group queued
 #pragma unroll 1
         for (int i = 0; i < n;) {
             while (i >= wbase + 32) {
@@ -682,7 +728,12 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                 const int est = have ? 32 + (first ? XB : 0) + XB + (int)(d.pb_sch & 0xffffffu) + (int)d.nv * VB : 0;
                 const int cum = warp_inclusive_sum(est, lane);
                 const unsigned okm = __ballot_sync(kFull, have && contig && (lane == 0 || cum <= kGroupBytes));
-                const int L = __ffs(~okm) - 1;  // leading tiles that form the group (lane 0 always qualifies)
+                int L = __ffs(~okm) - 1;  // leading tiles that form the group (lane 0 always qualifies)
+                // end the group with the last block row it completes, so that
+                // the next group starts a block row (and may go to another team)
+                const unsigned lasts = __ballot_sync(kFull, lane < L && (d.info & kLast) != 0);
+                if (lasts != 0)
+                    L = 32 - __clz(lasts);
                 const unsigned firsts = __ballot_sync(kFull, lane < L && first);
                 yk = __popc(firsts & ((1u << lane) - 1u));
                 gg.ntiles = L;
@@ -733,7 +784,11 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
             }
             const bool drop = P.drop >= eb + i && P.drop < eb + i + L;
             const mat_view mv = view_of<B>(P, mid_of<B>(__shfl_sync(kFull, d.col, 0)));
-            issue_group<S, K, VT, B>(P, mv, d, yk, gg, (uint32_t)off, issued % kMaxQ, sm, drop, lane);
+            // a group that starts a block row goes to the next team; one that
+            // continues a block row stays with the team holding its sums
+            if (__shfl_sync(kFull, d.info, 0) & kFirst)
+                team = team + 1 == TM ? 0 : team + 1;
+            issue_group<S, K, VT, B>(P, mv, d, yk, gg, (uint32_t)off, issued % kMaxQ, team, sm, drop, lane);
             if (lane == issued % kMaxQ)
                 my_off = off;
             if (issued == done)
@@ -743,6 +798,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
             i += L;
         }
     } else {
+        const int team = warp / NC, wl = warp % NC;  // wl: the warp's rows 32 wl .. 32 wl + 31 of a block row
         typename val_traits<VT>::T acc[K];  // the lane's row of the current block row
 #pragma unroll
         for (int h = 0; h < K; ++h)
@@ -757,12 +813,14 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
                 break;
             }
             const slot_rec& r = sm.rec[q];
-            const uint8_t* slot = sm.ring + r.off;
             const int L = r.ntiles;
-            int yk = 0;
+            if (r.team == team) {
+                const uint8_t* slot = sm.ring + r.off;
+                int yk = 0;
 #pragma unroll 1
-            for (int j = 0; j < L; ++j)
-                sum_tile<S, K, VT, B>(P, slot, r, j, yk, sm, acc, warp, lane);
+                for (int j = 0; j < L; ++j)
+                    sum_tile<S, K, VT, B>(P, slot, r, j, yk, sm.rng[warp], acc, wl, lane);
+            }
             __syncwarp();
             if (lane == 0)
                 mbar_arrive(&sm.empty[q]);
@@ -774,7 +832,7 @@ __global__ void __launch_bounds__(S + 32, kCtasPerSm) k_spmv_f64_ring(ring_args 
         // leave no copy in flight into this CTA's shared memory
         if (tid == 0)
             atomicOr(P.status, ABHSF_DEVSTAT_WAIT_TIMEOUT);
-        if (warp == NC) {
+        if (warp == NW) {
             for (int i = max(0, issued - kMaxQ); i < issued; ++i)
                 mbar_wait(&sm.full[i % kMaxQ], (uint32_t)(i / kMaxQ) & 1u, P.polls);
             cp_wait_all();
@@ -834,25 +892,36 @@ __global__ void k_ring_max_pv(int64_t T, tiles_view A, int vsize, unsigned int* 
 
 // One pass: K right-hand sides, X and Y starting at their first column.
 template <int S, int K, int VT>
-void launch_ring(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int64_t ldy, cudaStream_t st)
+void launch_ring(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int64_t ldy, cudaStream_t st,
+                 bool tuning = false)
 {
     static_assert(((sizeof(ring_smem<S, K, VT>) + 1023) / 1024 + 1) * 1024 * kCtasPerSm <= 233472,
                   "kCtasPerSm CTAs fit an SM even with shared memory allocated in 1 KiB granules");
     ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()),
                 a.ring_wbeg.get(), x, y, ldx, ldy, nullptr, nullptr, nullptr,
-                a.dev_status.get(), g_drop_desc, g_spin_limit ? g_spin_limit : kWaitPolls};
-    k_spmv_f64_ring<S, K, VT, false><<<(unsigned)a.ring_warps, S + 32, sizeof(ring_smem<S, K, VT>), st>>>(P);
+                a.dev_status.get(), a.ring_bulk, tuning ? -1 : g_drop_desc,
+                (g_spin_limit && !tuning) ? g_spin_limit : kWaitPolls};
+    if constexpr (K == 1) {
+        if (a.ring_teams == 2) {
+            k_spmv_f64_ring<S, K, VT, false, 2>
+                <<<(unsigned)a.ring_warps, ring_threads<S, 2>(), sizeof(ring_smem<S, K, VT>), st>>>(P);
+            ABHSF_CUDA(cudaGetLastError());
+            return;
+        }
+    }
+    k_spmv_f64_ring<S, K, VT, false, 1>
+        <<<(unsigned)a.ring_warps, ring_threads<S, 1>(), sizeof(ring_smem<S, K, VT>), st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }
 
-template <int S, int K, int VT, bool B = false>
+template <int S, int K, int VT, bool B = false, int TM = 1>
 int ring_ctas_per_sm()
 {
     int nb = 0;
-    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S, K, VT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S, K, VT, B, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sizeof(ring_smem<S, K, VT>)));
-    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S, K, VT, B>, S + 32,
-                                                             sizeof(ring_smem<S, K, VT>)));
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S, K, VT, B, TM>,
+                                                             ring_threads<S, TM>(), sizeof(ring_smem<S, K, VT>)));
     return std::max(nb, 1);
 }
 
@@ -886,13 +955,93 @@ void spmm_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, doubl
     }
 }
 
+// Resident CTAs per SM of the single-right-hand-side kernels (both team
+// counts; the grid is sized for the smaller), setting their shared memory.
+template <int S, int VT, bool B = false>
+int ring_per_sm_of()
+{
+    return std::min(ring_ctas_per_sm<S, 1, VT, B, 1>(), ring_ctas_per_sm<S, 1, VT, B, 2>());
+}
+
 int ring_per_sm(int s, int vt)
 {
     if (vt == ABHSF_VALUE_F64)
-        return s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_F64>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_F64>();
+        return s == 32 ? ring_per_sm_of<32, ABHSF_VALUE_F64>() : ring_per_sm_of<64, ABHSF_VALUE_F64>();
     if (vt == ABHSF_VALUE_F32)
-        return s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_F32>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_F32>();
-    return s == 32 ? ring_ctas_per_sm<32, 1, ABHSF_VALUE_BF16>() : ring_ctas_per_sm<64, 1, ABHSF_VALUE_BF16>();
+        return s == 32 ? ring_per_sm_of<32, ABHSF_VALUE_F32>() : ring_per_sm_of<64, ABHSF_VALUE_F32>();
+    return s == 32 ? ring_per_sm_of<32, ABHSF_VALUE_BF16>() : ring_per_sm_of<64, ABHSF_VALUE_BF16>();
+}
+
+struct event_pair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    event_pair()
+    {
+        ABHSF_CUDA(cudaEventCreate(&a));
+        if (cudaEventCreate(&b) != cudaSuccess) {
+            cudaEventDestroy(a);
+            fail(ABHSF_ERROR_CUDA, "cudaEventCreate failed");
+        }
+    }
+    ~event_pair()
+    {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    event_pair(const event_pair&) = delete;
+    event_pair& operator=(const event_pair&) = delete;
+};
+
+// The variant (teams 1 or 2, bulk x / y copies or not) whose launches of
+// run(teams, bulk) take least time on st: one untimed and two timed each.
+template <typename F>
+void time_variants(F&& run, cudaStream_t st, int& teams, int& bulk)
+{
+    constexpr int kReps = 5;
+    event_pair ev[kReps];
+    float best = 3.4e38f;
+    for (int tm = 1; tm <= kMaxTeams; ++tm)
+        for (int bk = 0; bk <= 1; ++bk) {
+            run(tm, bk);
+            for (int r = 0; r < kReps; ++r) {
+                ABHSF_CUDA(cudaEventRecord(ev[r].a, st));
+                run(tm, bk);
+                ABHSF_CUDA(cudaEventRecord(ev[r].b, st));
+            }
+            float t[kReps];
+            for (int r = 0; r < kReps; ++r) {
+                ABHSF_CUDA(cudaEventSynchronize(ev[r].b));
+                ABHSF_CUDA(cudaEventElapsedTime(&t[r], ev[r].a, ev[r].b));
+            }
+            std::sort(t, t + kReps);
+            if (t[kReps / 2] < best) {
+                best = t[kReps / 2];
+                teams = tm;
+                bulk = bk;
+            }
+        }
+}
+
+// Times the single-right-hand-side variants on zero x and y and keeps the
+// fastest for the matrix (each gives the same y bit for bit).
+template <int S, int VT>
+void tune_ring(abhsf_matrix& a, cudaStream_t st)
+{
+    using T = typename val_traits<VT>::T;
+    dbuf<T> x(a.n), y(a.m);
+    ABHSF_CUDA(cudaMemsetAsync(x.get(), 0, a.n * sizeof(T), st));
+    ABHSF_CUDA(cudaMemsetAsync(y.get(), 0, a.m * sizeof(T), st));
+    int teams = 1, bulk = 0;
+    time_variants(
+        [&](int tm, int bk) {
+            a.ring_teams = tm;
+            a.ring_bulk = bk;
+            launch_ring<S, 1, VT>(a, x.get(), 1, y.get(), 1, st, true);
+        },
+        st, teams, bulk);
+    a.ring_teams = teams;
+    a.ring_bulk = bulk;
+    ABHSF_CUDA(cudaMemsetAsync(a.dev_status.get(), 0, sizeof(int), st));
+    ABHSF_CUDA(cudaStreamSynchronize(st));
 }
 
 // Deals the non-empty block rows of one or several matrices (same block size
@@ -1017,6 +1166,33 @@ void ring_set_up_all()
     ring_ctas_per_sm<S, 8, ABHSF_VALUE_F64>();
 }
 
+void batch_launch(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st, bool tuning)
+{
+    ring_args P{};
+    P.desc = reinterpret_cast<const ring_desc*>(b.desc.get());
+    P.wbeg = b.wbeg.get();
+    P.ldx = P.ldy = 1;
+    P.mats = reinterpret_cast<const ring_mat*>(b.table.get());
+    P.xs = reinterpret_cast<const void* const*>(xs);
+    P.ys = reinterpret_cast<void* const*>(ys);
+    P.status = b.dev_status.get();
+    P.bulk = b.bulk;
+    P.drop = -1;
+    P.polls = (g_spin_limit && !tuning) ? g_spin_limit : kWaitPolls;
+    constexpr int M32 = sizeof(ring_smem<32, 1, ABHSF_VALUE_F64>), M64 = sizeof(ring_smem<64, 1, ABHSF_VALUE_F64>);
+    const unsigned g = (unsigned)b.ctas;
+    if (b.s == 32 && b.teams == 2)
+        k_spmv_f64_ring<32, 1, ABHSF_VALUE_F64, true, 2><<<g, ring_threads<32, 2>(), M32, st>>>(P);
+    else if (b.s == 32)
+        k_spmv_f64_ring<32, 1, ABHSF_VALUE_F64, true, 1><<<g, ring_threads<32, 1>(), M32, st>>>(P);
+    else if (b.teams == 2)
+        k_spmv_f64_ring<64, 1, ABHSF_VALUE_F64, true, 2><<<g, ring_threads<64, 2>(), M64, st>>>(P);
+    else
+        k_spmv_f64_ring<64, 1, ABHSF_VALUE_F64, true, 1><<<g, ring_threads<64, 1>(), M64, st>>>(P);
+    ABHSF_CUDA(cudaGetLastError());
+}
+
+
 }  // namespace
 
 void prepare_ring(abhsf_matrix& a, cudaStream_t st)
@@ -1035,14 +1211,20 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
         return;  // the streaming kernel serves this matrix
     a.ring_max_pv = mpv;
     a.ring_warps = ctas;
+    if (a.value_type == ABHSF_VALUE_F64)
+        a.s == 32 ? tune_ring<32, ABHSF_VALUE_F64>(a, st) : tune_ring<64, ABHSF_VALUE_F64>(a, st);
+    else if (a.value_type == ABHSF_VALUE_F32)
+        a.s == 32 ? tune_ring<32, ABHSF_VALUE_F32>(a, st) : tune_ring<64, ABHSF_VALUE_F32>(a, st);
+    else
+        a.s == 32 ? tune_ring<32, ABHSF_VALUE_BF16>(a, st) : tune_ring<64, ABHSF_VALUE_BF16>(a, st);
 }
 
 void prepare_batch(abhsf_batch& b, cudaStream_t st)
 {
     if (b.s == 32)
-        ring_ctas_per_sm<32, 1, ABHSF_VALUE_F64, true>();
+        ring_per_sm_of<32, ABHSF_VALUE_F64, true>();
     else
-        ring_ctas_per_sm<64, 1, ABHSF_VALUE_F64, true>();
+        ring_per_sm_of<64, ABHSF_VALUE_F64, true>();
     std::vector<ring_mat> table;
     for (const abhsf_matrix* a : b.mats)
         table.push_back(ring_mat{a->payload.get(), a->values.get(), a->m, a->n});
@@ -1055,6 +1237,34 @@ void prepare_batch(abhsf_batch& b, cudaStream_t st)
     b.ctas = 0;
     if (!build_ring_schedule(b.mats, kBatchColBits, b.desc, b.wbeg, b.ctas, mpv, st) && b.total_tiles > 0)
         fail(ABHSF_ERROR_UNSUPPORTED, "batch too large for the ring kernel's per-CTA counters");
+    if (b.ctas > 0) {
+        // time the variants with every matrix reading one zero x and writing one scratch y
+        int64_t mx = 1, my = 1;
+        for (const abhsf_matrix* a : b.mats) {
+            mx = std::max(mx, a->n);
+            my = std::max(my, a->m);
+        }
+        dbuf<double> x(mx), y(my);
+        ABHSF_CUDA(cudaMemsetAsync(x.get(), 0, mx * sizeof(double), st));
+        ABHSF_CUDA(cudaMemsetAsync(y.get(), 0, my * sizeof(double), st));
+        std::vector<const double*> xs(b.mats.size(), x.get());
+        std::vector<double*> ys(b.mats.size(), y.get());
+        dbuf<const double*> xs_d(xs.size());
+        dbuf<double*> ys_d(ys.size());
+        ABHSF_CUDA(cudaMemcpyAsync(xs_d.get(), xs.data(), xs.size() * sizeof(double*), cudaMemcpyHostToDevice, st));
+        ABHSF_CUDA(cudaMemcpyAsync(ys_d.get(), ys.data(), ys.size() * sizeof(double*), cudaMemcpyHostToDevice, st));
+        int teams = 1, bulk = 0;
+        time_variants(
+            [&](int tm, int bk) {
+                b.teams = tm;
+                b.bulk = bk;
+                batch_launch(b, xs_d.get(), ys_d.get(), st, true);
+            },
+            st, teams, bulk);
+        b.teams = teams;
+        b.bulk = bulk;
+        ABHSF_CUDA(cudaMemsetAsync(b.dev_status.get(), 0, sizeof(int), st));
+    }
     ABHSF_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -1062,24 +1272,10 @@ void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys
 {
     if (b.ctas == 0)
         return;
-    ring_args P{};
-    P.desc = reinterpret_cast<const ring_desc*>(b.desc.get());
-    P.wbeg = b.wbeg.get();
-    P.ldx = P.ldy = 1;
-    P.mats = reinterpret_cast<const ring_mat*>(b.table.get());
-    P.xs = reinterpret_cast<const void* const*>(xs);
-    P.ys = reinterpret_cast<void* const*>(ys);
-    P.status = b.dev_status.get();
-    P.drop = -1;
-    P.polls = g_spin_limit ? g_spin_limit : kWaitPolls;
-    if (b.s == 32)
-        k_spmv_f64_ring<32, 1, ABHSF_VALUE_F64, true>
-            <<<(unsigned)b.ctas, 32 + 32, sizeof(ring_smem<32, 1, ABHSF_VALUE_F64>), st>>>(P);
-    else
-        k_spmv_f64_ring<64, 1, ABHSF_VALUE_F64, true>
-            <<<(unsigned)b.ctas, 64 + 32, sizeof(ring_smem<64, 1, ABHSF_VALUE_F64>), st>>>(P);
-    ABHSF_CUDA(cudaGetLastError());
+    batch_launch(b, xs, ys, st, false);
 }
+
+
 
 bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
@@ -1125,6 +1321,22 @@ bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, d
 }
 
 }  // namespace abhsf
+
+extern "C" abhsf_status abhsf_test_ring_variant(abhsf_matrix* a, int32_t set, int32_t* teams, int32_t* bulk)
+{
+    return abhsf::guarded([&] {
+        if (!a || !teams || !bulk)
+            abhsf::fail(ABHSF_ERROR_INVALID_VALUE, "NULL argument");
+        if (set) {
+            if (*teams < 1 || *teams > abhsf::kMaxTeams || (*bulk != 0 && *bulk != 1))
+                abhsf::fail(ABHSF_ERROR_INVALID_VALUE, "teams 1 or 2, bulk 0 or 1");
+            a->ring_teams = *teams;
+            a->ring_bulk = *bulk;
+        }
+        *teams = a->ring_warps ? a->ring_teams : 0;
+        *bulk = a->ring_bulk;
+    });
+}
 
 extern "C" void abhsf_test_set_hooks(int64_t drop_desc, uint32_t spin_limit)
 {

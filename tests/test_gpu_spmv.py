@@ -209,3 +209,29 @@ def test_tiled_mixture_medium_every_row(gpu):
     x = np.random.default_rng(3).uniform(-1, 1, c.n)
     y0 = np.random.default_rng(4).standard_normal(c.m)
     np.testing.assert_array_equal(run_spmv(A, x, y0), reference_order_y(c, x, y0))
+
+
+@pytest.mark.parametrize("s", [32, 64])
+def test_every_ring_variant_gives_the_reference_y(gpu, s):
+    """The ring kernel's launch variants (one or two consumer teams; x / y
+    blocks as bulk copies or element copies) that the build times and chooses
+    among give the reference CSR's y bit for bit, on matrices of few large
+    tiles, of many small tiles (a 3D stencil) and with ragged edges."""
+    import ctypes as C
+    cases = [W.random_blocky(2100, 1900, s, 60, seed=3), W.laplacian_3d(20), W.rmat(3000, 8, seed=4),
+             W.tiled_mixture(n=65536 + 37, p=1e-3, seed=2)]
+    for coo in cases:
+        x = W.rhs(coo.n, 21)
+        y0 = W.rhs(coo.m, 22)
+        want = reference_order_y(coo, x, y0)
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s)
+        t, b = C.c_int32(), C.c_int32()
+        assert capi.lib.abhsf_test_ring_variant(A.handle, 0, C.byref(t), C.byref(b)) == capi.SUCCESS
+        assert t.value in (1, 2) and b.value in (0, 1)
+        for teams in (1, 2):
+            for bulk in (0, 1):
+                t.value, b.value = teams, bulk
+                assert capi.lib.abhsf_test_ring_variant(A.handle, 1, C.byref(t), C.byref(b)) == capi.SUCCESS
+                np.testing.assert_array_equal(run_spmv(A, x, y0), want, err_msg=f"{coo.name} {teams} {bulk}")
+        assert A.device_status() == 0
+        A.release()
