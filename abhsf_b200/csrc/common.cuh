@@ -172,7 +172,7 @@ struct abhsf_matrix {
     abhsf::dbuf<int64_t> ring_wbeg;
     int ring_max_pv = 0;  // largest payload + values bytes of one tile (picks the SpMM pass width)
     int ring_warps = 0;  // CTAs of the ring kernel; 0: the streaming kernel serves this matrix
-    int ring_teams = 1;  // consumer teams per CTA of its single-right-hand-side launches (timed at build)
+    int ring_layout = 0;  // consumer layout of its single-right-hand-side launches (timed at build)
     int ring_bulk = 0;   // x / y blocks as bulk copies (timed at build)
     abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
     // staging for abhsf_spmv_host
@@ -203,6 +203,6 @@ struct abhsf_batch {
     abhsf::dbuf<uint8_t> table;  // per matrix: arrays and shape
     abhsf::dbuf<int> dev_status;
     int ctas = 0;
-    int teams = 1;  // consumer teams per CTA (timed at creation)
+    int layout = 0;  // consumer layout of the ring kernel (timed at creation)
     int bulk = 0;   // x / y blocks as bulk copies (timed at creation)
 };

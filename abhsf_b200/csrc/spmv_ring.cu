@@ -56,12 +56,22 @@ namespace {
 #define ABHSF_RING_Q 16
 #endif
 constexpr int kCtasPerSm = ABHSF_RING_CTAS;  // resident CTAs per SM
-// Consumer teams per CTA (a template parameter, 1 or 2): S / 32 warps each,
-// one row per lane.  Teams take block rows in turn, so while one team's
-// dependent loads wait the other sums; matrices of few large tiles run
-// faster with one team, matrices of many small tiles with two (the choice is
-// timed per matrix when it is prepared).
-constexpr int kMaxTeams = 2;
+// Consumer layouts (a template parameter L): TM teams of NC warps.  Teams
+// take block rows in turn, so while one team's dependent loads wait another
+// sums; a team of one warp sums S / 32 rows per lane.  Matrices of few large
+// tiles run faster with one team of S / 32 warps, matrices of many small tiles
+// with several teams (the layout is timed per matrix when it is prepared).
+//   L = 0: 1 team of S/32 warps   L = 1: 2 teams of S/32 warps
+//   L = 2: 4 teams of 1 warp      L = 3: 2 teams of 1 warp
+constexpr int kLayouts = 4;
+constexpr int kMaxConsumerWarps = 4;
+template <int S, int L>
+struct layout {
+    static constexpr int TM = L == 0 ? 1 : L == 2 ? 4 : 2;
+    static constexpr int NC = L <= 1 ? S / 32 : 1;
+    static constexpr int RPL = S / (32 * NC);
+    static_assert(TM * NC <= kMaxConsumerWarps, "consumer warps");
+};
 constexpr int kMaxQ = ABHSF_RING_Q;          // tiles in flight per CTA (queue slots, one mbarrier each)
 static_assert(kMaxQ <= 32, "the producer keeps one queue slot's ring offset per lane");
 constexpr uint32_t kWaitPolls = 1u << 21;      // try_wait polls of at most ~1 us each
@@ -109,13 +119,13 @@ struct val_traits<ABHSF_VALUE_BF16> {
 template <int S, int K, int VT>
 constexpr int ring_overhead()
 {
-    return kMaxQ * (64 + 16) + kMaxTeams * (S / 32) * 64 * 2 + 64;
+    return kMaxQ * (64 + 16) + kMaxConsumerWarps * 2 * S * 2 + 64;
 }
 
-template <int S, int TM>
+template <int S, int L>
 constexpr int ring_threads()
 {
-    return TM * S + 32;
+    return 32 * layout<S, L>::TM * layout<S, L>::NC + 32;
 }
 
 // The ring: the shared memory of an SM (228 KiB, allocated in 1 KiB granules
@@ -182,7 +192,7 @@ struct ring_smem {
     slot_rec rec[kMaxQ];              // queue slot g % kMaxQ
     unsigned long long full[kMaxQ];   // the slot's copies have landed
     unsigned long long empty[kMaxQ];  // the consumers are done with the slot
-    uint16_t rng[kMaxTeams * (S / 32)][64];  // each consumer warp's COO row ranges: first, end
+    uint16_t rng[kMaxConsumerWarps][2 * S];  // each consumer warp's COO row marks: starts, ends
     int abort;                        // a wait ran out: everyone stops
 };
 
@@ -458,42 +468,61 @@ __device__ __forceinline__ int warp_inclusive_sum(int v, int lane)
     return v;
 }
 
-__device__ __forceinline__ int warp_sum(int v)
+// The rows a consumer lane sums: a team of NC warps covers the S rows of a
+// block row, warp wl of the team rows 32 (wl + NC i) + lane for i < RPL
+// (RPL = S / (32 NC) rows per lane).  With several rows per lane the lane's
+// independent add chains interleave, and a tile's per-tile work (descriptor,
+// COO row marks, bitmap offsets) is done once per tile instead of per warp.
+template <int S, int NC>
+__device__ __forceinline__ int row_of(int wl, int i, int lane)
 {
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1)
-        v += __shfl_xor_sync(kFull, v, d);
-    return v;
+    return 32 * (wl + NC * i) + lane;
 }
 
-// Bitmap tile, row `row` = 32 warp + lane.  Row r's bits are u32 words
-// r * W .. r * W + W - 1 (W = S / 32), bit b of word j = column 32 j + b.
-template <int S, int K, int VT>
+// Bitmap tile.  Row r's bits are u32 words r * W .. r * W + W - 1 (W = S / 32),
+// bit b of word j = column 32 j + b; a row's values start after the set bits
+// of all earlier rows.
+template <int S, int K, int VT, int NC>
 __device__ __forceinline__ void sum_bitmap(const typename val_traits<VT>::T* xs, const uint8_t* pay,
                                            const typename val_traits<VT>::V* vs,
-                                           typename val_traits<VT>::T (&acc)[K], int warp, int lane)
+                                           typename val_traits<VT>::T (&acc)[S / (32 * NC)][K], int wl, int lane)
 {
     using T = typename val_traits<VT>::T;
-    constexpr int W = S / 32;
-    const int row = 32 * warp + lane;
-    uint32_t w[W];
-    int cnt = 0, before = 0;
-    if (W == 2) {
-        const uint2* bm = reinterpret_cast<const uint2*>(pay);
-        const uint2 ww = bm[row];
-        w[0] = ww.x;
-        w[W - 1] = ww.y;
-        if (warp == 1) {  // values of rows 0..31 come first
-            const uint2 u = bm[lane];
-            before = warp_sum(__popc(u.x) + __popc(u.y));
-        }
-    } else {
-        w[0] = reinterpret_cast<const uint32_t*>(pay)[row];
-    }
+    constexpr int W = S / 32, RPL = S / (32 * NC), NB = S / 32;  // NB blocks of 32 rows
+    uint32_t w[RPL][W];
+    int q[RPL];
+    int base = 0;  // set bits of the 32-row blocks before block b
+    const int last = wl + NC * (RPL - 1);  // the lane's last block
 #pragma unroll
-    for (int j = 0; j < W; ++j)
-        cnt += __popc(w[j]);
-    int q = before + warp_inclusive_sum(cnt, lane) - cnt;
+    for (int b = 0; b < NB; ++b) {
+        if (b > last)
+            break;
+        uint32_t wb[W];
+        if (W == 2) {
+            const uint2 u = reinterpret_cast<const uint2*>(pay)[32 * b + lane];
+            wb[0] = u.x;
+            wb[W - 1] = u.y;
+        } else {
+            wb[0] = reinterpret_cast<const uint32_t*>(pay)[32 * b + lane];
+        }
+        int cnt = 0;
+#pragma unroll
+        for (int j = 0; j < W; ++j)
+            cnt += __popc(wb[j]);
+        const int inc = warp_inclusive_sum(cnt, lane);
+        if ((b - wl) % NC == 0 && b >= wl) {  // one of the lane's rows
+            const int i = (b - wl) / NC;
+#pragma unroll
+            for (int ii = 0; ii < RPL; ++ii)
+                if (ii == i) {
+#pragma unroll
+                    for (int j = 0; j < W; ++j)
+                        w[ii][j] = wb[j];
+                    q[ii] = base + inc - cnt;
+                }
+        }
+        base += __shfl_sync(kFull, inc, 31);
+    }
 #pragma unroll
     for (int j = 0; j < W; ++j) {
 #pragma unroll
@@ -502,12 +531,15 @@ __device__ __forceinline__ void sum_bitmap(const typename val_traits<VT>::T* xs,
 #pragma unroll
             for (int h = 0; h < K; ++h)
                 xv[h] = xs[(32 * j + b) * K + h];
-            if ((w[j] >> b) & 1u) {
-                const T v = widen(vs[q]);
 #pragma unroll
-                for (int h = 0; h < K; ++h)
-                    acc[h] = fadd(acc[h], fmul(v, xv[h]));
-                ++q;
+            for (int i = 0; i < RPL; ++i) {
+                if ((w[i][j] >> b) & 1u) {
+                    const T v = widen(vs[q[i]]);
+#pragma unroll
+                    for (int h = 0; h < K; ++h)
+                        acc[i][h] = fadd(acc[i][h], fmul(v, xv[h]));
+                    ++q[i];
+                }
             }
         }
     }
@@ -515,44 +547,47 @@ __device__ __forceinline__ void sum_bitmap(const typename val_traits<VT>::T* xs,
 
 // Dense tile: all S * S values, row-major.  Lane l runs l columns behind
 // lane 0 so that the lanes' values fall in different banks.
-template <int S, int K, int VT>
+template <int S, int K, int VT, int NC>
 __device__ __forceinline__ void sum_dense(const typename val_traits<VT>::T* xs,
                                           const typename val_traits<VT>::V* vs,
-                                          typename val_traits<VT>::T (&acc)[K], int warp, int lane)
+                                          typename val_traits<VT>::T (&acc)[S / (32 * NC)][K], int wl, int lane)
 {
     using T = typename val_traits<VT>::T;
-    const int row = 32 * warp + lane;
+    constexpr int RPL = S / (32 * NC);
 #pragma unroll 4
     for (int k = 0; k < S + 31; ++k) {
         const int c = k - lane;
         if (c >= 0 && c < S) {
-            const T v = widen(vs[row * S + c]);
-            if (v != T(0)) {  // stored zeros and the zero padding past n
 #pragma unroll
-                for (int h = 0; h < K; ++h)
-                    acc[h] = fadd(acc[h], fmul(v, xs[c * K + h]));
+            for (int i = 0; i < RPL; ++i) {
+                const T v = widen(vs[row_of<S, NC>(wl, i, lane) * S + c]);
+                if (v != T(0)) {  // stored zeros and the zero padding past n
+#pragma unroll
+                    for (int h = 0; h < K; ++h)
+                        acc[i][h] = fadd(acc[i][h], fmul(v, xs[c * K + h]));
+                }
             }
         }
     }
 }
 
-// COO / CSR tile, row `row` = 32 warp + lane: the lane adds its row's
-// elements in stored order (columns ascending).  A CSR tile gives each row's
-// range in its row_end array; for a COO tile the warp first marks where each
-// of its rows starts and ends in the sorted keys.
-template <int S, int K, int VT, bool CSR>
+// COO / CSR tile: the lane adds each of its rows' elements in stored order
+// (columns ascending), the rows' chains interleaved.  A CSR tile gives each
+// row's range in its row_end array; for a COO tile the warp first marks where
+// each of its rows starts and ends in the sorted keys (rng: 2 S marks).
+template <int S, int K, int VT, int NC, bool CSR>
 __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs, const uint8_t* pay,
                                            const typename val_traits<VT>::V* vs, int z,
-                                           typename val_traits<VT>::T (&acc)[K], uint16_t* rng, int warp, int lane)
+                                           typename val_traits<VT>::T (&acc)[S / (32 * NC)][K], uint16_t* rng,
+                                           int wl, int lane)
 {
     using T = typename val_traits<VT>::T;
-    constexpr int LG = S == 32 ? 5 : 6;
+    constexpr int LG = S == 32 ? 5 : 6, RPL = S / (32 * NC);
     const uint16_t* key16 = reinterpret_cast<const uint16_t*>(pay);  // COO keys / CSR row ends
     const uint8_t* col8 = pay + 2 * S;                                // CSR local columns
-    const int row = 32 * warp + lane;
     if (!CSR && z <= 32) {
         // few elements: element lane k forms its product, and each row lane
-        // takes the products of its row from the element lanes in key order
+        // takes the products of its rows from the element lanes in key order
         int rk = -1, ck = 0;
         T vk = T(0);
         if (lane < z) {
@@ -570,92 +605,121 @@ __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs,
 #pragma unroll
             for (int h = 0; h < K; ++h) {
                 const T p = __shfl_sync(kFull, pk[h], k);
-                if (r == row)
-                    acc[h] = fadd(acc[h], p);
+#pragma unroll
+                for (int i = 0; i < RPL; ++i)
+                    if (r == row_of<S, NC>(wl, i, lane))
+                        acc[i][h] = fadd(acc[i][h], p);
             }
         }
         return;
     }
-    int lo, hi;
+    int lo[RPL], len[RPL];
     if (CSR) {
-        lo = row > 0 ? key16[row - 1] : 0;
-        hi = key16[row];
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+            const int row = row_of<S, NC>(wl, i, lane);
+            lo[i] = row > 0 ? key16[row - 1] : 0;
+            len[i] = key16[row] - lo[i];
+        }
     } else {
         // every element whose row is one of this warp's marks where the row
         // starts and ends (keys sorted by row, so a row's elements are a run)
-        rng[lane] = 0;
-        rng[32 + lane] = 0;
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+            const int row = row_of<S, NC>(wl, i, lane);
+            rng[row] = 0;
+            rng[S + row] = 0;
+        }
         __syncwarp();
         for (int k = lane; k < z; k += 32) {
             const int rk = key16[k] >> LG;
-            const int r = rk - 32 * warp;
-            if (r >= 0 && r < 32) {
+            if (NC == 1 || (rk >> 5) % NC == wl) {
                 if (k == 0 || (key16[k - 1] >> LG) != rk)
-                    rng[r] = k;
+                    rng[rk] = (uint16_t)k;
                 if (k + 1 == z || (key16[k + 1] >> LG) != rk)
-                    rng[32 + r] = k + 1;
+                    rng[S + rk] = (uint16_t)(k + 1);
             }
         }
         __syncwarp();
-        lo = rng[lane];
-        hi = rng[32 + lane];
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+            const int row = row_of<S, NC>(wl, i, lane);
+            lo[i] = rng[row];
+            len[i] = rng[S + row] - lo[i];
+        }
         __syncwarp();  // read before the next tile rewrites rng
     }
-    for (int k = lo; k < hi; ++k) {
-        const int c = CSR ? (int)col8[k] : (int)(key16[k] & (S - 1));
-        const T v = widen(vs[k]);
+    int most = len[0];
 #pragma unroll
-        for (int h = 0; h < K; ++h)
-            acc[h] = fadd(acc[h], fmul(v, xs[c * K + h]));
+    for (int i = 1; i < RPL; ++i)
+        most = max(most, len[i]);
+    for (int t = 0; t < most; ++t) {
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+            if (t < len[i]) {
+                const int k = lo[i] + t;
+                const int c = CSR ? (int)col8[k] : (int)(key16[k] & (S - 1));
+                const T v = widen(vs[k]);
+#pragma unroll
+                for (int h = 0; h < K; ++h)
+                    acc[i][h] = fadd(acc[i][h], fmul(v, xs[c * K + h]));
+            }
+        }
     }
 }
 
 // Adds tile j of a queued group onto the lane's row accumulators; the first
 // tile of a block row loads them from its y block, the last writes them to y.
-template <int S, int K, int VT, bool B>
+template <int S, int K, int VT, bool B, int NC>
 __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot, const slot_rec& r, int j, int& yk,
-                                         uint16_t* rng, typename val_traits<VT>::T (&acc)[K], int warp, int lane)
+                                         uint16_t* rng, typename val_traits<VT>::T (&acc)[S / (32 * NC)][K], int wl,
+                                         int lane)
 {
     using T = typename val_traits<VT>::T;
     using V = typename val_traits<VT>::V;
-    constexpr int XB = S * K * (int)sizeof(T);
+    constexpr int XB = S * K * (int)sizeof(T), RPL = S / (32 * NC);
     const ring_desc d = reinterpret_cast<const ring_desc*>(slot)[j];
-    const int row = 32 * warp + lane;
     if (d.info & kFirst) {
         const T* ys = reinterpret_cast<const T*>(slot + r.y_off + yk * XB);
 #pragma unroll
-        for (int h = 0; h < K; ++h)
-            acc[h] = ys[row * K + h];
+        for (int i = 0; i < RPL; ++i)
+#pragma unroll
+            for (int h = 0; h < K; ++h)
+                acc[i][h] = ys[row_of<S, NC>(wl, i, lane) * K + h];
         ++yk;
     }
     const T* xs = reinterpret_cast<const T*>(slot + r.x_off + j * XB);
     const uint8_t* pay = slot + r.pay_off + (d.io - r.io0);
     const V* vs = reinterpret_cast<const V*>(slot + r.val_off) + (d.vo - r.vbase);
     switch (d.pb_sch >> 24) {
-    case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K, VT>(xs, pay, vs, acc, warp, lane); break;
-    case ABHSF_SCHEME_DENSE: sum_dense<S, K, VT>(xs, vs, acc, warp, lane); break;
-    case ABHSF_SCHEME_CSR: sum_sparse<S, K, VT, true>(xs, pay, vs, (int)d.nv, acc, rng, warp, lane); break;
-    default: sum_sparse<S, K, VT, false>(xs, pay, vs, (int)d.nv, acc, rng, warp, lane); break;
+    case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K, VT, NC>(xs, pay, vs, acc, wl, lane); break;
+    case ABHSF_SCHEME_DENSE: sum_dense<S, K, VT, NC>(xs, vs, acc, wl, lane); break;
+    case ABHSF_SCHEME_CSR: sum_sparse<S, K, VT, NC, true>(xs, pay, vs, (int)d.nv, acc, rng, wl, lane); break;
+    default: sum_sparse<S, K, VT, NC, false>(xs, pay, vs, (int)d.nv, acc, rng, wl, lane); break;
     }
     if (d.info & kLast) {
-        const int64_t rr = (int64_t)(d.info & kRowMask) * S + row;
         const int64_t m = B ? r.m : P.A.m;
         T* y = static_cast<T*>(B ? r.y : P.y);
-        if (rr < m) {
 #pragma unroll
-            for (int h = 0; h < K; ++h)
-                y[rr * P.ldy + h] = acc[h];
+        for (int i = 0; i < RPL; ++i) {
+            const int64_t rr = (int64_t)(d.info & kRowMask) * S + row_of<S, NC>(wl, i, lane);
+            if (rr < m) {
+#pragma unroll
+                for (int h = 0; h < K; ++h)
+                    y[rr * P.ldy + h] = acc[i][h];
+            }
         }
     }
 }
 
-// Warps 0 .. TM * S/32 - 1 sum, S/32 per team; the last warp produces.
-template <int S, int K, int VT, bool B, int TM>
-__global__ void __launch_bounds__(ring_threads<S, TM>(), kCtasPerSm) k_spmv_f64_ring(ring_args P)
+// Warps 0 .. TM NC - 1 sum, NC per team; the last warp produces.
+template <int S, int K, int VT, bool B, int LY>
+__global__ void __launch_bounds__(ring_threads<S, LY>(), kCtasPerSm) k_spmv_f64_ring(ring_args P)
 {
-    static_assert(TM >= 1 && TM <= kMaxTeams, "teams");
-    constexpr int NC = S / 32;    // consumer warps of a team
-    constexpr int NW = TM * NC;  // consumer warps
+    constexpr int TM = layout<S, LY>::TM;    // consumer teams
+    constexpr int NC = layout<S, LY>::NC;    // warps of a team
+    constexpr int RPL = layout<S, LY>::RPL;  // rows per lane
+    constexpr int NW = TM * NC;             // consumer warps
     constexpr int kRingBytes = ring_bytes<S, K, VT>();
     extern __shared__ __align__(16) uint8_t smem_raw[];
     ring_smem<S, K, VT>& sm = *reinterpret_cast<ring_smem<S, K, VT>*>(smem_raw);
@@ -798,11 +862,13 @@ __global__ void __launch_bounds__(ring_threads<S, TM>(), kCtasPerSm) k_spmv_f64_
             i += L;
         }
     } else {
-        const int team = warp / NC, wl = warp % NC;  // wl: the warp's rows 32 wl .. 32 wl + 31 of a block row
-        typename val_traits<VT>::T acc[K];  // the lane's row of the current block row
+        const int team = warp / NC, wl = warp % NC;  // wl: the warp within its team
+        typename val_traits<VT>::T acc[RPL][K];      // the lane's rows of the current block row
 #pragma unroll
-        for (int h = 0; h < K; ++h)
-            acc[h] = 0;
+        for (int i = 0; i < RPL; ++i)
+#pragma unroll
+            for (int h = 0; h < K; ++h)
+                acc[i][h] = 0;
 #pragma unroll 1
         for (int g = 0, t = 0; t < n; ++g) {
             const int q = g % kMaxQ;
@@ -819,7 +885,7 @@ __global__ void __launch_bounds__(ring_threads<S, TM>(), kCtasPerSm) k_spmv_f64_
                 int yk = 0;
 #pragma unroll 1
                 for (int j = 0; j < L; ++j)
-                    sum_tile<S, K, VT, B>(P, slot, r, j, yk, sm.rng[warp], acc, wl, lane);
+                    sum_tile<S, K, VT, B, NC>(P, slot, r, j, yk, sm.rng[warp], acc, wl, lane);
             }
             __syncwarp();
             if (lane == 0)
@@ -890,6 +956,30 @@ __global__ void k_ring_max_pv(int64_t T, tiles_view A, int vsize, unsigned int* 
     atomicMax(out, best);
 }
 
+// The kernel in consumer layout L (single right-hand side; passes of K > 1
+// right-hand sides use layout 0).
+template <int S, int K, int VT, bool B, int L>
+void launch_layout(unsigned grid, const ring_args& P, cudaStream_t st)
+{
+    k_spmv_f64_ring<S, K, VT, B, L><<<grid, ring_threads<S, L>(), sizeof(ring_smem<S, K, VT>), st>>>(P);
+}
+
+template <int S, int K, int VT, bool B>
+void launch_any(int layout, unsigned grid, const ring_args& P, cudaStream_t st)
+{
+    if constexpr (K == 1) {
+        switch (layout) {
+        case 1: launch_layout<S, K, VT, B, 1>(grid, P, st); break;
+        case 2: launch_layout<S, K, VT, B, 2>(grid, P, st); break;
+        case 3: launch_layout<S, K, VT, B, 3>(grid, P, st); break;
+        default: launch_layout<S, K, VT, B, 0>(grid, P, st); break;
+        }
+    } else {
+        launch_layout<S, K, VT, B, 0>(grid, P, st);
+    }
+    ABHSF_CUDA(cudaGetLastError());
+}
+
 // One pass: K right-hand sides, X and Y starting at their first column.
 template <int S, int K, int VT>
 void launch_ring(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int64_t ldy, cudaStream_t st,
@@ -901,27 +991,17 @@ void launch_ring(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int
                 a.ring_wbeg.get(), x, y, ldx, ldy, nullptr, nullptr, nullptr,
                 a.dev_status.get(), a.ring_bulk, tuning ? -1 : g_drop_desc,
                 (g_spin_limit && !tuning) ? g_spin_limit : kWaitPolls};
-    if constexpr (K == 1) {
-        if (a.ring_teams == 2) {
-            k_spmv_f64_ring<S, K, VT, false, 2>
-                <<<(unsigned)a.ring_warps, ring_threads<S, 2>(), sizeof(ring_smem<S, K, VT>), st>>>(P);
-            ABHSF_CUDA(cudaGetLastError());
-            return;
-        }
-    }
-    k_spmv_f64_ring<S, K, VT, false, 1>
-        <<<(unsigned)a.ring_warps, ring_threads<S, 1>(), sizeof(ring_smem<S, K, VT>), st>>>(P);
-    ABHSF_CUDA(cudaGetLastError());
+    launch_any<S, K, VT, false>(a.ring_layout, (unsigned)a.ring_warps, P, st);
 }
 
-template <int S, int K, int VT, bool B = false, int TM = 1>
+template <int S, int K, int VT, bool B = false, int L = 0>
 int ring_ctas_per_sm()
 {
     int nb = 0;
-    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S, K, VT, B, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ABHSF_CUDA(cudaFuncSetAttribute(k_spmv_f64_ring<S, K, VT, B, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sizeof(ring_smem<S, K, VT>)));
-    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S, K, VT, B, TM>,
-                                                             ring_threads<S, TM>(), sizeof(ring_smem<S, K, VT>)));
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmv_f64_ring<S, K, VT, B, L>,
+                                                             ring_threads<S, L>(), sizeof(ring_smem<S, K, VT>)));
     return std::max(nb, 1);
 }
 
@@ -955,12 +1035,13 @@ void spmm_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, doubl
     }
 }
 
-// Resident CTAs per SM of the single-right-hand-side kernels (both team
-// counts; the grid is sized for the smaller), setting their shared memory.
+// Resident CTAs per SM of the single-right-hand-side kernels (every layout;
+// the grid is sized for the smallest), setting their shared memory.
 template <int S, int VT, bool B = false>
 int ring_per_sm_of()
 {
-    return std::min(ring_ctas_per_sm<S, 1, VT, B, 1>(), ring_ctas_per_sm<S, 1, VT, B, 2>());
+    return std::min(std::min(ring_ctas_per_sm<S, 1, VT, B, 0>(), ring_ctas_per_sm<S, 1, VT, B, 1>()),
+                    std::min(ring_ctas_per_sm<S, 1, VT, B, 2>(), ring_ctas_per_sm<S, 1, VT, B, 3>()));
 }
 
 int ring_per_sm(int s, int vt)
@@ -991,16 +1072,19 @@ struct event_pair {
     event_pair& operator=(const event_pair&) = delete;
 };
 
-// The variant (teams 1 or 2, bulk x / y copies or not) whose launches of
-// run(teams, bulk) take least time on st: one untimed and two timed each.
+// The variant (consumer layout, bulk x / y copies or not) whose launches of
+// run(layout, bulk) take least time on st: one untimed and five timed each,
+// the median compared.  At s = 32 layout 3 is layout 1 and is skipped.
 template <typename F>
-void time_variants(F&& run, cudaStream_t st, int& teams, int& bulk)
+void time_variants(F&& run, int s, cudaStream_t st, int& layout, int& bulk)
 {
     constexpr int kReps = 5;
     event_pair ev[kReps];
     float best = 3.4e38f;
-    for (int tm = 1; tm <= kMaxTeams; ++tm)
+    for (int tm = 0; tm < kLayouts; ++tm)
         for (int bk = 0; bk <= 1; ++bk) {
+            if (s == 32 && tm == 3)
+                continue;
             run(tm, bk);
             for (int r = 0; r < kReps; ++r) {
                 ABHSF_CUDA(cudaEventRecord(ev[r].a, st));
@@ -1015,7 +1099,7 @@ void time_variants(F&& run, cudaStream_t st, int& teams, int& bulk)
             std::sort(t, t + kReps);
             if (t[kReps / 2] < best) {
                 best = t[kReps / 2];
-                teams = tm;
+                layout = tm;
                 bulk = bk;
             }
         }
@@ -1030,15 +1114,15 @@ void tune_ring(abhsf_matrix& a, cudaStream_t st)
     dbuf<T> x(a.n), y(a.m);
     ABHSF_CUDA(cudaMemsetAsync(x.get(), 0, a.n * sizeof(T), st));
     ABHSF_CUDA(cudaMemsetAsync(y.get(), 0, a.m * sizeof(T), st));
-    int teams = 1, bulk = 0;
+    int layout = 0, bulk = 0;
     time_variants(
         [&](int tm, int bk) {
-            a.ring_teams = tm;
+            a.ring_layout = tm;
             a.ring_bulk = bk;
             launch_ring<S, 1, VT>(a, x.get(), 1, y.get(), 1, st, true);
         },
-        st, teams, bulk);
-    a.ring_teams = teams;
+        S, st, layout, bulk);
+    a.ring_layout = layout;
     a.ring_bulk = bulk;
     ABHSF_CUDA(cudaMemsetAsync(a.dev_status.get(), 0, sizeof(int), st));
     ABHSF_CUDA(cudaStreamSynchronize(st));
@@ -1179,17 +1263,10 @@ void batch_launch(const abhsf_batch& b, const double* const* xs, double* const* 
     P.bulk = b.bulk;
     P.drop = -1;
     P.polls = (g_spin_limit && !tuning) ? g_spin_limit : kWaitPolls;
-    constexpr int M32 = sizeof(ring_smem<32, 1, ABHSF_VALUE_F64>), M64 = sizeof(ring_smem<64, 1, ABHSF_VALUE_F64>);
-    const unsigned g = (unsigned)b.ctas;
-    if (b.s == 32 && b.teams == 2)
-        k_spmv_f64_ring<32, 1, ABHSF_VALUE_F64, true, 2><<<g, ring_threads<32, 2>(), M32, st>>>(P);
-    else if (b.s == 32)
-        k_spmv_f64_ring<32, 1, ABHSF_VALUE_F64, true, 1><<<g, ring_threads<32, 1>(), M32, st>>>(P);
-    else if (b.teams == 2)
-        k_spmv_f64_ring<64, 1, ABHSF_VALUE_F64, true, 2><<<g, ring_threads<64, 2>(), M64, st>>>(P);
+    if (b.s == 32)
+        launch_any<32, 1, ABHSF_VALUE_F64, true>(b.layout, (unsigned)b.ctas, P, st);
     else
-        k_spmv_f64_ring<64, 1, ABHSF_VALUE_F64, true, 1><<<g, ring_threads<64, 1>(), M64, st>>>(P);
-    ABHSF_CUDA(cudaGetLastError());
+        launch_any<64, 1, ABHSF_VALUE_F64, true>(b.layout, (unsigned)b.ctas, P, st);
 }
 
 
@@ -1253,15 +1330,15 @@ void prepare_batch(abhsf_batch& b, cudaStream_t st)
         dbuf<double*> ys_d(ys.size());
         ABHSF_CUDA(cudaMemcpyAsync(xs_d.get(), xs.data(), xs.size() * sizeof(double*), cudaMemcpyHostToDevice, st));
         ABHSF_CUDA(cudaMemcpyAsync(ys_d.get(), ys.data(), ys.size() * sizeof(double*), cudaMemcpyHostToDevice, st));
-        int teams = 1, bulk = 0;
+        int layout = 0, bulk = 0;
         time_variants(
             [&](int tm, int bk) {
-                b.teams = tm;
+                b.layout = tm;
                 b.bulk = bk;
                 batch_launch(b, xs_d.get(), ys_d.get(), st, true);
             },
-            st, teams, bulk);
-        b.teams = teams;
+            b.s, st, layout, bulk);
+        b.layout = layout;
         b.bulk = bulk;
         ABHSF_CUDA(cudaMemsetAsync(b.dev_status.get(), 0, sizeof(int), st));
     }
@@ -1322,18 +1399,18 @@ bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, d
 
 }  // namespace abhsf
 
-extern "C" abhsf_status abhsf_test_ring_variant(abhsf_matrix* a, int32_t set, int32_t* teams, int32_t* bulk)
+extern "C" abhsf_status abhsf_test_ring_variant(abhsf_matrix* a, int32_t set, int32_t* layout, int32_t* bulk)
 {
     return abhsf::guarded([&] {
-        if (!a || !teams || !bulk)
+        if (!a || !layout || !bulk)
             abhsf::fail(ABHSF_ERROR_INVALID_VALUE, "NULL argument");
         if (set) {
-            if (*teams < 1 || *teams > abhsf::kMaxTeams || (*bulk != 0 && *bulk != 1))
-                abhsf::fail(ABHSF_ERROR_INVALID_VALUE, "teams 1 or 2, bulk 0 or 1");
-            a->ring_teams = *teams;
+            if (*layout < 0 || *layout >= abhsf::kLayouts || (*bulk != 0 && *bulk != 1))
+                abhsf::fail(ABHSF_ERROR_INVALID_VALUE, "layout 0 .. 3, bulk 0 or 1");
+            a->ring_layout = *layout;
             a->ring_bulk = *bulk;
         }
-        *teams = a->ring_warps ? a->ring_teams : 0;
+        *layout = a->ring_warps ? a->ring_layout : -1;
         *bulk = a->ring_bulk;
     });
 }

@@ -23,12 +23,14 @@ extern "C" {
 ABHSF_API void abhsf_test_set_hooks(int64_t drop_desc, uint32_t spin_limit);
 
 /* The launch variant the build chose for a matrix's single-right-hand-side
- * ring kernel (consumer teams per CTA: 1 or 2; x / y blocks as bulk copies:
- * 0 or 1), and a way to force one, so that a test can check that every
- * variant gives the same y and a benchmark can time each.  teams = 0 on a
- * matrix the ring kernel does not serve.  Not thread-safe with SpMVs of the
- * same matrix. */
-ABHSF_API abhsf_status abhsf_test_ring_variant(abhsf_matrix* a, int32_t set, int32_t* teams, int32_t* bulk);
+ * ring kernel, and a way to force one, so that a test can check that every
+ * variant gives the same y and a benchmark can time each.  layout: the
+ * consumers' arrangement, 0 = one team of s/32 warps (a row per lane),
+ * 1 = two such teams, 2 = four teams of one warp (s/32 rows per lane),
+ * 3 = two teams of one warp; bulk: x / y blocks as bulk copies (1) or element
+ * copies (0).  layout = -1 on a matrix the ring kernel does not serve.  Not
+ * thread-safe with SpMVs of the same matrix. */
+ABHSF_API abhsf_status abhsf_test_ring_variant(abhsf_matrix* a, int32_t set, int32_t* layout, int32_t* bulk);
 
 #ifdef __cplusplus
 }

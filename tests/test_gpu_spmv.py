@@ -213,7 +213,8 @@ def test_tiled_mixture_medium_every_row(gpu):
 
 @pytest.mark.parametrize("s", [32, 64])
 def test_every_ring_variant_gives_the_reference_y(gpu, s):
-    """The ring kernel's launch variants (one or two consumer teams; x / y
+    """The ring kernel's launch variants (consumer layouts: one or two teams
+    of s/32 warps, four or two teams of one warp with s/32 rows per lane; x / y
     blocks as bulk copies or element copies) that the build times and chooses
     among give the reference CSR's y bit for bit, on matrices of few large
     tiles, of many small tiles (a 3D stencil) and with ragged edges."""
@@ -227,11 +228,11 @@ def test_every_ring_variant_gives_the_reference_y(gpu, s):
         A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s)
         t, b = C.c_int32(), C.c_int32()
         assert capi.lib.abhsf_test_ring_variant(A.handle, 0, C.byref(t), C.byref(b)) == capi.SUCCESS
-        assert t.value in (1, 2) and b.value in (0, 1)
-        for teams in (1, 2):
+        assert t.value in (0, 1, 2, 3) and b.value in (0, 1)
+        for layout in (0, 1, 2, 3):
             for bulk in (0, 1):
-                t.value, b.value = teams, bulk
+                t.value, b.value = layout, bulk
                 assert capi.lib.abhsf_test_ring_variant(A.handle, 1, C.byref(t), C.byref(b)) == capi.SUCCESS
-                np.testing.assert_array_equal(run_spmv(A, x, y0), want, err_msg=f"{coo.name} {teams} {bulk}")
+                np.testing.assert_array_equal(run_spmv(A, x, y0), want, err_msg=f"{coo.name} {layout} {bulk}")
         assert A.device_status() == 0
         A.release()
