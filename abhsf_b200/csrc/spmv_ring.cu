@@ -573,8 +573,11 @@ __device__ __forceinline__ void sum_dense(const typename val_traits<VT>::T* xs,
 
 // COO / CSR tile: the lane adds each of its rows' elements in stored order
 // (columns ascending), the rows' chains interleaved.  A CSR tile gives each
-// row's range in its row_end array; for a COO tile the warp first marks where
-// each of its rows starts and ends in the sorted keys (rng: 2 S marks).
+// row's range in its row_end array.  A COO tile whose rows hold one element
+// each (stencil and band diagonals, sparse graph tiles) finds a row's element
+// by a popcount over the warp's bit set of occupied rows; other COO tiles
+// hand few products to the row lanes by shuffles, or mark where each row
+// starts and ends in the sorted keys (rng: 2 S marks).
 template <int S, int K, int VT, int NC, bool CSR>
 __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs, const uint8_t* pay,
                                            const typename val_traits<VT>::V* vs, int z,
@@ -585,6 +588,39 @@ __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs,
     constexpr int LG = S == 32 ? 5 : 6, RPL = S / (32 * NC);
     const uint16_t* key16 = reinterpret_cast<const uint16_t*>(pay);  // COO keys / CSR row ends
     const uint8_t* col8 = pay + 2 * S;                                // CSR local columns
+    if (!CSR && z <= S) {
+        // the rows holding elements as a bit set; when no row holds two, a
+        // row's element index is the number of such rows above it
+        uint32_t mlo = 0, mhi = 0;
+        for (int k = lane; k < z; k += 32) {
+            const int rk = key16[k] >> LG;
+            if (rk < 32)
+                mlo |= 1u << rk;
+            else
+                mhi |= 1u << (rk - 32);
+        }
+        mlo = __reduce_or_sync(kFull, mlo);
+        if (S == 64)
+            mhi = __reduce_or_sync(kFull, mhi);
+        if (__popc(mlo) + __popc(mhi) == z) {
+#pragma unroll
+            for (int i = 0; i < RPL; ++i) {
+                const int row = row_of<S, NC>(wl, i, lane);
+                const bool lower = row < 32;
+                const uint32_t bits = lower ? mlo : mhi;
+                const int rb = lower ? row : row - 32;
+                if ((bits >> rb) & 1u) {
+                    const int k = (lower ? 0 : __popc(mlo)) + __popc(bits & ((1u << rb) - 1u));
+                    const int c = (int)(key16[k] & (S - 1));
+                    const T v = widen(vs[k]);
+#pragma unroll
+                    for (int h = 0; h < K; ++h)
+                        acc[i][h] = fadd(acc[i][h], fmul(v, xs[c * K + h]));
+                }
+            }
+            return;
+        }
+    }
     if (!CSR && z <= 32) {
         // few elements: element lane k forms its product, and each row lane
         // takes the products of its rows from the element lanes in key order
