@@ -105,11 +105,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def workload(n: int = 4_194_304):
+def workload(args):
+    """The timed matrix: the tiled mixture (default), or for profiling the 3D
+    7-point Laplacian on a grid^3 mesh."""
     from abhsf_b200 import workloads as W
     t0 = time.time()
-    c = W.tiled_mixture(n=n)
-    log(f"workload: tiled mixture n={c.n} nnz={c.nnz} ({time.time() - t0:.1f} s to generate)")
+    if args.matrix == "laplacian3d":
+        c = W.laplacian_3d(args.grid)
+        c.name = f"laplacian3d g={args.grid} (7-point, diag 6, off -1)"
+    else:
+        c = W.tiled_mixture(n=args.n)
+        c.name = f"tiled_mixture n={c.n} tile=64 p=1.2266e-5 seed=1 (values N(0,1))"
+    log(f"workload: {c.name} nnz={c.nnz} ({time.time() - t0:.1f} s to generate)")
     return c
 
 
@@ -451,7 +458,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    c = workload(args.n)
+    c = workload(args)
     st = build_format_stats(c)
     B = algorithmic_bytes(st, c.m, c.n)
     cpu = cpu_reference_run(c, B, max_seconds=30.0, max_iters=max(args.steps, 10))
@@ -459,7 +466,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"tiled_mixture n={c.n} tile=64 p=1.2266e-5 seed=1 (values N(0,1))",
+        "config": {"workload": c.name,
                    "nnz": c.nnz, "bytes_per_step": B, "gflops": cpu["gflops"]},
         "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -473,16 +480,15 @@ def run_ours(args):
 
     from abhsf_b200 import AbhsfMatrix
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from abhsf_b200.replicas import aggregate_rate, max_over_ranks, rank_info
+    rank, local, world = rank_info()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
 
-    c = workload(args.n)
+    c = workload(args)
     t0 = time.time()
     A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64, sum_order=args.sum_order)
     torch.cuda.synchronize()
@@ -529,10 +535,7 @@ def run_ours(args):
     clk = clocks.stop()
     times_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     t_mean = sum(times_ms) / len(times_ms)
-    t_red = torch.tensor([t_mean], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_red, op=dist.ReduceOp.MAX)
-    t_max = float(t_red.item())
+    t_max = max_over_ranks(t_mean, dev)
 
     # e2e: host buffers (pinned), copies inside every step
     x_pin = torch.from_numpy(x_h).pin_memory().numpy()
@@ -546,10 +549,7 @@ def run_ours(args):
     for _ in range(e2e_steps):
         A.spmv(x_pin, y_pin)
     e2e_s = (time.perf_counter() - t0) / max(1, e2e_steps)
-    e_red = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e_red, op=dist.ReduceOp.MAX)
-    e2e_s = float(e_red.item())
+    e2e_s = max_over_ranks(e2e_s, dev)
 
     spmm = None if args.no_spmm else time_spmm(A, c, st, dev, stream, l2_flush, args.warmup)
     lowprec = None if args.no_lowprec else time_lowprec(c, dev, l2_flush, args.warmup)
@@ -569,11 +569,11 @@ def run_ours(args):
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:
         line = {
-            "metric": METRIC, "value": world * B / (t_max * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
+            "metric": METRIC, "value": aggregate_rate(B, t_max * 1e-3, world), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {
-                "workload": f"tiled_mixture n={c.n} tile=64 p=1.2266e-5 seed=1 (values N(0,1), x U[-1,1])",
+                "workload": c.name + ", x U[-1,1]",
                 "block_size": 64, "nnz": c.nnz, "tiles": st["tiles"], "tiles_per_scheme": st["tiles_per_scheme"],
                 "bytes_per_step": B, "format_bytes": st["format_bytes"],
                 "msmf_min_bytes_per_step": st["msmf_bits"][6] // 8 + 8 * c.n + 16 * c.m,
@@ -582,7 +582,8 @@ def run_ours(args):
                 "parallelism": f"replicas x{world}", "sum_order": args.sum_order,
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": ncu_traffic_per_launch(args.sum_order, c.n),
+                         "frac": achieved / peak,
+                         "traffic": ncu_traffic_per_launch(args.sum_order, c.n) if args.matrix == "tiled_mixture" else None,
                          "peak_source": peak_src,
                          "kernel": KERNELS[args.sum_order] + "<64>"},
             "cpu_baseline": cpu,
@@ -592,7 +593,7 @@ def run_ours(args):
             "batched": batched,
             "cusparse_csr": cusparse,
             "selector": selector,
-            "e2e": {"value": world * B / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
+            "e2e": {"value": aggregate_rate(B, e2e_s, world), "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
                     "d2h_bytes_per_step": 8 * c.m, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": args.steps,
             "clocks": clk,
@@ -621,6 +622,9 @@ def main():
                     help="reference: bitwise the reference CSR's y; tree: warp reduction trees")
     ap.add_argument("--n", type=int, default=DEFAULT_N,
                     help="matrix order of the tiled mixture (smaller only for profiling captures)")
+    ap.add_argument("--matrix", choices=["tiled_mixture", "laplacian3d"], default="tiled_mixture",
+                    help="the timed matrix (laplacian3d only for profiling the stencil case)")
+    ap.add_argument("--grid", type=int, default=128, help="grid side of --matrix laplacian3d")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
