@@ -80,6 +80,8 @@ constexpr uint32_t kWaitPolls = 1u << 21;      // try_wait polls of at most ~1 u
 #endif
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kFirst = 1u << 30, kLast = 1u << 31, kRowMask = kFirst - 1;
+// a COO tile of more than 32 elements whose rows hold one element each
+constexpr uint32_t kDistinctRows = 1u << 26;
 
 // test hooks (abhsf_test_set_hooks)
 int64_t g_drop_desc = -1;
@@ -91,7 +93,7 @@ struct __align__(16) ring_desc {
     int64_t io;       // payload byte offset (16-byte aligned)
     uint32_t col;     // block column
     uint32_t nv;      // stored values
-    uint32_t pb_sch;  // payload bytes | scheme << 24
+    uint32_t pb_sch;  // payload bytes | scheme << 24 | kDistinctRows
     uint32_t info;    // block row | kFirst (first tile of its block row) | kLast
 };
 static_assert(sizeof(ring_desc) == 32, "ring_desc is 32 bytes");
@@ -571,13 +573,51 @@ __device__ __forceinline__ void sum_dense(const typename val_traits<VT>::T* xs,
     }
 }
 
+// A COO tile of more than 32 elements whose rows hold one element each
+// (flagged when the descriptors are built; stencil and band diagonals): the
+// warp forms the bit set of occupied rows, and a row's element index is the
+// number of occupied rows above it.
+template <int S, int K, int VT, int NC>
+__device__ __forceinline__ void sum_distinct(const typename val_traits<VT>::T* xs, const uint8_t* pay,
+                                             const typename val_traits<VT>::V* vs, int z,
+                                             typename val_traits<VT>::T (&acc)[S / (32 * NC)][K], int wl, int lane)
+{
+    using T = typename val_traits<VT>::T;
+    constexpr int LG = S == 32 ? 5 : 6, RPL = S / (32 * NC);
+    const uint16_t* key16 = reinterpret_cast<const uint16_t*>(pay);
+    uint32_t mlo = 0, mhi = 0;
+    for (int k = lane; k < z; k += 32) {  // 32 < z <= S
+        const int rk = key16[k] >> LG;
+        if (rk < 32)
+            mlo |= 1u << rk;
+        else
+            mhi |= 1u << (rk - 32);
+    }
+    mlo = __reduce_or_sync(kFull, mlo);
+    if (S == 64)
+        mhi = __reduce_or_sync(kFull, mhi);
+#pragma unroll
+    for (int i = 0; i < RPL; ++i) {
+        const int row = row_of<S, NC>(wl, i, lane);
+        const bool lower = row < 32;
+        const uint32_t bits = lower ? mlo : mhi;
+        const int rb = lower ? row : row - 32;
+        if ((bits >> rb) & 1u) {
+            const int k = (lower ? 0 : __popc(mlo)) + __popc(bits & ((1u << rb) - 1u));
+            const int c = (int)(key16[k] & (S - 1));
+            const T v = widen(vs[k]);
+#pragma unroll
+            for (int h = 0; h < K; ++h)
+                acc[i][h] = fadd(acc[i][h], fmul(v, xs[c * K + h]));
+        }
+    }
+}
+
 // COO / CSR tile: the lane adds each of its rows' elements in stored order
 // (columns ascending), the rows' chains interleaved.  A CSR tile gives each
-// row's range in its row_end array.  A COO tile whose rows hold one element
-// each (stencil and band diagonals, sparse graph tiles) finds a row's element
-// by a popcount over the warp's bit set of occupied rows; other COO tiles
-// hand few products to the row lanes by shuffles, or mark where each row
-// starts and ends in the sorted keys (rng: 2 S marks).
+// row's range in its row_end array; a COO tile hands few products to the row
+// lanes by shuffles, or marks where each row starts and ends in the sorted
+// keys (rng: 2 S marks).
 template <int S, int K, int VT, int NC, bool CSR>
 __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs, const uint8_t* pay,
                                            const typename val_traits<VT>::V* vs, int z,
@@ -588,39 +628,6 @@ __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs,
     constexpr int LG = S == 32 ? 5 : 6, RPL = S / (32 * NC);
     const uint16_t* key16 = reinterpret_cast<const uint16_t*>(pay);  // COO keys / CSR row ends
     const uint8_t* col8 = pay + 2 * S;                                // CSR local columns
-    if (!CSR && z <= S) {
-        // the rows holding elements as a bit set; when no row holds two, a
-        // row's element index is the number of such rows above it
-        uint32_t mlo = 0, mhi = 0;
-        for (int k = lane; k < z; k += 32) {
-            const int rk = key16[k] >> LG;
-            if (rk < 32)
-                mlo |= 1u << rk;
-            else
-                mhi |= 1u << (rk - 32);
-        }
-        mlo = __reduce_or_sync(kFull, mlo);
-        if (S == 64)
-            mhi = __reduce_or_sync(kFull, mhi);
-        if (__popc(mlo) + __popc(mhi) == z) {
-#pragma unroll
-            for (int i = 0; i < RPL; ++i) {
-                const int row = row_of<S, NC>(wl, i, lane);
-                const bool lower = row < 32;
-                const uint32_t bits = lower ? mlo : mhi;
-                const int rb = lower ? row : row - 32;
-                if ((bits >> rb) & 1u) {
-                    const int k = (lower ? 0 : __popc(mlo)) + __popc(bits & ((1u << rb) - 1u));
-                    const int c = (int)(key16[k] & (S - 1));
-                    const T v = widen(vs[k]);
-#pragma unroll
-                    for (int h = 0; h < K; ++h)
-                        acc[i][h] = fadd(acc[i][h], fmul(v, xs[c * K + h]));
-                }
-            }
-            return;
-        }
-    }
     if (!CSR && z <= 32) {
         // few elements: element lane k forms its product, and each row lane
         // takes the products of its rows from the element lanes in key order
@@ -727,11 +734,16 @@ __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot
     const T* xs = reinterpret_cast<const T*>(slot + r.x_off + j * XB);
     const uint8_t* pay = slot + r.pay_off + (d.io - r.io0);
     const V* vs = reinterpret_cast<const V*>(slot + r.val_off) + (d.vo - r.vbase);
-    switch (d.pb_sch >> 24) {
+    switch ((d.pb_sch >> 24) & 3u) {
     case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K, VT, NC>(xs, pay, vs, acc, wl, lane); break;
     case ABHSF_SCHEME_DENSE: sum_dense<S, K, VT, NC>(xs, vs, acc, wl, lane); break;
     case ABHSF_SCHEME_CSR: sum_sparse<S, K, VT, NC, true>(xs, pay, vs, (int)d.nv, acc, rng, wl, lane); break;
-    default: sum_sparse<S, K, VT, NC, false>(xs, pay, vs, (int)d.nv, acc, rng, wl, lane); break;
+    default:
+        if (d.pb_sch & kDistinctRows)
+            sum_distinct<S, K, VT, NC>(xs, pay, vs, (int)d.nv, acc, wl, lane);
+        else
+            sum_sparse<S, K, VT, NC, false>(xs, pay, vs, (int)d.nv, acc, rng, wl, lane);
+        break;
     }
     if (d.info & kLast) {
         const int64_t m = B ? r.m : P.A.m;
@@ -958,7 +970,7 @@ __global__ void k_ring_weight(int64_t nr, const uint32_t* __restrict__ rows, til
 }
 
 __global__ void k_ring_fill(int64_t nitems, const uint32_t* __restrict__ rows, const int64_t* __restrict__ base,
-                            tiles_view A, uint32_t col_or, ring_desc* __restrict__ out)
+                            tiles_view A, int s, uint32_t col_or, ring_desc* __restrict__ out)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nitems;
          k += (int64_t)gridDim.x * blockDim.x) {
@@ -971,6 +983,15 @@ __global__ void k_ring_fill(int64_t nitems, const uint32_t* __restrict__ rows, c
             d.col = A.tile_col[t] | col_or;
             d.nv = (uint32_t)(A.tile_val_off[t + 1] - d.vo);
             d.pb_sch = (uint32_t)(A.tile_idx_off[t + 1] - d.io) | ((uint32_t)A.tile_scheme[t] << 24);
+            if (A.tile_scheme[t] == ABHSF_SCHEME_COO && d.nv > 32 && d.nv <= (uint32_t)s) {
+                const uint16_t* key = reinterpret_cast<const uint16_t*>(A.payload + d.io);
+                const int lg = s == 32 ? 5 : 6;
+                bool distinct = true;
+                for (uint32_t e = 1; e < d.nv && distinct; ++e)
+                    distinct = (key[e] >> lg) != (key[e - 1] >> lg);
+                if (distinct)
+                    d.pb_sch |= kDistinctRows;
+            }
             d.info = I | (t == t0 ? kFirst : 0u) | (t == t1 - 1 ? kLast : 0u);
             out[base[k] + (t - t0)] = d;
         }
@@ -1268,7 +1289,7 @@ bool build_ring_schedule(const std::vector<const abhsf_matrix*>& mats, int col_b
         ABHSF_CUDA(cudaMemcpyAsync(base_d.get(), m_base[i].data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
         const uint32_t col_or = col_bits >= 32 ? 0u : (uint32_t)i << col_bits;
         const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 4096));
-        k_ring_fill<<<g, 256, 0, st>>>(n, rows_d.get(), base_d.get(), mats[i]->view(), col_or,
+        k_ring_fill<<<g, 256, 0, st>>>(n, rows_d.get(), base_d.get(), mats[i]->view(), s, col_or,
                                        reinterpret_cast<ring_desc*>(desc.get()));
         ABHSF_CUDA(cudaGetLastError());
         ABHSF_CUDA(cudaStreamSynchronize(st));  // before the host vectors and staging buffers go
