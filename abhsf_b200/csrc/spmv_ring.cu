@@ -525,14 +525,33 @@ __device__ __forceinline__ void sum_bitmap(const typename val_traits<VT>::T* xs,
         }
         base += __shfl_sync(kFull, inc, 31);
     }
+    // x of this word's 32 columns in registers, read as 16-byte vectors
+    // (every lane reads the same address: a broadcast)
+    // (one right-hand side; with several the word's x would not fit registers)
+    constexpr int XW = K == 1 ? 32 : 1, XV = 16 / (int)sizeof(T);  // x values of a word; values per 16-byte read
 #pragma unroll
     for (int j = 0; j < W; ++j) {
+        T xw[XW];
+#pragma unroll
+        for (int e = 0; K == 1 && e < XW; e += XV) {
+            if (XV == 2) {
+                const double2 t = reinterpret_cast<const double2*>(xs + 32 * j * K)[e / 2];
+                xw[e] = t.x;
+                xw[e + 1] = t.y;
+            } else {
+                const float4 t = reinterpret_cast<const float4*>(xs + 32 * j * K)[e / 4];
+                xw[e] = t.x;
+                xw[e + 1] = t.y;
+                xw[e + 2] = t.z;
+                xw[e + 3] = t.w;
+            }
+        }
 #pragma unroll
         for (int b = 0; b < 32; ++b) {
             T xv[K];
 #pragma unroll
             for (int h = 0; h < K; ++h)
-                xv[h] = xs[(32 * j + b) * K + h];
+                xv[h] = K == 1 ? xw[b % XW] : xs[(32 * j + b) * K + h];
 #pragma unroll
             for (int i = 0; i < RPL; ++i) {
                 if ((w[i][j] >> b) & 1u) {
