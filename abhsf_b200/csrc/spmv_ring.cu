@@ -39,6 +39,8 @@
 // a lane keeps K accumulators for its row, and each of the K sums follows the
 // same order: column j of Y is bitwise what the SpMV of column j gives.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <queue>
 #include <vector>
 
@@ -1148,6 +1150,21 @@ struct event_pair {
     event_pair& operator=(const event_pair&) = delete;
 };
 
+// ABHSF_RING_VARIANT="<layout>,<bulk>" (e.g. "0,1") fixes the launch variant
+// instead of timing the four layouts: for profiles that must show one
+// variant, and for runs that must not depend on timing.  Malformed values are
+// ignored.
+bool forced_variant(int& layout, int& bulk)
+{
+    const char* v = std::getenv("ABHSF_RING_VARIANT");
+    int l = -1, b = -1;
+    if (!v || std::sscanf(v, "%d,%d", &l, &b) != 2 || l < 0 || l >= kLayouts || (b != 0 && b != 1))
+        return false;
+    layout = l;
+    bulk = b;
+    return true;
+}
+
 // The variant (consumer layout, bulk x / y copies or not) whose launches of
 // run(layout, bulk) take least time on st: one untimed and five timed each,
 // the median compared.  At s = 32 layout 3 is layout 1 and is skipped.
@@ -1187,6 +1204,8 @@ template <int S, int VT>
 void tune_ring(abhsf_matrix& a, cudaStream_t st)
 {
     using T = typename val_traits<VT>::T;
+    if (forced_variant(a.ring_layout, a.ring_bulk))
+        return;
     dbuf<T> x(a.n), y(a.m);
     ABHSF_CUDA(cudaMemsetAsync(x.get(), 0, a.n * sizeof(T), st));
     ABHSF_CUDA(cudaMemsetAsync(y.get(), 0, a.m * sizeof(T), st));
@@ -1407,13 +1426,14 @@ void prepare_batch(abhsf_batch& b, cudaStream_t st)
         ABHSF_CUDA(cudaMemcpyAsync(xs_d.get(), xs.data(), xs.size() * sizeof(double*), cudaMemcpyHostToDevice, st));
         ABHSF_CUDA(cudaMemcpyAsync(ys_d.get(), ys.data(), ys.size() * sizeof(double*), cudaMemcpyHostToDevice, st));
         int layout = 0, bulk = 0;
-        time_variants(
-            [&](int tm, int bk) {
-                b.layout = tm;
-                b.bulk = bk;
-                batch_launch(b, xs_d.get(), ys_d.get(), st, true);
-            },
-            b.s, st, layout, bulk);
+        if (!forced_variant(layout, bulk))
+            time_variants(
+                [&](int tm, int bk) {
+                    b.layout = tm;
+                    b.bulk = bk;
+                    batch_launch(b, xs_d.get(), ys_d.get(), st, true);
+                },
+                b.s, st, layout, bulk);
         b.layout = layout;
         b.bulk = bulk;
         ABHSF_CUDA(cudaMemsetAsync(b.dev_status.get(), 0, sizeof(int), st));
