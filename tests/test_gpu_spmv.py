@@ -236,3 +236,24 @@ def test_every_ring_variant_gives_the_reference_y(gpu, s):
                 np.testing.assert_array_equal(run_spmv(A, x, y0), want, err_msg=f"{coo.name} {layout} {bulk}")
         assert A.device_status() == 0
         A.release()
+
+
+def test_ring_variant_environment_override(gpu, monkeypatch):
+    """ABHSF_RING_VARIANT fixes the launch variant the build would time;
+    malformed values fall back to timing."""
+    import ctypes as C
+    coo = W.laplacian_3d(12)
+    t, b = C.c_int32(), C.c_int32()
+    for value, want in (("2,0", (2, 0)), ("3,1", (3, 1))):
+        monkeypatch.setenv("ABHSF_RING_VARIANT", value)
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+        assert capi.lib.abhsf_test_ring_variant(A.handle, 0, C.byref(t), C.byref(b)) == capi.SUCCESS
+        assert (t.value, b.value) == want
+        A.release()
+    monkeypatch.setenv("ABHSF_RING_VARIANT", "7,1")
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    assert capi.lib.abhsf_test_ring_variant(A.handle, 0, C.byref(t), C.byref(b)) == capi.SUCCESS
+    assert t.value in (0, 1, 2, 3)
+    x, y0 = W.rhs(coo.n, 1), W.rhs(coo.m, 2)
+    np.testing.assert_array_equal(run_spmv(A, x, y0), reference_order_y(coo, x, y0))
+    A.release()
