@@ -20,6 +20,7 @@ VALUE_TYPES = {"f64": 0, "f32": 1, "bf16": 2}
 MATRIX_TYPES = {"binary": 0, "integer": 1, "real": 2, "complex": 3}
 SUM_ORDERS = {"reference": 0, "tree": 1}
 NOALLOC_MAX_NNZ = 1048576
+BSTATS_ALL_LEN = 260164
 DEVSTAT_WAIT_TIMEOUT = 1
 SELECTORS = {"minbss": 0, "learned": 1, "autotune": 2}
 FEATURES, MLP_HIDDEN, MLP_CLASSES = 12, 64, 5
@@ -114,6 +115,7 @@ PROTOTYPES = {
     "abhsf_export_host": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "abhsf_block_histogram": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _i32, _i32, _vp, _u64p, _i64,
                                         C.POINTER(_i64)]),
+    "abhsf_block_histogram_all": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _vp, _u64p, C.POINTER(_i64)]),
     "abhsf_block_histogram_noalloc": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _i32, _vp, _u64p, _i64,
                                                 C.POINTER(_i64)]),
     "abhsf_mmf_line": (C.c_int, [_i64, _i64, _i64, _i32, _i32, _i32, _u64p, _i64, _u64p, _u64p]),

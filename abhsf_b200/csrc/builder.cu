@@ -10,6 +10,7 @@
 // adds whose result does not depend on their order.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
 
 #include <algorithm>
 #include <map>
@@ -229,6 +230,92 @@ __global__ void k_block_keys(const int64_t* __restrict__ rows, const int64_t* __
         }
         // block_statistics/block_stats.cpp:69-74
         keys[i] = ((uint64_t(r) >> k) << 32) + (uint64_t(c) >> l);
+    }
+}
+
+// All 64 block sizes: elements sorted by (column >> l, row) put every block
+// of 2^k x 2^l (k = 1..8) in one run, so one sort per column width l serves
+// eight block heights.
+__global__ void k_col_row_keys(const int64_t* __restrict__ rows, const int64_t* __restrict__ cols, int64_t nnz,
+                               int64_t m, int64_t n, int l, uint64_t* __restrict__ keys, int* __restrict__ err)
+{
+    GRID_STRIDE(i, nnz)
+    {
+        const int64_t r = rows[i], c = cols[i];
+        if (r < 0 || r >= m || c < 0 || c >= n) {
+            atomicOr(err, kErrRange);
+            keys[i] = 0;
+            continue;
+        }
+        keys[i] = ((uint64_t(c) >> l) << 32) | uint64_t(r);
+    }
+}
+
+// Bit k - 1 of heads[e]: element e starts a 2^k x 2^l block in the sorted order.
+__global__ void k_block_heads_all(const uint64_t* __restrict__ keys, int64_t nnz, uint8_t* __restrict__ heads)
+{
+    GRID_STRIDE(e, nnz)
+    {
+        uint8_t h = 0xff;
+        if (e > 0) {
+            const uint64_t a = keys[e - 1], b = keys[e];
+            if ((a >> 32) == (b >> 32)) {
+                const uint32_t ra = (uint32_t)a, rb = (uint32_t)b;
+                h = 0;
+#pragma unroll
+                for (int k = 1; k <= 8; ++k)
+                    h |= (uint8_t)(((ra >> k) != (rb >> k)) << (k - 1));
+            }
+        }
+        heads[e] = h;
+    }
+}
+
+__global__ void k_head_bit(const uint8_t* __restrict__ heads, int64_t nnz, int bit, uint8_t* __restrict__ flag)
+{
+    GRID_STRIDE(e, nnz)
+    flag[e] = (heads[e] >> bit) & 1u;
+}
+
+__global__ void k_iota(int64_t nnz, int64_t* __restrict__ out)
+{
+    GRID_STRIDE(e, nnz)
+    out[e] = e;
+}
+
+// Block lengths into a histogram held in shared memory (hist_len <= 8192),
+// then added to the global one.
+__global__ void k_len_hist_shared(int64_t B, const int64_t* __restrict__ start, int64_t nnz,
+                                  unsigned long long* __restrict__ hist, int hist_len, int* __restrict__ err)
+{
+    extern __shared__ unsigned int sh[];
+    for (int i = threadIdx.x; i < hist_len; i += blockDim.x)
+        sh[i] = 0;
+    __syncthreads();
+    GRID_STRIDE(b, B)
+    {
+        const int64_t len = (b + 1 < B ? start[b + 1] : nnz) - start[b];
+        if (len < hist_len)
+            atomicAdd(&sh[len], 1u);
+        else
+            atomicOr(err, kErrHistOverflow);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < hist_len; i += blockDim.x)
+        if (sh[i])
+            atomicAdd(hist + i, (unsigned long long)sh[i]);
+}
+
+__global__ void k_len_hist_global(int64_t B, const int64_t* __restrict__ start, int64_t nnz,
+                                  unsigned long long* __restrict__ hist, int64_t hist_len, int* __restrict__ err)
+{
+    GRID_STRIDE(b, B)
+    {
+        const int64_t len = (b + 1 < B ? start[b + 1] : nnz) - start[b];
+        if (len < hist_len)
+            atomicAdd(hist + len, 1ull);
+        else
+            atomicOr(err, kErrHistOverflow);
     }
 }
 
@@ -668,6 +755,80 @@ struct scratch_arena {
 };
 
 }  // namespace
+
+void block_histogram_all(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, bool on_device,
+                         cudaStream_t st, uint64_t* hist, int64_t* blocks)
+{
+    if (m <= 0 || n <= 0 || nnz < 0)
+        fail(ABHSF_ERROR_INVALID_VALUE, "m and n must be positive and nnz non-negative");
+    if (!hist)
+        fail(ABHSF_ERROR_INVALID_VALUE, "hist must hold ABHSF_BSTATS_ALL_LEN counters");
+    if ((uint64_t)(m - 1) >= (uint64_t(1) << 32) || ((uint64_t)(n - 1) >> 1) >= (uint64_t(1) << 32))
+        fail(ABHSF_ERROR_UNSUPPORTED, "row index or block column index beyond 32 bits");
+    std::fill(hist, hist + ABHSF_BSTATS_ALL_LEN, 0);
+    if (blocks)
+        std::fill(blocks, blocks + 64, 0);
+    if (nnz == 0)
+        return;
+    if (!rows || !cols)
+        fail(ABHSF_ERROR_INVALID_VALUE, "rows and cols must be non-NULL");
+    coo_inputs in(rows, cols, nullptr, nnz, on_device, st);
+    dbuf<int> err(1);
+    ABHSF_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
+    dbuf<unsigned long long> dh(ABHSF_BSTATS_ALL_LEN);
+    ABHSF_CUDA(cudaMemsetAsync(dh.get(), 0, ABHSF_BSTATS_ALL_LEN * sizeof(unsigned long long), st));
+    dbuf<uint64_t> keys(nnz), sorted(nnz);
+    dbuf<uint8_t> heads(nnz), flag(nnz);
+    dbuf<int64_t> iota(nnz), starts(nnz);
+    dbuf<int64_t> nsel(1);
+    k_iota<<<grid_for(nnz), kThreads, 0, st>>>(nnz, iota.get());
+    check_launch("k_iota");
+    size_t sort_bytes = 0, sel_bytes = 0;
+    ABHSF_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, keys.get(), sorted.get(), nnz, 0, 64, st));
+    ABHSF_CUDA(cub::DeviceSelect::Flagged(nullptr, sel_bytes, iota.get(), flag.get(), starts.get(), nsel.get(), nnz,
+                                          st));
+    dbuf<uint8_t> tmp(std::max(sort_bytes, sel_bytes));
+    std::vector<int64_t> count(64, 0);
+    int64_t off[64];
+    for (int p = 0, o = 0; p < 64; ++p) {
+        off[p] = o;
+        o += (1 << (p / 8 + 1)) * (1 << (p % 8 + 1)) + 1;
+    }
+    for (int l = 1; l <= 8; ++l) {
+        k_col_row_keys<<<grid_for(nnz), kThreads, 0, st>>>(in.rows, in.cols, nnz, m, n, l, keys.get(), err.get());
+        check_launch("k_col_row_keys");
+        if (l == 1)
+            raise_err(read_scalar(err.get(), st));
+        const int end_bit = 32 + bit_length((uint64_t)(n - 1) >> l);
+        size_t b1 = sort_bytes;
+        ABHSF_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), b1, keys.get(), sorted.get(), nnz, 0, end_bit, st));
+        k_block_heads_all<<<grid_for(nnz), kThreads, 0, st>>>(sorted.get(), nnz, heads.get());
+        check_launch("k_block_heads_all");
+        for (int k = 1; k <= 8; ++k) {
+            const int p = (k - 1) * 8 + (l - 1);
+            const int64_t hl = (int64_t(1) << k) * (int64_t(1) << l) + 1;
+            k_head_bit<<<grid_for(nnz), kThreads, 0, st>>>(heads.get(), nnz, k - 1, flag.get());
+            check_launch("k_head_bit");
+            size_t b2 = sel_bytes;
+            ABHSF_CUDA(cub::DeviceSelect::Flagged(tmp.get(), b2, iota.get(), flag.get(), starts.get(), nsel.get(), nnz,
+                                                  st));
+            const int64_t B = read_scalar(nsel.get(), st);
+            count[p] = B;
+            if (hl <= 8192)
+                k_len_hist_shared<<<grid_for(B), kThreads, hl * sizeof(unsigned int), st>>>(
+                    B, starts.get(), nnz, dh.get() + off[p], (int)hl, err.get());
+            else
+                k_len_hist_global<<<grid_for(B), kThreads, 0, st>>>(B, starts.get(), nnz, dh.get() + off[p], hl,
+                                                                     err.get());
+            check_launch("k_len_hist");
+        }
+    }
+    raise_err(read_scalar(err.get(), st));
+    ABHSF_CUDA(cudaMemcpyAsync(hist, dh.get(), ABHSF_BSTATS_ALL_LEN * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    ABHSF_CUDA(cudaStreamSynchronize(st));
+    if (blocks)
+        std::copy(count.begin(), count.end(), blocks);
+}
 
 void block_histogram_noalloc(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r,
                              int s, cudaStream_t st, uint64_t* hist, int64_t hist_len, int64_t* blocks)

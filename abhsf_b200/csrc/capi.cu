@@ -356,6 +356,16 @@ abhsf_status abhsf_block_histogram(const int64_t* rows, const int64_t* cols, int
     });
 }
 
+abhsf_status abhsf_block_histogram_all(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n,
+                                       int32_t inputs_on_device, abhsf_stream_t stream, uint64_t* hist,
+                                       int64_t* blocks)
+{
+    return guarded([&] {
+        abhsf::block_histogram_all(rows, cols, nnz, m, n, inputs_on_device != 0,
+                                   reinterpret_cast<cudaStream_t>(stream), hist, blocks);
+    });
+}
+
 abhsf_status abhsf_block_histogram_noalloc(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m,
                                            int64_t n, int32_t r, int32_t s, abhsf_stream_t stream, uint64_t* hist,
                                            int64_t hist_len, int64_t* blocks)

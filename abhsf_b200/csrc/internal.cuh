@@ -14,6 +14,10 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
 void block_histogram(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r, int s,
                      bool on_device, cudaStream_t st, uint64_t* hist, int64_t hist_len, int64_t* blocks);
 
+// All 64 block sizes 2^k x 2^l (k, l = 1..8) in one call (abhsf_block_histogram_all).
+void block_histogram_all(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, bool on_device,
+                         cudaStream_t st, uint64_t* hist, int64_t* blocks);
+
 // abhsf_block_histogram with device inputs and all scratch in a static array.
 void block_histogram_noalloc(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, int r,
                              int s, cudaStream_t st, uint64_t* hist, int64_t hist_len, int64_t* blocks);

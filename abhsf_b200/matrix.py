@@ -259,6 +259,35 @@ def block_histogram(rows, cols, m: int, n: int, r: int, s: int, stream=None) -> 
     return {int(z): int(hist[z]) for z in nz}
 
 
+def block_histograms_all(rows, cols, m: int, n: int, stream=None) -> dict[str, dict[int, int]]:
+    """"RxS" -> {block nnz: blocks} for all 64 block sizes 2..256 x 2..256 in one
+    GPU call (the 64 .bstats files of block_statistics/block_stats.cpp:144-170)."""
+    on_dev = _is_cuda(rows)
+    if on_dev:
+        rows = rows.to(torch.int64).contiguous()
+        cols = cols.to(torch.int64).contiguous()
+        nnz = rows.numel()
+    else:
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        cols = np.ascontiguousarray(cols, dtype=np.int64)
+        nnz = rows.size
+    hist = np.zeros(capi.BSTATS_ALL_LEN, dtype=np.uint64)
+    blocks = np.zeros(64, dtype=np.int64)
+    capi.check(capi.lib.abhsf_block_histogram_all(_ptr(rows) if nnz else None, _ptr(cols) if nnz else None, nnz, m, n,
+                                                  1 if on_dev else 0, _stream_ptr(stream),
+                                                  hist.ctypes.data_as(capi._u64p),
+                                                  blocks.ctypes.data_as(C.POINTER(C.c_int64))))
+    out, off = {}, 0
+    for p in range(64):
+        r, s = 2 << (p // 8), 2 << (p % 8)
+        h = hist[off:off + r * s + 1]
+        nz = np.nonzero(h)[0]
+        out[f"{r}x{s}"] = {int(z): int(h[z]) for z in nz}
+        assert sum(out[f"{r}x{s}"].values()) == blocks[p]
+        off += r * s + 1
+    return out
+
+
 def mmf_line(m: int, n: int, nnz: int, matrix_type: str | int, r: int, s: int, hist: dict[int, int]):
     """One line of the reference's mmf-single / mmf-double
     (block_statistics/mmf.cpp:53-138): [coo32, csr32, coo, csr, bitmap, dense,

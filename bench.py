@@ -406,6 +406,33 @@ def time_selector(dev, seeds=range(2000, 2050)):
     return out
 
 
+def time_bstats(c, dev):
+    """The reference's whole block-statistics sweep (the 64 block sizes 2..256 x
+    2..256 of block_statistics/block_stats.cpp:144-170) on the timed matrix,
+    inputs on the GPU: one abhsf_block_histogram call per size (one sort
+    each, as the reference) against one abhsf_block_histogram_all call (one
+    sort per column width)."""
+    import torch
+    from abhsf_b200 import block_histogram, block_histograms_all
+    rows = torch.from_numpy(c.rows).to(dev)
+    cols = torch.from_numpy(c.cols).to(dev)
+    block_histograms_all(rows, cols, c.m, c.n)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    allh = block_histograms_all(rows, cols, c.m, c.n)
+    t_all = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    same = True
+    for k in range(1, 9):
+        for l in range(1, 9):
+            h = block_histogram(rows, cols, c.m, c.n, 1 << k, 1 << l)
+            same = same and h == allh[f"{1 << k}x{1 << l}"]
+    t_per = time.perf_counter() - t0
+    del rows, cols
+    return {"workload": "the timed matrix, 64 block sizes", "per_size_s": t_per, "one_call_s": t_all,
+            "speedup": t_per / t_all, "identical": same}
+
+
 def cpu_reference_run(c, bytes_per_step: float, max_seconds: float, max_iters: int):
     """Reference CSR spmv_naive (oracle/_ref, compiled from the reference
     sources) on all host threads; falls back to the single-thread oracle port."""
@@ -557,6 +584,7 @@ def run_ours(args):
     batched = None if args.no_batched or rank != 0 else time_batched(dev, l2_flush, args.warmup)
     cusparse = None if args.no_cusparse or rank != 0 else time_cusparse(c, dev, l2_flush, args.warmup, t_mean)
     selector = None if args.no_selector or rank != 0 else time_selector(dev)
+    bstats = None if args.no_bstats or rank != 0 else time_bstats(c, dev)
 
     peak, peak_src = hbm_peak()
     achieved = B / (t_mean * 1e-3) / 1e9
@@ -593,6 +621,7 @@ def run_ours(args):
             "batched": batched,
             "cusparse_csr": cusparse,
             "selector": selector,
+            "block_stats_sweep": bstats,
             "e2e": {"value": aggregate_rate(B, e2e_s, world), "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
                     "d2h_bytes_per_step": 8 * c.m, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": args.steps,
@@ -618,6 +647,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-matrix batched launch")
     ap.add_argument("--no-cusparse", action="store_true", help="skip the cuSPARSE CSR reference point")
     ap.add_argument("--no-selector", action="store_true", help="skip the block-size selector evaluation")
+    ap.add_argument("--no-bstats", action="store_true", help="skip the 64-size block-statistics sweep")
     ap.add_argument("--sum-order", choices=["reference", "tree"], default="reference",
                     help="reference: bitwise the reference CSR's y; tree: warp reduction trees")
     ap.add_argument("--n", type=int, default=DEFAULT_N,

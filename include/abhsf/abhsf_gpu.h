@@ -272,6 +272,22 @@ ABHSF_API abhsf_status abhsf_block_histogram(const int64_t* rows, const int64_t*
                                    abhsf_stream_t stream, uint64_t* hist, int64_t hist_len,
                                    int64_t* blocks);
 
+/* Counters abhsf_block_histogram_all writes: the sum over r, s = 2..256 of r*s + 1. */
+#define ABHSF_BSTATS_ALL_LEN 260164
+
+/* The block histograms of all 64 block sizes r x s = 2^k x 2^l (k, l = 1..8)
+ * in one call, as block_statistics/block_stats.cpp:144-170 writes its 64
+ * RxS.bstats files: size p = (k - 1) * 8 + (l - 1) occupies
+ * hist[off_p .. off_p + r*s], off_p = the sum of r'*s' + 1 over the sizes
+ * before it, and hist[off_p + z] = blocks holding z nonzeros.  blocks[64]
+ * (NULL allowed): nonzero blocks of each size.  The reference sorts the
+ * elements once per size; here elements sorted by (column >> l, row) put the
+ * blocks of all eight heights in runs, so one sort per width serves eight
+ * sizes.  Synchronises stream. */
+ABHSF_API abhsf_status abhsf_block_histogram_all(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m,
+                                                 int64_t n, int32_t inputs_on_device, abhsf_stream_t stream,
+                                                 uint64_t* hist, int64_t* blocks);
+
 /* Largest nnz abhsf_block_histogram_noalloc accepts. */
 #define ABHSF_NOALLOC_MAX_NNZ 1048576
 

@@ -130,3 +130,32 @@ def test_empty_matrix(gpu):
     A.spmv(x, y)
     torch.cuda.synchronize()
     assert torch.all(y == 2.0)
+
+
+@pytest.mark.parametrize("name", sorted(golden_stats()))
+def test_all_block_sizes_in_one_call_match_reference_block_stats(gpu, name):
+    """abhsf_block_histogram_all: the 64 .bstats histograms of the reference's
+    block_stats (block_statistics/block_stats.cpp:144-170) from one call."""
+    from abhsf_b200 import block_histograms_all
+    g = golden_stats()[name]
+    coo = W.laplacian_2d(512) if name == "laplace2d_512" else golden_matrices()[name]
+    got = block_histograms_all(coo.rows, coo.cols, coo.m, coo.n)
+    want = {rs: {int(z): c for z, c in h.items()} for rs, h in g["bstats"].items()}
+    assert set(got) == set(want)
+    for rs in want:
+        assert got[rs] == want[rs], rs
+
+
+def test_all_block_sizes_equal_per_size_histograms(gpu):
+    import torch
+    from abhsf_b200 import block_histogram, block_histograms_all
+    coo = W.tiled_mixture(n=65536 + 37, p=1e-3, seed=5)
+    for rows, cols in ((coo.rows, coo.cols), (torch.from_numpy(coo.rows).cuda(), torch.from_numpy(coo.cols).cuda())):
+        got = block_histograms_all(rows, cols, coo.m, coo.n)
+        for rs in ("2x2", "4x256", "64x64", "256x2", "256x256", "128x32"):
+            r, s = (int(t) for t in rs.split("x"))
+            assert got[rs] == block_histogram(coo.rows, coo.cols, coo.m, coo.n, r, s), rs
+    with pytest.raises(capi.IndexOutOfRange):
+        block_histograms_all(np.array([0, 9]), np.array([0, 1]), 5, 5)
+    empty = block_histograms_all(np.zeros(0, np.int64), np.zeros(0, np.int64), 5, 5)
+    assert all(h == {} for h in empty.values())
