@@ -2,7 +2,7 @@
 
 The reference picks the block size of a matrix by computing its block
 statistics at every candidate size and taking the one of least storage
-(block_statistics/min-bss.cpp:14-58), and judges restricted choices by their
+(block_statistics/min-bss.cpp:14-58), and scores restricted choices by their
 regret, the storage above the minimum in percent, averaged and maximised over
 matrices (block_statistics/consistency.cpp:140-174).
 
