@@ -287,10 +287,12 @@ abhsf_status abhsf_spmv_host(abhsf_matrix* a, const double* x, double* y, abhsf_
             a->x_stage.alloc(a->n);
         if (!a->y_stage.get() || a->y_stage.size() < (size_t)a->m)
             a->y_stage.alloc(a->m);
-        ABHSF_CUDA(cudaMemcpyAsync(a->x_stage.get(), x, a->n * sizeof(double), cudaMemcpyHostToDevice, st));
-        ABHSF_CUDA(cudaMemcpyAsync(a->y_stage.get(), y, a->m * sizeof(double), cudaMemcpyHostToDevice, st));
-        abhsf::spmv_dispatch(*a, a->x_stage.get(), a->y_stage.get(), st);
-        ABHSF_CUDA(cudaMemcpyAsync(y, a->y_stage.get(), a->m * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (!abhsf::spmv_f64_ring_host(*a, x, y, st)) {
+            ABHSF_CUDA(cudaMemcpyAsync(a->x_stage.get(), x, a->n * sizeof(double), cudaMemcpyHostToDevice, st));
+            ABHSF_CUDA(cudaMemcpyAsync(a->y_stage.get(), y, a->m * sizeof(double), cudaMemcpyHostToDevice, st));
+            abhsf::spmv_dispatch(*a, a->x_stage.get(), a->y_stage.get(), st);
+            ABHSF_CUDA(cudaMemcpyAsync(y, a->y_stage.get(), a->m * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
         ABHSF_CUDA(cudaStreamSynchronize(st));
     });
 }

@@ -177,6 +177,31 @@ struct abhsf_matrix {
     abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
     // staging for abhsf_spmv_host
     abhsf::dbuf<double> x_stage, y_stage;
+    // abhsf_spmv_host's pipeline (ring kernel): the block rows in chunks, each
+    // with its own schedule, so that copying y in and out overlaps the sums
+    struct host_chunk {
+        int64_t brow0 = 0, brow1 = 0;  // block rows [brow0, brow1)
+        abhsf::dbuf<uint8_t> desc;
+        abhsf::dbuf<int64_t> wbeg;
+        int ctas = 0;
+    };
+    std::vector<host_chunk> host_chunks;
+    bool host_ready = false;
+    cudaStream_t host_in = nullptr, host_out = nullptr;
+    std::vector<cudaEvent_t> host_events;
+
+    abhsf_matrix() = default;
+    abhsf_matrix(const abhsf_matrix&) = delete;
+    abhsf_matrix& operator=(const abhsf_matrix&) = delete;
+    ~abhsf_matrix()
+    {
+        for (cudaEvent_t e : host_events)
+            cudaEventDestroy(e);
+        if (host_in)
+            cudaStreamDestroy(host_in);
+        if (host_out)
+            cudaStreamDestroy(host_out);
+    }
 
     abhsf::tiles_view view() const
     {

@@ -66,6 +66,10 @@ void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_
 // The same order through per-warp shared-memory rings (s = 32, 64); false
 // when the matrix has no ring schedule.
 bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
+// y += A x with x and y in host memory through the ring kernel, the block rows
+// in chunks so that y's copies overlap the sums (ordered on st, not
+// synchronised); false where the one-shot path serves (other kernels, small m).
+bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_t st);
 // Batches (spmv_ring.cu): the ring kernel's schedule over every matrix of the
 // batch, and y_i += A_i x_i for all of them in one launch (xs, ys: device
 // arrays of device pointers).

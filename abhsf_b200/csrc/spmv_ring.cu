@@ -1061,15 +1061,19 @@ void launch_any(int layout, unsigned grid, const ring_args& P, cudaStream_t st)
 // One pass: K right-hand sides, X and Y starting at their first column.
 template <int S, int K, int VT>
 void launch_ring(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int64_t ldy, cudaStream_t st,
-                 bool tuning = false)
+                 bool tuning = false, const uint8_t* desc = nullptr, const int64_t* wbeg = nullptr, int ctas = 0)
 {
     static_assert(((sizeof(ring_smem<S, K, VT>) + 1023) / 1024 + 1) * 1024 * kCtasPerSm <= 233472,
                   "kCtasPerSm CTAs fit an SM even with shared memory allocated in 1 KiB granules");
-    ring_args P{a.view(), reinterpret_cast<const ring_desc*>(a.ring_desc.get()),
-                a.ring_wbeg.get(), x, y, ldx, ldy, nullptr, nullptr, nullptr,
+    if (!desc) {  // the whole matrix's schedule (else one chunk of block rows, abhsf_spmv_host)
+        desc = a.ring_desc.get();
+        wbeg = a.ring_wbeg.get();
+        ctas = a.ring_warps;
+    }
+    ring_args P{a.view(), reinterpret_cast<const ring_desc*>(desc), wbeg, x, y, ldx, ldy, nullptr, nullptr, nullptr,
                 a.dev_status.get(), a.ring_bulk, tuning ? -1 : g_drop_desc,
                 (g_spin_limit && !tuning) ? g_spin_limit : kWaitPolls};
-    launch_any<S, K, VT, false>(a.ring_layout, (unsigned)a.ring_warps, P, st);
+    launch_any<S, K, VT, false>(a.ring_layout, (unsigned)ctas, P, st);
 }
 
 template <int S, int K, int VT, bool B = false, int L = 0>
@@ -1229,7 +1233,8 @@ void tune_ring(abhsf_matrix& a, cudaStream_t st)
 // i << col_bits.  Returns false when a CTA would get more tiles than its
 // counters hold.
 bool build_ring_schedule(const std::vector<const abhsf_matrix*>& mats, int col_bits, dbuf<uint8_t>& desc,
-                         dbuf<int64_t>& wbeg_d, int& ctas_out, int& max_pv_out, cudaStream_t st)
+                         dbuf<int64_t>& wbeg_d, int& ctas_out, int& max_pv_out, cudaStream_t st, int64_t brow_lo = 0,
+                         int64_t brow_hi = INT64_MAX)
 {
     const int s = mats[0]->s, vt = mats[0]->value_type;
     const int vsize = (int)value_size(vt);
@@ -1270,6 +1275,23 @@ bool build_ring_schedule(const std::vector<const abhsf_matrix*>& mats, int col_b
         ABHSF_CUDA(cudaMemcpyAsync(&m_pv, max_pv.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
         ABHSF_CUDA(cudaStreamSynchronize(st));
         mpv = std::max(mpv, m_pv);
+    }
+    if (brow_lo > 0 || brow_hi < INT64_MAX) {  // only block rows [brow_lo, brow_hi)
+        size_t o = 0;
+        total_tiles = 0;
+        for (size_t k = 0; k < rows.size(); ++k)
+            if (rows[k] >= brow_lo && rows[k] < brow_hi) {
+                rows[o] = rows[k];
+                ntiles[o] = ntiles[k];
+                wt[o] = wt[k];
+                mid[o] = mid[k];
+                total_tiles += ntiles[k];
+                ++o;
+            }
+        rows.resize(o);
+        ntiles.resize(o);
+        wt.resize(o);
+        mid.resize(o);
     }
     const int64_t nitems = (int64_t)rows.size();
     if (nitems == 0)
@@ -1478,6 +1500,68 @@ bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t
     } else {
         return false;
     }
+    return true;
+}
+
+bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+{
+    constexpr int kChunks = 4;
+    if (a.ring_warps == 0 || a.value_type != ABHSF_VALUE_F64 || a.sum_order != ABHSF_SUM_REFERENCE ||
+        a.M < 4 * kChunks || a.m < (int64_t(1) << 20))
+        return false;  // small matrices: one copy each way is as fast
+    if (!a.host_ready) {
+        a.host_chunks.clear();
+        a.host_chunks.resize(kChunks);
+        for (int c = 0; c < kChunks; ++c) {
+            auto& ch = a.host_chunks[c];
+            ch.brow0 = a.M * c / kChunks;
+            ch.brow1 = a.M * (c + 1) / kChunks;
+            int mpv = 0;
+            if (!build_ring_schedule({&a}, 32, ch.desc, ch.wbeg, ch.ctas, mpv, st, ch.brow0, ch.brow1))
+                ch.ctas = 0;  // no tiles in these block rows
+        }
+        if (!a.host_in)
+            ABHSF_CUDA(cudaStreamCreateWithFlags(&a.host_in, cudaStreamNonBlocking));
+        if (!a.host_out)
+            ABHSF_CUDA(cudaStreamCreateWithFlags(&a.host_out, cudaStreamNonBlocking));
+        while (a.host_events.size() < 2 * kChunks + 2) {  // the matrix destroys what was created
+            cudaEvent_t e = nullptr;
+            ABHSF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            a.host_events.push_back(e);
+        }
+        a.host_ready = true;
+    }
+    cudaEvent_t* ev = a.host_events.data();  // [0] start, [1..C] y chunk in, [C+1..2C] chunk summed, [2C+1] end
+    double* xs = a.x_stage.get();
+    double* ys = a.y_stage.get();
+    ABHSF_CUDA(cudaEventRecord(ev[0], st));  // after the caller's earlier work on st
+    ABHSF_CUDA(cudaStreamWaitEvent(a.host_in, ev[0], 0));
+    ABHSF_CUDA(cudaMemcpyAsync(xs, x, a.n * sizeof(double), cudaMemcpyHostToDevice, a.host_in));
+    for (int c = 0; c < kChunks; ++c) {
+        const auto& ch = a.host_chunks[c];
+        const int64_t r0 = ch.brow0 * a.s, r1 = std::min(ch.brow1 * a.s, a.m);
+        ABHSF_CUDA(cudaMemcpyAsync(ys + r0, y + r0, (r1 - r0) * sizeof(double), cudaMemcpyHostToDevice, a.host_in));
+        ABHSF_CUDA(cudaEventRecord(ev[1 + c], a.host_in));
+    }
+    for (int c = 0; c < kChunks; ++c) {
+        const auto& ch = a.host_chunks[c];
+        ABHSF_CUDA(cudaStreamWaitEvent(st, ev[1 + c], 0));
+        if (ch.ctas > 0) {
+            if (a.s == 32)
+                launch_ring<32, 1, ABHSF_VALUE_F64>(a, xs, 1, ys, 1, st, false, ch.desc.get(), ch.wbeg.get(), ch.ctas);
+            else
+                launch_ring<64, 1, ABHSF_VALUE_F64>(a, xs, 1, ys, 1, st, false, ch.desc.get(), ch.wbeg.get(), ch.ctas);
+        }
+        ABHSF_CUDA(cudaEventRecord(ev[1 + kChunks + c], st));
+    }
+    for (int c = 0; c < kChunks; ++c) {
+        const auto& ch = a.host_chunks[c];
+        const int64_t r0 = ch.brow0 * a.s, r1 = std::min(ch.brow1 * a.s, a.m);
+        ABHSF_CUDA(cudaStreamWaitEvent(a.host_out, ev[1 + kChunks + c], 0));
+        ABHSF_CUDA(cudaMemcpyAsync(y + r0, ys + r0, (r1 - r0) * sizeof(double), cudaMemcpyDeviceToHost, a.host_out));
+    }
+    ABHSF_CUDA(cudaEventRecord(ev[2 * kChunks + 1], a.host_out));
+    ABHSF_CUDA(cudaStreamWaitEvent(st, ev[2 * kChunks + 1], 0));
     return true;
 }
 

@@ -131,6 +131,36 @@ def test_host_pointer_path_equals_device_path(gpu):
     np.testing.assert_array_equal(yh, yd)
 
 
+@pytest.mark.parametrize("s", [32, 64])
+def test_pipelined_host_path_equals_device_path(gpu, s):
+    """Host-memory x and y of a matrix with at least 2^20 rows go through the
+    chunked pipeline (y copied in and out chunk by chunk around one kernel
+    launch per chunk of block rows): y is bitwise the device path's, on
+    consecutive calls, with empty and non-empty chunks."""
+    import torch
+    n = (1 << 20) + 37
+    band = W.banded(n, 3, seed=5)
+    M = -(-n // s)  # block rows; the second of the pipeline's four chunks, [M/4, M/2), left empty
+    keep = (band.rows < (M // 4) * s) | (band.rows >= (M // 2) * s)
+    cases = [W.Coo(band.rows[keep], band.cols[keep], band.vals[keep], n, n, "band_gap"),
+             W.tiled_mixture(n=n, p=2e-5, seed=6)]
+    for coo in cases:
+        x = W.rhs(coo.n, 5)
+        y0 = W.rhs(coo.m, 6)
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s)
+        want = run_spmv(A, x, y0)
+        x_pin = torch.from_numpy(x).pin_memory().numpy()
+        for _ in range(2):
+            yh = torch.from_numpy(y0.copy()).pin_memory().numpy()
+            A.spmv(x_pin, yh)
+            np.testing.assert_array_equal(yh, want, err_msg=coo.name)
+        yp = y0.copy()  # pageable host memory works too
+        A.spmv(x, yp)
+        np.testing.assert_array_equal(yp, want, err_msg=coo.name)
+        assert A.device_status() == 0
+        A.release()
+
+
 @pytest.mark.parametrize("order", ["reference", "tree"])
 def test_spmv_is_deterministic(gpu, order):
     coo = W.random_blocky(3000, 3000, 64, 400, seed=21)
