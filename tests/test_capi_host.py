@@ -89,3 +89,44 @@ def test_block_histogram_argument_checks():
     with pytest.raises(capi.InvalidValue):
         mx.block_histogram(np.zeros(1, np.int64), np.zeros(1, np.int64), 4, 4, 512, 4)
     assert mx.block_histogram(np.zeros(0, np.int64), np.zeros(0, np.int64), 4, 4, 2, 2) == {}
+
+
+def test_selection_entry_points_reject_bad_arguments_before_device_work():
+    """The block-size selection and MLP entry points check their arguments
+    on the host (no GPU needed to see the error)."""
+    one = np.zeros(1, np.int64)
+    ms = np.zeros(5, np.float32)
+    best = C.c_int32()
+    fp = C.POINTER(C.c_float)
+    # autotune: candidate mask outside the five sizes, non-positive reps, bad shape
+    for cand, reps, m in ((32, 1, 4), (-1, 1, 4), (1, 0, 4), (1, 1, 0)):
+        st = capi.lib.abhsf_autotune(one.ctypes.data, one.ctypes.data, None, 1, m, 4, None, cand, reps, None,
+                                     ms.ctypes.data_as(fp), C.byref(best), None)
+        assert st == capi.INVALID_VALUE, (cand, reps, m)
+    assert capi.lib.abhsf_autotune(one.ctypes.data, one.ctypes.data, None, 1, 4, 4, None, 0, 1, None, None,
+                                   C.byref(best), None) == capi.INVALID_VALUE
+    # the storage sweep and the all-sizes histograms need their output arrays
+    assert capi.lib.abhsf_block_size_storage(one.ctypes.data, one.ctypes.data, 1, 4, 4, None, None, None,
+                                             None) == capi.INVALID_VALUE
+    assert capi.lib.abhsf_block_histogram_all(one.ctypes.data, one.ctypes.data, 1, 4, 4, 0, None, None,
+                                              None) == capi.INVALID_VALUE
+    assert capi.lib.abhsf_block_size_storage(one.ctypes.data, one.ctypes.data, 1, 0, 4, None, None,
+                                             np.zeros(5, np.uint64).ctypes.data_as(capi._u64p),
+                                             None) == capi.INVALID_VALUE
+    # the selector and the MLP kernels
+    assert capi.lib.abhsf_selector_predict(None, None, None, C.byref(best)) == capi.INVALID_VALUE
+    assert capi.lib.abhsf_selector_predict(None, ms.ctypes.data_as(fp), None, None) == capi.INVALID_VALUE
+    assert capi.lib.abhsf_selector_builtin_model(None) == capi.INVALID_VALUE
+    assert capi.lib.abhsf_selector_features(one.ctypes.data, one.ctypes.data, 1, 0, 4, 0, None,
+                                            ms.ctypes.data_as(fp)) == capi.INVALID_VALUE
+    assert capi.lib.abhsf_mlp_forward(None, None, -1, None, None, None) == capi.INVALID_VALUE
+    assert capi.lib.abhsf_mlp_backward(None, None, None, 0, None, None, None, None, None, None) == capi.INVALID_VALUE
+    assert capi.lib.abhsf_mlp_adam(None, None, None, None, 1, 1e-3, None) == capi.INVALID_VALUE
+    assert capi.lib.abhsf_last_error_string()
+
+
+def test_selector_option_defaults_and_struct():
+    o = capi.BuildOpts()
+    capi.lib.abhsf_build_opts_default(C.byref(o))
+    assert o.block_size == 64 and o.selector == capi.SELECTORS["minbss"] and o.selector_model is None
+    assert o.reserved == 0
