@@ -472,6 +472,31 @@ def cpu_reference_run(c, bytes_per_step: float, max_seconds: float, max_iters: i
             "ms_per_step": t * 1e3, "gflops": 2.0 * c.nnz / t / 1e9}
 
 
+def cpu_abhsf_run(c, bytes_per_step: float, max_seconds: float = 10.0, max_iters: int = 20):
+    """A second CPU reference point: the project's C restatement of the ABHSF
+    SpMV (the oracle's, the same format at s = 64) on all host threads
+    (OpenMP over block rows), same matrix, same unit."""
+    from oracle import oracle
+    t0 = time.time()
+    b = oracle.build(c.rows, c.cols, c.vals, c.m, c.n, 64)
+    build_s = time.time() - t0
+    x = np.random.default_rng(0).uniform(-1, 1, c.n)
+    y = np.zeros(c.m)
+    b.spmv_omp(x, y)  # warm-up
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max_iters and time.perf_counter() - t_start < max_seconds:
+        t1 = time.perf_counter()
+        b.spmv_omp(x, y)
+        times.append(time.perf_counter() - t1)
+    t = statistics.median(times)
+    cores = oracle.Built.threads()
+    b.close()
+    return {"value": bytes_per_step / t / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+            "ms_per_step": t * 1e3, "build_s": build_s,
+            "sample": f"{len(times)} full y += A x, the oracle's C ABHSF SpMV (s = 64) with OpenMP over block rows"}
+
+
 def build_format_stats(c):
     """Format statistics without a GPU (for the reference arm): the oracle
     builder gives the same bytes as the device format."""
@@ -588,13 +613,14 @@ def run_ours(args):
 
     peak, peak_src = hbm_peak()
     achieved = B / (t_mean * 1e-3) / 1e9
-    cpu = None
+    cpu = cpu_abhsf = None
     status = A.device_status()
     if status:
         raise RuntimeError(f"SpMV kernel reported device status {status}")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_run(c, B, max_seconds=20.0, max_iters=40)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu_abhsf = cpu_abhsf_run(c, B)
     if rank == 0:
         line = {
             "metric": METRIC, "value": aggregate_rate(B, t_max * 1e-3, world), "unit": UNIT, "n_gpus": world,
@@ -615,6 +641,7 @@ def run_ours(args):
                          "peak_source": peak_src,
                          "kernel": KERNELS[args.sum_order] + "<64>"},
             "cpu_baseline": cpu,
+            "cpu_abhsf": cpu_abhsf,
             "spmm": spmm,
             "lowprec": lowprec,
             "cg": cg_times,

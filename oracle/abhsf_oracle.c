@@ -9,6 +9,9 @@
 
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 /* ---------------------------------------------------------------- cost model */
 
@@ -487,55 +490,81 @@ static double value_at(const orc_matrix* a, int64_t i)
     }
 }
 
-void orc_spmv_abhsf(const orc_matrix* a, const double* x, double* y)
+/* y += A x over block row I: its tiles in column order, each tile's
+ * elements in stored order (row-major), so every row adds its products
+ * columns ascending. */
+static void spmv_block_row(const orc_matrix* a, int64_t I, const double* x, double* y)
 {
     const int s = a->s, lg = a->log2s;
-    for (int64_t I = 0; I < a->M; ++I) {
-        for (int64_t t = a->brow_ptr[I]; t < a->brow_ptr[I + 1]; ++t) {
-            const int64_t J = a->tile_col[t];
-            const int64_t z = a->tile_nnz[t];
-            const int64_t vo = a->tile_val_off[t];
-            const uint8_t* pay = a->idx + a->tile_idx_off[t];
-            const int64_t r0 = I * s, c0 = J * s;
-            switch (a->tile_scheme[t]) {
-            case ORC_COO:
-                for (int64_t p = 0; p < z; ++p) {
-                    uint16_t k;
-                    memcpy(&k, pay + 2 * p, 2);
-                    y[r0 + (k >> lg)] += value_at(a, vo + p) * x[c0 + (k & (s - 1))];
-                }
-                break;
-            case ORC_CSR: {
-                int64_t p = 0;
-                for (int r = 0; r < s; ++r) {
-                    uint16_t e;
-                    memcpy(&e, pay + 2 * r, 2);
-                    for (; p < e; ++p)
-                        y[r0 + r] += value_at(a, vo + p) * x[c0 + pay[2 * s + p]];
-                }
-                break;
+    for (int64_t t = a->brow_ptr[I]; t < a->brow_ptr[I + 1]; ++t) {
+        const int64_t J = a->tile_col[t];
+        const int64_t z = a->tile_nnz[t];
+        const int64_t vo = a->tile_val_off[t];
+        const uint8_t* pay = a->idx + a->tile_idx_off[t];
+        const int64_t r0 = I * s, c0 = J * s;
+        switch (a->tile_scheme[t]) {
+        case ORC_COO:
+            for (int64_t p = 0; p < z; ++p) {
+                uint16_t k;
+                memcpy(&k, pay + 2 * p, 2);
+                y[r0 + (k >> lg)] += value_at(a, vo + p) * x[c0 + (k & (s - 1))];
             }
-            case ORC_BITMAP: {
-                int64_t p = 0;
-                for (int64_t b = 0; b < (int64_t)s * s; ++b) {
-                    uint64_t w;
-                    memcpy(&w, pay + 8 * (b >> 6), 8);
-                    if ((w >> (b & 63)) & 1) {
-                        y[r0 + (b >> lg)] += value_at(a, vo + p) * x[c0 + (b & (s - 1))];
-                        p++;
-                    }
-                }
-                break;
+            break;
+        case ORC_CSR: {
+            int64_t p = 0;
+            for (int r = 0; r < s; ++r) {
+                uint16_t e;
+                memcpy(&e, pay + 2 * r, 2);
+                for (; p < e; ++p)
+                    y[r0 + r] += value_at(a, vo + p) * x[c0 + pay[2 * s + p]];
             }
-            default:
-                for (int64_t b = 0; b < (int64_t)s * s; ++b) {
-                    int64_t r = r0 + (b >> lg), c = c0 + (b & (s - 1));
-                    if (r < a->m && c < a->n)
-                        y[r] += value_at(a, vo + b) * x[c];
+            break;
+        }
+        case ORC_BITMAP: {
+            int64_t p = 0;
+            for (int64_t b = 0; b < (int64_t)s * s; ++b) {
+                uint64_t w;
+                memcpy(&w, pay + 8 * (b >> 6), 8);
+                if ((w >> (b & 63)) & 1) {
+                    y[r0 + (b >> lg)] += value_at(a, vo + p) * x[c0 + (b & (s - 1))];
+                    p++;
                 }
+            }
+            break;
+        }
+        default:
+            for (int64_t b = 0; b < (int64_t)s * s; ++b) {
+                int64_t r = r0 + (b >> lg), c = c0 + (b & (s - 1));
+                if (r < a->m && c < a->n)
+                    y[r] += value_at(a, vo + b) * x[c];
             }
         }
     }
+}
+
+void orc_spmv_abhsf(const orc_matrix* a, const double* x, double* y)
+{
+    for (int64_t I = 0; I < a->M; ++I)
+        spmv_block_row(a, I, x, y);
+}
+
+/* The same over the host's threads (OpenMP, block rows dealt dynamically):
+ * block rows write disjoint rows of y, so y is the serial one bit for bit.
+ * A CPU ABHSF SpMV to time beside the reference's CSR kernel. */
+void orc_spmv_abhsf_omp(const orc_matrix* a, const double* x, double* y)
+{
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t I = 0; I < a->M; ++I)
+        spmv_block_row(a, I, x, y);
+}
+
+int orc_omp_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
 }
 
 void orc_spmv_elements(const int64_t* rows, const int64_t* cols, const double* vals,

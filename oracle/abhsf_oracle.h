@@ -100,6 +100,9 @@ void orc_free(orc_matrix* a);
  * (dense), generalised to s x s and FP64).  Values of f32/bf16 matrices are
  * widened to double. */
 void orc_spmv_abhsf(const orc_matrix* a, const double* x, double* y);
+/* The same on all host threads (OpenMP over block rows), bit for bit. */
+void orc_spmv_abhsf_omp(const orc_matrix* a, const double* x, double* y);
+int orc_omp_threads(void);
 
 /* The reference's verification loop, spmv/unified/spmv.cpp:1195-1201 and
  * spmv/bottlenecks/spmv.cpp:307-313: y[row] += val * x[col] in element order. */

@@ -84,6 +84,10 @@ def lib() -> C.CDLL:
         L.orc_free.argtypes = [C.POINTER(OrcMatrix)]
         L.orc_spmv_abhsf.restype = None
         L.orc_spmv_abhsf.argtypes = [C.POINTER(OrcMatrix), _f64p, _f64p]
+        L.orc_spmv_abhsf_omp.restype = None
+        L.orc_spmv_abhsf_omp.argtypes = [C.POINTER(OrcMatrix), _f64p, _f64p]
+        L.orc_omp_threads.restype = C.c_int
+        L.orc_omp_threads.argtypes = []
         for name in ("orc_spmv_elements", "orc_abs_spmv_elements"):
             getattr(L, name).restype = None
             getattr(L, name).argtypes = [_i64p, _i64p, _f64p, C.c_int64, _f64p, _f64p]
@@ -188,6 +192,16 @@ class Built:
         x = np.ascontiguousarray(x, dtype=np.float64)
         assert y.dtype == np.float64 and y.flags.c_contiguous
         lib().orc_spmv_abhsf(self._ptr, _p(x, _f64p), _p(y, _f64p))
+
+    def spmv_omp(self, x: np.ndarray, y: np.ndarray) -> None:
+        """y += A x on all host threads (bitwise spmv's y)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert y.dtype == np.float64 and y.flags.c_contiguous
+        lib().orc_spmv_abhsf_omp(self._ptr, _p(x, _f64p), _p(y, _f64p))
+
+    @staticmethod
+    def threads() -> int:
+        return int(lib().orc_omp_threads())
 
     def close(self):
         if self._ptr is not None:

@@ -131,3 +131,19 @@ def test_bf16_conversion_rne():
         u = int(f32.view(np.uint32))
         want = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) & 0xFFFF
         assert int(b) == want, v
+
+
+@pytest.mark.parametrize("s", [16, 64, 256])
+def test_oracle_openmp_abhsf_spmv_equals_serial(s):
+    """The OpenMP ABHSF SpMV (a CPU baseline) gives the serial oracle's y bit
+    for bit: block rows write disjoint rows."""
+    for name in ("blocky64", "rand_real", "edge_ragged_empty_rows"):
+        coo = MATS[name]
+        b = oracle.build(coo.rows, coo.cols, coo.vals, coo.m, coo.n, s)
+        x = W.rhs(coo.n, 3)
+        y1 = W.rhs(coo.m, 4)
+        y2 = y1.copy()
+        b.spmv(x, y1)
+        b.spmv_omp(x, y2)
+        np.testing.assert_array_equal(y1, y2)
+    assert oracle.Built.threads() >= 1
