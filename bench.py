@@ -631,6 +631,7 @@ def run_ours(args):
                 "block_size": 64, "nnz": c.nnz, "tiles": st["tiles"], "tiles_per_scheme": st["tiles_per_scheme"],
                 "bytes_per_step": B, "format_bytes": st["format_bytes"],
                 "msmf_min_bytes_per_step": st["msmf_bits"][6] // 8 + 8 * c.n + 16 * c.m,
+                "csr_bytes_per_step": 12 * c.nnz + 4 * (c.m + 1) + 8 * c.n + 16 * c.m,
                 "l2": "between steps a 256 MiB buffer is written, then another 256 MiB read (dirty lines written back before the timed SpMV); working set 600 MB > 126 MB L2",
                 "gflops": 2.0 * c.nnz / (t_mean * 1e-3) / 1e9, "build_s": build_s,
                 "parallelism": f"replicas x{world}", "sum_order": args.sum_order,
