@@ -612,6 +612,15 @@ def run_ours(args):
     bstats = None if args.no_bstats or rank != 0 else time_bstats(c, dev)
 
     peak, peak_src = hbm_peak()
+    # every section's rate also as a fraction of the measured copy peak
+    for sec in (spmm or {}).values():
+        sec["frac_of_peak"] = sec["GB/s"] / peak
+    for key in ("f32", "bf16"):
+        if lowprec and key in lowprec:
+            lowprec[key]["frac_of_peak"] = lowprec[key]["GB/s"] / peak
+    if batched:
+        for key in ("batched", "one_by_one"):
+            batched[key]["frac_of_peak"] = batched[key]["GB/s"] / peak
     achieved = B / (t_mean * 1e-3) / 1e9
     cpu = cpu_abhsf = None
     status = A.device_status()
