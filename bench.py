@@ -307,6 +307,23 @@ def time_cg(dev, g=256, rtol=1e-10):
     b = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, lap.n)).to(dev)
     out = {"workload": f"3D 7-point Laplacian {g}^3 (n={lap.n}, nnz={lap.nnz}, diag 6, off -1), b U[-1,1] seed 1, "
                        f"x0 = 0, block size 64", "rtol": rtol}
+    # the solver's SpMV alone (working set > L2; CUDA events, 10 launches after 3)
+    xs = torch.rand(lap.n, dtype=torch.float64, device=dev)
+    ys = torch.zeros(lap.n, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        A64.spmv(xs, ys)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        A64.spmv(xs, ys)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 10
+    byts = int(A64.stats()["format_bytes"]) + 8 * lap.n + 16 * lap.n
+    peak, _ = hbm_peak()
+    out["spmv_f64"] = {"ms": t, "GB/s": byts / (t * 1e-3) / 1e9, "frac_of_peak": byts / (t * 1e-3) / 1e9 / peak,
+                       "bytes": byts}
+    del xs, ys
     from abhsf_b200 import selector as sel
     t0 = time.perf_counter()
     _, s64, T64 = sel.autotune(lap.rows, lap.cols, lap.vals, lap.m, lap.n, candidates=(32, 64), keep=True)
