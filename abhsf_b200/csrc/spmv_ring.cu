@@ -7,21 +7,26 @@
 // columns ascending, onto y[row], each product rounded before its add.  This
 // kernel keeps that order and so returns y bitwise equal to the reference's.
 //
-// A CTA is s / 32 consumer warps and one producer warp; consumer warp w owns
-// rows 32 w .. 32 w + 31 of every tile, one row per lane, and keeps the row's
-// accumulator in a register for the whole block row.  At build time the
-// non-empty block rows are dealt to the CTAs (longest processing time first,
-// by the bytes each block row moves) and every CTA gets its tiles as a list
-// of 32-byte descriptors, in block-row order.  The producer streams them
-// through a ring in shared memory several slots ahead of the consumers.  A
-// slot carries one tile, or a group of up to kGroupMax small tiles that are
-// contiguous in the format arrays: their descriptors, the y blocks of the
-// tiles that start a block row, one x block per tile (8- or 4-byte cp.async by
-// the producer lanes), and one bulk copy (cp.async.bulk) each for the group's
-// index payloads and values, all completing on the slot's mbarrier.  Every
-// wait on an mbarrier is bounded: a wait that runs out sets
-// ABHSF_DEVSTAT_WAIT_TIMEOUT in the matrix's status word, the CTA waits (again
-// bounded) for the copies it still has in flight, and returns.
+// A CTA is one producer warp and consumer teams (the layout, a template
+// parameter: one or two teams of s / 32 warps with one row per lane, or four
+// or two teams of one warp with s / 32 rows per lane).  A team keeps its
+// rows' accumulators in registers for a whole block row; teams take block
+// rows in turn.  At build time the non-empty block rows are dealt to the CTAs
+// (longest processing time first, by the bytes each block row moves), every
+// CTA gets its tiles as a list of 32-byte descriptors in block-row order, and
+// the launch variant (layout, x / y copy mode) is timed on the matrix.  The
+// producer streams the tiles through a ring in shared memory several slots
+// ahead of the consumers.  A slot carries one tile, or a group of up to
+// kGroupMax small tiles that are contiguous in the format arrays, ending with
+// the last block row it completes: their descriptors, the y blocks of the
+// tiles that start a block row, one x block per tile, and one bulk copy
+// (cp.async.bulk) each for the group's index payloads and values -- issued
+// first -- all completing on the slot's mbarrier.  x and y blocks travel as
+// bulk copies where whole, contiguous and aligned, else as 8- or 4-byte
+// cp.async by the producer lanes.  Every wait on an mbarrier is bounded: a
+// wait that runs out sets ABHSF_DEVSTAT_WAIT_TIMEOUT in the matrix's status
+// word, the CTA waits (again bounded) for the copies it still has in flight,
+// and returns.
 //
 // Summing a bitmap tile, a lane walks its row's bits in column order and adds
 // v * x, where the value sits at the row's first value (a warp scan of the
@@ -31,8 +36,10 @@
 // bank; its stored zeros are skipped (an exact identity for the sum).  A CSR
 // tile gives each lane its row's range in row_end.  A COO tile of up to 32
 // elements hands each element's product to its row's lane by warp shuffles,
-// in key order; a larger one first marks where each row's run of keys starts
-// and ends.  In every case a row's products are added in column order.
+// in key order; a larger one whose rows hold one element each finds a row's
+// element by a popcount over the occupied rows, and any other first marks
+// where each row's run of keys starts and ends.  In every case a row's
+// products are added in column order.
 //
 // With K right-hand sides (X and Y row-major, leading dimensions ldx / ldy)
 // a slot holds the tile's S x K block of X (and of Y at a block row's start),
