@@ -11,6 +11,7 @@ _EXPORTS = {
     "Unsupported": "capi",
     "AbhsfMatrix": "matrix", "AbhsfBatch": "matrix", "block_histogram": "matrix", "block_histograms_all": "matrix", "block_scheme_bits": "matrix",
     "block_select_scheme": "matrix", "mmf_line": "matrix", "cg": "matrix", "cg_mixed": "matrix",
+    "ShardedMatrix": "sharded",
 }
 
 __all__ = sorted(_EXPORTS)
