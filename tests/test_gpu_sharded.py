@@ -1,0 +1,42 @@
+"""The row-sharded SpMV on one GPU (a one-rank NCCL group): the gather and
+the local kernel give abhsf_spmv's y bit for bit.  More ranks need more GPUs
+than a run here has; their host logic is tested on gloo ranks."""
+import socket
+
+import numpy as np
+import pytest
+
+from abhsf_b200 import AbhsfMatrix
+from abhsf_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def test_one_rank_sharded_spmv_equals_spmv(gpu):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from abhsf_b200.sharded import ShardedMatrix
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        coo = W.random_blocky(3000, 2500, 64, 200, seed=9)
+        x = torch.from_numpy(W.rhs(coo.n, 1)).cuda()
+        y0 = torch.from_numpy(W.rhs(coo.m, 2)).cuda()
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+        want = y0.clone()
+        A.spmv(x, want)
+        S = ShardedMatrix(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+        assert (S.row0, S.row1, S.x0, S.x1) == (0, coo.m, 0, coo.n)
+        y = y0.clone()
+        S.spmv(x[S.x0:S.x1].contiguous(), y)
+        torch.cuda.synchronize()
+        assert torch.equal(y, want)
+        S.release()
+        A.release()
+    finally:
+        dist.destroy_process_group()
