@@ -70,6 +70,12 @@ class BuildOpts(C.Structure):
                 ("reserved", C.c_int32), ("selector_model", C.c_void_p)]
 
 
+class CooHost(C.Structure):
+    _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("nnz", C.c_int64), ("matrix_type", C.c_int32),
+                ("symmetry", C.c_int32), ("stored_triangle", C.c_int32), ("reserved", C.c_int32),
+                ("rows", C.POINTER(C.c_int64)), ("cols", C.POINTER(C.c_int64)), ("vals", C.POINTER(C.c_double))]
+
+
 class CgInfo(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("outer_iterations", C.c_int32), ("converged", C.c_int32),
                 ("reserved", C.c_int32), ("rel_residual", C.c_double)]
@@ -129,6 +135,8 @@ PROTOTYPES = {
     "abhsf_mlp_forward": (C.c_int, [_vp, _vp, _i32, _vp, _vp, _vp]),
     "abhsf_mlp_backward": (C.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp]),
     "abhsf_mlp_adam": (C.c_int, [_vp, _vp, _vp, _vp, _i32, C.c_float, _vp]),
+    "abhsf_read_mtx": (C.c_int, [C.c_char_p, _i32, C.POINTER(CooHost)]),
+    "abhsf_coo_host_free": (C.c_int, [C.POINTER(CooHost)]),
     "abhsf_block_scheme_bits": (C.c_uint64, [_i32, _i64, _i64, _i64, _i64]),
     "abhsf_block_select_scheme": (_i32, [_i64, _i64, _i64, _i64, _i32, _i32]),
 }

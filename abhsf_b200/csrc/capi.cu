@@ -1,5 +1,6 @@
 // capi.cu -- the extern "C" boundary declared in include/abhsf/abhsf_gpu.h.
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <string>
@@ -473,6 +474,29 @@ abhsf_status abhsf_mlp_adam(float* params, const float* grad, float* m, float* v
 {
     return guarded([&] {
         abhsf::mlp_adam(params, grad, m, v, step, lr, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+abhsf_status abhsf_read_mtx(const char* path, int32_t threads, abhsf_coo_host* out)
+{
+    return guarded([&] {
+        if (!out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "out must be non-NULL");
+        abhsf::read_mtx(path, threads, *out);
+    });
+}
+
+abhsf_status abhsf_coo_host_free(abhsf_coo_host* coo)
+{
+    return guarded([&] {
+        if (!coo)
+            return;
+        std::free(coo->rows);
+        std::free(coo->cols);
+        std::free(coo->vals);
+        coo->rows = coo->cols = nullptr;
+        coo->vals = nullptr;
+        coo->nnz = 0;
     });
 }
 

@@ -1,0 +1,251 @@
+// mtx.cu -- Matrix Market ingest on the host (the library's data loader).
+//
+// Reads a coordinate-format Matrix Market file the way the reference's
+// read_mtx_real_or_binary does (include/abhsf/utils/matrix_market_reader.h:146-200,
+// banner and size line through mmio's mm_read_banner / mm_read_mtx_crd_size):
+// real or pattern matrices (pattern values 1.0), 1-based indices made 0-based,
+// explicit zeros of a real matrix dropped, a symmetric / skew / hermitian
+// file's stored triangle kept as stored (no expansion) and rejected when both
+// triangles appear.  Values are converted by strtod, which rounds exactly as
+// the reference's fscanf("%lf") does.  Unlike the reference, indices outside
+// the declared m x n are an error here, and the entry lines are parsed by
+// several host threads at once (the file is read whole, split at line ends).
+#include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+
+namespace abhsf {
+namespace {
+
+std::string lower(std::string s)
+{
+    for (char& c : s)
+        c = (char)std::tolower((unsigned char)c);
+    return s;
+}
+
+// The next line of buf starting at pos (without the line end); pos moves past it.
+bool next_line(const std::string& buf, size_t& pos, std::string& line)
+{
+    if (pos >= buf.size())
+        return false;
+    size_t e = buf.find('\n', pos);
+    if (e == std::string::npos)
+        e = buf.size();
+    line.assign(buf, pos, e - pos);
+    if (!line.empty() && line.back() == '\r')
+        line.pop_back();
+    pos = e + 1;
+    return true;
+}
+
+struct chunk_out {
+    std::vector<int64_t> rows, cols;
+    std::vector<double> vals;
+    int64_t entries = 0, zeros = 0;
+    bool lower = false, upper = false, bad = false, range = false;
+};
+
+// Entries of buf[b, e) (whole lines), at most `limit` of them.
+void parse_chunk(const char* b, const char* e, bool pattern, int64_t m, int64_t n, int64_t limit, chunk_out& o)
+{
+    const char* p = b;
+    while (p < e && o.entries < limit) {
+        while (p < e && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n'))
+            ++p;
+        if (p >= e)
+            break;
+        char* q = nullptr;
+        errno = 0;
+        const unsigned long long r = std::strtoull(p, &q, 10);
+        if (q == p || errno) {
+            o.bad = true;
+            return;
+        }
+        p = q;
+        const unsigned long long c = std::strtoull(p, &q, 10);
+        if (q == p || errno) {
+            o.bad = true;
+            return;
+        }
+        p = q;
+        double v = 1.0;
+        if (!pattern) {
+            v = std::strtod(p, &q);
+            if (q == p) {
+                o.bad = true;
+                return;
+            }
+            p = q;
+        }
+        while (p < e && *p != '\n')  // the rest of the line (a complex part, a comment) is not read
+            ++p;
+        ++o.entries;
+        if (r < 1 || c < 1 || (int64_t)r > m || (int64_t)c > n) {
+            o.range = true;
+            return;
+        }
+        const int64_t i = (int64_t)r - 1, j = (int64_t)c - 1;
+        if (i > j)
+            o.lower = true;
+        if (j > i)
+            o.upper = true;
+        if (!pattern && v == 0.0) {
+            ++o.zeros;
+            continue;
+        }
+        o.rows.push_back(i);
+        o.cols.push_back(j);
+        o.vals.push_back(v);
+    }
+}
+
+}  // namespace
+
+void read_mtx(const char* path, int threads, abhsf_coo_host& out)
+{
+    out = abhsf_coo_host{};
+    if (!path)
+        fail(ABHSF_ERROR_INVALID_VALUE, "path must be non-NULL");
+    FILE* f = std::fopen(path, "rb");
+    if (!f)
+        fail(ABHSF_ERROR_INVALID_VALUE, std::string("cannot open input file: ") + path);
+    std::string buf;
+    {
+        char tmp[1 << 16];
+        size_t k;
+        while ((k = std::fread(tmp, 1, sizeof(tmp), f)) > 0)
+            buf.append(tmp, k);
+        std::fclose(f);
+    }
+    size_t pos = 0;
+    std::string line;
+    // banner: %%MatrixMarket matrix coordinate <field> <symmetry>
+    if (!next_line(buf, pos, line))
+        fail(ABHSF_ERROR_INVALID_VALUE, "could not process Matrix Market banner");
+    char w[5][64] = {};
+    if (std::sscanf(line.c_str(), "%63s %63s %63s %63s %63s", w[0], w[1], w[2], w[3], w[4]) != 5 ||
+        std::string(w[0]) != "%%MatrixMarket")
+        fail(ABHSF_ERROR_INVALID_VALUE, "could not process Matrix Market banner");
+    if (lower(w[1]) != "matrix" || lower(w[2]) != "coordinate")
+        fail(ABHSF_ERROR_UNSUPPORTED, "only sparse matrices in coordinate format are supported");
+    const std::string field = lower(w[3]), sym = lower(w[4]);
+    int type;
+    if (field == "pattern")
+        type = ABHSF_MATRIX_BINARY;
+    else if (field == "real")
+        type = ABHSF_MATRIX_REAL;
+    else if (field == "integer" || field == "complex")
+        fail(ABHSF_ERROR_UNSUPPORTED, "only real and pattern matrices are read (read_mtx_real_or_binary)");
+    else
+        fail(ABHSF_ERROR_INVALID_VALUE, "unsupported matrix type");
+    int symmetry;
+    if (sym == "general")
+        symmetry = ABHSF_SYMMETRY_GENERAL;
+    else if (sym == "symmetric")
+        symmetry = ABHSF_SYMMETRY_SYMMETRIC;
+    else if (sym == "skew-symmetric")
+        symmetry = ABHSF_SYMMETRY_SKEW;
+    else if (sym == "hermitian")
+        symmetry = ABHSF_SYMMETRY_HERMITIAN;
+    else
+        fail(ABHSF_ERROR_INVALID_VALUE, "unsupported type of matrix symmetry");
+    // comments, then the size line
+    long long m = 0, n = 0, nnz = 0;
+    for (;;) {
+        if (!next_line(buf, pos, line))
+            fail(ABHSF_ERROR_INVALID_VALUE, "could not retrieve matrix sizes");
+        if (!line.empty() && line[0] == '%')
+            continue;
+        if (line.find_first_not_of(" \t") == std::string::npos)
+            continue;
+        if (std::sscanf(line.c_str(), "%lld %lld %lld", &m, &n, &nnz) != 3 || m <= 0 || n <= 0 || nnz < 0)
+            fail(ABHSF_ERROR_INVALID_VALUE, "could not retrieve matrix sizes");
+        break;
+    }
+    // entry lines: split the rest at line ends over the threads
+    const size_t rest = pos <= buf.size() ? buf.size() - pos : 0;
+    int T = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    T = (int)std::max<size_t>(1, std::min<size_t>((size_t)T, rest / (1 << 20) + 1));
+    std::vector<size_t> cut(T + 1, pos);
+    cut[T] = buf.size();
+    for (int t = 1; t < T; ++t) {
+        size_t c = pos + rest * t / T;
+        c = std::max(c, cut[t - 1]);
+        const size_t e = buf.find('\n', c);
+        cut[t] = e == std::string::npos ? buf.size() : e + 1;
+    }
+    std::vector<chunk_out> parts(T);
+    const bool pattern = type == ABHSF_MATRIX_BINARY;
+    {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < T; ++t)
+            pool.emplace_back([&, t] {
+                parse_chunk(buf.data() + cut[t], buf.data() + cut[t + 1], pattern, m, n, (int64_t)nnz, parts[t]);
+            });
+        for (auto& th : pool)
+            th.join();
+    }
+    // the first nnz entries in file order, as the reference reads exactly nnz
+    // (lines after them are not looked at)
+    int64_t left = nnz, kept = 0;
+    bool L = false, U = false;
+    std::vector<int64_t> take;
+    for (int t = 0; t < T && left > 0; ++t) {
+        if (parts[t].entries > left || (parts[t].bad && parts[t].entries >= left)) {
+            chunk_out again;  // this chunk holds the nnz-th entry: read only up to it
+            parse_chunk(buf.data() + cut[t], buf.data() + cut[t + 1], pattern, m, n, left, again);
+            parts[t] = std::move(again);
+        }
+        const chunk_out& c = parts[t];
+        if (c.range)
+            fail(ABHSF_ERROR_INDEX_OUT_OF_RANGE, "an element lies outside the declared m x n");
+        if (c.bad)
+            fail(ABHSF_ERROR_INVALID_VALUE, "could not read matrix element");
+        take.push_back((int64_t)c.rows.size());
+        L = L || c.lower;
+        U = U || c.upper;
+        left -= c.entries;
+    }
+    if (left > 0)
+        fail(ABHSF_ERROR_INVALID_VALUE, "could not read matrix element (fewer entries than declared)");
+    const int used = (int)take.size();
+    if (symmetry != ABHSF_SYMMETRY_GENERAL && L && U)
+        fail(ABHSF_ERROR_INVALID_VALUE, "elements from both L and U parts stored for not-unsymmetric matrix");
+    for (int64_t k : take)
+        kept += k;
+    out.m = m;
+    out.n = n;
+    out.nnz = kept;
+    out.matrix_type = type;
+    out.symmetry = symmetry;
+    out.stored_triangle = symmetry == ABHSF_SYMMETRY_GENERAL ? 0 : (L ? 1 : 2);
+    out.rows = static_cast<int64_t*>(std::malloc(std::max<int64_t>(kept, 1) * sizeof(int64_t)));
+    out.cols = static_cast<int64_t*>(std::malloc(std::max<int64_t>(kept, 1) * sizeof(int64_t)));
+    out.vals = static_cast<double*>(std::malloc(std::max<int64_t>(kept, 1) * sizeof(double)));
+    if (!out.rows || !out.cols || !out.vals) {
+        std::free(out.rows);
+        std::free(out.cols);
+        std::free(out.vals);
+        out = abhsf_coo_host{};
+        fail(ABHSF_ERROR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    int64_t o = 0;
+    for (int t = 0; t < used; ++t) {
+        const chunk_out& c = parts[t];
+        std::copy(c.rows.begin(), c.rows.begin() + take[t], out.rows + o);
+        std::copy(c.cols.begin(), c.cols.begin() + take[t], out.cols + o);
+        std::copy(c.vals.begin(), c.vals.begin() + take[t], out.vals + o);
+        o += take[t];
+    }
+}
+
+}  // namespace abhsf

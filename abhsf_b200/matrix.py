@@ -17,6 +17,7 @@ the reference's ``std::runtime_error``.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -286,6 +287,27 @@ def block_histograms_all(rows, cols, m: int, n: int, stream=None) -> dict[str, d
         assert sum(out[f"{r}x{s}"].values()) == blocks[p]
         off += r * s + 1
     return out
+
+
+def read_mtx(path: str, threads: int = 0):
+    """A Matrix Market coordinate file as the reference's read_mtx_real_or_binary
+    reads it (include/abhsf/utils/matrix_market_reader.h:146-200), parsed on
+    the host by the library: (rows, cols, vals, m, n, info) with 0-based int64
+    indices, float64 values, info = {"matrix_type", "symmetry",
+    "stored_triangle"}."""
+    c = capi.CooHost()
+    capi.check(capi.lib.abhsf_read_mtx(os.fsencode(path), int(threads), C.byref(c)))
+    try:
+        k = int(c.nnz)
+        rows = np.ctypeslib.as_array(c.rows, shape=(k,)).copy() if k else np.zeros(0, np.int64)
+        cols = np.ctypeslib.as_array(c.cols, shape=(k,)).copy() if k else np.zeros(0, np.int64)
+        vals = np.ctypeslib.as_array(c.vals, shape=(k,)).copy() if k else np.zeros(0, np.float64)
+        info = {"matrix_type": {0: "binary", 2: "real"}[int(c.matrix_type)],
+                "symmetry": ("symmetric", "hermitian", "skew", "general")[int(c.symmetry)],
+                "stored_triangle": ("", "lower", "upper")[int(c.stored_triangle)]}
+        return rows, cols, vals, int(c.m), int(c.n), info
+    finally:
+        capi.lib.abhsf_coo_host_free(C.byref(c))
 
 
 def mmf_line(m: int, n: int, nnz: int, matrix_type: str | int, r: int, s: int, hist: dict[int, int]):

@@ -142,6 +142,28 @@ typedef struct abhsf_build_opts {
     const float* selector_model; /* host, ABHSF_MLP_PARAMS floats; NULL = the model built into the library */
 } abhsf_build_opts;
 
+/* include/abhsf/utils/matrix_properties.h:17-23 (kept apart from abhsf_matrix_type) */
+typedef enum abhsf_symmetry {
+    ABHSF_SYMMETRY_SYMMETRIC = 0,
+    ABHSF_SYMMETRY_HERMITIAN = 1,
+    ABHSF_SYMMETRY_SKEW = 2,
+    ABHSF_SYMMETRY_GENERAL = 3
+} abhsf_symmetry;
+
+/* A matrix read from a file into host memory (abhsf_read_mtx): 0-based COO
+ * arrays of nnz elements, allocated by the library, freed by
+ * abhsf_coo_host_free. */
+typedef struct abhsf_coo_host {
+    int64_t m, n, nnz;
+    int32_t matrix_type;     /* ABHSF_MATRIX_REAL or ABHSF_MATRIX_BINARY (values 1.0) */
+    int32_t symmetry;        /* abhsf_symmetry of the file */
+    int32_t stored_triangle; /* symmetric files: 1 lower, 2 upper (the part stored, not expanded); else 0 */
+    int32_t reserved;
+    int64_t* rows;
+    int64_t* cols;
+    double* vals;
+} abhsf_coo_host;
+
 typedef struct abhsf_matrix abhsf_matrix;
 typedef struct abhsf_batch abhsf_batch;
 
@@ -390,6 +412,19 @@ ABHSF_API abhsf_status abhsf_mlp_backward(const float* params, const float* x, c
                                           float* loss, abhsf_stream_t stream);
 ABHSF_API abhsf_status abhsf_mlp_adam(float* params, const float* grad, float* m, float* v, int32_t step, float lr,
                                       abhsf_stream_t stream);
+
+/* Reads a Matrix Market coordinate file as read_mtx_real_or_binary does
+ * (include/abhsf/utils/matrix_market_reader.h:146-200): real or pattern
+ * (values 1.0), indices made 0-based, explicit zeros of a real matrix
+ * dropped, a symmetric / skew / hermitian file's stored triangle kept as
+ * stored (ABHSF_ERROR_INVALID_VALUE when both triangles appear), the first nnz
+ * entries read.  Integer and complex files are ABHSF_ERROR_UNSUPPORTED (the
+ * reference reader throws for them); indices outside m x n are
+ * ABHSF_ERROR_INDEX_OUT_OF_RANGE (the reference does not check).  The entry
+ * lines are parsed by `threads` host threads (0: all).  The arrays go to
+ * abhsf_build as they are. */
+ABHSF_API abhsf_status abhsf_read_mtx(const char* path, int32_t threads, abhsf_coo_host* out);
+ABHSF_API abhsf_status abhsf_coo_host_free(abhsf_coo_host* coo);
 
 /* Waits for the work queued on stream, then returns the matrix's device
  * status word (ABHSF_DEVSTAT_* bits; 0 = every SpMV so far completed) and,

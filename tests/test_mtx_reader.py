@@ -1,0 +1,69 @@
+"""Matrix Market ingest (abhsf_read_mtx, host code of the library) against
+what the reference's own reader, read_mtx_real_or_binary, read from the same
+files (tests/golden/mtx_ref.npz, written by tests/golden/make_mtx_golden.py
+with the reference reader compiled from its sources)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from abhsf_b200 import capi
+from abhsf_b200 import matrix as mx
+
+REF = np.load(os.path.join(GOLDEN, "mtx_ref.npz"))
+NAMES = sorted({k.split("__")[0] for k in REF.files})
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("threads", [1, 4])
+def test_reader_matches_reference_reader(name, threads):
+    rows, cols, vals, m, n, info = mx.read_mtx(os.path.join(GOLDEN, "mtx", name + ".mtx"), threads)
+    assert [m, n] == REF[name + "__shape"].tolist()
+    np.testing.assert_array_equal(rows, REF[name + "__rows"])
+    np.testing.assert_array_equal(cols, REF[name + "__cols"])
+    np.testing.assert_array_equal(vals.view(np.uint64), REF[name + "__vals"].view(np.uint64))  # bit for bit
+    if "symmetric" in name:
+        assert info["symmetry"] == "symmetric" and info["stored_triangle"] in ("lower", "upper")
+    if "pattern" in name:
+        assert info["matrix_type"] == "binary" and np.all(vals == 1.0)
+
+
+def test_many_threads_read_a_large_file_in_order(tmp_path):
+    rng = np.random.default_rng(3)
+    m, n, k = 20000, 30000, 400000
+    r = rng.integers(1, m + 1, k)
+    c = rng.integers(1, n + 1, k)
+    v = rng.standard_normal(k)
+    p = tmp_path / "big.mtx"
+    with open(p, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate real general\n{m} {n} {k}\n")
+        f.write("\n".join(f"{a} {b} {x:.17g}" for a, b, x in zip(r, c, v)) + "\n")
+    one = mx.read_mtx(str(p), 1)
+    many = mx.read_mtx(str(p), 8)
+    for a, b in zip(one[:3], many[:3]):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(one[0], r - 1)
+    np.testing.assert_array_equal(one[1], c - 1)
+    np.testing.assert_array_equal(one[2], v)
+
+
+@pytest.mark.parametrize("text,exc", [
+    ("%%MatrixMarket matrix coordinate real symmetric\n3 3 2\n2 1 1\n1 2 1\n", capi.InvalidValue),  # both triangles
+    ("%%MatrixMarket matrix coordinate integer general\n2 2 1\n1 1 3\n", capi.Unsupported),
+    ("%%MatrixMarket matrix array real general\n2 2\n1\n2\n3\n4\n", capi.Unsupported),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1\n", capi.IndexOutOfRange),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 3\n1 1 1\n2 2 2\n", capi.InvalidValue),  # too few
+    ("%%MatrixMarket matrix coordinate real general\n2 2 1\n1 x 1\n", capi.InvalidValue),
+    ("not a banner\n", capi.InvalidValue),
+])
+def test_reader_errors(tmp_path, text, exc):
+    p = tmp_path / "bad.mtx"
+    p.write_text(text)
+    with pytest.raises(exc):
+        mx.read_mtx(str(p))
+
+
+def test_missing_file():
+    with pytest.raises(capi.InvalidValue):
+        mx.read_mtx("/nonexistent/file.mtx")
