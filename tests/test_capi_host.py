@@ -130,3 +130,20 @@ def test_selector_option_defaults_and_struct():
     capi.lib.abhsf_build_opts_default(C.byref(o))
     assert o.block_size == 64 and o.selector == capi.SELECTORS["minbss"] and o.selector_model is None
     assert o.reserved == 0
+
+
+def test_cost_model_exhaustive_small_blocks():
+    """Every (r, s) with r, s <= 16 and every block nonzero count 1 .. r*s:
+    the library's scheme costs and choices equal the oracle's restatement of
+    include/abhsf/msmf.h:9-63, for f64 and f32 widths, with and without CSR."""
+    for r in (2, 4, 8, 16):
+        for s in (2, 4, 8, 16):
+            for z in range(1, r * s + 1):
+                for bits in (64, 32):
+                    for sch in range(4):
+                        assert mx.block_scheme_bits(sch, r, s, z, bits) == oracle.block_bits(sch, r, s, z, bits)
+                    for binary in (False, True):
+                        for allow in (False, True):
+                            got = mx.block_select_scheme(r, s, z, bits, binary, allow)
+                            assert capi.SCHEME_NAMES.index(got) == oracle.select_scheme(r, s, z, bits, binary,
+                                                                                        allow), (r, s, z)

@@ -152,6 +152,8 @@ def test_all_block_sizes_equal_per_size_histograms(gpu):
     coo = W.tiled_mixture(n=65536 + 37, p=1e-3, seed=5)
     for rows, cols in ((coo.rows, coo.cols), (torch.from_numpy(coo.rows).cuda(), torch.from_numpy(coo.cols).cuda())):
         got = block_histograms_all(rows, cols, coo.m, coo.n)
+        for rs, h in got.items():  # conservation, block_statistics/block_stats.cpp:165-168
+            assert sum(z * c for z, c in h.items()) == coo.nnz, rs
         for rs in ("2x2", "4x256", "64x64", "256x2", "256x256", "128x32"):
             r, s = (int(t) for t in rs.split("x"))
             assert got[rs] == block_histogram(coo.rows, coo.cols, coo.m, coo.n, r, s), rs
