@@ -40,3 +40,40 @@ def test_one_rank_sharded_spmv_equals_spmv(gpu):
         A.release()
     finally:
         dist.destroy_process_group()
+
+
+def test_one_rank_sharded_cg_matches_cg(gpu):
+    """The sharded CG on a one-rank NCCL group (the library's SpMV on the
+    rank's rows, the scalars all-reduced) solves the 2D Laplacian like
+    abhsf_cg: both converge to rtol, to the same solution."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from abhsf_b200 import cg
+    from abhsf_b200.sharded import ShardedMatrix
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        coo = W.laplacian_2d(64)
+        b = torch.from_numpy(W.rhs(coo.n, 5)).cuda()
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+        x1 = torch.zeros_like(b)
+        want = cg(A, b, x1, rtol=1e-10, max_iters=5000)
+        S = ShardedMatrix(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+        x2 = torch.zeros_like(b)
+        got = S.cg(b[S.row0:S.row1], x2, rtol=1e-10, max_iters=5000)
+        torch.cuda.synchronize()
+        assert want["converged"] and got["converged"] and got["rel_residual"] <= 1e-10
+        # the dot products round differently (one all-reduced torch.dot against the
+        # library's block partials), so the trajectories part slightly
+        assert abs(got["iterations"] - want["iterations"]) <= max(3, want["iterations"] // 50)
+        # both lie within kappa * rtol (kappa ~ 1.7e3 at g = 64) of the exact solution
+        assert torch.linalg.norm(x2 - x1) <= 1e-6 * torch.linalg.norm(x1)
+        S.release()
+        A.release()
+    finally:
+        dist.destroy_process_group()

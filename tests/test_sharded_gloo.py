@@ -81,3 +81,98 @@ def test_two_gloo_ranks_compose_the_full_product():
     y = np.concatenate([r[4] for r in res])
     assert res[0][1] == 0 and res[0][2] == res[1][1] and res[1][2] == coo.m
     np.testing.assert_array_equal(y, want)  # row sums never cross ranks: bitwise the one-GPU order
+
+
+def test_partition_gives_empty_ranges_past_the_last_block_row():
+    assert sharded.partition_block_rows(np.arange(50), 50, 64, 2) == [(0, 50), (50, 50)]
+    parts = sharded.partition_block_rows(np.arange(200) % 130, 130, 64, 4)
+    assert parts[0][0] == 0 and parts[-1][1] == 130
+    for a0, a1 in parts:
+        assert 0 <= a0 <= a1 <= 130
+    for (a0, a1), (b0, b1) in zip(parts, parts[1:]):
+        assert a1 == b0
+
+
+def _cg_ref(coo, b, rtol, max_iters):
+    """One-process CG with the sharded solver's recurrences (numpy, f64)."""
+    from oracle import oracle
+
+    def A(v):
+        return oracle.spmv_elements(coo.rows, coo.cols, coo.vals, v, np.zeros(coo.m))
+    x = np.zeros(coo.n)
+    bb = float(b @ b)
+    r = b - A(x)
+    p = r.copy()
+    rr = float(r @ r)
+    it = 0
+    while rr > rtol * rtol * bb and it < max_iters:
+        q = A(p)
+        alpha = rr / float(p @ q)
+        x += alpha * p
+        r -= alpha * q
+        rr_new = float(r @ r)
+        p = r + (rr_new / rr) * p
+        rr = rr_new
+        it += 1
+    return x, it
+
+
+def _cg_rank_main(rank, world, port, g, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from oracle import oracle
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        coo = W.laplacian_2d(g)
+        b = W.rhs(coo.n, 5)
+        ranges = sharded.partition_block_rows(coo.rows, coo.m, 64, world)
+        r0, r1 = ranges[rank]
+        lr, lc, lv = sharded.local_elements(coo.rows, coo.cols, coo.vals, r0, r1)
+
+        def local_spmv(v, q):  # the oracle's product on this rank's rows (the checker)
+            q.copy_(torch.from_numpy(oracle.spmv_elements(lr, lc, lv, v.numpy(), q.numpy().copy())))
+        xl = torch.zeros(r1 - r0, dtype=torch.float64)
+        info = sharded.cg(local_spmv, torch.from_numpy(b[r0:r1].copy()), xl, ranges, rtol=1e-10, max_iters=2000)
+        full = sharded.gather_ranges(xl, ranges).numpy()
+        out.put((rank, r0, r1, info, xl.numpy().copy(), full))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,g", [(3, 24), (2, 7)])
+def test_gloo_ranks_sharded_cg_converges_like_one_process(world, g):
+    """Rows, b and x split by block rows over the ranks (g = 7: 49 rows, one
+    block row, so rank 1 owns nothing and still takes part in every
+    exchange); the solution, residual and iteration count agree with a
+    one-process CG of the same recurrences."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_cg_rank_main, args=(r, world, port, g, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=180) for _ in procs), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    coo = W.laplacian_2d(g)
+    b = W.rhs(coo.n, 5)
+    x_ref, it_ref = _cg_ref(coo, b, 1e-10, 2000)
+    x = np.concatenate([r[4] for r in res])
+    assert x.size == coo.n
+    for r in res:
+        np.testing.assert_array_equal(r[5], x)  # every rank gathered the same full vector
+        assert r[3]["converged"] and r[3]["rel_residual"] <= 1e-10
+        assert r[3]["iterations"] == res[0][3]["iterations"]
+    assert abs(res[0][3]["iterations"] - it_ref) <= 2
+    dense = np.zeros((coo.n, coo.n))
+    dense[coo.rows, coo.cols] = coo.vals
+    exact = np.linalg.solve(dense, b)
+    assert np.linalg.norm(x - exact) <= 1e-7 * np.linalg.norm(exact)
+    assert np.linalg.norm(x - x_ref) <= 1e-7 * np.linalg.norm(x_ref)
+    if g == 7:
+        assert res[1][1] == res[1][2] == coo.m  # the empty rank
