@@ -136,6 +136,8 @@ PROTOTYPES = {
     "abhsf_mlp_backward": (C.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp]),
     "abhsf_mlp_adam": (C.c_int, [_vp, _vp, _vp, _vp, _i32, C.c_float, _vp]),
     "abhsf_read_mtx": (C.c_int, [C.c_char_p, _i32, C.POINTER(CooHost)]),
+    "abhsf_read_mm": (C.c_int, [C.c_char_p, C.POINTER(CooHost)]),
+    "abhsf_write_mm": (C.c_int, [C.c_char_p, C.POINTER(CooHost)]),
     "abhsf_coo_host_free": (C.c_int, [C.POINTER(CooHost)]),
     "abhsf_block_scheme_bits": (C.c_uint64, [_i32, _i64, _i64, _i64, _i64]),
     "abhsf_block_select_scheme": (_i32, [_i64, _i64, _i64, _i64, _i32, _i32]),

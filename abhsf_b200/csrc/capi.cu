@@ -486,6 +486,24 @@ abhsf_status abhsf_read_mtx(const char* path, int32_t threads, abhsf_coo_host* o
     });
 }
 
+abhsf_status abhsf_read_mm(const char* path, abhsf_coo_host* out)
+{
+    return guarded([&] {
+        if (!out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "out must be non-NULL");
+        abhsf::read_mm(path, *out);
+    });
+}
+
+abhsf_status abhsf_write_mm(const char* path, const abhsf_coo_host* coo)
+{
+    return guarded([&] {
+        if (!coo)
+            fail(ABHSF_ERROR_INVALID_VALUE, "coo must be non-NULL");
+        abhsf::write_mm(path, *coo);
+    });
+}
+
 abhsf_status abhsf_coo_host_free(abhsf_coo_host* coo)
 {
     return guarded([&] {

@@ -10,6 +10,8 @@ namespace abhsf {
 
 // Matrix Market ingest on the host (mtx.cu).
 void read_mtx(const char* path, int threads, abhsf_coo_host& out);
+void read_mm(const char* path, abhsf_coo_host& out);
+void write_mm(const char* path, const abhsf_coo_host& a);
 
 void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, int64_t nnz, int64_t m, int64_t n,
                   const abhsf_build_opts& o, cudaStream_t st, abhsf_matrix& a);

@@ -248,4 +248,162 @@ void read_mtx(const char* path, int threads, abhsf_coo_host& out)
     }
 }
 
+// ---------------------------------------------------------------- .mm binary
+// The reference's binary matrix file, written by utils/mtx2mm/mtx2mm.cpp:102-135
+// (and read back by the commented-out read_mm of preprocessing/test.cpp:194-235):
+// five u64 words m, n, nnz, type (matrix_type_t numbering: 0 pattern, 1 integer,
+// 2 real, 3 complex) and a symmetry flag (mtx2mm's bool `hermit`), then u32
+// rows[nnz] and u32 cols[nnz] (0-based), then the values by type: f64[nnz] for
+// real, none for pattern.  The flag is written here as 0 for a general matrix and
+// 1 / 2 / 3 for symmetric / hermitian / skew, so a reader that takes it as a
+// bool (the reference) sees "not general" for all three, and a 1 written by
+// mtx2mm reads as symmetric.
+
+namespace {
+
+struct file_closer {
+    FILE* f;
+    ~file_closer()
+    {
+        if (f)
+            std::fclose(f);
+    }
+};
+
+constexpr uint64_t kMmHeaderWords = 5;
+
+void set_triangle(abhsf_coo_host& o)
+{
+    bool L = false, U = false;
+    for (int64_t k = 0; k < o.nnz; ++k) {
+        L = L || o.rows[k] > o.cols[k];
+        U = U || o.cols[k] > o.rows[k];
+    }
+    if (o.symmetry != ABHSF_SYMMETRY_GENERAL && L && U)
+        fail(ABHSF_ERROR_INVALID_VALUE, "elements from both L and U parts stored for not-unsymmetric matrix");
+    o.stored_triangle = o.symmetry == ABHSF_SYMMETRY_GENERAL ? 0 : (L ? 1 : 2);
+}
+
+}  // namespace
+
+void read_mm(const char* path, abhsf_coo_host& out)
+{
+    out = abhsf_coo_host{};
+    if (!path)
+        fail(ABHSF_ERROR_INVALID_VALUE, "path must be non-NULL");
+    file_closer fc{std::fopen(path, "rb")};
+    if (!fc.f)
+        fail(ABHSF_ERROR_INVALID_VALUE, std::string("cannot open input file: ") + path);
+    uint64_t h[kMmHeaderWords];
+    if (std::fread(h, sizeof(uint64_t), kMmHeaderWords, fc.f) != kMmHeaderWords)
+        fail(ABHSF_ERROR_INVALID_VALUE, "could not read the .mm header");
+    const uint64_t m = h[0], n = h[1], nnz = h[2], type = h[3], flag = h[4];
+    if (type == ABHSF_MATRIX_INTEGER || type == ABHSF_MATRIX_COMPLEX)
+        fail(ABHSF_ERROR_UNSUPPORTED, "only real and pattern matrices are read (read_mtx_real_or_binary)");
+    if (type != ABHSF_MATRIX_REAL && type != ABHSF_MATRIX_BINARY)
+        fail(ABHSF_ERROR_INVALID_VALUE, "unsupported matrix type");
+    if (flag > 3)
+        fail(ABHSF_ERROR_INVALID_VALUE, "unsupported type of matrix symmetry");
+    if (m < 1 || n < 1 || m > (uint64_t(1) << 32) || n > (uint64_t(1) << 32))
+        fail(ABHSF_ERROR_INVALID_VALUE, "matrix sizes out of the .mm range (1 .. 2^32)");
+    // the file holds exactly the arrays the header announces
+    const uint64_t per = 8 + (type == ABHSF_MATRIX_REAL ? 8 : 0);
+    if (std::fseek(fc.f, 0, SEEK_END) != 0)
+        fail(ABHSF_ERROR_INVALID_VALUE, "cannot seek in the .mm file");
+    const long size = std::ftell(fc.f);
+    if (size < 0 || nnz > (uint64_t(size) / per) || uint64_t(size) != 8 * kMmHeaderWords + nnz * per)
+        fail(ABHSF_ERROR_INVALID_VALUE, "the .mm file size does not match its header");
+    std::fseek(fc.f, long(8 * kMmHeaderWords), SEEK_SET);
+    std::vector<uint32_t> r32(nnz), c32(nnz);
+    std::vector<double> v(type == ABHSF_MATRIX_REAL ? nnz : 0);
+    if (std::fread(r32.data(), 4, nnz, fc.f) != nnz || std::fread(c32.data(), 4, nnz, fc.f) != nnz ||
+        std::fread(v.data(), 8, v.size(), fc.f) != v.size())
+        fail(ABHSF_ERROR_INVALID_VALUE, "could not read matrix element");
+    // explicit zeros of a real matrix are dropped, as read_mtx_real_or_binary
+    // drops them from the text file the .mm was made from
+    int64_t kept = 0;
+    for (uint64_t k = 0; k < nnz; ++k) {
+        if (r32[k] >= m || c32[k] >= n)
+            fail(ABHSF_ERROR_INDEX_OUT_OF_RANGE, "an element lies outside the declared m x n");
+        kept += type == ABHSF_MATRIX_BINARY || v[k] != 0.0;
+    }
+    abhsf_coo_host o{};
+    o.m = int64_t(m);
+    o.n = int64_t(n);
+    o.matrix_type = int32_t(type);
+    o.symmetry = flag == 0 ? ABHSF_SYMMETRY_GENERAL
+                           : (flag == 1 ? ABHSF_SYMMETRY_SYMMETRIC
+                                        : (flag == 2 ? ABHSF_SYMMETRY_HERMITIAN : ABHSF_SYMMETRY_SKEW));
+    o.rows = static_cast<int64_t*>(std::malloc(std::max<int64_t>(kept, 1) * sizeof(int64_t)));
+    o.cols = static_cast<int64_t*>(std::malloc(std::max<int64_t>(kept, 1) * sizeof(int64_t)));
+    o.vals = static_cast<double*>(std::malloc(std::max<int64_t>(kept, 1) * sizeof(double)));
+    if (!o.rows || !o.cols || !o.vals) {
+        std::free(o.rows);
+        std::free(o.cols);
+        std::free(o.vals);
+        fail(ABHSF_ERROR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    int64_t j = 0;
+    for (uint64_t k = 0; k < nnz; ++k) {
+        const double val = type == ABHSF_MATRIX_BINARY ? 1.0 : v[k];
+        if (val == 0.0)
+            continue;
+        o.rows[j] = r32[k];
+        o.cols[j] = c32[k];
+        o.vals[j] = val;
+        ++j;
+    }
+    o.nnz = kept;
+    try {
+        set_triangle(o);
+    } catch (...) {
+        std::free(o.rows);
+        std::free(o.cols);
+        std::free(o.vals);
+        throw;
+    }
+    out = o;
+}
+
+void write_mm(const char* path, const abhsf_coo_host& a)
+{
+    if (!path)
+        fail(ABHSF_ERROR_INVALID_VALUE, "path must be non-NULL");
+    if (a.matrix_type != ABHSF_MATRIX_REAL && a.matrix_type != ABHSF_MATRIX_BINARY)
+        fail(ABHSF_ERROR_UNSUPPORTED, "only real and pattern matrices are written");
+    if (a.symmetry < ABHSF_SYMMETRY_SYMMETRIC || a.symmetry > ABHSF_SYMMETRY_GENERAL)
+        fail(ABHSF_ERROR_INVALID_VALUE, "symmetry must be an abhsf_symmetry");
+    if (a.m < 1 || a.n < 1 || a.m > (int64_t(1) << 32) || a.n > (int64_t(1) << 32) || a.nnz < 0)
+        fail(ABHSF_ERROR_INVALID_VALUE, "sizes out of the .mm range (m, n in 1 .. 2^32, nnz >= 0)");
+    const bool real = a.matrix_type == ABHSF_MATRIX_REAL;
+    if (a.nnz > 0 && (!a.rows || !a.cols || (real && !a.vals)))
+        fail(ABHSF_ERROR_INVALID_VALUE, "rows, cols (and vals of a real matrix) must be non-NULL");
+    for (int64_t k = 0; k < a.nnz; ++k)
+        if (a.rows[k] < 0 || a.rows[k] >= a.m || a.cols[k] < 0 || a.cols[k] >= a.n)
+            fail(ABHSF_ERROR_INDEX_OUT_OF_RANGE, "an element lies outside m x n");
+    file_closer fc{std::fopen(path, "wb")};
+    if (!fc.f)
+        fail(ABHSF_ERROR_INVALID_VALUE, std::string("cannot open output file: ") + path);
+    const uint64_t flag = a.symmetry == ABHSF_SYMMETRY_GENERAL
+                              ? 0
+                              : (a.symmetry == ABHSF_SYMMETRY_SYMMETRIC ? 1
+                                                                        : (a.symmetry == ABHSF_SYMMETRY_HERMITIAN ? 2 : 3));
+    const uint64_t h[kMmHeaderWords] = {uint64_t(a.m), uint64_t(a.n), uint64_t(a.nnz), uint64_t(a.matrix_type), flag};
+    bool ok = std::fwrite(h, sizeof(uint64_t), kMmHeaderWords, fc.f) == kMmHeaderWords;
+    std::vector<uint32_t> buf;
+    for (const int64_t* idx : {a.rows, a.cols}) {
+        constexpr int64_t kChunk = 1 << 20;
+        for (int64_t k0 = 0; ok && k0 < a.nnz; k0 += kChunk) {
+            const int64_t k1 = std::min(a.nnz, k0 + kChunk);
+            buf.assign(idx + k0, idx + k1);
+            ok = std::fwrite(buf.data(), 4, size_t(k1 - k0), fc.f) == size_t(k1 - k0);
+        }
+    }
+    if (ok && real && a.nnz > 0)
+        ok = std::fwrite(a.vals, 8, size_t(a.nnz), fc.f) == size_t(a.nnz);
+    ok = (std::fflush(fc.f) == 0) && ok;
+    if (!ok)
+        fail(ABHSF_ERROR_INVALID_VALUE, std::string("could not write ") + path);
+}
+
 }  // namespace abhsf

@@ -289,6 +289,25 @@ def block_histograms_all(rows, cols, m: int, n: int, stream=None) -> dict[str, d
     return out
 
 
+def _coo_result(c: "capi.CooHost"):
+    """(rows, cols, vals, m, n, info) copied out of a library-owned CooHost,
+    which is freed."""
+    try:
+        k = int(c.nnz)
+        rows = np.ctypeslib.as_array(c.rows, shape=(k,)).copy() if k else np.zeros(0, np.int64)
+        cols = np.ctypeslib.as_array(c.cols, shape=(k,)).copy() if k else np.zeros(0, np.int64)
+        vals = np.ctypeslib.as_array(c.vals, shape=(k,)).copy() if k else np.zeros(0, np.float64)
+        info = {"matrix_type": {0: "binary", 2: "real"}[int(c.matrix_type)],
+                "symmetry": _SYMMETRIES[int(c.symmetry)],
+                "stored_triangle": ("", "lower", "upper")[int(c.stored_triangle)]}
+        return rows, cols, vals, int(c.m), int(c.n), info
+    finally:
+        capi.lib.abhsf_coo_host_free(C.byref(c))
+
+
+_SYMMETRIES = ("symmetric", "hermitian", "skew", "general")
+
+
 def read_mtx(path: str, threads: int = 0):
     """A Matrix Market coordinate file as the reference's read_mtx_real_or_binary
     reads it (include/abhsf/utils/matrix_market_reader.h:146-200), parsed on
@@ -297,17 +316,46 @@ def read_mtx(path: str, threads: int = 0):
     "stored_triangle"}."""
     c = capi.CooHost()
     capi.check(capi.lib.abhsf_read_mtx(os.fsencode(path), int(threads), C.byref(c)))
-    try:
-        k = int(c.nnz)
-        rows = np.ctypeslib.as_array(c.rows, shape=(k,)).copy() if k else np.zeros(0, np.int64)
-        cols = np.ctypeslib.as_array(c.cols, shape=(k,)).copy() if k else np.zeros(0, np.int64)
-        vals = np.ctypeslib.as_array(c.vals, shape=(k,)).copy() if k else np.zeros(0, np.float64)
-        info = {"matrix_type": {0: "binary", 2: "real"}[int(c.matrix_type)],
-                "symmetry": ("symmetric", "hermitian", "skew", "general")[int(c.symmetry)],
-                "stored_triangle": ("", "lower", "upper")[int(c.stored_triangle)]}
-        return rows, cols, vals, int(c.m), int(c.n), info
-    finally:
-        capi.lib.abhsf_coo_host_free(C.byref(c))
+    return _coo_result(c)
+
+
+def read_mm(path: str):
+    """A binary .mm matrix file (the layout utils/mtx2mm/mtx2mm.cpp:102-135
+    writes), returned as read_mtx returns the text file it was made from."""
+    c = capi.CooHost()
+    capi.check(capi.lib.abhsf_read_mm(os.fsencode(path), C.byref(c)))
+    return _coo_result(c)
+
+
+def write_mm(path: str, rows, cols, vals, m: int, n: int, matrix_type: str = "real",
+             symmetry: str = "general") -> None:
+    """Writes 0-based COO arrays as a binary .mm file (vals ignored for a
+    "binary" matrix)."""
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    cols = np.ascontiguousarray(cols, dtype=np.int64)
+    if rows.shape != cols.shape or rows.ndim != 1:
+        raise capi.InvalidValue(capi.INVALID_VALUE, "rows and cols must be 1-D arrays of one length")
+    if matrix_type not in ("real", "binary") or symmetry not in _SYMMETRIES:
+        raise capi.InvalidValue(capi.INVALID_VALUE, "matrix_type real / binary; symmetry " + " / ".join(_SYMMETRIES))
+    c = capi.CooHost()
+    c.m, c.n, c.nnz = int(m), int(n), rows.size
+    c.matrix_type = capi.MATRIX_TYPES[matrix_type]
+    c.symmetry = _SYMMETRIES.index(symmetry)
+    c.rows = rows.ctypes.data_as(C.POINTER(C.c_int64))
+    c.cols = cols.ctypes.data_as(C.POINTER(C.c_int64))
+    if matrix_type == "real":
+        vals = np.ascontiguousarray(vals, dtype=np.float64)
+        if vals.shape != rows.shape:
+            raise capi.InvalidValue(capi.INVALID_VALUE, "vals must have one value per element")
+        c.vals = vals.ctypes.data_as(C.POINTER(C.c_double))
+    capi.check(capi.lib.abhsf_write_mm(os.fsencode(path), C.byref(c)))
+
+
+def mtx2mm(src: str, dst: str, threads: int = 0) -> None:
+    """Converts a Matrix Market file to the binary .mm layout (what
+    utils/mtx2mm does, after read_mtx's zero-drop)."""
+    rows, cols, vals, m, n, info = read_mtx(src, threads)
+    write_mm(dst, rows, cols, vals, m, n, info["matrix_type"], info["symmetry"])
 
 
 def mmf_line(m: int, n: int, nnz: int, matrix_type: str | int, r: int, s: int, hist: dict[int, int]):

@@ -426,6 +426,20 @@ ABHSF_API abhsf_status abhsf_mlp_adam(float* params, const float* grad, float* m
 ABHSF_API abhsf_status abhsf_read_mtx(const char* path, int32_t threads, abhsf_coo_host* out);
 ABHSF_API abhsf_status abhsf_coo_host_free(abhsf_coo_host* coo);
 
+/* The reference's binary matrix file (".mm", written by
+ * utils/mtx2mm/mtx2mm.cpp:102-135): u64 m, n, nnz, type (0 pattern, 2 real),
+ * symmetry flag (0 general; 1 symmetric, 2 hermitian, 3 skew; the reference
+ * writes a bool), then u32 rows[nnz], u32 cols[nnz] (0-based) and, for a real
+ * matrix, f64 vals[nnz].  abhsf_read_mm returns what abhsf_read_mtx returns for
+ * the text file the .mm was made from: explicit zeros dropped, the stored
+ * triangle found (ABHSF_ERROR_INVALID_VALUE when a non-general file holds both),
+ * indices checked against m x n; integer and complex files are
+ * ABHSF_ERROR_UNSUPPORTED, a file whose size differs from its header's arrays
+ * ABHSF_ERROR_INVALID_VALUE.  abhsf_write_mm writes coo (real or pattern, m and
+ * n at most 2^32) in that layout. */
+ABHSF_API abhsf_status abhsf_read_mm(const char* path, abhsf_coo_host* out);
+ABHSF_API abhsf_status abhsf_write_mm(const char* path, const abhsf_coo_host* coo);
+
 /* Waits for the work queued on stream, then returns the matrix's device
  * status word (ABHSF_DEVSTAT_* bits; 0 = every SpMV so far completed) and,
  * if clear != 0, resets it.  No reference counterpart (the reference has no
