@@ -176,3 +176,122 @@ def test_gloo_ranks_sharded_cg_converges_like_one_process(world, g):
     assert np.linalg.norm(x - x_ref) <= 1e-7 * np.linalg.norm(x_ref)
     if g == 7:
         assert res[1][1] == res[1][2] == coo.m  # the empty rank
+
+
+def test_block_row_bytes_weigh_the_format():
+    """Per block row: the least-storage scheme's bits, the values, a tile
+    header and an x block per tile; a row of bitmap tiles weighs more per
+    nonzero than a row of COO tiles, and the weights balance the ranks."""
+    from abhsf_b200 import matrix as mx
+    s = 64
+    # block row 0: one tile with 2000 nonzeros (bitmap); block row 1: 100 tiles of 20 (COO)
+    r0 = np.repeat(np.arange(64), 32)[:2000]
+    c0 = np.tile(np.arange(0, 64, 2), 64)[:2000]
+    r1 = 64 + np.tile(np.arange(20), 100)
+    c1 = np.repeat(np.arange(100) * 64, 20) + np.tile(np.arange(20), 100)
+    rows, cols = np.concatenate([r0, r1]), np.concatenate([c0, c1])
+    w = sharded.block_row_bytes(rows, cols, 128, 6400, s)
+    assert mx.block_select_scheme(s, s, 2000) == "bitmap" and mx.block_select_scheme(s, s, 20) == "coo"
+    want0 = (mx.block_scheme_bits("bitmap", s, s, 2000) + 2) / 8 + 8 * 2000 + 8 + 8 * s
+    want1 = 100 * ((mx.block_scheme_bits("coo", s, s, 20) + 2) / 8 + 8 * 20 + 8 + 8 * s)
+    np.testing.assert_allclose(w, [want0, want1])
+    assert w[0] / 2000 < w[1] / 2000  # same nonzeros; many COO tiles read many x blocks
+    coo = W.tiled_mixture(n=8192, tile=64, p=0.02, seed=4)
+    wb = sharded.block_row_bytes(coo.rows, coo.cols, coo.m, coo.n, 64)
+    parts = sharded.partition_block_rows(coo.rows, coo.m, 64, 4, weights=wb)
+    got = [wb[a // 64: -(-b // 64)].sum() for a, b in parts]
+    assert abs(sum(got) - wb.sum()) < 1e-6 * wb.sum()
+    assert max(got) - wb.sum() / 4 <= wb.max()
+    with pytest.raises(ValueError):
+        sharded.partition_block_rows(coo.rows, coo.m, 64, 4, weights=wb[:-1])
+
+
+def _halo_rank_main(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from oracle import oracle
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        res = {}
+        # SpMV: a banded matrix, x held in equal slices
+        coo = W.banded(3000, 40, seed=2)
+        x = W.rhs(coo.n, 1)
+        y0 = W.rhs(coo.m, 2)
+        wb = sharded.block_row_bytes(coo.rows, coo.cols, coo.m, coo.n, 64)
+        r0, r1 = sharded.partition_block_rows(coo.rows, coo.m, 64, world, wb)[rank]
+        x0, x1 = sharded.x_slices(coo.n, world)[rank]
+        lr, lc, lv = sharded.local_elements(coo.rows, coo.cols, coo.vals, r0, r1)
+        plan = sharded.HaloPlan(lc, sharded.x_slices(coo.n, world))
+        xc = plan.fetch(torch.from_numpy(x[x0:x1].copy())).numpy()
+        res["fetched_ok"] = bool(np.array_equal(xc[: plan.need.size], x[plan.need]))
+        res["halo"] = plan.halo_entries(rank)
+        order = np.lexsort((lc, lr))
+        res["y"] = oracle.spmv_elements(lr[order], plan.local_columns(lc[order]), lv[order], xc,
+                                        y0[r0:r1].copy())
+        res["r"] = (r0, r1)
+        # CG on the 2D Laplacian: halo exchange against all-gather
+        lap = W.laplacian_2d(20)
+        b = W.rhs(lap.n, 5)
+        ranges = sharded.partition_block_rows(lap.rows, lap.m, 64, world)
+        q0, q1 = ranges[rank]
+        lr, lc, lv = sharded.local_elements(lap.rows, lap.cols, lap.vals, q0, q1)
+        hp = sharded.HaloPlan(lc, ranges)
+        lcc = hp.local_columns(lc)
+
+        def full_product(v, q):
+            q.copy_(torch.from_numpy(oracle.spmv_elements(lr, lc, lv, v.numpy(), q.numpy().copy())))
+
+        def halo_product(v, q):
+            q.copy_(torch.from_numpy(oracle.spmv_elements(lr, lcc, lv, v.numpy(), q.numpy().copy())))
+        xa = torch.zeros(q1 - q0, dtype=torch.float64)
+        xh = torch.zeros(q1 - q0, dtype=torch.float64)
+        bl = torch.from_numpy(b[q0:q1].copy())
+        res["cg_all"] = sharded.cg(full_product, bl, xa, ranges, 1e-10, 2000)
+        res["cg_halo"] = sharded.cg(halo_product, bl, xh, ranges, 1e-10, 2000, fetch=hp.fetch)
+        res["cg_same_bits"] = bool(np.array_equal(xa.numpy().view(np.uint64), xh.numpy().view(np.uint64)))
+        res["cg_halo_entries"] = hp.halo_entries(rank)
+        out.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_halo_exchange_gives_the_full_product_bits(world):
+    """Each rank fetches only the x entries its columns read (a banded
+    matrix: its slice and about a band's width from each neighbour); the
+    products on renumbered columns compose to the full product bit for bit,
+    and CG through the halo exchange retraces CG through the all-gather
+    bit for bit."""
+    import torch.multiprocessing as mp
+    from oracle import oracle
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_halo_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [r for _, r in sorted((q.get(timeout=180) for _ in procs), key=lambda t: t[0])]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    coo = W.banded(3000, 40, seed=2)
+    x = W.rhs(coo.n, 1)
+    y0 = W.rhs(coo.m, 2)
+    order = np.lexsort((coo.cols, coo.rows))
+    want = oracle.spmv_elements(coo.rows[order], coo.cols[order], coo.vals[order], x, y0.copy())
+    assert all(r["fetched_ok"] for r in res)
+    assert res[0]["r"][0] == 0 and res[-1]["r"][1] == coo.m
+    np.testing.assert_array_equal(np.concatenate([r["y"] for r in res]), want)
+    # a rank reads columns [r0 - 40, r1 + 40) and holds x[x0:x1): it fetches at
+    # most the difference (none when its rows sit inside its slice)
+    for r, (x0, x1) in zip(res, sharded.x_slices(coo.n, world)):
+        r0, r1 = r["r"]
+        assert 0 <= r["halo"] <= abs(r0 - x0) + abs(r1 - x1) + 2 * 40
+    assert sum(r["halo"] for r in res) > 0
+    for r in res:
+        assert r["cg_all"]["converged"] and r["cg_same_bits"]
+        assert r["cg_halo"] == r["cg_all"]
+        assert 0 < r["cg_halo_entries"] <= 2 * 20  # one grid row from each neighbour
