@@ -13,6 +13,13 @@
 // as the reference's std::vector<std::tuple<int, int, double>>
 // (spmv/unified/spmv.cpp:68-69).  Unlike the reference's from_elements, the
 // caller's elements are not reordered.
+//
+// The reader has the reference's call shape too:
+//
+//   abhsf::read_mtx_real_or_binary(filename, elements, props);  // matrix_market_reader.h:146-200
+//
+// with the library's multi-threaded parser behind it (abhsf_read_mtx), and
+// abhsf::read_mm reads the binary .mm layout of utils/mtx2mm the same way.
 #pragma once
 
 #include <cstdint>
@@ -98,5 +105,50 @@ class gpu_matrix {
     abhsf_matrix* h_ = nullptr;
     abhsf_build_opts opts_;
 };
+
+namespace detail {
+
+struct host_coo {
+    abhsf_coo_host c{};
+    host_coo() = default;
+    host_coo(const host_coo&) = delete;
+    host_coo& operator=(const host_coo&) = delete;
+    ~host_coo() { abhsf_coo_host_free(&c); }
+};
+
+template <typename Elements, typename Props>
+void append_elements(const host_coo& f, Elements& elements, Props& props)
+{
+    elements.reserve(elements.size() + (size_t)f.c.nnz);
+    for (int64_t k = 0; k < f.c.nnz; ++k)
+        elements.emplace_back(f.c.rows[k], f.c.cols[k], f.c.vals[k]);
+    props.m = f.c.m;
+    props.n = f.c.n;
+    props.nnz = f.c.nnz;  // after the zero-drop, as the reference's props.nnz -= zeros
+}
+
+}  // namespace detail
+
+// Appends the elements of a Matrix Market file (0-based row, col, value;
+// explicit zeros dropped; pattern values 1.0) and sets props.m, props.n and
+// props.nnz, as the reference's read_mtx_real_or_binary does
+// (include/abhsf/utils/matrix_market_reader.h:146-200); failures throw
+// std::runtime_error.  Props is any type with members m, n and nnz.
+template <typename Elements, typename Props>
+void read_mtx_real_or_binary(const std::string& filename, Elements& elements, Props& props, int threads = 0)
+{
+    detail::host_coo f;
+    throw_if_error(abhsf_read_mtx(filename.c_str(), threads, &f.c));
+    detail::append_elements(f, elements, props);
+}
+
+// The same for a binary .mm file (utils/mtx2mm/mtx2mm.cpp:102-135).
+template <typename Elements, typename Props>
+void read_mm(const std::string& filename, Elements& elements, Props& props)
+{
+    detail::host_coo f;
+    throw_if_error(abhsf_read_mm(filename.c_str(), &f.c));
+    detail::append_elements(f, elements, props);
+}
 
 }  // namespace abhsf

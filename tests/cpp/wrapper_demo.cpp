@@ -19,6 +19,24 @@ struct props_t {
 
 int main(int argc, char** argv)
 {
+    // --read FILE: the reference-shaped reader (host only); prints the sizes
+    // and order-sensitive sums of what it appended
+    if (argc > 2 && (std::strcmp(argv[1], "--read") == 0 || std::strcmp(argv[1], "--read-mm") == 0)) {
+        std::vector<std::tuple<int, int, double>> el{{7, 7, 7.0}};  // appended to, as the reference does
+        props_t p{0, 0, 0};
+        if (std::strcmp(argv[1], "--read") == 0)
+            abhsf::read_mtx_real_or_binary(argv[2], el, p);
+        else
+            abhsf::read_mm(argv[2], el, p);
+        double wr = 0.0, wc = 0.0, sv = 0.0;
+        for (size_t k = 1; k < el.size(); ++k) {
+            wr += (double)k * std::get<0>(el[k]);
+            wc += (double)k * std::get<1>(el[k]);
+            sv += std::get<2>(el[k]);
+        }
+        std::printf("read %ld %ld %ld %zu %.17g %.17g %.17g\n", p.m, p.n, p.nnz, el.size(), wr, wc, sv);
+        return 0;
+    }
     const bool run_gpu = argc > 1 && std::strcmp(argv[1], "--gpu") == 0;
     // invalid block size: must throw before touching a device
     {
