@@ -176,6 +176,67 @@ def edge_shapes(n: int = 1000) -> list[Coo]:
     return out
 
 
+BLOCKGEN_SEED = 0x0498BC04  # the reference generator's seed (spmv/orig/88.cpp:46)
+
+
+def block_pattern(bnnz: int = 1, kind: str = "random", block: int = 8, seed: int = BLOCKGEN_SEED) -> np.ndarray:
+    """The (row, col) positions of one block as the reference's
+    block_generator forms them (spmv/orig/88.cpp:43-141), sorted row-major
+    (its std::set order, which finalize walks): "random" draws (row, col)
+    pairs uniformly over the block until bnnz distinct ones are held
+    (generate_random, 48-68); "diagonal", "single_row" and "single_col" are
+    generate_diagonal / _single_row / _single_col (70-95).  The random draws
+    come from numpy's PCG64 with the reference's seed, not from std::mt19937
+    through std::uniform_int_distribution (whose mapping differs between
+    standard-library versions): the same procedure and shape, another
+    pattern."""
+    if kind == "random":
+        if not 0 < bnnz <= block * block:
+            raise ValueError("bnnz must lie in 1 .. block * block")
+        rng = np.random.default_rng(seed)
+        held: set[tuple[int, int]] = set()
+        while len(held) < bnnz:
+            r, c = rng.integers(0, block, 2)
+            held.add((int(r), int(c)))
+        pos = sorted(held)
+    elif kind == "diagonal":
+        pos = [(k, k) for k in range(block)]
+    elif kind == "single_row":
+        pos = [(0, k) for k in range(block)]
+    elif kind == "single_col":
+        pos = [(k, 0) for k in range(block)]
+    else:
+        raise ValueError("kind: random, diagonal, single_row or single_col")
+    return np.array(pos, dtype=np.int64).reshape(-1, 2)
+
+
+def identical_blocks(num_blocks: int, bnnz: int = 1, kind: str = "random", block: int = 8,
+                     seed: int = BLOCKGEN_SEED) -> Coo:
+    """The reference's per-scheme block benchmark matrix (spmv/orig/88.cpp:716-840,
+    4096 x 4096 blocks there): num_blocks x num_blocks copies of one block
+    pattern (block_pattern), every value 1.0, elements in row order.  With
+    x = 1 every SpMV adds bnnz * num_blocks^2 to the sum of y, the known
+    answer the reference prints as its "y-vector sum"."""
+    pat = block_pattern(bnnz, kind, block, seed)
+    nb = int(num_blocks)
+    # rows: block row I, pattern row; within a row, block columns J then pattern columns
+    br = np.arange(nb, dtype=np.int64)
+    rows_l, cols_l = [], []
+    for pr in range(block):
+        pc = pat[pat[:, 0] == pr, 1]
+        if pc.size == 0:
+            continue
+        cols_one_row = (br[:, None] * block + pc[None, :]).reshape(-1)  # J-major, then pattern column
+        rows_l.append((br * block + pr)[:, None].repeat(cols_one_row.size, axis=1))
+        cols_l.append(np.broadcast_to(cols_one_row, (nb, cols_one_row.size)))
+    rows = np.concatenate([r.reshape(-1) for r in rows_l])
+    cols = np.concatenate([c.reshape(-1) for c in cols_l])
+    order = np.lexsort((cols, rows))
+    rows, cols = rows[order], cols[order]
+    n = nb * block
+    return Coo(rows, cols, np.ones(rows.size), n, n, f"identical_blocks_{nb}_{kind}_{pat.shape[0]}")
+
+
 def banded(n: int, bandwidth: int, seed: int = 0) -> Coo:
     """Every entry within `bandwidth` of the diagonal (|i - j| <= bandwidth),
     values N(0,1): the banded half of the batched workload."""
