@@ -295,3 +295,49 @@ def test_gloo_halo_exchange_gives_the_full_product_bits(world):
         assert r["cg_all"]["converged"] and r["cg_same_bits"]
         assert r["cg_halo"] == r["cg_all"]
         assert 0 < r["cg_halo_entries"] <= 2 * 20  # one grid row from each neighbour
+
+
+def _halo_empty_rank_main(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from oracle import oracle
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        coo = W.laplacian_2d(7)  # 49 rows, one block row: rank 1 owns no rows
+        x = W.rhs(coo.n, 1)
+        r0, r1 = sharded.partition_block_rows(coo.rows, coo.m, 64, world)[rank]
+        x0, x1 = sharded.x_slices(coo.n, world)[rank]
+        lr, lc, lv = sharded.local_elements(coo.rows, coo.cols, coo.vals, r0, r1)
+        plan = sharded.HaloPlan(lc, sharded.x_slices(coo.n, world))
+        xc = plan.fetch(torch.from_numpy(x[x0:x1].copy())).numpy()
+        y = oracle.spmv_elements(lr, plan.local_columns(lc), lv, xc, np.zeros(r1 - r0))
+        out.put((rank, (r0, r1), int(plan.need.size), int(plan.send_counts.sum()), plan.width, y))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_halo_with_a_rank_that_reads_nothing():
+    """A rank without rows needs no x entries (its fetch is a zero-length
+    receive, its local width 1) but still sends the part of x it holds."""
+    import torch.multiprocessing as mp
+    from oracle import oracle
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_halo_empty_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=120) for _ in procs), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    coo = W.laplacian_2d(7)
+    assert res[0][1] == (0, 49) and res[1][1] == (49, 49)
+    assert res[0][2] == 49 and res[1][2] == 0 and res[1][4] == 1
+    assert res[0][3] == 25 and res[1][3] == 24  # each sends what rank 0 reads of its slice
+    want = oracle.spmv_elements(coo.rows, coo.cols, coo.vals, W.rhs(coo.n, 1), np.zeros(coo.m))
+    np.testing.assert_array_equal(res[0][5], want)
+    assert res[1][5].size == 0
