@@ -1,0 +1,92 @@
+"""The oracle's block histograms and the library's mmf lines against the
+reference's own block_stats and mmf programs (compiled from the reference
+sources into oracle/_ref/, the checker) on generated matrices: random sizes
+up to 600 x 600, elements scattered, clustered into a few tiles (dense and
+bitmap tiles) or laid along bands, for all 64 block sizes.  Without the
+reference programs the test is skipped; the committed golden fixtures cover
+the same comparison on fixed matrices."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from abhsf_b200 import matrix as mx
+from oracle import oracle
+
+hyp = pytest.importorskip("hypothesis")
+st = pytest.importorskip("hypothesis.strategies")
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+pytestmark = pytest.mark.skipif(
+    not all(os.path.exists(os.path.join(REF_DIR, p)) for p in ("block_stats", "mmf")),
+    reason="reference block_stats / mmf not built (make -C oracle ref)")
+
+
+@st.composite
+def matrices(draw):
+    m = draw(st.integers(1, 600))
+    n = draw(st.integers(1, 600))
+    kind = draw(st.sampled_from(["scatter", "cluster", "band"]))
+    seed = draw(st.integers(0, 2 ** 31 - 1))
+    rng = np.random.default_rng(seed)
+    k = draw(st.integers(1, 3000))
+    if kind == "scatter":
+        key = rng.integers(0, m * n, k)
+    elif kind == "cluster":  # a few dense corners: 1..64 x 1..64 windows filled at random density
+        keys = []
+        for _ in range(draw(st.integers(1, 4))):
+            h, w = rng.integers(1, 65, 2)
+            r0, c0 = rng.integers(0, m), rng.integers(0, n)
+            rr, cc = np.meshgrid(np.arange(r0, min(r0 + h, m)), np.arange(c0, min(c0 + w, n)), indexing="ij")
+            win = (rr * n + cc).reshape(-1)
+            keys.append(win[rng.random(win.size) < rng.uniform(0.2, 1.0)])
+        key = np.concatenate(keys + [rng.integers(0, m * n, 5)])
+    else:
+        i = rng.integers(0, m, k)
+        j = np.clip(i * n // m + rng.integers(-8, 9, k), 0, n - 1)
+        key = i * n + j
+    key = np.unique(key)
+    vals = rng.standard_normal(key.size)
+    vals[vals == 0] = 1.0
+    return m, n, key // n, key % n, vals
+
+
+def reference_stats(m, n, rows, cols, vals, d):
+    p = os.path.join(d, "a.mtx")
+    with open(p, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate real general\n{m} {n} {rows.size}\n")
+        f.write("".join(f"{i + 1} {j + 1} {v:.17g}\n" for i, j, v in zip(rows, cols, vals)))
+    subprocess.run([os.path.join(REF_DIR, "block_stats"), p], cwd=d, check=True, stdout=subprocess.DEVNULL)
+    subprocess.run([os.path.join(REF_DIR, "mmf")], cwd=d, check=True, stdout=subprocess.DEVNULL)
+    props = [int(t) for t in open(os.path.join(d, "props")).read().split()]
+    hists = {}
+    for k in range(1, 9):
+        for l in range(1, 9):
+            h = {}
+            for line in open(os.path.join(d, f"{1 << k}x{1 << l}.bstats")):
+                z, c = line.split()
+                h[int(z)] = int(c)
+            hists[(k, l)] = h
+    mmf = {prec: {(t[0], t[1]): t[2:] for t in ([int(v) for v in line.split()]
+                                                 for line in open(os.path.join(d, "mmf-" + prec)) if line.strip())}
+           for prec in ("single", "double")}
+    return props, hists, mmf
+
+
+@hyp.settings(max_examples=60, deadline=None, derandomize=True)
+@hyp.given(mat=matrices())
+def test_generated_matrices_match_block_stats_and_mmf(mat):
+    m, n, rows, cols, vals = mat
+    with tempfile.TemporaryDirectory() as d:
+        props, hists, mmf = reference_stats(m, n, rows, cols, vals, d)
+    assert props[:4] == [m, n, rows.size, rows.size]
+    for (k, l), h in hists.items():
+        assert oracle.block_histogram(rows, cols, k, l) == h, (k, l)
+        assert sum(z * c for z, c in h.items()) == rows.size
+        r, s = 1 << k, 1 << l
+        o1, o2 = mx.mmf_line(m, n, rows.size, "real", r, s, h)
+        assert o1 == mmf["single"][(r, s)] and o2 == mmf["double"][(r, s)], (r, s)
+        assert (o1, o2) == tuple(oracle.mmf_line(m, n, rows.size, 2, r, s, h))
