@@ -90,3 +90,30 @@ def test_generated_matrices_match_block_stats_and_mmf(mat):
         o1, o2 = mx.mmf_line(m, n, rows.size, "real", r, s, h)
         assert o1 == mmf["single"][(r, s)] and o2 == mmf["double"][(r, s)], (r, s)
         assert (o1, o2) == tuple(oracle.mmf_line(m, n, rows.size, 2, r, s, h))
+
+
+@pytest.mark.skipif(not oracle.RefCSR.available(), reason="reference CSR not built (make -C oracle ref)")
+@hyp.settings(max_examples=60, deadline=None, derandomize=True)
+@hyp.given(mat=matrices(), s=st.sampled_from([16, 32, 64, 128, 256]), seed=st.integers(0, 1000))
+def test_generated_matrices_spmv_bits_match_reference_csr(mat, s, seed):
+    """y from the reference's CSR spmv_naive (spmv/bottlenecks/spmv.cpp:58-64),
+    from the oracle's element loop on row-major elements, and from the oracle's
+    ABHSF format at block size s (serial and on all host threads): the same
+    bits, with random values, x and y."""
+    m, n, rows, cols, vals = mat
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-1, 1, n)
+    y0 = rng.standard_normal(m)
+    ref = oracle.RefCSR(rows, cols, vals, m, n)
+    y_ref = y0.copy()
+    ref.spmv(x, y_ref)
+    ref.release()
+    y_loop = oracle.spmv_elements(rows, cols, vals, x, y0.copy())  # rows, cols come row-major from np.unique
+    np.testing.assert_array_equal(y_loop, y_ref)
+    b = oracle.build(rows, cols, vals, m, n, s)
+    y_fmt = y0.copy()
+    b.spmv(x, y_fmt)
+    np.testing.assert_array_equal(y_fmt, y_ref)
+    y_omp = y0.copy()
+    b.spmv_omp(x, y_omp)
+    np.testing.assert_array_equal(y_omp, y_ref)
