@@ -1,0 +1,51 @@
+"""bench.py's host-side helpers (no GPU): the roofline denominator comes from
+the measured peaks file, the ncu traffic from the committed profile summary,
+algorithmic bytes follow B = B_fmt + 8 n + 16 m, and the clock sampler's
+parse keeps only the throttle reasons nvidia-smi reports Active."""
+import json
+import os
+
+import bench
+
+
+def test_peak_is_the_measured_copy_bandwidth():
+    with open(os.path.join(bench.ROOT, "MEASURED_PEAKS.json")) as f:
+        want = float(json.load(f)["hbm_gbs"])
+    assert bench.hbm_peak() == (want, "measured")
+
+
+def test_ncu_traffic_comes_from_the_committed_summary():
+    t = bench.ncu_traffic_per_launch("reference", bench.DEFAULT_N)
+    assert t is not None and t > 0
+    assert bench.ncu_traffic_per_launch("reference", bench.DEFAULT_N // 2) is None  # other sizes: not captured
+
+
+def test_algorithmic_bytes():
+    assert bench.algorithmic_bytes({"format_bytes": 1000}, m=3, n=5) == 1000 + 8 * 5 + 16 * 3
+
+
+class _FakeSmi:
+    def __init__(self, text):
+        self.text = text
+
+    def terminate(self):
+        pass
+
+    def communicate(self, timeout=None):
+        return self.text, ""
+
+
+def test_clock_sampler_parse():
+    rows = [
+        "0, 1965, 1965, 700.1, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+        "0, 1800, 1965, 990.0, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+        "0, 1700, 1965, 999.0, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+        "garbage line",
+    ]
+    cs = object.__new__(bench.ClockSampler)
+    cs.proc = _FakeSmi("\n".join(rows) + "\n")
+    cs.idx = 0
+    got = cs.stop()
+    assert got == {"sm_mhz": 1800.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    cs.proc = None
+    assert cs.stop() is None
