@@ -10,8 +10,13 @@
 // the reference's fscanf("%lf") does.  Unlike the reference, indices outside
 // the declared m x n are an error here, and the entry lines are parsed by
 // several host threads at once (the file is read whole, split at line ends).
+// Numbers in their plain spellings go through std::from_chars, which rounds
+// a decimal exactly as strtod does; every other spelling (a sign on an index,
+// '+', hexadecimal, inf / nan words, a value out of the double range) goes
+// through strtoull / strtod as before.
 #include <algorithm>
 #include <cctype>
+#include <charconv>
 #include <cerrno>
 #include <cstdio>
 #include <cstdlib>
@@ -54,37 +59,79 @@ struct chunk_out {
     bool lower = false, upper = false, bad = false, range = false;
 };
 
+inline bool is_space(char c)
+{
+    return c == ' ' || c == '\t' || c == '\r' || c == '\n' || c == '\v' || c == '\f';
+}
+
+// An index at p (leading white space skipped, as strtoull skips it); false if
+// none can be read.  p is within a NUL-terminated buffer.
+inline bool read_index(const char*& p, const char* e, unsigned long long& v)
+{
+    const char* s = p;
+    while (s < e && is_space(*s))
+        ++s;
+    if (s < e && *s >= '0' && *s <= '9') {
+        const auto r = std::from_chars(s, e, v);
+        if (r.ec == std::errc()) {
+            p = r.ptr;
+            return true;
+        }
+    }
+    char* q = nullptr;
+    errno = 0;
+    v = std::strtoull(p, &q, 10);
+    if (q == p || errno)
+        return false;
+    p = q;
+    return true;
+}
+
+// A value at p, rounded as strtod rounds it.
+inline bool read_value(const char*& p, const char* e, double& v)
+{
+    const char* s = p;
+    while (s < e && is_space(*s))
+        ++s;
+    if (s < e && ((*s >= '0' && *s <= '9') || *s == '-' || *s == '.')) {
+        const auto r = std::from_chars(s, e, v);
+        if (r.ec == std::errc() && (r.ptr == e || (*r.ptr != 'x' && *r.ptr != 'X'))) {
+            p = r.ptr;
+            return true;
+        }
+    }
+    char* q = nullptr;
+    v = std::strtod(p, &q);
+    if (q == p)
+        return false;
+    p = q;
+    return true;
+}
+
 // Entries of buf[b, e) (whole lines), at most `limit` of them.
 void parse_chunk(const char* b, const char* e, bool pattern, int64_t m, int64_t n, int64_t limit, chunk_out& o)
 {
+    // about 24 bytes per entry line in the files this reads; growth past it is amortised
+    const size_t guess = size_t(e - b) / 24 + 16;
+    o.rows.reserve(guess);
+    o.cols.reserve(guess);
+    if (!pattern)
+        o.vals.reserve(guess);
     const char* p = b;
     while (p < e && o.entries < limit) {
-        while (p < e && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n'))
+        while (p < e && is_space(*p))
             ++p;
         if (p >= e)
             break;
-        char* q = nullptr;
-        errno = 0;
-        const unsigned long long r = std::strtoull(p, &q, 10);
-        if (q == p || errno) {
+        unsigned long long r, c;
+        if (!read_index(p, e, r) || !read_index(p, e, c)) {
             o.bad = true;
             return;
         }
-        p = q;
-        const unsigned long long c = std::strtoull(p, &q, 10);
-        if (q == p || errno) {
-            o.bad = true;
-            return;
-        }
-        p = q;
         double v = 1.0;
-        if (!pattern) {
-            v = std::strtod(p, &q);
-            if (q == p) {
-                o.bad = true;
-                return;
-            }
-            p = q;
+        if (!pattern && !read_value(p, e, v)) {
+            o.bad = true;
+            return;
         }
         while (p < e && *p != '\n')  // the rest of the line (a complex part, a comment) is not read
             ++p;
@@ -120,6 +167,14 @@ void read_mtx(const char* path, int threads, abhsf_coo_host& out)
         fail(ABHSF_ERROR_INVALID_VALUE, std::string("cannot open input file: ") + path);
     std::string buf;
     {
+        // one read of the whole file when its size is known, else by pieces
+        long size = -1;
+        if (std::fseek(f, 0, SEEK_END) == 0)
+            size = std::ftell(f);
+        if (size >= 0 && std::fseek(f, 0, SEEK_SET) == 0) {
+            buf.resize(size_t(size));
+            buf.resize(std::fread(&buf[0], 1, buf.size(), f));
+        }
         char tmp[1 << 16];
         size_t k;
         while ((k = std::fread(tmp, 1, sizeof(tmp), f)) > 0)
@@ -238,13 +293,23 @@ void read_mtx(const char* path, int threads, abhsf_coo_host& out)
         out = abhsf_coo_host{};
         fail(ABHSF_ERROR_OUT_OF_MEMORY, "host allocation failed");
     }
-    int64_t o = 0;
-    for (int t = 0; t < used; ++t) {
+    std::vector<int64_t> at(used + 1, 0);
+    for (int t = 0; t < used; ++t)
+        at[t + 1] = at[t] + take[t];
+    auto copy_part = [&](int t) {
         const chunk_out& c = parts[t];
-        std::copy(c.rows.begin(), c.rows.begin() + take[t], out.rows + o);
-        std::copy(c.cols.begin(), c.cols.begin() + take[t], out.cols + o);
-        std::copy(c.vals.begin(), c.vals.begin() + take[t], out.vals + o);
-        o += take[t];
+        std::copy(c.rows.begin(), c.rows.begin() + take[t], out.rows + at[t]);
+        std::copy(c.cols.begin(), c.cols.begin() + take[t], out.cols + at[t]);
+        std::copy(c.vals.begin(), c.vals.begin() + take[t], out.vals + at[t]);
+    };
+    if (used > 1) {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < used; ++t)
+            pool.emplace_back(copy_part, t);
+        for (auto& th : pool)
+            th.join();
+    } else if (used == 1) {
+        copy_part(0);
     }
 }
 
