@@ -341,3 +341,98 @@ def test_gloo_halo_with_a_rank_that_reads_nothing():
     want = oracle.spmv_elements(coo.rows, coo.cols, coo.vals, W.rhs(coo.n, 1), np.zeros(coo.m))
     np.testing.assert_array_equal(res[0][5], want)
     assert res[1][5].size == 0
+
+
+class _OracleLocal:
+    """Stands in for the rank's GPU matrix in ShardedMatrix on gloo ranks: the
+    oracle's product (the checker) on the same elements."""
+
+    def __init__(self, rows, cols, vals, m, n):
+        order = np.lexsort((cols, rows))
+        self.rows, self.cols, self.vals = rows[order], cols[order], np.asarray(vals)[order]
+        self.m, self.n = m, n
+
+    @classmethod
+    def from_elements(cls, rows, cols, vals, m, n, block_size=64, **build):
+        return cls(np.asarray(rows), np.asarray(cols), vals, m, n)
+
+    def spmv(self, x, y):
+        import torch
+        from oracle import oracle
+        assert x.numel() == self.n and y.numel() == self.m
+        y.copy_(torch.from_numpy(oracle.spmv_elements(self.rows, self.cols, self.vals, x.numpy(), y.numpy().copy())))
+
+    def release(self):
+        pass
+
+
+def _class_rank_main(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from abhsf_b200 import matrix as mxm
+    mxm.AbhsfMatrix = _OracleLocal
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        res = {}
+        coo = W.banded(2000, 30, seed=4)
+        x = W.rhs(coo.n, 1)
+        y0 = W.rhs(coo.m, 2)
+        for ex in ("allgather", "halo"):
+            S = sharded.ShardedMatrix(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64, exchange=ex)
+            y = torch.from_numpy(y0[S.row0:S.row1].copy())
+            S.spmv(torch.from_numpy(x[S.x0:S.x1].copy()), y)
+            res["spmv_" + ex] = (S.row0, S.row1, y.numpy().copy())
+            if ex == "halo":
+                res["halo_width"] = S.local.n if S.local is not None else 0
+            S.release()
+        lap = W.laplacian_2d(20)
+        b = W.rhs(lap.n, 5)
+        for ex in ("allgather", "halo"):
+            S = sharded.ShardedMatrix(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=64, exchange=ex)
+            xs = torch.zeros(S.row1 - S.row0, dtype=torch.float64)
+            info = S.cg(torch.from_numpy(b[S.row0:S.row1].copy()), xs, rtol=1e-10, max_iters=2000)
+            res["cg_" + ex] = (info, xs.numpy().copy())
+            S.release()
+        out.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_sharded_matrix_class_both_exchanges():
+    """ShardedMatrix on three gloo ranks, its local GPU matrix replaced by
+    the oracle's product: y composes to the full product bit for bit with
+    either exchange (the halo rank's matrix is only as wide as the columns it
+    reads), and CG gives the same bits and iterations with either."""
+    import torch.multiprocessing as mp
+    from oracle import oracle
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    world = 3
+    procs = [ctx.Process(target=_class_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [r for _, r in sorted((q.get(timeout=180) for _ in procs), key=lambda t: t[0])]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    coo = W.banded(2000, 30, seed=4)
+    x = W.rhs(coo.n, 1)
+    y0 = W.rhs(coo.m, 2)
+    order = np.lexsort((coo.cols, coo.rows))
+    want = oracle.spmv_elements(coo.rows[order], coo.cols[order], coo.vals[order], x, y0.copy())
+    for ex in ("allgather", "halo"):
+        parts = [r["spmv_" + ex] for r in res]
+        assert parts[0][0] == 0 and parts[-1][1] == coo.m
+        np.testing.assert_array_equal(np.concatenate([p[2] for p in parts]), want)
+    for r in res:
+        r0, r1 = r["spmv_halo"][:2]
+        assert 0 < r["halo_width"] <= (r1 - r0) + 2 * 30  # its rows' band, not all 2000 columns
+        a_info, a_x = r["cg_allgather"]
+        h_info, h_x = r["cg_halo"]
+        assert a_info["converged"] and a_info == h_info
+        np.testing.assert_array_equal(a_x.view(np.uint64), h_x.view(np.uint64))
