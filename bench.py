@@ -521,6 +521,39 @@ def cpu_abhsf_run(c, bytes_per_step: float, max_seconds: float = 10.0, max_iters
             "sample": f"{len(times)} full y += A x, the oracle's C ABHSF SpMV (s = 64) with OpenMP over block rows"}
 
 
+def block_kernel_lines(text: str) -> list[dict]:
+    """The result lines the reference's block micro-benchmarks print
+    (spmv/orig/44_bitmap.cpp:759-768), colour codes removed."""
+    text = re.sub(r"\x1b\[[0-9;]*m", "", text)
+    lines = []
+    for m in re.finditer(r"Block nonzeros =\s*(\d+), MFLOP/s: min =\s*([0-9.]+), avg =\s*([0-9.]+), "
+                         r"max =\s*([0-9.]+); y-vector sum:\s*([0-9.eE+-]+)", text):
+        lines.append({"bnnz": int(m.group(1)), "mflops_min": float(m.group(2)), "mflops_avg": float(m.group(3)),
+                      "mflops_max": float(m.group(4)), "y_sum": float(m.group(5))})
+    return lines
+
+
+def cpu_block_kernel_run(max_seconds: float = 25.0):
+    """The reference's format-level micro-baseline: its AVX2 4 x 4 bitmap
+    block kernel spmv_temp (spmv/orig/44_bitmap.cpp:330-396), one thread, on
+    its own synthetic matrix (8192 x 8192 identical random blocks, values 1,
+    x = 1), compiled unmodified into oracle/_ref/44_bitmap.  It prints one
+    line per block nonzero count, 1..16; the lines that arrive within
+    max_seconds are kept (the run stops there)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "44_bitmap")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/44_bitmap not built (make -C oracle ref)"}
+    try:
+        out = subprocess.run([exe, "4"], capture_output=True, timeout=max_seconds).stdout
+    except subprocess.TimeoutExpired as e:
+        out = e.stdout or b""
+    lines = block_kernel_lines(out.decode(errors="replace"))
+    return {"kernel": "44_bitmap spmv_temp (spmv/orig/44_bitmap.cpp:330-396), AVX2, 4 x 4 bitmap blocks",
+            "unit": "MFLOP/s", "cores": 1, "kind": "reference", "lines": lines,
+            "sample": f"the block nonzero counts finished within {max_seconds:.0f} s (of 1..16), "
+                      "each 5 random patterns x 8 timed products over 8192^2 blocks"}
+
+
 def build_format_stats(c):
     """Format statistics without a GPU (for the reference arm): the oracle
     builder gives the same bytes as the device format."""
@@ -646,7 +679,7 @@ def run_ours(args):
         for key in ("batched", "one_by_one"):
             batched[key]["frac_of_peak"] = batched[key]["GB/s"] / peak
     achieved = B / (t_mean * 1e-3) / 1e9
-    cpu = cpu_abhsf = None
+    cpu = cpu_abhsf = cpu_block = None
     status = A.device_status()
     if status:
         raise RuntimeError(f"SpMV kernel reported device status {status}")
@@ -657,6 +690,11 @@ def run_ours(args):
             cpu_abhsf = cpu_abhsf_run(c, B)
         except Exception as e:  # a secondary reference point: report why it is missing
             cpu_abhsf = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+        if not args.no_block_kernel:
+            try:
+                cpu_block = cpu_block_kernel_run()
+            except Exception as e:
+                cpu_block = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
     if rank == 0:
         line = {
             "metric": METRIC, "value": aggregate_rate(B, t_max * 1e-3, world), "unit": UNIT, "n_gpus": world,
@@ -679,6 +717,7 @@ def run_ours(args):
                          "kernel": KERNELS[args.sum_order] + "<64>"},
             "cpu_baseline": cpu,
             "cpu_abhsf": cpu_abhsf,
+            "cpu_block_kernel": cpu_block,
             "spmm": spmm,
             "lowprec": lowprec,
             "cg": cg_times,
@@ -704,6 +743,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-block-kernel", action="store_true",
+                    help="skip the reference's 4 x 4 bitmap block micro-baseline (25 s on one host core)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
     ap.add_argument("--no-spmm", action="store_true", help="skip the multi-right-hand-side timings")
     ap.add_argument("--no-lowprec", action="store_true", help="skip the f32 / bf16 SpMV timings")

@@ -49,3 +49,16 @@ def test_clock_sampler_parse():
     assert got == {"sm_mhz": 1800.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
     cs.proc = None
     assert cs.stop() is None
+
+
+def test_block_kernel_lines_parse():
+    text = ("Bitmap SpMV type: \x1b[1;33mBITMAP TEMP\x1b[0m\n"
+            "Block nonzeros = \x1b[0;36m   1\x1b[0m, MFLOP/s: min = \x1b[1;32m    425.55\x1b[0m, avg = \x1b[1;32m"
+            "    430.74\x1b[0m, max = \x1b[1;32m    436.60\x1b[0m; y-vector sum: \x1b[0;31m4.697620400000000e+09\x1b[0m\n"
+            "Block nonzeros =    2, MFLOP/s: min =     767.85, avg =     822.91, max =     861.93; "
+            "y-vector sum: 7.381974950000000e+09\n")
+    got = bench.block_kernel_lines(text)
+    assert [g["bnnz"] for g in got] == [1, 2]
+    assert got[0] == {"bnnz": 1, "mflops_min": 425.55, "mflops_avg": 430.74, "mflops_max": 436.6,
+                      "y_sum": 4.6976204e9}
+    assert bench.block_kernel_lines("") == []
