@@ -85,6 +85,47 @@ def block_size_storage(rows, cols, m: int, n: int, allow_csr: bool = True, value
     return bits, int(best.value)
 
 
+MMF_COLUMNS = ("coo32", "csr32", "coo", "csr", "bitmap", "dense", "abhsf", "abhsf134")
+
+
+def mmf_table(hists: dict, m: int, n: int, nnz: int, matrix_type: str = "real") -> dict:
+    """The 64 lines of the reference's mmf-single and mmf-double
+    (block_statistics/mmf.cpp:53-138) from the 64 block histograms
+    (matrix.block_histograms_all, one GPU call): {(h, w): (single[8],
+    double[8])}, columns MMF_COLUMNS, bits with values included."""
+    from .matrix import mmf_line
+    out = {}
+    for key, h in hists.items():
+        r, s = (int(t) for t in key.split("x"))
+        out[(r, s)] = tuple(mmf_line(m, n, nnz, matrix_type, r, s, h))
+    return out
+
+
+def min_bss(table: dict, precision: str = "double") -> dict:
+    """One matrix's column of the reference's mmf-bss-single / -double
+    (block_statistics/min-bss.cpp:35-55): per block size (h, w), ascending,
+    the least storage over the coo, csr, bitmap, dense and abhsf columns."""
+    i = {"single": 0, "double": 1}[precision]
+    return {bs: min(lines[i][2:7]) for bs, lines in sorted(table.items())}
+
+
+def block_opt(table: dict, precision: str = "double") -> tuple[tuple[int, int], str, int]:
+    """mmf_t::block_opt (block_statistics/mmf.h:77-102): the least storage
+    over every block size and the coo .. abhsf columns, visited in the
+    reference's order (block sizes ascending by (h, w), then the columns),
+    the first strict minimum kept.  Returns ((h, w), column, bits)."""
+    i = {"single": 0, "double": 1}[precision]
+    best = None
+    for bs, lines in sorted(table.items()):
+        for k in range(2, 7):
+            v = lines[i][k]
+            if best is None or v < best[2]:
+                best = (bs, MMF_COLUMNS[k], v)
+    if best is None:
+        raise ValueError("empty table")
+    return best
+
+
 def features(rows, cols, m: int, n: int, stream=None) -> np.ndarray:
     """The selector's 12 features of a matrix (float32), computed on the GPU."""
     rows, cols, nnz, rp, cp, on_dev = _coo_args(rows, cols)

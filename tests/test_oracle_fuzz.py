@@ -117,3 +117,43 @@ def test_generated_matrices_spmv_bits_match_reference_csr(mat, s, seed):
     y_omp = y0.copy()
     b.spmv_omp(x, y_omp)
     np.testing.assert_array_equal(y_omp, y_ref)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DIR, "min-bss")), reason="reference min-bss not built")
+@hyp.settings(max_examples=8, deadline=None, derandomize=True)
+@hyp.given(mats=st.lists(matrices(), min_size=1, max_size=4))
+def test_generated_matrices_match_min_bss(mats):
+    """The reference's min-bss over several matrices at once (one directory
+    each, as block_statistics/min-bss.cpp reads them): its mmf-bss-single /
+    -double columns equal selector.min_bss of the library's mmf table, and
+    block_opt is the least of them."""
+    from abhsf_b200 import selector
+    with tempfile.TemporaryDirectory() as d:
+        ours = {}
+        for i, (m, n, rows, cols, vals) in enumerate(mats):
+            sub = os.path.join(d, f"m{i}")
+            os.mkdir(sub)
+            reference_stats(m, n, rows, cols, vals, sub)
+            hists = {f"{1 << k}x{1 << l}": oracle.block_histogram(rows, cols, k, l)
+                     for k in range(1, 9) for l in range(1, 9)}
+            ours[f"m{i}"] = selector.mmf_table(hists, m, n, rows.size)
+        subprocess.run([os.path.join(REF_DIR, "min-bss")], cwd=d, check=True, stdout=subprocess.DEVNULL)
+        for prec in ("single", "double"):
+            text = open(os.path.join(d, "mmf-bss-" + prec)).read().split("\n")
+            names = text[0].split()[2:]
+            assert names == sorted(ours)
+            ref = {}
+            for line in text[1:]:
+                t = line.split()
+                if t:
+                    ref[(int(t[0]), int(t[1]))] = [int(v) for v in t[2:]]
+            assert len(ref) == 64
+            for j, name in enumerate(names):
+                mb = selector.min_bss(ours[name], prec)
+                assert list(mb) == sorted(ref)
+                assert [mb[bs] for bs in sorted(ref)] == [ref[bs][j] for bs in sorted(ref)]
+                (h, w), col, bits = selector.block_opt(ours[name], prec)
+                assert bits == min(mb.values()) and mb[(h, w)] == bits
+                first = next(bs for bs in sorted(mb) if mb[bs] == bits)  # strict '<': the first size wins
+                assert (h, w) == first
+                assert ours[name][(h, w)][{"single": 0, "double": 1}[prec]][selector.MMF_COLUMNS.index(col)] == bits
