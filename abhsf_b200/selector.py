@@ -126,6 +126,48 @@ def block_opt(table: dict, precision: str = "double") -> tuple[tuple[int, int], 
     return best
 
 
+def min_schemes(table: dict, precision: str = "double") -> tuple[list[int], tuple[int, int]]:
+    """One matrix's line of the reference's mmf-schemes-single / -double
+    (block_statistics/min-schemes.cpp:24-44): each of the eight mmf columns'
+    least storage over all 64 block sizes, and block_opt's block size."""
+    i = {"single": 0, "double": 1}[precision]
+    mins = [min(r[i][k] for r in table.values()) for k in range(8)]
+    return mins, block_opt(table, precision)[0]
+
+
+def _size_sets() -> dict[str, list[tuple[int, int]]]:
+    """The restricted block-size sets of block_statistics/consistency.cpp:101-123."""
+    b8 = [(h, h) for h in (2, 4, 8, 16, 32, 64, 128, 256)]
+    b14 = sorted(set(b8) | {(h, w) for h in (4, 8, 16) for w in (4, 8, 16)})
+    b20 = sorted(set(b8) | {(h, w) for h in (4, 8, 16, 32) for w in (4, 8, 16, 32)})
+    b64 = [(h, w) for h in (2, 4, 8, 16, 32, 64, 128, 256) for w in (2, 4, 8, 16, 32, 64, 128, 256)]
+    return {"B_64": b64, "B_20": b20, "B_14": b14, "B_8": b8}
+
+
+def consistency(tables: list[dict], scheme: str = "adaptive", precision: str = "double") -> dict:
+    """The reference's consistency study (block_statistics/consistency.cpp:
+    56-188) over matrices' mmf tables: per matrix the least storage over all
+    64 sizes and the coo, csr, bitmap, dense and abhsf columns; the storage
+    at a block size is abhsf134 ("adaptive") or the least of coo, bitmap and
+    dense plus 2 tag bits ("min-fixed"), both without CSR; for each of the
+    size sets B_64, B_20, B_14 and B_8 the excess of the set's best size
+    over that least storage, in percent: {set: (average, maximum)}."""
+    i = {"single": 0, "double": 1}[precision]
+    if scheme not in ("adaptive", "min-fixed"):
+        raise ValueError("scheme: adaptive or min-fixed")
+    sets = _size_sets()
+    acc = {k: [] for k in sets}
+    for t in tables:
+        least = min(min(min(r[i][2:6]), r[i][6]) for r in t.values())
+        at = {}
+        for bs, r in t.items():
+            coo, csr, bitmap, dense, abhsf, abhsf134 = r[i][2:8]
+            at[bs] = min(coo, bitmap, dense) + 2 if scheme == "min-fixed" else abhsf134
+        for k, members in sets.items():
+            acc[k].append((min(at[bs] for bs in members) - least) / least * 100.0)
+    return {k: (float(np.mean(v)), float(np.max(v))) for k, v in acc.items()}
+
+
 def features(rows, cols, m: int, n: int, stream=None) -> np.ndarray:
     """The selector's 12 features of a matrix (float32), computed on the GPU."""
     rows, cols, nnz, rp, cp, on_dev = _coo_args(rows, cols)

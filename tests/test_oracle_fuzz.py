@@ -157,3 +157,63 @@ def test_generated_matrices_match_min_bss(mats):
                 first = next(bs for bs in sorted(mb) if mb[bs] == bits)  # strict '<': the first size wins
                 assert (h, w) == first
                 assert ours[name][(h, w)][{"single": 0, "double": 1}[prec]][selector.MMF_COLUMNS.index(col)] == bits
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DIR, "consistency")), reason="reference consistency not built")
+@hyp.settings(max_examples=6, deadline=None, derandomize=True)
+@hyp.given(mats=st.lists(matrices(), min_size=2, max_size=5))
+def test_generated_matrices_match_consistency(mats):
+    """The reference's consistency program over all the matrices (both
+    schemes, both precisions): its B_64 / B_20 / B_14 / B_8 average and
+    maximum excess equal selector.consistency of the library's mmf tables
+    (to the 6 digits it prints)."""
+    import re
+
+    from abhsf_b200 import selector
+    with tempfile.TemporaryDirectory() as d:
+        tables = []
+        for i, (m, n, rows, cols, vals) in enumerate(mats):
+            sub = os.path.join(d, f"m{i}")
+            os.mkdir(sub)
+            reference_stats(m, n, rows, cols, vals, sub)
+            hists = {f"{1 << k}x{1 << l}": oracle.block_histogram(rows, cols, k, l)
+                     for k in range(1, 9) for l in range(1, 9)}
+            tables.append(selector.mmf_table(hists, m, n, rows.size))
+        for scheme, sname in ((0, "min-fixed"), (1, "adaptive")):
+            for prec, pname in ((0, "single"), (1, "double")):
+                r = subprocess.run([os.path.join(REF_DIR, "consistency"), str(scheme), str(prec), str(len(mats))],
+                                   cwd=d, check=True, capture_output=True, text=True)
+                text = re.sub(r"\x1b\[[0-9;]*m", "", r.stdout)
+                ref = {k: (float(a), float(b)) for k, a, b in
+                       re.findall(r"(B_\d+): Average = ([0-9.eE+-]+), Maximum = ([0-9.eE+-]+)", text)}
+                ours = selector.consistency(tables, sname, pname)
+                assert set(ref) == set(ours)
+                for k in ref:
+                    for a, b in zip(ours[k], ref[k]):
+                        assert abs(a - b) <= 1e-5 * max(abs(b), 1e-3), (sname, pname, k, ours[k], ref[k])
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DIR, "min-schemes")), reason="reference min-schemes not built")
+@hyp.settings(max_examples=6, deadline=None, derandomize=True)
+@hyp.given(mats=st.lists(matrices(), min_size=1, max_size=4))
+def test_generated_matrices_match_min_schemes(mats):
+    """The reference's min-schemes lines (each column's least storage over
+    the 64 sizes, and block_opt's size) equal selector.min_schemes."""
+    from abhsf_b200 import selector
+    with tempfile.TemporaryDirectory() as d:
+        ours = {}
+        for i, (m, n, rows, cols, vals) in enumerate(mats):
+            sub = os.path.join(d, f"m{i}")
+            os.mkdir(sub)
+            reference_stats(m, n, rows, cols, vals, sub)
+            hists = {f"{1 << k}x{1 << l}": oracle.block_histogram(rows, cols, k, l)
+                     for k in range(1, 9) for l in range(1, 9)}
+            ours[f"m{i}"] = selector.mmf_table(hists, m, n, rows.size)
+        subprocess.run([os.path.join(REF_DIR, "min-schemes")], cwd=d, check=True, stdout=subprocess.DEVNULL)
+        for prec in ("single", "double"):
+            lines = [l.split() for l in open(os.path.join(d, "mmf-schemes-" + prec)) if l.strip()]
+            assert sorted(l[0] for l in lines) == sorted(ours)
+            for l in lines:
+                mins, (h, w) = selector.min_schemes(ours[l[0]], prec)
+                assert [int(v) for v in l[1:9]] == mins
+                assert (int(l[9]), int(l[10])) == (h, w)
