@@ -217,3 +217,23 @@ def test_generated_matrices_match_min_schemes(mats):
                 mins, (h, w) = selector.min_schemes(ours[l[0]], prec)
                 assert [int(v) for v in l[1:9]] == mins
                 assert (int(l[9]), int(l[10])) == (h, w)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DIR, "rows-nnz-stdev")), reason="rows-nnz-stdev not built")
+@hyp.settings(max_examples=20, deadline=None, derandomize=True)
+@hyp.given(mat=matrices())
+def test_generated_matrices_row_stdev_matches_rows_nnz_stdev(mat):
+    """The selector's row-count feature is the population standard deviation
+    the reference's rows-nnz-stdev prints (from block_stats' rows_nnz_stored),
+    to the 6 digits it prints; also as a share of n."""
+    from oracle import selector_oracle
+    m, n, rows, cols, vals = mat
+    with tempfile.TemporaryDirectory() as d:
+        reference_stats(m, n, rows, cols, vals, d)
+        r = subprocess.run([os.path.join(REF_DIR, "rows-nnz-stdev")], cwd=d, check=True, capture_output=True,
+                           text=True)
+    ref_stored, ref_all, ref_pct, _ = (float(t) for t in r.stdout.split())
+    std = 2.0 ** selector_oracle.features(rows, cols, m, n)[3] - 1.0
+    assert abs(std - ref_stored) <= 1e-5 * ref_stored + 1e-9
+    assert ref_all == ref_stored  # general matrices: nothing mirrored
+    assert abs(std / n * 100.0 - ref_pct) <= 1e-5 * ref_pct + 1e-9
