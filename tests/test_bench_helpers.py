@@ -9,7 +9,11 @@ import bench
 
 
 def test_peak_is_the_measured_copy_bandwidth():
-    with open(os.path.join(bench.ROOT, "MEASURED_PEAKS.json")) as f:
+    p = os.path.join(bench.ROOT, "MEASURED_PEAKS.json")
+    if not os.path.exists(p):  # the file is written per machine; without it the stated fallback
+        assert bench.hbm_peak() == (bench.FALLBACK_HBM_GBS, "fallback")
+        return
+    with open(p) as f:
         want = float(json.load(f)["hbm_gbs"])
     assert bench.hbm_peak() == (want, "measured")
 
