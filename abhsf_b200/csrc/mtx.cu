@@ -56,7 +56,7 @@ struct chunk_out {
     std::vector<int64_t> rows, cols;
     std::vector<double> vals;
     int64_t entries = 0, zeros = 0;
-    bool lower = false, upper = false, bad = false, range = false;
+    bool lower = false, upper = false, bad = false, range = false, oom = false;
 };
 
 inline bool is_space(char c)
@@ -111,6 +111,8 @@ inline bool read_value(const char*& p, const char* e, double& v)
 // Entries of buf[b, e) (whole lines), at most `limit` of them.
 void parse_chunk(const char* b, const char* e, bool pattern, int64_t m, int64_t n, int64_t limit, chunk_out& o)
 {
+    if (e <= b)
+        return;
     // about 24 bytes per entry line in the files this reads; growth past it is amortised
     const size_t guess = size_t(e - b) / 24 + 16;
     o.rows.reserve(guess);
@@ -226,8 +228,10 @@ void read_mtx(const char* path, int threads, abhsf_coo_host& out)
             fail(ABHSF_ERROR_INVALID_VALUE, "could not retrieve matrix sizes");
         break;
     }
-    // entry lines: split the rest at line ends over the threads
-    const size_t rest = pos <= buf.size() ? buf.size() - pos : 0;
+    // entry lines: split the rest at line ends over the threads (a size line
+    // without a line end leaves pos one past the buffer)
+    pos = std::min(pos, buf.size());
+    const size_t rest = buf.size() - pos;
     int T = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
     T = (int)std::max<size_t>(1, std::min<size_t>((size_t)T, rest / (1 << 20) + 1));
     std::vector<size_t> cut(T + 1, pos);
@@ -244,11 +248,18 @@ void read_mtx(const char* path, int threads, abhsf_coo_host& out)
         std::vector<std::thread> pool;
         for (int t = 0; t < T; ++t)
             pool.emplace_back([&, t] {
-                parse_chunk(buf.data() + cut[t], buf.data() + cut[t + 1], pattern, m, n, (int64_t)nnz, parts[t]);
+                try {  // nothing may leave a worker thread
+                    parse_chunk(buf.data() + cut[t], buf.data() + cut[t + 1], pattern, m, n, (int64_t)nnz, parts[t]);
+                } catch (...) {
+                    parts[t].oom = true;
+                }
             });
         for (auto& th : pool)
             th.join();
     }
+    for (const chunk_out& c : parts)
+        if (c.oom)
+            fail(ABHSF_ERROR_OUT_OF_MEMORY, "host allocation failed while parsing");
     // the first nnz entries in file order, as the reference reads exactly nnz
     // (lines after them are not looked at)
     int64_t left = nnz, kept = 0;

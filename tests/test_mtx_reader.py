@@ -67,3 +67,18 @@ def test_reader_errors(tmp_path, text, exc):
 def test_missing_file():
     with pytest.raises(capi.InvalidValue):
         mx.read_mtx("/nonexistent/file.mtx")
+
+
+@pytest.mark.parametrize("threads", [1, 4])
+def test_size_line_without_line_end(tmp_path, threads):
+    """A file that ends on its size line: no elements (nnz 0), or too few."""
+    p = tmp_path / "a.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate real general\n1 1 0")
+    rows, cols, vals, m, n, _ = mx.read_mtx(str(p), threads)
+    assert rows.size == cols.size == vals.size == 0 and (m, n) == (1, 1)
+    p.write_text("%%MatrixMarket matrix coordinate real general\n3 3 2")
+    with pytest.raises(capi.InvalidValue):
+        mx.read_mtx(str(p), threads)
+    p.write_text("%%MatrixMarket matrix coordinate real general\n3 3 1\n2 3 4.5")  # last entry without line end
+    rows, cols, vals, _, _, _ = mx.read_mtx(str(p), threads)
+    assert rows.tolist() == [1] and cols.tolist() == [2] and vals.tolist() == [4.5]
