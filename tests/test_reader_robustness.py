@@ -77,3 +77,43 @@ def test_mtx_reader_on_noisy_files(text, threads):
         for a, b in zip(back[:3], res[:3]):
             np.testing.assert_array_equal(np.asarray(a).view(np.uint64) if a.dtype == np.float64 else a,
                                           np.asarray(b).view(np.uint64) if b.dtype == np.float64 else b)
+
+
+def _no_gpu() -> bool:
+    import torch
+    return not torch.cuda.is_available()
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="host-side validation check for machines without a GPU")
+@hyp.settings(max_examples=300, deadline=None, derandomize=True)
+@hyp.given(block_size=st.sampled_from([-1, 0, 1, 8, 16, 48, 64, 256, 512, 1 << 30]),
+           value_type=st.integers(-1, 4), allow_csr=st.integers(-1, 2), matrix_type=st.integers(-1, 4),
+           forced=st.integers(-2, 5), on_dev=st.integers(0, 1), sum_order=st.integers(-1, 2),
+           bits=st.sampled_from([-1, 0, 16, 32, 64, 1 << 40]), selector=st.integers(-1, 4),
+           reserved=st.integers(0, 1), nnz=st.integers(-1, 5), m=st.integers(-1, 70), n=st.integers(-1, 70),
+           null_rows=st.booleans())
+def test_build_validation_never_crashes(block_size, value_type, allow_csr, matrix_type, forced, on_dev, sum_order,
+                                        bits, selector, reserved, nnz, m, n, null_rows):
+    """abhsf_build with any options and sizes returns a status: invalid ones
+    are refused on the host, and on this machine (no GPU) every valid call
+    fails at the device with a status too.  on_dev is only ever set together
+    with NULL pointers here, which the library refuses before any device
+    work whenever nnz > 0."""
+    import ctypes as C
+    o = capi.BuildOpts()
+    capi.lib.abhsf_build_opts_default(C.byref(o))
+    o.block_size, o.value_type, o.allow_csr, o.matrix_type = block_size, value_type, allow_csr, matrix_type
+    o.forced_scheme, o.inputs_on_device, o.sum_order = forced, on_dev, sum_order
+    o.bits_per_value, o.selector, o.reserved = bits, selector, reserved
+    k = max(nnz, 0)
+    rows = np.zeros(max(k, 1), np.int64)
+    cols = np.arange(max(k, 1), dtype=np.int64)
+    vals = np.ones(max(k, 1))
+    use_null = null_rows or on_dev
+    h = C.c_void_p()
+    rc = capi.lib.abhsf_build(None if use_null else rows.ctypes.data, None if use_null else cols.ctypes.data,
+                              None if use_null else vals.ctypes.data, nnz, m, n, C.byref(o), None, C.byref(h))
+    if rc == 0:  # only on a GPU machine
+        assert capi.lib.abhsf_release(h) == 0
+    else:
+        assert isinstance(capi.lib.abhsf_last_error_string(), (bytes, str))
