@@ -156,12 +156,12 @@ def main():
             spmv[name + "__y"] = y
 
     c1 = W.laplacian_2d(512)
-    p = os.path.join(work, "config1.mtx")
+    p = os.path.join(work, "laplace2d_512.mtx")
     write_mtx(p, c1)
     stats["laplace2d_512"] = run_reference_stats(p)
     stats["laplace2d_512"]["field"] = "real"
     stats["laplace2d_512"]["symmetry"] = "general"
-    # reference CSR y on config 1 with x from seed 0 (stored as a checksum set:
+    # reference CSR y on the 512 x 512 2D Laplacian with x from seed 0 (stored as a checksum set:
     # the full vector is regenerated at test time and compared through these)
     x = W.rhs(c1.n, seed=0)
     y = np.zeros(c1.m)

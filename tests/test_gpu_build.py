@@ -65,11 +65,11 @@ def test_format_bit_exact_low_precision_values(gpu, vt, bits):
         A.release()
 
 
-def test_format_bit_exact_config1(gpu):
+def test_format_bit_exact_laplace2d_512(gpu):
     c = W.laplacian_2d(512)
     A = AbhsfMatrix.from_elements(c.rows, c.cols, c.vals, c.m, c.n, block_size=64)
     b = oracle.build(c.rows, c.cols, c.vals, c.m, c.n, 64)
-    assert_same_format(A, b, "config1")
+    assert_same_format(A, b, "laplace2d_512")
     st = A.stats()
     assert st["tiles"] == 19440
     assert st["tiles_per_scheme"] == {"coo": 7168 + 8176, "csr": 4096, "bitmap": 0, "dense": 0}

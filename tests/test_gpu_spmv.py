@@ -81,7 +81,7 @@ def test_spmv_matches_reference_csr_golden(gpu, order):
 
 
 @pytest.mark.parametrize("order", ["reference", "tree"])
-def test_spmv_config1_against_golden(gpu, order):
+def test_spmv_laplace2d_512_against_golden(gpu, order):
     c = W.laplacian_2d(512)
     x = W.rhs(c.n, 0)
     yr = golden_spmv()["laplace2d_512__y_seed0"]

@@ -40,7 +40,7 @@ def test_mmf_lines_match_reference_mmf(name):
         assert o1 == line1[2:] and o2 == line2[2:], (r, s)
 
 
-def test_known_answers_config1():
+def test_known_answers_laplace2d_512():
     g = STATS["laplace2d_512"]
     assert g["props"] == [262144, 262144, 1308672, 1308672, 1308672, 2, 3]
     assert g["bstats"]["64x64"] == {"1": 7168, "64": 8176, "190": 4096}
