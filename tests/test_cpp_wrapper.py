@@ -14,7 +14,9 @@ LIBDIR = os.path.join(ROOT, "abhsf_b200")
 
 def _build(tmp_path):
     exe = str(tmp_path / "wrapper_demo")
-    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), SRC, "-o", exe,
+    # the reference's own language level, warnings as errors
+    subprocess.run(["g++", "-std=c++11", "-Wall", "-Wextra", "-Werror", "-pedantic", "-O1", "-I",
+                    os.path.join(ROOT, "include"), SRC, "-o", exe,
                     "-L", LIBDIR, "-labhsf_b200", f"-Wl,-rpath,{LIBDIR}"], check=True)
     return exe
 
