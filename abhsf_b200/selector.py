@@ -155,6 +155,8 @@ def consistency(tables: list[dict], scheme: str = "adaptive", precision: str = "
     i = {"single": 0, "double": 1}[precision]
     if scheme not in ("adaptive", "min-fixed"):
         raise ValueError("scheme: adaptive or min-fixed")
+    if not tables:
+        raise ValueError("no matrices")
     sets = _size_sets()
     acc = {k: [] for k in sets}
     for t in tables:
