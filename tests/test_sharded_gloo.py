@@ -436,3 +436,31 @@ def test_gloo_sharded_matrix_class_both_exchanges():
         h_info, h_x = r["cg_halo"]
         assert a_info["converged"] and a_info == h_info
         np.testing.assert_array_equal(a_x.view(np.uint64), h_x.view(np.uint64))
+
+
+def test_partition_properties_on_generated_inputs():
+    hyp = pytest.importorskip("hypothesis")
+    st = pytest.importorskip("hypothesis.strategies")
+
+    @hyp.settings(max_examples=300, deadline=None, derandomize=True)
+    @hyp.given(m=st.integers(1, 5000), s=st.sampled_from([16, 32, 64, 128, 256]), world=st.integers(1, 9),
+               k=st.integers(0, 3000), seed=st.integers(0, 10 ** 6), use_weights=st.booleans())
+    def check(m, s, world, k, seed, use_weights):
+        rng = np.random.default_rng(seed)
+        rows = rng.integers(0, m, k)
+        M = -(-m // s)
+        w = rng.uniform(0, 5, M) if use_weights else None
+        parts = sharded.partition_block_rows(rows, m, s, world, w)
+        assert len(parts) == world and parts[0][0] == 0 and parts[-1][1] == m
+        per = w if use_weights else np.bincount(rows // s, minlength=M).astype(float)
+        got = []
+        for r, (a, b) in enumerate(parts):
+            assert 0 <= a <= b <= m and (a % s == 0 or a == m)
+            if r + 1 < world:
+                assert b == parts[r + 1][0]
+            got.append(per[a // s: -(-b // s)].sum() if b > a else 0.0)
+        assert abs(sum(got) - per.sum()) <= 1e-9 * max(per.sum(), 1.0)
+        # each cut lands at the first block row where the prefix reaches its target
+        assert max(got) <= per.sum() / world + (per.max() if per.size else 0.0) + 1e-9
+
+    check()
