@@ -319,6 +319,29 @@ def read_mtx(path: str, threads: int = 0):
     return _coo_result(c)
 
 
+def expand_symmetric(rows, cols, vals, symmetry: str):
+    """The whole matrix from the stored triangle of a symmetric, skew or
+    hermitian (real) file, as read_mtx returns it: every off-diagonal element
+    (i, j, v) gains its mirror (j, i, v), or (j, i, -v) for skew, the
+    pairs block_statistics/block_stats.cpp:122-127,183-188 count as
+    "nnz_all"; sorted row-major, ready for AbhsfMatrix.from_elements.  A
+    general matrix comes back unchanged."""
+    rows = np.asarray(rows, np.int64)
+    cols = np.asarray(cols, np.int64)
+    vals = np.asarray(vals, np.float64)
+    if symmetry == "general":
+        return rows, cols, vals
+    if symmetry not in ("symmetric", "skew", "hermitian"):
+        raise ValueError("symmetry: general, symmetric, skew or hermitian")
+    off = rows != cols
+    mv = -vals[off] if symmetry == "skew" else vals[off]
+    r = np.concatenate([rows, cols[off]])
+    c = np.concatenate([cols, rows[off]])
+    v = np.concatenate([vals, mv])
+    order = np.lexsort((c, r))
+    return r[order], c[order], v[order]
+
+
 def read_mm(path: str):
     """A binary .mm matrix file (the layout utils/mtx2mm/mtx2mm.cpp:102-135
     writes), returned as read_mtx returns the text file it was made from."""

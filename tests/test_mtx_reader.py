@@ -82,3 +82,32 @@ def test_size_line_without_line_end(tmp_path, threads):
     p.write_text("%%MatrixMarket matrix coordinate real general\n3 3 1\n2 3 4.5")  # last entry without line end
     rows, cols, vals, _, _, _ = mx.read_mtx(str(p), threads)
     assert rows.tolist() == [1] and cols.tolist() == [2] and vals.tolist() == [4.5]
+
+
+def test_expand_symmetric_counts_like_block_stats():
+    """The mirrored element count equals block_stats' "nnz_all" (props
+    field 5) for the golden symmetric matrix; skew negates the mirror; the
+    stored triangle of the fixture file expands to the full matrix."""
+    import json
+
+    from conftest import golden_matrices
+    props = json.load(open(os.path.join(GOLDEN, "block_stats.json")))["sym_lower"]["props"]
+    coo = golden_matrices()["sym_lower"]
+    r, c, v = mx.expand_symmetric(coo.rows, coo.cols, coo.vals, "symmetric")
+    assert (coo.nnz, r.size) == (props[3], props[4]) == (1293, 2576)
+    dense = np.zeros((coo.m, coo.n))
+    dense[r, c] = v
+    np.testing.assert_array_equal(dense, dense.T)
+    assert np.all(np.diff(r * coo.n + c) > 0)  # row-major, no duplicates
+    r, c, v = mx.expand_symmetric(coo.rows, coo.cols, coo.vals, "skew")
+    dense = np.zeros((coo.m, coo.n))
+    dense[r, c] = v
+    off = ~np.eye(coo.m, dtype=bool)
+    np.testing.assert_array_equal(dense[off], -dense.T[off])
+    rows, cols, vals, m, n, info = mx.read_mtx(os.path.join(GOLDEN, "mtx", "real_symmetric_lower.mtx"))
+    r, c, v = mx.expand_symmetric(rows, cols, vals, info["symmetry"])
+    assert r.size == 2 * rows.size - int((rows == cols).sum())
+    g = mx.expand_symmetric(rows, cols, vals, "general")
+    assert g[0] is not None and g[0].size == rows.size
+    with pytest.raises(ValueError):
+        mx.expand_symmetric(rows, cols, vals, "upper")
