@@ -554,6 +554,68 @@ def cpu_block_kernel_run(max_seconds: float = 25.0):
                       "each 5 random patterns x 8 timed products over 8192^2 blocks"}
 
 
+def ingest_run(c, max_entries: int = 3_000_000):
+    """Matrix Market ingest, the path's data loader: the first max_entries
+    elements of the workload written as a real general .mtx (17 significant
+    digits), read by abhsf_read_mtx on all host threads and by the
+    reference's read_mtx_real_or_binary (compiled from its sources into
+    oracle/_ref/libref_mtx.so), best of two reads each, MB/s of file."""
+    import ctypes as C
+    import tempfile
+
+    from abhsf_b200 import matrix as mx
+    k = min(int(max_entries), c.nnz)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "sample.mtx")
+        with open(p, "w") as f:
+            f.write(f"%%MatrixMarket matrix coordinate real general\n{c.m} {c.n} {k}\n")
+            step = 1 << 18
+            for a in range(0, k, step):
+                b = min(k, a + step)
+                f.write("\n".join(f"{i} {j} {v:.17g}" for i, j, v in
+                                  zip((c.rows[a:b] + 1).tolist(), (c.cols[a:b] + 1).tolist(), c.vals[a:b].tolist())))
+                f.write("\n")
+        size = os.path.getsize(p)
+        ours = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            got = mx.read_mtx(p)
+            ours.append(time.perf_counter() - t0)
+        out = {"entries": k, "file_bytes": size, "unit": "MB/s",
+               "abhsf_read_mtx": {"MB/s": size / min(ours) / 1e6, "s": min(ours), "threads": os.cpu_count()}}
+        lib = os.path.join(ROOT, "oracle", "_ref", "libref_mtx.so")
+        if os.path.exists(lib):
+            f_ = C.CDLL(lib).ref_mtx_read
+            f_.restype = C.c_long
+            rows = np.zeros(k, np.int64)
+            cols = np.zeros(k, np.int64)
+            vals = np.zeros(k)
+            m_, n_ = C.c_long(), C.c_long()
+            ref = []
+            # the reference's reader logs to stdout, which carries only the JSON line
+            sys.stdout.flush()
+            saved = os.dup(1)
+            null = os.open(os.devnull, os.O_WRONLY)
+            try:
+                os.dup2(null, 1)
+                for _ in range(2):
+                    t0 = time.perf_counter()
+                    cnt = f_(os.fsencode(p), C.byref(m_), C.byref(n_), C.c_long(k), rows.ctypes.data_as(C.c_void_p),
+                             cols.ctypes.data_as(C.c_void_p), vals.ctypes.data_as(C.c_void_p))
+                    ref.append(time.perf_counter() - t0)
+            finally:
+                os.dup2(saved, 1)
+                os.close(saved)
+                os.close(null)
+            same = (cnt == got[0].size and np.array_equal(rows[:cnt], got[0]) and np.array_equal(cols[:cnt], got[1])
+                    and np.array_equal(vals[:cnt].view(np.uint64), got[2].view(np.uint64)))
+            out["reference_reader"] = {"MB/s": size / min(ref) / 1e6, "s": min(ref), "threads": 1,
+                                       "same_elements": bool(same)}
+        else:
+            out["reference_reader"] = {"unavailable": "oracle/_ref/libref_mtx.so not built"}
+    return out
+
+
 def build_format_stats(c):
     """Format statistics without a GPU (for the reference arm): the oracle
     builder gives the same bytes as the device format."""
@@ -679,7 +741,7 @@ def run_ours(args):
         for key in ("batched", "one_by_one"):
             batched[key]["frac_of_peak"] = batched[key]["GB/s"] / peak
     achieved = B / (t_mean * 1e-3) / 1e9
-    cpu = cpu_abhsf = cpu_block = None
+    cpu = cpu_abhsf = cpu_block = ingest = None
     status = A.device_status()
     if status:
         raise RuntimeError(f"SpMV kernel reported device status {status}")
@@ -695,6 +757,11 @@ def run_ours(args):
                 cpu_block = cpu_block_kernel_run()
             except Exception as e:
                 cpu_block = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+        if not args.no_ingest:
+            try:
+                ingest = ingest_run(c)
+            except Exception as e:
+                ingest = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
     if rank == 0:
         line = {
             "metric": METRIC, "value": aggregate_rate(B, t_max * 1e-3, world), "unit": UNIT, "n_gpus": world,
@@ -718,6 +785,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "cpu_abhsf": cpu_abhsf,
             "cpu_block_kernel": cpu_block,
+            "ingest": ingest,
             "spmm": spmm,
             "lowprec": lowprec,
             "cg": cg_times,
@@ -743,6 +811,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ingest", action="store_true",
+                    help="skip the Matrix Market ingest timing (ours against the reference's reader, 3M entries)")
     ap.add_argument("--no-block-kernel", action="store_true",
                     help="skip the reference's 4 x 4 bitmap block micro-baseline (25 s on one host core)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")

@@ -66,3 +66,25 @@ def test_block_kernel_lines_parse():
     assert got[0] == {"bnnz": 1, "mflops_min": 425.55, "mflops_avg": 430.74, "mflops_max": 436.6,
                       "y_sum": 4.6976204e9}
     assert bench.block_kernel_lines("") == []
+
+
+def test_ingest_leg_keeps_stdout_to_the_json_line():
+    """The ingest leg times abhsf_read_mtx and, where it is built, the
+    reference's reader on the same sample file; they read the same elements,
+    and the reference reader's log does not reach stdout (which carries only
+    the bench's JSON line)."""
+    import subprocess
+    import sys
+    code = ("import sys, json; sys.path.insert(0, %r)\n"
+            "import bench\n"
+            "from abhsf_b200 import workloads as W\n"
+            "r = bench.ingest_run(W.tiled_mixture(n=65536), 20000)\n"
+            "print(json.dumps(r))\n") % bench.ROOT
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = p.stdout.strip().splitlines()
+    assert len(lines) == 1
+    r = json.loads(lines[0])
+    assert r["entries"] > 0 and r["abhsf_read_mtx"]["MB/s"] > 0
+    ref = r["reference_reader"]
+    assert "unavailable" in ref or ref["same_elements"] is True
