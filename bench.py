@@ -467,8 +467,8 @@ def cpu_reference_run(c, bytes_per_step: float, max_seconds: float, max_iters: i
         t0 = time.time()
         R = oracle.RefCSR(c.rows, c.cols, c.vals, c.m, c.n)
         log(f"reference CSR built in {time.time() - t0:.1f} s")
-        R.spmv(x, y)  # warm-up
-        R.spmv(x, y)
+        for _ in range(4):  # warmup_iters, spmv/bottlenecks/spmv.cpp:33 (then up to its n_iters = 40)
+            R.spmv(x, y)
         times = []
         t_start = time.perf_counter()
         while len(times) < max_iters and time.perf_counter() - t_start < max_seconds:
