@@ -58,8 +58,28 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         return LIB
     os.makedirs(OBJ, exist_ok=True)
     extra = extra or []
+    # a source is recompiled when it, a shared header or the flags changed
+    headers = [d for d in _deps() if not d.endswith(".cu")]
+    stamp = os.path.join(OBJ, "flags.txt")
+    flags = " ".join(FLAGS + extra)
+    same_flags = os.path.exists(stamp) and open(stamp).read() == flags
+
+    def fresh(src: str) -> bool:
+        obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
+        if force or not same_flags or not os.path.exists(obj):
+            return False
+        t = os.path.getmtime(obj)
+        return all(os.path.getmtime(d) <= t for d in [src] + headers)
+
+    def one(src: str) -> str:
+        if fresh(src):
+            return os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
+        return _compile(src, verbose, extra)
+
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose, extra), _sources()))
+        objs = list(ex.map(one, _sources()))
+    with open(stamp, "w") as f:
+        f.write(flags)
     tmp = LIB + ".tmp"
     cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart", "static"]
     if verbose:

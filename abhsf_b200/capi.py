@@ -102,6 +102,7 @@ PROTOTYPES = {
     "abhsf_device_status": (C.c_int, [_vp, _vp, _i32, C.POINTER(_i32)]),
     "abhsf_test_set_hooks": (None, [_i64, C.c_uint32]),
     "abhsf_test_ring_variant": (C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32)]),
+    "abhsf_test_device_allocations": (_i64, []),
     "abhsf_last_error_string": (C.c_char_p, []),
     "abhsf_build_opts_default": (None, [C.POINTER(BuildOpts)]),
     "abhsf_build": (C.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, C.POINTER(BuildOpts), _vp, C.POINTER(_vp)]),

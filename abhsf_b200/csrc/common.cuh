@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -58,6 +59,14 @@ abhsf_status guarded(F&& f) noexcept
     }
 }
 
+// Device allocations made by dbuf since the library was loaded (read by the
+// test hook abhsf_test_device_allocations).
+inline std::atomic<int64_t>& dbuf_allocations()
+{
+    static std::atomic<int64_t> count{0};
+    return count;
+}
+
 // Owning device allocation (cudaMalloc / cudaFree).
 template <typename T>
 class dbuf {
@@ -83,6 +92,7 @@ class dbuf {
         if (count == 0)
             count = 1;
         ABHSF_CUDA(cudaMalloc(reinterpret_cast<void**>(&p_), count * sizeof(T)));
+        dbuf_allocations().fetch_add(1, std::memory_order_relaxed);
         n_ = count;
     }
     void reset()

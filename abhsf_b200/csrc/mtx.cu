@@ -138,7 +138,8 @@ void parse_chunk(const char* b, const char* e, bool pattern, int64_t m, int64_t 
         while (p < e && *p != '\n')  // the rest of the line (a complex part, a comment) is not read
             ++p;
         ++o.entries;
-        if (r < 1 || c < 1 || (int64_t)r > m || (int64_t)c > n) {
+        // unsigned compares: a signed index ("-1") wraps to 2^64 - 1 and fails r <= m
+        if (r < 1 || c < 1 || r > (unsigned long long)m || c > (unsigned long long)n) {
             o.range = true;
             return;
         }

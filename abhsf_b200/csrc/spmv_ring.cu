@@ -1607,3 +1607,5 @@ extern "C" void abhsf_test_set_hooks(int64_t drop_desc, uint32_t spin_limit)
     abhsf::g_drop_desc = drop_desc < 0 ? -1 : drop_desc;
     abhsf::g_spin_limit = spin_limit;
 }
+
+extern "C" int64_t abhsf_test_device_allocations(void) { return abhsf::dbuf_allocations().load(); }

@@ -323,8 +323,11 @@ ABHSF_API abhsf_status abhsf_block_histogram_all(const int64_t* rows, const int6
  * scratch is one 64 MiB array inside the library's device image, held by
  * every GPU that loads the library until the process exits.  The first call
  * on a device looks up that array's device address, so make it before any
- * stream capture.  All calls share the array: calls whose GPU work overlaps
- * (other streams, other host threads) race on it.  Synchronises stream. */
+ * stream capture.  The address is kept for the life of the process: after a
+ * cudaDeviceReset of that device the kept address is stale, so do not call
+ * this entry point again in that process.  All calls share the array: calls
+ * whose GPU work overlaps (other streams, other host threads) race on it.
+ * Synchronises stream. */
 ABHSF_API abhsf_status abhsf_block_histogram_noalloc(const int64_t* rows, const int64_t* cols, int64_t nnz,
                                                      int64_t m, int64_t n, int32_t r, int32_t s,
                                                      abhsf_stream_t stream, uint64_t* hist, int64_t hist_len,

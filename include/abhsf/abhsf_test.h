@@ -32,6 +32,11 @@ ABHSF_API void abhsf_test_set_hooks(int64_t drop_desc, uint32_t spin_limit);
  * thread-safe with SpMVs of the same matrix. */
 ABHSF_API abhsf_status abhsf_test_ring_variant(abhsf_matrix* a, int32_t set, int32_t* layout, int32_t* bulk);
 
+/* Device allocations (cudaMalloc) the library has made since it was loaded,
+ * so that a test can check that an entry point which promises to allocate
+ * nothing keeps that promise. */
+ABHSF_API int64_t abhsf_test_device_allocations(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,7 +8,7 @@ own programs, compiled from the reference sources by ``make -C oracle ref``:
 * ``oracle/_ref/libref_csr.so`` (csr_matrix::spmv_naive,
   spmv/bottlenecks/spmv.cpp:58-64) -> y += A x for seeded x and y.
 
-Needs the reference tree (REF, default /root/reference) and is run by hand in
+Needs the reference tree (REF, default: a "reference" directory beside the repository) and is run by hand in
 the development container; the fixtures it writes are committed, so nothing
 at test time reads the reference.
 
@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 from abhsf_b200 import workloads as W  # noqa: E402
 from oracle import oracle  # noqa: E402
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF") or os.path.join(os.path.dirname(ROOT), "reference")
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 

@@ -148,15 +148,3 @@ def test_cost_model_exhaustive_small_blocks():
                             assert capi.SCHEME_NAMES.index(got) == oracle.select_scheme(r, s, z, bits, binary,
                                                                                         allow), (r, s, z)
 
-
-def test_every_declared_entry_point_has_an_integration_row():
-    """Each function the C ABI declares is listed with the reference
-    interface it replaces (or says it has none) in the integration guide."""
-    import os
-    import re
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    h = open(os.path.join(root, "include", "abhsf", "abhsf_gpu.h")).read()
-    names = sorted(set(re.findall(r"ABHSF_API\s+[\w\s\*]+?\b(abhsf_\w+)\s*\(", h)))
-    assert len(names) > 30
-    doc = open(os.path.join(root, "INTEGRATION.md")).read()
-    assert [n for n in names if f"`{n}`" not in doc] == []

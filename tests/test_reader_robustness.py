@@ -117,3 +117,19 @@ def test_build_validation_never_crashes(block_size, value_type, allow_csr, matri
         assert capi.lib.abhsf_release(h) == 0
     else:
         assert isinstance(capi.lib.abhsf_last_error_string(), (bytes, str))
+
+
+@pytest.mark.parametrize("threads", [1, 4])
+@pytest.mark.parametrize("entry", ["-1 2 4.5", "2 -3 1.0", "-0 1 1.0", "18446744073709551615 1 2.0"])
+def test_mtx_reader_refuses_signed_and_wrapped_indices(entry, threads):
+    """An index written with a sign, or one that only fits after wrapping,
+    lies outside m x n: the reference's fscanf("%lu") reads "-1" as 2^64 - 1,
+    which is not a row of a 3 x 3 matrix."""
+    text = f"%%MatrixMarket matrix coordinate real general\n3 3 2\n1 1 1.0\n{entry}\n"
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "a.mtx")
+        with open(p, "w") as f:
+            f.write(text)
+        with pytest.raises(capi.AbhsfError) as e:
+            mx.read_mtx(p, threads)
+        assert e.value.status == capi.INDEX_OUT_OF_RANGE

@@ -53,6 +53,38 @@ def test_noalloc_histogram_equals_allocating_histogram_on_consecutive_calls(gpu)
         assert int((h_ref * np.arange(h_ref.size, dtype=np.uint64)).sum()) == coo.nnz
 
 
+def test_noalloc_histogram_makes_no_device_allocation(gpu):
+    """After its first call on the device (which looks up the scratch array's
+    address), a call makes no cudaMalloc inside the library and leaves the
+    device's free memory as it was: the property the entry point exists for."""
+    import torch
+    coo = W.random_blocky(4000, 5000, 64, 300, seed=43)
+    stream = torch.cuda.current_stream().cuda_stream
+    rows = torch.from_numpy(coo.rows).cuda()
+    cols = torch.from_numpy(coo.cols).cuda()
+    hist = np.zeros(64 * 64 + 1, dtype=np.uint64)
+
+    def call():
+        capi.check(capi.lib.abhsf_block_histogram_noalloc(rows.data_ptr(), cols.data_ptr(), coo.nnz, coo.m, coo.n,
+                                                          64, 64, stream, hist.ctypes.data_as(capi._u64p),
+                                                          hist.size, None))
+
+    call()  # set-up on this device
+    torch.cuda.synchronize()
+    before = capi.lib.abhsf_test_device_allocations()
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    assert capi.lib.abhsf_test_device_allocations() == before
+    assert torch.cuda.mem_get_info()[0] == free_before
+    # the counter does see the allocating histogram's scratch
+    blocks = C.c_int64(-1)
+    capi.check(capi.lib.abhsf_block_histogram(rows.data_ptr(), cols.data_ptr(), coo.nnz, coo.m, coo.n, 64, 64, 1,
+                                              stream, hist.ctypes.data_as(capi._u64p), hist.size, C.byref(blocks)))
+    assert capi.lib.abhsf_test_device_allocations() > before
+
+
 def test_noalloc_histogram_rejects_inputs_beyond_its_limit(gpu):
     import torch
     n = capi.NOALLOC_MAX_NNZ + 1
