@@ -67,7 +67,7 @@ class BuildOpts(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("value_type", C.c_int32), ("allow_csr", C.c_int32),
                 ("matrix_type", C.c_int32), ("forced_scheme", C.c_int32), ("inputs_on_device", C.c_int32),
                 ("sum_order", C.c_int32), ("bits_per_value", C.c_int64), ("selector", C.c_int32),
-                ("reserved", C.c_int32), ("selector_model", C.c_void_p)]
+                ("slice_tile_nnz", C.c_int32), ("selector_model", C.c_void_p)]
 
 
 class CooHost(C.Structure):
@@ -103,6 +103,8 @@ PROTOTYPES = {
     "abhsf_test_set_hooks": (None, [_i64, C.c_uint32]),
     "abhsf_test_ring_variant": (C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32)]),
     "abhsf_test_device_allocations": (_i64, []),
+    "abhsf_slices_info": (C.c_int, [_vp] + [C.POINTER(_i64)] * 5),
+    "abhsf_slices_export": (C.c_int, [_vp] * 10),
     "abhsf_last_error_string": (C.c_char_p, []),
     "abhsf_build_opts_default": (None, [C.POINTER(BuildOpts)]),
     "abhsf_build": (C.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, C.POINTER(BuildOpts), _vp, C.POINTER(_vp)]),

@@ -569,6 +569,8 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
         fail(ABHSF_ERROR_INVALID_VALUE, "forced_scheme must be -1 or 0..3");
     if (o.sum_order != ABHSF_SUM_REFERENCE && o.sum_order != ABHSF_SUM_TREE)
         fail(ABHSF_ERROR_INVALID_VALUE, "sum_order must be ABHSF_SUM_REFERENCE or ABHSF_SUM_TREE");
+    if (o.slice_tile_nnz < -1)
+        fail(ABHSF_ERROR_INVALID_VALUE, "slice_tile_nnz must be -1, 0 or positive");
     const bool binary = (o.matrix_type == ABHSF_MATRIX_BINARY);
     if (binary && o.forced_scheme == ABHSF_SCHEME_DENSE)
         fail(ABHSF_ERROR_INVALID_VALUE, "dense scheme is never used for binary matrices");
@@ -590,6 +592,7 @@ void build_matrix(const int64_t* rows, const int64_t* cols, const double* vals, 
     a.m = m; a.n = n; a.nnz = nnz; a.s = (int32_t)s; a.lg = lg;
     a.value_type = o.value_type; a.matrix_type = o.matrix_type;
     a.sum_order = o.sum_order;
+    a.dc_avg = o.slice_tile_nnz < 0 ? 0.f : o.slice_tile_nnz == 0 ? kSliceTileNnzDefault : (float)o.slice_tile_nnz;
     a.M = M; a.N = N;
     ABHSF_CUDA(cudaGetDevice(&a.device));
 

@@ -79,7 +79,7 @@ void abhsf_build_opts_default(abhsf_build_opts* o)
     o->sum_order = ABHSF_SUM_REFERENCE;
     o->bits_per_value = 0;
     o->selector = ABHSF_SELECT_MINBSS;
-    o->reserved = 0;
+    o->slice_tile_nnz = 0;
     o->selector_model = nullptr;
 }
 

@@ -124,6 +124,10 @@ struct tiles_view {
     const void* values;
 };
 
+// Mean elements per tile up to which a block row goes to the delta-coded
+// row slices unless abhsf_build_opts.slice_tile_nnz says otherwise.
+constexpr float kSliceTileNnzDefault = 32.f;
+
 inline int log2_exact(int64_t s)
 {
     int lg = 0;
@@ -184,6 +188,24 @@ struct abhsf_matrix {
     int ring_warps = 0;  // CTAs of the ring kernel; 0: the streaming kernel serves this matrix
     int ring_layout = 0;  // consumer layout of its single-right-hand-side launches (timed at build)
     int ring_bulk = 0;   // x / y blocks as bulk copies (timed at build)
+    bool ring_ready = false;  // the ring kernel and the slice kernel together serve this matrix
+    // delta-coded row slices of the hypersparse block rows (spmv_stream.cu)
+    struct dc_slice_host {
+        int64_t base = 0;   // first slot of its words and values
+        int64_t meta = 0;   // sliced: first of its 32 lane records; chain: the row within the block row
+        uint32_t brow = 0, steps = 0, lanes = 0;
+        bool chain = false;
+    };
+    std::vector<dc_slice_host> dc_host;  // block rows ascending; per block row its chains, then its sliced rows
+    std::vector<uint8_t> dc_tree_flag;   // per non-empty block row (tree_rows order): served by the slices
+    abhsf::dbuf<uint32_t> dc_words;      // one word per slot (delta-coded columns)
+    abhsf::dbuf<uint8_t> dc_vals;        // the values in slot order
+    abhsf::dbuf<uint32_t> dc_lane;       // lane records: row << 24 | length
+    abhsf::dbuf<uint8_t> dc_sched;       // the matrix's own launch: slices in warp order
+    abhsf::dbuf<int64_t> dc_wbeg;
+    int dc_warps = 0;
+    int64_t dc_elements = 0, dc_rows = 0, dc_slots = 0, dc_lane_records = 0;
+    float dc_avg = 0.f;                  // largest mean elements per tile of a slice block row (0: none)
     abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
     // staging for abhsf_spmv_host
     abhsf::dbuf<double> x_stage, y_stage;
@@ -194,6 +216,9 @@ struct abhsf_matrix {
         abhsf::dbuf<uint8_t> desc;
         abhsf::dbuf<int64_t> wbeg;
         int ctas = 0;
+        abhsf::dbuf<uint8_t> dc_sched;  // the chunk's slices
+        abhsf::dbuf<int64_t> dc_wbeg;
+        int dc_warps = 0;
     };
     std::vector<host_chunk> host_chunks;
     bool host_ready = false;
@@ -240,4 +265,9 @@ struct abhsf_batch {
     int ctas = 0;
     int layout = 0;  // consumer layout of the ring kernel (timed at creation)
     int bulk = 0;   // x / y blocks as bulk copies (timed at creation)
+    // the matrices' delta-coded row slices, one launch (spmv_stream.cu)
+    abhsf::dbuf<uint8_t> dc_table;
+    abhsf::dbuf<uint8_t> dc_sched;
+    abhsf::dbuf<int64_t> dc_wbeg;
+    int dc_warps = 0;
 };

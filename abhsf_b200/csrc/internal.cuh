@@ -81,6 +81,20 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
 void prepare_batch(abhsf_batch& b, cudaStream_t st);
 void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);
 
+// Delta-coded row slices of the hypersparse block rows (spmv_stream.cu):
+// prepare_stream picks the block rows (no dense tile, at most `avg`
+// elements per tile on average), encodes them and deals the slices;
+// deal_slices deals the slices of block rows [brow_lo, brow_hi) of several
+// matrices over one launch; spmv_stream adds A x over the slice rows
+// (x[i * ldx], y[i * ldy]; the matrix's own schedule unless one is given).
+void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st);
+void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sched, dbuf<int64_t>& wbeg,
+                 int& warps, cudaStream_t st, int64_t brow_lo, int64_t brow_hi);
+bool spmv_stream(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int64_t ldy, cudaStream_t st,
+                 const uint8_t* sched = nullptr, const int64_t* wbeg = nullptr, int warps = 0);
+void prepare_batch_stream(abhsf_batch& b, cudaStream_t st);
+void batch_stream(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);
+
 // Conjugate gradients (cg.cu).
 void cg_solve(const abhsf_matrix& a, const double* b, double* x, double rtol, int max_iters, abhsf_cg_info* info,
               cudaStream_t st);

@@ -1283,11 +1283,28 @@ bool build_ring_schedule(const std::vector<const abhsf_matrix*>& mats, int col_b
         ABHSF_CUDA(cudaStreamSynchronize(st));
         mpv = std::max(mpv, m_pv);
     }
-    if (brow_lo > 0 || brow_hi < INT64_MAX) {  // only block rows [brow_lo, brow_hi)
+    // the slice kernel's block rows stay out (spmv_stream.cu)
+    std::vector<uint8_t> skip(rows.size(), 0);
+    bool any_skip = false;
+    {
+        size_t o = 0;
+        for (size_t i = 0; i < mats.size(); ++i) {
+            const auto& f = mats[i]->dc_tree_flag;
+            const int64_t nr = mats[i]->tree_nrows;
+            if (nr == 0)
+                continue;
+            for (int64_t k = 0; k < nr; ++k, ++o)
+                if ((size_t)k < f.size() && f[k]) {
+                    skip[o] = 1;
+                    any_skip = true;
+                }
+        }
+    }
+    if (brow_lo > 0 || brow_hi < INT64_MAX || any_skip) {  // only block rows [brow_lo, brow_hi)
         size_t o = 0;
         total_tiles = 0;
         for (size_t k = 0; k < rows.size(); ++k)
-            if (rows[k] >= brow_lo && rows[k] < brow_hi) {
+            if (rows[k] >= brow_lo && rows[k] < brow_hi && !skip[k]) {
                 rows[o] = rows[k];
                 ntiles[o] = ntiles[k];
                 wt[o] = wt[k];
@@ -1399,6 +1416,7 @@ void batch_launch(const abhsf_batch& b, const double* const* xs, double* const* 
 void prepare_ring(abhsf_matrix& a, cudaStream_t st)
 {
     a.ring_warps = 0;
+    a.ring_ready = false;
     if ((a.s != 32 && a.s != 64) || a.tree_nrows == 0 || a.M > (int64_t)kRowMask)
         return;
     if (a.value_type == ABHSF_VALUE_F64) {
@@ -1407,9 +1425,14 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
         else
             ring_set_up_all<64>();
     }
+    prepare_stream(a, a.dc_avg, st);
     int ctas = 0, mpv = 0;
-    if (!build_ring_schedule({&a}, 32, a.ring_desc, a.ring_wbeg, ctas, mpv, st))
-        return;  // the streaming kernel serves this matrix
+    if (!build_ring_schedule({&a}, 32, a.ring_desc, a.ring_wbeg, ctas, mpv, st)) {
+        // every block row is a slice row, or the ring's counters would overflow
+        a.ring_ready = a.dc_warps > 0 && a.dc_rows == a.tree_nrows;
+        return;  // else the streaming kernel serves this matrix
+    }
+    a.ring_ready = true;
     a.ring_max_pv = mpv;
     a.ring_warps = ctas;
     if (a.value_type == ABHSF_VALUE_F64)
@@ -1436,7 +1459,15 @@ void prepare_batch(abhsf_batch& b, cudaStream_t st)
     ABHSF_CUDA(cudaMemsetAsync(b.dev_status.get(), 0, sizeof(int), st));
     int mpv = 0;
     b.ctas = 0;
-    if (!build_ring_schedule(b.mats, kBatchColBits, b.desc, b.wbeg, b.ctas, mpv, st) && b.total_tiles > 0)
+    prepare_batch_stream(b, st);
+    int64_t ring_rows = 0;  // non-empty block rows left to the ring kernel
+    for (const abhsf_matrix* a : b.mats)
+        for (uint8_t f : a->dc_tree_flag)
+            ring_rows += f ? 0 : 1;
+    for (const abhsf_matrix* a : b.mats)
+        if (a->dc_tree_flag.size() != (size_t)a->tree_nrows)
+            ring_rows += a->tree_nrows;
+    if (!build_ring_schedule(b.mats, kBatchColBits, b.desc, b.wbeg, b.ctas, mpv, st) && ring_rows > 0)
         fail(ABHSF_ERROR_UNSUPPORTED, "batch too large for the ring kernel's per-CTA counters");
     if (b.ctas > 0) {
         // time the variants with every matrix reading one zero x and writing one scratch y
@@ -1472,48 +1503,52 @@ void prepare_batch(abhsf_batch& b, cudaStream_t st)
 
 void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st)
 {
-    if (b.ctas == 0)
-        return;
-    batch_launch(b, xs, ys, st, false);
+    if (b.ctas > 0)
+        batch_launch(b, xs, ys, st, false);
+    batch_stream(b, xs, ys, st);
 }
 
 
 
 bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
-    if (a.ring_warps == 0 || a.value_type != ABHSF_VALUE_F64)
+    if (!a.ring_ready || a.value_type != ABHSF_VALUE_F64)
         return false;
-    if (a.s == 32)
-        launch_ring<32, 1, ABHSF_VALUE_F64>(a, x, 1, y, 1, st);
-    else
-        launch_ring<64, 1, ABHSF_VALUE_F64>(a, x, 1, y, 1, st);
+    if (a.ring_warps) {
+        if (a.s == 32)
+            launch_ring<32, 1, ABHSF_VALUE_F64>(a, x, 1, y, 1, st);
+        else
+            launch_ring<64, 1, ABHSF_VALUE_F64>(a, x, 1, y, 1, st);
+    }
+    spmv_stream(a, x, 1, y, 1, st);
     return true;
 }
 
 bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st)
 {
-    if (a.ring_warps == 0)
+    if (!a.ring_ready || a.value_type == ABHSF_VALUE_F64)
         return false;
-    if (a.value_type == ABHSF_VALUE_F32) {
-        if (a.s == 32)
-            launch_ring<32, 1, ABHSF_VALUE_F32>(a, x, 1, y, 1, st);
-        else
-            launch_ring<64, 1, ABHSF_VALUE_F32>(a, x, 1, y, 1, st);
-    } else if (a.value_type == ABHSF_VALUE_BF16) {
-        if (a.s == 32)
-            launch_ring<32, 1, ABHSF_VALUE_BF16>(a, x, 1, y, 1, st);
-        else
-            launch_ring<64, 1, ABHSF_VALUE_BF16>(a, x, 1, y, 1, st);
-    } else {
-        return false;
+    if (a.ring_warps) {
+        if (a.value_type == ABHSF_VALUE_F32) {
+            if (a.s == 32)
+                launch_ring<32, 1, ABHSF_VALUE_F32>(a, x, 1, y, 1, st);
+            else
+                launch_ring<64, 1, ABHSF_VALUE_F32>(a, x, 1, y, 1, st);
+        } else {
+            if (a.s == 32)
+                launch_ring<32, 1, ABHSF_VALUE_BF16>(a, x, 1, y, 1, st);
+            else
+                launch_ring<64, 1, ABHSF_VALUE_BF16>(a, x, 1, y, 1, st);
+        }
     }
+    spmv_stream(a, x, 1, y, 1, st);
     return true;
 }
 
 bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
     constexpr int kChunks = 4;
-    if (a.ring_warps == 0 || a.value_type != ABHSF_VALUE_F64 || a.sum_order != ABHSF_SUM_REFERENCE ||
+    if (!a.ring_ready || a.value_type != ABHSF_VALUE_F64 || a.sum_order != ABHSF_SUM_REFERENCE ||
         a.M < 4 * kChunks || a.m < (int64_t(1) << 20))
         return false;  // small matrices: one copy each way is as fast
     if (!a.host_ready) {
@@ -1524,8 +1559,10 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
             ch.brow0 = a.M * c / kChunks;
             ch.brow1 = a.M * (c + 1) / kChunks;
             int mpv = 0;
-            if (!build_ring_schedule({&a}, 32, ch.desc, ch.wbeg, ch.ctas, mpv, st, ch.brow0, ch.brow1))
-                ch.ctas = 0;  // no tiles in these block rows
+            if (a.ring_warps == 0 ||
+                !build_ring_schedule({&a}, 32, ch.desc, ch.wbeg, ch.ctas, mpv, st, ch.brow0, ch.brow1))
+                ch.ctas = 0;  // no ring tiles in these block rows
+            deal_slices({&a}, ch.dc_sched, ch.dc_wbeg, ch.dc_warps, st, ch.brow0, ch.brow1);
         }
         if (!a.host_in)
             ABHSF_CUDA(cudaStreamCreateWithFlags(&a.host_in, cudaStreamNonBlocking));
@@ -1559,6 +1596,8 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
             else
                 launch_ring<64, 1, ABHSF_VALUE_F64>(a, xs, 1, ys, 1, st, false, ch.desc.get(), ch.wbeg.get(), ch.ctas);
         }
+        if (ch.dc_warps > 0)
+            spmv_stream(a, xs, 1, ys, 1, st, ch.dc_sched.get(), ch.dc_wbeg.get(), ch.dc_warps);
         ABHSF_CUDA(cudaEventRecord(ev[1 + kChunks + c], st));
     }
     for (int c = 0; c < kChunks; ++c) {
@@ -1575,12 +1614,16 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
 bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,
                    cudaStream_t st)
 {
-    if (a.ring_warps == 0 || a.value_type != ABHSF_VALUE_F64)
+    if (!a.ring_ready || a.value_type != ABHSF_VALUE_F64)
         return false;
-    if (a.s == 32)
-        spmm_ring<32>(a, k, X, ldx, Y, ldy, st);
-    else
-        spmm_ring<64>(a, k, X, ldx, Y, ldy, st);
+    if (a.ring_warps) {
+        if (a.s == 32)
+            spmm_ring<32>(a, k, X, ldx, Y, ldy, st);
+        else
+            spmm_ring<64>(a, k, X, ldx, Y, ldy, st);
+    }
+    for (int j = 0; j < k && a.dc_warps; ++j)  // the slice rows, column by column
+        spmv_stream(a, X + j, ldx, Y + j, ldy, st);
     return true;
 }
 

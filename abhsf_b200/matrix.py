@@ -48,7 +48,7 @@ def _ptr(a) -> int:
 
 
 def _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_device,
-          sum_order="reference", selector="minbss", selector_model=None) -> capi.BuildOpts:
+          sum_order="reference", selector="minbss", selector_model=None, slice_tile_nnz=0) -> capi.BuildOpts:
     o = capi.BuildOpts()
     capi.lib.abhsf_build_opts_default(C.byref(o))
     o.block_size = 0 if block_size == "auto" else int(block_size)
@@ -68,6 +68,7 @@ def _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_pe
     o.bits_per_value = int(bits_per_value)
     o.inputs_on_device = 1 if on_device else 0
     o.sum_order = capi.SUM_ORDERS[sum_order]
+    o.slice_tile_nnz = int(slice_tile_nnz)
     return o
 
 
@@ -85,7 +86,8 @@ class AbhsfMatrix:
     def from_elements(cls, rows, cols, vals, m: int, n: int, *, block_size: int | str = 64,
                       value_type: str = "f64", allow_csr: bool = True, matrix_type: str = "real",
                       forced_scheme=None, bits_per_value: int = 0, sum_order: str = "reference",
-                      selector: str = "minbss", selector_model=None, stream=None) -> "AbhsfMatrix":
+                      selector: str = "minbss", selector_model=None, slice_tile_nnz: int = 0,
+                      stream=None) -> "AbhsfMatrix":
         """Builds from COO triplets (0-based, any order, no duplicates).
         Scheme per tile by exact minimum storage (msmf.h:35-63) unless
         forced_scheme names one.  vals may be None for binary matrices.
@@ -93,7 +95,9 @@ class AbhsfMatrix:
         spmv_naive; "tree" uses warp reduction trees.  block_size "auto"
         lets `selector` choose it: "minbss" (least storage over 16..256, the
         exhaustive sweep) or "learned" (the MLP; selector_model: float32
-        parameters, None = the built-in model)."""
+        parameters, None = the built-in model).  slice_tile_nnz: block rows
+        whose tiles hold at most this many elements on average are summed
+        from delta-coded row slices (0: the library's default, -1: none)."""
         on_dev = _is_cuda(rows)
         if on_dev:
             if not (_is_cuda(cols) and (vals is None or _is_cuda(vals))):
@@ -110,7 +114,7 @@ class AbhsfMatrix:
                 vals is not None and (vals.numel() if on_dev else vals.size) != nnz):
             raise capi.InvalidValue(capi.INVALID_VALUE, "rows, cols and vals differ in length")
         o = _opts(block_size, value_type, allow_csr, matrix_type, forced_scheme, bits_per_value, on_dev, sum_order,
-                  selector, selector_model)
+                  selector, selector_model, slice_tile_nnz)
         h = C.c_void_p()
         capi.check(capi.lib.abhsf_build(_ptr(rows) if nnz else None, _ptr(cols) if nnz else None,
                                         _ptr(vals) if (vals is not None and nnz) else None, nnz, int(m), int(n),
@@ -235,6 +239,25 @@ class AbhsfMatrix:
         p = [out[k].ctypes.data if out[k].size else None for k in
              ("brow_ptr", "tile_col", "tile_nnz", "tile_scheme", "tile_val_off", "tile_idx_off", "payload", "values")]
         capi.check(capi.lib.abhsf_export_host(self._h, *p))
+        return out
+
+    def slices(self) -> dict:
+        """The delta-coded row slices the SpMV reads for the hypersparse block
+        rows (abhsf_slices_info / abhsf_slices_export): per-slice arrays in
+        slice order, the lane records, and the words and values of every slot."""
+        self._check_open()
+        ns, nslot, nlr, ne, nb = (C.c_int64() for _ in range(5))
+        capi.check(capi.lib.abhsf_slices_info(self._h, C.byref(ns), C.byref(nslot), C.byref(nlr), C.byref(ne),
+                                              C.byref(nb)))
+        S, SL, LR = ns.value, nslot.value, nlr.value
+        vdt = {"f64": np.float64, "f32": np.float32, "bf16": np.uint16}[self.value_type]
+        out = {"slices": S, "slots": SL, "lane_records": LR, "elements": ne.value, "block_rows": nb.value,
+               "base": np.zeros(S, np.int64), "meta": np.zeros(S, np.int64), "brow": np.zeros(S, np.uint32),
+               "steps": np.zeros(S, np.uint32), "lanes": np.zeros(S, np.uint32), "chain": np.zeros(S, np.uint8),
+               "lane": np.zeros(LR, np.uint32), "words": np.zeros(SL, np.uint32), "values": np.zeros(SL, vdt)}
+        keys = ("base", "meta", "brow", "steps", "lanes", "chain", "lane", "words", "values")
+        capi.check(capi.lib.abhsf_slices_export(self._h, *[out[k].ctypes.data if out[k].size else None
+                                                          for k in keys]))
         return out
 
 

@@ -138,7 +138,9 @@ typedef struct abhsf_build_opts {
     int32_t sum_order;        /* abhsf_sum_order of abhsf_spmv / abhsf_spmv_host */
     int64_t bits_per_value;   /* dense-cost element width; 0 = width of value_type */
     int32_t selector;         /* abhsf_selector, used when block_size is 0 */
-    int32_t reserved;         /* must be 0 */
+    int32_t slice_tile_nnz;   /* reference-order SpMV at s = 32 / 64: block rows without a dense tile whose
+                                 tiles hold at most this many elements on average are summed from
+                                 delta-coded row slices; 0 = the library's default (32), -1 = none */
     const float* selector_model; /* host, ABHSF_MLP_PARAMS floats; NULL = the model built into the library */
 } abhsf_build_opts;
 
@@ -332,6 +334,32 @@ ABHSF_API abhsf_status abhsf_block_histogram_noalloc(const int64_t* rows, const 
                                                      int64_t m, int64_t n, int32_t r, int32_t s,
                                                      abhsf_stream_t stream, uint64_t* hist, int64_t hist_len,
                                                      int64_t* blocks);
+
+/* The delta-coded row slices through which the reference-order SpMV sums the
+ * matrix's hypersparse block rows (abhsf_build_opts.slice_tile_nnz): slices,
+ * slots (words and values, padding included), lane records, elements and
+ * block rows.  The encoding follows the reference's delta COO
+ * (spmv/orig/delta.cpp:118-219, spmv/unified/spmv.cpp:815-1032: row by row,
+ * each column the difference to the row's previous one).  Per block row, the
+ * non-empty rows ordered by length (longest first, then ascending row): a row
+ * of more than 256 elements is a chain slice (its elements at slots
+ * base .. base + length - 1, each word the absolute column); the others go to
+ * slices of up to 32 rows, one per lane, element k of lane l at slot
+ * base + 32 k + l, each word the column minus the row's previous column (the
+ * first absolute), lane record l = row << 24 | length at meta + l (0 past
+ * the slice's rows), steps = the longest row's length.  Values: a copy in
+ * slot order; padding slots hold 0. */
+ABHSF_API abhsf_status abhsf_slices_info(const abhsf_matrix* a, int64_t* slices, int64_t* slots,
+                                         int64_t* lane_records, int64_t* elements, int64_t* block_rows);
+
+/* The slices into host arrays (any may be NULL), in slice order: base, meta
+ * (the first lane record, or a chain's row within its block row), block row,
+ * steps, lanes, chain flag; the lane records; the words and values of every
+ * slot.  No counterpart in the reference (its delta COO lives in host
+ * memory). */
+ABHSF_API abhsf_status abhsf_slices_export(const abhsf_matrix* a, int64_t* base, int64_t* meta, uint32_t* brow,
+                                           uint32_t* steps, uint32_t* lanes, uint8_t* chain,
+                                           uint32_t* lane_records, uint32_t* words, void* values);
 
 /* One line of the reference's mmf-single / mmf-double (block_statistics/mmf.cpp:53-138)
  * from props and a block histogram; out_* = coo32 csr32 coo csr bitmap dense abhsf abhsf134. */

@@ -602,3 +602,267 @@ void orc_abs_spmv_elements(const int64_t* rows, const int64_t* cols, const doubl
         out[rows[k]] += p < 0 ? -p : p;
     }
 }
+
+/* ---------------------------------------------------------------------------
+ * Delta-coded row slices of the hypersparse block rows: the encoding the
+ * library's SpMV reads for those block rows, restated element by element.
+ * The reference's delta COO (spmv/orig/delta.cpp:118-219,
+ * spmv/unified/spmv.cpp:815-1032) keeps the elements row by row and each
+ * column as the difference to the previous one; here a block row's rows go
+ * to slices of up to 32 (one per lane, stored column-major), a row of more
+ * than ORC_CHAIN_MIN elements alone as a chain with absolute columns.
+ * ------------------------------------------------------------------------ */
+#define ORC_CHAIN_MIN 256
+
+/* Elements of tile t in the format's order: local row / column of each. */
+static int64_t tile_elements(const orc_matrix* a, int64_t t, int* lr, int* lc)
+{
+    const int s = a->s, lg = a->log2s;
+    const uint8_t* pay = a->idx + a->tile_idx_off[t];
+    const int64_t z = a->tile_val_off[t + 1] - a->tile_val_off[t];
+    int64_t e = 0;
+    switch (a->tile_scheme[t]) {
+    case ORC_COO:
+        for (e = 0; e < z; ++e) {
+            const uint16_t k = ((const uint16_t*)pay)[e];
+            lr[e] = k >> lg;
+            lc[e] = k & (s - 1);
+        }
+        break;
+    case ORC_CSR: {
+        const uint16_t* re = (const uint16_t*)pay;
+        for (int r = 0; r < s; ++r)
+            for (int64_t q = r ? re[r - 1] : 0; q < re[r]; ++q) {
+                lr[e] = r;
+                lc[e] = pay[2 * s + q];
+                ++e;
+            }
+        break;
+    }
+    case ORC_BITMAP: {
+        const uint64_t* bm = (const uint64_t*)pay;
+        for (int64_t bit = 0; bit < (int64_t)s * s; ++bit)
+            if ((bm[bit >> 6] >> (bit & 63)) & 1u) {
+                lr[e] = (int)(bit >> lg);
+                lc[e] = (int)(bit & (s - 1));
+                ++e;
+            }
+        break;
+    }
+    default:
+        return -1;
+    }
+    return e;
+}
+
+static const int64_t* g_len_cmp;  /* row lengths for the comparator below */
+static int by_length(const void* p, const void* q)
+{
+    const int a = *(const int*)p, b = *(const int*)q;
+    if (g_len_cmp[a] != g_len_cmp[b])
+        return g_len_cmp[a] > g_len_cmp[b] ? -1 : 1;
+    return a < b ? -1 : a > b;
+}
+
+/* Row lengths of block row I (len[r], r < s). */
+static void row_lengths(const orc_matrix* a, int64_t I, int* lr, int* lc, int64_t* len)
+{
+    for (int r = 0; r < a->s; ++r)
+        len[r] = 0;
+    for (int64_t t = a->brow_ptr[I]; t < a->brow_ptr[I + 1]; ++t) {
+        const int64_t z = tile_elements(a, t, lr, lc);
+        for (int64_t e = 0; e < z; ++e)
+            len[lr[e]]++;
+    }
+}
+
+/* The non-empty rows of a block row by length (longest first, then row). */
+static int rows_by_length(int s, const int64_t* len, int* order)
+{
+    int live = 0;
+    for (int r = 0; r < s; ++r)
+        if (len[r])
+            order[live++] = r;
+    g_len_cmp = len;
+    qsort(order, (size_t)live, sizeof(int), by_length);
+    return live;
+}
+
+int orc_slices_build(const orc_matrix* a, double avg, orc_slices** out)
+{
+    *out = (orc_slices*)calloc(1, sizeof(orc_slices));
+    orc_slices* P = *out;
+    if (!P)
+        return ORC_ERR_NOMEM;
+    const int s = a->s;
+    if (avg <= 0 || (uint64_t)a->n > ((uint64_t)1 << 32))
+        return ORC_OK;
+    /* the block rows: non-empty, no dense tile, at most avg elements per tile */
+    uint8_t* sel = (uint8_t*)calloc((size_t)a->M + 1, 1);
+    int64_t E = 0, ns = 0;
+    for (int64_t I = 0; I < a->M; ++I) {
+        const int64_t t0 = a->brow_ptr[I], t1 = a->brow_ptr[I + 1];
+        if (t1 == t0)
+            continue;
+        int ok = 1;
+        for (int64_t t = t0; t < t1; ++t)
+            ok = ok && a->tile_scheme[t] != ORC_DENSE;
+        const int64_t e = a->tile_val_off[t1] - a->tile_val_off[t0];
+        if (ok && (double)e <= avg * (double)(t1 - t0)) {
+            sel[I] = 1;
+            E += e;
+            ++ns;
+        }
+    }
+    if (ns == 0 || E == 0 || E >= ((int64_t)1 << 31) || ns * (int64_t)s >= ((int64_t)1 << 32)) {
+        free(sel);
+        return ORC_OK;
+    }
+    int* lr = (int*)malloc((size_t)s * s * sizeof(int));
+    int* lc = (int*)malloc((size_t)s * s * sizeof(int));
+    int64_t* len = (int64_t*)malloc(s * sizeof(int64_t));
+    int* order = (int*)malloc(s * sizeof(int));
+    /* pass 1: count slices, slots and lane records */
+    int64_t nsl = 0, slots = 0, nlr = 0;
+    for (int64_t I = 0; I < a->M; ++I) {
+        if (!sel[I])
+            continue;
+        row_lengths(a, I, lr, lc, len);
+        const int live = rows_by_length(s, len, order);
+        int i = 0;
+        for (; i < live && len[order[i]] > ORC_CHAIN_MIN; ++i) {
+            ++nsl;
+            slots += len[order[i]];
+        }
+        for (; i < live; i += 32) {
+            ++nsl;
+            nlr += 32;
+            slots += 32 * len[order[i]];
+        }
+    }
+    P->base = (int64_t*)malloc((nsl + 1) * sizeof(int64_t));
+    P->meta = (int64_t*)malloc((nsl + 1) * sizeof(int64_t));
+    P->brow = (uint32_t*)malloc((nsl + 1) * sizeof(uint32_t));
+    P->steps = (uint32_t*)malloc((nsl + 1) * sizeof(uint32_t));
+    P->lanes = (uint32_t*)malloc((nsl + 1) * sizeof(uint32_t));
+    P->chain = (uint8_t*)malloc(nsl + 1);
+    P->lane = (uint32_t*)calloc(nlr + 1, sizeof(uint32_t));
+    P->words = (uint32_t*)calloc(slots + 1, sizeof(uint32_t));
+    P->vidx = (int64_t*)malloc((slots + 1) * sizeof(int64_t));
+    int64_t* slot0 = (int64_t*)malloc(s * sizeof(int64_t));
+    int64_t* fill = (int64_t*)malloc(s * sizeof(int64_t));
+    int64_t* prev = (int64_t*)malloc(s * sizeof(int64_t));
+    uint8_t* chain = (uint8_t*)malloc(s);
+    for (int64_t q = 0; q < slots; ++q)
+        P->vidx[q] = -1;
+    /* pass 2: the slices, then every element at its slot */
+    for (int64_t I = 0; I < a->M; ++I) {
+        if (!sel[I])
+            continue;
+        row_lengths(a, I, lr, lc, len);
+        const int live = rows_by_length(s, len, order);
+        int i = 0;
+        for (; i < live && len[order[i]] > ORC_CHAIN_MIN; ++i) {
+            const int r = order[i];
+            P->base[P->n] = P->slots;
+            P->meta[P->n] = r;
+            P->brow[P->n] = (uint32_t)I;
+            P->steps[P->n] = (uint32_t)len[r];
+            P->lanes[P->n] = 1;
+            P->chain[P->n] = 1;
+            slot0[r] = P->slots;
+            chain[r] = 1;
+            P->slots += len[r];
+            P->n++;
+        }
+        for (; i < live; i += 32) {
+            const int n32 = live - i < 32 ? live - i : 32;
+            P->base[P->n] = P->slots;
+            P->meta[P->n] = P->lane_records;
+            P->brow[P->n] = (uint32_t)I;
+            P->steps[P->n] = (uint32_t)len[order[i]];
+            P->lanes[P->n] = (uint32_t)n32;
+            P->chain[P->n] = 0;
+            for (int l = 0; l < n32; ++l) {
+                const int r = order[i + l];
+                P->lane[P->lane_records + l] = (uint32_t)r << 24 | (uint32_t)len[r];
+                slot0[r] = P->slots + l;
+                chain[r] = 0;
+            }
+            P->lane_records += 32;
+            P->slots += 32 * len[order[i]];
+            P->n++;
+        }
+        for (int r = 0; r < s; ++r) {
+            fill[r] = 0;
+            prev[r] = 0;
+        }
+        /* the k-th element of row r (format order keeps a row's columns
+         * ascending) at slot0[r] + k (chain) or slot0[r] + 32 k (sliced) */
+        for (int64_t t = a->brow_ptr[I]; t < a->brow_ptr[I + 1]; ++t) {
+            const int64_t z = tile_elements(a, t, lr, lc);
+            const int64_t c0 = (int64_t)a->tile_col[t] * s;
+            for (int64_t e = 0; e < z; ++e) {
+                const int r = lr[e];
+                const int64_t col = c0 + lc[e];
+                const int64_t k = fill[r]++;
+                const int64_t slot = slot0[r] + (chain[r] ? k : 32 * k);
+                P->words[slot] = (uint32_t)((chain[r] || k == 0) ? col : col - prev[r]);
+                P->vidx[slot] = a->tile_val_off[t] + e;
+                prev[r] = col;
+            }
+        }
+    }
+    P->E = E;
+    P->block_rows = ns;
+    free(sel);
+    free(lr);
+    free(lc);
+    free(len);
+    free(order);
+    free(slot0);
+    free(fill);
+    free(prev);
+    free(chain);
+    return ORC_OK;
+}
+
+void orc_slices_free(orc_slices* p)
+{
+    if (!p)
+        return;
+    free(p->base);
+    free(p->meta);
+    free(p->brow);
+    free(p->steps);
+    free(p->lanes);
+    free(p->chain);
+    free(p->lane);
+    free(p->words);
+    free(p->vidx);
+    free(p);
+}
+
+/* y += A x over the slice rows: every row's words decoded in order (a
+ * running column), each product added onto its row from y (f64 values). */
+void orc_spmv_slices(const orc_matrix* a, const orc_slices* P, const double* x, double* y)
+{
+    const int s = a->s;
+    const double* v = (const double*)a->values;
+    for (int64_t q = 0; q < P->n; ++q) {
+        const int nl = P->chain[q] ? 1 : (int)P->lanes[q];
+        for (int l = 0; l < nl; ++l) {
+            const uint32_t rec = P->chain[q] ? 0 : P->lane[P->meta[q] + l];
+            const int64_t r = P->chain[q] ? P->meta[q] : (int64_t)(rec >> 24);
+            const int64_t n = P->chain[q] ? (int64_t)P->steps[q] : (int64_t)(rec & 0xffffffu);
+            const int64_t row = (int64_t)P->brow[q] * s + r;
+            uint64_t col = 0;
+            for (int64_t k = 0; k < n; ++k) {
+                const int64_t slot = P->base[q] + (P->chain[q] ? k : 32 * k + l);
+                const uint32_t w = P->words[slot];
+                col = P->chain[q] ? w : (uint32_t)(col + w);
+                y[row] += v[P->vidx[slot]] * x[col];
+            }
+        }
+    }
+}

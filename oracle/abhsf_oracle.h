@@ -122,6 +122,35 @@ void orc_spmv_elements_f32(const int64_t* rows, const int64_t* cols, const float
 uint16_t orc_f64_to_bf16(double v);
 double orc_bf16_to_f64(uint16_t b);
 
+/* Delta-coded row slices of the hypersparse block rows (the encoding the
+ * library's SpMV reads for them; spmv/orig/delta.cpp:118-219 is the
+ * reference's row-by-row delta COO it follows).  Block rows: non-empty, no
+ * dense tile, at most avg elements per tile on average; none when n > 2^32
+ * or the elements reach 2^31.  Per block row (ascending), its non-empty rows
+ * by length (longest first, then row): each row of more than 256 elements a
+ * chain slice (lanes 1, meta = the row, steps = its length, its elements at
+ * slots base + k with absolute columns), then the rest in slices of up to 32
+ * (steps = the first row's length, lane record l = row << 24 | length at
+ * lane[meta + l], element k of lane l at slot base + 32 k + l, each word the
+ * column minus the row's previous column, the first absolute).  vidx: each
+ * slot's index in the format's values (-1 for padding, whose word is 0). */
+typedef struct orc_slices {
+    int64_t n, slots, lane_records, E, block_rows;
+    int64_t* base;
+    int64_t* meta;
+    uint32_t* brow;
+    uint32_t* steps;
+    uint32_t* lanes;
+    uint8_t* chain;
+    uint32_t* lane;
+    uint32_t* words;
+    int64_t* vidx;
+} orc_slices;
+int orc_slices_build(const orc_matrix* a, double avg, orc_slices** out);
+void orc_slices_free(orc_slices* p);
+/* y += A x over the slice rows only, each row's words decoded in order. */
+void orc_spmv_slices(const orc_matrix* a, const orc_slices* p, const double* x, double* y);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,6 +96,12 @@ def lib() -> C.CDLL:
         L.orc_spmv_elements_f32.argtypes = [_i64p, _i64p, f32p, C.c_int64, f32p, f32p]
         L.orc_values_as_f32.restype = None
         L.orc_values_as_f32.argtypes = [_f64p, C.c_int64, C.c_int, f32p]
+        L.orc_slices_build.restype = C.c_int
+        L.orc_slices_build.argtypes = [C.POINTER(OrcMatrix), C.c_double, C.POINTER(C.POINTER(OrcSlices))]
+        L.orc_slices_free.restype = None
+        L.orc_slices_free.argtypes = [C.POINTER(OrcSlices)]
+        L.orc_spmv_slices.restype = None
+        L.orc_spmv_slices.argtypes = [C.POINTER(OrcMatrix), C.POINTER(OrcSlices), _f64p, _f64p]
         _lib = L
     return _lib
 
@@ -158,6 +164,14 @@ def mmf_line(m, n, nnz, mtype, r, s, hist: dict[int, int]):
 
 
 # ----------------------------------------------------------------- builder
+class OrcSlices(C.Structure):
+    _fields_ = [("n", C.c_int64), ("slots", C.c_int64), ("lane_records", C.c_int64), ("E", C.c_int64),
+                ("block_rows", C.c_int64), ("base", C.POINTER(C.c_int64)), ("meta", C.POINTER(C.c_int64)),
+                ("brow", C.POINTER(C.c_uint32)), ("steps", C.POINTER(C.c_uint32)), ("lanes", C.POINTER(C.c_uint32)),
+                ("chain", C.POINTER(C.c_uint8)), ("lane", C.POINTER(C.c_uint32)), ("words", C.POINTER(C.c_uint32)),
+                ("vidx", C.POINTER(C.c_int64))]
+
+
 class Built:
     """Host copy of the arrays the oracle builder emits."""
 
@@ -202,6 +216,47 @@ class Built:
     @staticmethod
     def threads() -> int:
         return int(lib().orc_omp_threads())
+
+    def slices(self, avg: float) -> dict:
+        """The delta-coded row slices of the hypersparse block rows
+        (orc_slices_build): per-slice arrays in slice order, the lane
+        records, and every slot's word and value index (-1: padding)."""
+        out = C.POINTER(OrcSlices)()
+        rc = lib().orc_slices_build(self._ptr, float(avg), C.byref(out))
+        try:
+            if rc != 0:
+                raise ValueError("oracle slices: " + ERRORS.get(rc, str(rc)))
+            P = out.contents
+
+            def arr(ptr, count, dt):
+                if count == 0:
+                    return np.zeros(0, dtype=dt)
+                return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+            res = {"slices": int(P.n), "slots": int(P.slots), "lane_records": int(P.lane_records),
+                   "elements": int(P.E), "block_rows": int(P.block_rows)}
+            for k, dt in (("base", np.int64), ("meta", np.int64), ("brow", np.uint32), ("steps", np.uint32),
+                          ("lanes", np.uint32), ("chain", np.uint8)):
+                res[k] = arr(getattr(P, k), P.n, dt)
+            res["lane"] = arr(P.lane, P.lane_records, np.uint32)
+            res["words"] = arr(P.words, P.slots, np.uint32)
+            res["vidx"] = arr(P.vidx, P.slots, np.int64)
+            return res
+        finally:
+            lib().orc_slices_free(out)
+
+    def spmv_slices(self, avg: float, x: np.ndarray, y: np.ndarray) -> None:
+        """y += A x over the slice rows only, decoding the oracle's slices."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert y.dtype == np.float64 and y.flags.c_contiguous
+        out = C.POINTER(OrcSlices)()
+        rc = lib().orc_slices_build(self._ptr, float(avg), C.byref(out))
+        try:
+            if rc != 0:
+                raise ValueError("oracle slices: " + ERRORS.get(rc, str(rc)))
+            lib().orc_spmv_slices(self._ptr, out, _p(x, _f64p), _p(y, _f64p))
+        finally:
+            lib().orc_slices_free(out)
 
     def close(self):
         if self._ptr is not None:

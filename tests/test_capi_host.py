@@ -129,7 +129,7 @@ def test_selector_option_defaults_and_struct():
     o = capi.BuildOpts()
     capi.lib.abhsf_build_opts_default(C.byref(o))
     assert o.block_size == 64 and o.selector == capi.SELECTORS["minbss"] and o.selector_model is None
-    assert o.reserved == 0
+    assert o.slice_tile_nnz == 0
 
 
 def test_cost_model_exhaustive_small_blocks():

@@ -104,7 +104,7 @@ def test_wait_timeout_sets_status_and_context_survives(gpu):
     the context and the matrix stay usable."""
     import torch
     coo = W.random_blocky(2000, 2000, 64, 300, seed=31)
-    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64, slice_tile_nnz=-1)
     x = W.rhs(coo.n, 1)
     y0 = np.zeros(coo.m)
     try:
@@ -247,7 +247,8 @@ def test_every_ring_variant_gives_the_reference_y(gpu, s):
     of s/32 warps, four or two teams of one warp with s/32 rows per lane; x / y
     blocks as bulk copies or element copies) that the build times and chooses
     among give the reference CSR's y bit for bit, on matrices of few large
-    tiles, of many small tiles (a 3D stencil) and with ragged edges."""
+    tiles, of many small tiles (a 3D stencil) and with ragged edges (every
+    block row on the ring: no row slices)."""
     import ctypes as C
     cases = [W.random_blocky(2100, 1900, s, 60, seed=3), W.laplacian_3d(20), W.rmat(3000, 8, seed=4),
              W.tiled_mixture(n=65536 + 37, p=1e-3, seed=2)]
@@ -255,7 +256,7 @@ def test_every_ring_variant_gives_the_reference_y(gpu, s):
         x = W.rhs(coo.n, 21)
         y0 = W.rhs(coo.m, 22)
         want = reference_order_y(coo, x, y0)
-        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s)
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, slice_tile_nnz=-1)
         t, b = C.c_int32(), C.c_int32()
         assert capi.lib.abhsf_test_ring_variant(A.handle, 0, C.byref(t), C.byref(b)) == capi.SUCCESS
         assert t.value in (0, 1, 2, 3) and b.value in (0, 1)
@@ -276,12 +277,12 @@ def test_ring_variant_environment_override(gpu, monkeypatch):
     t, b = C.c_int32(), C.c_int32()
     for value, want in (("2,0", (2, 0)), ("3,1", (3, 1))):
         monkeypatch.setenv("ABHSF_RING_VARIANT", value)
-        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64, slice_tile_nnz=-1)
         assert capi.lib.abhsf_test_ring_variant(A.handle, 0, C.byref(t), C.byref(b)) == capi.SUCCESS
         assert (t.value, b.value) == want
         A.release()
     monkeypatch.setenv("ABHSF_RING_VARIANT", "7,1")
-    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64, slice_tile_nnz=-1)
     assert capi.lib.abhsf_test_ring_variant(A.handle, 0, C.byref(t), C.byref(b)) == capi.SUCCESS
     assert t.value in (0, 1, 2, 3)
     x, y0 = W.rhs(coo.n, 1), W.rhs(coo.m, 2)

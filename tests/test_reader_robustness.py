@@ -90,10 +90,10 @@ def _no_gpu() -> bool:
            value_type=st.integers(-1, 4), allow_csr=st.integers(-1, 2), matrix_type=st.integers(-1, 4),
            forced=st.integers(-2, 5), on_dev=st.integers(0, 1), sum_order=st.integers(-1, 2),
            bits=st.sampled_from([-1, 0, 16, 32, 64, 1 << 40]), selector=st.integers(-1, 4),
-           reserved=st.integers(0, 1), nnz=st.integers(-1, 5), m=st.integers(-1, 70), n=st.integers(-1, 70),
+           panel=st.integers(-2, 40), nnz=st.integers(-1, 5), m=st.integers(-1, 70), n=st.integers(-1, 70),
            null_rows=st.booleans())
 def test_build_validation_never_crashes(block_size, value_type, allow_csr, matrix_type, forced, on_dev, sum_order,
-                                        bits, selector, reserved, nnz, m, n, null_rows):
+                                        bits, selector, panel, nnz, m, n, null_rows):
     """abhsf_build with any options and sizes returns a status: invalid ones
     are refused on the host, and on this machine (no GPU) every valid call
     fails at the device with a status too.  on_dev is only ever set together
@@ -104,7 +104,7 @@ def test_build_validation_never_crashes(block_size, value_type, allow_csr, matri
     capi.lib.abhsf_build_opts_default(C.byref(o))
     o.block_size, o.value_type, o.allow_csr, o.matrix_type = block_size, value_type, allow_csr, matrix_type
     o.forced_scheme, o.inputs_on_device, o.sum_order = forced, on_dev, sum_order
-    o.bits_per_value, o.selector, o.reserved = bits, selector, reserved
+    o.bits_per_value, o.selector, o.slice_tile_nnz = bits, selector, panel
     k = max(nnz, 0)
     rows = np.zeros(max(k, 1), np.int64)
     cols = np.arange(max(k, 1), dtype=np.int64)
