@@ -87,7 +87,7 @@ class Stats(C.Structure):
                 ("block_rows", C.c_int64), ("block_cols", C.c_int64), ("tiles", C.c_int64),
                 ("tiles_per_scheme", C.c_int64 * 4), ("nnz_per_scheme", C.c_int64 * 4),
                 ("stored_values", C.c_int64), ("payload_bytes", C.c_int64), ("format_bytes", C.c_int64),
-                ("msmf_bits", C.c_uint64 * 8)]
+                ("msmf_bits", C.c_uint64 * 8), ("spmv_bytes", C.c_int64)]
 
 
 _vp = C.c_void_p

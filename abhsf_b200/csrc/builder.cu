@@ -543,6 +543,7 @@ void finish_stats(abhsf_matrix& a, uint64_t dense_bits, cudaStream_t st)
     s.payload_bytes = a.payload_bytes;
     s.format_bytes = (a.M + 1) * 8 + a.T * (4 + 4 + 1) + (a.T + 1) * 16 + a.payload_bytes +
                      a.n_values * (int64_t)value_size(a.value_type);
+    s.spmv_bytes = s.format_bytes;  // the row slices, where prepared, replace their block rows' part
     // mmf line at this block size whose "double" column has the dense-cost
     // width; binary matrices carry no value bits (mmf.cpp:45-46).
     uint64_t o1[8], o2[8];

@@ -6,6 +6,7 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -201,9 +202,15 @@ struct abhsf_matrix {
     abhsf::dbuf<uint32_t> dc_words;      // one word per slot (delta-coded columns)
     abhsf::dbuf<uint8_t> dc_vals;        // the values in slot order
     abhsf::dbuf<uint32_t> dc_lane;       // lane records: row << 24 | length
-    abhsf::dbuf<uint8_t> dc_sched;       // the matrix's own launch: slices in warp order
+    abhsf::dbuf<uint8_t> dc_sched;       // the matrix's own launch: sliced rows in warp order
     abhsf::dbuf<int64_t> dc_wbeg;
     int dc_warps = 0;
+    abhsf::dbuf<uint8_t> dc_csched;      // ... and its chains, launched on dc_side beside the others
+    abhsf::dbuf<int64_t> dc_cwbeg;
+    int dc_cwarps = 0;
+    cudaStream_t dc_side = nullptr;      // created with the first chain; forked from the caller's stream
+    cudaEvent_t dc_fork = nullptr, dc_join = nullptr;
+    mutable std::mutex dc_mu;            // one fork / join sequence at a time
     int64_t dc_elements = 0, dc_rows = 0, dc_slots = 0, dc_lane_records = 0;
     float dc_avg = 0.f;                  // largest mean elements per tile of a slice block row (0: none)
     abhsf::dbuf<int> dev_status;  // ABHSF_DEVSTAT_* bits set by kernels
@@ -216,9 +223,12 @@ struct abhsf_matrix {
         abhsf::dbuf<uint8_t> desc;
         abhsf::dbuf<int64_t> wbeg;
         int ctas = 0;
-        abhsf::dbuf<uint8_t> dc_sched;  // the chunk's slices
+        abhsf::dbuf<uint8_t> dc_sched;  // the chunk's sliced rows and chains
         abhsf::dbuf<int64_t> dc_wbeg;
         int dc_warps = 0;
+        abhsf::dbuf<uint8_t> dc_csched;
+        abhsf::dbuf<int64_t> dc_cwbeg;
+        int dc_cwarps = 0;
     };
     std::vector<host_chunk> host_chunks;
     bool host_ready = false;
@@ -230,6 +240,12 @@ struct abhsf_matrix {
     abhsf_matrix& operator=(const abhsf_matrix&) = delete;
     ~abhsf_matrix()
     {
+        if (dc_fork)
+            cudaEventDestroy(dc_fork);
+        if (dc_join)
+            cudaEventDestroy(dc_join);
+        if (dc_side)
+            cudaStreamDestroy(dc_side);
         for (cudaEvent_t e : host_events)
             cudaEventDestroy(e);
         if (host_in)
@@ -270,4 +286,23 @@ struct abhsf_batch {
     abhsf::dbuf<uint8_t> dc_sched;
     abhsf::dbuf<int64_t> dc_wbeg;
     int dc_warps = 0;
+    abhsf::dbuf<uint8_t> dc_csched;
+    abhsf::dbuf<int64_t> dc_cwbeg;
+    int dc_cwarps = 0;
+    cudaStream_t dc_side = nullptr;
+    cudaEvent_t dc_fork = nullptr, dc_join = nullptr;
+    mutable std::mutex dc_mu;
+
+    abhsf_batch() = default;
+    abhsf_batch(const abhsf_batch&) = delete;
+    abhsf_batch& operator=(const abhsf_batch&) = delete;
+    ~abhsf_batch()
+    {
+        if (dc_fork)
+            cudaEventDestroy(dc_fork);
+        if (dc_join)
+            cudaEventDestroy(dc_join);
+        if (dc_side)
+            cudaStreamDestroy(dc_side);
+    }
 };

@@ -84,16 +84,31 @@ void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys
 // Delta-coded row slices of the hypersparse block rows (spmv_stream.cu):
 // prepare_stream picks the block rows (no dense tile, at most `avg`
 // elements per tile on average), encodes them and deals the slices;
-// deal_slices deals the slices of block rows [brow_lo, brow_hi) of several
-// matrices over one launch; spmv_stream adds A x over the slice rows
-// (x[i * ldx], y[i * ldy]; the matrix's own schedule unless one is given).
+// deal_slices deals the sliced rows (chains = false) or the chains of block
+// rows [brow_lo, brow_hi) of several matrices over one launch.  A launch plan
+// names both schedules; slices_begin forks the chains onto the side stream
+// (call it before the ring kernel, so that they run beside it) and
+// slices_end adds the sliced rows on st and joins the chains back (x[i * ldx],
+// y[i * ldy]).  The caller holds dc_mu across the pair.
 void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st);
 void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sched, dbuf<int64_t>& wbeg,
-                 int& warps, cudaStream_t st, int64_t brow_lo, int64_t brow_hi);
-bool spmv_stream(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int64_t ldy, cudaStream_t st,
-                 const uint8_t* sched = nullptr, const int64_t* wbeg = nullptr, int warps = 0);
+                 int& warps, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, bool chains);
+struct dc_plan {
+    const uint8_t* sched = nullptr;
+    const int64_t* wbeg = nullptr;
+    int warps = 0;
+    const uint8_t* csched = nullptr;
+    const int64_t* cwbeg = nullptr;
+    int cwarps = 0;
+};
+dc_plan plan_of(const abhsf_matrix& a);
+void slices_begin(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
+                  cudaStream_t st);
+void slices_end(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
+                cudaStream_t st);
 void prepare_batch_stream(abhsf_batch& b, cudaStream_t st);
-void batch_stream(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);
+void batch_stream_begin(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);
+void batch_stream_end(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);
 
 // Conjugate gradients (cg.cu).
 void cg_solve(const abhsf_matrix& a, const double* b, double* x, double rtol, int max_iters, abhsf_cg_info* info,

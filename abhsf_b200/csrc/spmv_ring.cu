@@ -1429,7 +1429,7 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     int ctas = 0, mpv = 0;
     if (!build_ring_schedule({&a}, 32, a.ring_desc, a.ring_wbeg, ctas, mpv, st)) {
         // every block row is a slice row, or the ring's counters would overflow
-        a.ring_ready = a.dc_warps > 0 && a.dc_rows == a.tree_nrows;
+        a.ring_ready = (a.dc_warps > 0 || a.dc_cwarps > 0) && a.dc_rows == a.tree_nrows;
         return;  // else the streaming kernel serves this matrix
     }
     a.ring_ready = true;
@@ -1503,9 +1503,11 @@ void prepare_batch(abhsf_batch& b, cudaStream_t st)
 
 void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st)
 {
+    std::lock_guard<std::mutex> lock(b.dc_mu);
+    batch_stream_begin(b, xs, ys, st);  // the chains, beside the rest
     if (b.ctas > 0)
         batch_launch(b, xs, ys, st, false);
-    batch_stream(b, xs, ys, st);
+    batch_stream_end(b, xs, ys, st);
 }
 
 
@@ -1514,13 +1516,16 @@ bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream
 {
     if (!a.ring_ready || a.value_type != ABHSF_VALUE_F64)
         return false;
+    std::lock_guard<std::mutex> lock(a.dc_mu);
+    const dc_plan p = plan_of(a);
+    slices_begin(a, p, x, 1, y, 1, st);  // the chains, beside the rest
     if (a.ring_warps) {
         if (a.s == 32)
             launch_ring<32, 1, ABHSF_VALUE_F64>(a, x, 1, y, 1, st);
         else
             launch_ring<64, 1, ABHSF_VALUE_F64>(a, x, 1, y, 1, st);
     }
-    spmv_stream(a, x, 1, y, 1, st);
+    slices_end(a, p, x, 1, y, 1, st);
     return true;
 }
 
@@ -1528,6 +1533,9 @@ bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t
 {
     if (!a.ring_ready || a.value_type == ABHSF_VALUE_F64)
         return false;
+    std::lock_guard<std::mutex> lock(a.dc_mu);
+    const dc_plan p = plan_of(a);
+    slices_begin(a, p, x, 1, y, 1, st);
     if (a.ring_warps) {
         if (a.value_type == ABHSF_VALUE_F32) {
             if (a.s == 32)
@@ -1541,7 +1549,7 @@ bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t
                 launch_ring<64, 1, ABHSF_VALUE_BF16>(a, x, 1, y, 1, st);
         }
     }
-    spmv_stream(a, x, 1, y, 1, st);
+    slices_end(a, p, x, 1, y, 1, st);
     return true;
 }
 
@@ -1562,7 +1570,8 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
             if (a.ring_warps == 0 ||
                 !build_ring_schedule({&a}, 32, ch.desc, ch.wbeg, ch.ctas, mpv, st, ch.brow0, ch.brow1))
                 ch.ctas = 0;  // no ring tiles in these block rows
-            deal_slices({&a}, ch.dc_sched, ch.dc_wbeg, ch.dc_warps, st, ch.brow0, ch.brow1);
+            deal_slices({&a}, ch.dc_sched, ch.dc_wbeg, ch.dc_warps, st, ch.brow0, ch.brow1, false);
+            deal_slices({&a}, ch.dc_csched, ch.dc_cwbeg, ch.dc_cwarps, st, ch.brow0, ch.brow1, true);
         }
         if (!a.host_in)
             ABHSF_CUDA(cudaStreamCreateWithFlags(&a.host_in, cudaStreamNonBlocking));
@@ -1587,17 +1596,25 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
         ABHSF_CUDA(cudaMemcpyAsync(ys + r0, y + r0, (r1 - r0) * sizeof(double), cudaMemcpyHostToDevice, a.host_in));
         ABHSF_CUDA(cudaEventRecord(ev[1 + c], a.host_in));
     }
+    std::lock_guard<std::mutex> lock(a.dc_mu);
     for (int c = 0; c < kChunks; ++c) {
         const auto& ch = a.host_chunks[c];
         ABHSF_CUDA(cudaStreamWaitEvent(st, ev[1 + c], 0));
+        dc_plan p;
+        p.sched = ch.dc_sched.get();
+        p.wbeg = ch.dc_wbeg.get();
+        p.warps = ch.dc_warps;
+        p.csched = ch.dc_csched.get();
+        p.cwbeg = ch.dc_cwbeg.get();
+        p.cwarps = ch.dc_cwarps;
+        slices_begin(a, p, xs, 1, ys, 1, st);
         if (ch.ctas > 0) {
             if (a.s == 32)
                 launch_ring<32, 1, ABHSF_VALUE_F64>(a, xs, 1, ys, 1, st, false, ch.desc.get(), ch.wbeg.get(), ch.ctas);
             else
                 launch_ring<64, 1, ABHSF_VALUE_F64>(a, xs, 1, ys, 1, st, false, ch.desc.get(), ch.wbeg.get(), ch.ctas);
         }
-        if (ch.dc_warps > 0)
-            spmv_stream(a, xs, 1, ys, 1, st, ch.dc_sched.get(), ch.dc_wbeg.get(), ch.dc_warps);
+        slices_end(a, p, xs, 1, ys, 1, st);
         ABHSF_CUDA(cudaEventRecord(ev[1 + kChunks + c], st));
     }
     for (int c = 0; c < kChunks; ++c) {
@@ -1616,14 +1633,18 @@ bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, d
 {
     if (!a.ring_ready || a.value_type != ABHSF_VALUE_F64)
         return false;
+    std::lock_guard<std::mutex> lock(a.dc_mu);
+    const dc_plan p = plan_of(a);
     if (a.ring_warps) {
         if (a.s == 32)
             spmm_ring<32>(a, k, X, ldx, Y, ldy, st);
         else
             spmm_ring<64>(a, k, X, ldx, Y, ldy, st);
     }
-    for (int j = 0; j < k && a.dc_warps; ++j)  // the slice rows, column by column
-        spmv_stream(a, X + j, ldx, Y + j, ldy, st);
+    for (int j = 0; j < k; ++j) {  // the slice rows, column by column
+        slices_begin(a, p, X + j, ldx, Y + j, ldy, st);
+        slices_end(a, p, X + j, ldx, Y + j, ldy, st);
+    }
     return true;
 }
 

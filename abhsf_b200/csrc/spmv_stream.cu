@@ -24,10 +24,12 @@
 // running sum of the deltas, x gathered through L2 -- and adds each product
 // onto its row's sum in column order, starting from y: the order of the
 // reference CSR's spmv_naive (spmv/bottlenecks/spmv.cpp:58-64), so y is
-// bitwise the same.  A chain: the lanes form 32 products at a time, kAhead
-// steps ahead, and every lane adds them in order from shared memory.  Slices
-// are dealt to warps at preparation time, longest first.  No waits: nothing
-// here can stall on another warp.
+// bitwise the same.  A chain (its own kernel, on a side stream forked from
+// the caller's so that it runs beside the others): the lanes form 32
+// products at a time, kChainAhead steps ahead, and every lane adds them in
+// order.  Slices and chains are dealt to warps at
+// preparation time, longest first.  No waits: nothing here can stall on
+// another warp.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -44,13 +46,17 @@ namespace abhsf {
 namespace {
 
 constexpr int kWarpsPerCta = 8;
-constexpr int kCtasPerSm = 4;     // the grid: resident CTAs per SM (64 registers a thread)
+constexpr int kCtasPerSm = 4;     // CTAs per SM in the grid (64 registers a thread)
 constexpr int kUnroll = 4;        // elements a lane loads per step of a sliced row
-constexpr int kAhead = 4;         // chain: steps of 32 products formed ahead of the sums
+constexpr int kChainWarps = 4;    // warps per CTA of the chain kernel
+constexpr int kChainCtasPerSm = 4;  // register bound of the chain kernel (128 a thread)
+constexpr int kChainGridPerSm = 1;  // chain CTAs per SM in the grid: the rest of the SM is left to the others
+constexpr int kChainAhead = 8;    // chain: steps of 32 products in flight ahead of the sums
 constexpr uint32_t kChain = 1u;   // dc_slice::geo: a one-row chain
 constexpr int kMidShift = 20;     // dc_slice::geo: matrix index of a batch
 constexpr uint32_t kLenMask = (1u << 24) - 1u;
 constexpr int kChainMin = 256;   // rows longer than this are summed alone, as a chain
+constexpr int kRingTilesMax = 256;  // block rows of more tiles go to the slices whatever their density
 
 // What the kernel needs of one slice (32 bytes, in schedule order).
 struct __align__(16) dc_slice {
@@ -117,34 +123,36 @@ struct dc_args {
     void* const* ys;
 };
 
-// Adds nv of the 32 products in p (shared memory, in order) onto run.
+// Adds the first nv of the warp's 32 products (lane k holds product k) onto
+// run in lane order, every lane the same chain.  The products come by
+// shuffles taken ahead of the adds, so that nothing but the adds themselves
+// lies on the chain; a full step adds all 32 without a test in the chain.
 template <typename T>
-__device__ __forceinline__ T add_in_order(T run, const T* p, int nv)
+__device__ __forceinline__ T add_in_order(T run, T p, int nv)
 {
-    if constexpr (sizeof(T) == 8) {
-        const double2* q = reinterpret_cast<const double2*>(p);
+    if (nv == 32) {
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            const double2 t = q[k];
-            if (2 * k < nv)
-                run = dadd(run, t.x);
-            if (2 * k + 1 < nv)
-                run = dadd(run, t.y);
-        }
-    } else {
-        const float4* q = reinterpret_cast<const float4*>(p);
+        for (int k0 = 0; k0 < 32; k0 += 8) {
+            T t[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const float4 t = q[k];
-            if (4 * k < nv)
-                run = dadd(run, t.x);
-            if (4 * k + 1 < nv)
-                run = dadd(run, t.y);
-            if (4 * k + 2 < nv)
-                run = dadd(run, t.z);
-            if (4 * k + 3 < nv)
-                run = dadd(run, t.w);
+            for (int k = 0; k < 8; ++k)
+                t[k] = __shfl_sync(0xffffffffu, p, k0 + k);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                run = dadd(run, t[k]);
         }
+        return run;
+    }
+#pragma unroll
+    for (int k0 = 0; k0 < 32; k0 += 8) {
+        T t[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            t[k] = __shfl_sync(0xffffffffu, p, k0 + k);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (k0 + k < nv)
+                run = dadd(run, t[k]);
     }
     return run;
 }
@@ -154,7 +162,6 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmv_slices(dc_args P)
 {
     using T = typename vt_of<VT>::T;
     using V = typename vt_of<VT>::V;
-    __shared__ __align__(16) T pbuf[kWarpsPerCta][32];  // a chain's products of one step
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gw = blockIdx.x * kWarpsPerCta + warp;
     if (gw >= P.warps)
@@ -170,7 +177,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmv_slices(dc_args P)
         const int64_t ldx = B ? 1 : P.ldx, ldy = B ? 1 : P.ldy;
         const uint32_t* W = M.words + sl.base;
         const V* Vv = static_cast<const V*>(M.vals) + sl.base;
-        if (!(sl.geo & kChain)) {
+        {
             // one row per lane, element k of the lane's row at slot 32 k + lane
             const uint32_t rec = lane < (int)sl.lanes ? M.lane[sl.meta + lane] : 0u;
             const int len = (int)(rec & kLenMask);
@@ -200,44 +207,80 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmv_slices(dc_args P)
             }
             if (len)
                 Y[row * ldy] = acc;
-            continue;
         }
-        // a chain: one row, its elements in order, each word the absolute column
+    }
+}
+
+// The chains: one warp per row, the row's elements in order (each word the
+// absolute column).  Lane l forms the product of element 32 c + l; every
+// lane adds the step's 32 products in order, taken by shuffles.  The values
+// and gathered x of the next kChainAhead steps are in flight meanwhile, so
+// that the chain of adds -- the one thing that must run in sequence -- does
+// not wait on memory.
+template <int S, int VT, bool B>
+__global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmv_chains(dc_args P)
+{
+    using T = typename vt_of<VT>::T;
+    using V = typename vt_of<VT>::V;
+    constexpr int AH = kChainAhead;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * kChainWarps + warp;
+    if (gw >= P.warps)
+        return;
+    const int64_t s1 = P.wbeg[gw + 1];
+#pragma unroll 1
+    for (int64_t si = P.wbeg[gw]; si < s1; ++si) {
+        const dc_slice sl = P.slices[si];
+        const int mid = (int)(sl.geo >> kMidShift);
+        const dc_mat& M = B ? P.mats[mid] : P.A;
+        const T* X = static_cast<const T*>(B ? P.xs[mid] : P.x);
+        T* Y = static_cast<T*>(B ? P.ys[mid] : P.y);
+        const int64_t ldx = B ? 1 : P.ldx, ldy = B ? 1 : P.ldy;
+        const uint32_t* W = M.words + sl.base;
+        const V* Vv = static_cast<const V*>(M.vals) + sl.base;
         const int64_t row = (int64_t)sl.brow * S + sl.meta;
         const int len = (int)sl.steps;
-        T* pb = pbuf[warp];
-        // slot j: the value and x of step c + j; the word of step c + j + kAhead
-        uint32_t wq[kAhead];
-        T vq[kAhead], xq[kAhead];
+        // slot j: the value and x of step c + j; the word of step c + j + AH
+        uint32_t wq[AH];
+        T vq[AH], xq[AH];
 #pragma unroll
-        for (int j = 0; j < kAhead; ++j) {
+        for (int j = 0; j < AH; ++j) {
             const int e = 32 * j + lane;
             wq[j] = e < len ? ld_stream(W + e) : 0u;
         }
 #pragma unroll
-        for (int j = 0; j < kAhead; ++j) {
+        for (int j = 0; j < AH; ++j) {
             const int e = 32 * j + lane;
             vq[j] = e < len ? wide(ld_stream(Vv + e)) : T(0);
             xq[j] = e < len ? __ldg(X + (int64_t)wq[j] * ldx) : T(0);
-            wq[j] = e + 32 * kAhead < len ? ld_stream(W + e + 32 * kAhead) : 0u;
+            wq[j] = e + 32 * AH < len ? ld_stream(W + e + 32 * AH) : 0u;
         }
         T run = Y[row * ldy];
+        // whole groups of AH full steps: straight-line code, the refills
+        // clamped to the row (what they fetch past its end is never used), so
+        // that the next steps' loads and shuffles interleave with this step's
+        // adds
+        int b0 = 0;
 #pragma unroll 1
-        for (int b0 = 0; b0 < len; b0 += 32 * kAhead) {
+        for (; b0 + 32 * AH <= len; b0 += 32 * AH) {
 #pragma unroll
-            for (int j = 0; j < kAhead; ++j) {
-                const int base = b0 + 32 * j;
-                if (base >= len)
-                    break;
-                pb[lane] = base + lane < len ? dmul(vq[j], xq[j]) : T(0);
-                const int e = base + 32 * kAhead + lane;  // refill slot j: kAhead steps on
-                vq[j] = e < len ? wide(ld_stream(Vv + e)) : T(0);
-                xq[j] = e < len ? __ldg(X + (int64_t)wq[j] * ldx) : T(0);
-                wq[j] = e + 32 * kAhead < len ? ld_stream(W + e + 32 * kAhead) : 0u;
-                __syncwarp();
-                run = add_in_order(run, pb, min(32, len - base));
-                __syncwarp();
+            for (int j = 0; j < AH; ++j) {
+                const T p = dmul(vq[j], xq[j]);
+                const int e = b0 + 32 * j + 32 * AH + lane;  // refill slot j: AH steps on
+                vq[j] = wide(ld_stream(Vv + min(e, len - 1)));
+                xq[j] = __ldg(X + (int64_t)wq[j] * ldx);
+                wq[j] = ld_stream(W + min(e + 32 * AH, len - 1));
+                run = add_in_order(run, p, 32);
             }
+        }
+        // the last, partial group
+#pragma unroll
+        for (int j = 0; j < AH; ++j) {
+            const int base = b0 + 32 * j;
+            if (base >= len)
+                break;
+            const T p = base + lane < len ? dmul(vq[j], xq[j]) : T(0);
+            run = add_in_order(run, p, min(32, len - base));
         }
         if (lane == 0)
             Y[row * ldy] = run;
@@ -246,10 +289,14 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmv_slices(dc_args P)
 
 // --------------------------------------------------------------- preparation
 
-// Block rows the slices may serve: no dense tile (its stored zeros would
-// need words too) and at most `avg` elements per tile on average.
-__global__ void k_dc_classify(int64_t nr, const uint32_t* __restrict__ rows, tiles_view A, float avg,
-                              uint8_t* __restrict__ ok, int64_t* __restrict__ elems)
+// Block rows the slices serve: no dense tile (its stored zeros would need
+// words too), and at most `avg` elements per tile on average or more than
+// kRingTilesMax tiles (one CTA of the ring kernel sums a whole block row, so
+// a block row of very many tiles would keep one SM busy long after the rest).
+// fbytes[k]: the block row's share of the format bytes (its brow_ptr entry,
+// its tiles' headers, payloads and values).
+__global__ void k_dc_classify(int64_t nr, const uint32_t* __restrict__ rows, tiles_view A, float avg, int vsize,
+                              uint8_t* __restrict__ ok, int64_t* __restrict__ elems, int64_t* __restrict__ fbytes)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nr; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t I = rows[k], t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
@@ -257,8 +304,9 @@ __global__ void k_dc_classify(int64_t nr, const uint32_t* __restrict__ rows, til
         for (int64_t t = t0; t < t1 && sparse; ++t)
             sparse = A.tile_scheme[t] != ABHSF_SCHEME_DENSE;
         const int64_t e = A.tile_val_off[t1] - A.tile_val_off[t0];
-        ok[k] = sparse && (double)e <= (double)avg * (double)(t1 - t0) ? 1 : 0;
+        ok[k] = sparse && ((double)e <= (double)avg * (double)(t1 - t0) || t1 - t0 > kRingTilesMax) ? 1 : 0;
         elems[k] = e;
+        fbytes[k] = 8 + (t1 - t0) * (4 + 4 + 1 + 8 + 8) + (A.tile_idx_off[t1] - A.tile_idx_off[t0]) + vsize * e;
     }
 }
 
@@ -381,13 +429,28 @@ __global__ void k_dc_emit(int64_t E, const uint32_t* __restrict__ key, const uin
 
 inline unsigned grid_of(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 8192)); }
 
-int stream_grid_warps(int64_t items)
+// Warps of a launch: the chains one CTA per SM; the sliced rows every
+// resident CTA, less one per SM when chains run beside them (their CTA needs
+// the registers).
+int stream_grid_warps(int64_t items, bool chains, bool beside_chains)
 {
     int dev = 0, nsm = 0;
     ABHSF_CUDA(cudaGetDevice(&dev));
     ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const int64_t full = (int64_t)nsm * kCtasPerSm * kWarpsPerCta;
+    const int64_t full = chains ? (int64_t)nsm * kChainGridPerSm * kChainWarps
+                                : (int64_t)nsm * (kCtasPerSm - (beside_chains ? 1 : 0)) * kWarpsPerCta;
     return (int)std::max<int64_t>(1, std::min<int64_t>(full, items));
+}
+
+// The side stream and the fork / join events of a handle with chains.
+void make_side(cudaStream_t& side, cudaEvent_t& fork, cudaEvent_t& join)
+{
+    if (!side)
+        ABHSF_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    if (!fork)
+        ABHSF_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    if (!join)
+        ABHSF_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
 }
 
 // Time a slice takes, for the deal: a sliced one walks its longest row, a
@@ -399,10 +462,11 @@ inline uint64_t slice_weight(const abhsf_matrix::dc_slice_host& p)
 
 }  // namespace
 
-// Longest-processing-time deal of the slices of several matrices (block rows
-// in [brow_lo, brow_hi) only) over the warps of one launch.
+// Longest-processing-time deal of the sliced rows (or the chains) of several
+// matrices (block rows in [brow_lo, brow_hi) only) over the warps of one
+// launch.
 void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sched, dbuf<int64_t>& wbeg_d,
-                 int& warps_out, cudaStream_t st, int64_t brow_lo, int64_t brow_hi)
+                 int& warps_out, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, bool chains)
 {
     struct item {
         uint64_t w;
@@ -410,16 +474,21 @@ void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sc
         uint32_t k;
     };
     std::vector<item> items;
+    bool other = false;  // a slice of the other kind in the range
     for (size_t i = 0; i < mats.size(); ++i) {
         const auto& ps = mats[i]->dc_host;
         for (size_t k = 0; k < ps.size(); ++k)
-            if ((int64_t)ps[k].brow >= brow_lo && (int64_t)ps[k].brow < brow_hi)
-                items.push_back(item{slice_weight(ps[k]), (uint32_t)i, (uint32_t)k});
+            if ((int64_t)ps[k].brow >= brow_lo && (int64_t)ps[k].brow < brow_hi) {
+                if (ps[k].chain == chains)
+                    items.push_back(item{slice_weight(ps[k]), (uint32_t)i, (uint32_t)k});
+                else
+                    other = true;
+            }
     }
     warps_out = 0;
     if (items.empty())
         return;
-    const int W = stream_grid_warps((int64_t)items.size());
+    const int W = stream_grid_warps((int64_t)items.size(), chains, !chains && other);
     std::stable_sort(items.begin(), items.end(), [](const item& a, const item& b) { return a.w > b.w; });
     using load_t = std::pair<uint64_t, int>;
     std::priority_queue<load_t, std::vector<load_t>, std::greater<load_t>> heap;
@@ -466,21 +535,24 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
 {
     a.dc_host.clear();
     a.dc_tree_flag.assign((size_t)a.tree_nrows, 0);
-    a.dc_warps = 0;
+    a.dc_warps = a.dc_cwarps = 0;
     a.dc_elements = a.dc_rows = a.dc_slots = a.dc_lane_records = 0;
     const int s = a.s, lg = a.lg;
     if (avg <= 0.f || a.tree_nrows == 0 || a.sum_order != ABHSF_SUM_REFERENCE || (uint64_t)a.n > (uint64_t(1) << 32))
         return;
     const int64_t nr = a.tree_nrows;
     dbuf<uint8_t> ok(nr);
-    dbuf<int64_t> elems(nr);
-    k_dc_classify<<<grid_of(nr), 256, 0, st>>>(nr, a.tree_rows.get(), a.view(), avg, ok.get(), elems.get());
+    dbuf<int64_t> elems(nr), fbytes(nr);
+    const int vsize = (int)value_size(a.value_type);
+    k_dc_classify<<<grid_of(nr), 256, 0, st>>>(nr, a.tree_rows.get(), a.view(), avg, vsize, ok.get(), elems.get(),
+                                                fbytes.get());
     ABHSF_CUDA(cudaGetLastError());
     std::vector<uint8_t> okh(nr);
-    std::vector<int64_t> eh(nr);
+    std::vector<int64_t> eh(nr), fh(nr);
     std::vector<uint32_t> rows(nr);
     ABHSF_CUDA(cudaMemcpyAsync(okh.data(), ok.get(), nr, cudaMemcpyDeviceToHost, st));
     ABHSF_CUDA(cudaMemcpyAsync(eh.data(), elems.get(), nr * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    ABHSF_CUDA(cudaMemcpyAsync(fh.data(), fbytes.get(), nr * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     ABHSF_CUDA(cudaMemcpyAsync(rows.data(), a.tree_rows.get(), nr * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     ABHSF_CUDA(cudaStreamSynchronize(st));
     // slice block rows in ascending block-row order
@@ -613,67 +685,71 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
         emit(uint16_t{});
     ABHSF_CUDA(cudaGetLastError());
     ABHSF_CUDA(cudaStreamSynchronize(st));
-    for (int64_t k = 0; k < ns; ++k)
+    int64_t moved = 0;  // format bytes of the block rows the slices take over
+    for (int64_t k = 0; k < ns; ++k) {
         a.dc_tree_flag[sel[k].second] = 1;
+        moved += fh[sel[k].second];
+    }
+    int64_t live_lanes = 0;
+    for (const auto& h : SL)
+        live_lanes += h.chain ? 0 : h.lanes;
+    a.stats.spmv_bytes = a.stats.format_bytes - moved + E * (int64_t)(sizeof(uint32_t) + vs) +
+                         (int64_t)SL.size() * (int64_t)sizeof(dc_slice) + live_lanes * (int64_t)sizeof(uint32_t);
     a.dc_elements = E;
     a.dc_rows = ns;
     a.dc_slots = slots;
     a.dc_lane_records = (int64_t)lane_rec.size();
-    deal_slices({&a}, a.dc_sched, a.dc_wbeg, a.dc_warps, st, 0, INT64_MAX);
+    deal_slices({&a}, a.dc_sched, a.dc_wbeg, a.dc_warps, st, 0, INT64_MAX, false);
+    deal_slices({&a}, a.dc_csched, a.dc_cwbeg, a.dc_cwarps, st, 0, INT64_MAX, true);
+    if (a.dc_cwarps)
+        make_side(a.dc_side, a.dc_fork, a.dc_join);
 }
 
 namespace {
 
 template <int S, int VT, bool B>
-void launch_slices_s(const dc_args& P, cudaStream_t st)
+void launch_kind(bool chains, const dc_args& P, cudaStream_t st)
 {
-    const unsigned grid = (unsigned)((P.warps + kWarpsPerCta - 1) / kWarpsPerCta);
-    k_spmv_slices<S, VT, B><<<grid, 32 * kWarpsPerCta, 0, st>>>(P);
+    if (chains) {
+        const unsigned grid = (unsigned)((P.warps + kChainWarps - 1) / kChainWarps);
+        k_spmv_chains<S, VT, B><<<grid, 32 * kChainWarps, 0, st>>>(P);
+    } else {
+        const unsigned grid = (unsigned)((P.warps + kWarpsPerCta - 1) / kWarpsPerCta);
+        k_spmv_slices<S, VT, B><<<grid, 32 * kWarpsPerCta, 0, st>>>(P);
+    }
     ABHSF_CUDA(cudaGetLastError());
 }
 
 template <int VT, bool B>
-void launch_slices_vt(int s, const dc_args& P, cudaStream_t st)
+void launch_vt(int s, bool chains, const dc_args& P, cudaStream_t st)
 {
     switch (s) {
-    case 16: launch_slices_s<16, VT, B>(P, st); break;
-    case 32: launch_slices_s<32, VT, B>(P, st); break;
-    case 64: launch_slices_s<64, VT, B>(P, st); break;
-    case 128: launch_slices_s<128, VT, B>(P, st); break;
-    default: launch_slices_s<256, VT, B>(P, st); break;
+    case 16: launch_kind<16, VT, B>(chains, P, st); break;
+    case 32: launch_kind<32, VT, B>(chains, P, st); break;
+    case 64: launch_kind<64, VT, B>(chains, P, st); break;
+    case 128: launch_kind<128, VT, B>(chains, P, st); break;
+    default: launch_kind<256, VT, B>(chains, P, st); break;
     }
 }
 
-void launch_slices(int s, int vt, bool batch, const dc_args& P, cudaStream_t st)
+void launch(int s, int vt, bool batch, bool chains, const dc_args& P, cudaStream_t st)
 {
     if (P.warps == 0)
         return;
     if (vt == ABHSF_VALUE_F64)
-        batch ? launch_slices_vt<ABHSF_VALUE_F64, true>(s, P, st) : launch_slices_vt<ABHSF_VALUE_F64, false>(s, P, st);
+        batch ? launch_vt<ABHSF_VALUE_F64, true>(s, chains, P, st) : launch_vt<ABHSF_VALUE_F64, false>(s, chains, P, st);
     else if (vt == ABHSF_VALUE_F32)
-        batch ? launch_slices_vt<ABHSF_VALUE_F32, true>(s, P, st) : launch_slices_vt<ABHSF_VALUE_F32, false>(s, P, st);
+        batch ? launch_vt<ABHSF_VALUE_F32, true>(s, chains, P, st) : launch_vt<ABHSF_VALUE_F32, false>(s, chains, P, st);
     else
-        batch ? launch_slices_vt<ABHSF_VALUE_BF16, true>(s, P, st)
-              : launch_slices_vt<ABHSF_VALUE_BF16, false>(s, P, st);
+        batch ? launch_vt<ABHSF_VALUE_BF16, true>(s, chains, P, st)
+              : launch_vt<ABHSF_VALUE_BF16, false>(s, chains, P, st);
 }
 
 dc_mat mat_of(const abhsf_matrix& a) { return dc_mat{a.dc_words.get(), a.dc_vals.get(), a.dc_lane.get(), a.m}; }
 
-}  // namespace
-
-// y += A x over the slice block rows (x[i * ldx], y[i * ldy], elements of
-// the matrix's compute type); sched / wbeg / warps default to the matrix's
-// own schedule.  Returns false when the matrix has no slices.
-bool spmv_stream(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int64_t ldy, cudaStream_t st,
-                 const uint8_t* sched, const int64_t* wbeg, int warps)
+dc_args args_of(const abhsf_matrix& a, const uint8_t* sched, const int64_t* wbeg, int warps, const void* x,
+                int64_t ldx, void* y, int64_t ldy)
 {
-    if (!sched) {
-        sched = a.dc_sched.get();
-        wbeg = a.dc_wbeg.get();
-        warps = a.dc_warps;
-    }
-    if (warps == 0)
-        return false;
     dc_args P{};
     P.slices = reinterpret_cast<const dc_slice*>(sched);
     P.wbeg = wbeg;
@@ -683,14 +759,71 @@ bool spmv_stream(const abhsf_matrix& a, const void* x, int64_t ldx, void* y, int
     P.y = y;
     P.ldx = ldx;
     P.ldy = ldy;
-    launch_slices(a.s, a.value_type, false, P, st);
-    return true;
+    return P;
 }
 
-// The slices of every matrix of a batch in one launch.
+dc_args batch_args(const abhsf_batch& b, const uint8_t* sched, const int64_t* wbeg, int warps,
+                   const double* const* xs, double* const* ys)
+{
+    dc_args P{};
+    P.slices = reinterpret_cast<const dc_slice*>(sched);
+    P.wbeg = wbeg;
+    P.warps = warps;
+    P.mats = reinterpret_cast<const dc_mat*>(b.dc_table.get());
+    P.xs = reinterpret_cast<const void* const*>(xs);
+    P.ys = reinterpret_cast<void* const*>(ys);
+    P.ldx = P.ldy = 1;
+    return P;
+}
+
+// Chains on the side stream, after everything queued on st so far.
+void fork_chains(cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, int s, int vt, bool batch,
+                 const dc_args& P)
+{
+    ABHSF_CUDA(cudaEventRecord(fork, st));
+    ABHSF_CUDA(cudaStreamWaitEvent(side, fork, 0));
+    launch(s, vt, batch, true, P, side);
+    ABHSF_CUDA(cudaEventRecord(join, side));
+}
+
+}  // namespace
+
+dc_plan plan_of(const abhsf_matrix& a)
+{
+    dc_plan p;
+    p.sched = a.dc_sched.get();
+    p.wbeg = a.dc_wbeg.get();
+    p.warps = a.dc_warps;
+    p.csched = a.dc_csched.get();
+    p.cwbeg = a.dc_cwbeg.get();
+    p.cwarps = a.dc_cwarps;
+    return p;
+}
+
+void slices_begin(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
+                  cudaStream_t st)
+{
+    if (p.cwarps == 0)
+        return;
+    if (!a.dc_side)
+        fail(ABHSF_ERROR_CUDA, "matrix has chains but no side stream");
+    fork_chains(st, a.dc_side, a.dc_fork, a.dc_join, a.s, a.value_type, false,
+                args_of(a, p.csched, p.cwbeg, p.cwarps, x, ldx, y, ldy));
+}
+
+void slices_end(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
+                cudaStream_t st)
+{
+    if (p.warps)
+        launch(a.s, a.value_type, false, false, args_of(a, p.sched, p.wbeg, p.warps, x, ldx, y, ldy), st);
+    if (p.cwarps)
+        ABHSF_CUDA(cudaStreamWaitEvent(st, a.dc_join, 0));
+}
+
+// The slices of every matrix of a batch in one launch (and its chains in one more).
 void prepare_batch_stream(abhsf_batch& b, cudaStream_t st)
 {
-    b.dc_warps = 0;
+    b.dc_warps = b.dc_cwarps = 0;
     std::vector<dc_mat> t;
     bool any = false;
     for (const abhsf_matrix* a : b.mats) {
@@ -701,22 +834,26 @@ void prepare_batch_stream(abhsf_batch& b, cudaStream_t st)
         return;
     b.dc_table.alloc(t.size() * sizeof(dc_mat));
     ABHSF_CUDA(cudaMemcpyAsync(b.dc_table.get(), t.data(), t.size() * sizeof(dc_mat), cudaMemcpyHostToDevice, st));
-    deal_slices(b.mats, b.dc_sched, b.dc_wbeg, b.dc_warps, st, 0, INT64_MAX);
+    deal_slices(b.mats, b.dc_sched, b.dc_wbeg, b.dc_warps, st, 0, INT64_MAX, false);
+    deal_slices(b.mats, b.dc_csched, b.dc_cwbeg, b.dc_cwarps, st, 0, INT64_MAX, true);
+    if (b.dc_cwarps)
+        make_side(b.dc_side, b.dc_fork, b.dc_join);
 }
 
-void batch_stream(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st)
+void batch_stream_begin(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st)
 {
-    if (b.dc_warps == 0)
-        return;
-    dc_args P{};
-    P.slices = reinterpret_cast<const dc_slice*>(b.dc_sched.get());
-    P.wbeg = b.dc_wbeg.get();
-    P.warps = b.dc_warps;
-    P.mats = reinterpret_cast<const dc_mat*>(b.dc_table.get());
-    P.xs = reinterpret_cast<const void* const*>(xs);
-    P.ys = reinterpret_cast<void* const*>(ys);
-    P.ldx = P.ldy = 1;
-    launch_slices(b.s, ABHSF_VALUE_F64, true, P, st);
+    if (b.dc_cwarps)
+        fork_chains(st, b.dc_side, b.dc_fork, b.dc_join, b.s, ABHSF_VALUE_F64, true,
+                    batch_args(b, b.dc_csched.get(), b.dc_cwbeg.get(), b.dc_cwarps, xs, ys));
+}
+
+void batch_stream_end(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st)
+{
+    if (b.dc_warps)
+        launch(b.s, ABHSF_VALUE_F64, true, false, batch_args(b, b.dc_sched.get(), b.dc_wbeg.get(), b.dc_warps, xs, ys),
+               st);
+    if (b.dc_cwarps)
+        ABHSF_CUDA(cudaStreamWaitEvent(st, b.dc_join, 0));
 }
 
 }  // namespace abhsf

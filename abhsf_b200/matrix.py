@@ -222,7 +222,7 @@ class AbhsfMatrix:
             "tiles_per_scheme": dict(zip(capi.SCHEME_NAMES, list(s.tiles_per_scheme))),
             "nnz_per_scheme": dict(zip(capi.SCHEME_NAMES, list(s.nnz_per_scheme))),
             "stored_values": s.stored_values, "payload_bytes": s.payload_bytes, "format_bytes": s.format_bytes,
-            "msmf_bits": list(s.msmf_bits),
+            "msmf_bits": list(s.msmf_bits), "spmv_bytes": s.spmv_bytes,
         }
 
     def export(self) -> dict:

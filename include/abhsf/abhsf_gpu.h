@@ -139,8 +139,9 @@ typedef struct abhsf_build_opts {
     int64_t bits_per_value;   /* dense-cost element width; 0 = width of value_type */
     int32_t selector;         /* abhsf_selector, used when block_size is 0 */
     int32_t slice_tile_nnz;   /* reference-order SpMV at s = 32 / 64: block rows without a dense tile whose
-                                 tiles hold at most this many elements on average are summed from
-                                 delta-coded row slices; 0 = the library's default (32), -1 = none */
+                                 tiles hold at most this many elements on average, or that have more
+                                 than 256 tiles, are summed from delta-coded row slices; 0 = the
+                                 library's default (32), -1 = none */
     const float* selector_model; /* host, ABHSF_MLP_PARAMS floats; NULL = the model built into the library */
 } abhsf_build_opts;
 
@@ -190,6 +191,10 @@ typedef struct abhsf_stats {
     uint64_t msmf_bits[8];  /* this block size's mmf line at the dense-cost width:
                                coo32 csr32 coo csr bitmap dense abhsf abhsf134,
                                values included (block_statistics/mmf.cpp:122-138) */
+    int64_t spmv_bytes;     /* what one reference-order SpMV reads of the matrix (x and y excluded): the
+                               format bytes of the block rows the tile kernel sums, and for the block
+                               rows in row slices their words, values, lane records and slice records
+                               (format_bytes when no block row is in slices) */
 } abhsf_stats;
 
 /* Fills the defaults: s = 64, f64, CSR allowed, REAL, minimum storage, host

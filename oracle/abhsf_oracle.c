@@ -613,6 +613,7 @@ void orc_abs_spmv_elements(const int64_t* rows, const int64_t* cols, const doubl
  * than ORC_CHAIN_MIN elements alone as a chain with absolute columns.
  * ------------------------------------------------------------------------ */
 #define ORC_CHAIN_MIN 256
+#define ORC_RING_TILES_MAX 256
 
 /* Elements of tile t in the format's order: local row / column of each. */
 static int64_t tile_elements(const orc_matrix* a, int64_t t, int* lr, int* lc)
@@ -697,7 +698,8 @@ int orc_slices_build(const orc_matrix* a, double avg, orc_slices** out)
     const int s = a->s;
     if (avg <= 0 || (uint64_t)a->n > ((uint64_t)1 << 32))
         return ORC_OK;
-    /* the block rows: non-empty, no dense tile, at most avg elements per tile */
+    /* the block rows: non-empty, no dense tile, at most avg elements per tile
+     * on average or more than ORC_RING_TILES_MAX tiles */
     uint8_t* sel = (uint8_t*)calloc((size_t)a->M + 1, 1);
     int64_t E = 0, ns = 0;
     for (int64_t I = 0; I < a->M; ++I) {
@@ -708,7 +710,7 @@ int orc_slices_build(const orc_matrix* a, double avg, orc_slices** out)
         for (int64_t t = t0; t < t1; ++t)
             ok = ok && a->tile_scheme[t] != ORC_DENSE;
         const int64_t e = a->tile_val_off[t1] - a->tile_val_off[t0];
-        if (ok && (double)e <= avg * (double)(t1 - t0)) {
+        if (ok && ((double)e <= avg * (double)(t1 - t0) || t1 - t0 > ORC_RING_TILES_MAX)) {
             sel[I] = 1;
             E += e;
             ++ns;

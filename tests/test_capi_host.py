@@ -24,7 +24,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_layouts():
     assert C.sizeof(capi.BuildOpts) == 56
-    assert C.sizeof(capi.Stats) == 208
+    assert C.sizeof(capi.Stats) == 216
 
 
 def test_cost_model_matches_oracle():
