@@ -104,6 +104,8 @@ PROTOTYPES = {
     "abhsf_test_ring_variant": (C.c_int, [_vp, _i32, C.POINTER(_i32), C.POINTER(_i32)]),
     "abhsf_test_device_allocations": (_i64, []),
     "abhsf_slices_info": (C.c_int, [_vp] + [C.POINTER(_i64)] * 5),
+    "abhsf_batch_kernels": (C.c_int, [_vp, C.POINTER(_i32)]),
+    "abhsf_spmv_kernels": (C.c_int, [_vp, C.POINTER(_i32)]),
     "abhsf_slices_export": (C.c_int, [_vp] * 10),
     "abhsf_last_error_string": (C.c_char_p, []),
     "abhsf_build_opts_default": (None, [C.POINTER(BuildOpts)]),

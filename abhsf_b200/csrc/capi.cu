@@ -121,6 +121,25 @@ abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, const double*
     });
 }
 
+abhsf_status abhsf_spmv_kernels(const abhsf_matrix* a, int32_t* kernels)
+{
+    return guarded([&] {
+        if (!a || !kernels)
+            fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle and kernels must be non-NULL");
+        int k = 0;
+        if (a->T > 0) {
+            if (a->sum_order != ABHSF_SUM_REFERENCE)
+                k = 1;  // the tree-order kernel
+            else {
+                const bool seq = !a->ring_ready && (a->s == 32 || a->s == 64 ? true : a->seq_nrows > 0 || a->dc_rows == 0);
+                k = (a->ring_ready ? (a->ring_warps > 0 ? 1 : 0) : (seq ? 1 : 0)) + (a->dc_warps > 0 ? 1 : 0) +
+                    (a->dc_cwarps > 0 ? 1 : 0);
+            }
+        }
+        *kernels = k;
+    });
+}
+
 abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double* y, abhsf_stream_t stream)
 {
     return guarded([&] {
@@ -150,7 +169,8 @@ abhsf_status abhsf_spmv_f32(const abhsf_matrix* a, const float* x, float* y, abh
         if (a->m == 0 || a->T == 0)
             return;
         if (!abhsf::spmv_f32_ring(*a, x, y, reinterpret_cast<cudaStream_t>(stream)))
-            fail(ABHSF_ERROR_UNSUPPORTED, "abhsf_spmv_f32 supports block sizes 32 and 64");
+            fail(ABHSF_ERROR_UNSUPPORTED,
+                 "abhsf_spmv_f32 supports block sizes 32 and 64, and others where every block row is in row slices");
     });
 }
 
@@ -229,6 +249,15 @@ abhsf_status abhsf_batch_spmv(const abhsf_batch* b, const double* const* xs, dou
         if (!xs || !ys)
             fail(ABHSF_ERROR_INVALID_VALUE, "xs and ys must be non-NULL device arrays");
         abhsf::batch_spmv(*b, xs, ys, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+abhsf_status abhsf_batch_kernels(const abhsf_batch* b, int32_t* kernels)
+{
+    return guarded([&] {
+        if (!b || !kernels)
+            fail(ABHSF_ERROR_INVALID_VALUE, "batch handle and kernels must be non-NULL");
+        *kernels = (b->ctas > 0 ? 1 : 0) + (b->dc_warps > 0 ? 1 : 0) + (b->dc_cwarps > 0 ? 1 : 0);
     });
 }
 

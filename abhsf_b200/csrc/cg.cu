@@ -337,7 +337,7 @@ void cg_solve_mixed(const abhsf_matrix& a64, const abhsf_matrix& a32, const doub
     check_square(a64);
     if (a32.m != a64.m || a32.n != a64.n)
         fail(ABHSF_ERROR_INVALID_VALUE, "the two matrices of the mixed solver differ in shape");
-    if (!a32.ring_ready && a32.T > 0)
+    if (!(a32.ring_ready || (a32.dc_rows > 0 && a32.dc_rows == a32.tree_nrows)) && a32.T > 0)
         fail(ABHSF_ERROR_UNSUPPORTED, "the f32 SpMV of the mixed solver supports block sizes 32 and 64");
     const int64_t n = a64.n;
     const double f2 = update_factor * update_factor;

@@ -205,6 +205,8 @@ struct abhsf_matrix {
     abhsf::dbuf<uint8_t> dc_sched;       // the matrix's own launch: sliced rows in warp order
     abhsf::dbuf<int64_t> dc_wbeg;
     int dc_warps = 0;
+    abhsf::dbuf<uint32_t> seq_rows;      // block sizes 16 / 128 / 256: the block rows the streaming kernel sums
+    int64_t seq_nrows = 0;               // (the others are in slices)
     abhsf::dbuf<uint8_t> dc_csched;      // ... and its chains, launched on dc_side beside the others
     abhsf::dbuf<int64_t> dc_cwbeg;
     int dc_cwarps = 0;

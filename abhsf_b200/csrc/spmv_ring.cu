@@ -1417,7 +1417,30 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
 {
     a.ring_warps = 0;
     a.ring_ready = false;
-    if ((a.s != 32 && a.s != 64) || a.tree_nrows == 0 || a.M > (int64_t)kRowMask)
+    if (a.tree_nrows == 0)
+        return;
+    if (a.s != 32 && a.s != 64) {
+        // no ring kernel: the slices take the hypersparse block rows, the
+        // streaming kernel (spmv_seq.cu) the rest
+        prepare_stream(a, a.dc_avg, st);
+        if (a.dc_rows > 0) {
+            std::vector<uint32_t> rows(a.tree_nrows), keep;
+            ABHSF_CUDA(cudaMemcpyAsync(rows.data(), a.tree_rows.get(), a.tree_nrows * sizeof(uint32_t),
+                                       cudaMemcpyDeviceToHost, st));
+            ABHSF_CUDA(cudaStreamSynchronize(st));
+            for (int64_t k = 0; k < a.tree_nrows; ++k)
+                if (!a.dc_tree_flag[k])
+                    keep.push_back(rows[k]);
+            a.seq_nrows = (int64_t)keep.size();
+            a.seq_rows.alloc(std::max<size_t>(keep.size(), 1));
+            if (!keep.empty())
+                ABHSF_CUDA(cudaMemcpyAsync(a.seq_rows.get(), keep.data(), keep.size() * sizeof(uint32_t),
+                                           cudaMemcpyHostToDevice, st));
+            ABHSF_CUDA(cudaStreamSynchronize(st));
+        }
+        return;
+    }
+    if (a.M > (int64_t)kRowMask)
         return;
     if (a.value_type == ABHSF_VALUE_F64) {
         if (a.s == 32)
@@ -1531,8 +1554,17 @@ bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream
 
 bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st)
 {
-    if (!a.ring_ready || a.value_type == ABHSF_VALUE_F64)
+    if (a.value_type == ABHSF_VALUE_F64)
         return false;
+    if (!a.ring_ready) {
+        if (a.dc_rows == 0 || a.dc_rows != a.tree_nrows)
+            return false;
+        std::lock_guard<std::mutex> lock(a.dc_mu);  // every block row in slices (block sizes 16, 128, 256)
+        const dc_plan p = plan_of(a);
+        slices_begin(a, p, x, 1, y, 1, st);
+        slices_end(a, p, x, 1, y, 1, st);
+        return true;
+    }
     std::lock_guard<std::mutex> lock(a.dc_mu);
     const dc_plan p = plan_of(a);
     slices_begin(a, p, x, 1, y, 1, st);

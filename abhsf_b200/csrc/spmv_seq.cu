@@ -400,17 +400,18 @@ __global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_f64_seq(seq
 }
 
 template <int S>
-void launch_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+void launch_seq(const abhsf_matrix& a, const uint32_t* rows, int64_t nrows, const double* x, double* y,
+                cudaStream_t st)
 {
-    if (a.tree_nrows == 0)
+    if (nrows == 0)
         return;
     int dev = 0, nsm = 0, per_sm = 0;
     ABHSF_CUDA(cudaGetDevice(&dev));
     ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_f64_seq<S>, kWarps * 32, 0));
-    seq_args P{a.view(), a.tree_rows.get(), a.tree_nrows, a.tree_counter.get(), x, y};
+    seq_args P{a.view(), rows, nrows, a.tree_counter.get(), x, y};
     ABHSF_CUDA(cudaMemsetAsync(a.tree_counter.get(), 0, sizeof(unsigned int), st));
-    const int64_t ctas = (a.tree_nrows + kWarps - 1) / kWarps;
+    const int64_t ctas = (nrows + kWarps - 1) / kWarps;
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)nsm * std::max(per_sm, 1)));
     k_spmv_f64_seq<S><<<grid, kWarps * 32, 0, st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
@@ -418,18 +419,35 @@ void launch_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_t 
 
 }  // namespace
 
+// The streaming kernel over the block rows it serves: all of them, or those
+// the row slices leave (block sizes 16 / 128 / 256), the slices beside it.
 void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
     if (a.M == 0 || a.T == 0)
         return;
+    const bool slices = a.dc_rows > 0 && a.value_type == ABHSF_VALUE_F64 && a.sum_order == ABHSF_SUM_REFERENCE &&
+                        a.s != 32 && a.s != 64;
+    std::unique_lock<std::mutex> lock(a.dc_mu, std::defer_lock);
+    dc_plan p;
+    const uint32_t* rows = a.tree_rows.get();
+    int64_t nrows = a.tree_nrows;
+    if (slices) {
+        lock.lock();
+        p = plan_of(a);
+        slices_begin(a, p, x, 1, y, 1, st);
+        rows = a.seq_rows.get();
+        nrows = a.seq_nrows;
+    }
     switch (a.s) {
-    case 16: launch_seq<16>(a, x, y, st); break;
-    case 32: launch_seq<32>(a, x, y, st); break;
-    case 64: launch_seq<64>(a, x, y, st); break;
-    case 128: launch_seq<128>(a, x, y, st); break;
-    case 256: launch_seq<256>(a, x, y, st); break;
+    case 16: launch_seq<16>(a, rows, nrows, x, y, st); break;
+    case 32: launch_seq<32>(a, rows, nrows, x, y, st); break;
+    case 64: launch_seq<64>(a, rows, nrows, x, y, st); break;
+    case 128: launch_seq<128>(a, rows, nrows, x, y, st); break;
+    case 256: launch_seq<256>(a, rows, nrows, x, y, st); break;
     default: fail(ABHSF_ERROR_UNSUPPORTED, "block size without an SpMV kernel");
     }
+    if (slices)
+        slices_end(a, p, x, 1, y, 1, st);
 }
 
 }  // namespace abhsf

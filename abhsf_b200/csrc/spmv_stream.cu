@@ -290,9 +290,11 @@ __global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmv_chai
 // --------------------------------------------------------------- preparation
 
 // Block rows the slices serve: no dense tile (its stored zeros would need
-// words too), and at most `avg` elements per tile on average or more than
-// kRingTilesMax tiles (one CTA of the ring kernel sums a whole block row, so
-// a block row of very many tiles would keep one SM busy long after the rest).
+// words too), and no bitmap tile (the ring kernel's bitmap walk reads a bit
+// per position where a slice reads a word per element), at most `avg`
+// elements per tile on average, or more than kRingTilesMax tiles (one CTA of
+// the ring kernel sums a whole block row, so a block row of very many tiles
+// would keep one SM busy long after the rest).
 // fbytes[k]: the block row's share of the format bytes (its brow_ptr entry,
 // its tiles' headers, payloads and values).
 __global__ void k_dc_classify(int64_t nr, const uint32_t* __restrict__ rows, tiles_view A, float avg, int vsize,
@@ -300,11 +302,13 @@ __global__ void k_dc_classify(int64_t nr, const uint32_t* __restrict__ rows, til
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nr; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t I = rows[k], t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
-        bool sparse = true;
-        for (int64_t t = t0; t < t1 && sparse; ++t)
+        bool sparse = true, bitmap = false;
+        for (int64_t t = t0; t < t1 && sparse; ++t) {
             sparse = A.tile_scheme[t] != ABHSF_SCHEME_DENSE;
+            bitmap = bitmap || A.tile_scheme[t] == ABHSF_SCHEME_BITMAP;
+        }
         const int64_t e = A.tile_val_off[t1] - A.tile_val_off[t0];
-        ok[k] = sparse && ((double)e <= (double)avg * (double)(t1 - t0) || t1 - t0 > kRingTilesMax) ? 1 : 0;
+        ok[k] = sparse && ((double)e <= (double)avg * (double)(t1 - t0) || t1 - t0 > kRingTilesMax || !bitmap) ? 1 : 0;
         elems[k] = e;
         fbytes[k] = 8 + (t1 - t0) * (4 + 4 + 1 + 8 + 8) + (A.tile_idx_off[t1] - A.tile_idx_off[t0]) + vsize * e;
     }

@@ -241,6 +241,13 @@ class AbhsfMatrix:
         capi.check(capi.lib.abhsf_export_host(self._h, *p))
         return out
 
+    def kernels(self) -> int:
+        """Kernels one spmv of this matrix launches (abhsf_spmv_kernels)."""
+        self._check_open()
+        v = C.c_int32()
+        capi.check(capi.lib.abhsf_spmv_kernels(self._h, C.byref(v)))
+        return int(v.value)
+
     def slices(self) -> dict:
         """The delta-coded row slices the SpMV reads for the hypersparse block
         rows (abhsf_slices_info / abhsf_slices_export): per-slice arrays in
@@ -508,6 +515,13 @@ class AbhsfBatch:
     def status(self, clear: bool = False, stream=None) -> int:
         v = C.c_int32()
         capi.check(capi.lib.abhsf_batch_status(self._h, _stream_ptr(stream), int(clear), C.byref(v)))
+        return int(v.value)
+
+    def launches(self) -> int:
+        """Kernels one spmv launches (the tile kernel, the row-slice kernel,
+        the chain kernel: those the batch's matrices need)."""
+        v = C.c_int32()
+        capi.check(capi.lib.abhsf_batch_kernels(self._h, C.byref(v)))
         return int(v.value)
 
     def release(self) -> None:

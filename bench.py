@@ -9,6 +9,10 @@ step / kernel time, where algorithmic bytes B = format bytes + 8 n (x read
 once) + 16 m (y read and written).  e2e is the same metric through the
 host-memory call (x, y in pinned host memory; copies inside the timed region).
 
+Every further measurement (SpMM, the batch, low precision, CG, the other
+matrix shapes, cuSPARSE, the selector, ...) is printed as a JSON line of its
+own ({"section": name, ...}) before the headline line, which comes last.
+
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
 Multi-GPU (torchrun): every rank runs an independent replica (the SpMV has no
@@ -24,8 +28,11 @@ import statistics
 import subprocess
 import sys
 import time
+import warnings
 
 import numpy as np
+
+warnings.filterwarnings("ignore", message=".*[Ss]parse.*")  # torch's beta-state notes on CSR tensors
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -35,6 +42,7 @@ UNIT = "GB/s"
 FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 256 << 20
 DEFAULT_N = 4_194_304
+X_SEED = 1  # x U[-1, 1] of the timed matrix, in both arms
 KERNELS = {"reference": "k_spmv_f64_ring", "tree": "k_spmv_f64"}
 
 
@@ -115,7 +123,7 @@ def workload(args):
         c.name = f"laplacian3d g={args.grid} (7-point, diag 6, off -1)"
     else:
         c = W.tiled_mixture(n=args.n)
-        c.name = f"tiled_mixture n={c.n} tile=64 p=1.2266e-5 seed=1 (values N(0,1))"
+        c.name = f"tiled_mixture n={c.n} tile=64 p=1.2266e-5 seed=1 (values N(0,1)), x U[-1,1] seed {X_SEED}"
     log(f"workload: {c.name} nnz={c.nnz} ({time.time() - t0:.1f} s to generate)")
     return c
 
@@ -154,24 +162,22 @@ def time_spmm(A, c, st, dev, stream, l2_flush, warmup, ks=(4, 8, 16, 32), steps=
 
 
 def time_lowprec(c, dev, l2_flush, warmup, steps=10):
-    """f32 and bf16 copies of the same matrix: f32 SpMV time, algorithmic GB/s
-    (B_fmt + 4 n + 8 m) and error against the FP64 product of the same (f32)
-    x: normwise, and the largest |y - y64| / (|A| |x|) per element.  The same
-    errors on R-MAT scale 22 (n = 4,194,304, edge factor 16, values N(0,1))."""
+    """f32 and bf16 copies of the same matrix: f32 SpMV time, GB/s over what
+    one SpMV reads (spmv_bytes + 4 n + 8 m) and error against an FP64 product
+    of the same (f32) x computed apart from this library (torch's CSR SpMV,
+    cuSPARSE, in FP64): normwise, and the largest |y - y64| / (|A| |x|) per
+    element.  The same errors on R-MAT scale 22 (n = 4,194,304, edge factor
+    16, values N(0,1))."""
     import torch
     from abhsf_b200 import AbhsfMatrix
     from abhsf_b200 import workloads as W
 
     def errors(rows, cols, vals, m, n, vt, x32):
-        A64 = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=64)
-        y64 = torch.zeros(m, dtype=torch.float64, device=dev)
-        A64.spmv(x32.double(), y64)
-        A64.release()
-        absA = AbhsfMatrix.from_elements(rows, cols, vals.abs() if torch.is_tensor(vals) else np.abs(vals), m, n,
-                                         block_size=64)
-        scale = torch.zeros(m, dtype=torch.float64, device=dev)
-        absA.spmv(x32.double().abs(), scale)
-        absA.release()
+        Acs = _csr_tensor(rows, cols, vals, m, n, dev)
+        y64 = torch.mv(Acs, x32.double())
+        Aabs = torch.sparse_csr_tensor(Acs.crow_indices(), Acs.col_indices(), Acs.values().abs(), size=(m, n))
+        scale = torch.mv(Aabs, x32.double().abs())
+        del Acs, Aabs
         A = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=64, value_type=vt)
         y = torch.zeros(m, dtype=torch.float32, device=dev)
         A.spmv_f32(x32, y)
@@ -198,13 +204,14 @@ def time_lowprec(c, dev, l2_flush, warmup, steps=10):
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
         t = sum(ts) / len(ts)
-        b = int(A.stats()["format_bytes"]) + 4 * c.n + 8 * c.m
+        b = int(A.stats()["spmv_bytes"]) + 4 * c.n + 8 * c.m
         out[vt] = dict(err, ms=t, bytes=b, **{"GB/s": b / (t * 1e-3) / 1e9})
         A.release()
     rows, cols, vals, n = W.rmat_device(22, 16, seed=1, device=dev)
     x32 = torch.rand(n, dtype=torch.float32, device=dev) * 2 - 1
     out["rmat22"] = {"workload": f"R-MAT scale 22 edge factor 16 (0.57, 0.19, 0.19), nnz={rows.numel()}, "
-                                 "values N(0,1), x U[-1,1] f32, block size 64"}
+                                 "values N(0,1), x U[-1,1] f32, block size 64",
+                     "fp64_reference": "torch.mv on a CSR tensor (cuSPARSE), FP64"}
     for vt in ("f32", "bf16"):
         A, _, err = errors(rows, cols, vals, n, n, vt, x32)
         A.release()
@@ -225,11 +232,14 @@ def time_batched(dev, l2_flush, warmup, count=256, steps=10):
     sets = {32: [], 64: []}
     byts = {32: 0, 64: 0}
     nnz = 0
+    fbyts = {32: 0, 64: 0}
     for rows, cols, vals, m, n, _ in W.batched_set_device(count, seed=0, device=dev):
         for s in sets:
             A = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=s)
             sets[s].append(A)
-            byts[s] += int(A.stats()["format_bytes"]) + 8 * n + 16 * m
+            st_ = A.stats()
+            byts[s] += int(st_["spmv_bytes"]) + 8 * n + 16 * m
+            fbyts[s] += int(st_["format_bytes"]) + 8 * n + 16 * m
         nnz += int(rows.numel())
         del rows, cols, vals
     build_s = time.time() - t0
@@ -262,6 +272,7 @@ def time_batched(dev, l2_flush, warmup, count=256, steps=10):
     s_best = min(tune, key=tune.get)
     mats = sets[s_best]
     byts = byts[s_best]
+    fbyts = fbyts[s_best]
     batch = AbhsfBatch(mats)
     px, py = batch.pointer_tables(xs, ys)
 
@@ -283,8 +294,12 @@ def time_batched(dev, l2_flush, warmup, count=256, steps=10):
     out = {"workload": f"{count} matrices, n log-uniform [1k, 200k], even banded (bandwidth U[3,64]), odd R-MAT"
                        f"(0.57, 0.19, 0.19) edge factor 8, values N(0,1), generated on the GPU",
            "block_size": s_best, "autotune_ms": {str(k): v for k, v in tune.items()},
-           "nnz": nnz, "bytes_per_step": byts, "build_s": build_s,
-           "batched": {"ms": t_batch, "GB/s": byts / (t_batch * 1e-3) / 1e9, "launches": 1},
+           "nnz": nnz, "bytes_per_step": byts, "format_bytes_per_step": fbyts,
+           "bytes_note": "what one SpMV of every matrix reads (spmv_bytes + 8 n + 16 m); format_bytes_per_step counts "
+                         "the ABHSF arrays instead",
+           "build_s": build_s,
+           "batched": {"ms": t_batch, "GB/s": byts / (t_batch * 1e-3) / 1e9, "launches": batch.launches(),
+                       "graph": "capturable (one graph node per launch)"},
            "one_by_one": {"ms": t_loop, "GB/s": byts / (t_loop * 1e-3) / 1e9, "launches": count},
            "speedup": t_loop / t_batch, "matrix0_bitwise": same}
     batch.release()
@@ -296,47 +311,59 @@ def time_batched(dev, l2_flush, warmup, count=256, steps=10):
 
 def time_cg(dev, g=256, rtol=1e-10):
     """CG solve time on the 3D 7-point Laplacian g^3 (n = g^3, SPD, b U[-1,1]
-    seed 1, x0 = 0) to ||b - A x|| <= rtol ||b||: plain FP64 CG against the
-    tuned solver (f32 CG on an f32 copy, FP64 solution and reliable updates)."""
+    seed 1, x0 = 0) to ||b - A x|| <= rtol ||b||: the plain form (FP64 CG,
+    block size 64) against the tuned form: the block size the learned selector
+    picks, and mixed precision -- f32 CG on an f32 or a bf16 copy, the
+    solution, the residual replacement and the convergence test in FP64 --
+    with every 8 iterations replayed as one CUDA graph.  (6 and -1 are exact
+    in bf16, so the bf16 copy is the matrix itself.)"""
     import torch
     from abhsf_b200 import AbhsfMatrix, cg, cg_mixed
+    from abhsf_b200 import selector as sel
     from abhsf_b200 import workloads as W
     lap = W.laplacian_3d(g)
+    rows_d = torch.from_numpy(lap.rows).to(dev)
+    cols_d = torch.from_numpy(lap.cols).to(dev)
+    t0 = time.perf_counter()
+    s_learned = sel.predict(sel.features(rows_d, cols_d, lap.m, lap.n))
+    t_select = time.perf_counter() - t0
+    del rows_d, cols_d
     A64 = AbhsfMatrix.from_elements(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=64)
-    A32 = AbhsfMatrix.from_elements(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=64, value_type="f32")
+    L64 = AbhsfMatrix.from_elements(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=s_learned)
+    L32 = AbhsfMatrix.from_elements(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=s_learned,
+                                    value_type="f32")
+    L16 = AbhsfMatrix.from_elements(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=s_learned,
+                                    value_type="bf16")
     b = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, lap.n)).to(dev)
     out = {"workload": f"3D 7-point Laplacian {g}^3 (n={lap.n}, nnz={lap.nnz}, diag 6, off -1), b U[-1,1] seed 1, "
-                       f"x0 = 0, block size 64", "rtol": rtol}
-    # the solver's SpMV alone (working set > L2; CUDA events, 10 launches after 3)
-    xs = torch.rand(lap.n, dtype=torch.float64, device=dev)
-    ys = torch.zeros(lap.n, dtype=torch.float64, device=dev)
-    for _ in range(3):
-        A64.spmv(xs, ys)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(10):
-        A64.spmv(xs, ys)
-    e1.record()
-    torch.cuda.synchronize()
-    t = e0.elapsed_time(e1) / 10
-    byts = int(A64.stats()["format_bytes"]) + 8 * lap.n + 16 * lap.n
+                       f"x0 = 0", "rtol": rtol, "learned_block_size": s_learned, "select_s": t_select}
+    # each solver's SpMV alone (working set > L2; CUDA events, 10 launches after 3)
     peak, _ = hbm_peak()
-    out["spmv_f64"] = {"ms": t, "GB/s": byts / (t * 1e-3) / 1e9, "frac_of_peak": byts / (t * 1e-3) / 1e9 / peak,
-                       "bytes": byts}
-    del xs, ys
-    from abhsf_b200 import selector as sel
-    t0 = time.perf_counter()
-    _, s64, T64 = sel.autotune(lap.rows, lap.cols, lap.vals, lap.m, lap.n, candidates=(32, 64), keep=True)
-    ms32, s32, T32 = sel.autotune(lap.rows, lap.cols, lap.vals, lap.m, lap.n, candidates=(32, 64), value_type="f32",
-                                  keep=True)
-    out["autotune"] = {"f64_block_size": s64, "f32_block_size": s32, "f32_ms": ms32[1:3].tolist(),
-                       "seconds": time.perf_counter() - t0}
+    for key, M, dt in (("spmv_f64", A64, torch.float64), ("spmv_f32_copy", L32, torch.float32),
+                       ("spmv_bf16_copy", L16, torch.float32)):
+        xs = torch.rand(lap.n, dtype=dt, device=dev)
+        ys = torch.zeros(lap.n, dtype=dt, device=dev)
+        fn = (lambda: M.spmv(xs, ys)) if dt == torch.float64 else (lambda: M.spmv_f32(xs, ys))
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 10
+        es = 8 if dt == torch.float64 else 4
+        byts = int(M.stats()["spmv_bytes"]) + es * lap.n + 2 * es * lap.n
+        out[key] = {"ms": t, "GB/s": byts / (t * 1e-3) / 1e9, "frac_of_peak": byts / (t * 1e-3) / 1e9 / peak,
+                    "bytes": byts, "block_size": M.block_size}
+        del xs, ys
     # each solver twice from x0 = 0 (same iterations both times); the faster
     # solve is reported, both are listed, and the SM clocks are sampled
     clocks = ClockSampler(torch.cuda.current_device())
     for name, fn in (("plain", lambda x: cg(A64, b, x, rtol=rtol)),
-                     ("tuned", lambda x: cg_mixed(A64, A32, b, x, rtol=rtol, update_factor=0.1)),
-                     ("tuned_autotuned", lambda x: cg_mixed(T64, T32, b, x, rtol=rtol, update_factor=0.1))):
+                     ("tuned_f32", lambda x: cg_mixed(L64, L32, b, x, rtol=rtol, update_factor=0.1)),
+                     ("tuned_bf16", lambda x: cg_mixed(L64, L16, b, x, rtol=rtol, update_factor=0.1))):
         runs = []
         for _ in range(2):
             x = torch.zeros(lap.n, dtype=torch.float64, device=dev)
@@ -347,12 +374,13 @@ def time_cg(dev, g=256, rtol=1e-10):
             runs.append(time.perf_counter() - t0)
         out[name] = dict(info, seconds=min(runs), runs_s=runs)
     out["clocks"] = clocks.stop()
-    out["plain"]["solver"] = "FP64 CG, reference-order f64 SpMV"
-    out["tuned"]["solver"] = "f32 CG on an f32 copy, FP64 solution, FP64 residual replacement each 10x drop"
-    out["tuned_autotuned"]["solver"] = out["tuned"]["solver"] + ", block sizes autotuned over {32, 64}"
-    out["tuned_speedup"] = out["plain"]["seconds"] / out["tuned"]["seconds"]
-    out["tuned_autotuned_speedup"] = out["plain"]["seconds"] / out["tuned_autotuned"]["seconds"]
-    for M in (A64, A32, T64, T32):
+    out["plain"]["solver"] = "FP64 CG, block size 64, reference-order f64 SpMV"
+    out["tuned_f32"]["solver"] = (f"learned block size {s_learned}: f32 CG on an f32 copy, FP64 solution, FP64 "
+                                  "residual replacement each 10x drop")
+    out["tuned_bf16"]["solver"] = out["tuned_f32"]["solver"].replace("an f32 copy", "a bf16 copy")
+    out["tuned_f32_speedup"] = out["plain"]["seconds"] / out["tuned_f32"]["seconds"]
+    out["tuned_bf16_speedup"] = out["plain"]["seconds"] / out["tuned_bf16"]["seconds"]
+    for M in (A64, L64, L32, L16):
         M.release()
     return out
 
@@ -392,6 +420,93 @@ def time_cusparse(c, dev, l2_flush, warmup, ours_ms, steps=10):
                 "call": "torch.mv(sparse_csr_tensor int32 indices, f64 values) -> cuSPARSE SpMV"}
     except Exception as e:  # a reference point only: report why it is missing
         return {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+
+
+def _events_time(fn, l2_flush, warmup, steps):
+    """Mean CUDA-event time (ms) of fn on the current stream, L2 flushed
+    before every call."""
+    import torch
+    for _ in range(max(warmup, 1)):
+        l2_flush()
+        fn()
+    ts = []
+    for _ in range(steps):
+        l2_flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return sum(ts) / len(ts)
+
+
+def _csr_tensor(rows, cols, vals, m, n, dev):
+    """torch CSR tensor (int32 indices, f64 values) of COO triplets on dev."""
+    import torch
+    rows = torch.as_tensor(rows, device=dev)
+    cols = torch.as_tensor(cols, device=dev)
+    vals = torch.as_tensor(vals, device=dev, dtype=torch.float64)
+    order = torch.argsort(rows * n + cols)
+    crow = torch.zeros(m + 1, dtype=torch.int64, device=dev)
+    crow[1:] = torch.cumsum(torch.bincount(rows, minlength=m), 0)
+    return torch.sparse_csr_tensor(crow.to(torch.int32), cols[order].to(torch.int32), vals[order], size=(m, n))
+
+
+def time_shapes(dev, l2_flush, warmup, steps=10):
+    """The named shapes beside the timed matrix: the 2D 5-point Laplacian
+    512^2 (the reference's CPU-runnable configuration), the 3D 7-point
+    Laplacian 256^3 and R-MAT scale 22 (edge factor 16, values N(0,1)), block
+    size 64, the default build: FP64 SpMV time, GB/s over what one SpMV reads
+    (spmv_bytes + 8 n + 16 m) and over the format bytes, the fraction of the
+    measured copy peak, how much of the matrix is in row slices, and
+    cuSPARSE's CSR SpMV (torch.mv, int32 indices) on the same matrix and GPU."""
+    import torch
+    from abhsf_b200 import AbhsfMatrix
+    from abhsf_b200 import workloads as W
+    peak, _ = hbm_peak()
+    out = {}
+
+    def one(name, rows, cols, vals, m, n, desc):
+        A = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=64)
+        st = A.stats()
+        P = A.slices()
+        x = torch.rand(n, dtype=torch.float64, device=dev) * 2 - 1
+        y = torch.zeros(m, dtype=torch.float64, device=dev)
+        ms = _events_time(lambda: A.spmv(x, y), l2_flush, warmup, steps)
+        if A.device_status():
+            raise RuntimeError(f"{name}: device status {A.device_status()}")
+        A.release()
+        b = int(st["spmv_bytes"]) + 8 * n + 16 * m
+        bf = int(st["format_bytes"]) + 8 * n + 16 * m
+        r = {"workload": desc, "nnz": int(st["nnz"]), "ms": ms, "GB/s": b / (ms * 1e-3) / 1e9,
+             "frac_of_peak": b / (ms * 1e-3) / 1e9 / peak, "bytes": b, "format_bytes_per_step": bf,
+             "gflops": 2.0 * st["nnz"] / (ms * 1e-3) / 1e9,
+             "slice_elements": int(P["elements"]), "chains": int(P["chain"].sum()),
+             "schemes": st["tiles_per_scheme"]}
+        try:
+            Acs = _csr_tensor(rows, cols, vals, m, n, dev)
+            ms_c = _events_time(lambda: torch.mv(Acs, x), l2_flush, warmup, steps)
+            r["cusparse_ms"] = ms_c
+            r["cusparse_over_ours"] = ms_c / ms
+            del Acs
+        except Exception as e:  # a reference point only: report why it is missing
+            r["cusparse_unavailable"] = f"{type(e).__name__}: {e}"[:200]
+        out[name] = r
+        torch.cuda.empty_cache()
+
+    c = W.laplacian_2d(512)
+    one("laplacian2d_512", c.rows, c.cols, c.vals, c.m, c.n,
+        "2D 5-point Laplacian 512^2 (n=262144, diag 4, off -1); working set < L2, flushed between calls")
+    c = W.laplacian_3d(256)
+    one("laplacian3d_256", c.rows, c.cols, c.vals, c.m, c.n, "3D 7-point Laplacian 256^3 (diag 6, off -1)")
+    del c
+    rows, cols, vals, n = W.rmat_device(22, 16, seed=1, device=dev)
+    one("rmat22_f64", rows, cols, vals, n, n, "R-MAT scale 22 (0.57, 0.19, 0.19), edge factor 16, values N(0,1)")
+    del rows, cols, vals
+    torch.cuda.empty_cache()
+    return out
 
 
 def time_selector(dev, seeds=range(2000, 2050)):
@@ -461,7 +576,7 @@ def cpu_reference_run(c, bytes_per_step: float, max_seconds: float, max_iters: i
     """Reference CSR spmv_naive (oracle/_ref, compiled from the reference
     sources) on all host threads; falls back to the single-thread oracle port."""
     from oracle import oracle
-    x = np.random.default_rng(0).uniform(-1, 1, c.n)
+    x = np.random.default_rng(X_SEED).uniform(-1, 1, c.n)
     y = np.zeros(c.m)
     if oracle.RefCSR.available():
         t0 = time.time()
@@ -491,7 +606,7 @@ def cpu_reference_run(c, bytes_per_step: float, max_seconds: float, max_iters: i
         cores = 1
         kind = "port"
         sample = f"{len(times)} full y += A x with the oracle's element-order FP64 loop (1 thread)"
-    t = statistics.median(times)
+    t = sum(times) / len(times)  # the mean, as the GPU arm reports
     return {"value": bytes_per_step / t / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
             "ms_per_step": t * 1e3, "gflops": 2.0 * c.nnz / t / 1e9}
 
@@ -504,7 +619,7 @@ def cpu_abhsf_run(c, bytes_per_step: float, max_seconds: float = 10.0, max_iters
     t0 = time.time()
     b = oracle.build(c.rows, c.cols, c.vals, c.m, c.n, 64)
     build_s = time.time() - t0
-    x = np.random.default_rng(0).uniform(-1, 1, c.n)
+    x = np.random.default_rng(X_SEED).uniform(-1, 1, c.n)
     y = np.zeros(c.m)
     b.spmv_omp(x, y)  # warm-up
     times = []
@@ -669,7 +784,7 @@ def run_ours(args):
     log(f"built in {build_s:.2f} s: tiles {st['tiles']} {st['tiles_per_scheme']}, format {st['format_bytes']/1e6:.1f} MB, "
         f"B = {B/1e6:.1f} MB per step")
 
-    rng = np.random.default_rng(1)
+    rng = np.random.default_rng(X_SEED)
     x_h = rng.uniform(-1, 1, c.n)
     xd = torch.from_numpy(x_h).to(dev)
     yd = torch.zeros(c.m, dtype=torch.float64, device=dev)
@@ -724,6 +839,7 @@ def run_ours(args):
 
     spmm = None if args.no_spmm else time_spmm(A, c, st, dev, stream, l2_flush, args.warmup)
     lowprec = None if args.no_lowprec else time_lowprec(c, dev, l2_flush, args.warmup)
+    shapes = None if args.no_shapes or rank != 0 else time_shapes(dev, l2_flush, args.warmup)
     cg_times = None if args.no_cg or rank != 0 else time_cg(dev)
     batched = None if args.no_batched or rank != 0 else time_batched(dev, l2_flush, args.warmup)
     cusparse = None if args.no_cusparse or rank != 0 else time_cusparse(c, dev, l2_flush, args.warmup, t_mean)
@@ -763,19 +879,45 @@ def run_ours(args):
             except Exception as e:
                 ingest = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
     if rank == 0:
+        # every further measurement on a line of its own, the headline last
+        sections = (("cpu_abhsf", cpu_abhsf), ("cpu_block_kernel", cpu_block), ("ingest", ingest),
+                    ("block_stats_sweep", bstats), ("selector", selector), ("cusparse_csr", cusparse),
+                    ("lowprec", lowprec), ("spmm", spmm), ("shapes", shapes), ("cg", cg_times),
+                    ("batched", batched))
+        for name, sec in sections:
+            if sec is not None:
+                print(json.dumps({"section": name, **sec}), flush=True)
+        summary = {}
+        if batched:
+            summary["batched_ms"] = batched["batched"]["ms"]
+            summary["batched_frac_of_peak"] = batched["batched"]["frac_of_peak"]
+        if shapes:
+            for k, v in shapes.items():
+                summary[f"{k}_ms"] = v["ms"]
+                if "cusparse_over_ours" in v:
+                    summary[f"{k}_cusparse_over_ours"] = v["cusparse_over_ours"]
+        if cg_times:
+            summary["cg_plain_s"] = cg_times["plain"]["seconds"]
+            summary["cg_tuned_bf16_s"] = cg_times["tuned_bf16"]["seconds"]
+            summary["cg_tuned_bf16_speedup"] = cg_times["tuned_bf16_speedup"]
+        if spmm:
+            summary["spmm_frac_of_peak"] = {k: v["frac_of_peak"] for k, v in spmm.items()}
+        if cusparse and "ours_speedup" in cusparse:
+            summary["cusparse_over_ours"] = cusparse["ours_speedup"]
         line = {
             "metric": METRIC, "value": aggregate_rate(B, t_max * 1e-3, world), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {
-                "workload": c.name + ", x U[-1,1]",
+                "workload": c.name,
                 "block_size": 64, "nnz": c.nnz, "tiles": st["tiles"], "tiles_per_scheme": st["tiles_per_scheme"],
-                "bytes_per_step": B, "format_bytes": st["format_bytes"],
+                "bytes_per_step": B, "format_bytes": st["format_bytes"], "spmv_bytes": st["spmv_bytes"],
                 "msmf_min_bytes_per_step": st["msmf_bits"][6] // 8 + 8 * c.n + 16 * c.m,
                 "csr_bytes_per_step": 12 * c.nnz + 4 * (c.m + 1) + 8 * c.n + 16 * c.m,
                 "l2": "between steps a 256 MiB buffer is written, then another 256 MiB read (dirty lines written back before the timed SpMV); working set 600 MB > 126 MB L2",
                 "gflops": 2.0 * c.nnz / (t_mean * 1e-3) / 1e9, "build_s": build_s,
                 "parallelism": f"replicas x{world}", "sum_order": args.sum_order,
+                "kernels_per_step": A.kernels(),
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
@@ -783,19 +925,10 @@ def run_ours(args):
                          "peak_source": peak_src,
                          "kernel": KERNELS[args.sum_order] + "<64>"},
             "cpu_baseline": cpu,
-            "cpu_abhsf": cpu_abhsf,
-            "cpu_block_kernel": cpu_block,
-            "ingest": ingest,
-            "spmm": spmm,
-            "lowprec": lowprec,
-            "cg": cg_times,
-            "batched": batched,
-            "cusparse_csr": cusparse,
-            "selector": selector,
-            "block_stats_sweep": bstats,
             "e2e": {"value": aggregate_rate(B, e2e_s, world), "unit": UNIT, "h2d_bytes_per_step": 8 * c.n + 8 * c.m,
                     "d2h_bytes_per_step": 8 * c.m, "ms_per_step": e2e_s * 1e3},
-            "gpu_launches": args.steps,
+            "summary": summary,
+            "gpu_launches": args.steps * A.kernels(),
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -819,6 +952,8 @@ def main():
     ap.add_argument("--no-spmm", action="store_true", help="skip the multi-right-hand-side timings")
     ap.add_argument("--no-lowprec", action="store_true", help="skip the f32 / bf16 SpMV timings")
     ap.add_argument("--no-cg", action="store_true", help="skip the CG solves on the 3D Laplacian")
+    ap.add_argument("--no-shapes", action="store_true",
+                    help="skip the 2D / 3D Laplacian and R-MAT scale 22 SpMVs (with cuSPARSE beside them)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-matrix batched launch")
     ap.add_argument("--no-cusparse", action="store_true", help="skip the cuSPARSE CSR reference point")
     ap.add_argument("--no-selector", action="store_true", help="skip the block-size selector evaluation")

@@ -138,10 +138,10 @@ typedef struct abhsf_build_opts {
     int32_t sum_order;        /* abhsf_sum_order of abhsf_spmv / abhsf_spmv_host */
     int64_t bits_per_value;   /* dense-cost element width; 0 = width of value_type */
     int32_t selector;         /* abhsf_selector, used when block_size is 0 */
-    int32_t slice_tile_nnz;   /* reference-order SpMV at s = 32 / 64: block rows without a dense tile whose
-                                 tiles hold at most this many elements on average, or that have more
-                                 than 256 tiles, are summed from delta-coded row slices; 0 = the
-                                 library's default (32), -1 = none */
+    int32_t slice_tile_nnz;   /* reference-order SpMV: block rows without a dense tile that have no bitmap
+                                 tile, whose tiles hold at most this many elements on average, or that
+                                 have more than 256 tiles, are summed from delta-coded row slices;
+                                 0 = the library's default (32), -1 = none */
     const float* selector_model; /* host, ABHSF_MLP_PARAMS floats; NULL = the model built into the library */
 } abhsf_build_opts;
 
@@ -210,15 +210,22 @@ ABHSF_API abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, con
                          int64_t m, int64_t n, const abhsf_build_opts* opts, abhsf_stream_t stream,
                          abhsf_matrix** out);
 
+/* How many kernels one abhsf_spmv of this matrix launches (the tile kernel
+ * or the streaming kernel for the block rows it serves, the row-slice kernel
+ * and the chain kernel for those in slices).  No counterpart in the
+ * reference. */
+ABHSF_API abhsf_status abhsf_spmv_kernels(const abhsf_matrix* a, int32_t* kernels);
+
 /* y += A x, x[n] and y[m] float64 in device memory; matrix stored as f64.
  * Replaces spmv(x, y) (spmv/bottlenecks/spmv.cpp:58-64, spmv/orig/88.cpp:204-236). */
 ABHSF_API abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double* y, abhsf_stream_t stream);
 
 /* y += A x in f32 for a matrix stored as f32 or bf16: x[n], y[m] float in
  * device memory, values widened to f32, each product and each sum rounded to
- * f32, per row in the reference's column order.  Block sizes 32 and 64.  The
- * reference's f32 kernels (spmv/orig/88.cpp:204-236, value type float) are
- * the counterpart. */
+ * f32, per row in the reference's column order.  Block sizes 32 and 64, and
+ * the other sizes when every block row is in row slices (abhsf_slices_info).
+ * The reference's f32 kernels (spmv/orig/88.cpp:204-236, value type float)
+ * are the counterpart. */
 ABHSF_API abhsf_status abhsf_spmv_f32(const abhsf_matrix* a, const float* x, float* y, abhsf_stream_t stream);
 
 /* Solves A x = b by conjugate gradients in FP64 (A symmetric positive
@@ -251,13 +258,20 @@ ABHSF_API abhsf_status abhsf_cg_mixed(const abhsf_matrix* a64, const abhsf_matri
 ABHSF_API abhsf_status abhsf_batch_create(const abhsf_matrix* const* mats, int32_t count, abhsf_stream_t stream,
                                           abhsf_batch** out);
 
-/* y_i += A_i x_i for every matrix of the batch in one kernel launch, in the
- * reference's summation order (each y_i bitwise what abhsf_spmv gives).  xs
- * and ys are DEVICE arrays of count device pointers (x_i of n_i doubles,
- * y_i of m_i), so the call can be captured in a CUDA graph.  Calls on one
- * batch must not overlap on the GPU. */
+/* y_i += A_i x_i for every matrix of the batch in one call: one launch of
+ * each kernel the matrices need (the tile kernel, the row-slice kernel, and
+ * the chain kernel on a side stream forked from `stream` and joined back;
+ * abhsf_batch_kernels), in the reference's summation order (each y_i bitwise
+ * what abhsf_spmv gives).  xs and ys are DEVICE arrays of count device
+ * pointers (x_i of n_i doubles, y_i of m_i), so the call can be captured in
+ * a CUDA graph.  Calls on one batch must not overlap on the GPU. */
 ABHSF_API abhsf_status abhsf_batch_spmv(const abhsf_batch* b, const double* const* xs, double* const* ys,
                                         abhsf_stream_t stream);
+
+/* How many kernels one abhsf_batch_spmv launches: the tile kernel (when some
+ * block row is its), the row-slice kernel and the chain kernel (when some
+ * block row is in slices), 0 to 3.  No counterpart in the reference. */
+ABHSF_API abhsf_status abhsf_batch_kernels(const abhsf_batch* b, int32_t* kernels);
 
 /* The batch's device status word (ABHSF_DEVSTAT_* bits), as abhsf_device_status. */
 ABHSF_API abhsf_status abhsf_batch_status(abhsf_batch* b, abhsf_stream_t stream, int32_t clear, int32_t* out);

@@ -698,19 +698,21 @@ int orc_slices_build(const orc_matrix* a, double avg, orc_slices** out)
     const int s = a->s;
     if (avg <= 0 || (uint64_t)a->n > ((uint64_t)1 << 32))
         return ORC_OK;
-    /* the block rows: non-empty, no dense tile, at most avg elements per tile
-     * on average or more than ORC_RING_TILES_MAX tiles */
+    /* the block rows: non-empty, no dense tile, and no bitmap tile, at most
+     * avg elements per tile on average or more than ORC_RING_TILES_MAX tiles */
     uint8_t* sel = (uint8_t*)calloc((size_t)a->M + 1, 1);
     int64_t E = 0, ns = 0;
     for (int64_t I = 0; I < a->M; ++I) {
         const int64_t t0 = a->brow_ptr[I], t1 = a->brow_ptr[I + 1];
         if (t1 == t0)
             continue;
-        int ok = 1;
-        for (int64_t t = t0; t < t1; ++t)
+        int ok = 1, bitmap = 0;
+        for (int64_t t = t0; t < t1; ++t) {
             ok = ok && a->tile_scheme[t] != ORC_DENSE;
+            bitmap = bitmap || a->tile_scheme[t] == ORC_BITMAP;
+        }
         const int64_t e = a->tile_val_off[t1] - a->tile_val_off[t0];
-        if (ok && ((double)e <= avg * (double)(t1 - t0) || t1 - t0 > ORC_RING_TILES_MAX)) {
+        if (ok && ((double)e <= avg * (double)(t1 - t0) || t1 - t0 > ORC_RING_TILES_MAX || !bitmap)) {
             sel[I] = 1;
             E += e;
             ++ns;

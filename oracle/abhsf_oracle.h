@@ -125,8 +125,8 @@ double orc_bf16_to_f64(uint16_t b);
 /* Delta-coded row slices of the hypersparse block rows (the encoding the
  * library's SpMV reads for them; spmv/orig/delta.cpp:118-219 is the
  * reference's row-by-row delta COO it follows).  Block rows: non-empty, no
- * dense tile, at most avg elements per tile on average or more than 256
- * tiles; none when n > 2^32
+ * dense tile, and no bitmap tile, at most avg elements per tile on average or
+ * more than 256 tiles; none when n > 2^32
  * or the elements reach 2^31.  Per block row (ascending), its non-empty rows
  * by length (longest first, then row): each row of more than 256 elements a
  * chain slice (lanes 1, meta = the row, steps = its length, its elements at

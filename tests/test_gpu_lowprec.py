@@ -74,5 +74,6 @@ def test_spmv_f32_arguments(gpu):
     x = torch.zeros(200, dtype=torch.float32, device="cuda")
     y = torch.zeros(300, dtype=torch.float32, device="cuda")
     assert capi.lib.abhsf_spmv_f32(A64.handle, x.data_ptr(), y.data_ptr(), None) == capi.INVALID_VALUE
-    A16 = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=16, value_type="f32")
+    A16 = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=16, value_type="f32",
+                                    slice_tile_nnz=-1)
     assert capi.lib.abhsf_spmv_f32(A16.handle, x.data_ptr(), y.data_ptr(), None) == capi.UNSUPPORTED

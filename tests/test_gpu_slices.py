@@ -68,7 +68,7 @@ def _spmv(A, x, y0):
     return yd.cpu().numpy()
 
 
-@pytest.mark.parametrize("s", [32, 64])
+@pytest.mark.parametrize("s", [16, 32, 64, 128, 256])
 @pytest.mark.parametrize("tile_nnz", [-1, 4, 0, 1000000])
 def test_slice_spmv_is_the_reference_order(gpu, s, tile_nnz):
     for coo in cases():
@@ -81,7 +81,7 @@ def test_slice_spmv_is_the_reference_order(gpu, s, tile_nnz):
         A.release()
 
 
-@pytest.mark.parametrize("s", [32, 64])
+@pytest.mark.parametrize("s", [16, 32, 64, 128, 256])
 @pytest.mark.parametrize("tile_nnz", [4, 0, 1000000])
 def test_slices_equal_the_oracle_encoding(gpu, s, tile_nnz):
     avg = DEFAULT_TILE_NNZ if tile_nnz == 0 else tile_nnz
@@ -117,10 +117,14 @@ def test_chains_and_bitmap_tiles_are_exercised(gpu):
 
 
 @pytest.mark.parametrize("vt", ["f32", "bf16"])
-def test_slice_spmv_f32_bitwise_against_oracle(gpu, vt):
+@pytest.mark.parametrize("s", [16, 64, 256])
+def test_slice_spmv_f32_bitwise_against_oracle(gpu, vt, s):
+    """f32 / bf16 values through the slices; at block sizes 16 and 256 the
+    slices serve these matrices alone (no dense tile)."""
     import torch
     for coo in (W.rmat(1 << 14, 8, seed=4), heavy_rows(seed=2)):
-        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64, value_type=vt)
+        A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, value_type=vt,
+                                      slice_tile_nnz=1000000)
         assert A.slices()["slices"] > 0
         rng = np.random.default_rng(4)
         x32 = rng.uniform(-1, 1, coo.n).astype(np.float32)
