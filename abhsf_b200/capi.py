@@ -22,7 +22,7 @@ SUM_ORDERS = {"reference": 0, "tree": 1}
 NOALLOC_MAX_NNZ = 1048576
 BSTATS_ALL_LEN = 260164
 DEVSTAT_WAIT_TIMEOUT = 1
-SELECTORS = {"minbss": 0, "learned": 1, "autotune": 2}
+SELECTORS = {"minbss": 0, "learned": 1, "autotune": 2, "learned_time": 3}
 FEATURES, MLP_HIDDEN, MLP_CLASSES = 12, 64, 5
 MLP_PARAMS = (FEATURES * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN +
               MLP_HIDDEN * MLP_CLASSES + MLP_CLASSES + 2 * FEATURES)
@@ -137,6 +137,7 @@ PROTOTYPES = {
     "abhsf_selector_features": (C.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, _vp, _fp]),
     "abhsf_selector_predict": (C.c_int, [_vp, _fp, _vp, C.POINTER(_i32)]),
     "abhsf_selector_builtin_model": (C.c_int, [_fp]),
+    "abhsf_selector_builtin_time_model": (C.c_int, [_fp]),
     "abhsf_mlp_forward": (C.c_int, [_vp, _vp, _i32, _vp, _vp, _vp]),
     "abhsf_mlp_backward": (C.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp]),
     "abhsf_mlp_adam": (C.c_int, [_vp, _vp, _vp, _vp, _i32, C.c_float, _vp]),

@@ -100,10 +100,13 @@ abhsf_status abhsf_build(const int64_t* rows, const int64_t* cols, const double*
                 uint64_t bits[abhsf::kNumBlockSizes];
                 abhsf::block_size_storage(rows, cols, nnz, m, n, o, st, bits);
                 o.block_size = abhsf::select_block_size(bits);
-            } else if (o.selector == ABHSF_SELECT_LEARNED) {
+            } else if (o.selector == ABHSF_SELECT_LEARNED || o.selector == ABHSF_SELECT_LEARNED_TIME) {
                 float f[ABHSF_FEATURES];
                 abhsf::selector_features(rows, cols, nnz, m, n, o.inputs_on_device != 0, st, f);
-                o.block_size = abhsf::mlp_predict(o.selector_model, f, st);
+                const float* model = o.selector_model ? o.selector_model
+                                     : o.selector == ABHSF_SELECT_LEARNED_TIME ? abhsf::builtin_time_model()
+                                                                               : nullptr;
+                o.block_size = abhsf::mlp_predict(model, f, st);
             } else if (o.selector == ABHSF_SELECT_AUTOTUNE) {
                 float ms[abhsf::kNumBlockSizes];
                 int best = 0;
@@ -477,6 +480,15 @@ abhsf_status abhsf_selector_builtin_model(float* out)
         if (!out)
             fail(ABHSF_ERROR_INVALID_VALUE, "out must be non-NULL");
         std::copy(abhsf::builtin_model(), abhsf::builtin_model() + ABHSF_MLP_PARAMS, out);
+    });
+}
+
+abhsf_status abhsf_selector_builtin_time_model(float* out)
+{
+    return guarded([&] {
+        if (!out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "out must be non-NULL");
+        std::copy(abhsf::builtin_time_model(), abhsf::builtin_time_model() + ABHSF_MLP_PARAMS, out);
     });
 }
 

@@ -49,7 +49,8 @@ void mlp_backward(const float* p, const float* x, const float* target, int batch
                   float* delta, float* grad, float* loss, cudaStream_t st);
 void mlp_adam(float* p, const float* g, float* m, float* v, int step, float lr, cudaStream_t st);
 int mlp_predict(const float* model_host, const float features[ABHSF_FEATURES], cudaStream_t st);
-const float* builtin_model();  // ABHSF_MLP_PARAMS floats, host memory
+const float* builtin_model();       // ABHSF_MLP_PARAMS floats, host memory: trained on storage
+const float* builtin_time_model();  // ... trained on measured SpMV time
 
 void mmf_line_from_hist(int64_t m, int64_t n, int64_t nnz, int type, int64_t r, int64_t s,
                         const std::map<uint64_t, uint64_t>& hist, uint64_t bits1, uint64_t o1[8], uint64_t o2[8]);

@@ -31,9 +31,12 @@ constexpr int kTrainable = OMEAN;  // the normalisation is fixed, not trained
 constexpr int ACT = 2 * H;         // per-sample activations kept for backward: h1, h2
 constexpr int DLT = C + 2 * H;     // per-sample deltas: logits, h2, h1
 
-// The trained model shipped with the library (written by abhsf_b200/selector.py).
+// The trained models shipped with the library (written by abhsf_b200/selector.py):
+// one trained on the storage of each size, one on the measured SpMV time.
 #include "selector_model.inc"
+#include "selector_model_time.inc"
 static_assert(sizeof(kBuiltinModel) == ABHSF_MLP_PARAMS * sizeof(float), "built-in model size");
+static_assert(sizeof(kBuiltinTimeModel) == ABHSF_MLP_PARAMS * sizeof(float), "built-in model size");
 
 // ---------------------------------------------------------------- features
 
@@ -232,6 +235,7 @@ unsigned grid_of(int64_t work)
 }  // namespace
 
 const float* builtin_model() { return kBuiltinModel; }
+const float* builtin_time_model() { return kBuiltinTimeModel; }
 
 void selector_features(const int64_t* rows, const int64_t* cols, int64_t nnz, int64_t m, int64_t n, bool on_device,
                        cudaStream_t st, float out[ABHSF_FEATURES])

@@ -181,9 +181,16 @@ def features(rows, cols, m: int, n: int, stream=None) -> np.ndarray:
 
 
 def builtin_model() -> np.ndarray:
-    """The model built into the library (float32[MLP_PARAMS])."""
+    """The model built into the library (float32[MLP_PARAMS]), trained on storage."""
     out = np.zeros(P, np.float32)
     capi.check(capi.lib.abhsf_selector_builtin_model(out.ctypes.data_as(C.POINTER(C.c_float))))
+    return out
+
+
+def builtin_time_model() -> np.ndarray:
+    """The model built into the library that was trained on measured SpMV time."""
+    out = np.zeros(P, np.float32)
+    capi.check(capi.lib.abhsf_selector_builtin_time_model(out.ctypes.data_as(C.POINTER(C.c_float))))
     return out
 
 
@@ -311,6 +318,32 @@ def targets_from_bits(bits: np.ndarray, tau: float = 0.0) -> np.ndarray:
     return (e / e.sum(axis=1, keepdims=True)).astype(np.float32)
 
 
+def targets_from_times(ms: np.ndarray, tau: float = 0.05) -> np.ndarray:
+    """Training targets from the measured SpMV time at each size: a softmax of
+    -excess / tau, excess being the time above the fastest as a fraction of it
+    (sizes without a time, ms <= 0, get no weight)."""
+    t = np.where(ms > 0, ms.astype(np.float64), np.inf)
+    mn = t.min(axis=1, keepdims=True)
+    z = -(t - mn) / mn / tau
+    z -= z.max(axis=1, keepdims=True)
+    e = np.exp(z)
+    return (e / e.sum(axis=1, keepdims=True)).astype(np.float32)
+
+
+def time_regret_summary(ms: np.ndarray, choice: np.ndarray) -> dict:
+    """Per matrix the SpMV time at the chosen size over the fastest one, minus
+    one, in percent (the storage regret of consistency.cpp:147-160 with time
+    in place of storage): its average and maximum, the share of matrices whose
+    choice is the fastest, and the summed time of the choices over the summed
+    fastest times."""
+    t = np.where(ms > 0, ms.astype(np.float64), np.inf)
+    mn = t.min(axis=1)
+    got = t[np.arange(t.shape[0]), choice]
+    r = (got - mn) / mn * 100.0
+    return {"avg_pct": float(r.mean()), "max_pct": float(r.max()), "exact": float((r == 0).mean()),
+            "total_over_best": float(got.sum() / mn.sum())}
+
+
 def regret(bits: np.ndarray, choice: np.ndarray) -> np.ndarray:
     """Per matrix: (storage of the chosen size - least storage) / least
     storage * 100 (block_statistics/consistency.cpp:147-160); choice holds
@@ -327,13 +360,14 @@ def regret_summary(bits: np.ndarray, choice: np.ndarray) -> dict:
     return {"avg_pct": float(r.mean()), "max_pct": float(r.max()), "exact": float((r == 0).mean())}
 
 
-def write_model_inc(params: np.ndarray, path: str) -> None:
+def write_model_inc(params: np.ndarray, path: str, name: str = "kBuiltinModel",
+                    what: str = "Trained block-size selector") -> None:
     """The model as the C++ initialiser selector.cu includes."""
     params = np.asarray(params, dtype=np.float32)
     assert params.size == P
-    lines = ["// Trained block-size selector: ABHSF_MLP_PARAMS floats in the layout of",
+    lines = [f"// {what}: ABHSF_MLP_PARAMS floats in the layout of",
              "// include/abhsf/abhsf_gpu.h.  Written by abhsf_b200/selector.py; do not edit.",
-             "static const float kBuiltinModel[ABHSF_MLP_PARAMS] = {"]
+             f"static const float {name}[ABHSF_MLP_PARAMS] = {{"]
     vals = [np.format_float_scientific(v, precision=8, unique=False) + "f" for v in params]
     for i in range(0, P, 8):
         lines.append("    " + ", ".join(vals[i:i + 8]) + ",")
@@ -379,13 +413,14 @@ def dataset(seeds, n_min=10_000, n_max=4_000_000, nnz_max=16_000_000, log=None):
 
 
 def train(X: np.ndarray, bits: np.ndarray, steps: int = 6000, batch: int = 256, lr: float = 3e-3,
-          tau: float = 0.02, seed: int = 0, log=None) -> np.ndarray:
+          tau: float = 0.02, seed: int = 0, log=None, targets: np.ndarray | None = None) -> np.ndarray:
     """Adam on the GPU kernels, mini-batches drawn by numpy's default_rng(seed),
-    learning rate decayed by cosine to lr / 20."""
+    learning rate decayed by cosine to lr / 20.  Targets: from the storage
+    (targets_from_bits(bits, tau)) unless given."""
     import torch
     net = Mlp(init_params(X, seed))
     xt = torch.from_numpy(X).cuda()
-    tt = torch.from_numpy(targets_from_bits(bits, tau)).cuda()
+    tt = torch.from_numpy(targets_from_bits(bits, tau) if targets is None else targets).cuda()
     rng = np.random.default_rng(seed)
     for step in range(steps):
         idx = torch.from_numpy(rng.integers(0, X.shape[0], min(batch, X.shape[0]))).cuda()
@@ -398,6 +433,48 @@ def train(X: np.ndarray, bits: np.ndarray, steps: int = 6000, batch: int = 256, 
     return net.params()
 
 
+def time_dataset(seeds, n_min=10_000, n_max=2_000_000, nnz_max=8_000_000, reps=5, log=None):
+    """Features, storage at sizes 16..256 and the measured FP64 SpMV time at
+    each size (ms, the median of reps CUDA-event-timed launches after two;
+    the library's default build at that size, values N(0,1)) of the selector
+    workload's matrices."""
+    import torch
+    from . import workloads as W
+    from .matrix import AbhsfMatrix
+    X = np.zeros((len(seeds), F), np.float32)
+    B = np.zeros((len(seeds), 5), np.uint64)
+    T = np.zeros((len(seeds), 5), np.float32)
+    names = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i, seed in enumerate(seeds):
+        rows, cols, m, n, name = W.selector_matrix(int(seed), n_min, n_max, nnz_max)
+        g = torch.Generator(device=rows.device)
+        g.manual_seed(int(seed))
+        vals = torch.randn(rows.numel(), dtype=torch.float64, device=rows.device, generator=g)
+        X[i] = features(rows, cols, m, n)
+        B[i], _ = block_size_storage(rows, cols, m, n)
+        x = torch.rand(n, dtype=torch.float64, device=rows.device)
+        y = torch.zeros(m, dtype=torch.float64, device=rows.device)
+        for k, s in enumerate(SIZES):
+            A = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=s)
+            for _ in range(2):
+                A.spmv(x, y)
+            ts = []
+            for _ in range(reps):
+                e0.record()
+                A.spmv(x, y)
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            T[i, k] = float(np.median(ts))
+            A.release()
+        names.append(name)
+        if log and (i + 1) % 50 == 0:
+            log(f"{i + 1}/{len(seeds)} matrices timed")
+        del rows, cols, vals, x, y
+    return X, B, T, names
+
+
 def choose(model: np.ndarray, X: np.ndarray) -> np.ndarray:
     """Indices 0..4 of the sizes the model picks for each row of X, through
     the library's forward kernel."""
@@ -407,15 +484,54 @@ def choose(model: np.ndarray, X: np.ndarray) -> np.ndarray:
     return probs.argmax(dim=1).cpu().numpy()
 
 
+def main_time(args) -> int:
+    """train-time: the selector trained on measured SpMV times."""
+    os.makedirs(args.out, exist_ok=True)
+
+    def log(msg):
+        print(msg, flush=True)
+
+    seeds_train = np.arange(args.train)
+    seeds_held = np.arange(2000, 2000 + args.heldout)
+    Xtr, Btr, Ttr, ntr = time_dataset(seeds_train, n_max=args.n_max, log=log)
+    Xho, Bho, Tho, nho = time_dataset(seeds_held, n_max=args.n_max, log=log)
+    np.savez_compressed(os.path.join(args.out, "selector_time_heldout.npz"), X=Xho, bits=Bho, ms=Tho,
+                        names=np.array(nho))
+    t0 = time.perf_counter()
+    model = train(Xtr, Btr, steps=args.steps, log=log, targets=targets_from_times(Ttr))
+    t_train = time.perf_counter() - t0
+    model.tofile(os.path.join(args.out, "selector_model_time.f32"))
+    write_model_inc(model, os.path.join(args.out, "selector_model_time.inc"), "kBuiltinTimeModel",
+                    "Block-size selector trained on measured SpMV times")
+    report = {"train": len(seeds_train), "heldout": len(seeds_held), "train_s": t_train}
+    for split, X, B, T in (("train", Xtr, Btr, Ttr), ("heldout", Xho, Bho, Tho)):
+        c_time = choose(model, X)
+        c_store = choose(builtin_model(), X)
+        minbss = B.astype(np.float64).argmin(axis=1)
+        report[split + "_time_model"] = {"time": time_regret_summary(T, c_time), "storage": regret_summary(B, c_time)}
+        report[split + "_storage_model"] = {"time": time_regret_summary(T, c_store),
+                                            "storage": regret_summary(B, c_store)}
+        report[split + "_minbss"] = {"time": time_regret_summary(T, minbss), "storage": regret_summary(B, minbss)}
+        for s in SIZES:
+            k = np.full(B.shape[0], SIZES.index(s))
+            report[f"{split}_fixed{s}"] = {"time": time_regret_summary(T, k), "storage": regret_summary(B, k)}
+    with open(os.path.join(args.out, "selector_time_report.json"), "w") as f:
+        json.dump(report, f, indent=1)
+    log(json.dumps(report))
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("cmd", choices=["train", "train-time"])
     ap.add_argument("--out", required=True)
     ap.add_argument("--train", type=int, default=2000)
     ap.add_argument("--heldout", type=int, default=200)
     ap.add_argument("--n-max", type=int, default=4_000_000)
     ap.add_argument("--steps", type=int, default=6000)
     args = ap.parse_args(argv)
+    if args.cmd == "train-time":
+        return main_time(args)
     os.makedirs(args.out, exist_ok=True)
 
     def log(msg):

@@ -104,7 +104,9 @@ typedef enum abhsf_matrix_type {
  * builds the block histograms of all five sizes and takes the one of least
  * ABHSF storage, ties to the smaller (block_statistics/min-bss.cpp:14-58).
  * LEARNED computes ABHSF_FEATURES features in one pass and lets a small MLP
- * predict that size.  AUTOTUNE builds the matrix at every size and keeps the
+ * predict that size.  LEARNED_TIME does the same with the MLP trained on the
+ * library's measured SpMV time at each size: it predicts the fastest size,
+ * not the smallest.  AUTOTUNE builds the matrix at every size and keeps the
  * one whose SpMV (abhsf_spmv, or abhsf_spmv_f32 for f32 / bf16 values) ran
  * fastest on the stream (abhsf_autotune, 10 timed calls each).  Whichever
  * selector, only the block size is chosen: every tile's scheme, indices and
@@ -112,7 +114,8 @@ typedef enum abhsf_matrix_type {
 typedef enum abhsf_selector {
     ABHSF_SELECT_MINBSS = 0,
     ABHSF_SELECT_LEARNED = 1,
-    ABHSF_SELECT_AUTOTUNE = 2
+    ABHSF_SELECT_AUTOTUNE = 2,
+    ABHSF_SELECT_LEARNED_TIME = 3
 } abhsf_selector;
 
 /* The learned selector's MLP: ABHSF_FEATURES inputs, two hidden layers of
@@ -441,6 +444,10 @@ ABHSF_API abhsf_status abhsf_selector_predict(const float* model, const float fe
 
 /* The built-in model (ABHSF_MLP_PARAMS floats) into out. */
 ABHSF_API abhsf_status abhsf_selector_builtin_model(float* out);
+
+/* The built-in model trained on measured SpMV times (ABHSF_SELECT_LEARNED_TIME)
+ * into out.  No counterpart in the reference. */
+ABHSF_API abhsf_status abhsf_selector_builtin_time_model(float* out);
 
 /* Training kernels of the MLP, all pointers device memory, ordered on stream.
  * forward: probs[batch][C] = softmax of the network at x[batch][F]; act
