@@ -103,10 +103,12 @@ struct dc_plan {
     int cwarps = 0;
 };
 dc_plan plan_of(const abhsf_matrix& a);
+// cols > 1 (FP64 only: 2, 4, 8, 16 or 32): Y += A X over that many columns
+// in one pass, each column bitwise its SpMV.
 void slices_begin(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
-                  cudaStream_t st);
+                  cudaStream_t st, int cols = 1);
 void slices_end(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
-                cudaStream_t st);
+                cudaStream_t st, int cols = 1);
 void prepare_batch_stream(abhsf_batch& b, cudaStream_t st);
 void batch_stream_begin(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);
 void batch_stream_end(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);

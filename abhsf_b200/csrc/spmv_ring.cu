@@ -1673,9 +1673,13 @@ bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, d
         else
             spmm_ring<64>(a, k, X, ldx, Y, ldy, st);
     }
-    for (int j = 0; j < k; ++j) {  // the slice rows, column by column
-        slices_begin(a, p, X + j, ldx, Y + j, ldy, st);
-        slices_end(a, p, X + j, ldx, Y + j, ldy, st);
+    for (int j = 0; j < k;) {  // the slice rows, up to 32 columns a pass
+        int cols = 32;
+        while (cols > k - j)
+            cols /= 2;
+        slices_begin(a, p, X + j, ldx, Y + j, ldy, st, cols);
+        slices_end(a, p, X + j, ldx, Y + j, ldy, st, cols);
+        j += cols;
     }
     return true;
 }

@@ -123,36 +123,64 @@ struct dc_args {
     void* const* ys;
 };
 
-// Adds the first nv of the warp's 32 products (lane k holds product k) onto
-// run in lane order, every lane the same chain.  The products come by
-// shuffles taken ahead of the adds, so that nothing but the adds themselves
-// lies on the chain; a full step adds all 32 without a test in the chain.
-template <typename T>
-__device__ __forceinline__ T add_in_order(T run, T p, int nv)
+// Eight consecutive products from shared memory (every lane the same
+// address: a broadcast), in two or four 16-byte loads.
+__device__ __forceinline__ void load8(const double* q, double (&t)[8])
 {
-    if (nv == 32) {
 #pragma unroll
-        for (int k0 = 0; k0 < 32; k0 += 8) {
-            T t[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-                t[k] = __shfl_sync(0xffffffffu, p, k0 + k);
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-                run = dadd(run, t[k]);
-        }
-        return run;
+    for (int k = 0; k < 4; ++k) {
+        const double2 u = reinterpret_cast<const double2*>(q)[k];
+        t[2 * k] = u.x;
+        t[2 * k + 1] = u.y;
     }
+}
+__device__ __forceinline__ void load8(const float* q, float (&t)[8])
+{
 #pragma unroll
-    for (int k0 = 0; k0 < 32; k0 += 8) {
-        T t[8];
+    for (int k = 0; k < 2; ++k) {
+        const float4 u = reinterpret_cast<const float4*>(q)[k];
+        t[4 * k] = u.x;
+        t[4 * k + 1] = u.y;
+        t[4 * k + 2] = u.z;
+        t[4 * k + 3] = u.w;
+    }
+}
+
+// Adds the first nv products of q (shared memory, 16-byte aligned) onto run
+// in order.  The loads of the next eight are issued before the adds of the
+// current eight, so that nothing but the adds themselves lies on the chain.
+template <int N, typename T>
+__device__ __forceinline__ T add_products(T run, const T* q, int nv)
+{
+    T t[2][8];
+    load8(q, t[0]);
+#pragma unroll
+    for (int b = 0; b < N / 8; ++b) {
+        if (8 * b >= nv)
+            break;
+        if (b + 1 < N / 8)
+            load8(q + 8 * (b + 1), t[(b + 1) & 1]);
 #pragma unroll
         for (int k = 0; k < 8; ++k)
-            t[k] = __shfl_sync(0xffffffffu, p, k0 + k);
+            if (8 * b + k < nv)
+                run = dadd(run, t[b & 1][k]);
+    }
+    return run;
+}
+
+// All N products, no tests in the chain.
+template <int N, typename T>
+__device__ __forceinline__ T add_products_full(T run, const T* q)
+{
+    T t[2][8];
+    load8(q, t[0]);
+#pragma unroll
+    for (int b = 0; b < N / 8; ++b) {
+        if (b + 1 < N / 8)
+            load8(q + 8 * (b + 1), t[(b + 1) & 1]);
 #pragma unroll
         for (int k = 0; k < 8; ++k)
-            if (k0 + k < nv)
-                run = dadd(run, t[k]);
+            run = dadd(run, t[b & 1][k]);
     }
     return run;
 }
@@ -212,9 +240,11 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmv_slices(dc_args P)
 }
 
 // The chains: one warp per row, the row's elements in order (each word the
-// absolute column).  Lane l forms the product of element 32 c + l; every
-// lane adds the step's 32 products in order, taken by shuffles.  The values
-// and gathered x of the next kChainAhead steps are in flight meanwhile, so
+// absolute column).  Lane l forms the product of element 32 j + l of a group
+// of kChainAhead x 32 and stores it in the warp's shared buffer; every lane
+// then adds the group's products in order, read back by broadcast loads (a
+// shuffle per product would cost more issue slots than the add it feeds).
+// The values and gathered x of the next group are in flight meanwhile, so
 // that the chain of adds -- the one thing that must run in sequence -- does
 // not wait on memory.
 template <int S, int VT, bool B>
@@ -222,11 +252,13 @@ __global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmv_chai
 {
     using T = typename vt_of<VT>::T;
     using V = typename vt_of<VT>::V;
-    constexpr int AH = kChainAhead;
+    constexpr int AH = kChainAhead, G = 32 * AH;
+    __shared__ __align__(16) T sbuf[kChainWarps][G];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gw = blockIdx.x * kChainWarps + warp;
     if (gw >= P.warps)
         return;
+    T* buf = sbuf[warp];
     const int64_t s1 = P.wbeg[gw + 1];
 #pragma unroll 1
     for (int64_t si = P.wbeg[gw]; si < s1; ++si) {
@@ -240,7 +272,8 @@ __global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmv_chai
         const V* Vv = static_cast<const V*>(M.vals) + sl.base;
         const int64_t row = (int64_t)sl.brow * S + sl.meta;
         const int len = (int)sl.steps;
-        // slot j: the value and x of step c + j; the word of step c + j + AH
+        // slot j: the value and x of element 32 j + lane of the current
+        // group; the word of the same element of the next group
         uint32_t wq[AH];
         T vq[AH], xq[AH];
 #pragma unroll
@@ -253,37 +286,159 @@ __global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmv_chai
             const int e = 32 * j + lane;
             vq[j] = e < len ? wide(ld_stream(Vv + e)) : T(0);
             xq[j] = e < len ? __ldg(X + (int64_t)wq[j] * ldx) : T(0);
-            wq[j] = e + 32 * AH < len ? ld_stream(W + e + 32 * AH) : 0u;
+            wq[j] = e + G < len ? ld_stream(W + e + G) : 0u;
         }
         T run = Y[row * ldy];
-        // whole groups of AH full steps: straight-line code, the refills
-        // clamped to the row (what they fetch past its end is never used), so
-        // that the next steps' loads and shuffles interleave with this step's
-        // adds
+        // whole groups: the refills clamped to the row (what they fetch past
+        // its end is never used)
         int b0 = 0;
 #pragma unroll 1
-        for (; b0 + 32 * AH <= len; b0 += 32 * AH) {
+        for (; b0 + G <= len; b0 += G) {
+            __syncwarp();  // the previous group's products are read
 #pragma unroll
             for (int j = 0; j < AH; ++j) {
-                const T p = dmul(vq[j], xq[j]);
-                const int e = b0 + 32 * j + 32 * AH + lane;  // refill slot j: AH steps on
+                buf[32 * j + lane] = dmul(vq[j], xq[j]);
+                const int e = b0 + G + 32 * j + lane;  // the same element of the next group
                 vq[j] = wide(ld_stream(Vv + min(e, len - 1)));
                 xq[j] = __ldg(X + (int64_t)wq[j] * ldx);
-                wq[j] = ld_stream(W + min(e + 32 * AH, len - 1));
-                run = add_in_order(run, p, 32);
+                wq[j] = ld_stream(W + min(e + G, len - 1));
             }
+            __syncwarp();
+            run = add_products_full<G>(run, buf);
         }
         // the last, partial group
+        const int rem = len - b0;
+        if (rem > 0) {
+            __syncwarp();
 #pragma unroll
-        for (int j = 0; j < AH; ++j) {
-            const int base = b0 + 32 * j;
-            if (base >= len)
-                break;
-            const T p = base + lane < len ? dmul(vq[j], xq[j]) : T(0);
-            run = add_in_order(run, p, min(32, len - base));
+            for (int j = 0; j < AH; ++j)
+                buf[32 * j + lane] = 32 * j + lane < rem ? dmul(vq[j], xq[j]) : T(0);
+            __syncwarp();
+            run = add_products<G>(run, buf, rem);
         }
         if (lane == 0)
             Y[row * ldy] = run;
+    }
+}
+
+// Y += A X over K columns of X and Y (FP64, K = 2 .. 32), sliced rows.  Lane
+// (g, h) = (lane / K, lane % K) keeps the sums of column h for rows g, g + G,
+// ... of the slice (G = 32 / K): the group of K lanes reads one row of X, K
+// contiguous values, per product.  Each step loads the slice's 32 words and
+// values as the SpMV does (lane r: row r); lane r keeps row r's running
+// column, and the groups take column and value by shuffles.  Every (row,
+// column) sum adds its products in the row's column order from Y's value:
+// column j of Y is bitwise the SpMV of column j of X.
+template <int K>
+__global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmm_slices(dc_args P, int S)
+{
+    constexpr int G = 32 / K;
+    constexpr int CH = K < 8 ? K : 8;  // rows whose gathers are in flight together
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane / K, h = lane % K;
+    const int gw = blockIdx.x * kWarpsPerCta + warp;
+    if (gw >= P.warps)
+        return;
+    const double* X = static_cast<const double*>(P.x) + h;
+    double* Y = static_cast<double*>(P.y) + h;
+    const int64_t s1 = P.wbeg[gw + 1];
+#pragma unroll 1
+    for (int64_t si = P.wbeg[gw]; si < s1; ++si) {
+        const dc_slice sl = P.slices[si];
+        const uint32_t* W = P.A.words + sl.base;
+        const double* Vv = static_cast<const double*>(P.A.vals) + sl.base;
+        const uint32_t rec = lane < (int)sl.lanes ? P.A.lane[sl.meta + lane] : 0u;
+        const int len = (int)(rec & kLenMask);
+        const int64_t row0 = (int64_t)sl.brow * S;
+        double acc[K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const uint32_t ri = __shfl_sync(0xffffffffu, rec, g + G * i);
+            acc[i] = (ri & kLenMask) ? Y[(row0 + (ri >> 24)) * P.ldy] : 0.0;
+        }
+        uint32_t col = 0;  // lane r: row r's column
+#pragma unroll 1
+        for (int k = 0; k < (int)sl.steps; ++k) {
+            const bool on = k < len;
+            const int64_t slot = (int64_t)k * 32 + lane;
+            col += on ? ld_stream(W + slot) : 0u;
+            const double v = on ? ld_stream(Vv + slot) : 0.0;
+            const uint32_t act = __ballot_sync(0xffffffffu, on);
+#pragma unroll
+            for (int i0 = 0; i0 < K; i0 += CH) {
+                double x[CH], vv[CH];
+#pragma unroll
+                for (int i = 0; i < CH; ++i) {
+                    const int r = g + G * (i0 + i);
+                    const uint32_t c = __shfl_sync(0xffffffffu, col, r);
+                    vv[i] = __shfl_sync(0xffffffffu, v, r);
+                    x[i] = (act >> r) & 1u ? __ldg(X + (int64_t)c * P.ldx) : 0.0;
+                }
+#pragma unroll
+                for (int i = 0; i < CH; ++i)
+                    if ((act >> (g + G * (i0 + i))) & 1u)
+                        acc[i0 + i] = dadd(acc[i0 + i], dmul(vv[i], x[i]));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            const uint32_t ri = __shfl_sync(0xffffffffu, rec, g + G * i);
+            if (ri & kLenMask)
+                Y[(row0 + (ri >> 24)) * P.ldy] = acc[i];
+        }
+    }
+}
+
+// Y += A X over K columns, the chains: one row per warp, lane h (of the first
+// K; the others repeat them and store nothing) keeps column h's sum and adds
+// the row's products one after another, 32 elements' words and values loaded
+// at a time (the next 32 in flight meanwhile) and taken by shuffles.
+template <int K>
+__global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmm_chains(dc_args P, int S)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int h = lane % K;
+    const int gw = blockIdx.x * kChainWarps + warp;
+    if (gw >= P.warps)
+        return;
+    const double* X = static_cast<const double*>(P.x) + h;
+    double* Y = static_cast<double*>(P.y) + h;
+    const int64_t s1 = P.wbeg[gw + 1];
+#pragma unroll 1
+    for (int64_t si = P.wbeg[gw]; si < s1; ++si) {
+        const dc_slice sl = P.slices[si];
+        const uint32_t* W = P.A.words + sl.base;
+        const double* Vv = static_cast<const double*>(P.A.vals) + sl.base;
+        const int64_t row = (int64_t)sl.brow * S + sl.meta;
+        const int len = (int)sl.steps;
+        double acc = Y[row * P.ldy];
+        uint32_t c = lane < len ? ld_stream(W + lane) : 0u;
+        double v = lane < len ? ld_stream(Vv + lane) : 0.0;
+#pragma unroll 1
+        for (int e0 = 0; e0 < len; e0 += 32) {
+            const int n = min(32, len - e0);
+            const int en = e0 + 32 + lane;
+            const uint32_t cn = en < len ? ld_stream(W + en) : 0u;
+            const double vn = en < len ? ld_stream(Vv + en) : 0.0;
+#pragma unroll
+            for (int j0 = 0; j0 < 32; j0 += 8) {
+                double x[8], vv[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const uint32_t cj = __shfl_sync(0xffffffffu, c, j0 + j);
+                    vv[j] = __shfl_sync(0xffffffffu, v, j0 + j);
+                    x[j] = j0 + j < n ? __ldg(X + (int64_t)cj * P.ldx) : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (j0 + j < n)
+                        acc = dadd(acc, dmul(vv[j], x[j]));
+            }
+            c = cn;
+            v = vn;
+        }
+        if (lane < K)
+            Y[row * P.ldy] = acc;
     }
 }
 
@@ -711,13 +866,37 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
 
 namespace {
 
+// The chain kernel keeps its products in shared memory, the sliced-row
+// kernels use none.  An SM set up for a kernel without shared memory (all of
+// it L1) takes no CTA that needs some until it drains, so the chains would
+// wait for the sliced rows instead of running beside them: every kernel here
+// asks for the same split of L1 and shared memory.
+constexpr int kCarveoutPct = 25;
+
+// Sets the split for kernel Kern once per device (the attribute belongs to
+// the device's context).
+template <auto Kern>
+void same_carveout()
+{
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    ABHSF_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = uint64_t(1) << (dev & 63);
+    if (done.load(std::memory_order_relaxed) & bit)
+        return;
+    ABHSF_CUDA(cudaFuncSetAttribute(Kern, cudaFuncAttributePreferredSharedMemoryCarveout, kCarveoutPct));
+    done.fetch_or(bit, std::memory_order_relaxed);
+}
+
 template <int S, int VT, bool B>
 void launch_kind(bool chains, const dc_args& P, cudaStream_t st)
 {
     if (chains) {
+        same_carveout<k_spmv_chains<S, VT, B>>();
         const unsigned grid = (unsigned)((P.warps + kChainWarps - 1) / kChainWarps);
         k_spmv_chains<S, VT, B><<<grid, 32 * kChainWarps, 0, st>>>(P);
     } else {
+        same_carveout<k_spmv_slices<S, VT, B>>();
         const unsigned grid = (unsigned)((P.warps + kWarpsPerCta - 1) / kWarpsPerCta);
         k_spmv_slices<S, VT, B><<<grid, 32 * kWarpsPerCta, 0, st>>>(P);
     }
@@ -780,13 +959,45 @@ dc_args batch_args(const abhsf_batch& b, const uint8_t* sched, const int64_t* wb
     return P;
 }
 
+template <int K>
+void launch_mm_k(bool chains, int s, const dc_args& P, cudaStream_t st)
+{
+    same_carveout<k_spmm_chains<K>>();
+    same_carveout<k_spmm_slices<K>>();
+    if (chains)
+        k_spmm_chains<K><<<(unsigned)((P.warps + kChainWarps - 1) / kChainWarps), 32 * kChainWarps, 0, st>>>(P, s);
+    else
+        k_spmm_slices<K><<<(unsigned)((P.warps + kWarpsPerCta - 1) / kWarpsPerCta), 32 * kWarpsPerCta, 0, st>>>(P, s);
+    ABHSF_CUDA(cudaGetLastError());
+}
+
+// One pass over `cols` columns: the SpMV kernels for one, the K-column ones
+// (FP64) otherwise.
+void launch_cols(int cols, int s, int vt, bool chains, const dc_args& P, cudaStream_t st)
+{
+    if (P.warps == 0)
+        return;
+    switch (cols) {
+    case 1: launch(s, vt, false, chains, P, st); break;
+    case 2: launch_mm_k<2>(chains, s, P, st); break;
+    case 4: launch_mm_k<4>(chains, s, P, st); break;
+    case 8: launch_mm_k<8>(chains, s, P, st); break;
+    case 16: launch_mm_k<16>(chains, s, P, st); break;
+    case 32: launch_mm_k<32>(chains, s, P, st); break;
+    default: fail(ABHSF_ERROR_UNSUPPORTED, "slices: a pass of 1, 2, 4, 8, 16 or 32 columns");
+    }
+}
+
 // Chains on the side stream, after everything queued on st so far.
 void fork_chains(cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, int s, int vt, bool batch,
-                 const dc_args& P)
+                 const dc_args& P, int cols = 1)
 {
     ABHSF_CUDA(cudaEventRecord(fork, st));
     ABHSF_CUDA(cudaStreamWaitEvent(side, fork, 0));
-    launch(s, vt, batch, true, P, side);
+    if (batch)
+        launch(s, vt, batch, true, P, side);
+    else
+        launch_cols(cols, s, vt, true, P, side);
     ABHSF_CUDA(cudaEventRecord(join, side));
 }
 
@@ -805,21 +1016,21 @@ dc_plan plan_of(const abhsf_matrix& a)
 }
 
 void slices_begin(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
-                  cudaStream_t st)
+                  cudaStream_t st, int cols)
 {
     if (p.cwarps == 0)
         return;
     if (!a.dc_side)
         fail(ABHSF_ERROR_CUDA, "matrix has chains but no side stream");
     fork_chains(st, a.dc_side, a.dc_fork, a.dc_join, a.s, a.value_type, false,
-                args_of(a, p.csched, p.cwbeg, p.cwarps, x, ldx, y, ldy));
+                args_of(a, p.csched, p.cwbeg, p.cwarps, x, ldx, y, ldy), cols);
 }
 
 void slices_end(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
-                cudaStream_t st)
+                cudaStream_t st, int cols)
 {
     if (p.warps)
-        launch(a.s, a.value_type, false, false, args_of(a, p.sched, p.wbeg, p.warps, x, ldx, y, ldy), st);
+        launch_cols(cols, a.s, a.value_type, false, args_of(a, p.sched, p.wbeg, p.warps, x, ldx, y, ldy), st);
     if (p.cwarps)
         ABHSF_CUDA(cudaStreamWaitEvent(st, a.dc_join, 0));
 }

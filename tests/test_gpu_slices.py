@@ -143,15 +143,21 @@ def test_slice_spmm_columns_equal_their_spmv(gpu):
     coo = heavy_rows(seed=3)
     A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
     rng = np.random.default_rng(5)
-    for k in (1, 3, 8, 13):
-        X = torch.from_numpy(rng.uniform(-1, 1, (coo.n, k))).cuda()
-        Y0 = torch.from_numpy(rng.standard_normal((coo.m, k))).cuda()
-        Y = Y0.clone()
+    # passes of 32, 16, 8, 4, 2 and 1 columns through the sliced rows and the
+    # chains; X and Y inside wider buffers (ldx = k + 3, ldy = k + 5)
+    for k in (1, 2, 3, 8, 13, 16, 32, 63):
+        Xb = torch.from_numpy(rng.uniform(-1, 1, (coo.n, k + 3))).cuda()
+        Yb = torch.from_numpy(rng.standard_normal((coo.m, k + 5))).cuda()
+        Yc = Yb.clone()
+        X, Y = Xb[:, :k], Yc[:, :k]
         A.spmm(X, Y)
+        assert torch.equal(Yc[:, k:], Yb[:, k:])  # nothing outside the k columns
         for j in range(k):
-            y = Y0[:, j].contiguous()
+            y = Yb[:, j].contiguous()
             A.spmv(X[:, j].contiguous(), y)
             assert torch.equal(Y[:, j], y), (k, j)
+    sl = A.slices()
+    assert sl["chain"].sum() > 0 and (sl["chain"] == 0).sum() > 0  # both kernels ran
 
 
 def test_slice_batch_equals_each_matrix_alone(gpu):

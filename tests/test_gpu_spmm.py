@@ -102,6 +102,23 @@ def test_spmm_tiled_mixture_matches_spmv(gpu):
     np.testing.assert_array_equal(_spmm(A, X, Y0), _spmv_columns(A, X, Y0))
 
 
+@pytest.mark.parametrize("k", [32, 45])
+def test_spmm_power_law_wide_passes(gpu, k):
+    """R-MAT (power-law rows): sliced rows and chains through the passes of 32
+    (then 8, 4, 1) columns, against the reference order per column."""
+    coo = W.rmat(1 << 13, 24, seed=9)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    sl = A.slices()
+    assert sl["slices"] > 0
+    X, Y0 = _inputs(coo, k, seed=k)
+    Y = _spmm(A, X, Y0, 2, 1)
+    order = np.lexsort((coo.cols, coo.rows))
+    r, c, v = coo.rows[order], coo.cols[order], coo.vals[order]
+    for j in (0, 7, k - 1):
+        np.testing.assert_array_equal(Y[:, j], oracle.spmv_elements(r, c, v, X[:, j].copy(), Y0[:, j].copy()))
+    np.testing.assert_array_equal(Y, _spmv_columns(A, X, Y0))
+
+
 def test_spmm_arguments(gpu):
     import torch
     coo = W.random_blocky(300, 200, 64, 10, seed=1)
