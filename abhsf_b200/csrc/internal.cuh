@@ -85,15 +85,21 @@ void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys
 // Delta-coded row slices of the hypersparse block rows (spmv_stream.cu):
 // prepare_stream picks the block rows (no dense tile, at most `avg`
 // elements per tile on average), encodes them and deals the slices;
-// deal_slices deals the sliced rows (chains = false) or the chains of block
-// rows [brow_lo, brow_hi) of several matrices over one launch.  A launch plan
-// names both schedules; slices_begin forks the chains onto the side stream
+// deal_slices deals the slices of one kind (deal_kind) of block rows
+// [brow_lo, brow_hi) of several matrices over one launch.  A launch plan
+// names the schedules; slices_begin forks the chains onto the side stream
 // (call it before the ring kernel, so that they run beside it) and
 // slices_end adds the sliced rows on st and joins the chains back (x[i * ldx],
 // y[i * ldy]).  The caller holds dc_mu across the pair.
 void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st);
+enum deal_kind {
+    kDealSliced = 0,    // the sliced rows
+    kDealChains = 1,    // every chain
+    kDealPlain = 2,     // the chains that are not critical
+    kDealCritical = 3,  // the critical chains, one a warp
+};
 void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sched, dbuf<int64_t>& wbeg,
-                 int& warps, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, bool chains);
+                 int& warps, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, int kind);
 struct dc_plan {
     const uint8_t* sched = nullptr;
     const int64_t* wbeg = nullptr;
@@ -101,6 +107,9 @@ struct dc_plan {
     const uint8_t* csched = nullptr;
     const int64_t* cwbeg = nullptr;
     int cwarps = 0;
+    const uint8_t* xsched = nullptr;  // critical chains
+    const int64_t* xwbeg = nullptr;
+    int xwarps = 0;
 };
 dc_plan plan_of(const abhsf_matrix& a);
 // cols > 1 (FP64 only: 2, 4, 8, 16 or 32): Y += A X over that many columns

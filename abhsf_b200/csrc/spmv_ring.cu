@@ -1452,7 +1452,7 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     int ctas = 0, mpv = 0;
     if (!build_ring_schedule({&a}, 32, a.ring_desc, a.ring_wbeg, ctas, mpv, st)) {
         // every block row is a slice row, or the ring's counters would overflow
-        a.ring_ready = (a.dc_warps > 0 || a.dc_cwarps > 0) && a.dc_rows == a.tree_nrows;
+        a.ring_ready = (a.dc_warps > 0 || a.dc_cwarps > 0 || a.dc_xwarps > 0) && a.dc_rows == a.tree_nrows;
         return;  // else the streaming kernel serves this matrix
     }
     a.ring_ready = true;
@@ -1602,8 +1602,8 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
             if (a.ring_warps == 0 ||
                 !build_ring_schedule({&a}, 32, ch.desc, ch.wbeg, ch.ctas, mpv, st, ch.brow0, ch.brow1))
                 ch.ctas = 0;  // no ring tiles in these block rows
-            deal_slices({&a}, ch.dc_sched, ch.dc_wbeg, ch.dc_warps, st, ch.brow0, ch.brow1, false);
-            deal_slices({&a}, ch.dc_csched, ch.dc_cwbeg, ch.dc_cwarps, st, ch.brow0, ch.brow1, true);
+            deal_slices({&a}, ch.dc_sched, ch.dc_wbeg, ch.dc_warps, st, ch.brow0, ch.brow1, kDealSliced);
+            deal_slices({&a}, ch.dc_csched, ch.dc_cwbeg, ch.dc_cwarps, st, ch.brow0, ch.brow1, kDealChains);
         }
         if (!a.host_in)
             ABHSF_CUDA(cudaStreamCreateWithFlags(&a.host_in, cudaStreamNonBlocking));

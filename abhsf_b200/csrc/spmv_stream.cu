@@ -33,6 +33,8 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <queue>
 #include <vector>
 
@@ -57,6 +59,12 @@ constexpr int kMidShift = 20;     // dc_slice::geo: matrix index of a batch
 constexpr uint32_t kLenMask = (1u << 24) - 1u;
 constexpr int kChainMin = 256;   // rows longer than this are summed alone, as a chain
 constexpr int kRingTilesMax = 256;  // block rows of more tiles go to the slices whatever their density
+// A chain of at least kCriticalMin elements and at least half the longest
+// one's is critical: the launch cannot end before it does, so it runs on an
+// SM of its own (one warp per chain, up to kChainWarps on an SM), where no
+// other warp takes issue slots from its adds.  At most kCriticalMax.
+constexpr int kCriticalMin = 16384;
+constexpr int kCriticalMax = 8;
 
 // What the kernel needs of one slice (32 bytes, in schedule order).
 struct __align__(16) dc_slice {
@@ -185,57 +193,85 @@ __device__ __forceinline__ T add_products_full(T run, const T* q)
     return run;
 }
 
+// Sliced rows.  A warp sums its dealt slices one after another, each lane
+// one row.  The next slice's descriptor and lane record, and the next step's
+// words and values, are loaded while the current ones are summed, so that a
+// step waits only on its x gathers.
 template <int S, int VT, bool B>
 __global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmv_slices(dc_args P)
 {
     using T = typename vt_of<VT>::T;
     using V = typename vt_of<VT>::V;
+    constexpr int U = kUnroll;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gw = blockIdx.x * kWarpsPerCta + warp;
     if (gw >= P.warps)
         return;
+    int64_t si = P.wbeg[gw];
     const int64_t s1 = P.wbeg[gw + 1];
+    if (si >= s1)
+        return;
+    auto mat = [&](const dc_slice& q) -> const dc_mat& { return B ? P.mats[q.geo >> kMidShift] : P.A; };
+    auto record = [&](const dc_slice& q) -> uint32_t {
+        return lane < (int)q.lanes ? mat(q).lane[q.meta + lane] : 0u;
+    };
+    dc_slice sl = P.slices[si];
+    dc_slice nx = si + 1 < s1 ? P.slices[si + 1] : sl;
+    uint32_t rec = record(sl);
 #pragma unroll 1
-    for (int64_t si = P.wbeg[gw]; si < s1; ++si) {
-        const dc_slice sl = P.slices[si];
+    for (; si < s1; ++si) {
+        const bool more = si + 1 < s1;
+        const dc_slice nn = si + 2 < s1 ? P.slices[si + 2] : nx;
+        const uint32_t rec_n = more ? record(nx) : 0u;
         const int mid = (int)(sl.geo >> kMidShift);
-        const dc_mat& M = B ? P.mats[mid] : P.A;
+        const dc_mat& M = mat(sl);
         const T* X = static_cast<const T*>(B ? P.xs[mid] : P.x);
         T* Y = static_cast<T*>(B ? P.ys[mid] : P.y);
         const int64_t ldx = B ? 1 : P.ldx, ldy = B ? 1 : P.ldy;
-        const uint32_t* W = M.words + sl.base;
-        const V* Vv = static_cast<const V*>(M.vals) + sl.base;
-        {
-            // one row per lane, element k of the lane's row at slot 32 k + lane
-            const uint32_t rec = lane < (int)sl.lanes ? M.lane[sl.meta + lane] : 0u;
-            const int len = (int)(rec & kLenMask);
-            const int64_t row = (int64_t)sl.brow * S + (int64_t)(rec >> 24);
-            T acc = len ? Y[row * ldy] : T(0);
-            uint32_t col = 0;
-#pragma unroll 1
-            for (int k0 = 0; k0 < (int)sl.steps; k0 += kUnroll) {
-                uint32_t w[kUnroll];
-                T v[kUnroll], x[kUnroll];
+        const uint32_t* W = M.words + sl.base + lane;
+        const V* Vv = static_cast<const V*>(M.vals) + sl.base + lane;
+        // one row per lane, element k of the lane's row at slot 32 k + lane
+        const int len = (int)(rec & kLenMask);
+        const int64_t row = (int64_t)sl.brow * S + (int64_t)(rec >> 24);
+        T acc = len ? Y[row * ldy] : T(0);
+        uint32_t col = 0;
+        uint32_t w[U];
+        T v[U];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
-                    const bool ok = k0 + u < len;
-                    const int64_t slot = (int64_t)(k0 + u) * 32 + lane;
-                    w[u] = ok ? ld_stream(W + slot) : 0u;
-                    v[u] = ok ? wide(ld_stream(Vv + slot)) : T(0);
-                }
-#pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
-                    col += w[u];
-                    x[u] = k0 + u < len ? __ldg(X + (int64_t)col * ldx) : T(0);
-                }
-#pragma unroll
-                for (int u = 0; u < kUnroll; ++u)
-                    if (k0 + u < len)
-                        acc = dadd(acc, dmul(v[u], x[u]));
-            }
-            if (len)
-                Y[row * ldy] = acc;
+        for (int u = 0; u < U; ++u) {
+            w[u] = u < len ? ld_stream(W + 32 * u) : 0u;
+            v[u] = u < len ? wide(ld_stream(Vv + 32 * u)) : T(0);
         }
+#pragma unroll 1
+        for (int k0 = 0; k0 < (int)sl.steps; k0 += U) {
+            uint32_t wn[U];
+            T vn[U], x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {  // the next step's words and values
+                const int k = k0 + U + u;
+                wn[u] = k < len ? ld_stream(W + 32 * k) : 0u;
+                vn[u] = k < len ? wide(ld_stream(Vv + 32 * k)) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                col += w[u];
+                x[u] = k0 + u < len ? __ldg(X + (int64_t)col * ldx) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (k0 + u < len)
+                    acc = dadd(acc, dmul(v[u], x[u]));
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                w[u] = wn[u];
+                v[u] = vn[u];
+            }
+        }
+        if (len)
+            Y[row * ldy] = acc;
+        sl = nx;
+        nx = nn;
+        rec = rec_n;
     }
 }
 
@@ -604,8 +640,13 @@ int stream_grid_warps(int64_t items, bool chains, bool beside_chains)
 // The side stream and the fork / join events of a handle with chains.
 void make_side(cudaStream_t& side, cudaEvent_t& fork, cudaEvent_t& join)
 {
-    if (!side)
-        ABHSF_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    if (!side) {
+        // the highest priority: the chains' CTAs are placed before the others
+        // when both wait for SMs, the critical ones on SMs still empty
+        int least = 0, greatest = 0;
+        ABHSF_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        ABHSF_CUDA(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, greatest));
+    }
     if (!fork)
         ABHSF_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     if (!join)
@@ -625,8 +666,9 @@ inline uint64_t slice_weight(const abhsf_matrix::dc_slice_host& p)
 // matrices (block rows in [brow_lo, brow_hi) only) over the warps of one
 // launch.
 void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sched, dbuf<int64_t>& wbeg_d,
-                 int& warps_out, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, bool chains)
+                 int& warps_out, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, int kind)
 {
+    const bool chains = kind != kDealSliced;
     struct item {
         uint64_t w;
         uint32_t mid;
@@ -638,16 +680,18 @@ void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sc
         const auto& ps = mats[i]->dc_host;
         for (size_t k = 0; k < ps.size(); ++k)
             if ((int64_t)ps[k].brow >= brow_lo && (int64_t)ps[k].brow < brow_hi) {
-                if (ps[k].chain == chains)
-                    items.push_back(item{slice_weight(ps[k]), (uint32_t)i, (uint32_t)k});
-                else
+                if (ps[k].chain != chains)
                     other = true;
+                else if (kind == kDealSliced || kind == kDealChains ||
+                         ps[k].critical == (kind == kDealCritical))
+                    items.push_back(item{slice_weight(ps[k]), (uint32_t)i, (uint32_t)k});
             }
     }
     warps_out = 0;
     if (items.empty())
         return;
-    const int W = stream_grid_warps((int64_t)items.size(), chains, !chains && other);
+    const int W = kind == kDealCritical ? (int)items.size()
+                                        : stream_grid_warps((int64_t)items.size(), chains, !chains && other);
     std::stable_sort(items.begin(), items.end(), [](const item& a, const item& b) { return a.w > b.w; });
     using load_t = std::pair<uint64_t, int>;
     std::priority_queue<load_t, std::vector<load_t>, std::greater<load_t>> heap;
@@ -694,7 +738,7 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
 {
     a.dc_host.clear();
     a.dc_tree_flag.assign((size_t)a.tree_nrows, 0);
-    a.dc_warps = a.dc_cwarps = 0;
+    a.dc_warps = a.dc_cwarps = a.dc_xwarps = 0;
     a.dc_elements = a.dc_rows = a.dc_slots = a.dc_lane_records = 0;
     const int s = a.s, lg = a.lg;
     if (avg <= 0.f || a.tree_nrows == 0 || a.sum_order != ABHSF_SUM_REFERENCE || (uint64_t)a.n > (uint64_t(1) << 32))
@@ -858,9 +902,23 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
     a.dc_rows = ns;
     a.dc_slots = slots;
     a.dc_lane_records = (int64_t)lane_rec.size();
-    deal_slices({&a}, a.dc_sched, a.dc_wbeg, a.dc_warps, st, 0, INT64_MAX, false);
-    deal_slices({&a}, a.dc_csched, a.dc_cwbeg, a.dc_cwarps, st, 0, INT64_MAX, true);
-    if (a.dc_cwarps)
+    {  // the critical chains
+        std::vector<size_t> ch;
+        for (size_t k = 0; k < SL.size(); ++k)
+            if (SL[k].chain)
+                ch.push_back(k);
+        std::stable_sort(ch.begin(), ch.end(), [&](size_t p, size_t q) { return SL[p].steps > SL[q].steps; });
+        for (size_t j = 0; j < ch.size() && j < (size_t)kCriticalMax; ++j) {
+            auto& c = SL[ch[j]];
+            if (c.steps < (uint32_t)kCriticalMin || 2ull * c.steps < SL[ch[0]].steps)
+                break;
+            c.critical = true;
+        }
+    }
+    deal_slices({&a}, a.dc_sched, a.dc_wbeg, a.dc_warps, st, 0, INT64_MAX, kDealSliced);
+    deal_slices({&a}, a.dc_csched, a.dc_cwbeg, a.dc_cwarps, st, 0, INT64_MAX, kDealPlain);
+    deal_slices({&a}, a.dc_xsched, a.dc_xwbeg, a.dc_xwarps, st, 0, INT64_MAX, kDealCritical);
+    if (a.dc_cwarps || a.dc_xwarps)
         make_side(a.dc_side, a.dc_fork, a.dc_join);
 }
 
@@ -888,13 +946,37 @@ void same_carveout()
     done.fetch_or(bit, std::memory_order_relaxed);
 }
 
+// Dynamic shared memory that, with the kernel's own, fills an SM: a CTA
+// launched with it has the SM to itself.  Set up once per device.
+template <auto Kern>
+size_t whole_sm_smem()
+{
+    static std::mutex mu;
+    static std::map<int, size_t> per_dev;
+    int dev = 0;
+    ABHSF_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = per_dev.find(dev);
+    if (it != per_dev.end())
+        return it->second;
+    int optin = 0;
+    ABHSF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa{};
+    ABHSF_CUDA(cudaFuncGetAttributes(&fa, Kern));
+    const size_t dyn = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+    ABHSF_CUDA(cudaFuncSetAttribute(Kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    per_dev[dev] = dyn;
+    return dyn;
+}
+
 template <int S, int VT, bool B>
-void launch_kind(bool chains, const dc_args& P, cudaStream_t st)
+void launch_kind(bool chains, const dc_args& P, cudaStream_t st, bool whole_sm)
 {
     if (chains) {
         same_carveout<k_spmv_chains<S, VT, B>>();
+        const size_t dyn = whole_sm ? whole_sm_smem<k_spmv_chains<S, VT, B>>() : 0;
         const unsigned grid = (unsigned)((P.warps + kChainWarps - 1) / kChainWarps);
-        k_spmv_chains<S, VT, B><<<grid, 32 * kChainWarps, 0, st>>>(P);
+        k_spmv_chains<S, VT, B><<<grid, 32 * kChainWarps, dyn, st>>>(P);
     } else {
         same_carveout<k_spmv_slices<S, VT, B>>();
         const unsigned grid = (unsigned)((P.warps + kWarpsPerCta - 1) / kWarpsPerCta);
@@ -904,28 +986,31 @@ void launch_kind(bool chains, const dc_args& P, cudaStream_t st)
 }
 
 template <int VT, bool B>
-void launch_vt(int s, bool chains, const dc_args& P, cudaStream_t st)
+void launch_vt(int s, bool chains, const dc_args& P, cudaStream_t st, bool whole_sm)
 {
     switch (s) {
-    case 16: launch_kind<16, VT, B>(chains, P, st); break;
-    case 32: launch_kind<32, VT, B>(chains, P, st); break;
-    case 64: launch_kind<64, VT, B>(chains, P, st); break;
-    case 128: launch_kind<128, VT, B>(chains, P, st); break;
-    default: launch_kind<256, VT, B>(chains, P, st); break;
+    case 16: launch_kind<16, VT, B>(chains, P, st, whole_sm); break;
+    case 32: launch_kind<32, VT, B>(chains, P, st, whole_sm); break;
+    case 64: launch_kind<64, VT, B>(chains, P, st, whole_sm); break;
+    case 128: launch_kind<128, VT, B>(chains, P, st, whole_sm); break;
+    default: launch_kind<256, VT, B>(chains, P, st, whole_sm); break;
     }
 }
 
-void launch(int s, int vt, bool batch, bool chains, const dc_args& P, cudaStream_t st)
+// whole_sm (chains only): every CTA on an SM of its own.
+void launch(int s, int vt, bool batch, bool chains, const dc_args& P, cudaStream_t st, bool whole_sm = false)
 {
     if (P.warps == 0)
         return;
     if (vt == ABHSF_VALUE_F64)
-        batch ? launch_vt<ABHSF_VALUE_F64, true>(s, chains, P, st) : launch_vt<ABHSF_VALUE_F64, false>(s, chains, P, st);
+        batch ? launch_vt<ABHSF_VALUE_F64, true>(s, chains, P, st, whole_sm)
+              : launch_vt<ABHSF_VALUE_F64, false>(s, chains, P, st, whole_sm);
     else if (vt == ABHSF_VALUE_F32)
-        batch ? launch_vt<ABHSF_VALUE_F32, true>(s, chains, P, st) : launch_vt<ABHSF_VALUE_F32, false>(s, chains, P, st);
+        batch ? launch_vt<ABHSF_VALUE_F32, true>(s, chains, P, st, whole_sm)
+              : launch_vt<ABHSF_VALUE_F32, false>(s, chains, P, st, whole_sm);
     else
-        batch ? launch_vt<ABHSF_VALUE_BF16, true>(s, chains, P, st)
-              : launch_vt<ABHSF_VALUE_BF16, false>(s, chains, P, st);
+        batch ? launch_vt<ABHSF_VALUE_BF16, true>(s, chains, P, st, whole_sm)
+              : launch_vt<ABHSF_VALUE_BF16, false>(s, chains, P, st, whole_sm);
 }
 
 dc_mat mat_of(const abhsf_matrix& a) { return dc_mat{a.dc_words.get(), a.dc_vals.get(), a.dc_lane.get(), a.m}; }
@@ -988,12 +1073,20 @@ void launch_cols(int cols, int s, int vt, bool chains, const dc_args& P, cudaStr
     }
 }
 
-// Chains on the side stream, after everything queued on st so far.
+// Chains on the side stream, after everything queued on st so far: the
+// critical ones first (crit; SMs of their own for a single column), then
+// the others.
 void fork_chains(cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, int s, int vt, bool batch,
-                 const dc_args& P, int cols = 1)
+                 const dc_args& P, int cols = 1, const dc_args* crit = nullptr)
 {
     ABHSF_CUDA(cudaEventRecord(fork, st));
     ABHSF_CUDA(cudaStreamWaitEvent(side, fork, 0));
+    if (crit && crit->warps) {
+        if (cols == 1)
+            launch(s, vt, false, true, *crit, side, true);
+        else
+            launch_cols(cols, s, vt, true, *crit, side);
+    }
     if (batch)
         launch(s, vt, batch, true, P, side);
     else
@@ -1012,18 +1105,22 @@ dc_plan plan_of(const abhsf_matrix& a)
     p.csched = a.dc_csched.get();
     p.cwbeg = a.dc_cwbeg.get();
     p.cwarps = a.dc_cwarps;
+    p.xsched = a.dc_xsched.get();
+    p.xwbeg = a.dc_xwbeg.get();
+    p.xwarps = a.dc_xwarps;
     return p;
 }
 
 void slices_begin(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
                   cudaStream_t st, int cols)
 {
-    if (p.cwarps == 0)
+    if (p.cwarps == 0 && p.xwarps == 0)
         return;
     if (!a.dc_side)
         fail(ABHSF_ERROR_CUDA, "matrix has chains but no side stream");
+    const dc_args crit = args_of(a, p.xsched, p.xwbeg, p.xwarps, x, ldx, y, ldy);
     fork_chains(st, a.dc_side, a.dc_fork, a.dc_join, a.s, a.value_type, false,
-                args_of(a, p.csched, p.cwbeg, p.cwarps, x, ldx, y, ldy), cols);
+                args_of(a, p.csched, p.cwbeg, p.cwarps, x, ldx, y, ldy), cols, &crit);
 }
 
 void slices_end(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
@@ -1031,7 +1128,7 @@ void slices_end(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t 
 {
     if (p.warps)
         launch_cols(cols, a.s, a.value_type, false, args_of(a, p.sched, p.wbeg, p.warps, x, ldx, y, ldy), st);
-    if (p.cwarps)
+    if (p.cwarps || p.xwarps)
         ABHSF_CUDA(cudaStreamWaitEvent(st, a.dc_join, 0));
 }
 
@@ -1049,8 +1146,8 @@ void prepare_batch_stream(abhsf_batch& b, cudaStream_t st)
         return;
     b.dc_table.alloc(t.size() * sizeof(dc_mat));
     ABHSF_CUDA(cudaMemcpyAsync(b.dc_table.get(), t.data(), t.size() * sizeof(dc_mat), cudaMemcpyHostToDevice, st));
-    deal_slices(b.mats, b.dc_sched, b.dc_wbeg, b.dc_warps, st, 0, INT64_MAX, false);
-    deal_slices(b.mats, b.dc_csched, b.dc_cwbeg, b.dc_cwarps, st, 0, INT64_MAX, true);
+    deal_slices(b.mats, b.dc_sched, b.dc_wbeg, b.dc_warps, st, 0, INT64_MAX, kDealSliced);
+    deal_slices(b.mats, b.dc_csched, b.dc_cwbeg, b.dc_cwarps, st, 0, INT64_MAX, kDealChains);
     if (b.dc_cwarps)
         make_side(b.dc_side, b.dc_fork, b.dc_join);
 }

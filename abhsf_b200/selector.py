@@ -19,6 +19,20 @@ writes DIR/selector_model.inc (the model built into the library, copied to
 abhsf_b200/csrc/), DIR/selector_model.f32, DIR/selector_data.npz (features
 and storage of every matrix), DIR/selector_heldout.npz (the held-out part,
 copied to tests/golden/) and DIR/selector_report.json.
+
+The same network trained on measured time instead of storage:
+
+    python -m abhsf_b200.selector train-time --out DIR [--train 1500 --heldout 300] [--data DIR/selector_time_data.npz]
+
+labels each matrix with the FP64 SpMV time at each size (median of five
+launches of the default build), targets softmax(-excess time / tau), picks
+tau and the number of steps on a validation fifth of the training matrices,
+and writes DIR/selector_model_time.inc (copied to abhsf_b200/csrc/, the model
+of ABHSF_SELECT_LEARNED_TIME), DIR/selector_time_data.npz (every matrix's
+features, storage and times; --data reuses it instead of timing anew),
+DIR/selector_time_heldout.npz (copied to tests/golden/) and
+DIR/selector_time_report.json (regret in time and in storage of the model,
+of the storage model, of min-bss and of every fixed size).
 """
 from __future__ import annotations
 
@@ -485,25 +499,46 @@ def choose(model: np.ndarray, X: np.ndarray) -> np.ndarray:
 
 
 def main_time(args) -> int:
-    """train-time: the selector trained on measured SpMV times."""
+    """train-time: the selector trained on measured SpMV times.  The targets'
+    temperature and the number of steps are picked on a validation split (the
+    last fifth of the training matrices), the model then trained on all of
+    them; the held-out matrices are only scored."""
     os.makedirs(args.out, exist_ok=True)
 
     def log(msg):
         print(msg, flush=True)
 
-    seeds_train = np.arange(args.train)
-    seeds_held = np.arange(2000, 2000 + args.heldout)
-    Xtr, Btr, Ttr, ntr = time_dataset(seeds_train, n_max=args.n_max, log=log)
-    Xho, Bho, Tho, nho = time_dataset(seeds_held, n_max=args.n_max, log=log)
+    if args.data:
+        d = np.load(args.data)
+        Xtr, Btr, Ttr = d["X_train"], d["bits_train"], d["ms_train"]
+        Xho, Bho, Tho, nho = d["X_heldout"], d["bits_heldout"], d["ms_heldout"], list(d["names_heldout"])
+    else:
+        seeds_train = np.arange(args.train)
+        seeds_held = np.arange(2000, 2000 + args.heldout)
+        Xtr, Btr, Ttr, ntr = time_dataset(seeds_train, n_max=args.n_max, log=log)
+        Xho, Bho, Tho, nho = time_dataset(seeds_held, n_max=args.n_max, log=log)
+        np.savez_compressed(os.path.join(args.out, "selector_time_data.npz"), X_train=Xtr, bits_train=Btr,
+                            ms_train=Ttr, names_train=np.array(ntr), X_heldout=Xho, bits_heldout=Bho, ms_heldout=Tho,
+                            names_heldout=np.array(nho))
     np.savez_compressed(os.path.join(args.out, "selector_time_heldout.npz"), X=Xho, bits=Bho, ms=Tho,
                         names=np.array(nho))
+    cut = (4 * Xtr.shape[0]) // 5
+    search = {}
+    for tau in (0.05, 0.15, 0.4):
+        for steps in (500, 1500, 4000):
+            mdl = train(Xtr[:cut], Btr[:cut], steps=steps, targets=targets_from_times(Ttr[:cut], tau))
+            search[f"tau={tau} steps={steps}"] = time_regret_summary(Ttr[cut:], choose(mdl, Xtr[cut:]))
+    best = min(search, key=lambda k: (search[k]["total_over_best"], search[k]["avg_pct"]))
+    tau, steps = (float(v.split("=")[1]) for v in best.split())
+    log(f"validation: {json.dumps(search)}\nchosen: {best}")
     t0 = time.perf_counter()
-    model = train(Xtr, Btr, steps=args.steps, log=log, targets=targets_from_times(Ttr))
+    model = train(Xtr, Btr, steps=int(steps), log=log, targets=targets_from_times(Ttr, tau))
     t_train = time.perf_counter() - t0
     model.tofile(os.path.join(args.out, "selector_model_time.f32"))
     write_model_inc(model, os.path.join(args.out, "selector_model_time.inc"), "kBuiltinTimeModel",
                     "Block-size selector trained on measured SpMV times")
-    report = {"train": len(seeds_train), "heldout": len(seeds_held), "train_s": t_train}
+    report = {"train": int(Xtr.shape[0]), "heldout": int(Xho.shape[0]), "train_s": t_train, "chosen": best,
+              "validation": search}
     for split, X, B, T in (("train", Xtr, Btr, Ttr), ("heldout", Xho, Bho, Tho)):
         c_time = choose(model, X)
         c_store = choose(builtin_model(), X)
@@ -529,6 +564,7 @@ def main(argv=None) -> int:
     ap.add_argument("--heldout", type=int, default=200)
     ap.add_argument("--n-max", type=int, default=4_000_000)
     ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--data", help="train-time: a saved selector_time_data.npz instead of timing anew")
     args = ap.parse_args(argv)
     if args.cmd == "train-time":
         return main_time(args)

@@ -194,3 +194,45 @@ def test_slice_host_pipeline(gpu):
     ref = reference_y(coo, x, y)
     A.spmv(x, y)
     np.testing.assert_array_equal(y, ref)
+
+
+def test_critical_chains_on_their_own_sms(gpu):
+    """Rows of 40,000 and 25,000 elements (critical: at least 16,384 elements
+    and half the longest, summed on SMs of their own, first on the side
+    stream), one of 9,000 (a chain beside the others) and a hypersparse rest:
+    FP64 SpMV, f32 SpMV and SpMM bitwise in the reference order."""
+    import torch
+    coo = heavy_rows(n=120000, heavy=(3, 777), per_heavy=40000, sparse=150000, seed=8)
+    rng = np.random.default_rng(9)
+    extra_r = np.concatenate([np.full(25000, 9001, np.int64), np.full(9000, 50000, np.int64)])
+    extra_c = np.concatenate([rng.choice(coo.n, 25000, replace=False), rng.choice(coo.n, 9000, replace=False)])
+    rows = np.concatenate([coo.rows[coo.rows != 777], extra_r])
+    cols = np.concatenate([coo.cols[coo.rows != 777], extra_c])
+    key = np.unique(rows * coo.n + cols)
+    rows, cols = key // coo.n, key % coo.n
+    vals = rng.standard_normal(rows.size)
+    A = AbhsfMatrix.from_elements(rows, cols, vals, coo.n, coo.n, block_size=64)
+    sl = A.slices()
+    lens = sl["steps"][sl["chain"] == 1]
+    assert sorted(lens[lens >= 16384].tolist()) == [25000, 40000] and (lens == 9000).sum() == 1
+    assert A.kernels() == 3  # sliced rows, chains, critical chains
+    x = rng.uniform(-1, 1, coo.n)
+    y0 = rng.standard_normal(coo.n)
+    for _ in range(2):
+        yd = torch.from_numpy(y0.copy()).cuda()
+        A.spmv(torch.from_numpy(x).cuda(), yd)
+        np.testing.assert_array_equal(yd.cpu().numpy(), oracle.spmv_elements(rows, cols, vals, x, y0.copy()))
+    X = rng.uniform(-1, 1, (coo.n, 3))
+    Y0 = rng.standard_normal((coo.n, 3))
+    Y = torch.from_numpy(Y0.copy()).cuda()
+    A.spmm(torch.from_numpy(X).cuda(), Y)
+    for j in range(3):
+        np.testing.assert_array_equal(Y[:, j].cpu().numpy(),
+                                      oracle.spmv_elements(rows, cols, vals, X[:, j].copy(), Y0[:, j].copy()))
+    A32 = AbhsfMatrix.from_elements(rows, cols, vals, coo.n, coo.n, block_size=64, value_type="f32")
+    x32 = x.astype(np.float32)
+    y32 = y0.astype(np.float32)
+    yd = torch.from_numpy(y32.copy()).cuda()
+    A32.spmv_f32(torch.from_numpy(x32).cuda(), yd)
+    v32 = oracle.values_as_f32(vals, "f32")
+    np.testing.assert_array_equal(yd.cpu().numpy(), oracle.spmv_elements_f32(rows, cols, v32, x32, y32.copy()))

@@ -126,3 +126,29 @@ def test_builtin_model_regret_on_heldout_fixture():
     assert learned["avg_pct"] < 0.1 * min(f["avg_pct"] for f in fixed), (learned, fixed)
     assert learned["max_pct"] < min(f["max_pct"] for f in fixed)
     assert learned["exact"] >= 0.9
+
+
+def test_builtin_time_model_on_heldout_fixture():
+    """The model trained on measured SpMV time, on the 300 held-out matrices
+    of its training run (tests/golden/selector_time_heldout.npz, written by
+    `python -m abhsf_b200.selector train-time`: features, storage and the
+    FP64 SpMV time at each size, timed on a B200): forward pass in the
+    float64 oracle.  Its choices are faster in total than min-bss's and than
+    every fixed size's, and its time regret (the consistency.cpp:147-173
+    measure with time in place of storage) is below theirs on average."""
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "selector_time_heldout.npz"))
+    X, bits, ms = z["X"], z["bits"], z["ms"]
+    assert X.shape == (300, 12) and bits.shape == (300, 5) and ms.shape == (300, 5)
+    assert np.all(ms > 0)
+    probs, _ = so.forward(sel.builtin_time_model(), X)
+    learned = sel.time_regret_summary(ms, probs.argmax(axis=1))
+    minbss = sel.time_regret_summary(ms, bits.astype(np.float64).argmin(axis=1))
+    fixed = [sel.time_regret_summary(ms, np.full(len(X), k)) for k in range(5)]
+    assert learned["total_over_best"] < minbss["total_over_best"], (learned, minbss)
+    assert learned["total_over_best"] < min(f["total_over_best"] for f in fixed), (learned, fixed)
+    assert learned["avg_pct"] < min([minbss["avg_pct"]] + [f["avg_pct"] for f in fixed])
+    # the storage model picks by storage; its choices are no faster than min-bss's
+    store = sel.time_regret_summary(ms, so.forward(sel.builtin_model(), X)[0].argmax(axis=1))
+    assert store["total_over_best"] > learned["total_over_best"]
