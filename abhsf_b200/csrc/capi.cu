@@ -136,7 +136,7 @@ abhsf_status abhsf_spmv_kernels(const abhsf_matrix* a, int32_t* kernels)
             else {
                 const bool seq = !a->ring_ready && (a->s == 32 || a->s == 64 ? true : a->seq_nrows > 0 || a->dc_rows == 0);
                 k = (a->ring_ready ? (a->ring_warps > 0 ? 1 : 0) : (seq ? 1 : 0)) + (a->dc_warps > 0 ? 1 : 0) +
-                    (a->dc_cwarps > 0 ? 1 : 0) + (a->dc_xwarps > 0 ? 1 : 0);
+                    (a->dc_cwarps > 0 ? 1 : 0);
             }
         }
         *kernels = k;

@@ -196,7 +196,6 @@ struct abhsf_matrix {
         int64_t meta = 0;   // sliced: first of its 32 lane records; chain: the row within the block row
         uint32_t brow = 0, steps = 0, lanes = 0;
         bool chain = false;
-        bool critical = false;  // a chain long enough to run on an SM of its own
     };
     std::vector<dc_slice_host> dc_host;  // block rows ascending; per block row its chains, then its sliced rows
     std::vector<uint8_t> dc_tree_flag;   // per non-empty block row (tree_rows order): served by the slices
@@ -211,9 +210,6 @@ struct abhsf_matrix {
     abhsf::dbuf<uint8_t> dc_csched;      // ... and its chains, launched on dc_side beside the others
     abhsf::dbuf<int64_t> dc_cwbeg;
     int dc_cwarps = 0;
-    abhsf::dbuf<uint8_t> dc_xsched;      // ... the critical chains (one a warp), launched first on dc_side
-    abhsf::dbuf<int64_t> dc_xwbeg;
-    int dc_xwarps = 0;
     cudaStream_t dc_side = nullptr;      // created with the first chain; forked from the caller's stream
     cudaEvent_t dc_fork = nullptr, dc_join = nullptr;
     mutable std::mutex dc_mu;            // one fork / join sequence at a time

@@ -93,10 +93,8 @@ void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys
 // y[i * ldy]).  The caller holds dc_mu across the pair.
 void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st);
 enum deal_kind {
-    kDealSliced = 0,    // the sliced rows
-    kDealChains = 1,    // every chain
-    kDealPlain = 2,     // the chains that are not critical
-    kDealCritical = 3,  // the critical chains, one a warp
+    kDealSliced = 0,  // the sliced rows
+    kDealChains = 1,  // the chains
 };
 void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sched, dbuf<int64_t>& wbeg,
                  int& warps, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, int kind);
@@ -107,9 +105,6 @@ struct dc_plan {
     const uint8_t* csched = nullptr;
     const int64_t* cwbeg = nullptr;
     int cwarps = 0;
-    const uint8_t* xsched = nullptr;  // critical chains
-    const int64_t* xwbeg = nullptr;
-    int xwarps = 0;
 };
 dc_plan plan_of(const abhsf_matrix& a);
 // cols > 1 (FP64 only: 2, 4, 8, 16 or 32): Y += A X over that many columns

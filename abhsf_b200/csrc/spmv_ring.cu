@@ -1452,7 +1452,7 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     int ctas = 0, mpv = 0;
     if (!build_ring_schedule({&a}, 32, a.ring_desc, a.ring_wbeg, ctas, mpv, st)) {
         // every block row is a slice row, or the ring's counters would overflow
-        a.ring_ready = (a.dc_warps > 0 || a.dc_cwarps > 0 || a.dc_xwarps > 0) && a.dc_rows == a.tree_nrows;
+        a.ring_ready = (a.dc_warps > 0 || a.dc_cwarps > 0) && a.dc_rows == a.tree_nrows;
         return;  // else the streaming kernel serves this matrix
     }
     a.ring_ready = true;

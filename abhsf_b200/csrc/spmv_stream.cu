@@ -33,7 +33,6 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
-#include <map>
 #include <mutex>
 #include <queue>
 #include <vector>
@@ -59,12 +58,6 @@ constexpr int kMidShift = 20;     // dc_slice::geo: matrix index of a batch
 constexpr uint32_t kLenMask = (1u << 24) - 1u;
 constexpr int kChainMin = 256;   // rows longer than this are summed alone, as a chain
 constexpr int kRingTilesMax = 256;  // block rows of more tiles go to the slices whatever their density
-// A chain of at least kCriticalMin elements and at least half the longest
-// one's is critical: the launch cannot end before it does, so it runs on an
-// SM of its own (one warp per chain, up to kChainWarps on an SM), where no
-// other warp takes issue slots from its adds.  At most kCriticalMax.
-constexpr int kCriticalMin = 16384;
-constexpr int kCriticalMax = 8;
 
 // What the kernel needs of one slice (32 bytes, in schedule order).
 struct __align__(16) dc_slice {
@@ -642,7 +635,7 @@ void make_side(cudaStream_t& side, cudaEvent_t& fork, cudaEvent_t& join)
 {
     if (!side) {
         // the highest priority: the chains' CTAs are placed before the others
-        // when both wait for SMs, the critical ones on SMs still empty
+        // when both wait for SMs (the longest chain bounds the launch)
         int least = 0, greatest = 0;
         ABHSF_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         ABHSF_CUDA(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, greatest));
@@ -682,16 +675,14 @@ void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sc
             if ((int64_t)ps[k].brow >= brow_lo && (int64_t)ps[k].brow < brow_hi) {
                 if (ps[k].chain != chains)
                     other = true;
-                else if (kind == kDealSliced || kind == kDealChains ||
-                         ps[k].critical == (kind == kDealCritical))
+                else
                     items.push_back(item{slice_weight(ps[k]), (uint32_t)i, (uint32_t)k});
             }
     }
     warps_out = 0;
     if (items.empty())
         return;
-    const int W = kind == kDealCritical ? (int)items.size()
-                                        : stream_grid_warps((int64_t)items.size(), chains, !chains && other);
+    const int W = stream_grid_warps((int64_t)items.size(), chains, !chains && other);
     std::stable_sort(items.begin(), items.end(), [](const item& a, const item& b) { return a.w > b.w; });
     using load_t = std::pair<uint64_t, int>;
     std::priority_queue<load_t, std::vector<load_t>, std::greater<load_t>> heap;
@@ -738,7 +729,7 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
 {
     a.dc_host.clear();
     a.dc_tree_flag.assign((size_t)a.tree_nrows, 0);
-    a.dc_warps = a.dc_cwarps = a.dc_xwarps = 0;
+    a.dc_warps = a.dc_cwarps = 0;
     a.dc_elements = a.dc_rows = a.dc_slots = a.dc_lane_records = 0;
     const int s = a.s, lg = a.lg;
     if (avg <= 0.f || a.tree_nrows == 0 || a.sum_order != ABHSF_SUM_REFERENCE || (uint64_t)a.n > (uint64_t(1) << 32))
@@ -902,23 +893,9 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
     a.dc_rows = ns;
     a.dc_slots = slots;
     a.dc_lane_records = (int64_t)lane_rec.size();
-    {  // the critical chains
-        std::vector<size_t> ch;
-        for (size_t k = 0; k < SL.size(); ++k)
-            if (SL[k].chain)
-                ch.push_back(k);
-        std::stable_sort(ch.begin(), ch.end(), [&](size_t p, size_t q) { return SL[p].steps > SL[q].steps; });
-        for (size_t j = 0; j < ch.size() && j < (size_t)kCriticalMax; ++j) {
-            auto& c = SL[ch[j]];
-            if (c.steps < (uint32_t)kCriticalMin || 2ull * c.steps < SL[ch[0]].steps)
-                break;
-            c.critical = true;
-        }
-    }
     deal_slices({&a}, a.dc_sched, a.dc_wbeg, a.dc_warps, st, 0, INT64_MAX, kDealSliced);
-    deal_slices({&a}, a.dc_csched, a.dc_cwbeg, a.dc_cwarps, st, 0, INT64_MAX, kDealPlain);
-    deal_slices({&a}, a.dc_xsched, a.dc_xwbeg, a.dc_xwarps, st, 0, INT64_MAX, kDealCritical);
-    if (a.dc_cwarps || a.dc_xwarps)
+    deal_slices({&a}, a.dc_csched, a.dc_cwbeg, a.dc_cwarps, st, 0, INT64_MAX, kDealChains);
+    if (a.dc_cwarps)
         make_side(a.dc_side, a.dc_fork, a.dc_join);
 }
 
@@ -946,37 +923,13 @@ void same_carveout()
     done.fetch_or(bit, std::memory_order_relaxed);
 }
 
-// Dynamic shared memory that, with the kernel's own, fills an SM: a CTA
-// launched with it has the SM to itself.  Set up once per device.
-template <auto Kern>
-size_t whole_sm_smem()
-{
-    static std::mutex mu;
-    static std::map<int, size_t> per_dev;
-    int dev = 0;
-    ABHSF_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = per_dev.find(dev);
-    if (it != per_dev.end())
-        return it->second;
-    int optin = 0;
-    ABHSF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    cudaFuncAttributes fa{};
-    ABHSF_CUDA(cudaFuncGetAttributes(&fa, Kern));
-    const size_t dyn = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
-    ABHSF_CUDA(cudaFuncSetAttribute(Kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    per_dev[dev] = dyn;
-    return dyn;
-}
-
 template <int S, int VT, bool B>
-void launch_kind(bool chains, const dc_args& P, cudaStream_t st, bool whole_sm)
+void launch_kind(bool chains, const dc_args& P, cudaStream_t st)
 {
     if (chains) {
         same_carveout<k_spmv_chains<S, VT, B>>();
-        const size_t dyn = whole_sm ? whole_sm_smem<k_spmv_chains<S, VT, B>>() : 0;
         const unsigned grid = (unsigned)((P.warps + kChainWarps - 1) / kChainWarps);
-        k_spmv_chains<S, VT, B><<<grid, 32 * kChainWarps, dyn, st>>>(P);
+        k_spmv_chains<S, VT, B><<<grid, 32 * kChainWarps, 0, st>>>(P);
     } else {
         same_carveout<k_spmv_slices<S, VT, B>>();
         const unsigned grid = (unsigned)((P.warps + kWarpsPerCta - 1) / kWarpsPerCta);
@@ -986,31 +939,28 @@ void launch_kind(bool chains, const dc_args& P, cudaStream_t st, bool whole_sm)
 }
 
 template <int VT, bool B>
-void launch_vt(int s, bool chains, const dc_args& P, cudaStream_t st, bool whole_sm)
+void launch_vt(int s, bool chains, const dc_args& P, cudaStream_t st)
 {
     switch (s) {
-    case 16: launch_kind<16, VT, B>(chains, P, st, whole_sm); break;
-    case 32: launch_kind<32, VT, B>(chains, P, st, whole_sm); break;
-    case 64: launch_kind<64, VT, B>(chains, P, st, whole_sm); break;
-    case 128: launch_kind<128, VT, B>(chains, P, st, whole_sm); break;
-    default: launch_kind<256, VT, B>(chains, P, st, whole_sm); break;
+    case 16: launch_kind<16, VT, B>(chains, P, st); break;
+    case 32: launch_kind<32, VT, B>(chains, P, st); break;
+    case 64: launch_kind<64, VT, B>(chains, P, st); break;
+    case 128: launch_kind<128, VT, B>(chains, P, st); break;
+    default: launch_kind<256, VT, B>(chains, P, st); break;
     }
 }
 
-// whole_sm (chains only): every CTA on an SM of its own.
-void launch(int s, int vt, bool batch, bool chains, const dc_args& P, cudaStream_t st, bool whole_sm = false)
+void launch(int s, int vt, bool batch, bool chains, const dc_args& P, cudaStream_t st)
 {
     if (P.warps == 0)
         return;
     if (vt == ABHSF_VALUE_F64)
-        batch ? launch_vt<ABHSF_VALUE_F64, true>(s, chains, P, st, whole_sm)
-              : launch_vt<ABHSF_VALUE_F64, false>(s, chains, P, st, whole_sm);
+        batch ? launch_vt<ABHSF_VALUE_F64, true>(s, chains, P, st) : launch_vt<ABHSF_VALUE_F64, false>(s, chains, P, st);
     else if (vt == ABHSF_VALUE_F32)
-        batch ? launch_vt<ABHSF_VALUE_F32, true>(s, chains, P, st, whole_sm)
-              : launch_vt<ABHSF_VALUE_F32, false>(s, chains, P, st, whole_sm);
+        batch ? launch_vt<ABHSF_VALUE_F32, true>(s, chains, P, st) : launch_vt<ABHSF_VALUE_F32, false>(s, chains, P, st);
     else
-        batch ? launch_vt<ABHSF_VALUE_BF16, true>(s, chains, P, st, whole_sm)
-              : launch_vt<ABHSF_VALUE_BF16, false>(s, chains, P, st, whole_sm);
+        batch ? launch_vt<ABHSF_VALUE_BF16, true>(s, chains, P, st)
+              : launch_vt<ABHSF_VALUE_BF16, false>(s, chains, P, st);
 }
 
 dc_mat mat_of(const abhsf_matrix& a) { return dc_mat{a.dc_words.get(), a.dc_vals.get(), a.dc_lane.get(), a.m}; }
@@ -1073,20 +1023,12 @@ void launch_cols(int cols, int s, int vt, bool chains, const dc_args& P, cudaStr
     }
 }
 
-// Chains on the side stream, after everything queued on st so far: the
-// critical ones first (crit; SMs of their own for a single column), then
-// the others.
+// Chains on the side stream, after everything queued on st so far.
 void fork_chains(cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, int s, int vt, bool batch,
-                 const dc_args& P, int cols = 1, const dc_args* crit = nullptr)
+                 const dc_args& P, int cols = 1)
 {
     ABHSF_CUDA(cudaEventRecord(fork, st));
     ABHSF_CUDA(cudaStreamWaitEvent(side, fork, 0));
-    if (crit && crit->warps) {
-        if (cols == 1)
-            launch(s, vt, false, true, *crit, side, true);
-        else
-            launch_cols(cols, s, vt, true, *crit, side);
-    }
     if (batch)
         launch(s, vt, batch, true, P, side);
     else
@@ -1105,22 +1047,18 @@ dc_plan plan_of(const abhsf_matrix& a)
     p.csched = a.dc_csched.get();
     p.cwbeg = a.dc_cwbeg.get();
     p.cwarps = a.dc_cwarps;
-    p.xsched = a.dc_xsched.get();
-    p.xwbeg = a.dc_xwbeg.get();
-    p.xwarps = a.dc_xwarps;
     return p;
 }
 
 void slices_begin(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
                   cudaStream_t st, int cols)
 {
-    if (p.cwarps == 0 && p.xwarps == 0)
+    if (p.cwarps == 0)
         return;
     if (!a.dc_side)
         fail(ABHSF_ERROR_CUDA, "matrix has chains but no side stream");
-    const dc_args crit = args_of(a, p.xsched, p.xwbeg, p.xwarps, x, ldx, y, ldy);
     fork_chains(st, a.dc_side, a.dc_fork, a.dc_join, a.s, a.value_type, false,
-                args_of(a, p.csched, p.cwbeg, p.cwarps, x, ldx, y, ldy), cols, &crit);
+                args_of(a, p.csched, p.cwbeg, p.cwarps, x, ldx, y, ldy), cols);
 }
 
 void slices_end(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
@@ -1128,7 +1066,7 @@ void slices_end(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t 
 {
     if (p.warps)
         launch_cols(cols, a.s, a.value_type, false, args_of(a, p.sched, p.wbeg, p.warps, x, ldx, y, ldy), st);
-    if (p.cwarps || p.xwarps)
+    if (p.cwarps)
         ABHSF_CUDA(cudaStreamWaitEvent(st, a.dc_join, 0));
 }
 

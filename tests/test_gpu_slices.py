@@ -196,11 +196,11 @@ def test_slice_host_pipeline(gpu):
     np.testing.assert_array_equal(y, ref)
 
 
-def test_critical_chains_on_their_own_sms(gpu):
-    """Rows of 40,000 and 25,000 elements (critical: at least 16,384 elements
-    and half the longest, summed on SMs of their own, first on the side
-    stream), one of 9,000 (a chain beside the others) and a hypersparse rest:
-    FP64 SpMV, f32 SpMV and SpMM bitwise in the reference order."""
+def test_long_chains(gpu):
+    """Rows of 40,000, 25,000 and 9,000 elements (chains: many full groups of
+    256 products through the shared buffer, and a partial last group) over a
+    hypersparse rest: FP64 SpMV (twice, from the same y), f32 SpMV and SpMM
+    bitwise in the reference order."""
     import torch
     coo = heavy_rows(n=120000, heavy=(3, 777), per_heavy=40000, sparse=150000, seed=8)
     rng = np.random.default_rng(9)
@@ -214,8 +214,10 @@ def test_critical_chains_on_their_own_sms(gpu):
     A = AbhsfMatrix.from_elements(rows, cols, vals, coo.n, coo.n, block_size=64)
     sl = A.slices()
     lens = sl["steps"][sl["chain"] == 1]
-    assert sorted(lens[lens >= 16384].tolist()) == [25000, 40000] and (lens == 9000).sum() == 1
-    assert A.kernels() == 3  # sliced rows, chains, critical chains
+    big = sorted(lens[lens >= 16384].tolist())  # the rest adds a few elements to some heavy rows
+    assert len(big) == 2 and 25000 <= big[0] < 25100 and 40000 <= big[1] < 40100
+    assert ((lens >= 9000) & (lens < 9100)).sum() == 1
+    assert A.kernels() == 2  # sliced rows, chains
     x = rng.uniform(-1, 1, coo.n)
     y0 = rng.standard_normal(coo.n)
     for _ in range(2):
