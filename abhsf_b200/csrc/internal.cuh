@@ -92,6 +92,10 @@ void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys
 // slices_end adds the sliced rows on st and joins the chains back (x[i * ldx],
 // y[i * ldy]).  The caller holds dc_mu across the pair.
 void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st);
+// Parts of a matrix's block rows the host-memory SpMV (abhsf_spmv_host)
+// copies in, sums and copies out one after another: [M c / kHostChunks,
+// M (c + 1) / kHostChunks).
+constexpr int kHostChunks = 4;
 enum deal_kind {
     kDealSliced = 0,  // the sliced rows
     kDealChains = 1,  // the chains

@@ -1587,7 +1587,7 @@ bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t
 
 bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
 {
-    constexpr int kChunks = 4;
+    constexpr int kChunks = kHostChunks;
     if (!a.ring_ready || a.value_type != ABHSF_VALUE_F64 || a.sum_order != ABHSF_SUM_REFERENCE ||
         a.M < 4 * kChunks || a.m < (int64_t(1) << 20))
         return false;  // small matrices: one copy each way is as fast

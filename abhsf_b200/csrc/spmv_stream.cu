@@ -9,12 +9,14 @@
 // by row, columns ascending, each column stored as the difference to the
 // previous one), laid out for a warp:
 //
-// * A block row's non-empty rows are ordered by length (longest first) and
-//   dealt to slices of up to 32 rows, one row per lane.  A slice stores its
-//   rows' elements column-major -- element k of lane l at slot base + 32 k + l
-//   -- as one 32-bit word each, the column minus the row's previous column
-//   (the first one absolute), and a copy of the value.  A lane record
-//   (row << 24 | length) says which row a lane sums.
+// * The non-empty rows of a range of block rows (slice_segments) are ordered
+//   by length (longest first, then ascending row) and dealt to slices of up
+//   to 32 rows, one row per lane, so that a slice's rows end together.  A
+//   slice stores its rows' elements column-major -- element k of lane l at
+//   slot base + 32 k + l -- as one 32-bit word each, the column minus the
+//   row's previous column (the first one absolute), and a copy of the value.
+//   A lane record (offset << 8 | length - 1, the offset from the range's
+//   first row) says which row a lane sums.
 // * A row longer than kChainMin is a slice of its own (a chain): its elements
 //   stored in order, each word the absolute column.
 //
@@ -55,8 +57,10 @@ constexpr int kChainGridPerSm = 1;  // chain CTAs per SM in the grid: the rest o
 constexpr int kChainAhead = 8;    // chain: steps of 32 products in flight ahead of the sums
 constexpr uint32_t kChain = 1u;   // dc_slice::geo: a one-row chain
 constexpr int kMidShift = 20;     // dc_slice::geo: matrix index of a batch
-constexpr uint32_t kLenMask = (1u << 24) - 1u;
+constexpr int kLenBits = 8;       // lane record: row offset << kLenBits | (length - 1)
+constexpr uint32_t kLenMask = (1u << kLenBits) - 1u;
 constexpr int kChainMin = 256;   // rows longer than this are summed alone, as a chain
+static_assert(kChainMin <= (1 << kLenBits), "a sliced row's length - 1 fits the lane record");
 constexpr int kRingTilesMax = 256;  // block rows of more tiles go to the slices whatever their density
 
 // What the kernel needs of one slice (32 bytes, in schedule order).
@@ -224,8 +228,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmv_slices(dc_args P)
         const uint32_t* W = M.words + sl.base + lane;
         const V* Vv = static_cast<const V*>(M.vals) + sl.base + lane;
         // one row per lane, element k of the lane's row at slot 32 k + lane
-        const int len = (int)(rec & kLenMask);
-        const int64_t row = (int64_t)sl.brow * S + (int64_t)(rec >> 24);
+        const int len = lane < (int)sl.lanes ? (int)(rec & kLenMask) + 1 : 0;
+        const int64_t row = (int64_t)sl.brow * S + (int64_t)(rec >> kLenBits);
         T acc = len ? Y[row * ldy] : T(0);
         uint32_t col = 0;
         uint32_t w[U];
@@ -377,13 +381,15 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmm_slices(dc_args P, in
         const uint32_t* W = P.A.words + sl.base;
         const double* Vv = static_cast<const double*>(P.A.vals) + sl.base;
         const uint32_t rec = lane < (int)sl.lanes ? P.A.lane[sl.meta + lane] : 0u;
-        const int len = (int)(rec & kLenMask);
+        const int len = lane < (int)sl.lanes ? (int)(rec & kLenMask) + 1 : 0;
+        const uint32_t off = rec >> kLenBits;  // lane r: row r's offset from the slice's first row
         const int64_t row0 = (int64_t)sl.brow * S;
         double acc[K];
 #pragma unroll
         for (int i = 0; i < K; ++i) {
-            const uint32_t ri = __shfl_sync(0xffffffffu, rec, g + G * i);
-            acc[i] = (ri & kLenMask) ? Y[(row0 + (ri >> 24)) * P.ldy] : 0.0;
+            const int r = g + G * i;
+            const uint32_t oi = __shfl_sync(0xffffffffu, off, r);
+            acc[i] = r < (int)sl.lanes ? Y[(row0 + oi) * P.ldy] : 0.0;
         }
         uint32_t col = 0;  // lane r: row r's column
 #pragma unroll 1
@@ -411,9 +417,10 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmm_slices(dc_args P, in
         }
 #pragma unroll
         for (int i = 0; i < K; ++i) {
-            const uint32_t ri = __shfl_sync(0xffffffffu, rec, g + G * i);
-            if (ri & kLenMask)
-                Y[(row0 + (ri >> 24)) * P.ldy] = acc[i];
+            const int r = g + G * i;
+            const uint32_t oi = __shfl_sync(0xffffffffu, off, r);
+            if (r < (int)sl.lanes)
+                Y[(row0 + oi) * P.ldy] = acc[i];
         }
     }
 }
@@ -721,6 +728,24 @@ void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sc
     warps_out = W;
 }
 
+// Block-row boundaries of the ranges whose sliced rows may share a slice:
+// the kHostChunks parts the host-memory SpMV copies and sums one after
+// another (a part's slices must not reach into the next), each cut into
+// pieces of at most 2^24 rows (the row offset a lane record holds).
+std::vector<int64_t> slice_segments(int64_t M, int s)
+{
+    const int64_t piece = std::max<int64_t>(1, (int64_t(1) << (32 - kLenBits)) / s);
+    std::vector<int64_t> b{0};
+    for (int c = 1; c <= kHostChunks; ++c) {
+        const int64_t e = M * c / kHostChunks;
+        while (e - b.back() > piece)
+            b.push_back(b.back() + piece);
+        if (e > b.back())
+            b.push_back(e);
+    }
+    return b;
+}
+
 // The slices of a prepared matrix: which non-empty block rows they serve
 // (dc_tree_flag, by tree-row position), their words, values and lane
 // records, and the matrix's own schedule.  avg <= 0 leaves every block row
@@ -776,9 +801,11 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
     std::vector<unsigned int> ch(ns * s);
     ABHSF_CUDA(cudaMemcpyAsync(ch.data(), cnt.get(), ns * s * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
     ABHSF_CUDA(cudaStreamSynchronize(st));
-    // slices: per block row, the non-empty rows by length (longest first,
-    // then ascending row); a row longer than kChainMin alone, the rest in
-    // groups of 32
+    // chains: per block row, its rows longer than kChainMin, longest first
+    // (then ascending row).  Sliced rows: per segment (slice_segments), the
+    // other non-empty rows of its block rows by length, longest first, then
+    // ascending row, in groups of 32 -- rows of one length class share a
+    // slice whatever their block row, so that its lanes run out together.
     std::vector<int64_t> rstart(ns * s + 1, 0), slot0(ns * s, 0);
     std::vector<uint8_t> chain(ns * s, 0);
     for (int64_t q = 0; q < ns * s; ++q)
@@ -787,42 +814,53 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
     auto& SL = a.dc_host;
     int64_t slots = 0;
     std::vector<int> order(s);
-    for (int64_t k = 0; k < ns; ++k) {
-        const unsigned int* c = ch.data() + k * s;
-        int live = 0;
-        for (int r = 0; r < s; ++r)
-            if (c[r])
-                order[live++] = r;
-        std::stable_sort(order.begin(), order.begin() + live, [&](int p, int q) { return c[p] > c[q]; });
-        int i = 0;
-        while (i < live && c[order[i]] > (unsigned int)kChainMin) {
-            abhsf_matrix::dc_slice_host h;
-            h.base = slots;
-            h.meta = order[i];
-            h.brow = sel[k].first;
-            h.steps = c[order[i]];
-            h.lanes = 1;
-            h.chain = true;
-            slot0[k * s + order[i]] = slots;
-            chain[k * s + order[i]] = 1;
-            slots += c[order[i]];
-            SL.push_back(h);
-            ++i;
+    std::vector<int64_t> rest;  // sliced rows of a segment: k s + r
+    const std::vector<int64_t> seg = slice_segments(a.M, s);
+    int64_t k = 0;
+    for (size_t g = 0; g + 1 < seg.size(); ++g) {
+        const int64_t b0 = seg[g], b1 = seg[g + 1];
+        rest.clear();
+        for (; k < ns && (int64_t)sel[k].first < b1; ++k) {
+            const unsigned int* c = ch.data() + k * s;
+            int live = 0;
+            for (int r = 0; r < s; ++r)
+                if (c[r])
+                    order[live++] = r;
+            std::stable_sort(order.begin(), order.begin() + live, [&](int p, int q) { return c[p] > c[q]; });
+            int i = 0;
+            for (; i < live && c[order[i]] > (unsigned int)kChainMin; ++i) {
+                abhsf_matrix::dc_slice_host h;
+                h.base = slots;
+                h.meta = order[i];
+                h.brow = sel[k].first;
+                h.steps = c[order[i]];
+                h.lanes = 1;
+                h.chain = true;
+                slot0[k * s + order[i]] = slots;
+                chain[k * s + order[i]] = 1;
+                slots += c[order[i]];
+                SL.push_back(h);
+            }
+            std::sort(order.begin() + i, order.begin() + live);
+            for (; i < live; ++i)
+                rest.push_back(k * s + order[i]);
         }
-        for (; i < live; i += 32) {
-            const int n32 = std::min(32, live - i);
+        std::stable_sort(rest.begin(), rest.end(), [&](int64_t p, int64_t q) { return ch[p] > ch[q]; });
+        for (size_t i = 0; i < rest.size(); i += 32) {
+            const int n32 = (int)std::min<size_t>(32, rest.size() - i);
             abhsf_matrix::dc_slice_host h;
             h.base = slots;
             h.meta = (int64_t)lane_rec.size();
-            h.brow = sel[k].first;
-            h.steps = c[order[i]];
+            h.brow = (uint32_t)b0;
+            h.steps = ch[rest[i]];
             h.lanes = n32;
             h.chain = false;
             for (int l = 0; l < 32; ++l) {
                 if (l < n32) {
-                    const int r = order[i + l];
-                    lane_rec.push_back((uint32_t)r << 24 | c[r]);
-                    slot0[k * s + r] = slots + l;
+                    const int64_t q = rest[i + l];
+                    const int64_t off = (int64_t)sel[q / s].first * s + q % s - b0 * s;
+                    lane_rec.push_back((uint32_t)off << kLenBits | (ch[q] - 1u));
+                    slot0[q] = slots + l;
                 } else {
                     lane_rec.push_back(0u);
                 }

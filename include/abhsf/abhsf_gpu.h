@@ -362,20 +362,26 @@ ABHSF_API abhsf_status abhsf_block_histogram_noalloc(const int64_t* rows, const 
  * slots (words and values, padding included), lane records, elements and
  * block rows.  The encoding follows the reference's delta COO
  * (spmv/orig/delta.cpp:118-219, spmv/unified/spmv.cpp:815-1032: row by row,
- * each column the difference to the row's previous one).  Per block row, the
- * non-empty rows ordered by length (longest first, then ascending row): a row
- * of more than 256 elements is a chain slice (its elements at slots
- * base .. base + length - 1, each word the absolute column); the others go to
- * slices of up to 32 rows, one per lane, element k of lane l at slot
- * base + 32 k + l, each word the column minus the row's previous column (the
- * first absolute), lane record l = row << 24 | length at meta + l (0 past
- * the slice's rows), steps = the longest row's length.  Values: a copy in
- * slot order; padding slots hold 0. */
+ * each column the difference to the row's previous one).  The block rows go
+ * in segments: the quarters [M c / 4, M (c + 1) / 4) that abhsf_spmv_host
+ * works through one after another, each cut into pieces of at most 2^24 rows.
+ * Per segment, first, block row by block row, every row of more than 256
+ * elements as a chain slice (longest first, then ascending row; brow = its
+ * block row, meta = the row within it, its elements at slots
+ * base .. base + length - 1, each word the absolute column); then the
+ * segment's other non-empty rows, ordered by length (longest first, then
+ * ascending row), in slices of up to 32 rows, one per lane: brow = the
+ * segment's first block row, element k of lane l at slot base + 32 k + l,
+ * each word the column minus the row's previous column (the first absolute),
+ * lane record l = (row - brow s) << 8 | (length - 1) at meta + l (0 past the
+ * slice's rows), steps = the longest row's length.  Values: a copy in slot
+ * order; padding slots hold 0. */
 ABHSF_API abhsf_status abhsf_slices_info(const abhsf_matrix* a, int64_t* slices, int64_t* slots,
                                          int64_t* lane_records, int64_t* elements, int64_t* block_rows);
 
 /* The slices into host arrays (any may be NULL), in slice order: base, meta
- * (the first lane record, or a chain's row within its block row), block row,
+ * (the first lane record, or a chain's row within its block row), block row
+ * (a chain's own; a sliced slice's segment's first),
  * steps, lanes, chain flag; the lane records; the words and values of every
  * slot.  No counterpart in the reference (its delta COO lives in host
  * memory). */

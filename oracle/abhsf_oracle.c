@@ -608,12 +608,16 @@ void orc_abs_spmv_elements(const int64_t* rows, const int64_t* cols, const doubl
  * library's SpMV reads for those block rows, restated element by element.
  * The reference's delta COO (spmv/orig/delta.cpp:118-219,
  * spmv/unified/spmv.cpp:815-1032) keeps the elements row by row and each
- * column as the difference to the previous one; here a block row's rows go
- * to slices of up to 32 (one per lane, stored column-major), a row of more
- * than ORC_CHAIN_MIN elements alone as a chain with absolute columns.
+ * column as the difference to the previous one; here a row of more than
+ * ORC_CHAIN_MIN elements is a chain with absolute columns, and the other
+ * rows of a segment of block rows go to slices of up to 32 (one per lane,
+ * stored column-major) by length.  Segments: the ORC_HOST_CHUNKS parts
+ * [M c / 4, M (c + 1) / 4), each cut into pieces of at most 2^24 rows.
  * ------------------------------------------------------------------------ */
 #define ORC_CHAIN_MIN 256
 #define ORC_RING_TILES_MAX 256
+#define ORC_HOST_CHUNKS 4
+#define ORC_LEN_BITS 8
 
 /* Elements of tile t in the format's order: local row / column of each. */
 static int64_t tile_elements(const orc_matrix* a, int64_t t, int* lr, int* lc)
@@ -689,6 +693,35 @@ static int rows_by_length(int s, const int64_t* len, int* order)
     return live;
 }
 
+/* ascending (length desc, index asc) over rows q of the segment, lengths in g_seg_len */
+static const int64_t* g_seg_len;
+static int seg_by_length(const void* p, const void* q)
+{
+    const int64_t a = *(const int64_t*)p, b = *(const int64_t*)q;
+    if (g_seg_len[a] != g_seg_len[b])
+        return g_seg_len[a] > g_seg_len[b] ? -1 : 1;
+    return a < b ? -1 : a > b;
+}
+
+/* Segment boundaries (block rows): nb + 1 values in b (room for M + 5). */
+static int64_t slice_segments(int64_t M, int s, int64_t* b)
+{
+    int64_t piece = ((int64_t)1 << (32 - ORC_LEN_BITS)) / s, nb = 0;
+    if (piece < 1)
+        piece = 1;
+    b[0] = 0;
+    for (int c = 1; c <= ORC_HOST_CHUNKS; ++c) {
+        const int64_t e = M * c / ORC_HOST_CHUNKS;
+        while (e - b[nb] > piece) {
+            b[nb + 1] = b[nb] + piece;
+            ++nb;
+        }
+        if (e > b[nb])
+            b[++nb] = e;
+    }
+    return nb;
+}
+
 int orc_slices_build(const orc_matrix* a, double avg, orc_slices** out)
 {
     *out = (orc_slices*)calloc(1, sizeof(orc_slices));
@@ -700,9 +733,10 @@ int orc_slices_build(const orc_matrix* a, double avg, orc_slices** out)
         return ORC_OK;
     /* the block rows: non-empty, no dense tile, and no bitmap tile, at most
      * avg elements per tile on average or more than ORC_RING_TILES_MAX tiles */
-    uint8_t* sel = (uint8_t*)calloc((size_t)a->M + 1, 1);
+    int64_t* sidx = (int64_t*)malloc(((size_t)a->M + 1) * sizeof(int64_t));
     int64_t E = 0, ns = 0;
     for (int64_t I = 0; I < a->M; ++I) {
+        sidx[I] = -1;
         const int64_t t0 = a->brow_ptr[I], t1 = a->brow_ptr[I + 1];
         if (t1 == t0)
             continue;
@@ -713,105 +747,118 @@ int orc_slices_build(const orc_matrix* a, double avg, orc_slices** out)
         }
         const int64_t e = a->tile_val_off[t1] - a->tile_val_off[t0];
         if (ok && ((double)e <= avg * (double)(t1 - t0) || t1 - t0 > ORC_RING_TILES_MAX || !bitmap)) {
-            sel[I] = 1;
+            sidx[I] = ns++;
             E += e;
-            ++ns;
         }
     }
     if (ns == 0 || E == 0 || E >= ((int64_t)1 << 31) || ns * (int64_t)s >= ((int64_t)1 << 32)) {
-        free(sel);
+        free(sidx);
         return ORC_OK;
     }
     int* lr = (int*)malloc((size_t)s * s * sizeof(int));
     int* lc = (int*)malloc((size_t)s * s * sizeof(int));
-    int64_t* len = (int64_t*)malloc(s * sizeof(int64_t));
     int* order = (int*)malloc(s * sizeof(int));
-    /* pass 1: count slices, slots and lane records */
-    int64_t nsl = 0, slots = 0, nlr = 0;
-    for (int64_t I = 0; I < a->M; ++I) {
-        if (!sel[I])
-            continue;
-        row_lengths(a, I, lr, lc, len);
-        const int live = rows_by_length(s, len, order);
-        int i = 0;
-        for (; i < live && len[order[i]] > ORC_CHAIN_MIN; ++i) {
-            ++nsl;
-            slots += len[order[i]];
+    int64_t* len = (int64_t*)calloc((size_t)ns * s, sizeof(int64_t)); /* row q = k s + r */
+    int64_t* browk = (int64_t*)malloc(ns * sizeof(int64_t));          /* block row of slice row k */
+    for (int64_t I = 0; I < a->M; ++I)
+        if (sidx[I] >= 0) {
+            browk[sidx[I]] = I;
+            row_lengths(a, I, lr, lc, len + sidx[I] * s);
         }
-        for (; i < live; i += 32) {
-            ++nsl;
-            nlr += 32;
-            slots += 32 * len[order[i]];
+    int64_t* seg = (int64_t*)malloc(((size_t)a->M + 8) * sizeof(int64_t));
+    const int64_t nseg = slice_segments(a->M, s, seg);
+    int64_t* rest = (int64_t*)malloc(((size_t)ns * s + 1) * sizeof(int64_t));
+    int64_t* slot0 = (int64_t*)malloc(((size_t)ns * s + 1) * sizeof(int64_t));
+    uint8_t* chain = (uint8_t*)calloc((size_t)ns * s + 1, 1);
+    /* the slices (two passes: count, then fill) */
+    for (int pass = 0; pass < 2; ++pass) {
+        int64_t nsl = 0, slots = 0, nlr = 0, k = 0;
+        for (int64_t g = 0; g < nseg; ++g) {
+            int64_t nrest = 0;
+            for (; k < ns && browk[k] < seg[g + 1]; ++k) {
+                const int live = rows_by_length(s, len + k * s, order);
+                int i = 0;
+                for (; i < live && len[k * s + order[i]] > ORC_CHAIN_MIN; ++i) {
+                    const int64_t q = k * s + order[i];
+                    if (pass) {
+                        P->base[nsl] = slots;
+                        P->meta[nsl] = order[i];
+                        P->brow[nsl] = (uint32_t)browk[k];
+                        P->steps[nsl] = (uint32_t)len[q];
+                        P->lanes[nsl] = 1;
+                        P->chain[nsl] = 1;
+                        slot0[q] = slots;
+                        chain[q] = 1;
+                    }
+                    ++nsl;
+                    slots += len[q];
+                }
+                for (int r = 0; r < s; ++r) /* the others, ascending row */
+                    if (len[k * s + r] && len[k * s + r] <= ORC_CHAIN_MIN)
+                        rest[nrest++] = k * s + r;
+            }
+            g_seg_len = len;
+            qsort(rest, (size_t)nrest, sizeof(int64_t), seg_by_length);
+            for (int64_t i = 0; i < nrest; i += 32) {
+                const int n32 = nrest - i < 32 ? (int)(nrest - i) : 32;
+                if (pass) {
+                    P->base[nsl] = slots;
+                    P->meta[nsl] = nlr;
+                    P->brow[nsl] = (uint32_t)seg[g];
+                    P->steps[nsl] = (uint32_t)len[rest[i]];
+                    P->lanes[nsl] = (uint32_t)n32;
+                    P->chain[nsl] = 0;
+                    for (int l = 0; l < n32; ++l) {
+                        const int64_t q = rest[i + l];
+                        const int64_t off = browk[q / s] * s + q % s - seg[g] * s;
+                        P->lane[nlr + l] = (uint32_t)off << ORC_LEN_BITS | (uint32_t)(len[q] - 1);
+                        slot0[q] = slots + l;
+                    }
+                }
+                ++nsl;
+                nlr += 32;
+                slots += 32 * len[rest[i]];
+            }
+        }
+        if (!pass) {
+            P->base = (int64_t*)malloc((nsl + 1) * sizeof(int64_t));
+            P->meta = (int64_t*)malloc((nsl + 1) * sizeof(int64_t));
+            P->brow = (uint32_t*)malloc((nsl + 1) * sizeof(uint32_t));
+            P->steps = (uint32_t*)malloc((nsl + 1) * sizeof(uint32_t));
+            P->lanes = (uint32_t*)malloc((nsl + 1) * sizeof(uint32_t));
+            P->chain = (uint8_t*)malloc(nsl + 1);
+            P->lane = (uint32_t*)calloc(nlr + 1, sizeof(uint32_t));
+            P->words = (uint32_t*)calloc(slots + 1, sizeof(uint32_t));
+            P->vidx = (int64_t*)malloc((slots + 1) * sizeof(int64_t));
+            for (int64_t q = 0; q < slots; ++q)
+                P->vidx[q] = -1;
+        } else {
+            P->n = nsl;
+            P->slots = slots;
+            P->lane_records = nlr;
         }
     }
-    P->base = (int64_t*)malloc((nsl + 1) * sizeof(int64_t));
-    P->meta = (int64_t*)malloc((nsl + 1) * sizeof(int64_t));
-    P->brow = (uint32_t*)malloc((nsl + 1) * sizeof(uint32_t));
-    P->steps = (uint32_t*)malloc((nsl + 1) * sizeof(uint32_t));
-    P->lanes = (uint32_t*)malloc((nsl + 1) * sizeof(uint32_t));
-    P->chain = (uint8_t*)malloc(nsl + 1);
-    P->lane = (uint32_t*)calloc(nlr + 1, sizeof(uint32_t));
-    P->words = (uint32_t*)calloc(slots + 1, sizeof(uint32_t));
-    P->vidx = (int64_t*)malloc((slots + 1) * sizeof(int64_t));
-    int64_t* slot0 = (int64_t*)malloc(s * sizeof(int64_t));
+    /* every element at its slot: the k-th element of row q (format order
+     * keeps a row's columns ascending) at slot0[q] + k (chain) or
+     * slot0[q] + 32 k (sliced) */
     int64_t* fill = (int64_t*)malloc(s * sizeof(int64_t));
     int64_t* prev = (int64_t*)malloc(s * sizeof(int64_t));
-    uint8_t* chain = (uint8_t*)malloc(s);
-    for (int64_t q = 0; q < slots; ++q)
-        P->vidx[q] = -1;
-    /* pass 2: the slices, then every element at its slot */
-    for (int64_t I = 0; I < a->M; ++I) {
-        if (!sel[I])
-            continue;
-        row_lengths(a, I, lr, lc, len);
-        const int live = rows_by_length(s, len, order);
-        int i = 0;
-        for (; i < live && len[order[i]] > ORC_CHAIN_MIN; ++i) {
-            const int r = order[i];
-            P->base[P->n] = P->slots;
-            P->meta[P->n] = r;
-            P->brow[P->n] = (uint32_t)I;
-            P->steps[P->n] = (uint32_t)len[r];
-            P->lanes[P->n] = 1;
-            P->chain[P->n] = 1;
-            slot0[r] = P->slots;
-            chain[r] = 1;
-            P->slots += len[r];
-            P->n++;
-        }
-        for (; i < live; i += 32) {
-            const int n32 = live - i < 32 ? live - i : 32;
-            P->base[P->n] = P->slots;
-            P->meta[P->n] = P->lane_records;
-            P->brow[P->n] = (uint32_t)I;
-            P->steps[P->n] = (uint32_t)len[order[i]];
-            P->lanes[P->n] = (uint32_t)n32;
-            P->chain[P->n] = 0;
-            for (int l = 0; l < n32; ++l) {
-                const int r = order[i + l];
-                P->lane[P->lane_records + l] = (uint32_t)r << 24 | (uint32_t)len[r];
-                slot0[r] = P->slots + l;
-                chain[r] = 0;
-            }
-            P->lane_records += 32;
-            P->slots += 32 * len[order[i]];
-            P->n++;
-        }
+    for (int64_t k = 0; k < ns; ++k) {
+        const int64_t I = browk[k];
         for (int r = 0; r < s; ++r) {
             fill[r] = 0;
             prev[r] = 0;
         }
-        /* the k-th element of row r (format order keeps a row's columns
-         * ascending) at slot0[r] + k (chain) or slot0[r] + 32 k (sliced) */
         for (int64_t t = a->brow_ptr[I]; t < a->brow_ptr[I + 1]; ++t) {
             const int64_t z = tile_elements(a, t, lr, lc);
             const int64_t c0 = (int64_t)a->tile_col[t] * s;
             for (int64_t e = 0; e < z; ++e) {
                 const int r = lr[e];
+                const int64_t q = k * s + r;
                 const int64_t col = c0 + lc[e];
-                const int64_t k = fill[r]++;
-                const int64_t slot = slot0[r] + (chain[r] ? k : 32 * k);
-                P->words[slot] = (uint32_t)((chain[r] || k == 0) ? col : col - prev[r]);
+                const int64_t kk = fill[r]++;
+                const int64_t slot = slot0[q] + (chain[q] ? kk : 32 * kk);
+                P->words[slot] = (uint32_t)((chain[q] || kk == 0) ? col : col - prev[r]);
                 P->vidx[slot] = a->tile_val_off[t] + e;
                 prev[r] = col;
             }
@@ -819,15 +866,18 @@ int orc_slices_build(const orc_matrix* a, double avg, orc_slices** out)
     }
     P->E = E;
     P->block_rows = ns;
-    free(sel);
+    free(sidx);
     free(lr);
     free(lc);
-    free(len);
     free(order);
+    free(len);
+    free(browk);
+    free(seg);
+    free(rest);
     free(slot0);
+    free(chain);
     free(fill);
     free(prev);
-    free(chain);
     return ORC_OK;
 }
 
@@ -857,8 +907,8 @@ void orc_spmv_slices(const orc_matrix* a, const orc_slices* P, const double* x, 
         const int nl = P->chain[q] ? 1 : (int)P->lanes[q];
         for (int l = 0; l < nl; ++l) {
             const uint32_t rec = P->chain[q] ? 0 : P->lane[P->meta[q] + l];
-            const int64_t r = P->chain[q] ? P->meta[q] : (int64_t)(rec >> 24);
-            const int64_t n = P->chain[q] ? (int64_t)P->steps[q] : (int64_t)(rec & 0xffffffu);
+            const int64_t r = P->chain[q] ? P->meta[q] : (int64_t)(rec >> ORC_LEN_BITS);
+            const int64_t n = P->chain[q] ? (int64_t)P->steps[q] : (int64_t)(rec & ((1u << ORC_LEN_BITS) - 1u)) + 1;
             const int64_t row = (int64_t)P->brow[q] * s + r;
             uint64_t col = 0;
             for (int64_t k = 0; k < n; ++k) {

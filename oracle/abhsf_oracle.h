@@ -126,15 +126,19 @@ double orc_bf16_to_f64(uint16_t b);
  * library's SpMV reads for them; spmv/orig/delta.cpp:118-219 is the
  * reference's row-by-row delta COO it follows).  Block rows: non-empty, no
  * dense tile, and no bitmap tile, at most avg elements per tile on average or
- * more than 256 tiles; none when n > 2^32
- * or the elements reach 2^31.  Per block row (ascending), its non-empty rows
- * by length (longest first, then row): each row of more than 256 elements a
- * chain slice (lanes 1, meta = the row, steps = its length, its elements at
- * slots base + k with absolute columns), then the rest in slices of up to 32
- * (steps = the first row's length, lane record l = row << 24 | length at
- * lane[meta + l], element k of lane l at slot base + 32 k + l, each word the
- * column minus the row's previous column, the first absolute).  vidx: each
- * slot's index in the format's values (-1 for padding, whose word is 0). */
+ * more than 256 tiles; none when n > 2^32 or the elements reach 2^31.
+ * Segments of block rows: the quarters [M c / 4, M (c + 1) / 4), each cut
+ * into pieces of at most 2^24 rows.  Per segment: first, per block row
+ * (ascending), its rows of more than 256 elements by length (longest first,
+ * then row), each a chain slice (lanes 1, brow = its block row, meta = the
+ * row within it, steps = its length, its elements at slots base + k with
+ * absolute columns); then the segment's other non-empty rows by length
+ * (longest first, then ascending row) in slices of up to 32 (brow = the
+ * segment's first block row, steps = the first row's length, lane record
+ * l = (row - brow s) << 8 | (length - 1) at lane[meta + l], element k of lane
+ * l at slot base + 32 k + l, each word the column minus the row's previous
+ * column, the first absolute).  vidx: each slot's index in the format's
+ * values (-1 for padding, whose word is 0). */
 typedef struct orc_slices {
     int64_t n, slots, lane_records, E, block_rows;
     int64_t* base;

@@ -113,7 +113,14 @@ def test_chains_and_bitmap_tiles_are_exercised(gpu):
     e = A.export()
     bitmap_rows = {int(np.searchsorted(e["brow_ptr"], t, side="right") - 1)
                    for t in np.nonzero(e["tile_scheme"] == 2)[0]}
-    assert bitmap_rows and bitmap_rows <= set(P["brow"].tolist())
+    served = set()  # block rows the slices sum: a chain's own, a sliced lane's row's
+    for q in range(P["slices"]):
+        if P["chain"][q]:
+            served.add(int(P["brow"][q]))
+        else:
+            for l in range(int(P["lanes"][q])):
+                served.add((int(P["brow"][q]) * 64 + int(P["lane"][P["meta"][q] + l] >> 8)) // 64)
+    assert bitmap_rows and bitmap_rows <= served
 
 
 @pytest.mark.parametrize("vt", ["f32", "bf16"])
