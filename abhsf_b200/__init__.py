@@ -10,6 +10,7 @@ _EXPORTS = {
     "AbhsfError": "capi", "DuplicateEntry": "capi", "IndexOutOfRange": "capi", "InvalidValue": "capi",
     "Unsupported": "capi",
     "AbhsfMatrix": "matrix", "AbhsfBatch": "matrix", "block_histogram": "matrix", "read_mtx": "matrix",
+    "read_mtx_device": "matrix",
     "read_mm": "matrix", "write_mm": "matrix", "mtx2mm": "matrix", "expand_symmetric": "matrix", "block_histograms_all": "matrix", "block_scheme_bits": "matrix",
     "block_select_scheme": "matrix", "mmf_line": "matrix", "cg": "matrix", "cg_mixed": "matrix",
     "ShardedMatrix": "sharded",

@@ -76,6 +76,12 @@ class CooHost(C.Structure):
                 ("rows", C.POINTER(C.c_int64)), ("cols", C.POINTER(C.c_int64)), ("vals", C.POINTER(C.c_double))]
 
 
+class CooDevice(C.Structure):
+    _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("nnz", C.c_int64), ("matrix_type", C.c_int32),
+                ("symmetry", C.c_int32), ("stored_triangle", C.c_int32), ("reserved", C.c_int32),
+                ("rows", C.c_void_p), ("cols", C.c_void_p), ("vals", C.c_void_p), ("host_parsed", C.c_int64)]
+
+
 class CgInfo(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("outer_iterations", C.c_int32), ("converged", C.c_int32),
                 ("reserved", C.c_int32), ("rel_residual", C.c_double)]
@@ -142,6 +148,10 @@ PROTOTYPES = {
     "abhsf_mlp_backward": (C.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp]),
     "abhsf_mlp_adam": (C.c_int, [_vp, _vp, _vp, _vp, _i32, C.c_float, _vp]),
     "abhsf_read_mtx": (C.c_int, [C.c_char_p, _i32, C.POINTER(CooHost)]),
+    "abhsf_read_mtx_device": (C.c_int, [C.c_char_p, C.c_void_p, C.POINTER(CooDevice)]),
+    "abhsf_coo_device_free": (C.c_int, [C.POINTER(CooDevice)]),
+    "abhsf_coo_device_copy": (C.c_int, [C.POINTER(CooDevice), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "abhsf_test_parse_decimal": (_i32, [C.c_char_p, _i64, C.POINTER(C.c_double), C.POINTER(_i64)]),
     "abhsf_read_mm": (C.c_int, [C.c_char_p, C.POINTER(CooHost)]),
     "abhsf_write_mm": (C.c_int, [C.c_char_p, C.POINTER(CooHost)]),
     "abhsf_coo_host_free": (C.c_int, [C.POINTER(CooHost)]),

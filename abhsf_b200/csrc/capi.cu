@@ -527,6 +527,53 @@ abhsf_status abhsf_read_mtx(const char* path, int32_t threads, abhsf_coo_host* o
     });
 }
 
+abhsf_status abhsf_read_mtx_device(const char* path, abhsf_stream_t stream, abhsf_coo_device* out)
+{
+    const abhsf_status st = guarded([&] {
+        if (!out)
+            fail(ABHSF_ERROR_INVALID_VALUE, "out must be non-NULL");
+        abhsf::read_mtx_device(path, reinterpret_cast<cudaStream_t>(stream), *out);
+    });
+    if (st != ABHSF_SUCCESS && out) {  // nothing half-made stays behind
+        cudaFree(out->rows);
+        cudaFree(out->cols);
+        cudaFree(out->vals);
+        *out = abhsf_coo_device{};
+    }
+    return st;
+}
+
+abhsf_status abhsf_coo_device_free(abhsf_coo_device* coo)
+{
+    return guarded([&] {
+        if (!coo)
+            fail(ABHSF_ERROR_INVALID_VALUE, "coo must be non-NULL");
+        ABHSF_CUDA(cudaFree(coo->rows));
+        ABHSF_CUDA(cudaFree(coo->cols));
+        ABHSF_CUDA(cudaFree(coo->vals));
+        *coo = abhsf_coo_device{};
+    });
+}
+
+abhsf_status abhsf_coo_device_copy(const abhsf_coo_device* coo, int64_t* rows, int64_t* cols, double* vals,
+                                   abhsf_stream_t stream)
+{
+    return guarded([&] {
+        if (!coo)
+            fail(ABHSF_ERROR_INVALID_VALUE, "coo must be non-NULL");
+        const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        const size_t k = (size_t)std::max<int64_t>(coo->nnz, 0);
+        if (k == 0)
+            return;
+        if (rows)
+            ABHSF_CUDA(cudaMemcpyAsync(rows, coo->rows, k * sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
+        if (cols)
+            ABHSF_CUDA(cudaMemcpyAsync(cols, coo->cols, k * sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
+        if (vals)
+            ABHSF_CUDA(cudaMemcpyAsync(vals, coo->vals, k * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    });
+}
+
 abhsf_status abhsf_read_mm(const char* path, abhsf_coo_host* out)
 {
     return guarded([&] {

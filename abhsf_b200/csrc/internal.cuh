@@ -2,6 +2,7 @@
 #pragma once
 
 #include <map>
+#include <string>
 #include <memory>
 
 #include "common.cuh"
@@ -10,6 +11,20 @@ namespace abhsf {
 
 // Matrix Market ingest on the host (mtx.cu).
 void read_mtx(const char* path, int threads, abhsf_coo_host& out);
+std::string read_file(const char* path);
+struct mtx_header {
+    int type = 0, symmetry = 0;
+    long long m = 0, n = 0, nnz = 0;
+    size_t pos = 0;  // first byte after the size line
+};
+mtx_header read_mtx_header(const std::string& buf);
+// One entry from the text at b (leading white space, line ends included, skipped),
+// read as the host reader reads it: 0 read, 1 nothing but white space, 2 not
+// an entry.
+int parse_entry_host(const char* b, const char* e, bool pattern, unsigned long long& r, unsigned long long& c,
+                     double& v);
+// ... and on the device: the arrays in device memory (mtx_device.cu).
+void read_mtx_device(const char* path, cudaStream_t st, abhsf_coo_device& out);
 void read_mm(const char* path, abhsf_coo_host& out);
 void write_mm(const char* path, const abhsf_coo_host& a);
 

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "internal.cuh"
 
 namespace abhsf {
 namespace {
@@ -160,30 +161,33 @@ void parse_chunk(const char* b, const char* e, bool pattern, int64_t m, int64_t 
 
 }  // namespace
 
-void read_mtx(const char* path, int threads, abhsf_coo_host& out)
+std::string read_file(const char* path)
 {
-    out = abhsf_coo_host{};
     if (!path)
         fail(ABHSF_ERROR_INVALID_VALUE, "path must be non-NULL");
     FILE* f = std::fopen(path, "rb");
     if (!f)
         fail(ABHSF_ERROR_INVALID_VALUE, std::string("cannot open input file: ") + path);
     std::string buf;
-    {
-        // one read of the whole file when its size is known, else by pieces
-        long size = -1;
-        if (std::fseek(f, 0, SEEK_END) == 0)
-            size = std::ftell(f);
-        if (size >= 0 && std::fseek(f, 0, SEEK_SET) == 0) {
-            buf.resize(size_t(size));
-            buf.resize(std::fread(&buf[0], 1, buf.size(), f));
-        }
-        char tmp[1 << 16];
-        size_t k;
-        while ((k = std::fread(tmp, 1, sizeof(tmp), f)) > 0)
-            buf.append(tmp, k);
-        std::fclose(f);
+    // one read of the whole file when its size is known, else by pieces
+    long size = -1;
+    if (std::fseek(f, 0, SEEK_END) == 0)
+        size = std::ftell(f);
+    if (size >= 0 && std::fseek(f, 0, SEEK_SET) == 0) {
+        buf.resize(size_t(size));
+        buf.resize(std::fread(&buf[0], 1, buf.size(), f));
     }
+    char tmp[1 << 16];
+    size_t k;
+    while ((k = std::fread(tmp, 1, sizeof(tmp), f)) > 0)
+        buf.append(tmp, k);
+    std::fclose(f);
+    return buf;
+}
+
+mtx_header read_mtx_header(const std::string& buf)
+{
+    mtx_header h;
     size_t pos = 0;
     std::string line;
     // banner: %%MatrixMarket matrix coordinate <field> <symmetry>
@@ -196,28 +200,25 @@ void read_mtx(const char* path, int threads, abhsf_coo_host& out)
     if (lower(w[1]) != "matrix" || lower(w[2]) != "coordinate")
         fail(ABHSF_ERROR_UNSUPPORTED, "only sparse matrices in coordinate format are supported");
     const std::string field = lower(w[3]), sym = lower(w[4]);
-    int type;
     if (field == "pattern")
-        type = ABHSF_MATRIX_BINARY;
+        h.type = ABHSF_MATRIX_BINARY;
     else if (field == "real")
-        type = ABHSF_MATRIX_REAL;
+        h.type = ABHSF_MATRIX_REAL;
     else if (field == "integer" || field == "complex")
         fail(ABHSF_ERROR_UNSUPPORTED, "only real and pattern matrices are read (read_mtx_real_or_binary)");
     else
         fail(ABHSF_ERROR_INVALID_VALUE, "unsupported matrix type");
-    int symmetry;
     if (sym == "general")
-        symmetry = ABHSF_SYMMETRY_GENERAL;
+        h.symmetry = ABHSF_SYMMETRY_GENERAL;
     else if (sym == "symmetric")
-        symmetry = ABHSF_SYMMETRY_SYMMETRIC;
+        h.symmetry = ABHSF_SYMMETRY_SYMMETRIC;
     else if (sym == "skew-symmetric")
-        symmetry = ABHSF_SYMMETRY_SKEW;
+        h.symmetry = ABHSF_SYMMETRY_SKEW;
     else if (sym == "hermitian")
-        symmetry = ABHSF_SYMMETRY_HERMITIAN;
+        h.symmetry = ABHSF_SYMMETRY_HERMITIAN;
     else
         fail(ABHSF_ERROR_INVALID_VALUE, "unsupported type of matrix symmetry");
     // comments, then the size line
-    long long m = 0, n = 0, nnz = 0;
     for (;;) {
         if (!next_line(buf, pos, line))
             fail(ABHSF_ERROR_INVALID_VALUE, "could not retrieve matrix sizes");
@@ -225,13 +226,39 @@ void read_mtx(const char* path, int threads, abhsf_coo_host& out)
             continue;
         if (line.find_first_not_of(" \t") == std::string::npos)
             continue;
-        if (std::sscanf(line.c_str(), "%lld %lld %lld", &m, &n, &nnz) != 3 || m <= 0 || n <= 0 || nnz < 0)
+        if (std::sscanf(line.c_str(), "%lld %lld %lld", &h.m, &h.n, &h.nnz) != 3 || h.m <= 0 || h.n <= 0 ||
+            h.nnz < 0)
             fail(ABHSF_ERROR_INVALID_VALUE, "could not retrieve matrix sizes");
         break;
     }
-    // entry lines: split the rest at line ends over the threads (a size line
-    // without a line end leaves pos one past the buffer)
-    pos = std::min(pos, buf.size());
+    // a size line without a line end leaves pos one past the buffer
+    h.pos = std::min(pos, buf.size());
+    return h;
+}
+
+int parse_entry_host(const char* b, const char* e, bool pattern, unsigned long long& r, unsigned long long& c,
+                     double& v)
+{
+    const char* p = b;
+    while (p < e && is_space(*p))
+        ++p;
+    if (p >= e)
+        return 1;
+    v = 1.0;
+    if (!read_index(p, e, r) || !read_index(p, e, c) || (!pattern && !read_value(p, e, v)))
+        return 2;
+    return 0;
+}
+
+void read_mtx(const char* path, int threads, abhsf_coo_host& out)
+{
+    out = abhsf_coo_host{};
+    const std::string buf = read_file(path);
+    const mtx_header hd = read_mtx_header(buf);
+    const int type = hd.type, symmetry = hd.symmetry;
+    const long long m = hd.m, n = hd.n, nnz = hd.nnz;
+    const size_t pos = hd.pos;
+    // entry lines: split the rest at line ends over the threads
     const size_t rest = buf.size() - pos;
     int T = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
     T = (int)std::max<size_t>(1, std::min<size_t>((size_t)T, rest / (1 << 20) + 1));

@@ -349,6 +349,32 @@ def read_mtx(path: str, threads: int = 0):
     return _coo_result(c)
 
 
+def read_mtx_device(path: str, stream=None):
+    """read_mtx with the entry lines parsed on the GPU (abhsf_read_mtx_device):
+    (rows, cols, vals, m, n, info) as CUDA tensors (int64, int64, float64),
+    the elements read_mtx returns, in the same order; info also says how many
+    entries the host parsed ("host_parsed": spellings the device leaves to
+    it)."""
+    c = capi.CooDevice()
+    capi.check(capi.lib.abhsf_read_mtx_device(os.fsencode(path), _stream_ptr(stream), C.byref(c)))
+    try:
+        k = int(c.nnz)
+        rows = torch.empty(k, dtype=torch.int64, device="cuda")
+        cols = torch.empty(k, dtype=torch.int64, device="cuda")
+        vals = torch.empty(k, dtype=torch.float64, device="cuda")
+        if k:
+            capi.check(capi.lib.abhsf_coo_device_copy(C.byref(c), rows.data_ptr(), cols.data_ptr(), vals.data_ptr(),
+                                                       _stream_ptr(stream)))
+            torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+        info = {"matrix_type": {0: "binary", 2: "real"}[int(c.matrix_type)],
+                "symmetry": _SYMMETRIES[int(c.symmetry)],
+                "stored_triangle": ("", "lower", "upper")[int(c.stored_triangle)],
+                "host_parsed": int(c.host_parsed)}
+        return rows, cols, vals, int(c.m), int(c.n), info
+    finally:
+        capi.lib.abhsf_coo_device_free(C.byref(c))
+
+
 def expand_symmetric(rows, cols, vals, symmetry: str):
     """The whole matrix from the stored triangle of a symmetric, skew or
     hermitian (real) file, as read_mtx returns it: every off-diagonal element

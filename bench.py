@@ -312,8 +312,8 @@ def time_batched(dev, l2_flush, warmup, count=256, steps=10):
 def time_cg(dev, g=256, rtol=1e-10):
     """CG solve time on the 3D 7-point Laplacian g^3 (n = g^3, SPD, b U[-1,1]
     seed 1, x0 = 0) to ||b - A x|| <= rtol ||b||: the plain form (FP64 CG,
-    block size 64) against the tuned form: the block size the learned selector
-    picks, and mixed precision -- f32 CG on an f32 or a bf16 copy, the
+    block size 64) against the tuned form: the block size the selector trained
+    on measured SpMV time picks, and mixed precision -- f32 CG on an f32 or a bf16 copy, the
     solution, the residual replacement and the convergence test in FP64 --
     with every 8 iterations replayed as one CUDA graph.  (6 and -1 are exact
     in bf16, so the bf16 copy is the matrix itself.)"""
@@ -325,8 +325,10 @@ def time_cg(dev, g=256, rtol=1e-10):
     rows_d = torch.from_numpy(lap.rows).to(dev)
     cols_d = torch.from_numpy(lap.cols).to(dev)
     t0 = time.perf_counter()
-    s_learned = sel.predict(sel.features(rows_d, cols_d, lap.m, lap.n))
+    feats = sel.features(rows_d, cols_d, lap.m, lap.n)
+    s_learned = sel.predict(feats, model=sel.builtin_time_model())  # trained on measured SpMV time
     t_select = time.perf_counter() - t0
+    s_storage = sel.predict(feats)  # the storage-trained model's choice, for the record
     del rows_d, cols_d
     A64 = AbhsfMatrix.from_elements(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=64)
     L64 = AbhsfMatrix.from_elements(lap.rows, lap.cols, lap.vals, lap.m, lap.n, block_size=s_learned)
@@ -336,7 +338,8 @@ def time_cg(dev, g=256, rtol=1e-10):
                                     value_type="bf16")
     b = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, lap.n)).to(dev)
     out = {"workload": f"3D 7-point Laplacian {g}^3 (n={lap.n}, nnz={lap.nnz}, diag 6, off -1), b U[-1,1] seed 1, "
-                       f"x0 = 0", "rtol": rtol, "learned_block_size": s_learned, "select_s": t_select}
+                       f"x0 = 0", "rtol": rtol, "learned_block_size": s_learned, "select_s": t_select,
+           "selector": "learned_time (MLP trained on measured SpMV time)", "storage_model_block_size": s_storage}
     # each solver's SpMV alone (working set > L2; CUDA events, 10 launches after 3)
     peak, _ = hbm_peak()
     for key, M, dt in (("spmv_f64", A64, torch.float64), ("spmv_f32_copy", L32, torch.float32),
@@ -375,8 +378,8 @@ def time_cg(dev, g=256, rtol=1e-10):
         out[name] = dict(info, seconds=min(runs), runs_s=runs)
     out["clocks"] = clocks.stop()
     out["plain"]["solver"] = "FP64 CG, block size 64, reference-order f64 SpMV"
-    out["tuned_f32"]["solver"] = (f"learned block size {s_learned}: f32 CG on an f32 copy, FP64 solution, FP64 "
-                                  "residual replacement each 10x drop")
+    out["tuned_f32"]["solver"] = (f"block size {s_learned} (time-trained selector): f32 CG on an f32 copy, FP64 "
+                                  "solution, FP64 residual replacement each 10x drop")
     out["tuned_bf16"]["solver"] = out["tuned_f32"]["solver"].replace("an f32 copy", "a bf16 copy")
     out["tuned_f32_speedup"] = out["plain"]["seconds"] / out["tuned_f32"]["seconds"]
     out["tuned_bf16_speedup"] = out["plain"]["seconds"] / out["tuned_bf16"]["seconds"]
@@ -698,6 +701,23 @@ def ingest_run(c, max_entries: int = 3_000_000):
             ours.append(time.perf_counter() - t0)
         out = {"entries": k, "file_bytes": size, "unit": "MB/s",
                "abhsf_read_mtx": {"MB/s": size / min(ours) / 1e6, "s": min(ours), "threads": os.cpu_count()}}
+        try:  # the parse on the GPU: file read, copy, line scan, parse, checks, compaction
+            import torch
+            dev = []
+            for _ in range(3):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                gd = mx.read_mtx_device(p)
+                torch.cuda.synchronize()
+                dev.append(time.perf_counter() - t0)
+            same_d = (gd[0].numel() == got[0].size and np.array_equal(gd[0].cpu().numpy(), got[0])
+                      and np.array_equal(gd[1].cpu().numpy(), got[1])
+                      and np.array_equal(gd[2].cpu().numpy().view(np.uint64), got[2].view(np.uint64)))
+            out["abhsf_read_mtx_device"] = {"MB/s": size / min(dev[1:]) / 1e6, "s": min(dev[1:]),
+                                            "host_parsed": gd[5]["host_parsed"], "same_elements": bool(same_d)}
+            del gd
+        except Exception as exc:  # noqa: BLE001 -- reported, not fatal to the bench
+            out["abhsf_read_mtx_device"] = {"error": str(exc)[:200]}
         lib = os.path.join(ROOT, "oracle", "_ref", "libref_mtx.so")
         if os.path.exists(lib):
             f_ = C.CDLL(lib).ref_mtx_read

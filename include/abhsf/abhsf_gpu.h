@@ -170,6 +170,23 @@ typedef struct abhsf_coo_host {
     double* vals;
 } abhsf_coo_host;
 
+/* A matrix read from a file into device memory (abhsf_read_mtx_device): the
+ * fields of abhsf_coo_host, with rows, cols and vals in device memory
+ * (allocated by the library on the current device, freed by
+ * abhsf_coo_device_free), and how many entries the host parsed instead of the
+ * device (spellings other than plain decimal numbers). */
+typedef struct abhsf_coo_device {
+    int64_t m, n, nnz;
+    int32_t matrix_type;
+    int32_t symmetry;
+    int32_t stored_triangle;
+    int32_t reserved;
+    int64_t* rows;
+    int64_t* cols;
+    double* vals;
+    int64_t host_parsed;
+} abhsf_coo_device;
+
 typedef struct abhsf_matrix abhsf_matrix;
 typedef struct abhsf_batch abhsf_batch;
 
@@ -488,6 +505,24 @@ ABHSF_API abhsf_status abhsf_mlp_adam(float* params, const float* grad, float* m
  * abhsf_build as they are. */
 ABHSF_API abhsf_status abhsf_read_mtx(const char* path, int32_t threads, abhsf_coo_host* out);
 ABHSF_API abhsf_status abhsf_coo_host_free(abhsf_coo_host* coo);
+
+/* The same read with the parse on the GPU: the file is read into host memory
+ * and copied to the device, where one thread per line reads the entry (line
+ * ends found by a scan), rounds its value to the nearest double exactly as
+ * strtod does (a 64-bit significand times a 128-bit power of five; values of
+ * more than 19 significant digits, other spellings and the rare result that
+ * product cannot decide go to the host's parser, line by line), and the
+ * checks, the zero drop and the compaction of the first nnz entries run as
+ * kernels.  The elements equal abhsf_read_mtx's, in the same order, and the
+ * errors are its errors (a file whose entries span lines is read by the
+ * host's parser).  Ordered on stream; the arrays are ready when it returns. */
+ABHSF_API abhsf_status abhsf_read_mtx_device(const char* path, abhsf_stream_t stream, abhsf_coo_device* out);
+ABHSF_API abhsf_status abhsf_coo_device_free(abhsf_coo_device* coo);
+/* Copies the arrays of coo into the caller's device arrays of nnz elements
+ * each (any may be NULL), ordered on stream: for callers whose memory comes
+ * from their own allocator. */
+ABHSF_API abhsf_status abhsf_coo_device_copy(const abhsf_coo_device* coo, int64_t* rows, int64_t* cols,
+                                             double* vals, abhsf_stream_t stream);
 
 /* The reference's binary matrix file (".mm", written by
  * utils/mtx2mm/mtx2mm.cpp:102-135): u64 m, n, nnz, type (0 pattern, 2 real),

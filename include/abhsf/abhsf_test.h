@@ -37,6 +37,13 @@ ABHSF_API abhsf_status abhsf_test_ring_variant(abhsf_matrix* a, int32_t set, int
  * nothing keeps that promise. */
 ABHSF_API int64_t abhsf_test_device_allocations(void);
 
+/* The device Matrix Market parser's decimal conversion, run on the host on
+ * the len bytes at text: 0 = converted (*value, *used bytes read), 1 = left to
+ * the host's parser (not a plain decimal, more than 19 significant digits, a
+ * result the 128-bit product cannot round, or outside the normal range).  So
+ * that tests can compare it with strtod over many numbers without a GPU. */
+ABHSF_API int32_t abhsf_test_parse_decimal(const char* text, int64_t len, double* value, int64_t* used);
+
 #ifdef __cplusplus
 }
 #endif
