@@ -24,7 +24,9 @@
 // * The first nnz entries (the non-blank lines by rank, a scan) are checked
 //   for range and triangles, and the kept ones compacted in file order.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -255,10 +257,47 @@ __device__ uint8_t read_line(const char* p, const char* e, bool pattern, const p
     return parse_decimal(p, e, T, v, end) == 0 ? kEntry : kHost;
 }
 
-__global__ void k_line_heads(int64_t R, const char* __restrict__ buf, uint8_t* __restrict__ head)
+// Line index, two passes over the bytes: kLineChunk bytes a block, kLineBytes
+// a thread.  A line starts at 0 and after every '\n' that is not the last byte.
+constexpr int kLineThreads = 256, kLineBytes = 64, kLineChunk = kLineThreads * kLineBytes;
+
+__device__ inline int line_ends(const char* buf, int64_t a, int64_t b)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
-        head[i] = (i == 0 || buf[i - 1] == '\n') ? 1 : 0;
+    int k = 0;
+    for (int64_t i = a; i < b; ++i)
+        k += buf[i] == '\n';
+    return k;
+}
+
+__global__ void __launch_bounds__(kLineThreads) k_count_lines(int64_t R, const char* __restrict__ buf,
+                                                              int64_t* __restrict__ cnt)
+{
+    using reduce = cub::BlockReduce<int, kLineThreads>;
+    __shared__ typename reduce::TempStorage tmp;
+    const int64_t a = blockIdx.x * (int64_t)kLineChunk + threadIdx.x * (int64_t)kLineBytes;
+    const int k = a < R - 1 ? line_ends(buf, a, min(a + kLineBytes, R - 1)) : 0;  // not the last byte
+    const int total = reduce(tmp).Sum(k);
+    if (threadIdx.x == 0)
+        cnt[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kLineThreads) k_write_lines(int64_t R, const char* __restrict__ buf,
+                                                              const int64_t* __restrict__ off,
+                                                              int64_t* __restrict__ start)
+{
+    using scan = cub::BlockScan<int, kLineThreads>;
+    __shared__ typename scan::TempStorage tmp;
+    const int64_t a = blockIdx.x * (int64_t)kLineChunk + threadIdx.x * (int64_t)kLineBytes;
+    const int64_t b = min(a + kLineBytes, R - 1);
+    const int k = a < R - 1 ? line_ends(buf, a, b) : 0;
+    int before = 0;
+    scan(tmp).ExclusiveSum(k, before);
+    int64_t at = 1 + off[blockIdx.x] + before;  // start[0] = 0
+    for (int64_t i = a; i < b; ++i)
+        if (buf[i] == '\n')
+            start[at++] = i + 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        start[0] = 0;
 }
 
 __global__ void k_read_lines(int64_t L, int64_t R, const char* __restrict__ buf, const int64_t* __restrict__ start,
@@ -366,16 +405,35 @@ inline unsigned grid_for(int64_t n)
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32));
 }
 
-// Indices of the set flags (cub select over a counting iterator).
-int64_t select_flagged(const uint8_t* flags, int64_t n, dbuf<int64_t>& out, cudaStream_t st)
+// Device memory from the stream-ordered allocator, freed on the stream: the
+// reader's scratch neither waits for the device to go idle nor makes it.
+template <typename T>
+class sbuf {
+  public:
+    sbuf(size_t count, cudaStream_t st) : st_(st)
+    {
+        ABHSF_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p_), std::max<size_t>(count, 1) * sizeof(T), st));
+        dbuf_allocations().fetch_add(1, std::memory_order_relaxed);
+    }
+    ~sbuf() { cudaFreeAsync(p_, st_); }
+    sbuf(const sbuf&) = delete;
+    sbuf& operator=(const sbuf&) = delete;
+    T* get() const { return p_; }
+
+  private:
+    T* p_ = nullptr;
+    cudaStream_t st_;
+};
+
+// Indices of the set flags (cub select over a counting iterator) into out (n long).
+int64_t select_flagged(const uint8_t* flags, int64_t n, int64_t* out, cudaStream_t st)
 {
-    out.alloc(std::max<int64_t>(n, 1));
-    dbuf<int64_t> count(1);
+    sbuf<int64_t> count(1, st);
     cub::CountingInputIterator<int64_t> it(0);
     size_t tb = 0;
-    ABHSF_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, flags, out.get(), count.get(), n, st));
-    dbuf<uint8_t> tmp(std::max<size_t>(tb, 1));
-    ABHSF_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tb, it, flags, out.get(), count.get(), n, st));
+    ABHSF_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, flags, out, count.get(), n, st));
+    sbuf<uint8_t> tmp(tb, st);
+    ABHSF_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tb, it, flags, out, count.get(), n, st));
     int64_t k = 0;
     ABHSF_CUDA(cudaMemcpyAsync(&k, count.get(), sizeof k, cudaMemcpyDeviceToHost, st));
     ABHSF_CUDA(cudaStreamSynchronize(st));
@@ -415,21 +473,115 @@ void host_fallback(const char* path, cudaStream_t st, abhsf_coo_device& out)
     ABHSF_CUDA(cudaStreamSynchronize(st));
 }
 
+// Pinned host staging for the file's way to the device: two chunks, so that
+// reading one overlaps the copy of the other.  Allocated once per process.
+constexpr size_t kStage = size_t(16) << 20;
+
+struct staging {
+    std::mutex mu;
+    char* p[2] = {nullptr, nullptr};
+};
+
+staging& stage()
+{
+    static staging s;
+    return s;
+}
+
+// The file into device memory d (size bytes); its first min(size, kStage)
+// bytes also into head.  false: not a regular file of that size (the caller
+// reads it the plain way).
+bool file_to_device(FILE* f, int64_t size, char* d, std::string& head, cudaStream_t st)
+{
+    staging& S = stage();
+    std::lock_guard<std::mutex> lock(S.mu);
+    for (int k = 0; k < 2; ++k)
+        if (!S.p[k])
+            ABHSF_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&S.p[k]), kStage, cudaHostAllocPortable));
+    cudaEvent_t ev[2];
+    for (auto& e : ev)
+        ABHSF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    bool ok = true;
+    int64_t off = 0;
+    for (int i = 0; off < size; ++i) {
+        const int k = i & 1;
+        if (i >= 2)
+            cudaEventSynchronize(ev[k]);  // the copy that last used this chunk is done
+        const size_t want = (size_t)std::min<int64_t>((int64_t)kStage, size - off);
+        const size_t got = std::fread(S.p[k], 1, want, f);
+        if (got != want) {
+            ok = false;
+            break;
+        }
+        if (i == 0)
+            head.assign(S.p[0], got);
+        ABHSF_CUDA(cudaMemcpyAsync(d + off, S.p[k], got, cudaMemcpyHostToDevice, st));
+        ABHSF_CUDA(cudaEventRecord(ev[k], st));
+        off += (int64_t)got;
+    }
+    ABHSF_CUDA(cudaStreamSynchronize(st));  // before the staging is reused
+    for (auto& e : ev)
+        cudaEventDestroy(e);
+    return ok;
+}
+
+// Byte copies of lines [b[j], e[j]) of the device text, packed at at[j].
+__global__ void k_pack_lines(int64_t k, const char* __restrict__ text, const int64_t* __restrict__ b,
+                             const int64_t* __restrict__ e, const int64_t* __restrict__ at, char* __restrict__ out)
+{
+    for (int64_t j = blockIdx.x; j < k; j += gridDim.x)
+        for (int64_t i = b[j] + threadIdx.x; i < e[j]; i += blockDim.x)
+            out[at[j] + (i - b[j])] = text[i];
+}
+
 }  // namespace
 
 void read_mtx_device(const char* path, cudaStream_t st, abhsf_coo_device& out)
 {
     out = abhsf_coo_device{};
-    const std::string buf = read_file(path);
-    const mtx_header hd = read_mtx_header(buf);
+    if (!path)
+        fail(ABHSF_ERROR_INVALID_VALUE, "path must be non-NULL");
+    FILE* f = std::fopen(path, "rb");
+    if (!f)
+        fail(ABHSF_ERROR_INVALID_VALUE, std::string("cannot open input file: ") + path);
+    struct closer {
+        FILE* f;
+        ~closer() { std::fclose(f); }
+    } fc{f};
+    int64_t size = -1;
+    if (std::fseek(f, 0, SEEK_END) == 0)
+        size = (int64_t)std::ftell(f);
+    if (size < 0 || std::fseek(f, 0, SEEK_SET) != 0) {
+        host_fallback(path, st, out);  // not a seekable file: the host reader
+        return;
+    }
+    sbuf<char> d_file(size, st);
+    std::string head;
+    if (!file_to_device(f, size, d_file.get(), head, st)) {
+        host_fallback(path, st, out);  // the file changed under us: the host reader reports what it finds
+        return;
+    }
+    // banner and size line: from the first chunk (the whole file when they
+    // reach past it)
+    mtx_header hd;
+    const bool whole = (int64_t)head.size() == size;
+    try {
+        hd = read_mtx_header(head);
+    } catch (...) {
+        if (whole)
+            throw;
+        hd.pos = head.size();  // comments longer than the first chunk: read below
+    }
+    if (!whole && hd.pos >= head.size())  // the size line may not have ended inside the chunk
+        hd = read_mtx_header(read_file(path));
     const bool pattern = hd.type == ABHSF_MATRIX_BINARY;
-    const int64_t R = (int64_t)(buf.size() - hd.pos);
-    const char* text = buf.data() + hd.pos;
+    const int64_t R = size - (int64_t)hd.pos;
+    const char* text = d_file.get() + hd.pos;  // device
     out.m = hd.m;
     out.n = hd.n;
     out.matrix_type = hd.type;
     out.symmetry = hd.symmetry;
-    if (hd.nnz == 0 || R == 0) {
+    if (hd.nnz == 0 || R <= 0) {
         if (hd.nnz > 0)
             fail(ABHSF_ERROR_INVALID_VALUE, "could not read matrix element (fewer entries than declared)");
         out.stored_triangle = hd.symmetry == ABHSF_SYMMETRY_GENERAL ? 0 : 2;
@@ -439,21 +591,30 @@ void read_mtx_device(const char* path, cudaStream_t st, abhsf_coo_device& out)
         return;
     }
     // the lines
-    dbuf<char> d_buf(R);
-    ABHSF_CUDA(cudaMemcpyAsync(d_buf.get(), text, R, cudaMemcpyHostToDevice, st));
-    dbuf<int64_t> start;
+    const int64_t nb = (R + kLineChunk - 1) / kLineChunk;
+    sbuf<int64_t> bcnt(nb, st), boff(nb, st);
+    k_count_lines<<<(unsigned)nb, kLineThreads, 0, st>>>(R, text, bcnt.get());
+    ABHSF_CUDA(cudaGetLastError());
     int64_t L = 0;
     {
-        dbuf<uint8_t> head(R);
-        k_line_heads<<<grid_for(R), 256, 0, st>>>(R, d_buf.get(), head.get());
-        ABHSF_CUDA(cudaGetLastError());
-        L = select_flagged(head.get(), R, start, st);
+        size_t tb = 0;
+        ABHSF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, bcnt.get(), boff.get(), nb, st));
+        sbuf<uint8_t> tmp(tb, st);
+        ABHSF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, bcnt.get(), boff.get(), nb, st));
+        int64_t lo = 0, lc = 0;
+        ABHSF_CUDA(cudaMemcpyAsync(&lo, boff.get() + nb - 1, sizeof lo, cudaMemcpyDeviceToHost, st));
+        ABHSF_CUDA(cudaMemcpyAsync(&lc, bcnt.get() + nb - 1, sizeof lc, cudaMemcpyDeviceToHost, st));
+        ABHSF_CUDA(cudaStreamSynchronize(st));
+        L = 1 + lo + lc;
     }
-    dbuf<uint8_t> kind(L), live(L), flag(L);
-    dbuf<unsigned long long> ri(L), ci(L);
-    dbuf<double> vi(L);
-    dbuf<int64_t> rank(L);
-    k_read_lines<<<grid_for(L), 256, 0, st>>>(L, R, d_buf.get(), start.get(), pattern, kind.get(), ri.get(), ci.get(),
+    sbuf<int64_t> start(L, st);
+    k_write_lines<<<(unsigned)nb, kLineThreads, 0, st>>>(R, text, boff.get(), start.get());
+    ABHSF_CUDA(cudaGetLastError());
+    sbuf<uint8_t> kind(L, st), live(L, st), flag(L, st);
+    sbuf<unsigned long long> ri(L, st), ci(L, st);
+    sbuf<double> vi(L, st);
+    sbuf<int64_t> rank(L, st), idx(L, st);
+    k_read_lines<<<grid_for(L), 256, 0, st>>>(L, R, text, start.get(), pattern, kind.get(), ri.get(), ci.get(),
                                               vi.get(), live.get());
     ABHSF_CUDA(cudaGetLastError());
     int64_t entries = 0;  // non-blank lines
@@ -461,7 +622,7 @@ void read_mtx_device(const char* path, cudaStream_t st, abhsf_coo_device& out)
         // rank = exclusive count of non-blank lines before each line
         size_t tb = 0;
         ABHSF_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, live.get(), rank.get(), L, st));
-        dbuf<uint8_t> tmp(std::max<size_t>(tb, 1));
+        sbuf<uint8_t> tmp(tb, st);
         ABHSF_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, live.get(), rank.get(), L, st));
         int64_t last_rank = 0;
         uint8_t last_live = 0;
@@ -473,32 +634,43 @@ void read_mtx_device(const char* path, cudaStream_t st, abhsf_coo_device& out)
     // lines the host reads
     k_host_lines<<<grid_for(L), 256, 0, st>>>(L, hd.nnz, kind.get(), rank.get(), flag.get());
     ABHSF_CUDA(cudaGetLastError());
-    dbuf<int64_t> hidx;
-    const int64_t nh = select_flagged(flag.get(), L, hidx, st);
+    const int64_t nh = select_flagged(flag.get(), L, idx.get(), st);
     if (nh > 0) {
-        std::vector<int64_t> hb(nh), he(nh);
+        std::vector<int64_t> hb(nh), he(nh), at(nh + 1, 0);
         std::vector<uint8_t> hk(nh);
+        sbuf<int64_t> d_b(nh, st), d_e(nh, st), d_at(nh + 1, st);
+        sbuf<uint8_t> d_k(nh, st);
+        k_line_spans<<<grid_for(nh), 256, 0, st>>>(nh, idx.get(), L, R, start.get(), kind.get(), d_b.get(), d_e.get(),
+                                                   d_k.get());
+        ABHSF_CUDA(cudaGetLastError());
+        ABHSF_CUDA(cudaMemcpyAsync(hb.data(), d_b.get(), nh * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        ABHSF_CUDA(cudaMemcpyAsync(he.data(), d_e.get(), nh * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        ABHSF_CUDA(cudaMemcpyAsync(hk.data(), d_k.get(), nh, cudaMemcpyDeviceToHost, st));
+        ABHSF_CUDA(cudaStreamSynchronize(st));
+        for (int64_t j = 0; j < nh; ++j) {
+            if (hk[j] == kShort) {  // an entry spread over lines: the host reader, on the whole file
+                host_fallback(path, st, out);
+                return;
+            }
+            at[j + 1] = at[j] + (he[j] - hb[j]);
+        }
+        // the lines' text, packed on the device and brought over in one copy
+        std::string lines((size_t)at[nh], '\0');
         {
-            dbuf<int64_t> d_b(nh), d_e(nh);
-            dbuf<uint8_t> d_k(nh);
-            k_line_spans<<<grid_for(nh), 256, 0, st>>>(nh, hidx.get(), L, R, start.get(), kind.get(), d_b.get(),
-                                                       d_e.get(), d_k.get());
+            sbuf<char> packed(at[nh], st);
+            ABHSF_CUDA(cudaMemcpyAsync(d_at.get(), at.data(), (nh + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+            k_pack_lines<<<(unsigned)std::min<int64_t>(nh, 4096), 128, 0, st>>>(nh, text, d_b.get(), d_e.get(),
+                                                                             d_at.get(), packed.get());
             ABHSF_CUDA(cudaGetLastError());
-            ABHSF_CUDA(cudaMemcpyAsync(hb.data(), d_b.get(), nh * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-            ABHSF_CUDA(cudaMemcpyAsync(he.data(), d_e.get(), nh * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-            ABHSF_CUDA(cudaMemcpyAsync(hk.data(), d_k.get(), nh, cudaMemcpyDeviceToHost, st));
+            ABHSF_CUDA(cudaMemcpyAsync(&lines[0], packed.get(), at[nh], cudaMemcpyDeviceToHost, st));
             ABHSF_CUDA(cudaStreamSynchronize(st));
         }
         std::vector<unsigned long long> hr(nh), hc(nh);
         std::vector<double> hv(nh);
         std::string line;
         for (int64_t j = 0; j < nh; ++j) {
-            if (hk[j] == kShort) {  // an entry spread over lines: the host reader, on the whole file
-                host_fallback(path, st, out);
-                return;
-            }
             // the line alone (no line end), so that the host's parse cannot run into the next
-            line.assign(text + hb[j], text + he[j]);
+            line.assign(lines, (size_t)at[j], (size_t)(at[j + 1] - at[j]));
             while (!line.empty() && line.back() == '\n')
                 line.pop_back();
             if (parse_entry_host(line.c_str(), line.c_str() + line.size(), pattern, hr[j], hc[j], hv[j]) != 0) {
@@ -506,19 +678,19 @@ void read_mtx_device(const char* path, cudaStream_t st, abhsf_coo_device& out)
                 return;
             }
         }
-        dbuf<unsigned long long> d_hr(nh), d_hc(nh);
-        dbuf<double> d_hv(nh);
+        sbuf<unsigned long long> d_hr(nh, st), d_hc(nh, st);
+        sbuf<double> d_hv(nh, st);
         ABHSF_CUDA(cudaMemcpyAsync(d_hr.get(), hr.data(), nh * sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
         ABHSF_CUDA(cudaMemcpyAsync(d_hc.get(), hc.data(), nh * sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
         ABHSF_CUDA(cudaMemcpyAsync(d_hv.get(), hv.data(), nh * sizeof(double), cudaMemcpyHostToDevice, st));
-        k_put_host<<<grid_for(nh), 256, 0, st>>>(nh, hidx.get(), d_hr.get(), d_hc.get(), d_hv.get(), kind.get(),
+        k_put_host<<<grid_for(nh), 256, 0, st>>>(nh, idx.get(), d_hr.get(), d_hc.get(), d_hv.get(), kind.get(),
                                                  ri.get(), ci.get(), vi.get());
         ABHSF_CUDA(cudaGetLastError());
-        ABHSF_CUDA(cudaStreamSynchronize(st));
+        ABHSF_CUDA(cudaStreamSynchronize(st));  // before the host vectors go
     }
     out.host_parsed = nh;
     // checks and the kept entries
-    dbuf<check_out> chk(1);
+    sbuf<check_out> chk(1, st);
     const check_out init{~0ull, 0, 0};
     ABHSF_CUDA(cudaMemcpyAsync(chk.get(), &init, sizeof init, cudaMemcpyHostToDevice, st));
     k_check<<<grid_for(L), 256, 0, st>>>(L, hd.nnz, hd.m, hd.n, pattern, kind.get(), rank.get(), ri.get(), ci.get(),
@@ -534,15 +706,14 @@ void read_mtx_device(const char* path, cudaStream_t st, abhsf_coo_device& out)
     if (hd.symmetry != ABHSF_SYMMETRY_GENERAL && res.lower && res.upper)
         fail(ABHSF_ERROR_INVALID_VALUE, "elements from both L and U parts stored for not-unsymmetric matrix");
     out.stored_triangle = hd.symmetry == ABHSF_SYMMETRY_GENERAL ? 0 : (res.lower ? 1 : 2);
-    dbuf<int64_t> kidx;
-    const int64_t kept = select_flagged(flag.get(), L, kidx, st);
+    const int64_t kept = select_flagged(flag.get(), L, idx.get(), st);
     out.nnz = kept;
     const size_t k = (size_t)std::max<int64_t>(kept, 1);
-    ABHSF_CUDA(cudaMalloc(&out.rows, k * sizeof(int64_t)));
-    ABHSF_CUDA(cudaMalloc(&out.cols, k * sizeof(int64_t)));
-    ABHSF_CUDA(cudaMalloc(&out.vals, k * sizeof(double)));
+    ABHSF_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&out.rows), k * sizeof(int64_t), st));
+    ABHSF_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&out.cols), k * sizeof(int64_t), st));
+    ABHSF_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&out.vals), k * sizeof(double), st));
     if (kept > 0) {
-        k_gather<<<grid_for(kept), 256, 0, st>>>(kept, kidx.get(), ri.get(), ci.get(), vi.get(), out.rows, out.cols,
+        k_gather<<<grid_for(kept), 256, 0, st>>>(kept, idx.get(), ri.get(), ci.get(), vi.get(), out.rows, out.cols,
                                                  out.vals);
         ABHSF_CUDA(cudaGetLastError());
     }

@@ -76,6 +76,20 @@ def test_large_file_parsed_on_the_device(gpu, tmp_path):
     assert d[0].numel() == k and d[5]["host_parsed"] == 0
 
 
+def test_header_longer_than_the_first_chunk(gpu, tmp_path):
+    """The file travels to the device in 16 MiB chunks and the banner and
+    size line are read from the first; comments past it are read again from
+    the whole file."""
+    p = tmp_path / "long_header.mtx"
+    with open(p, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        for _ in range(18):
+            f.write("%" + "c" * (1 << 20) + "\n")
+        f.write("3 3 3\n1 1 1.5\n2 2 2.5\n3 3 -3.5\n")
+    d = check_file(str(p))
+    assert d[0].numel() == 3
+
+
 def test_other_spellings_go_to_the_host_line_by_line(gpu, tmp_path):
     text = ("%%MatrixMarket matrix coordinate real general\n4 4 6\n"
             "1 1 +2.5\n2 2 0x1p3\n  3 3 1.0000000000000000000001\n\n4 4 1e-320\n1 2 -0\n2 1 7.25 trailing words\n"
