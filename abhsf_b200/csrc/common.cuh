@@ -190,6 +190,7 @@ struct abhsf_matrix {
     int ring_layout = 0;  // consumer layout of its single-right-hand-side launches (timed at build)
     int ring_bulk = 0;   // x / y blocks as bulk copies (timed at build)
     bool ring_ready = false;  // the ring kernel and the slice kernel together serve this matrix
+    bool dc_beside_ring = false;  // the sliced rows run on dc_side beside the ring kernel (one CTA an SM)
     // delta-coded row slices of the hypersparse block rows (spmv_stream.cu)
     struct dc_slice_host {
         int64_t base = 0;   // first slot of its words and values

@@ -116,7 +116,9 @@ enum deal_kind {
     kDealChains = 1,  // the chains
 };
 void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sched, dbuf<int64_t>& wbeg,
-                 int& warps, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, int kind);
+                 int& warps, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, int kind, bool beside_ring = false);
+// After the ring schedule: deal the sliced rows to run beside the ring kernel.
+void slices_beside_ring(abhsf_matrix& a, cudaStream_t st);
 struct dc_plan {
     const uint8_t* sched = nullptr;
     const int64_t* wbeg = nullptr;

@@ -1458,6 +1458,8 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
     a.ring_ready = true;
     a.ring_max_pv = mpv;
     a.ring_warps = ctas;
+    if (ctas > 0)
+        slices_beside_ring(a, st);
     if (a.value_type == ABHSF_VALUE_F64)
         a.s == 32 ? tune_ring<32, ABHSF_VALUE_F64>(a, st) : tune_ring<64, ABHSF_VALUE_F64>(a, st);
     else if (a.value_type == ABHSF_VALUE_F32)

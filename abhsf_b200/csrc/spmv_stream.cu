@@ -626,14 +626,15 @@ inline unsigned grid_of(int64_t n) { return (unsigned)std::max<int64_t>(1, std::
 
 // Warps of a launch: the chains one CTA per SM; the sliced rows every
 // resident CTA, less one per SM when chains run beside them (their CTA needs
-// the registers).
-int stream_grid_warps(int64_t items, bool chains, bool beside_chains)
+// the registers), or one CTA per SM when they run beside the ring kernel
+// (which leaves an SM the registers and warps of one such CTA).
+int stream_grid_warps(int64_t items, bool chains, bool beside_chains, bool beside_ring)
 {
     int dev = 0, nsm = 0;
     ABHSF_CUDA(cudaGetDevice(&dev));
     ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const int64_t full = chains ? (int64_t)nsm * kChainGridPerSm * kChainWarps
-                                : (int64_t)nsm * (kCtasPerSm - (beside_chains ? 1 : 0)) * kWarpsPerCta;
+    const int ctas = beside_ring ? 1 : kCtasPerSm - (beside_chains ? 1 : 0);
+    const int64_t full = chains ? (int64_t)nsm * kChainGridPerSm * kChainWarps : (int64_t)nsm * ctas * kWarpsPerCta;
     return (int)std::max<int64_t>(1, std::min<int64_t>(full, items));
 }
 
@@ -666,7 +667,7 @@ inline uint64_t slice_weight(const abhsf_matrix::dc_slice_host& p)
 // matrices (block rows in [brow_lo, brow_hi) only) over the warps of one
 // launch.
 void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sched, dbuf<int64_t>& wbeg_d,
-                 int& warps_out, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, int kind)
+                 int& warps_out, cudaStream_t st, int64_t brow_lo, int64_t brow_hi, int kind, bool beside_ring)
 {
     const bool chains = kind != kDealSliced;
     struct item {
@@ -689,7 +690,7 @@ void deal_slices(const std::vector<const abhsf_matrix*>& mats, dbuf<uint8_t>& sc
     warps_out = 0;
     if (items.empty())
         return;
-    const int W = stream_grid_warps((int64_t)items.size(), chains, !chains && other);
+    const int W = stream_grid_warps((int64_t)items.size(), chains, !chains && other, beside_ring);
     std::stable_sort(items.begin(), items.end(), [](const item& a, const item& b) { return a.w > b.w; });
     using load_t = std::pair<uint64_t, int>;
     std::priority_queue<load_t, std::vector<load_t>, std::greater<load_t>> heap;
@@ -755,6 +756,7 @@ void prepare_stream(abhsf_matrix& a, float avg, cudaStream_t st)
     a.dc_host.clear();
     a.dc_tree_flag.assign((size_t)a.tree_nrows, 0);
     a.dc_warps = a.dc_cwarps = 0;
+    a.dc_beside_ring = false;
     a.dc_elements = a.dc_rows = a.dc_slots = a.dc_lane_records = 0;
     const int s = a.s, lg = a.lg;
     if (avg <= 0.f || a.tree_nrows == 0 || a.sum_order != ABHSF_SUM_REFERENCE || (uint64_t)a.n > (uint64_t(1) << 32))
@@ -1088,24 +1090,50 @@ dc_plan plan_of(const abhsf_matrix& a)
     return p;
 }
 
+// Whether this launch runs the sliced rows on the side stream, beside the ring
+// kernel queued on st after slices_begin (single right-hand sides only).
+inline bool sliced_beside(const abhsf_matrix& a, const dc_plan& p, int cols)
+{
+    return a.dc_beside_ring && cols == 1 && p.warps > 0 && p.sched == a.dc_sched.get();
+}
+
 void slices_begin(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
                   cudaStream_t st, int cols)
 {
-    if (p.cwarps == 0)
+    const bool beside = sliced_beside(a, p, cols);
+    if (p.cwarps == 0 && !beside)
         return;
     if (!a.dc_side)
         fail(ABHSF_ERROR_CUDA, "matrix has chains but no side stream");
-    fork_chains(st, a.dc_side, a.dc_fork, a.dc_join, a.s, a.value_type, false,
-                args_of(a, p.csched, p.cwbeg, p.cwarps, x, ldx, y, ldy), cols);
+    ABHSF_CUDA(cudaEventRecord(a.dc_fork, st));
+    ABHSF_CUDA(cudaStreamWaitEvent(a.dc_side, a.dc_fork, 0));
+    if (beside)  // first, so that its CTAs take their place before the ring's fill the SMs
+        launch(a.s, a.value_type, false, false, args_of(a, p.sched, p.wbeg, p.warps, x, ldx, y, ldy), a.dc_side);
+    if (p.cwarps)
+        launch_cols(cols, a.s, a.value_type, true, args_of(a, p.csched, p.cwbeg, p.cwarps, x, ldx, y, ldy),
+                    a.dc_side);
+    ABHSF_CUDA(cudaEventRecord(a.dc_join, a.dc_side));
 }
 
 void slices_end(const abhsf_matrix& a, const dc_plan& p, const void* x, int64_t ldx, void* y, int64_t ldy,
                 cudaStream_t st, int cols)
 {
-    if (p.warps)
+    const bool beside = sliced_beside(a, p, cols);
+    if (p.warps && !beside)
         launch_cols(cols, a.s, a.value_type, false, args_of(a, p.sched, p.wbeg, p.warps, x, ldx, y, ldy), st);
-    if (p.cwarps)
+    if (p.cwarps || beside)
         ABHSF_CUDA(cudaStreamWaitEvent(st, a.dc_join, 0));
+}
+
+// The ring kernel serves some block rows: the sliced rows go beside it, dealt
+// over one CTA an SM.
+void slices_beside_ring(abhsf_matrix& a, cudaStream_t st)
+{
+    if (a.dc_warps == 0)
+        return;
+    deal_slices({&a}, a.dc_sched, a.dc_wbeg, a.dc_warps, st, 0, INT64_MAX, kDealSliced, true);
+    make_side(a.dc_side, a.dc_fork, a.dc_join);
+    a.dc_beside_ring = true;
 }
 
 // The slices of every matrix of a batch in one launch (and its chains in one more).

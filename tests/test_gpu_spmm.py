@@ -102,6 +102,38 @@ def test_spmm_tiled_mixture_matches_spmv(gpu):
     np.testing.assert_array_equal(_spmm(A, X, Y0), _spmv_columns(A, X, Y0))
 
 
+@pytest.mark.parametrize("s", [32, 64])
+@pytest.mark.parametrize("forced", [None, "coo", "csr", "bitmap", "dense"])
+@pytest.mark.parametrize("k", [16, 32, 50])
+def test_spmm_wide_k_every_scheme(gpu, s, forced, k):
+    """16, 32 and 50 right-hand sides over every scheme (the ring's passes of
+    up to 8 columns, the row slices' passes of up to 32), with padded leading
+    dimensions: every column bitwise its SpMV, and the reference order per
+    column."""
+    coo = W.random_blocky(1300, 1500, s, 90, seed=15)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, forced_scheme=forced)
+    X, Y0 = _inputs(coo, k, seed=k + s)
+    Y = _spmm(A, X, Y0, 3, 1)
+    np.testing.assert_array_equal(Y, _spmv_columns(A, X, Y0))
+    order = np.lexsort((coo.cols, coo.rows))
+    r, c, v = coo.rows[order], coo.cols[order], coo.vals[order]
+    for j in (0, k - 1):
+        np.testing.assert_array_equal(Y[:, j], oracle.spmv_elements(r, c, v, X[:, j].copy(), Y0[:, j].copy()))
+
+
+def test_spmm_dense_zeros_like_the_spmv(gpu):
+    """A dense tile with stored zeros (explicit zero elements among them), 32
+    right-hand sides: the SpMM treats them as the SpMV does."""
+    rng = np.random.default_rng(3)
+    rows, cols = np.meshgrid(np.arange(64), np.arange(64), indexing="ij")
+    rows, cols = rows.ravel().astype(np.int64), cols.ravel().astype(np.int64)
+    vals = rng.standard_normal(rows.size)
+    vals[::7] = 0.0
+    A = AbhsfMatrix.from_elements(rows, cols, vals, 100, 90, block_size=64, forced_scheme="dense")
+    X, Y0 = rng.uniform(-1, 1, (90, 32)), rng.standard_normal((100, 32))
+    np.testing.assert_array_equal(_spmm(A, X, Y0), _spmv_columns(A, X, Y0))
+
+
 @pytest.mark.parametrize("k", [32, 45])
 def test_spmm_power_law_wide_passes(gpu, k):
     """R-MAT (power-law rows): sliced rows and chains through the passes of 32
