@@ -362,8 +362,10 @@ struct group_geo {
 // cannot complete before lane 0's arrival, which posts it.)  Where every x
 // block (and y block) of the group lies whole inside x (y), is contiguous
 // (one right-hand side per row of X, or ldx = K) and 16-byte aligned, each
-// travels as one bulk copy issued by its tile's lane; otherwise the warp
-// copies them element by element, filling zeros past n (m).
+// travels as one bulk copy issued by its tile's lane; where the K values of
+// each row are 16-byte aligned runs inside wider rows (ldx > K), each row
+// travels as a bulk copy; otherwise the warp copies them element by element,
+// filling zeros past n (m).
 template <int S, int K, int VT, bool B>
 __device__ __forceinline__ void issue_group(const ring_args& P, const mat_view& mv, const ring_desc& d, int yk,
                                             const group_geo& gg, uint32_t off, int q, int team,
@@ -396,6 +398,14 @@ __device__ __forceinline__ void issue_group(const ring_args& P, const mat_view& 
     const bool bulk = P.bulk && !drop && P.ldx == K && P.ldy == K &&
                       ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) & 15) == 0 &&
                       __all_sync(kFull, whole);
+    // several right-hand sides inside wider rows of X and Y (ldx, ldy > K):
+    // each of a block's S rows of K values as a bulk copy of its own, where
+    // those rows are whole and 16-byte aligned
+    constexpr int RB = K * TB;  // bytes of one row of a block
+    const bool row_bulk = !bulk && RB % 16 == 0 && P.bulk && !drop && ((P.ldx * TB) & 15) == 0 &&
+                          ((P.ldy * TB) & 15) == 0 &&
+                          ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) & 15) == 0 &&
+                          __all_sync(kFull, whole);
     uint32_t xy_bytes = 0;
     if (bulk) {
         xy_bytes = (uint32_t)(nt + __popc(__ballot_sync(kFull, lane < nt && first))) * XB;
@@ -404,6 +414,20 @@ __device__ __forceinline__ void issue_group(const ring_args& P, const mat_view& 
             bulk_g2s(base + gg.x_off + lane * XB, X + c0 * K, XB, bar);
             if (first)
                 bulk_g2s(base + gg.y_off + yk * XB, Y + r0 * K, XB, bar);
+        }
+    } else if (row_bulk) {
+        xy_bytes = (uint32_t)(nt + __popc(__ballot_sync(kFull, lane < nt && first))) * XB;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        for (int j = 0; j < nt; ++j) {
+            const int64_t cj = (int64_t)col_of<B>(__shfl_sync(kFull, d.col, j)) * S;
+            const uint32_t info = __shfl_sync(kFull, d.info, j);
+            const int ykj = __shfl_sync(kFull, yk, j);
+            const int64_t rj = (int64_t)(info & kRowMask) * S;
+            for (int c = lane; c < S; c += 32) {
+                bulk_g2s(base + gg.x_off + j * XB + c * RB, X + (cj + c) * P.ldx, RB, bar);
+                if (info & kFirst)
+                    bulk_g2s(base + gg.y_off + ykj * XB + c * RB, Y + (rj + c) * P.ldy, RB, bar);
+            }
         }
     } else if (nt == 1) {
         const uint32_t col = col_of<B>(__shfl_sync(kFull, d.col, 0)), info = __shfl_sync(kFull, d.info, 0);

@@ -105,15 +105,17 @@ def test_spmm_tiled_mixture_matches_spmv(gpu):
 @pytest.mark.parametrize("s", [32, 64])
 @pytest.mark.parametrize("forced", [None, "coo", "csr", "bitmap", "dense"])
 @pytest.mark.parametrize("k", [16, 32, 50])
-def test_spmm_wide_k_every_scheme(gpu, s, forced, k):
+@pytest.mark.parametrize("pads", [(3, 1), (2, 4), (0, 0)])
+def test_spmm_wide_k_every_scheme(gpu, s, forced, k, pads):
     """16, 32 and 50 right-hand sides over every scheme (the ring's passes of
-    up to 8 columns, the row slices' passes of up to 32), with padded leading
-    dimensions: every column bitwise its SpMV, and the reference order per
-    column."""
+    up to 8 columns, the row slices' passes of up to 32), inside wider rows
+    of X and Y: rows whose K values are 16-byte aligned travel as bulk copies
+    (pads 2, 4 and 0), the others element by element (pads 3, 1).  Every
+    column bitwise its SpMV, and the reference order per column."""
     coo = W.random_blocky(1300, 1500, s, 90, seed=15)
     A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, forced_scheme=forced)
     X, Y0 = _inputs(coo, k, seed=k + s)
-    Y = _spmm(A, X, Y0, 3, 1)
+    Y = _spmm(A, X, Y0, *pads)
     np.testing.assert_array_equal(Y, _spmv_columns(A, X, Y0))
     order = np.lexsort((coo.cols, coo.rows))
     r, c, v = coo.rows[order], coo.cols[order], coo.vals[order]
