@@ -195,11 +195,12 @@ __device__ __forceinline__ T add_products_full(T run, const T* q)
 // words and values, are loaded while the current ones are summed, so that a
 // step waits only on its x gathers.
 template <int S, int VT, bool B>
-__global__ void __launch_bounds__(32 * kWarpsPerCta) k_spmv_slices(dc_args P)
+__global__ void __launch_bounds__(32 * kWarpsPerCta, kCtasPerSm) k_spmv_slices(dc_args P)
 {
     using T = typename vt_of<VT>::T;
     using V = typename vt_of<VT>::V;
-    constexpr int U = kUnroll;
+    // f32 / bf16 values leave room in 64 registers for twice the steps in flight
+    constexpr int U = VT == ABHSF_VALUE_F64 ? kUnroll : 2 * kUnroll;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gw = blockIdx.x * kWarpsPerCta + warp;
     if (gw >= P.warps)
