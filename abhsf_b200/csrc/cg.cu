@@ -50,13 +50,46 @@ __device__ __forceinline__ double block_sum(double v)
     return v;  // valid in thread 0
 }
 
-// partial[blockIdx.x] = sum over this block's grid-stride share of a[i] b[i]
+// 16 bytes of T: the unit the vector kernels below load and store when every
+// array they touch is 16-byte aligned (VEC), so that an f32 pass moves as
+// many bytes per instruction as an f64 one.
 template <typename T>
+struct __align__(16) pack {
+    static constexpr int N = 16 / sizeof(T);
+    T v[N];
+};
+
+template <typename T>
+__device__ __forceinline__ pack<T> ld_pack(const T* p)
+{
+    return *reinterpret_cast<const pack<T>*>(p);
+}
+
+template <typename T>
+__device__ __forceinline__ void st_pack(T* p, const pack<T>& v)
+{
+    *reinterpret_cast<pack<T>*>(p) = v;
+}
+
+constexpr int64_t kStride = (int64_t)kRedBlocks * kRedThreads;
+
+// partial[blockIdx.x] = sum over this block's grid-stride share of a[i] b[i]
+// (with VEC, packs of 16 bytes, then the tail past the last whole pack)
+template <typename T, bool VEC>
 __global__ void __launch_bounds__(kRedThreads) k_dot(int64_t n, const T* __restrict__ a, const T* __restrict__ b,
                                                      double* __restrict__ partial)
 {
+    constexpr int N = pack<T>::N;
+    const int64_t tid = blockIdx.x * (int64_t)kRedThreads + threadIdx.x;
+    const int64_t nv = VEC ? n / N : 0;
     double s = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)kRedBlocks * kRedThreads)
+    for (int64_t i = tid; i < nv; i += kStride) {
+        const pack<T> va = ld_pack(a + i * N), vb = ld_pack(b + i * N);
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+            s += (double)va.v[k] * (double)vb.v[k];
+    }
+    for (int64_t i = nv * N + tid; i < n; i += kStride)
         s += (double)a[i] * (double)b[i];
     s = block_sum(s);
     if (threadIdx.x == 0)
@@ -117,14 +150,32 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_alpha(const double* __restri
 }
 
 // x += alpha p; r -= alpha Ap; Ap = 0 (ready for the next y += A p); partial r . r
-template <typename T>
+template <typename T, bool VEC>
 __global__ void __launch_bounds__(kRedThreads) k_cg_update_xr(int64_t n, T* __restrict__ x, T* __restrict__ r,
                                                               T* __restrict__ ap, const T* __restrict__ p,
                                                               const cg_state* st, double* __restrict__ partial)
 {
+    constexpr int N = pack<T>::N;
     const T alpha = (T)st->alpha;
+    const int64_t tid = blockIdx.x * (int64_t)kRedThreads + threadIdx.x;
+    const int64_t nv = VEC ? n / N : 0;
     double s = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)kRedThreads + threadIdx.x; i < n; i += (int64_t)kRedBlocks * kRedThreads) {
+    for (int64_t i = tid; i < nv; i += kStride) {
+        pack<T> vr = ld_pack(r + i * N), vx = ld_pack(x + i * N);
+        const pack<T> va = ld_pack(ap + i * N), vp = ld_pack(p + i * N);
+        pack<T> zero;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            vr.v[k] = vr.v[k] - alpha * va.v[k];
+            vx.v[k] += alpha * vp.v[k];
+            zero.v[k] = T(0);
+            s += (double)vr.v[k] * (double)vr.v[k];
+        }
+        st_pack(x + i * N, vx);
+        st_pack(r + i * N, vr);
+        st_pack(ap + i * N, zero);
+    }
+    for (int64_t i = nv * N + tid; i < n; i += kStride) {
         const T ri = r[i] - alpha * ap[i];
         x[i] += alpha * p[i];
         r[i] = ri;
@@ -150,13 +201,24 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_beta(const double* __restric
 
 // p = r + beta p, also in the iteration that met the tolerance, so that a
 // recurrence resumed from a replaced residual continues from the right p
-template <typename T>
+template <typename T, bool VEC>
 __global__ void k_cg_update_p(int64_t n, T* __restrict__ p, const T* __restrict__ r, const cg_state* st)
 {
     if (!st->active)
         return;
+    constexpr int N = pack<T>::N;
     const T beta = (T)st->beta;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t nv = VEC ? n / N : 0;
+    for (int64_t i = tid; i < nv; i += stride) {
+        pack<T> vp = ld_pack(p + i * N);
+        const pack<T> vr = ld_pack(r + i * N);
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+            vp.v[k] = vr.v[k] + beta * vp.v[k];
+        st_pack(p + i * N, vp);
+    }
+    for (int64_t i = nv * N + tid; i < n; i += stride)
         p[i] = r[i] + beta * p[i];
 }
 
@@ -208,10 +270,15 @@ void residual(const abhsf_matrix& a, const T* b, const T* x, T* r, T* xn, int64_
     spmv_t(a, xn, r, st);
 }
 
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 template <typename T>
 void dot(const T* a, const T* b, int64_t n, double* partial, cudaStream_t st)
 {
-    k_dot<T><<<kRedBlocks, kRedThreads, 0, st>>>(n, a, b, partial);
+    if (aligned16(a) && aligned16(b))
+        k_dot<T, true><<<kRedBlocks, kRedThreads, 0, st>>>(n, a, b, partial);
+    else
+        k_dot<T, false><<<kRedBlocks, kRedThreads, 0, st>>>(n, a, b, partial);
 }
 
 // p = r, Ap = 0 and the state from r . r: the start of a CG recurrence.
@@ -234,15 +301,23 @@ class cg_graph {
     cg_graph(const abhsf_matrix& a, T* x, cg_work<T>& w, int64_t n, cg_state* st_d, double* partial, cudaStream_t cs)
     {
         cudaGraph_t graph = nullptr;
+        const bool vec = aligned16(x) && aligned16(w.r.get()) && aligned16(w.ap.get()) && aligned16(w.p.get());
         ABHSF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
         for (int it = 0; it < kChunk; ++it) {
             spmv_t(a, w.p.get(), w.ap.get(), cs);
             dot<T>(w.p.get(), w.ap.get(), n, partial, cs);
             k_cg_alpha<<<1, kRedThreads, 0, cs>>>(partial, st_d);
-            k_cg_update_xr<T>
-                <<<kRedBlocks, kRedThreads, 0, cs>>>(n, x, w.r.get(), w.ap.get(), w.p.get(), st_d, partial);
+            if (vec)
+                k_cg_update_xr<T, true>
+                    <<<kRedBlocks, kRedThreads, 0, cs>>>(n, x, w.r.get(), w.ap.get(), w.p.get(), st_d, partial);
+            else
+                k_cg_update_xr<T, false>
+                    <<<kRedBlocks, kRedThreads, 0, cs>>>(n, x, w.r.get(), w.ap.get(), w.p.get(), st_d, partial);
             k_cg_beta<<<1, kRedThreads, 0, cs>>>(partial, st_d);
-            k_cg_update_p<T><<<elem_grid(n), 256, 0, cs>>>(n, w.p.get(), w.r.get(), st_d);
+            if (vec)
+                k_cg_update_p<T, true><<<elem_grid(n), 256, 0, cs>>>(n, w.p.get(), w.r.get(), st_d);
+            else
+                k_cg_update_p<T, false><<<elem_grid(n), 256, 0, cs>>>(n, w.p.get(), w.r.get(), st_d);
         }
         const cudaError_t cap = cudaStreamEndCapture(cs, &graph);
         if (cap != cudaSuccess || !graph)

@@ -33,6 +33,29 @@ def _shifted_laplacian_2d(g, shift, seed):
     return W.Coo(coo.rows, coo.cols, vals, coo.m, coo.n)
 
 
+@pytest.mark.parametrize("offset", [0, 1])
+def test_cg_unaligned_and_odd_length_vectors(gpu, offset):
+    """x and b 8 bytes past a 16-byte boundary (the vector kernels then take
+    their element-by-element path) and n not a multiple of the 16-byte packs:
+    the same solve, to the same residual, either way."""
+    import torch
+    coo = W.laplacian_3d(17)  # n = 4913, odd
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
+    b = np.random.default_rng(3).uniform(-1, 1, coo.n)
+    bb = torch.zeros(coo.n + 1, dtype=torch.float64, device="cuda")
+    xb = torch.zeros(coo.n + 1, dtype=torch.float64, device="cuda")
+    bd, xd = bb[offset:offset + coo.n], xb[offset:offset + coo.n]
+    bd.copy_(torch.from_numpy(b))
+    info = cg(A, bd, xd, rtol=1e-10)
+    assert info["converged"]
+    r = _cpu_rel_residual(coo, b, xd.cpu().numpy())
+    assert r <= 1e-10 and abs(r - info["rel_residual"]) <= 1e-12
+    A32 = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64, value_type="f32")
+    xd.zero_()
+    info = cg_mixed(A, A32, bd, xd, rtol=1e-10)
+    assert info["converged"] and _cpu_rel_residual(coo, b, xd.cpu().numpy()) <= 1e-10
+
+
 @pytest.mark.parametrize("s", [16, 64])
 def test_cg_fp64_laplacian_3d(gpu, s):
     coo = W.laplacian_3d(24)
