@@ -84,15 +84,13 @@ void autotune(const int64_t* rows, const int64_t* cols, const double* vals, int6
         o.block_size = 16 << k;
         auto a = std::make_unique<abhsf_matrix>();
         build_matrix(rows, cols, vals, nnz, m, n, o, st, *a);
-        auto run = [&]() -> bool {
-            if (f64) {
+        auto run = [&] {
+            if (f64)
                 spmv_dispatch(*a, reinterpret_cast<const double*>(x.get()), reinterpret_cast<double*>(y.get()), st);
-                return true;
-            }
-            return spmv_f32_ring(*a, reinterpret_cast<const float*>(x.get()), reinterpret_cast<float*>(y.get()), st);
+            else
+                spmv_f32_dispatch(*a, reinterpret_cast<const float*>(x.get()), reinterpret_cast<float*>(y.get()), st);
         };
-        if (!run())
-            continue;  // no f32 kernel for this size
+        run();
         ABHSF_CUDA(cudaEventRecord(ev.a, st));
         for (int r = 0; r < reps; ++r)
             run();

@@ -171,9 +171,7 @@ abhsf_status abhsf_spmv_f32(const abhsf_matrix* a, const float* x, float* y, abh
             fail(ABHSF_ERROR_INVALID_VALUE, "x and y must be 4-byte aligned");
         if (a->m == 0 || a->T == 0)
             return;
-        if (!abhsf::spmv_f32_ring(*a, x, y, reinterpret_cast<cudaStream_t>(stream)))
-            fail(ABHSF_ERROR_UNSUPPORTED,
-                 "abhsf_spmv_f32 supports block sizes 32 and 64, and others where every block row is in row slices");
+        abhsf::spmv_f32_dispatch(*a, x, y, reinterpret_cast<cudaStream_t>(stream));
     });
 }
 

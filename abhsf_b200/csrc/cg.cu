@@ -249,11 +249,7 @@ unsigned elem_grid(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<i
 
 // y += A x in T (f64 or f32 kernels)
 void spmv_t(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st) { spmv_dispatch(a, x, y, st); }
-void spmv_t(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st)
-{
-    if (!spmv_f32_ring(a, x, y, st))
-        fail(ABHSF_ERROR_UNSUPPORTED, "the f32 SpMV supports block sizes 32 and 64");
-}
+void spmv_t(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st) { spmv_f32_dispatch(a, x, y, st); }
 
 template <typename T>
 struct cg_work {
@@ -412,8 +408,6 @@ void cg_solve_mixed(const abhsf_matrix& a64, const abhsf_matrix& a32, const doub
     check_square(a64);
     if (a32.m != a64.m || a32.n != a64.n)
         fail(ABHSF_ERROR_INVALID_VALUE, "the two matrices of the mixed solver differ in shape");
-    if (!(a32.ring_ready || (a32.dc_rows > 0 && a32.dc_rows == a32.tree_nrows)) && a32.T > 0)
-        fail(ABHSF_ERROR_UNSUPPORTED, "the f32 SpMV of the mixed solver supports block sizes 32 and 64");
     const int64_t n = a64.n;
     const double f2 = update_factor * update_factor;
     solve_stream ss(user);

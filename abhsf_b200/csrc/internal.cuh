@@ -145,8 +145,11 @@ void cg_solve_mixed(const abhsf_matrix& a64, const abhsf_matrix& a32, const doub
                     int max_iters, double update_factor, int max_updates, abhsf_cg_info* info, cudaStream_t st);
 
 // y += A x in f32 for matrices stored as f32 or bf16 (values widened to f32,
-// same per-row order); false when the matrix has no ring schedule.
-bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st);
+// same per-row order): the ring kernel and slices where the matrix has a ring
+// schedule, else the streaming kernel (beside the slices of block sizes 16,
+// 128 and 256).
+void spmv_f32_dispatch(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st);
+void spmv_f32_seq(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st);
 // Y += A X (k columns, row-major X and Y) through the same kernel, several
 // right-hand sides per pass; false when the matrix has no ring schedule.
 bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,

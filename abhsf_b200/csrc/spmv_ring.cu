@@ -1578,18 +1578,13 @@ bool spmv_f64_ring(const abhsf_matrix& a, const double* x, double* y, cudaStream
     return true;
 }
 
-bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st)
+void spmv_f32_dispatch(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st)
 {
     if (a.value_type == ABHSF_VALUE_F64)
-        return false;
+        fail(ABHSF_ERROR_INVALID_VALUE, "the f32 SpMV needs a matrix stored as f32 or bf16");
     if (!a.ring_ready) {
-        if (a.dc_rows == 0 || a.dc_rows != a.tree_nrows)
-            return false;
-        std::lock_guard<std::mutex> lock(a.dc_mu);  // every block row in slices (block sizes 16, 128, 256)
-        const dc_plan p = plan_of(a);
-        slices_begin(a, p, x, 1, y, 1, st);
-        slices_end(a, p, x, 1, y, 1, st);
-        return true;
+        spmv_f32_seq(a, x, y, st);  // block sizes 16, 128, 256 (slices beside it), or no ring schedule
+        return;
     }
     std::lock_guard<std::mutex> lock(a.dc_mu);
     const dc_plan p = plan_of(a);
@@ -1608,7 +1603,6 @@ bool spmv_f32_ring(const abhsf_matrix& a, const float* x, float* y, cudaStream_t
         }
     }
     slices_end(a, p, x, 1, y, 1, st);
-    return true;
 }
 
 bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_t st)

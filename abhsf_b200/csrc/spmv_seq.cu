@@ -1,5 +1,6 @@
 // spmv_seq.cu -- y += A x over the ABHSF format in the reference's summation
-// order, FP64, sm_100a, streaming through registers.
+// order, sm_100a, streaming through registers: FP64, and f32 / bf16 values
+// widened to f32 with f32 x, y and sums (the same order in f32).
 //
 // The reference's CSR SpMV (csr_matrix::spmv_naive,
 // spmv/bottlenecks/spmv.cpp:58-64) adds a row's products one at a time,
@@ -50,13 +51,30 @@ struct sg {
     static constexpr int AUX = WPB > 8 ? WPB : 8;
 };
 
-template <int S>
+// Stored value type V and arithmetic type T of a value type.
+template <int VT>
+struct seq_t {
+    using V = double;
+    using T = double;
+};
+template <>
+struct seq_t<ABHSF_VALUE_F32> {
+    using V = float;
+    using T = float;
+};
+template <>
+struct seq_t<ABHSF_VALUE_BF16> {
+    using V = uint16_t;
+    using T = float;
+};
+
+template <int S, typename T>
 struct seq_smem {
     alignas(16) uint32_t aux[sg<S>::AUX];  // a staged bitmap block, or CSR row_end
-    double ys[S];                          // the block row's y segment
-    double xs[S];                          // x segment (element streams)
+    T ys[S];                               // the block row's y segment
+    T xs[S];                               // x segment (element streams)
     int32_t rowstart[sg<S>::RB + 1];       // staged rows' first values (tile-relative), + end
-    double buf[sg<S>::BUF];                // a group's products, row-major
+    T buf[sg<S>::BUF];                     // a group's products, row-major
 };
 
 struct seq_args {
@@ -64,20 +82,31 @@ struct seq_args {
     const uint32_t* rows;  // non-empty block rows, ascending
     int64_t nrows;
     unsigned int* counter;
-    const double* x;
-    double* y;
+    const void* x;  // T
+    void* y;        // T
 };
 
 __device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
+__device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
+__device__ __forceinline__ uint16_t ld_stream(const uint16_t* p)
+{
+    return __ldcs(reinterpret_cast<const unsigned short*>(p));
+}
+__device__ __forceinline__ double wide(double v) { return v; }
+__device__ __forceinline__ float wide(float v) { return v; }
+__device__ __forceinline__ float wide(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
 __device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 
 // acc + p[0] + p[1] + ... + p[n-1], one at a time, left to right.
-__device__ __forceinline__ double chain(double acc, const double* p, int n)
+template <typename T>
+__device__ __forceinline__ T chain(T acc, const T* p, int n)
 {
     int i = 0;
     for (; i + 8 <= n; i += 8) {
-        double t[8];
+        T t[8];
 #pragma unroll
         for (int v = 0; v < 8; ++v)
             t[v] = p[i + v];
@@ -91,10 +120,13 @@ __device__ __forceinline__ double chain(double acc, const double* p, int n)
 }
 
 // Bitmap tile, s >= 32: row r's columns 32j..32j+31 are bitmap word r*CPL + j.
-template <int S>
-__device__ __forceinline__ void seq_bitmap(const uint32_t* __restrict__ bm32, const double* __restrict__ vals,
-                                           const double (&xr)[sg<S>::CPL], seq_smem<S>& sm, int lane)
+template <int S, int VT>
+__device__ __forceinline__ void seq_bitmap(const uint32_t* __restrict__ bm32,
+                                           const typename seq_t<VT>::V* __restrict__ vals,
+                                           const typename seq_t<VT>::T (&xr)[sg<S>::CPL],
+                                           seq_smem<S, typename seq_t<VT>::T>& sm, int lane)
 {
+    using T = typename seq_t<VT>::T;
     constexpr int CPL = sg<S>::CPL, RB = sg<S>::RB, WPB = sg<S>::WPB, RG = sg<S>::RG;
     constexpr int NG = RB / RG;
     const uint32_t lt = (1u << lane) - 1u;
@@ -137,7 +169,7 @@ __device__ __forceinline__ void seq_bitmap(const uint32_t* __restrict__ bm32, co
 
         // a group's value indices (tile-relative; -1: bit clear) and values
         int idx[RG][CPL];
-        double v[RG][CPL];
+        T v[RG][CPL];
         auto load_group = [&](int g) {
 #pragma unroll
             for (int i = 0; i < RG; ++i) {
@@ -147,7 +179,7 @@ __device__ __forceinline__ void seq_bitmap(const uint32_t* __restrict__ bm32, co
                 for (int j = 0; j < CPL; ++j) {
                     const uint32_t w = sm.aux[row * CPL + j];
                     idx[i][j] = ((w >> lane) & 1u) ? run + __popc(w & lt) : -1;
-                    v[i][j] = idx[i][j] >= 0 ? ld_stream(vals + idx[i][j]) : 0.0;
+                    v[i][j] = idx[i][j] >= 0 ? wide(ld_stream(vals + idx[i][j])) : T(0);
                     run += __popc(w);
                 }
             }
@@ -168,7 +200,7 @@ __device__ __forceinline__ void seq_bitmap(const uint32_t* __restrict__ bm32, co
             if (lane < RG) {
                 const int row = g * RG + lane;
                 const int lo = sm.rowstart[row] - base, hi = sm.rowstart[row + 1] - base;
-                double& yr = sm.ys[blk * RB + row];
+                T& yr = sm.ys[blk * RB + row];
                 yr = chain(yr, sm.buf + lo, hi - lo);
             }
             __syncwarp();
@@ -177,18 +209,20 @@ __device__ __forceinline__ void seq_bitmap(const uint32_t* __restrict__ bm32, co
 }
 
 // Dense tile, s >= 32: all s*s values, row-major.
-template <int S>
-__device__ __forceinline__ void seq_dense(const double* __restrict__ vals, const double (&xr)[sg<S>::CPL],
-                                          int64_t c0, int64_t n, seq_smem<S>& sm, int lane)
+template <int S, int VT>
+__device__ __forceinline__ void seq_dense(const typename seq_t<VT>::V* __restrict__ vals,
+                                          const typename seq_t<VT>::T (&xr)[sg<S>::CPL], int64_t c0, int64_t n,
+                                          seq_smem<S, typename seq_t<VT>::T>& sm, int lane)
 {
+    using T = typename seq_t<VT>::T;
     constexpr int CPL = sg<S>::CPL, RG = sg<S>::RG, NG = S / RG;
-    double v[RG][CPL];
+    T v[RG][CPL];
     auto load_group = [&](int g) {
 #pragma unroll
         for (int i = 0; i < RG; ++i)
 #pragma unroll
             for (int j = 0; j < CPL; ++j)
-                v[i][j] = ld_stream(vals + (size_t)(g * RG + i) * S + lane + 32 * j);
+                v[i][j] = wide(ld_stream(vals + (size_t)(g * RG + i) * S + lane + 32 * j));
     };
     load_group(0);
 #pragma unroll 1
@@ -199,13 +233,13 @@ __device__ __forceinline__ void seq_dense(const double* __restrict__ vals, const
             for (int j = 0; j < CPL; ++j) {
                 const int c = lane + 32 * j;
                 // stored zeros become -0.0, a no-op in the sums
-                sm.buf[i * S + c] = (v[i][j] != 0.0 && c0 + c < n) ? fmul(v[i][j], xr[j]) : -0.0;
+                sm.buf[i * S + c] = (v[i][j] != T(0) && c0 + c < n) ? fmul(v[i][j], xr[j]) : T(-0.0);
             }
         __syncwarp();
         if (g + 1 < NG)
             load_group(g + 1);
         if (lane < RG) {
-            double& yr = sm.ys[g * RG + lane];
+            T& yr = sm.ys[g * RG + lane];
             yr = chain(yr, sm.buf + lane * S, S);
         }
         __syncwarp();
@@ -213,20 +247,22 @@ __device__ __forceinline__ void seq_dense(const double* __restrict__ vals, const
 }
 
 // s = 16 bitmap or dense: the whole tile (256 positions) at once.
-template <bool DENSE>
-__device__ __forceinline__ void seq_16(const uint32_t* __restrict__ bm32, const double* __restrict__ vals, double xl,
-                                       int64_t c0, int64_t n, seq_smem<16>& sm, int lane)
+template <bool DENSE, int VT>
+__device__ __forceinline__ void seq_16(const uint32_t* __restrict__ bm32, const typename seq_t<VT>::V* __restrict__ vals,
+                                       typename seq_t<VT>::T xl, int64_t c0, int64_t n,
+                                       seq_smem<16, typename seq_t<VT>::T>& sm, int lane)
 {
+    using T = typename seq_t<VT>::T;
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t w[8];
-    double v[8];
+    T v[8];
     int running = 0;
 #pragma unroll
     for (int it = 0; it < 8; ++it) {
         w[it] = DENSE ? 0xffffffffu : __ldcs(bm32 + it);
-        v[it] = 0.0;
+        v[it] = T(0);
         if ((w[it] >> lane) & 1u)
-            v[it] = ld_stream(vals + (DENSE ? it * 32 + lane : running + __popc(w[it] & lt)));
+            v[it] = wide(ld_stream(vals + (DENSE ? it * 32 + lane : running + __popc(w[it] & lt))));
         running += __popc(w[it]);
     }
     running = 0;
@@ -235,7 +271,7 @@ __device__ __forceinline__ void seq_16(const uint32_t* __restrict__ bm32, const 
     for (int it = 0; it < 8; ++it) {
         if ((w[it] >> lane) & 1u)
             sm.buf[running + __popc(w[it] & lt)] =
-                DENSE && !(v[it] != 0.0 && col_ok) ? -0.0 : fmul(v[it], xl);
+                DENSE && !(v[it] != T(0) && col_ok) ? T(-0.0) : fmul(v[it], xl);
         running += __popc(w[it]);
     }
     // row r's bits: half (r & 1) of word r >> 1
@@ -263,9 +299,10 @@ __device__ __forceinline__ void seq_16(const uint32_t* __restrict__ bm32, const 
 
 // COO / CSR tile: 32 stored elements at a time; the first lane of each row
 // segment adds the segment's products onto the row, in element order.
-template <int S, bool CSR>
-__device__ __forceinline__ void seq_stream(const uint8_t* __restrict__ pay, const double* __restrict__ vals, int z,
-                                           seq_smem<S>& sm, int lane)
+template <int S, bool CSR, int VT>
+__device__ __forceinline__ void seq_stream(const uint8_t* __restrict__ pay,
+                                           const typename seq_t<VT>::V* __restrict__ vals, int z,
+                                           seq_smem<S, typename seq_t<VT>::T>& sm, int lane)
 {
     constexpr int LG = S == 16 ? 4 : S == 32 ? 5 : S == 64 ? 6 : S == 128 ? 7 : 8;
     const uint16_t* key16 = reinterpret_cast<const uint16_t*>(pay);
@@ -301,7 +338,7 @@ __device__ __forceinline__ void seq_stream(const uint8_t* __restrict__ pay, cons
                 lr = (int)(key >> LG);
                 lc = (int)(key & (S - 1));
             }
-            sm.buf[lane] = fmul(ld_stream(vals + k), sm.xs[lc]);
+            sm.buf[lane] = fmul(wide(ld_stream(vals + k)), sm.xs[lc]);
         }
         const int plr = __shfl_up_sync(kFull, lr, 1);
         const bool head = k < z && (lane == 0 || plr != lr);
@@ -317,16 +354,21 @@ __device__ __forceinline__ void seq_stream(const uint8_t* __restrict__ pay, cons
     }
 }
 
-template <int S>
-__device__ __forceinline__ void seq_block_row(const seq_args& P, int64_t I, seq_smem<S>& sm, int lane)
+template <int S, int VT>
+__device__ __forceinline__ void seq_block_row(const seq_args& P, int64_t I, seq_smem<S, typename seq_t<VT>::T>& sm,
+                                              int lane)
 {
+    using T = typename seq_t<VT>::T;
+    using V = typename seq_t<VT>::V;
     constexpr int CPL = sg<S>::CPL;
     const tiles_view& A = P.A;
-    const double* __restrict__ values = static_cast<const double*>(A.values);
+    const V* __restrict__ values = static_cast<const V*>(A.values);
+    const T* __restrict__ X = static_cast<const T*>(P.x);
+    T* __restrict__ Y = static_cast<T*>(P.y);
     const int64_t t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
     const int64_t r0 = I * S;
     for (int r = lane; r < S; r += 32)
-        sm.ys[r] = (r0 + r < A.m) ? P.y[r0 + r] : 0.0;
+        sm.ys[r] = (r0 + r < A.m) ? Y[r0 + r] : T(0);
     __syncwarp();
     uint32_t n_col = A.tile_col[t0], n_z = A.tile_nnz[t0];
     uint8_t n_sch = A.tile_scheme[t0];
@@ -336,7 +378,7 @@ __device__ __forceinline__ void seq_block_row(const seq_args& P, int64_t I, seq_
         const int64_t c0 = (int64_t)n_col * S;
         const int z = (int)n_z;
         const int sch = n_sch;
-        const double* vals = values + n_vo;
+        const V* vals = values + n_vo;
         const uint8_t* pay = A.payload + n_io;
         if (t + 1 < t1) {
             n_col = A.tile_col[t + 1];
@@ -345,24 +387,24 @@ __device__ __forceinline__ void seq_block_row(const seq_args& P, int64_t I, seq_
             n_vo = A.tile_val_off[t + 1];
             n_io = A.tile_idx_off[t + 1];
         }
-        double xr[CPL];
+        T xr[CPL];
 #pragma unroll
         for (int j = 0; j < CPL; ++j) {
             const int64_t c = c0 + (S >= 32 ? 32 * j + lane : (lane & (S - 1)));
-            xr[j] = c < A.n ? __ldg(P.x + c) : 0.0;
+            xr[j] = c < A.n ? __ldg(X + c) : T(0);
         }
         if (S >= 32 && sch == ABHSF_SCHEME_BITMAP) {
             if constexpr (S >= 32)
-                seq_bitmap<S>(reinterpret_cast<const uint32_t*>(pay), vals, xr, sm, lane);
+                seq_bitmap<S, VT>(reinterpret_cast<const uint32_t*>(pay), vals, xr, sm, lane);
         } else if (S >= 32 && sch == ABHSF_SCHEME_DENSE) {
             if constexpr (S >= 32)
-                seq_dense<S>(vals, xr, c0, A.n, sm, lane);
+                seq_dense<S, VT>(vals, xr, c0, A.n, sm, lane);
         } else if (S == 16 && sch == ABHSF_SCHEME_BITMAP) {
             if constexpr (S == 16)
-                seq_16<false>(reinterpret_cast<const uint32_t*>(pay), vals, xr[0], c0, A.n, sm, lane);
+                seq_16<false, VT>(reinterpret_cast<const uint32_t*>(pay), vals, xr[0], c0, A.n, sm, lane);
         } else if (S == 16 && sch == ABHSF_SCHEME_DENSE) {
             if constexpr (S == 16)
-                seq_16<true>(nullptr, vals, xr[0], c0, A.n, sm, lane);
+                seq_16<true, VT>(nullptr, vals, xr[0], c0, A.n, sm, lane);
         } else {
 #pragma unroll
             for (int j = 0; j < CPL; ++j)
@@ -370,63 +412,74 @@ __device__ __forceinline__ void seq_block_row(const seq_args& P, int64_t I, seq_
                     sm.xs[S >= 32 ? 32 * j + lane : lane] = xr[j];
             __syncwarp();
             if (sch == ABHSF_SCHEME_CSR)
-                seq_stream<S, true>(pay, vals, z, sm, lane);
+                seq_stream<S, true, VT>(pay, vals, z, sm, lane);
             else
-                seq_stream<S, false>(pay, vals, z, sm, lane);
+                seq_stream<S, false, VT>(pay, vals, z, sm, lane);
         }
     }
     __syncwarp();
     for (int r = lane; r < S; r += 32)
         if (r0 + r < A.m)
-            P.y[r0 + r] = sm.ys[r];
+            Y[r0 + r] = sm.ys[r];
     __syncwarp();
 }
 
-template <int S>
-__global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_f64_seq(seq_args P)
+template <int S, int VT>
+__global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_seq(seq_args P)
 {
-    __shared__ seq_smem<S> smem[kWarps];
+    using T = typename seq_t<VT>::T;
+    __shared__ seq_smem<S, T> smem[kWarps];
     const int lane = threadIdx.x & 31;
-    seq_smem<S>& sm = smem[threadIdx.x >> 5];
+    seq_smem<S, T>& sm = smem[threadIdx.x >> 5];
     const unsigned int nw = gridDim.x * kWarps;
     unsigned int k = blockIdx.x * kWarps + (threadIdx.x >> 5);
     while ((int64_t)k < P.nrows) {
         unsigned int next = 0;
         if (lane == 0)
             next = atomicAdd(P.counter, 1u) + nw;  // in flight during this block row
-        seq_block_row<S>(P, (int64_t)P.rows[k], sm, lane);
+        seq_block_row<S, VT>(P, (int64_t)P.rows[k], sm, lane);
         k = __shfl_sync(kFull, next, 0);
     }
 }
 
-template <int S>
-void launch_seq(const abhsf_matrix& a, const uint32_t* rows, int64_t nrows, const double* x, double* y,
-                cudaStream_t st)
+template <int S, int VT>
+void launch_seq(const abhsf_matrix& a, const uint32_t* rows, int64_t nrows, const void* x, void* y, cudaStream_t st)
 {
     if (nrows == 0)
         return;
     int dev = 0, nsm = 0, per_sm = 0;
     ABHSF_CUDA(cudaGetDevice(&dev));
     ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_f64_seq<S>, kWarps * 32, 0));
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_seq<S, VT>, kWarps * 32, 0));
     seq_args P{a.view(), rows, nrows, a.tree_counter.get(), x, y};
     ABHSF_CUDA(cudaMemsetAsync(a.tree_counter.get(), 0, sizeof(unsigned int), st));
     const int64_t ctas = (nrows + kWarps - 1) / kWarps;
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)nsm * std::max(per_sm, 1)));
-    k_spmv_f64_seq<S><<<grid, kWarps * 32, 0, st>>>(P);
+    k_spmv_seq<S, VT><<<grid, kWarps * 32, 0, st>>>(P);
     ABHSF_CUDA(cudaGetLastError());
 }
 
-}  // namespace
+template <int VT>
+void launch_seq_vt(const abhsf_matrix& a, const uint32_t* rows, int64_t nrows, const void* x, void* y,
+                   cudaStream_t st)
+{
+    switch (a.s) {
+    case 16: launch_seq<16, VT>(a, rows, nrows, x, y, st); break;
+    case 32: launch_seq<32, VT>(a, rows, nrows, x, y, st); break;
+    case 64: launch_seq<64, VT>(a, rows, nrows, x, y, st); break;
+    case 128: launch_seq<128, VT>(a, rows, nrows, x, y, st); break;
+    case 256: launch_seq<256, VT>(a, rows, nrows, x, y, st); break;
+    default: fail(ABHSF_ERROR_UNSUPPORTED, "block size without an SpMV kernel");
+    }
+}
 
 // The streaming kernel over the block rows it serves: all of them, or those
 // the row slices leave (block sizes 16 / 128 / 256), the slices beside it.
-void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+void seq_any(const abhsf_matrix& a, const void* x, void* y, cudaStream_t st)
 {
     if (a.M == 0 || a.T == 0)
         return;
-    const bool slices = a.dc_rows > 0 && a.value_type == ABHSF_VALUE_F64 && a.sum_order == ABHSF_SUM_REFERENCE &&
-                        a.s != 32 && a.s != 64;
+    const bool slices = a.dc_rows > 0 && a.sum_order == ABHSF_SUM_REFERENCE && a.s != 32 && a.s != 64;
     std::unique_lock<std::mutex> lock(a.dc_mu, std::defer_lock);
     dc_plan p;
     const uint32_t* rows = a.tree_rows.get();
@@ -438,16 +491,30 @@ void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_
         rows = a.seq_rows.get();
         nrows = a.seq_nrows;
     }
-    switch (a.s) {
-    case 16: launch_seq<16>(a, rows, nrows, x, y, st); break;
-    case 32: launch_seq<32>(a, rows, nrows, x, y, st); break;
-    case 64: launch_seq<64>(a, rows, nrows, x, y, st); break;
-    case 128: launch_seq<128>(a, rows, nrows, x, y, st); break;
-    case 256: launch_seq<256>(a, rows, nrows, x, y, st); break;
-    default: fail(ABHSF_ERROR_UNSUPPORTED, "block size without an SpMV kernel");
-    }
+    if (a.value_type == ABHSF_VALUE_F64)
+        launch_seq_vt<ABHSF_VALUE_F64>(a, rows, nrows, x, y, st);
+    else if (a.value_type == ABHSF_VALUE_F32)
+        launch_seq_vt<ABHSF_VALUE_F32>(a, rows, nrows, x, y, st);
+    else
+        launch_seq_vt<ABHSF_VALUE_BF16>(a, rows, nrows, x, y, st);
     if (slices)
         slices_end(a, p, x, 1, y, 1, st);
+}
+
+}  // namespace
+
+void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_t st)
+{
+    if (a.value_type != ABHSF_VALUE_F64)
+        fail(ABHSF_ERROR_INVALID_VALUE, "the f64 streaming SpMV needs a matrix stored as f64");
+    seq_any(a, x, y, st);
+}
+
+void spmv_f32_seq(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st)
+{
+    if (a.value_type == ABHSF_VALUE_F64)
+        fail(ABHSF_ERROR_INVALID_VALUE, "the f32 streaming SpMV needs a matrix stored as f32 or bf16");
+    seq_any(a, x, y, st);
 }
 
 }  // namespace abhsf

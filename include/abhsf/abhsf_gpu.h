@@ -242,8 +242,7 @@ ABHSF_API abhsf_status abhsf_spmv(const abhsf_matrix* a, const double* x, double
 
 /* y += A x in f32 for a matrix stored as f32 or bf16: x[n], y[m] float in
  * device memory, values widened to f32, each product and each sum rounded to
- * f32, per row in the reference's column order.  Block sizes 32 and 64, and
- * the other sizes when every block row is in row slices (abhsf_slices_info).
+ * f32, per row in the reference's column order, at every block size.
  * The reference's f32 kernels (spmv/orig/88.cpp:204-236, value type float)
  * are the counterpart. */
 ABHSF_API abhsf_status abhsf_spmv_f32(const abhsf_matrix* a, const float* x, float* y, abhsf_stream_t stream);
@@ -259,7 +258,7 @@ ABHSF_API abhsf_status abhsf_cg(const abhsf_matrix* a, const double* b, double* 
                                 abhsf_cg_info* info, abhsf_stream_t stream);
 
 /* The same system solved in mixed precision: CG runs in f32 on a_lo (the
- * same matrix stored as f32 or bf16, block size 32 or 64) with f32 vectors;
+ * same matrix stored as f32 or bf16, any block size) with f32 vectors;
  * its solution is folded into x in FP64, and each time its residual has
  * fallen by update_factor (in (0, 1), e.g. 0.1) it is replaced by the FP64
  * residual b - A x of the f64 matrix a64 (a reliable update), the search
@@ -434,8 +433,8 @@ ABHSF_API abhsf_status abhsf_block_size_storage(const int64_t* rows, const int64
  * (bit k of candidates: size 16 << k; 0 = all five), runs one untimed and
  * then reps timed SpMVs of it on stream (x = 0, y = 0 device scratch; the
  * kernels' speed does not depend on the values) and writes the mean time per
- * SpMV in milliseconds to ms[k] (-1 for sizes not timed, and for f32 / bf16
- * values at sizes abhsf_spmv_f32 does not serve).  *best = the fastest size;
+ * SpMV in milliseconds to ms[k] (-1 for sizes not timed; abhsf_spmv_f32 for
+ * f32 / bf16 values).  *best = the fastest size;
  * out (NULL allowed) receives that size's matrix, which the caller releases.
  * Uses opts as abhsf_build does (block_size ignored).  No counterpart in the
  * reference, which chooses by storage only (block_statistics/min-bss.cpp:14-58).

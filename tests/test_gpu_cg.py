@@ -68,10 +68,11 @@ def test_cg_fp64_laplacian_3d(gpu, s):
 
 
 @pytest.mark.parametrize("vt", ["f32", "bf16"])
-def test_cg_mixed_laplacian_3d_reaches_fp64_tolerance(gpu, vt):
+@pytest.mark.parametrize("s", [16, 64, 128])
+def test_cg_mixed_laplacian_3d_reaches_fp64_tolerance(gpu, vt, s):
     coo = W.laplacian_3d(24)
     A64 = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64)
-    Alo = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=64, value_type=vt)
+    Alo = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, value_type=vt)
     b, bd, xd = _vectors(coo.n, 2)
     info = cg_mixed(A64, Alo, bd, xd, rtol=1e-10)
     assert info["converged"] and info["outer_iterations"] >= 2
