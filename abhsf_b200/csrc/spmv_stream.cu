@@ -233,22 +233,25 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kCtasPerSm) k_spmv_slices(d
         const int64_t row = (int64_t)sl.brow * S + (int64_t)(rec >> kLenBits);
         T acc = len ? Y[row * ldy] : T(0);
         uint32_t col = 0;
+        // values stay in their stored type until their product: a widening
+        // at the load would wait for the prefetch it belongs to
         uint32_t w[U];
-        T v[U];
+        V v[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             w[u] = u < len ? ld_stream(W + 32 * u) : 0u;
-            v[u] = u < len ? wide(ld_stream(Vv + 32 * u)) : T(0);
+            v[u] = u < len ? ld_stream(Vv + 32 * u) : V(0);
         }
 #pragma unroll 1
         for (int k0 = 0; k0 < (int)sl.steps; k0 += U) {
             uint32_t wn[U];
-            T vn[U], x[U];
+            V vn[U];
+            T x[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {  // the next step's words and values
                 const int k = k0 + U + u;
                 wn[u] = k < len ? ld_stream(W + 32 * k) : 0u;
-                vn[u] = k < len ? wide(ld_stream(Vv + 32 * k)) : T(0);
+                vn[u] = k < len ? ld_stream(Vv + 32 * k) : V(0);
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -258,7 +261,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kCtasPerSm) k_spmv_slices(d
 #pragma unroll
             for (int u = 0; u < U; ++u)
                 if (k0 + u < len)
-                    acc = dadd(acc, dmul(v[u], x[u]));
+                    acc = dadd(acc, dmul(wide(v[u]), x[u]));
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 w[u] = wn[u];
@@ -309,7 +312,8 @@ __global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmv_chai
         // slot j: the value and x of element 32 j + lane of the current
         // group; the word of the same element of the next group
         uint32_t wq[AH];
-        T vq[AH], xq[AH];
+        V vq[AH];  // widened at the product (see k_spmv_slices)
+        T xq[AH];
 #pragma unroll
         for (int j = 0; j < AH; ++j) {
             const int e = 32 * j + lane;
@@ -318,7 +322,7 @@ __global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmv_chai
 #pragma unroll
         for (int j = 0; j < AH; ++j) {
             const int e = 32 * j + lane;
-            vq[j] = e < len ? wide(ld_stream(Vv + e)) : T(0);
+            vq[j] = e < len ? ld_stream(Vv + e) : V(0);
             xq[j] = e < len ? __ldg(X + (int64_t)wq[j] * ldx) : T(0);
             wq[j] = e + G < len ? ld_stream(W + e + G) : 0u;
         }
@@ -331,9 +335,9 @@ __global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmv_chai
             __syncwarp();  // the previous group's products are read
 #pragma unroll
             for (int j = 0; j < AH; ++j) {
-                buf[32 * j + lane] = dmul(vq[j], xq[j]);
+                buf[32 * j + lane] = dmul(wide(vq[j]), xq[j]);
                 const int e = b0 + G + 32 * j + lane;  // the same element of the next group
-                vq[j] = wide(ld_stream(Vv + min(e, len - 1)));
+                vq[j] = ld_stream(Vv + min(e, len - 1));
                 xq[j] = __ldg(X + (int64_t)wq[j] * ldx);
                 wq[j] = ld_stream(W + min(e + G, len - 1));
             }
@@ -346,7 +350,7 @@ __global__ void __launch_bounds__(32 * kChainWarps, kChainCtasPerSm) k_spmv_chai
             __syncwarp();
 #pragma unroll
             for (int j = 0; j < AH; ++j)
-                buf[32 * j + lane] = 32 * j + lane < rem ? dmul(vq[j], xq[j]) : T(0);
+                buf[32 * j + lane] = 32 * j + lane < rem ? dmul(wide(vq[j]), xq[j]) : T(0);
             __syncwarp();
             run = add_products<G>(run, buf, rem);
         }
