@@ -24,16 +24,20 @@ void spmv_dispatch(const abhsf_matrix& a, const double* x, double* y, cudaStream
         spmv_f64(a, x, y, st);
 }
 
-// Y += A X, k columns.  The reference order for block sizes 32 / 64 runs the
-// ring kernel with several right-hand sides per pass; otherwise each column is
-// gathered into a contiguous vector, multiplied by the SpMV kernels and
-// scattered back, so column j is bitwise the SpMV of column j in every case.
+// Y += A X, k columns.  The reference order with k a multiple of 16 (block
+// sizes 16, 32, 64; X and Y 16-byte aligned with even leading dimensions)
+// runs the wide kernel, 16 or 32 columns a pass over A; for block sizes 32 /
+// 64 otherwise the ring kernel with up to 8 columns a pass; otherwise each
+// column is gathered into a contiguous vector, multiplied by the SpMV kernels
+// and scattered back, so column j is bitwise the SpMV of column j in every
+// case.
 void spmm_dispatch(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,
                    cudaStream_t st)
 {
     if (k == 0 || a.m == 0 || a.T == 0)
         return;
-    if (a.sum_order == ABHSF_SUM_REFERENCE && spmm_f64_ring(a, k, X, ldx, Y, ldy, st))
+    if (a.sum_order == ABHSF_SUM_REFERENCE && (spmm_f64_wide(a, k, X, ldx, Y, ldy, st) ||
+                                               spmm_f64_ring(a, k, X, ldx, Y, ldy, st)))
         return;
     if (k == 1 && ldx == 1 && ldy == 1) {
         spmv_dispatch(a, X, Y, st);

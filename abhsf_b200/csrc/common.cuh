@@ -206,8 +206,9 @@ struct abhsf_matrix {
     abhsf::dbuf<uint8_t> dc_sched;       // the matrix's own launch: sliced rows in warp order
     abhsf::dbuf<int64_t> dc_wbeg;
     int dc_warps = 0;
-    abhsf::dbuf<uint32_t> seq_rows;      // block sizes 16 / 128 / 256: the block rows the streaming kernel sums
-    int64_t seq_nrows = 0;               // (the others are in slices)
+    abhsf::dbuf<uint32_t> seq_rows;      // the non-empty block rows outside the slices (where there are slices):
+    int64_t seq_nrows = 0;               // the streaming kernel's (s = 16 / 128 / 256) and the wide SpMM's
+    int64_t wide_cap = 0;                // wide SpMM (spmm_wide.cu): bytes of a tile's payload and values (0: none)
     abhsf::dbuf<uint8_t> dc_csched;      // ... and its chains, launched on dc_side beside the others
     abhsf::dbuf<int64_t> dc_cwbeg;
     int dc_cwarps = 0;

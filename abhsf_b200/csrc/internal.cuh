@@ -150,6 +150,19 @@ void cg_solve_mixed(const abhsf_matrix& a64, const abhsf_matrix& a32, const doub
 // 128 and 256).
 void spmv_f32_dispatch(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st);
 void spmv_f32_seq(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st);
+// The non-empty block rows outside the slices (seq_rows; none without slices).
+void keep_rows(abhsf_matrix& a, cudaStream_t st);
+// Wide SpMM (spmm_wide.cu): sets wide_cap where the matrix can take it.
+void prepare_wide(abhsf_matrix& a, cudaStream_t st);
+// Y += A X with k a multiple of 16 columns, 16 or 32 per pass, each pass
+// reading A once (lanes as columns); false where it does not apply (value
+// type, sum order, block size, alignment of X and Y).
+bool spmm_f64_wide(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,
+                   cudaStream_t st);
+// ... its block sizes 32 and 64 (spmv_ring.cu): kt = 16 or 32 columns of X and
+// Y over the block rows given, with the ring's per-scheme sums (a row a lane).
+void spmm_staged(const abhsf_matrix& a, int kt, const uint32_t* rows, int64_t nrows, const double* X, int64_t ldx,
+                 double* Y, int64_t ldy, cudaStream_t st);
 // Y += A X (k columns, row-major X and Y) through the same kernel, several
 // right-hand sides per pass; false when the matrix has no ring schedule.
 bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,

@@ -54,6 +54,7 @@
 #include "abhsf/abhsf_test.h"
 #include "common.cuh"
 #include "internal.cuh"
+#include "spmm_stage.cuh"
 
 namespace abhsf {
 namespace {
@@ -503,6 +504,27 @@ __device__ __forceinline__ int warp_inclusive_sum(int v, int lane)
     return v;
 }
 
+// Row c of a staged x block (row stride XS), K values, as 16-byte reads where
+// the values are doubles and K is even (x blocks start 16-byte aligned, and
+// so do their rows then).
+template <int K, int XS, typename T>
+__device__ __forceinline__ void x_row(const T* xs, int c, T (&xv)[K])
+{
+    if constexpr (sizeof(T) == 8 && K % 2 == 0 && XS % 2 == 0) {
+        const double2* p = reinterpret_cast<const double2*>(xs + c * XS);
+#pragma unroll
+        for (int h = 0; h < K / 2; ++h) {
+            const double2 u = p[h];
+            xv[2 * h] = u.x;
+            xv[2 * h + 1] = u.y;
+        }
+    } else {
+#pragma unroll
+        for (int h = 0; h < K; ++h)
+            xv[h] = xs[c * XS + h];
+    }
+}
+
 // The rows a consumer lane sums: a team of NC warps covers the S rows of a
 // block row, warp wl of the team rows 32 (wl + NC i) + lane for i < RPL
 // (RPL = S / (32 NC) rows per lane).  With several rows per lane the lane's
@@ -517,7 +539,7 @@ __device__ __forceinline__ int row_of(int wl, int i, int lane)
 // Bitmap tile.  Row r's bits are u32 words r * W .. r * W + W - 1 (W = S / 32),
 // bit b of word j = column 32 j + b; a row's values start after the set bits
 // of all earlier rows.
-template <int S, int K, int VT, int NC>
+template <int S, int K, int VT, int NC, int XS = K>
 __device__ __forceinline__ void sum_bitmap(const typename val_traits<VT>::T* xs, const uint8_t* pay,
                                            const typename val_traits<VT>::V* vs,
                                            typename val_traits<VT>::T (&acc)[S / (32 * NC)][K], int wl, int lane)
@@ -582,9 +604,10 @@ __device__ __forceinline__ void sum_bitmap(const typename val_traits<VT>::T* xs,
 #pragma unroll
         for (int b = 0; b < 32; ++b) {
             T xv[K];
-#pragma unroll
-            for (int h = 0; h < K; ++h)
-                xv[h] = K == 1 ? xw[b % XW] : xs[(32 * j + b) * K + h];
+            if constexpr (K == 1)
+                xv[0] = xw[b % XW];
+            else
+                x_row<K, XS>(xs, 32 * j + b, xv);
 #pragma unroll
             for (int i = 0; i < RPL; ++i) {
                 if ((w[i][j] >> b) & 1u) {
@@ -601,7 +624,7 @@ __device__ __forceinline__ void sum_bitmap(const typename val_traits<VT>::T* xs,
 
 // Dense tile: all S * S values, row-major.  Lane l runs l columns behind
 // lane 0 so that the lanes' values fall in different banks.
-template <int S, int K, int VT, int NC>
+template <int S, int K, int VT, int NC, int XS = K>
 __device__ __forceinline__ void sum_dense(const typename val_traits<VT>::T* xs,
                                           const typename val_traits<VT>::V* vs,
                                           typename val_traits<VT>::T (&acc)[S / (32 * NC)][K], int wl, int lane)
@@ -616,9 +639,11 @@ __device__ __forceinline__ void sum_dense(const typename val_traits<VT>::T* xs,
             for (int i = 0; i < RPL; ++i) {
                 const T v = widen(vs[row_of<S, NC>(wl, i, lane) * S + c]);
                 if (v != T(0)) {  // stored zeros and the zero padding past n
+                    T xv[K];
+                    x_row<K, XS>(xs, c, xv);
 #pragma unroll
                     for (int h = 0; h < K; ++h)
-                        acc[i][h] = fadd(acc[i][h], fmul(v, xs[c * K + h]));
+                        acc[i][h] = fadd(acc[i][h], fmul(v, xv[h]));
                 }
             }
         }
@@ -629,7 +654,7 @@ __device__ __forceinline__ void sum_dense(const typename val_traits<VT>::T* xs,
 // (flagged when the descriptors are built; stencil and band diagonals): the
 // warp forms the bit set of occupied rows, and a row's element index is the
 // number of occupied rows above it.
-template <int S, int K, int VT, int NC>
+template <int S, int K, int VT, int NC, int XS = K>
 __device__ __forceinline__ void sum_distinct(const typename val_traits<VT>::T* xs, const uint8_t* pay,
                                              const typename val_traits<VT>::V* vs, int z,
                                              typename val_traits<VT>::T (&acc)[S / (32 * NC)][K], int wl, int lane)
@@ -658,9 +683,11 @@ __device__ __forceinline__ void sum_distinct(const typename val_traits<VT>::T* x
             const int k = (lower ? 0 : __popc(mlo)) + __popc(bits & ((1u << rb) - 1u));
             const int c = (int)(key16[k] & (S - 1));
             const T v = widen(vs[k]);
+            T xv[K];
+            x_row<K, XS>(xs, c, xv);
 #pragma unroll
             for (int h = 0; h < K; ++h)
-                acc[i][h] = fadd(acc[i][h], fmul(v, xs[c * K + h]));
+                acc[i][h] = fadd(acc[i][h], fmul(v, xv[h]));
         }
     }
 }
@@ -670,7 +697,7 @@ __device__ __forceinline__ void sum_distinct(const typename val_traits<VT>::T* x
 // row's range in its row_end array; a COO tile hands few products to the row
 // lanes by shuffles, or marks where each row starts and ends in the sorted
 // keys (rng: 2 S marks).
-template <int S, int K, int VT, int NC, bool CSR>
+template <int S, int K, int VT, int NC, bool CSR, int XS = K>
 __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs, const uint8_t* pay,
                                            const typename val_traits<VT>::V* vs, int z,
                                            typename val_traits<VT>::T (&acc)[S / (32 * NC)][K], uint16_t* rng,
@@ -692,9 +719,10 @@ __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs,
             vk = widen(vs[lane]);
         }
         T pk[K];
+        x_row<K, XS>(xs, ck, pk);
 #pragma unroll
         for (int h = 0; h < K; ++h)
-            pk[h] = lane < z ? fmul(vk, xs[ck * K + h]) : T(0);
+            pk[h] = lane < z ? fmul(vk, pk[h]) : T(0);
         for (int k = 0; k < z; ++k) {
             const int r = __shfl_sync(kFull, rk, k);
 #pragma unroll
@@ -755,9 +783,11 @@ __device__ __forceinline__ void sum_sparse(const typename val_traits<VT>::T* xs,
                 const int k = lo[i] + t;
                 const int c = CSR ? (int)col8[k] : (int)(key16[k] & (S - 1));
                 const T v = widen(vs[k]);
+                T xv[K];
+                x_row<K, XS>(xs, c, xv);
 #pragma unroll
                 for (int h = 0; h < K; ++h)
-                    acc[i][h] = fadd(acc[i][h], fmul(v, xs[c * K + h]));
+                    acc[i][h] = fadd(acc[i][h], fmul(v, xv[h]));
             }
         }
     }
@@ -810,6 +840,177 @@ __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot
             }
         }
     }
+}
+
+// One-pass SpMM with KT = 16 or 32 right-hand sides (FP64).  The ring's K
+// accumulators a lane do not fit its slots past K = 8, so here a CTA stages
+// whole tiles two deep instead (spmm_stage.cuh: the tile's S x KT block of X,
+// payload and values by cp.async while the previous tile is summed) and
+// splits the columns: warp w sums rows 32 (w % NC) + lane (NC = S / 32, a row
+// a lane, as the ring's one-team layout) for the KW columns KW (w / NC) ..
+// KW (w / NC) + KW - 1, with the ring's per-scheme sums over the staged block
+// (its row stride KT).  KW = 8: a CTA of 2 KT / 8 warps at s = 64 (measured
+// on the tiled mixture, k = 32: KW = 16 1.27 ms, 8 1.19 ms, 4 1.36 ms -- twice
+// the warps for the same stages against decoding each tile twice as often).
+// A tile's offsets are read a step before it is staged, and a block row's y
+// values a step before its first tile is summed.  A block row's sums stay in registers from its first
+// tile to its last; the CTA takes the block rows dealt to it round robin
+// (the list is heaviest first).  Waits: cp.async.wait_group and
+// __syncthreads only.
+template <int S, int KT, int KW>
+struct staged_cfg {
+    static constexpr int NC = S / 32;  // warps over a block row's rows
+    static constexpr int NW = NC * (KT / KW);
+    static constexpr int NT = 32 * NW;
+};
+
+struct staged_args {
+    tiles_view A;
+    const uint32_t* rows;  // block rows, heaviest first
+    int64_t nrows;
+    const double* X;
+    double* Y;
+    int64_t ldx, ldy;
+    int stage_bytes;  // X block + payload and values of the largest tile, 16-byte multiple
+};
+
+template <int S, int KT, int KW>
+__global__ void __launch_bounds__(staged_cfg<S, KT, KW>::NT) k_spmm_staged(staged_args P)
+{
+    constexpr int NC = staged_cfg<S, KT, KW>::NC, NT = staged_cfg<S, KT, KW>::NT, K = KW;
+    extern __shared__ __align__(16) uint8_t st_smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int wl = warp % NC, half = warp / NC;
+    const tiles_view& A = P.A;
+    uint16_t* rng = reinterpret_cast<uint16_t*>(st_smem + 2 * P.stage_bytes) + warp * 2 * S;
+    // the CTA's tiles in order: block rows k = blockIdx.x, + gridDim.x, ...,
+    // each block row's tiles; a position and the next one
+    struct pos {
+        int64_t k, I, t, tend;
+    };
+    auto advance = [&](const pos& p, pos& q) -> bool {  // q = the tile after p; false at the end
+        q = p;
+        ++q.t;
+        if (q.t < p.tend)
+            return true;
+        q.k = p.k + gridDim.x;
+        if (q.k >= P.nrows)
+            return false;
+        q.I = P.rows[q.k];
+        q.t = A.brow_ptr[q.I];
+        q.tend = A.brow_ptr[q.I + 1];
+        return true;
+    };
+    if ((int64_t)blockIdx.x >= P.nrows)
+        return;
+    pos p0;
+    p0.k = blockIdx.x;
+    p0.I = P.rows[p0.k];
+    p0.t = A.brow_ptr[p0.I];
+    p0.tend = A.brow_ptr[p0.I + 1];
+    stage::tile_meta m0 = stage::meta_of(A, p0.t);
+    stage::tile<S, KT, NT>(A, P.X, P.ldx, m0, st_smem, tid);
+    stage::commit();
+    // the next tile's offsets are read a step ahead, so that staging it waits on nothing
+    pos p1;
+    bool more1 = advance(p0, p1);
+    stage::tile_meta m1 = more1 ? stage::meta_of(A, p1.t) : m0;
+    const int row = row_of<S, NC>(wl, 0, lane);
+    // a block row's y values are loaded while the block row before it is
+    // summed (the rows of one block row are the same warps' lanes throughout)
+    double acc[1][K], ynext[K];
+    auto load_y = [&](int64_t brow) {
+        const int64_t r = brow * S + row;
+        if (r < A.m) {
+            const double2* yr = reinterpret_cast<const double2*>(P.Y + r * P.ldy + K * half);
+#pragma unroll
+            for (int h = 0; h < K / 2; ++h) {
+                const double2 u = yr[h];
+                ynext[2 * h] = u.x;
+                ynext[2 * h + 1] = u.y;
+            }
+        } else {
+#pragma unroll
+            for (int h = 0; h < K; ++h)
+                ynext[h] = 0.0;
+        }
+    };
+    load_y(p0.I);
+    int cur = 0;
+    bool first = true;
+#pragma unroll 1
+    for (;;) {
+        if (more1)
+            stage::tile<S, KT, NT>(A, P.X, P.ldx, m1, st_smem + (cur ^ 1) * P.stage_bytes, tid);
+        stage::commit();  // (an empty group at the end keeps the wait below uniform)
+        pos p2 = p1;
+        const bool more2 = more1 && advance(p1, p2);
+        const stage::tile_meta m2 = more2 ? stage::meta_of(A, p2.t) : m1;
+        const bool next_row = more1 && p1.k != p0.k;  // the next tile starts a block row
+        if (first) {
+#pragma unroll
+            for (int h = 0; h < K; ++h)
+                acc[0][h] = ynext[h];
+        }
+        if (next_row)
+            load_y(p1.I);
+        stage::wait_all_but_one();
+        __syncthreads();  // tile p0.t has landed
+        {
+            const uint8_t* stg = st_smem + cur * P.stage_bytes;
+            const double* xs = reinterpret_cast<const double*>(stg) + K * half;
+            const uint8_t* pay = stg + stage::x_block_bytes<S, KT>();
+            const double* vs = reinterpret_cast<const double*>(pay + m0.pb) + (m0.vo & 1);
+            switch (m0.sch) {
+            case ABHSF_SCHEME_BITMAP: sum_bitmap<S, K, ABHSF_VALUE_F64, NC, KT>(xs, pay, vs, acc, wl, lane); break;
+            case ABHSF_SCHEME_DENSE: sum_dense<S, K, ABHSF_VALUE_F64, NC, KT>(xs, vs, acc, wl, lane); break;
+            case ABHSF_SCHEME_CSR:
+                sum_sparse<S, K, ABHSF_VALUE_F64, NC, true, KT>(xs, pay, vs, m0.nv, acc, rng, wl, lane);
+                break;
+            default: sum_sparse<S, K, ABHSF_VALUE_F64, NC, false, KT>(xs, pay, vs, m0.nv, acc, rng, wl, lane); break;
+            }
+        }
+        const int64_t r = p0.I * S + row;
+        if (p0.t + 1 == p0.tend && r < A.m) {
+            double2* yr = reinterpret_cast<double2*>(P.Y + r * P.ldy + K * half);
+#pragma unroll
+            for (int h = 0; h < K / 2; ++h)
+                yr[h] = make_double2(acc[0][2 * h], acc[0][2 * h + 1]);
+        }
+        __syncthreads();  // everyone is done with this stage before it is refilled
+        if (!more1)
+            break;
+        first = next_row;
+        p0 = p1;
+        m0 = m1;
+        p1 = p2;
+        m1 = m2;
+        more1 = more2;
+        cur ^= 1;
+    }
+}
+
+template <int S, int KT, int KW>
+void launch_staged(const abhsf_matrix& a, const uint32_t* rows, int64_t nrows, const double* X, int64_t ldx,
+                   double* Y, int64_t ldy, cudaStream_t st)
+{
+    constexpr int NT = staged_cfg<S, KT, KW>::NT, NW = staged_cfg<S, KT, KW>::NW;
+    const int stage_bytes = stage::x_block_bytes<S, KT>() + (int)a.wide_cap;
+    const int smem = 2 * stage_bytes + NW * 2 * S * 2;
+    auto kern = k_spmm_staged<S, KT, KW>;
+    ABHSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ABHSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared));
+    int dev = 0, nsm = 0, per_sm = 0;
+    ABHSF_CUDA(cudaGetDevice(&dev));
+    ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+    if (per_sm < 1)
+        fail(ABHSF_ERROR_UNSUPPORTED, "staged SpMM: the stages do not fit shared memory");
+    const unsigned grid = (unsigned)std::min<int64_t>(nrows, (int64_t)nsm * per_sm);
+    staged_args P{a.view(), rows, nrows, X, Y, ldx, ldy, stage_bytes};
+    kern<<<grid, NT, smem, st>>>(P);
+    ABHSF_CUDA(cudaGetLastError());
 }
 
 // Warps 0 .. TM NC - 1 sum, NC per team; the last warp produces.
@@ -1437,6 +1638,27 @@ void batch_launch(const abhsf_batch& b, const double* const* xs, double* const* 
 
 }  // namespace
 
+// The non-empty block rows outside the slices, heaviest first (seq_rows).
+void keep_rows(abhsf_matrix& a, cudaStream_t st)
+{
+    a.seq_nrows = 0;
+    if (a.dc_rows == 0)
+        return;
+    std::vector<uint32_t> rows(a.tree_nrows), keep;
+    ABHSF_CUDA(cudaMemcpyAsync(rows.data(), a.tree_rows.get(), a.tree_nrows * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost, st));
+    ABHSF_CUDA(cudaStreamSynchronize(st));
+    for (int64_t k = 0; k < a.tree_nrows; ++k)
+        if (!a.dc_tree_flag[k])
+            keep.push_back(rows[k]);
+    a.seq_nrows = (int64_t)keep.size();
+    a.seq_rows.alloc(std::max<size_t>(keep.size(), 1));
+    if (!keep.empty())
+        ABHSF_CUDA(cudaMemcpyAsync(a.seq_rows.get(), keep.data(), keep.size() * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, st));
+    ABHSF_CUDA(cudaStreamSynchronize(st));
+}
+
 void prepare_ring(abhsf_matrix& a, cudaStream_t st)
 {
     a.ring_warps = 0;
@@ -1447,21 +1669,8 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
         // no ring kernel: the slices take the hypersparse block rows, the
         // streaming kernel (spmv_seq.cu) the rest
         prepare_stream(a, a.dc_avg, st);
-        if (a.dc_rows > 0) {
-            std::vector<uint32_t> rows(a.tree_nrows), keep;
-            ABHSF_CUDA(cudaMemcpyAsync(rows.data(), a.tree_rows.get(), a.tree_nrows * sizeof(uint32_t),
-                                       cudaMemcpyDeviceToHost, st));
-            ABHSF_CUDA(cudaStreamSynchronize(st));
-            for (int64_t k = 0; k < a.tree_nrows; ++k)
-                if (!a.dc_tree_flag[k])
-                    keep.push_back(rows[k]);
-            a.seq_nrows = (int64_t)keep.size();
-            a.seq_rows.alloc(std::max<size_t>(keep.size(), 1));
-            if (!keep.empty())
-                ABHSF_CUDA(cudaMemcpyAsync(a.seq_rows.get(), keep.data(), keep.size() * sizeof(uint32_t),
-                                           cudaMemcpyHostToDevice, st));
-            ABHSF_CUDA(cudaStreamSynchronize(st));
-        }
+        keep_rows(a, st);
+        prepare_wide(a, st);
         return;
     }
     if (a.M > (int64_t)kRowMask)
@@ -1473,6 +1682,8 @@ void prepare_ring(abhsf_matrix& a, cudaStream_t st)
             ring_set_up_all<64>();
     }
     prepare_stream(a, a.dc_avg, st);
+    keep_rows(a, st);
+    prepare_wide(a, st);
     int ctas = 0, mpv = 0;
     if (!build_ring_schedule({&a}, 32, a.ring_desc, a.ring_wbeg, ctas, mpv, st)) {
         // every block row is a slice row, or the ring's counters would overflow
@@ -1678,6 +1889,18 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
     ABHSF_CUDA(cudaEventRecord(ev[2 * kChunks + 1], a.host_out));
     ABHSF_CUDA(cudaStreamWaitEvent(st, ev[2 * kChunks + 1], 0));
     return true;
+}
+
+void spmm_staged(const abhsf_matrix& a, int kt, const uint32_t* rows, int64_t nrows, const double* X, int64_t ldx,
+                 double* Y, int64_t ldy, cudaStream_t st)
+{
+    if (a.s == 32) {
+        kt == 32 ? launch_staged<32, 32, 8>(a, rows, nrows, X, ldx, Y, ldy, st)
+                 : launch_staged<32, 16, 8>(a, rows, nrows, X, ldx, Y, ldy, st);
+    } else {
+        kt == 32 ? launch_staged<64, 32, 8>(a, rows, nrows, X, ldx, Y, ldy, st)
+                 : launch_staged<64, 16, 8>(a, rows, nrows, X, ldx, Y, ldy, st);
+    }
 }
 
 bool spmm_f64_ring(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,

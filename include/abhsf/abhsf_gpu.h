@@ -300,9 +300,11 @@ ABHSF_API abhsf_status abhsf_batch_release(abhsf_batch* b);
 /* Y += A X for k right-hand sides, X (n x k) and Y (m x k) float64 row-major
  * in device memory: element (i, j) of X at X[i * ldx + j], ldx >= k, and the
  * same for Y with ldy.  Column j of Y gets exactly what abhsf_spmv gives for
- * column j.  The matrix is read once per pass of up to 8 columns (block sizes
- * 32 and 64, reference order); otherwise the columns go through abhsf_spmv one
- * at a time.  No reference counterpart: the reference has single-vector
+ * column j.  In the reference order the matrix is read once per pass of 16
+ * or 32 columns when k is a multiple of 16, X and Y are 16-byte aligned and
+ * ldx, ldy are even (block sizes 16, 32, 64), else once per pass of up to 8
+ * columns (block sizes 32 and 64); otherwise the columns go through
+ * abhsf_spmv one at a time.  No reference counterpart: the reference has single-vector
  * SpMV only (spmv/bottlenecks/spmv.cpp:58-64); this is its multi-vector form. */
 ABHSF_API abhsf_status abhsf_spmm(const abhsf_matrix* a, int32_t k, const double* X, int64_t ldx, double* Y,
                                   int64_t ldy, abhsf_stream_t stream);

@@ -123,6 +123,34 @@ def test_spmm_wide_k_every_scheme(gpu, s, forced, k, pads):
         np.testing.assert_array_equal(Y[:, j], oracle.spmv_elements(r, c, v, X[:, j].copy(), Y0[:, j].copy()))
 
 
+@pytest.mark.parametrize("s", [16, 32, 64])
+@pytest.mark.parametrize("forced", [None, "coo", "csr", "bitmap", "dense"])
+@pytest.mark.parametrize("k,pads", [(16, (0, 0)), (32, (2, 6)), (48, (0, 2)), (64, (0, 0))])
+def test_spmm_one_pass_every_scheme(gpu, s, forced, k, pads):
+    """k a multiple of 16 with X and Y 16-byte aligned and even leading
+    dimensions: the wide kernel, 16 or 32 columns a pass with the lanes as
+    columns, ragged m and n.  Every column bitwise its SpMV."""
+    coo = W.random_blocky(1100, 1300, s, 80, seed=17)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s, forced_scheme=forced)
+    X, Y0 = _inputs(coo, k, seed=k + s + 1)
+    np.testing.assert_array_equal(_spmm(A, X, Y0, *pads), _spmv_columns(A, X, Y0))
+
+
+@pytest.mark.parametrize("s", [16, 64])
+def test_spmm_one_pass_beside_slices(gpu, s):
+    """Hypersparse and dense block rows together: the slice SpMM kernels take
+    the first, the wide kernel the rest, 32 columns in one pass."""
+    coo = W.rmat(1 << 12, 20, seed=5)
+    A = AbhsfMatrix.from_elements(coo.rows, coo.cols, coo.vals, coo.m, coo.n, block_size=s)
+    assert A.slices()["slices"] > 0
+    X, Y0 = _inputs(coo, 32, seed=s)
+    Y = _spmm(A, X, Y0)
+    np.testing.assert_array_equal(Y, _spmv_columns(A, X, Y0))
+    order = np.lexsort((coo.cols, coo.rows))
+    r, c, v = coo.rows[order], coo.cols[order], coo.vals[order]
+    np.testing.assert_array_equal(Y[:, 5], oracle.spmv_elements(r, c, v, X[:, 5].copy(), Y0[:, 5].copy()))
+
+
 def test_spmm_dense_zeros_like_the_spmv(gpu):
     """A dense tile with stored zeros (explicit zero elements among them), 32
     right-hand sides: the SpMM treats them as the SpMV does."""
