@@ -229,18 +229,20 @@ abhsf_status abhsf_batch_create(const abhsf_matrix* const* mats, int32_t count, 
                 fail(ABHSF_ERROR_INVALID_VALUE, "matrix handle is NULL");
             if (a->value_type != ABHSF_VALUE_F64)
                 fail(ABHSF_ERROR_INVALID_VALUE, "batched matrices must be stored as f64");
-            if (a->s != 32 && a->s != 64)
-                fail(ABHSF_ERROR_UNSUPPORTED, "batched matrices must have block size 32 or 64");
             if (i > 0 && a->s != mats[0]->s)
                 fail(ABHSF_ERROR_INVALID_VALUE, "batched matrices must share one block size");
-            if (a->N >= (int64_t(1) << abhsf::kBatchColBits) || a->M >= (int64_t(1) << 30))
+            if ((a->s == 32 || a->s == 64) &&
+                (a->N >= (int64_t(1) << abhsf::kBatchColBits) || a->M >= (int64_t(1) << 30)))
                 fail(ABHSF_ERROR_UNSUPPORTED, "a batched matrix has too many block rows or columns");
             b->mats.push_back(a);
             b->total_tiles += a->T;
         }
         b->s = mats[0]->s;
         ABHSF_CUDA(cudaGetDevice(&b->device));
-        abhsf::prepare_batch(*b, reinterpret_cast<cudaStream_t>(stream));
+        if (b->s == 32 || b->s == 64)
+            abhsf::prepare_batch(*b, reinterpret_cast<cudaStream_t>(stream));
+        else
+            abhsf::prepare_batch_seq(*b, reinterpret_cast<cudaStream_t>(stream));
         *out = b.release();
     });
 }
@@ -253,7 +255,10 @@ abhsf_status abhsf_batch_spmv(const abhsf_batch* b, const double* const* xs, dou
             fail(ABHSF_ERROR_INVALID_VALUE, "batch handle is NULL");
         if (!xs || !ys)
             fail(ABHSF_ERROR_INVALID_VALUE, "xs and ys must be non-NULL device arrays");
-        abhsf::batch_spmv(*b, xs, ys, reinterpret_cast<cudaStream_t>(stream));
+        if (b->s == 32 || b->s == 64)
+            abhsf::batch_spmv(*b, xs, ys, reinterpret_cast<cudaStream_t>(stream));
+        else
+            abhsf::batch_seq_spmv(*b, xs, ys, reinterpret_cast<cudaStream_t>(stream));
     });
 }
 
@@ -262,7 +267,8 @@ abhsf_status abhsf_batch_kernels(const abhsf_batch* b, int32_t* kernels)
     return guarded([&] {
         if (!b || !kernels)
             fail(ABHSF_ERROR_INVALID_VALUE, "batch handle and kernels must be non-NULL");
-        *kernels = (b->ctas > 0 ? 1 : 0) + (b->dc_warps > 0 ? 1 : 0) + (b->dc_cwarps > 0 ? 1 : 0);
+        *kernels = (b->ctas > 0 ? 1 : 0) + (b->seq_nitems > 0 ? 1 : 0) + (b->dc_warps > 0 ? 1 : 0) +
+                   (b->dc_cwarps > 0 ? 1 : 0);
     });
 }
 

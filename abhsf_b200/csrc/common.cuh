@@ -282,6 +282,12 @@ struct abhsf_batch {
     abhsf::dbuf<int64_t> wbeg;   // each CTA's range in desc
     abhsf::dbuf<uint8_t> table;  // per matrix: arrays and shape
     abhsf::dbuf<int> dev_status;
+    // block sizes 16 / 128 / 256: the streaming kernel over every matrix's
+    // block rows outside the slices, one launch (spmv_seq.cu)
+    abhsf::dbuf<uint8_t> seq_mats;  // per matrix: its tiles_view
+    abhsf::dbuf<uint2> seq_items;   // (matrix, block row), heaviest ranks first
+    int64_t seq_nitems = 0;
+    abhsf::dbuf<unsigned int> seq_counter;
     int ctas = 0;
     int layout = 0;  // consumer layout of the ring kernel (timed at creation)
     int bulk = 0;   // x / y blocks as bulk copies (timed at creation)

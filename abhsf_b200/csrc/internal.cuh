@@ -96,6 +96,10 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
 // arrays of device pointers).
 void prepare_batch(abhsf_batch& b, cudaStream_t st);
 void batch_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);
+// ... block sizes 16, 128, 256 (spmv_seq.cu): the streaming kernel over every
+// matrix's block rows outside the slices in one launch, the slices beside it.
+void prepare_batch_seq(abhsf_batch& b, cudaStream_t st);
+void batch_seq_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st);
 
 // Delta-coded row slices of the hypersparse block rows (spmv_stream.cu):
 // prepare_stream picks the block rows (no dense tile, at most `avg`

@@ -84,6 +84,12 @@ struct seq_args {
     unsigned int* counter;
     const void* x;  // T
     void* y;        // T
+    // a batch: work item k is block row items[k].y of matrix items[k].x,
+    // whose arrays are mats[i] and whose x and y are xs[i], ys[i]
+    const tiles_view* mats;
+    const uint2* items;
+    const void* const* xs;
+    void* const* ys;
 };
 
 __device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
@@ -355,16 +361,15 @@ __device__ __forceinline__ void seq_stream(const uint8_t* __restrict__ pay,
 }
 
 template <int S, int VT>
-__device__ __forceinline__ void seq_block_row(const seq_args& P, int64_t I, seq_smem<S, typename seq_t<VT>::T>& sm,
-                                              int lane)
+__device__ __forceinline__ void seq_block_row(const tiles_view& A, const void* x, void* y, int64_t I,
+                                              seq_smem<S, typename seq_t<VT>::T>& sm, int lane)
 {
     using T = typename seq_t<VT>::T;
     using V = typename seq_t<VT>::V;
     constexpr int CPL = sg<S>::CPL;
-    const tiles_view& A = P.A;
     const V* __restrict__ values = static_cast<const V*>(A.values);
-    const T* __restrict__ X = static_cast<const T*>(P.x);
-    T* __restrict__ Y = static_cast<T*>(P.y);
+    const T* __restrict__ X = static_cast<const T*>(x);
+    T* __restrict__ Y = static_cast<T*>(y);
     const int64_t t0 = A.brow_ptr[I], t1 = A.brow_ptr[I + 1];
     const int64_t r0 = I * S;
     for (int r = lane; r < S; r += 32)
@@ -424,7 +429,7 @@ __device__ __forceinline__ void seq_block_row(const seq_args& P, int64_t I, seq_
     __syncwarp();
 }
 
-template <int S, int VT>
+template <int S, int VT, bool B = false>
 __global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_seq(seq_args P)
 {
     using T = typename seq_t<VT>::T;
@@ -437,7 +442,13 @@ __global__ void __launch_bounds__(kWarps * 32, kMinCtasPerSm) k_spmv_seq(seq_arg
         unsigned int next = 0;
         if (lane == 0)
             next = atomicAdd(P.counter, 1u) + nw;  // in flight during this block row
-        seq_block_row<S, VT>(P, (int64_t)P.rows[k], sm, lane);
+        if constexpr (B) {
+            const uint2 it = P.items[k];
+            const tiles_view A = P.mats[it.x];
+            seq_block_row<S, VT>(A, P.xs[it.x], P.ys[it.x], (int64_t)it.y, sm, lane);
+        } else {
+            seq_block_row<S, VT>(P.A, P.x, P.y, (int64_t)P.rows[k], sm, lane);
+        }
         k = __shfl_sync(kFull, next, 0);
     }
 }
@@ -451,7 +462,7 @@ void launch_seq(const abhsf_matrix& a, const uint32_t* rows, int64_t nrows, cons
     ABHSF_CUDA(cudaGetDevice(&dev));
     ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_seq<S, VT>, kWarps * 32, 0));
-    seq_args P{a.view(), rows, nrows, a.tree_counter.get(), x, y};
+    seq_args P{a.view(), rows, nrows, a.tree_counter.get(), x, y, nullptr, nullptr, nullptr, nullptr};
     ABHSF_CUDA(cudaMemsetAsync(a.tree_counter.get(), 0, sizeof(unsigned int), st));
     const int64_t ctas = (nrows + kWarps - 1) / kWarps;
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)nsm * std::max(per_sm, 1)));
@@ -508,6 +519,91 @@ void spmv_f64_seq(const abhsf_matrix& a, const double* x, double* y, cudaStream_
     if (a.value_type != ABHSF_VALUE_F64)
         fail(ABHSF_ERROR_INVALID_VALUE, "the f64 streaming SpMV needs a matrix stored as f64");
     seq_any(a, x, y, st);
+}
+
+// A batch of block sizes 16 / 128 / 256: matrix i's block rows outside the
+// slices (heaviest first within a matrix) are interleaved by rank -- every
+// matrix's heaviest, then every matrix's second, ... -- so that the work
+// counter hands out the heavy block rows of all matrices first.
+void prepare_batch_seq(abhsf_batch& b, cudaStream_t st)
+{
+    std::vector<tiles_view> views;
+    std::vector<std::vector<uint32_t>> rows(b.mats.size());
+    size_t longest = 0;
+    for (size_t i = 0; i < b.mats.size(); ++i) {
+        const abhsf_matrix& a = *b.mats[i];
+        views.push_back(a.view());
+        const bool sliced = a.dc_rows > 0;
+        const int64_t nr = sliced ? a.seq_nrows : a.tree_nrows;
+        rows[i].resize((size_t)nr);
+        if (nr > 0 && a.T > 0)
+            ABHSF_CUDA(cudaMemcpyAsync(rows[i].data(), sliced ? a.seq_rows.get() : a.tree_rows.get(),
+                                       nr * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        else
+            rows[i].clear();
+        longest = std::max(longest, rows[i].size());
+    }
+    ABHSF_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint2> items;
+    for (size_t r = 0; r < longest; ++r)
+        for (size_t i = 0; i < rows.size(); ++i)
+            if (r < rows[i].size())
+                items.push_back(make_uint2((unsigned)i, rows[i][r]));
+    b.seq_mats.alloc(views.size() * sizeof(tiles_view));
+    ABHSF_CUDA(cudaMemcpyAsync(b.seq_mats.get(), views.data(), views.size() * sizeof(tiles_view),
+                               cudaMemcpyHostToDevice, st));
+    b.seq_nitems = (int64_t)items.size();
+    b.seq_items.alloc(std::max<size_t>(items.size(), 1));
+    if (!items.empty())
+        ABHSF_CUDA(cudaMemcpyAsync(b.seq_items.get(), items.data(), items.size() * sizeof(uint2),
+                                   cudaMemcpyHostToDevice, st));
+    b.seq_counter.alloc(1);
+    b.dev_status.alloc(1);
+    ABHSF_CUDA(cudaMemsetAsync(b.dev_status.get(), 0, sizeof(int), st));
+    b.ctas = 0;
+    prepare_batch_stream(b, st);
+    ABHSF_CUDA(cudaStreamSynchronize(st));
+}
+
+namespace {
+
+template <int S>
+void launch_batch_seq(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st)
+{
+    int dev = 0, nsm = 0, per_sm = 0;
+    ABHSF_CUDA(cudaGetDevice(&dev));
+    ABHSF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    auto kern = k_spmv_seq<S, ABHSF_VALUE_F64, true>;
+    ABHSF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWarps * 32, 0));
+    seq_args P{};
+    P.nrows = b.seq_nitems;
+    P.counter = b.seq_counter.get();
+    P.mats = reinterpret_cast<const tiles_view*>(b.seq_mats.get());
+    P.items = b.seq_items.get();
+    P.xs = reinterpret_cast<const void* const*>(xs);
+    P.ys = reinterpret_cast<void* const*>(ys);
+    ABHSF_CUDA(cudaMemsetAsync(b.seq_counter.get(), 0, sizeof(unsigned int), st));
+    const int64_t ctas = (b.seq_nitems + kWarps - 1) / kWarps;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ctas, (int64_t)nsm * std::max(per_sm, 1)));
+    kern<<<grid, kWarps * 32, 0, st>>>(P);
+    ABHSF_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void batch_seq_spmv(const abhsf_batch& b, const double* const* xs, double* const* ys, cudaStream_t st)
+{
+    std::lock_guard<std::mutex> lock(b.dc_mu);
+    batch_stream_begin(b, xs, ys, st);  // the chains, beside the rest
+    if (b.seq_nitems > 0) {
+        switch (b.s) {
+        case 16: launch_batch_seq<16>(b, xs, ys, st); break;
+        case 128: launch_batch_seq<128>(b, xs, ys, st); break;
+        case 256: launch_batch_seq<256>(b, xs, ys, st); break;
+        default: fail(ABHSF_ERROR_UNSUPPORTED, "the batched streaming kernel serves block sizes 16, 128, 256");
+        }
+    }
+    batch_stream_end(b, xs, ys, st);
 }
 
 void spmv_f32_seq(const abhsf_matrix& a, const float* x, float* y, cudaStream_t st)

@@ -503,8 +503,8 @@ def cg_mixed(A64: AbhsfMatrix, A_lo: AbhsfMatrix, b, x, rtol: float = 1e-10, max
 
 
 class AbhsfBatch:
-    """Several f64 matrices of one block size (32 or 64) whose SpMVs run as
-    one kernel launch (abhsf_batch_*).  Keeps the matrices alive."""
+    """Several f64 matrices of one block size whose SpMVs run as one
+    kernel launch (abhsf_batch_*).  Keeps the matrices alive."""
 
     def __init__(self, mats, stream=None):
         self._mats = list(mats)

@@ -228,16 +228,17 @@ def time_lowprec(c, dev, l2_flush, warmup, steps=10):
 def time_batched(dev, l2_flush, warmup, count=256, steps=10):
     """The batched workload (count matrices, n log-uniform [1k, 200k], half
     banded with bandwidth U[3, 64], half R-MAT(0.57, 0.19, 0.19) edge factor 8,
-    values N(0,1), generated on the GPU), block size 64: all SpMVs as one
-    launch (abhsf_batch_spmv) against one abhsf_spmv launch per matrix."""
+    values N(0,1), generated on the GPU), block size autotuned over the five
+    sizes (the batched launch timed at each): all SpMVs as one launch
+    (abhsf_batch_spmv) against one abhsf_spmv launch per matrix."""
     import torch
     from abhsf_b200 import AbhsfBatch, AbhsfMatrix
     from abhsf_b200 import workloads as W
     t0 = time.time()
-    sets = {32: [], 64: []}
-    byts = {32: 0, 64: 0}
+    sets = {s: [] for s in (16, 32, 64, 128, 256)}
+    byts = {s: 0 for s in sets}
     nnz = 0
-    fbyts = {32: 0, 64: 0}
+    fbyts = {s: 0 for s in sets}
     for rows, cols, vals, m, n, _ in W.batched_set_device(count, seed=0, device=dev):
         for s in sets:
             A = AbhsfMatrix.from_elements(rows, cols, vals, m, n, block_size=s)
@@ -267,7 +268,7 @@ def time_batched(dev, l2_flush, warmup, count=256, steps=10):
             ts.append(e0.elapsed_time(e1))
         return sum(ts) / len(ts)
 
-    # autotune the batch's block size: the one batched launch timed at each size the batched kernel serves
+    # autotune the batch's block size: the one batched launch timed at each size
     tune = {}
     for s, ms_ in sets.items():
         b_ = AbhsfBatch(ms_)

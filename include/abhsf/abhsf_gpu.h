@@ -269,8 +269,10 @@ ABHSF_API abhsf_status abhsf_cg_mixed(const abhsf_matrix* a64, const abhsf_matri
                                       double rtol, int32_t max_iters, double update_factor, int32_t max_updates,
                                       abhsf_cg_info* info, abhsf_stream_t stream);
 
-/* A batch: count f64 matrices of one block size (32 or 64), at most 4096,
- * each with fewer than 2^20 block columns, whose SpMVs run as one launch.
+/* A batch: count f64 matrices of one block size, at most 4096 (at block
+ * sizes 32 and 64 each with fewer than 2^20 block columns), whose SpMVs run
+ * as one launch: the ring kernel at 32 and 64, the streaming kernel at 16,
+ * 128 and 256.
  * The matrices stay owned by the caller and must outlive the batch.  The
  * non-empty block rows of all of them are dealt over one grid at creation.
  * No reference counterpart (the reference multiplies one matrix per call). */
@@ -288,8 +290,8 @@ ABHSF_API abhsf_status abhsf_batch_spmv(const abhsf_batch* b, const double* cons
                                         abhsf_stream_t stream);
 
 /* How many kernels one abhsf_batch_spmv launches: the tile kernel (when some
- * block row is its), the row-slice kernel and the chain kernel (when some
- * block row is in slices), 0 to 3.  No counterpart in the reference. */
+ * block row is its: ring or streaming kernel), the row-slice kernel and the
+ * chain kernel (when some block row is in slices), 0 to 3.  No counterpart in the reference. */
 ABHSF_API abhsf_status abhsf_batch_kernels(const abhsf_batch* b, int32_t* kernels);
 
 /* The batch's device status word (ABHSF_DEVSTAT_* bits), as abhsf_device_status. */

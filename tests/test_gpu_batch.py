@@ -1,5 +1,6 @@
 """GPU batches: y_i += A_i x_i for many matrices in one launch
-(abhsf_batch_spmv).  Every y_i must be bitwise what abhsf_spmv gives for that
+(abhsf_batch_spmv; the ring kernel at block sizes 32 and 64, the streaming
+kernel at 16, 128 and 256, the slices beside either).  Every y_i must be bitwise what abhsf_spmv gives for that
 matrix alone (the reference order), on consecutive calls, and when the launch
 is captured in a CUDA graph and replayed."""
 import ctypes as C
@@ -45,7 +46,7 @@ def _alone(A, x, y):
     return yy.cpu().numpy()
 
 
-@pytest.mark.parametrize("s", [32, 64])
+@pytest.mark.parametrize("s", [16, 32, 64, 128, 256])
 def test_batch_equals_each_matrix_alone_on_consecutive_calls(gpu, s):
     import torch
     coos = _mixed_set(s)
@@ -103,7 +104,10 @@ def test_batch_arguments(gpu):
 
     assert create([a64, a32]) == capi.INVALID_VALUE
     assert create([a64, f32]) == capi.INVALID_VALUE
-    assert create([a16]) == capi.UNSUPPORTED
+    assert create([a16, a16]) == capi.SUCCESS  # block size 16: the streaming kernel, one launch
+    k = C.c_int32()
+    assert capi.lib.abhsf_batch_kernels(h, C.byref(k)) == capi.SUCCESS and k.value >= 1
+    assert capi.lib.abhsf_batch_release(h) == capi.SUCCESS
     assert capi.lib.abhsf_batch_create(None, 0, None, C.byref(h)) == capi.INVALID_VALUE
     assert create([a64, a64]) == capi.SUCCESS  # the same matrix twice is allowed
     assert capi.lib.abhsf_batch_spmv(h, None, None, None) == capi.INVALID_VALUE
