@@ -853,13 +853,14 @@ __device__ __forceinline__ void sum_tile(const ring_args& P, const uint8_t* slot
 // on the tiled mixture, k = 32: KW = 16 1.27 ms, 8 1.19 ms, 4 1.36 ms -- twice
 // the warps for the same stages against decoding each tile twice as often).
 // A tile's offsets are read a step before it is staged, and a block row's y
-// values a step before its first tile is summed.  A block row's sums stay in registers from its first
-// tile to its last; the CTA takes the block rows dealt to it round robin
-// (the list is heaviest first).  Waits: cp.async.wait_group and
-// __syncthreads only.
-template <int S, int KT, int KW>
+// values a step before its first tile is summed.  A block row's sums stay
+// in registers from its first tile to its last; the CTA takes the block rows
+// dealt to it round robin (the list is heaviest first).  RPL rows a lane
+// (the ring's one-warp teams): NC = S / (32 RPL) warps cover the rows.
+// Waits: cp.async.wait_group and __syncthreads only.
+template <int S, int KT, int KW, int RPL>
 struct staged_cfg {
-    static constexpr int NC = S / 32;  // warps over a block row's rows
+    static constexpr int NC = S / (32 * RPL);  // warps over a block row's rows
     static constexpr int NW = NC * (KT / KW);
     static constexpr int NT = 32 * NW;
 };
@@ -874,10 +875,10 @@ struct staged_args {
     int stage_bytes;  // X block + payload and values of the largest tile, 16-byte multiple
 };
 
-template <int S, int KT, int KW>
-__global__ void __launch_bounds__(staged_cfg<S, KT, KW>::NT) k_spmm_staged(staged_args P)
+template <int S, int KT, int KW, int RPL>
+__global__ void __launch_bounds__(staged_cfg<S, KT, KW, RPL>::NT) k_spmm_staged(staged_args P)
 {
-    constexpr int NC = staged_cfg<S, KT, KW>::NC, NT = staged_cfg<S, KT, KW>::NT, K = KW;
+    constexpr int NC = staged_cfg<S, KT, KW, RPL>::NC, NT = staged_cfg<S, KT, KW, RPL>::NT, K = KW;
     extern __shared__ __align__(16) uint8_t st_smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int wl = warp % NC, half = warp / NC;
@@ -915,24 +916,26 @@ __global__ void __launch_bounds__(staged_cfg<S, KT, KW>::NT) k_spmm_staged(stage
     pos p1;
     bool more1 = advance(p0, p1);
     stage::tile_meta m1 = more1 ? stage::meta_of(A, p1.t) : m0;
-    const int row = row_of<S, NC>(wl, 0, lane);
     // a block row's y values are loaded while the block row before it is
     // summed (the rows of one block row are the same warps' lanes throughout)
-    double acc[1][K], ynext[K];
+    double acc[RPL][K], ynext[RPL][K];
     auto load_y = [&](int64_t brow) {
-        const int64_t r = brow * S + row;
-        if (r < A.m) {
-            const double2* yr = reinterpret_cast<const double2*>(P.Y + r * P.ldy + K * half);
 #pragma unroll
-            for (int h = 0; h < K / 2; ++h) {
-                const double2 u = yr[h];
-                ynext[2 * h] = u.x;
-                ynext[2 * h + 1] = u.y;
+        for (int i = 0; i < RPL; ++i) {
+            const int64_t r = brow * S + row_of<S, NC>(wl, i, lane);
+            if (r < A.m) {
+                const double2* yr = reinterpret_cast<const double2*>(P.Y + r * P.ldy + K * half);
+#pragma unroll
+                for (int h = 0; h < K / 2; ++h) {
+                    const double2 u = yr[h];
+                    ynext[i][2 * h] = u.x;
+                    ynext[i][2 * h + 1] = u.y;
+                }
+            } else {
+#pragma unroll
+                for (int h = 0; h < K; ++h)
+                    ynext[i][h] = 0.0;
             }
-        } else {
-#pragma unroll
-            for (int h = 0; h < K; ++h)
-                ynext[h] = 0.0;
         }
     };
     load_y(p0.I);
@@ -949,8 +952,10 @@ __global__ void __launch_bounds__(staged_cfg<S, KT, KW>::NT) k_spmm_staged(stage
         const bool next_row = more1 && p1.k != p0.k;  // the next tile starts a block row
         if (first) {
 #pragma unroll
-            for (int h = 0; h < K; ++h)
-                acc[0][h] = ynext[h];
+            for (int i = 0; i < RPL; ++i)
+#pragma unroll
+                for (int h = 0; h < K; ++h)
+                    acc[i][h] = ynext[i][h];
         }
         if (next_row)
             load_y(p1.I);
@@ -970,12 +975,17 @@ __global__ void __launch_bounds__(staged_cfg<S, KT, KW>::NT) k_spmm_staged(stage
             default: sum_sparse<S, K, ABHSF_VALUE_F64, NC, false, KT>(xs, pay, vs, m0.nv, acc, rng, wl, lane); break;
             }
         }
-        const int64_t r = p0.I * S + row;
-        if (p0.t + 1 == p0.tend && r < A.m) {
-            double2* yr = reinterpret_cast<double2*>(P.Y + r * P.ldy + K * half);
+        if (p0.t + 1 == p0.tend) {
 #pragma unroll
-            for (int h = 0; h < K / 2; ++h)
-                yr[h] = make_double2(acc[0][2 * h], acc[0][2 * h + 1]);
+            for (int i = 0; i < RPL; ++i) {
+                const int64_t r = p0.I * S + row_of<S, NC>(wl, i, lane);
+                if (r < A.m) {
+                    double2* yr = reinterpret_cast<double2*>(P.Y + r * P.ldy + K * half);
+#pragma unroll
+                    for (int h = 0; h < K / 2; ++h)
+                        yr[h] = make_double2(acc[i][2 * h], acc[i][2 * h + 1]);
+                }
+            }
         }
         __syncthreads();  // everyone is done with this stage before it is refilled
         if (!more1)
@@ -990,14 +1000,14 @@ __global__ void __launch_bounds__(staged_cfg<S, KT, KW>::NT) k_spmm_staged(stage
     }
 }
 
-template <int S, int KT, int KW>
+template <int S, int KT, int KW, int RPL>
 void launch_staged(const abhsf_matrix& a, const uint32_t* rows, int64_t nrows, const double* X, int64_t ldx,
                    double* Y, int64_t ldy, cudaStream_t st)
 {
-    constexpr int NT = staged_cfg<S, KT, KW>::NT, NW = staged_cfg<S, KT, KW>::NW;
+    constexpr int NT = staged_cfg<S, KT, KW, RPL>::NT, NW = staged_cfg<S, KT, KW, RPL>::NW;
     const int stage_bytes = stage::x_block_bytes<S, KT>() + (int)a.wide_cap;
     const int smem = 2 * stage_bytes + NW * 2 * S * 2;
-    auto kern = k_spmm_staged<S, KT, KW>;
+    auto kern = k_spmm_staged<S, KT, KW, RPL>;
     ABHSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     ABHSF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                     (int)cudaSharedmemCarveoutMaxShared));
@@ -1894,12 +1904,16 @@ bool spmv_f64_ring_host(abhsf_matrix& a, const double* x, double* y, cudaStream_
 void spmm_staged(const abhsf_matrix& a, int kt, const uint32_t* rows, int64_t nrows, const double* X, int64_t ldx,
                  double* Y, int64_t ldy, cudaStream_t st)
 {
+    // 16 columns: 4 a warp, so that a CTA keeps as many warps as at 32 (tiled
+    // mixture, 16 columns: 0.76 ms with 8 a warp, 0.75 with 4).  Two rows a
+    // lane (RPL = 2, each x row read once for the 64 rows) measured 1.31 ms
+    // at 32 columns against 1.07 with one: fewer warps for the same stages.
     if (a.s == 32) {
-        kt == 32 ? launch_staged<32, 32, 8>(a, rows, nrows, X, ldx, Y, ldy, st)
-                 : launch_staged<32, 16, 8>(a, rows, nrows, X, ldx, Y, ldy, st);
+        kt == 32 ? launch_staged<32, 32, 8, 1>(a, rows, nrows, X, ldx, Y, ldy, st)
+                 : launch_staged<32, 16, 4, 1>(a, rows, nrows, X, ldx, Y, ldy, st);
     } else {
-        kt == 32 ? launch_staged<64, 32, 8>(a, rows, nrows, X, ldx, Y, ldy, st)
-                 : launch_staged<64, 16, 8>(a, rows, nrows, X, ldx, Y, ldy, st);
+        kt == 32 ? launch_staged<64, 32, 8, 1>(a, rows, nrows, X, ldx, Y, ldy, st)
+                 : launch_staged<64, 16, 4, 1>(a, rows, nrows, X, ldx, Y, ldy, st);
     }
 }
 
