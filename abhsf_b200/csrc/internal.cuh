@@ -159,8 +159,9 @@ void keep_rows(abhsf_matrix& a, cudaStream_t st);
 // Wide SpMM (spmm_wide.cu): sets wide_cap where the matrix can take it.
 void prepare_wide(abhsf_matrix& a, cudaStream_t st);
 // Y += A X with k a multiple of 16 columns, 16 or 32 per pass, each pass
-// reading A once (lanes as columns); false where it does not apply (value
-// type, sum order, block size, alignment of X and Y).
+// reading A once (block sizes 32 / 64: spmm_staged below; 16: lanes as
+// columns); false where it does not apply (value type, sum order, block
+// size, alignment of X and Y).
 bool spmm_f64_wide(const abhsf_matrix& a, int k, const double* X, int64_t ldx, double* Y, int64_t ldy,
                    cudaStream_t st);
 // ... its block sizes 32 and 64 (spmv_ring.cu): kt = 16 or 32 columns of X and

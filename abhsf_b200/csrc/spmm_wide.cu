@@ -44,7 +44,7 @@ constexpr int kWideThreads = 32 * kWideWarps;
 template <int S>
 constexpr int wide_min_ctas()
 {
-    return S == 64 ? 2 : 4;
+    return S >= 64 ? 2 : 4;
 }
 
 using stage::x_block_bytes;
@@ -302,17 +302,6 @@ void launch_wide(const abhsf_matrix& a, const uint32_t* rows, int64_t nrows, con
     ABHSF_CUDA(cudaGetLastError());
 }
 
-template <int K>
-void launch_wide_s(const abhsf_matrix& a, const uint32_t* rows, int64_t nrows, const double* X, int64_t ldx,
-                   double* Y, int64_t ldy, cudaStream_t st)
-{
-    switch (a.s) {
-    case 16: launch_wide<16, K>(a, rows, nrows, X, ldx, Y, ldy, st); break;
-    case 32: launch_wide<32, K>(a, rows, nrows, X, ldx, Y, ldy, st); break;
-    default: launch_wide<64, K>(a, rows, nrows, X, ldx, Y, ldy, st); break;
-    }
-}
-
 }  // namespace
 
 void prepare_wide(abhsf_matrix& a, cudaStream_t st)
@@ -332,7 +321,8 @@ void prepare_wide(abhsf_matrix& a, cudaStream_t st)
     // the values start up to 8 bytes into their first granule and end on a whole one
     const int64_t cap = (int64_t)((h + 15) & ~15ull) + 16;
     const int64_t x32 = (int64_t)a.s * 32 * 8;
-    if (2 * (x32 + cap) + kWideWarps * 2 * (a.s / kWideWarps) * 2 > 232448)  // 227 KiB a CTA
+    // two stages and each warp's COO marks (at most 8 warps of 2 s marks of 2 bytes) in 227 KiB
+    if (2 * (x32 + cap) + 8 * 2 * a.s * 2 > 232448)
         return;
     a.wide_cap = cap;
 }
@@ -353,9 +343,9 @@ bool spmm_f64_wide(const abhsf_matrix& a, int k, const double* X, int64_t ldx, d
         if (nrows > 0 && (a.s == 32 || a.s == 64))
             spmm_staged(a, cols, rows, nrows, X + j, ldx, Y + j, ldy, st);
         else if (nrows > 0 && cols == 32)
-            launch_wide_s<32>(a, rows, nrows, X + j, ldx, Y + j, ldy, st);
+            launch_wide<16, 32>(a, rows, nrows, X + j, ldx, Y + j, ldy, st);
         else if (nrows > 0)
-            launch_wide_s<16>(a, rows, nrows, X + j, ldx, Y + j, ldy, st);
+            launch_wide<16, 16>(a, rows, nrows, X + j, ldx, Y + j, ldy, st);
         if (sliced) {
             slices_begin(a, p, X + j, ldx, Y + j, ldy, st, cols);
             slices_end(a, p, X + j, ldx, Y + j, ldy, st, cols);
